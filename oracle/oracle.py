@@ -1,0 +1,295 @@
+"""ctypes front-end of the CPU oracle (liboracle.so) and of the reference shim (_ref/libapg_ref.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and bench.py's CPU
+baseline leg, always as the checker or the timed CPU baseline, never as the product path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ORACLE_SO = HERE / "liboracle.so"
+REF_SO = HERE / "_ref" / "libapg_ref.so"
+
+FAST, BALANCED, HIGH_QUALITY = 0, 1, 2
+
+
+class PipelineConfig(C.Structure):
+    """ctypes mirror of apg_pipeline_config_t (include/apg_sgm/pipeline_config.h)."""
+
+    _fields_ = [
+        ("mode", C.c_int), ("min_disparity", C.c_int), ("max_disparity", C.c_int),
+        ("num_threads", C.c_int), ("volume_backend", C.c_int),
+        ("census_type", C.c_int),
+        ("lambda_census", C.c_float), ("lambda_ad", C.c_float), ("lambda_grad", C.c_float),
+        ("eta_ad", C.c_float), ("mu_grad", C.c_float),
+        ("use_ad", C.c_int), ("use_grad", C.c_int), ("cost_max", C.c_int),
+        ("agg_enable", C.c_int), ("max_arm_length", C.c_int), ("color_threshold", C.c_int),
+        ("agg_iterations", C.c_int),
+        ("paths", C.c_int), ("P1", C.c_int), ("P2_base", C.c_int), ("adaptive_penalties", C.c_int),
+        ("grad_t1", C.c_int), ("grad_t2", C.c_int), ("p2_alpha", C.c_float), ("piecewise_p2", C.c_int),
+        ("prior_enable", C.c_int), ("prior_uniqueness_ratio", C.c_float),
+        ("prior_texture_threshold", C.c_int), ("prior_lr_max_diff", C.c_int),
+        ("prior_search_radius", C.c_int), ("prior_min_supports", C.c_int),
+        ("prior_max_supports", C.c_int),
+        ("conf_uniqueness_ratio", C.c_float), ("conf_lr_max_diff", C.c_int),
+        ("conf_min_texture", C.c_float), ("conf_reliable_threshold", C.c_float),
+        ("refine_enable", C.c_int), ("refine_iterations", C.c_int), ("refine_random_radius", C.c_int),
+        ("subpixel", C.c_int), ("lr_check", C.c_int), ("post_lr_max_diff", C.c_int),
+        ("median_radius", C.c_int), ("max_fill_gap", C.c_int),
+    ]
+
+    def copy(self) -> "PipelineConfig":
+        c = PipelineConfig()
+        C.pointer(c)[0] = self
+        return c
+
+    @property
+    def D(self) -> int:
+        return self.max_disparity - self.min_disparity
+
+
+_orc = None
+_ref = None
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def lib():
+    global _orc
+    if _orc is None:
+        if not ORACLE_SO.exists():
+            raise RuntimeError(f"oracle library missing: {ORACLE_SO} (run make -C oracle oracle)")
+        _orc = C.CDLL(str(ORACLE_SO))
+        _orc.orc_fnv1a64.restype = C.c_uint64
+        _orc.orc_refine_count.restype = C.c_int
+        _orc.orc_extract_supports.restype = C.c_int
+        _orc.orc_rng_create.restype = C.c_void_p
+        _orc.orc_rng_create.argtypes = [C.c_uint32]
+        _orc.orc_rng_destroy.argtypes = [C.c_void_p]
+        _orc.orc_rng_draws.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p]
+    return _orc
+
+
+def ref_available() -> bool:
+    return REF_SO.exists()
+
+
+def ref_lib():
+    global _ref
+    if _ref is None:
+        if not REF_SO.exists():
+            raise RuntimeError(f"reference library missing: {REF_SO} (run make -C oracle ref)")
+        _ref = C.CDLL(str(REF_SO))
+        _ref.ref_session_create.restype = C.c_void_p
+        _ref.ref_session_create.argtypes = [C.POINTER(PipelineConfig), C.c_int]
+        _ref.ref_session_destroy.argtypes = [C.c_void_p]
+        _ref.ref_session_process.argtypes = [C.c_void_p] + [C.c_void_p] * 2 + [C.c_int] * 4 + [C.c_void_p] * 5
+        _ref.ref_max_threads.restype = C.c_int
+    return _ref
+
+
+def config(mode: int, max_disparity: int = 128, min_disparity: int = 0, **kw) -> PipelineConfig:
+    """PipelineConfig::from_mode(mode, max_disparity) (src/config.cpp:5-45) plus overrides."""
+    c = PipelineConfig()
+    lib().orc_config_from_mode(C.c_int(mode), C.c_int(max_disparity), C.byref(c))
+    c.min_disparity = min_disparity
+    for k, v in kw.items():
+        if not hasattr(c, k):
+            raise AttributeError(k)
+        setattr(c, k, v)
+    return c
+
+
+def fnv1a64(a: np.ndarray) -> int:
+    a = np.ascontiguousarray(a)
+    return int(lib().orc_fnv1a64(_p(a), C.c_uint64(a.nbytes)))
+
+
+def _as_u8(img):
+    img = np.asarray(img)
+    assert img.dtype == np.uint8
+    return img
+
+
+def _view(img):
+    """(contiguous-rows array, w, h, stride, channels) of an HxW or HxWxC uint8 array."""
+    img = _as_u8(img)
+    h, w = img.shape[:2]
+    ch = 1 if img.ndim == 2 else img.shape[2]
+    if not (img.strides[-1] == 1 and (img.ndim == 2 or img.strides[1] == ch)):
+        img = np.ascontiguousarray(img)
+    stride = img.strides[0]
+    return img, w, h, stride, ch
+
+
+class _OrcStages(C.Structure):
+    _fields_ = [(k, C.c_void_p) for k in ("disp_wta", "best", "second", "disp_right", "disp_refined",
+                                          "disp_lr", "disp_fill", "cost_raw", "cost_agg", "sgm_sum",
+                                          "range_min", "range_max", "d_prior")] + [("support_count", C.c_int)]
+
+
+def pipeline(cfg: PipelineConfig, left, right, stages: bool = False) -> dict:
+    """Oracle whole-pipeline run (Dense semantics).  Returns final outputs and, optionally,
+    every intermediate of orc_stages_t."""
+    L, w, h, stride, ch = _view(left)
+    R, _, _, _, _ = _view(right)
+    D = cfg.D
+    out = {
+        "disparity": np.empty((h, w), np.float32), "confidence": np.empty((h, w), np.float32),
+        "invalid_reason": np.empty((h, w), np.uint8), "reliable_mask": np.empty((h, w), np.uint8),
+    }
+    st = None
+    if stages:
+        out.update({
+            "disp_wta": np.empty((h, w), np.float32), "best": np.empty((h, w), np.float32),
+            "second": np.empty((h, w), np.float32), "disp_right": np.empty((h, w), np.float32),
+            "disp_refined": np.empty((h, w), np.float32), "disp_lr": np.empty((h, w), np.float32),
+            "disp_fill": np.empty((h, w), np.float32),
+            "cost_raw": np.empty((h, w, D), np.uint16), "cost_agg": np.empty((h, w, D), np.uint16),
+            "sgm_sum": np.empty((h, w, D), np.uint32),
+            "range_min": np.empty((h, w), np.int16), "range_max": np.empty((h, w), np.int16),
+            "d_prior": np.empty((h, w), np.float32),
+        })
+        st = _OrcStages()
+        for k, _ in _OrcStages._fields_[:-1]:
+            setattr(st, k, out[k].ctypes.data)
+    rc = lib().orc_pipeline(C.byref(cfg), _p(L), _p(R), w, h, stride, ch,
+                            _p(out["disparity"]), _p(out["confidence"]), _p(out["invalid_reason"]),
+                            _p(out["reliable_mask"]), C.byref(st) if stages else None)
+    if stages:
+        out["support_count"] = st.support_count
+    out["status"] = rc
+    return out
+
+
+def aux(left, right):
+    """gray, gx, gy, census(sym) of both images (oracle)."""
+    res = {}
+    for side, img in (("left", left), ("right", right)):
+        I, w, h, stride, ch = _view(img)
+        g = np.empty((h, w), np.uint8); gx = np.empty_like(g); gy = np.empty_like(g)
+        lib().orc_gray_grad(_p(I), w, h, stride, ch, _p(g), _p(gx), _p(gy))
+        cs = np.empty((h, w), np.uint32)
+        lib().orc_census_sym(_p(g), w, h, _p(cs))
+        c64 = np.empty((h, w), np.uint64)
+        lib().orc_census64(_p(g), w, h, _p(c64))
+        res[side] = {"gray": g, "gx": gx, "gy": gy, "census": cs, "census64": c64}
+    return res
+
+
+def sgm_path(cfg: PipelineConfig, gray, vol, acc, dx, dy):
+    h, w, D = vol.shape
+    lib().orc_sgm_path(C.byref(cfg), _p(gray), _p(vol), _p(acc), w, h, D, dx, dy)
+
+
+def wta(cfg: PipelineConfig, acc, rmin, rmax):
+    h, w, _ = acc.shape
+    disp = np.empty((h, w), np.float32); best = np.empty_like(disp); second = np.empty_like(disp)
+    lib().orc_wta(C.byref(cfg), _p(acc), _p(rmin), _p(rmax), w, h, _p(disp), _p(best), _p(second))
+    return disp, best, second
+
+
+def rng_draws(seed: int, plan):
+    """Concatenated draws of std::uniform_int_distribution(-r, r) over one mt19937(seed) for a
+    list of (radius, count) pairs."""
+    L = lib()
+    h = L.orc_rng_create(C.c_uint32(seed))
+    try:
+        outs = []
+        for r, n in plan:
+            a = np.empty(max(n, 1), np.int32)
+            L.orc_rng_draws(h, int(r), int(n), _p(a))
+            outs.append(a[:n])
+        return outs
+    finally:
+        L.orc_rng_destroy(h)
+
+
+# ----------------------------------------------------------------------------------------------
+# Reference (oracle/_ref) front-end
+# ----------------------------------------------------------------------------------------------
+
+_DUMP_FIELDS = [
+    ("left_gray", np.uint8, 2), ("left_gx", np.uint8, 2), ("left_gy", np.uint8, 2),
+    ("right_gray", np.uint8, 2), ("right_gx", np.uint8, 2), ("right_gy", np.uint8, 2),
+    ("census_left", np.uint32, 2), ("census_right", np.uint32, 2),
+    ("census_left64", np.uint64, 2), ("census_right64", np.uint64, 2),
+    ("range_min", np.int16, 2), ("range_max", np.int16, 2),
+    ("cost_raw", np.uint16, 3), ("cost_agg", np.uint16, 3), ("sgm_sum", np.uint32, 3),
+    ("disp_wta", np.float32, 2), ("best", np.float32, 2), ("second", np.float32, 2),
+    ("disp_right", np.float32, 2),
+    ("conf_confidence", np.float32, 2), ("conf_reliable", np.uint8, 2), ("conf_reason", np.uint8, 2),
+    ("d_prior", np.float32, 2), ("disp_refined", np.float32, 2),
+    ("disp_lr", np.float32, 2), ("reason_lr", np.uint8, 2), ("disp_fill", np.float32, 2),
+    ("disparity", np.float32, 2), ("confidence", np.float32, 2),
+    ("invalid_reason", np.uint8, 2), ("reliable_mask", np.uint8, 2),
+]
+_DUMP_TAIL = [("prior_conf", np.float32, 2), ("prior_spread", np.float32, 2),
+              ("prior_dmin", np.float32, 2), ("prior_dmax", np.float32, 2)]
+
+
+class _RefDump(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n, _, _ in _DUMP_FIELDS] + [("support_count", C.c_int)] + \
+               [(n, C.c_void_p) for n, _, _ in _DUMP_TAIL]
+
+
+def ref_dump(cfg: PipelineConfig, left, right) -> dict:
+    """Every stage output of the reference Dense pipeline on (left, right)."""
+    L, w, h, stride, ch = _view(left)
+    R, _, _, _, _ = _view(right)
+    D = cfg.D
+    out, d = {}, _RefDump()
+    sym = cfg.census_type == 1
+    for name, dt, nd in _DUMP_FIELDS + _DUMP_TAIL:
+        if name.endswith("64") and sym or (name in ("census_left", "census_right") and not sym):
+            continue
+        a = np.zeros((h, w, D) if nd == 3 else (h, w), dt)
+        out[name] = a
+        setattr(d, name, a.ctypes.data)
+    rc = ref_lib().ref_dump(C.byref(cfg), _p(L), _p(R), w, h, stride, ch, C.byref(d))
+    out["status"] = rc
+    out["support_count"] = d.support_count
+    return out
+
+
+class RefSession:
+    """The reference's public StereoSession (BoundedReuse) for timing its CPU path."""
+
+    def __init__(self, cfg: PipelineConfig, bounded_reuse: bool = True):
+        self._h = ref_lib().ref_session_create(C.byref(cfg), 1 if bounded_reuse else 0)
+
+    def process(self, left, right, want_stages=False):
+        L, w, h, stride, ch = _view(left)
+        R, _, _, _, _ = _view(right)
+        out = {"disparity": np.empty((h, w), np.float32), "confidence": np.empty((h, w), np.float32),
+               "invalid_reason": np.empty((h, w), np.uint8), "reliable_mask": np.empty((h, w), np.uint8)}
+        st = np.zeros(11, np.float64)
+        rc = ref_lib().ref_session_process(self._h, _p(L), _p(R), w, h, stride, ch,
+                                           _p(out["disparity"]), _p(out["confidence"]),
+                                           _p(out["invalid_reason"]), _p(out["reliable_mask"]), _p(st))
+        out["status"] = rc
+        out["stage_ms"] = dict(zip(["aux", "prior", "cost", "cross", "right_wta", "sgm", "wta",
+                                    "confidence", "refine", "post", "total"], st.tolist()))
+        return out
+
+    def close(self):
+        if self._h:
+            ref_lib().ref_session_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def ref_threads() -> int:
+    return int(ref_lib().ref_max_threads())

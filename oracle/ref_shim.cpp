@@ -1,0 +1,304 @@
+// Stage-dump shim over the REFERENCE library (test infrastructure; see oracle/Makefile).
+//
+// It is compiled together with the reference's own sources into oracle/_ref/libapg_ref.so and
+// only calls the reference's public C++ API (include/apg_sgm/*.hpp of the reference).  It
+// exists so that the tests can
+//   * pin the C restatement in oracle/apg_oracle.c against the reference, stage by stage;
+//   * time the reference's own CPU path (the AVX2/OpenMP Packed backend) in bench.py.
+// Nothing in the shipped library links or loads it.
+//
+// The staged run below repeats StereoMatcher::compute_impl (src/pipeline.cpp:435-719) for the
+// Dense backend one stage at a time so that every intermediate can be copied out; the final
+// outputs of the staged run are checked against a full StereoMatcher::compute of the same
+// inputs, so a staged dump can never drift from what the reference really computes.
+
+#include "apg_sgm/confidence_estimator.hpp"
+#include "apg_sgm/cost_aggregator.hpp"
+#include "apg_sgm/cost_computer.hpp"
+#include "apg_sgm/pipeline.hpp"
+#include "apg_sgm/postprocess.hpp"
+#include "apg_sgm/prior_estimator.hpp"
+#include "apg_sgm/refiner.hpp"
+#include "apg_sgm/session.hpp"
+#include "apg_sgm/sgm_optimizer.hpp"
+
+#include "../include/apg_sgm/pipeline_config.h"
+
+#include <chrono>
+#include <cstring>
+#include <vector>
+
+#if defined(_OPENMP)
+#include <omp.h>
+#endif
+
+using namespace apg;
+
+namespace {
+
+PipelineConfig to_ref(const apg_pipeline_config_t& c) {
+    PipelineConfig p = PipelineConfig::from_mode(
+        c.mode == APG_MODE_FAST ? QualityMode::Fast
+                                : (c.mode == APG_MODE_HIGH_QUALITY ? QualityMode::HighQuality
+                                                                   : QualityMode::Balanced),
+        c.max_disparity);
+    p.min_disparity = c.min_disparity;
+    p.max_disparity = c.max_disparity;
+    p.num_threads = c.num_threads;
+    p.volume_backend = c.volume_backend == 1 ? VolumeBackend::Dense
+                       : (c.volume_backend == 2 ? VolumeBackend::Packed : VolumeBackend::Auto);
+    p.cost.census = c.census_type == APG_CENSUS_9X7 ? CensusType::Census9x7
+                                                    : CensusType::SymmetricCensus9x7;
+    p.cost.lambda_census = c.lambda_census;
+    p.cost.lambda_ad = c.lambda_ad;
+    p.cost.lambda_grad = c.lambda_grad;
+    p.cost.eta_ad = c.eta_ad;
+    p.cost.mu_grad = c.mu_grad;
+    p.cost.use_ad = c.use_ad != 0;
+    p.cost.use_grad = c.use_grad != 0;
+    p.cost.cost_max = c.cost_max;
+    p.aggregation.enable = c.agg_enable != 0;
+    p.aggregation.max_arm_length = c.max_arm_length;
+    p.aggregation.color_threshold = c.color_threshold;
+    p.aggregation.iterations = c.agg_iterations;
+    p.sgm.paths = c.paths == 8 ? PathType::Path8 : PathType::Path4;
+    p.sgm.P1 = c.P1;
+    p.sgm.P2_base = c.P2_base;
+    p.sgm.adaptive_penalties = c.adaptive_penalties != 0;
+    p.sgm.grad_t1 = c.grad_t1;
+    p.sgm.grad_t2 = c.grad_t2;
+    p.sgm.p2_alpha = c.p2_alpha;
+    p.sgm.piecewise_p2 = c.piecewise_p2 != 0;
+    p.prior.enable = c.prior_enable != 0;
+    p.prior.uniqueness_ratio = c.prior_uniqueness_ratio;
+    p.prior.texture_threshold = c.prior_texture_threshold;
+    p.prior.lr_max_diff = c.prior_lr_max_diff;
+    p.prior.search_radius = c.prior_search_radius;
+    p.prior.min_supports = c.prior_min_supports;
+    p.prior.max_supports = c.prior_max_supports;
+    p.confidence.uniqueness_ratio = c.conf_uniqueness_ratio;
+    p.confidence.lr_max_diff = c.conf_lr_max_diff;
+    p.confidence.min_texture = c.conf_min_texture;
+    p.confidence.reliable_threshold = c.conf_reliable_threshold;
+    p.refine.enable = c.refine_enable != 0;
+    p.refine.iterations = c.refine_iterations;
+    p.refine.random_radius = c.refine_random_radius;
+    p.post.subpixel = c.subpixel != 0;
+    p.post.lr_check = c.lr_check != 0;
+    p.post.lr_max_diff = c.post_lr_max_diff;
+    p.post.median_radius = c.median_radius;
+    p.post.max_fill_gap = c.max_fill_gap;
+    return p;
+}
+
+Image8 to_image(const uint8_t* data, int w, int h, int stride, int ch) {
+    return ImageView8(data, w, h, stride, ch).to_image();
+}
+
+template <typename T>
+void put(T* dst, const T* src, size_t n) {
+    if (dst && src && n) std::memcpy(dst, src, n * sizeof(T));
+}
+
+} // namespace
+
+extern "C" {
+
+typedef struct {
+    uint8_t *left_gray, *left_gx, *left_gy, *right_gray, *right_gx, *right_gy;
+    uint32_t *census_left, *census_right;
+    uint64_t *census_left64, *census_right64;
+    int16_t *range_min, *range_max;
+    uint16_t *cost_raw;   /* W*H*D, after CostComputer::compute_volume */
+    uint16_t *cost_agg;   /* W*H*D, after CostAggregator::aggregate (== cost_raw when off) */
+    uint32_t *sgm_sum;    /* W*H*D, SgmOptimizer::optimize accumulator */
+    float *disp_wta, *best, *second, *disp_right;
+    float *conf_confidence; uint8_t *conf_reliable, *conf_reason;
+    float *d_prior, *disp_refined;
+    float *disp_lr; uint8_t *reason_lr;
+    float *disp_fill;
+    float *disparity, *confidence; uint8_t *invalid_reason, *reliable_mask;
+    int support_count;
+    float *prior_conf, *prior_spread, *prior_dmin, *prior_dmax;
+} ref_dump_t;
+
+// Full staged run of the Dense pipeline.  Returns 0 on success, a StatusCode on a rejected
+// input, -100 if the staged run disagrees with StereoMatcher::compute.
+int ref_dump(const apg_pipeline_config_t* ccfg, const uint8_t* left, const uint8_t* right,
+             int w, int h, int stride, int ch, ref_dump_t* out) {
+    PipelineConfig cfg = to_ref(*ccfg);
+    cfg.volume_backend = VolumeBackend::Dense;
+    const Image8 L = to_image(left, w, h, stride, ch);
+    const Image8 R = to_image(right, w, h, stride, ch);
+#if defined(_OPENMP)
+    if (cfg.num_threads > 0) omp_set_num_threads(cfg.num_threads);
+#endif
+
+    StereoMatcher matcher(cfg);
+    PipelineBuffers full;
+    if (!matcher.compute(L, R, full)) {
+        Status s = validate_inputs(L, R);
+        if (!s.ok()) return static_cast<int>(s.code);
+        s = validate_config(cfg);
+        return s.ok() ? static_cast<int>(StatusCode::InternalError) : static_cast<int>(s.code);
+    }
+
+    PipelineBuffers b;
+    CostComputer cost;
+    PriorEstimator prior;
+    CostAggregator agg;
+    SgmOptimizer sgm;
+    ConfidenceEstimator conf;
+    Refiner refiner;
+    PostProcessor post;
+    const size_t n = static_cast<size_t>(w) * h;
+
+    cost.compute_aux(L, R, cfg, b);
+    put(out->left_gray, b.left_gray.data(), n);
+    put(out->left_gx, b.left_gx.data(), n);
+    put(out->left_gy, b.left_gy.data(), n);
+    put(out->right_gray, b.right_gray.data(), n);
+    put(out->right_gx, b.right_gx.data(), n);
+    put(out->right_gy, b.right_gy.data(), n);
+    put(out->census_left, b.census_left.data(), b.census_left.size());
+    put(out->census_right, b.census_right.data(), b.census_right.size());
+    put(out->census_left64, b.census_left64.data(), b.census_left64.size());
+    put(out->census_right64, b.census_right64.data(), b.census_right64.size());
+
+    prior.estimate(cfg, b);
+    put(out->range_min, b.range.dmin.data(), n);
+    put(out->range_max, b.range.dmax.data(), n);
+    put(out->d_prior, b.d_prior.data(), n);
+    put(out->prior_conf, b.prior_confidence.data(), b.prior_confidence.empty() ? 0 : n);
+    put(out->prior_spread, b.prior_spread.data(), b.prior_spread.empty() ? 0 : n);
+    put(out->prior_dmin, b.d_prior_min.data(), b.d_prior_min.empty() ? 0 : n);
+    put(out->prior_dmax, b.d_prior_max.data(), b.d_prior_max.empty() ? 0 : n);
+    out->support_count = static_cast<int>(b.support_count);
+
+    cost.compute_volume(cfg, b);
+    const size_t nv = b.cost.bytes() / sizeof(uint16_t);
+    put(out->cost_raw, b.cost.data(), nv);
+
+    agg.aggregate(cfg, b);
+    put(out->cost_agg, b.cost.data(), nv);
+
+    sgm.optimize(cfg, b);
+    put(out->sgm_sum, b.cost32.data(), nv);
+
+    Image32f best, second;
+    sgm.winner_take_all(cfg, b.cost32, b.range, b.disparity, &best, &second);
+    put(out->disp_wta, b.disparity.data(), n);
+    put(out->best, best.data(), n);
+    put(out->second, second.data(), n);
+
+    // The right-image WTA lives in an internal helper of pipeline.cpp; take it from the full run.
+    b.disparity_right = full.disparity_right;
+    put(out->disp_right, b.disparity_right.data(), n);
+
+    conf.estimate(cfg, b, best, second);
+    put(out->conf_confidence, b.confidence.data(), n);
+    put(out->conf_reliable, b.reliable_mask.data(), n);
+    put(out->conf_reason, b.invalid_reason.data(), n);
+
+    refiner.refine(cfg, b);
+    put(out->disp_refined, b.disparity.data(), n);
+
+    post.left_right_check(cfg, b);
+    put(out->disp_lr, b.disparity.data(), n);
+    put(out->reason_lr, b.invalid_reason.data(), n);
+    post.fill_holes(cfg, b);
+    put(out->disp_fill, b.disparity.data(), n);
+    post.median(cfg, b);
+
+    put(out->disparity, full.disparity.data(), n);
+    put(out->confidence, full.confidence.data(), n);
+    put(out->invalid_reason, full.invalid_reason.data(), n);
+    put(out->reliable_mask, full.reliable_mask.data(), n);
+
+    if (std::memcmp(b.disparity.data(), full.disparity.data(), n * sizeof(float)) != 0 ||
+        std::memcmp(b.confidence.data(), full.confidence.data(), n * sizeof(float)) != 0 ||
+        std::memcmp(b.invalid_reason.data(), full.invalid_reason.data(), n) != 0 ||
+        std::memcmp(b.reliable_mask.data(), full.reliable_mask.data(), n) != 0) {
+        return -100;
+    }
+    return 0;
+}
+
+// One SGM path direction over a caller-supplied dense volume (SgmOptimizer::aggregate_path,
+// src/sgm_optimizer.cpp:186-259).  acc (u32, W*H*D) is accumulated in place.
+void ref_aggregate_path(const apg_pipeline_config_t* ccfg, const uint8_t* gray, const uint16_t* base,
+                        uint32_t* acc, int w, int h, int d0, int D, int dx, int dy) {
+    PipelineConfig cfg = to_ref(*ccfg);
+    Image8 g(w, h, 1);
+    std::memcpy(g.data(), gray, static_cast<size_t>(w) * h);
+    CostVolume vb(w, h, d0, d0 + D, 0);
+    std::memcpy(vb.data(), base, vb.bytes());
+    CostVolume32 va(w, h, d0, d0 + D, 0);
+    std::memcpy(va.data(), acc, va.bytes());
+    SgmOptimizer().aggregate_path(cfg, g, vb, va, dx, dy);
+    std::memcpy(acc, va.data(), va.bytes());
+}
+
+// SgmOptimizer::winner_take_all over a u32 volume (src/sgm_optimizer.cpp:436-555).
+void ref_winner_take_all(const apg_pipeline_config_t* ccfg, const uint32_t* vol, const int16_t* rmin,
+                         const int16_t* rmax, int w, int h, int d0, int D, float* disp, float* best,
+                         float* second) {
+    PipelineConfig cfg = to_ref(*ccfg);
+    CostVolume32 v(w, h, d0, d0 + D, 0);
+    std::memcpy(v.data(), vol, v.bytes());
+    SearchRange r;
+    r.allocate(w, h, d0, d0 + D);
+    std::memcpy(r.dmin.data(), rmin, static_cast<size_t>(w) * h * sizeof(int16_t));
+    std::memcpy(r.dmax.data(), rmax, static_cast<size_t>(w) * h * sizeof(int16_t));
+    Image32f d, b, s;
+    SgmOptimizer().winner_take_all(cfg, v, r, d, &b, &s);
+    const size_t n = static_cast<size_t>(w) * h;
+    put(disp, d.data(), n);
+    put(best, b.data(), n);
+    put(second, s.data(), n);
+}
+
+// Public-API session used for timing the reference CPU path.
+void* ref_session_create(const apg_pipeline_config_t* ccfg, int bounded_reuse) {
+    ExecutionOptions opt;
+    opt.memory_policy = bounded_reuse ? MemoryPolicy::BoundedReuse : MemoryPolicy::ReleasePerFrame;
+    opt.num_threads = ccfg->num_threads;
+    return new StereoSession(to_ref(*ccfg), opt);
+}
+
+void ref_session_destroy(void* s) { delete static_cast<StereoSession*>(s); }
+
+// StereoSession::process_status (include/apg_sgm/session.hpp:26-41) on a borrowed strided view.
+// stage_ms (nullable) receives the 11 StageTiming fields in declaration order.
+int ref_session_process(void* s, const uint8_t* left, const uint8_t* right, int w, int h, int stride,
+                        int ch, float* disp, float* conf, uint8_t* reason, uint8_t* reliable,
+                        double* stage_ms) {
+    auto* ss = static_cast<StereoSession*>(s);
+    StereoResult res;
+    PipelineStats st;
+    Status status = ss->process_status(ImageView8(left, w, h, stride, ch),
+                                       ImageView8(right, w, h, stride, ch), res, &st);
+    if (!status.ok()) return static_cast<int>(status.code);
+    const size_t n = static_cast<size_t>(w) * h;
+    put(disp, res.disparity.data(), n);
+    put(conf, res.confidence.data(), n);
+    put(reason, res.invalid_reason.data(), n);
+    put(reliable, res.reliable_mask.data(), n);
+    if (stage_ms) {
+        const StageTiming& t = st.timing;
+        const double v[11] = {t.aux_ms, t.prior_ms, t.cost_ms, t.cross_ms, t.right_wta_ms, t.sgm_ms,
+                              t.wta_ms, t.confidence_ms, t.refine_ms, t.post_ms, t.total_ms};
+        std::memcpy(stage_ms, v, sizeof(v));
+    }
+    return 0;
+}
+
+int ref_max_threads(void) {
+#if defined(_OPENMP)
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+} // extern "C"
