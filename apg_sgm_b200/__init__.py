@@ -1,0 +1,481 @@
+"""apg_sgm_b200: B200-native (sm_100a) apg-sgm dense stereo matching.
+
+Python front-end mirroring the reference binding (python/apg_sgm/__init__.py and
+python/src/binding.cpp of WildEgoLee/apg-sgm): the same StereoSession / StereoResult /
+PipelineStats / StageTiming classes, enums, keyword arguments and error behaviour, running on the
+CUDA engine in libapg_sgm_b200.so through its C-ABI (include/apg_sgm/c_api.h and
+include/apg_sgm_cuda.h).  `Engine` exposes the configuration-level engine used by tests, the
+benchmark and the batched/served forms.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import enum
+import threading
+
+import numpy as np
+
+from ._lib import ImageView, PipelineConfig, SessionOptions, lib
+
+__version__ = "1.0.0"
+
+
+class QualityMode(enum.IntEnum):
+    Fast = 0
+    Balanced = 1
+    HighQuality = 2
+
+
+class VolumeBackend(enum.IntEnum):
+    Auto = 0
+    Dense = 1
+    Packed = 2
+    CUDA = 3
+
+
+class MemoryPolicy(enum.IntEnum):
+    ReleasePerFrame = 0
+    BoundedReuse = 1
+
+
+class StatusCode(enum.IntEnum):
+    Ok = 0
+    EmptyInput = 1
+    SizeMismatch = 2
+    InvalidDisparityRange = 3
+    InvalidConfig = 4
+    UnsupportedBackend = 5
+    ResourceLimitExceeded = 6
+    AllocationFailure = 7
+    InternalError = 8
+
+
+class InvalidReason(enum.IntEnum):
+    Valid = 0
+    Occlusion = 1
+    Mismatch = 2
+    LowConfidence = 3
+    OutOfRange = 4
+
+
+_STAGES = ["aux_ms", "prior_ms", "cost_ms", "cross_ms", "right_wta_ms", "sgm_ms", "wta_ms",
+           "confidence_ms", "refine_ms", "post_ms", "total_ms"]
+
+
+class StageTiming:
+    """Per-stage device times in ms (include/apg_sgm/pipeline_stats.hpp:10-22).  The WTA is
+    fused into the last SGM sweep, so its time is part of sgm_ms and wta_ms is 0."""
+
+    def __init__(self, ms=None):
+        ms = ms if ms is not None else [0.0] * 11
+        for k, v in zip(_STAGES, ms):
+            setattr(self, k, float(v))
+
+    def to_dict(self):
+        return {k: getattr(self, k) for k in _STAGES}
+
+    def __repr__(self):
+        return f"<StageTiming total={self.total_ms}ms (sgm={self.sgm_ms}ms, cost={self.cost_ms}ms)>"
+
+
+class PipelineStats:
+    """PipelineStats (include/apg_sgm/pipeline_stats.hpp:24-142) for one frame."""
+
+    def __init__(self):
+        self.timing = StageTiming()
+        self.peak_workspace_bytes = 0
+        self.retained_workspace_bytes = 0
+        self.cost_bytes = 0
+        self.estimated_peak_bytes = 0
+        self.frame_allocation_count = 0
+        self.frame_reuse_count = 0
+        self.allocation_count = 0
+        self.reuse_count = 0
+        self.valid_disparity_ratio = 0.0
+        self.reliable_ratio = 0.0
+        self.unreliable_ratio = 0.0
+        self.refine_changed_ratio = 0.0
+        self.lr_fail_ratio = 0.0
+        self.effective_threads = 0
+        self.requested_threads = 0
+        self.requested_backend = "Auto"
+        self.resolved_backend = "CUDA"
+        self.memory_policy = "ReleasePerFrame"
+
+    def to_dict(self):
+        return {
+            "timing": self.timing.to_dict(),
+            "peak_workspace_bytes": self.peak_workspace_bytes,
+            "retained_workspace_bytes": self.retained_workspace_bytes,
+            "valid_disparity_ratio": self.valid_disparity_ratio,
+            "reliable_ratio": self.reliable_ratio,
+            "unreliable_ratio": self.unreliable_ratio,
+            "effective_threads": self.effective_threads,
+            "resolved_backend": self.resolved_backend,
+            "memory_policy": self.memory_policy,
+        }
+
+    def __repr__(self):
+        return (f"<PipelineStats total={self.timing.total_ms}ms valid_ratio={self.valid_disparity_ratio} "
+                f"peak_ws_mb={self.peak_workspace_bytes / (1024.0 * 1024.0)}>")
+
+
+class StereoResult:
+    def __init__(self, disparity, confidence, reliable_mask, invalid_reason, stats):
+        self._d, self._c, self._r, self._i = disparity, confidence, reliable_mask, invalid_reason
+        self._stats = stats
+
+    width = property(lambda self: 0 if self._d is None else self._d.shape[1])
+    height = property(lambda self: 0 if self._d is None else self._d.shape[0])
+    empty = property(lambda self: self._d is None or self._d.size == 0)
+    stats = property(lambda self: self._stats)
+    disparity = property(lambda self: self._d)
+    confidence = property(lambda self: self._c)
+    reliable_mask = property(lambda self: self._r)
+    invalid_reason = property(lambda self: self._i)
+
+    def __repr__(self):
+        return f"<apg_sgm.StereoResult {self.width}x{self.height} valid={'False' if self.empty else 'True'}>"
+
+
+def config_from_mode(mode=QualityMode.Balanced, max_disparity=128, min_disparity=0, **overrides) -> PipelineConfig:
+    """PipelineConfig::from_mode (src/config.cpp:5-45) plus field overrides."""
+    c = PipelineConfig()
+    lib().apgcu_config_from_mode(int(mode), int(max_disparity), C.byref(c))
+    c.min_disparity = int(min_disparity)
+    c.volume_backend = int(VolumeBackend.CUDA)
+    for k, v in overrides.items():
+        if not hasattr(c, k):
+            raise AttributeError(f"unknown configuration field {k!r}")
+        setattr(c, k, v)
+    return c
+
+
+def _image_view(a, name):
+    """Validate and wrap an HxW or HxWxC uint8 array (make_image_view, binding.cpp:37-119)."""
+    if not isinstance(a, np.ndarray):
+        a = np.asarray(a)
+    if a.dtype != np.uint8:
+        raise TypeError(f"{name} must have dtype uint8 (got format '{a.dtype.char}')")
+    if a.ndim not in (2, 3):
+        raise ValueError(f"{name} must be 2D (H, W) or 3D (H, W, C), got {a.ndim}D")
+    h, w = a.shape[:2]
+    c = 1 if a.ndim == 2 else a.shape[2]
+    if h <= 0 or w <= 0 or h > 2**31 - 1 or w > 2**31 - 1:
+        raise ValueError(f"{name} dimensions must be strictly positive and fit within INT_MAX ({w}x{h})")
+    if c not in (1, 3):
+        raise ValueError(f"{name} must have 1 or 3 channels, got {c}")
+    zero_copy = a.strides[1] == c and (a.ndim == 2 or a.strides[2] == 1) and a.strides[0] >= w * c
+    if not zero_copy:
+        a = np.ascontiguousarray(a)
+    v = ImageView(a.ctypes.data, w, h, a.strides[0], c)
+    return v, a
+
+
+def _parse(value, enum_cls, table, what):
+    if value is None:
+        return None
+    if isinstance(value, str):
+        s = value.lower()
+        if s not in table:
+            valid = ", ".join(f"'{k}'" for k in dict.fromkeys(table.values()).keys())
+            raise ValueError(f"Unrecognized {what} '{s}'. Valid: {valid}")
+        return table[s]
+    return enum_cls(int(value))
+
+
+_MODES = {"fast": QualityMode.Fast, "balanced": QualityMode.Balanced, "high_quality": QualityMode.HighQuality,
+          "hq": QualityMode.HighQuality, "highquality": QualityMode.HighQuality}
+_BACKENDS = {"auto": VolumeBackend.Auto, "dense": VolumeBackend.Dense, "packed": VolumeBackend.Packed,
+             "cuda": VolumeBackend.CUDA}
+_POLICIES = {"bounded_reuse": MemoryPolicy.BoundedReuse, "boundedreuse": MemoryPolicy.BoundedReuse,
+             "reuse": MemoryPolicy.BoundedReuse, "release_per_frame": MemoryPolicy.ReleasePerFrame,
+             "release": MemoryPolicy.ReleasePerFrame, "releaseperframe": MemoryPolicy.ReleasePerFrame}
+
+
+class StereoSession:
+    """Stateful streaming matcher session (PyStereoSession, binding.cpp:147-357).
+
+    Calls on one session are serialised by a lock; independent sessions run concurrently
+    (ctypes releases the GIL for the duration of every library call)."""
+
+    def __init__(self, mode="balanced", threads=0, max_disparity=128, min_disparity=0, backend="auto",
+                 memory_policy="release_per_frame", max_retained_bytes=0, config: PipelineConfig | None = None):
+        qm = _parse(mode, QualityMode, _MODES, "mode")
+        if qm is None:
+            qm = QualityMode.Balanced
+        be = _parse(backend, VolumeBackend, _BACKENDS, "backend")
+        mp = _parse(memory_policy, MemoryPolicy, _POLICIES, "memory_policy")
+        if mp is None:
+            mp = MemoryPolicy.ReleasePerFrame
+        if config is None:
+            cfg = config_from_mode(qm, max_disparity if max_disparity > 0 else 128)
+            if min_disparity != 0:
+                cfg.min_disparity = int(min_disparity)
+            if max_disparity > 0:
+                cfg.max_disparity = int(max_disparity)
+            if threads > 0:
+                cfg.num_threads = int(threads)
+        else:
+            cfg = config
+        if be is not None:
+            cfg.volume_backend = int(be)
+        err = _validate_config(cfg)
+        if err:
+            raise RuntimeError(err)
+        self._cfg = cfg
+        self._policy = mp
+        self._requested_backend = "Auto" if be in (None, VolumeBackend.Auto) else be.name
+        self._h = lib().apgcu_session_create_config(C.byref(cfg), int(mp), C.c_size_t(int(max_retained_bytes)))
+        if not self._h:
+            raise RuntimeError("failed to create session")
+        self._res = lib().apg_result_create()
+        self._mu = threading.Lock()
+
+    @property
+    def config(self) -> PipelineConfig:
+        return self._cfg
+
+    def process(self, left, right) -> StereoResult:
+        lv, la = _image_view(left, "left")
+        rv, ra = _image_view(right, "right")
+        if lv.width != rv.width or lv.height != rv.height:
+            raise ValueError(f"Left and right images must have identical dimensions ({lv.width}x{lv.height} vs "
+                             f"{rv.width}x{rv.height})")
+        if lv.channels != rv.channels:
+            raise ValueError(f"Left and right images must have matching channel counts ({lv.channels} vs "
+                             f"{rv.channels})")
+        L = lib()
+        with self._mu:
+            rc = L.apg_session_process(self._h, C.byref(lv), C.byref(rv), self._res)
+            if rc != 0:
+                msg = L.apg_session_get_last_error(self._h).decode()
+                raise RuntimeError(f"Stereo processing failed [{rc}]: {msg}")
+            w, h = C.c_int(), C.c_int()
+            n = lv.width * lv.height
+
+            def grab(fn, ctype, dtype):
+                p = fn(self._res, C.byref(w), C.byref(h))
+                return np.ctypeslib.as_array(C.cast(p, C.POINTER(ctype)), shape=(n,)).astype(dtype).reshape(
+                    h.value, w.value)
+
+            disp = grab(L.apg_result_get_disparity, C.c_float, np.float32)
+            conf = grab(L.apg_result_get_confidence, C.c_float, np.float32)
+            rel = grab(L.apg_result_get_reliable_mask, C.c_uint8, np.uint8)
+            reason = grab(L.apg_result_get_invalid_reason, C.c_uint8, np.uint8)
+            stats = self._stats(disp, rel, reason)
+        return StereoResult(disp, conf, rel, reason, stats)
+
+    compute = process
+
+    def _stats(self, disp, rel, reason) -> PipelineStats:
+        ms = (C.c_double * 11)()
+        cnt = (C.c_size_t * 4)()
+        lib().apgcu_session_get_stats(self._h, ms, cnt)
+        s = PipelineStats()
+        s.timing = StageTiming(list(ms))
+        s.frame_allocation_count = s.allocation_count = int(cnt[0])
+        s.frame_reuse_count = s.reuse_count = int(cnt[1])
+        s.peak_workspace_bytes = int(cnt[2])
+        s.retained_workspace_bytes = int(cnt[3])
+        n = disp.size
+        D = self._cfg.D
+        s.cost_bytes = n * D * 2
+        s.estimated_peak_bytes = int(lib().apgcu_session_estimate_bytes(self._h, disp.shape[1], disp.shape[0], 1))
+        s.valid_disparity_ratio = float((disp >= 0).sum()) / n if n else 0.0
+        rel_n = int((rel != 0).sum())
+        s.reliable_ratio = rel_n / n if n else 0.0
+        s.unreliable_ratio = (n - rel_n) / n if n else 0.0
+        s.lr_fail_ratio = float(np.isin(reason, (1, 2)).sum()) / n if n else 0.0
+        s.requested_threads = s.effective_threads = int(self._cfg.num_threads)
+        s.requested_backend = self._requested_backend
+        s.resolved_backend = "CUDA"
+        s.memory_policy = self._policy.name
+        return s
+
+    def reset(self):
+        with self._mu:
+            lib().apg_session_reset(self._h)
+
+    @property
+    def frame_count(self):
+        return int(lib().apg_session_get_frame_count(self._h))
+
+    @property
+    def total_time_ms(self):
+        return float(lib().apg_session_get_total_time_ms(self._h))
+
+    @property
+    def average_time_ms(self):
+        n = self.frame_count
+        return self.total_time_ms / n if n else 0.0
+
+    @property
+    def allocated_bytes(self):
+        return int(lib().apg_session_get_allocated_bytes(self._h))
+
+    @property
+    def last_error(self):
+        return lib().apg_session_get_last_error(self._h).decode()
+
+    def __repr__(self):
+        return (f"<apg_sgm.StereoSession frames={self.frame_count} avg_time_ms={self.average_time_ms} "
+                f"allocated_bytes={self.allocated_bytes}>")
+
+    def __del__(self):
+        try:
+            if getattr(self, "_h", None):
+                lib().apg_session_destroy(self._h)
+                self._h = None
+            if getattr(self, "_res", None):
+                lib().apg_result_destroy(self._res)
+                self._res = None
+        except Exception:
+            pass
+
+
+def _validate_config(cfg: PipelineConfig) -> str:
+    """validate_config (src/pipeline.cpp:171-213); returns the message or ''."""
+    if cfg.max_disparity <= cfg.min_disparity:
+        return "max_disparity must be strictly greater than min_disparity"
+    if cfg.cost_max < 0 or cfg.cost_max > 65535:
+        return "cost_max out of valid uint16 representation range [0, 65535]"
+    if cfg.P1 < 0:
+        return "SGM P1 penalty must be non-negative"
+    if cfg.P2_base <= cfg.P1:
+        return "SGM P2_base must be strictly greater than P1"
+    if cfg.grad_t1 < 0 or cfg.grad_t2 < cfg.grad_t1:
+        return "SGM gradient thresholds must satisfy 0 <= grad_t1 <= grad_t2"
+    if cfg.prior_enable and cfg.prior_search_radius < 0:
+        return "prior search_radius must be non-negative"
+    if cfg.refine_enable and cfg.refine_iterations < 0:
+        return "refine iterations must be non-negative"
+    return ""
+
+
+DUMPS = ["left_gray", "left_gx", "left_gy", "right_gray", "right_gx", "right_gy", "census_left", "census_right",
+         "range_min", "range_max", "cost_raw", "cost_agg", "sgm_sum", "disp_wta", "best", "second", "disp_right",
+         "confidence", "reliable", "reason_conf", "disp_refined", "disp_lr", "reason", "disp_fill", "disparity",
+         "d_prior"]
+_DUMP_DT = {"left_gray": np.uint8, "left_gx": np.uint8, "left_gy": np.uint8, "right_gray": np.uint8,
+            "right_gx": np.uint8, "right_gy": np.uint8, "census_left": np.uint32, "census_right": np.uint32,
+            "range_min": np.int16, "range_max": np.int16, "cost_raw": np.uint16, "cost_agg": np.uint16,
+            "sgm_sum": np.uint16, "reliable": np.uint8, "reason_conf": np.uint8, "reason": np.uint8}
+
+DEBUG_RAW_COST, DEBUG_KEEP_SUM, DEBUG_NO_FUSION, DEBUG_PROFILE = 1, 2, 4, 8
+
+
+class Engine:
+    """Configuration-level engine (apgcu_engine_*): host or device-resident processing, stage
+    dumps and per-stage device times."""
+
+    def __init__(self, config: PipelineConfig, device: int = 0, stream: int | None = None, debug: int = 0):
+        err = _validate_config(config)
+        if err:
+            raise RuntimeError(err)
+        self.config = config
+        self._h = lib().apgcu_engine_create(C.byref(config), int(device), C.c_void_p(stream) if stream else None)
+        if not self._h:
+            raise RuntimeError("apgcu_engine_create failed (configuration outside the CUDA backend's limits?)")
+        if debug:
+            lib().apgcu_engine_set_debug(self._h, int(debug))
+        self._shape = None
+
+    def process(self, left, right) -> dict:
+        lv, la = _image_view(left, "left")
+        rv, ra = _image_view(right, "right")
+        if lv.stride != rv.stride:
+            la, ra = np.ascontiguousarray(la), np.ascontiguousarray(ra)
+            lv, rv = _image_view(la, "left")[0], _image_view(ra, "right")[0]
+        h, w = lv.height, lv.width
+        out = {"disparity": np.empty((h, w), np.float32), "confidence": np.empty((h, w), np.float32),
+               "invalid_reason": np.empty((h, w), np.uint8), "reliable_mask": np.empty((h, w), np.uint8)}
+        rc = lib().apgcu_engine_process(self._h, lv.data, rv.data, w, h, lv.stride, lv.channels,
+                                        out["disparity"].ctypes.data, out["confidence"].ctypes.data,
+                                        out["invalid_reason"].ctypes.data, out["reliable_mask"].ctypes.data)
+        if rc != 0:
+            raise RuntimeError(f"processing failed [{rc}]: {self.last_error}")
+        self._shape = (h, w)
+        return out
+
+    def process_device(self, d_left: int, d_right: int, width: int, height: int, stride: int, channels: int,
+                       d_disp: int = 0, d_conf: int = 0, d_reason: int = 0, d_reliable: int = 0):
+        rc = lib().apgcu_engine_process_device(self._h, d_left, d_right, width, height, stride, channels,
+                                               d_disp or None, d_conf or None, d_reason or None, d_reliable or None)
+        if rc != 0:
+            raise RuntimeError(f"processing failed [{rc}]: {self.last_error}")
+        self._shape = (height, width)
+
+    def sync(self):
+        rc = lib().apgcu_engine_sync(self._h)
+        if rc != 0:
+            raise RuntimeError(self.last_error)
+
+    @property
+    def stream(self) -> int:
+        return int(lib().apgcu_engine_stream(self._h) or 0)
+
+    def dump(self, name: str) -> np.ndarray:
+        h, w = self._shape
+        D = self.config.D
+        idx = DUMPS.index(name)
+        if name in ("cost_raw", "cost_agg", "sgm_sum"):
+            a = np.empty((h, w, D), np.uint16)
+        elif name in ("census_left", "census_right") and self.config.census_type == 0:
+            a = np.empty((h, w), np.uint64)
+        else:
+            a = np.empty((h, w), _DUMP_DT.get(name, np.float32))
+        rc = lib().apgcu_engine_dump(self._h, idx, a.ctypes.data, a.nbytes)
+        if rc != 0:
+            raise RuntimeError(f"dump {name} failed [{rc}]: {self.last_error}")
+        return a
+
+    def stage_times(self) -> dict:
+        ms = (C.c_double * 11)()
+        lib().apgcu_engine_stage_times(self._h, ms)
+        return dict(zip(_STAGES, list(ms)))
+
+    def launch_profile(self) -> list:
+        """[(kernel name, ms)] of the last pair, in launch order (needs DEBUG_PROFILE)."""
+        names = (C.c_char_p * 64)()
+        ms = (C.c_float * 64)()
+        n = lib().apgcu_engine_launch_profile(self._h, 64, names, ms)
+        return [(names[i].decode(), float(ms[i])) for i in range(n)]
+
+    def set_debug(self, flags: int):
+        lib().apgcu_engine_set_debug(self._h, int(flags))
+
+    @property
+    def allocated_bytes(self) -> int:
+        return int(lib().apgcu_engine_allocated_bytes(self._h))
+
+    def release(self):
+        lib().apgcu_engine_release(self._h)
+
+    @property
+    def last_error(self) -> str:
+        return lib().apgcu_engine_last_error(self._h).decode()
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().apgcu_engine_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def kernel_launch_count() -> int:
+    return int(lib().apgcu_kernel_launch_count())
+
+
+def workspace_bytes(config: PipelineConfig, width: int, height: int) -> int:
+    return int(lib().apgcu_workspace_bytes(C.byref(config), int(width), int(height)))
+
+
+__all__ = ["QualityMode", "VolumeBackend", "MemoryPolicy", "StatusCode", "InvalidReason", "StageTiming",
+           "PipelineStats", "StereoResult", "StereoSession", "PipelineConfig", "config_from_mode", "Engine",
+           "kernel_launch_count", "workspace_bytes", "__version__"]

@@ -1,0 +1,95 @@
+// Gray conversion, gradients and census of one image, fused in one pass.
+//
+// Restates CostComputer::compute_aux (src/cost_computer.cpp:124-130): gray via
+// ImageView8::gray (include/apg_sgm/image_view.hpp:50-56), gx/gy as clamped absolute central
+// differences (src/cost_computer.cpp:63-88) and the 9x7 census (symmetric 31-bit,
+// :33-47, or plain 62-bit, :49-61), all with clamp-to-edge sampling (src/image.cpp:15-19).
+//
+// One CTA produces a 32x8 output tile.  It converts the (32+8)x(8+6) haloed input window to gray
+// once into shared memory (each gray value is needed by up to 63 census comparisons) and then
+// derives gradients and census from shared memory.  Bound: HBM, about ch + 7 (or 11) bytes per
+// pixel; the census comparisons are cheap integer work on staged data.
+#include "common.cuh"
+#include "kernels.h"
+
+namespace apgcu {
+
+namespace {
+constexpr int TX = 32, TY = 8, HX = 4, HY = 3;
+constexpr int SX = TX + 2 * HX, SY = TY + 2 * HY;
+
+template <bool C64>
+__global__ void __launch_bounds__(TX * TY) aux_kernel(const uint8_t* __restrict__ src, int stride, int ch,
+                                                      int w, int h, uint8_t* __restrict__ gray,
+                                                      uint8_t* __restrict__ gx, uint8_t* __restrict__ gy,
+                                                      uint32_t* __restrict__ census,
+                                                      unsigned long long* __restrict__ census64) {
+    __shared__ uint8_t g[SY][SX];
+    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+    const int tid = threadIdx.y * TX + threadIdx.x;
+    for (int i = tid; i < SX * SY; i += TX * TY) {
+        const int sy = i / SX, sx = i % SX;
+        const int yy = min(max(y0 + sy - HY, 0), h - 1);
+        const int xx = min(max(x0 + sx - HX, 0), w - 1);
+        const uint8_t* row = src + (size_t)yy * stride;
+        uint8_t v;
+        if (ch == 1) {
+            v = row[xx];
+        } else {
+            const int r = row[xx * ch], gg = row[xx * ch + 1], b = row[xx * ch + 2];
+            v = (uint8_t)((77 * r + 150 * gg + 29 * b) >> 8);
+        }
+        g[sy][sx] = v;
+    }
+    __syncthreads();
+    const int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
+    if (x >= w || y >= h) return;
+    const int cx = threadIdx.x + HX, cy = threadIdx.y + HY;
+    // Clamp-to-edge neighbours: outside the image the staged window already repeats the border
+    // value, so x+-1 / y+-1 read the clamped sample directly.
+    const int gxv = (int)g[cy][cx + 1] - (int)g[cy][cx - 1];
+    const int gyv = (int)g[cy + 1][cx] - (int)g[cy - 1][cx];
+    const size_t o = (size_t)y * w + x;
+    gray[o] = g[cy][cx];
+    gx[o] = (uint8_t)min(abs(gxv), 255);
+    gy[o] = (uint8_t)min(abs(gyv), 255);
+    if (C64) {
+        const uint8_t center = g[cy][cx];
+        unsigned long long bits = 0;
+        int b = 0;
+#pragma unroll
+        for (int dy = -3; dy <= 3; ++dy)
+#pragma unroll
+            for (int dx = -4; dx <= 4; ++dx) {
+                if (dx == 0 && dy == 0) continue;
+                if (g[cy + dy][cx + dx] > center) bits |= (1ull << b);
+                ++b;
+            }
+        census64[o] = bits;
+    } else {
+        uint32_t bits = 0;
+        int b = 0;
+#pragma unroll
+        for (int dy = -3; dy <= 3; ++dy)
+#pragma unroll
+            for (int dx = -4; dx <= 4; ++dx) {
+                if (dy < 0 || (dy == 0 && dx < 0)) {
+                    if (g[cy + dy][cx + dx] > g[cy - dy][cx - dx]) bits |= (1u << b);
+                    ++b;
+                }
+            }
+        census[o] = bits;
+    }
+}
+}  // namespace
+
+cudaError_t launch_aux(const uint8_t* src, int stride, int ch, int w, int h, int census64,
+                       uint8_t* gray, uint8_t* gx, uint8_t* gy, uint32_t* census,
+                       unsigned long long* census_wide, cudaStream_t s) {
+    dim3 grid((w + TX - 1) / TX, (h + TY - 1) / TY), block(TX, TY);
+    if (census64) aux_kernel<true><<<grid, block, 0, s>>>(src, stride, ch, w, h, gray, gx, gy, census, census_wide);
+    else aux_kernel<false><<<grid, block, 0, s>>>(src, stride, ch, w, h, gray, gx, gy, census, census_wide);
+    return cudaGetLastError();
+}
+
+}  // namespace apgcu

@@ -1,0 +1,131 @@
+// Shared device-side definitions of the apg-sgm B200 engine.
+//
+// Layouts in HBM (one stereo pair):
+//   * 2-D planes: row-major W*H (gray/gx/gy u8, census u32 or u64, range i16, maps f32/u8).
+//   * volumes: u16, pixel-major with the disparity axis innermost and padded to Dp, a multiple
+//     of 64:  vol[(y*W + x)*Dp + (d - d0)].  This is the reference Dense layout
+//     (include/apg_sgm/buffers.hpp:45-55) with a padded stride, so one pixel's costs are one
+//     128-byte-aligned run that a warp reads with one vector load per lane.  Padding entries
+//     hold the invalid marker 0xFFFF and behave as out-of-range disparities everywhere.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace apgcu {
+
+constexpr uint16_t kInvalidCost = 0xFFFFu;   // types.hpp:44 kInvalidCost
+constexpr uint32_t kInvalidWord = 0xFFFFFFFFu;
+constexpr int kLutCensus = 0;                 // offsets into the float LUT block
+constexpr int kLutAd = 65;
+constexpr int kLutGrad = 65 + 256;
+constexpr int kLutSize = 65 + 256 + 511;      // src/discrete_cost_lut.hpp:10-38
+
+enum InvalidReason : uint8_t { kValid = 0, kOcclusion = 1, kMismatch = 2, kLowConfidence = 3 };
+
+__host__ __device__ inline int round_up(int v, int m) { return (v + m - 1) / m * m; }
+
+// Everything a kernel needs to evaluate one matching cost.
+struct CostCtx {
+    int w, h, d0, D, Dp;
+    int census64;      // 1: plain 9x7 census (u64), 0: symmetric 9x7 (u32)
+    int use_ad, use_grad, cost_max;
+    float scale;       // cost_max / (1 + eta + mu), src/cost_computer.cpp:154-155
+    const float* lut;  // kLutSize floats built on the host with std::exp
+    const uint8_t *lgray, *lgx, *lgy, *rgray, *rgx, *rgy;
+    const uint32_t *cl, *cr;
+    const unsigned long long *cl64, *cr64;
+    const int16_t *rmin, *rmax;
+};
+
+// Quantised cost of left (x, y) against right (xr, y) from LUTs held in shared memory.
+// Same operation order as src/cost_computer.cpp:247-264; every float op is rounded on its own
+// (no contraction), so the u16 result equals the reference bit for bit.
+template <bool C64>
+__device__ __forceinline__ uint16_t quantised_cost(const CostCtx& c, const float* s_lut, uint32_t cl32,
+                                                   unsigned long long cl64v, int gl, int gxl, int gyl,
+                                                   int row, int xr) {
+    int pop;
+    if (C64) pop = __popcll(cl64v ^ c.cr64[row + xr]);
+    else pop = __popc(cl32 ^ c.cr[row + xr]);
+    float v = s_lut[kLutCensus + pop];
+    if (c.use_ad) {
+        const int ad = abs(gl - (int)c.rgray[row + xr]);
+        v = __fadd_rn(v, s_lut[kLutAd + ad]);
+    }
+    if (c.use_grad) {
+        const int g = abs(gxl - (int)c.rgx[row + xr]) + abs(gyl - (int)c.rgy[row + xr]);
+        v = __fadd_rn(v, s_lut[kLutGrad + g]);
+    }
+    int q = __float2int_rz(__fadd_rn(__fmul_rn(v, c.scale), 0.5f));
+    q = q < 0 ? 0 : (q > c.cost_max ? c.cost_max : q);
+    return (uint16_t)q;
+}
+
+// Unquantised (float) cost, used by the refiner's local cost (src/refiner.cpp:14-36).
+template <bool C64>
+__device__ __forceinline__ float raw_cost(const CostCtx& c, const float* lut, int x, int y, int xr) {
+    const int row = y * c.w;
+    int pop;
+    if (C64) pop = __popcll(c.cl64[row + x] ^ c.cr64[row + xr]);
+    else pop = __popc(c.cl[row + x] ^ c.cr[row + xr]);
+    float v = lut[kLutCensus + pop];
+    if (c.use_ad) v = __fadd_rn(v, lut[kLutAd + abs((int)c.lgray[row + x] - (int)c.rgray[row + xr])]);
+    if (c.use_grad) {
+        const int g = abs((int)c.lgx[row + x] - (int)c.rgx[row + xr]) +
+                      abs((int)c.lgy[row + x] - (int)c.rgy[row + xr]);
+        v = __fadd_rn(v, lut[kLutGrad + g]);
+    }
+    return v;
+}
+
+// Legacy parabolic sub-pixel offset, SubpixelEstimator::compute_legacy_delta
+// (src/subpixel_estimator.hpp:115-124).  Inputs are integer-valued floats.
+__device__ __forceinline__ float legacy_delta(float cm, float c0, float cp) {
+    const float denom = __fadd_rn(__fsub_rn(cm, __fmul_rn(2.0f, c0)), cp);
+    if (fabsf(denom) > 1e-6f) {
+        const float delta = __fdiv_rn(__fmul_rn(0.5f, __fsub_rn(cm, cp)), denom);
+        if (delta < -0.5f) return -0.5f;
+        if (delta > 0.5f) return 0.5f;
+        return delta;
+    }
+    return 0.0f;
+}
+
+// Exact q = n / d for n < 2^16 and 1 <= d < 2^16 with one high multiply:
+// m = floor(2^32 / d) + 1 gives n*m/2^32 = n/d + e with 0 < e < 2^-16 <= 1/d, so the floor is
+// exact (tests/test_host_logic.py checks every n, d used by the cross aggregation).
+__host__ __device__ inline uint32_t div_magic(uint32_t d) {
+    return d <= 1 ? 0u : (uint32_t)((0x100000000ull / d) + 1ull);
+}
+__device__ __forceinline__ uint32_t div_by_magic(uint32_t n, uint32_t d, uint32_t m) {
+    return d == 1 ? n : __umulhi(n, m);
+}
+
+// adaptive P2, detail::adaptive_p2 (src/sgm_common.hpp:25-39).
+struct SgmPen {
+    int P1, P2_base, adaptive, piecewise, t1, t2;
+    float alpha;
+};
+__device__ __forceinline__ int adaptive_p2(const SgmPen& p, int dI) {
+    dI = abs(dI);
+    int P2 = p.P2_base;
+    const int floor_p2 = p.P1 + 1;
+    if (!p.adaptive) return P2 > floor_p2 ? P2 : floor_p2;
+    if (p.piecewise) {
+        if (dI >= p.t2) P2 = p.P2_base / 4;
+        else if (dI >= p.t1) P2 = p.P2_base / 2;
+    } else {
+        P2 = __float2int_rz(__fadd_rn(
+            __fdiv_rn((float)p.P2_base, __fadd_rn(1.f, __fmul_rn(p.alpha, (float)dI))), 0.5f));
+    }
+    return P2 > floor_p2 ? P2 : floor_p2;
+}
+
+#define APGCU_CHECK(expr)                                                    \
+    do {                                                                     \
+        cudaError_t _e = (expr);                                             \
+        if (_e != cudaSuccess) return _e;                                    \
+    } while (0)
+
+}  // namespace apgcu

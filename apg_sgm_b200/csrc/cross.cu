@@ -1,0 +1,189 @@
+// Vertical half of the Cross-arm aggregation, CostAggregator::aggregate_hv
+// (src/cost_aggregator.cpp:107-138), and a standalone horizontal pass for the second and later
+// aggregation iterations (:77-105).
+//
+// Vertical kernel: a CTA owns `cols` adjacent pixel columns x and a 128-row segment; each thread
+// owns one 32-bit word (two disparities) of one column and slides down the segment keeping the
+// column prefix sums (sum and count, 16-bit lanes) of the last 2*Lmax+2 rows in a shared-memory
+// ring, so every input voxel is read once (plus a 2*Lmax row halo per segment) and every output
+// voxel is written once.  The up/down arms (build_cross_arms, :17-63) are computed once per
+// pixel into shared memory.  Bound: HBM, 4 bytes per voxel (read T, write C).
+#include "common.cuh"
+#include "kernels.h"
+
+namespace apgcu {
+
+namespace {
+constexpr int kSeg = 128;
+
+__global__ void cross_v_kernel(int w, int h, int d0, int D, int Dp, int lmax, int tau, int cols,
+                               const uint8_t* __restrict__ gray, const int16_t* __restrict__ rmin,
+                               const int16_t* __restrict__ rmax, const uint32_t* __restrict__ tin,
+                               uint32_t* __restrict__ cout, const uint32_t* __restrict__ magic) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int W2 = Dp / 2;
+    const int RS = 2 * lmax + 2;
+    const int nthr = W2 * cols;
+    uint32_t* ring_s = reinterpret_cast<uint32_t*>(smem);          // [RS][nthr]
+    uint32_t* ring_c = ring_s + (size_t)RS * nthr;                  // [RS][nthr]
+    uint8_t* armU = reinterpret_cast<uint8_t*>(ring_c + (size_t)RS * nthr);  // [cols][kSeg]
+    uint8_t* armD = armU + cols * kSeg;
+
+    const int xb = blockIdx.x * cols;
+    const int y0 = blockIdx.y * kSeg;
+    const int y1 = min(h, y0 + kSeg);
+    const int tid = threadIdx.x;
+
+    for (int i = tid; i < cols * kSeg; i += blockDim.x) {
+        const int ci = i / kSeg, yy = y0 + (i - ci * kSeg);
+        const int x = xb + ci;
+        int u = 0, v = 0;
+        if (x < w && yy < h) {
+            const int c0 = gray[yy * w + x];
+            while (u < lmax && yy - u - 1 >= 0 && abs((int)gray[(yy - u - 1) * w + x] - c0) <= tau) ++u;
+            while (v < lmax && yy + v + 1 < h && abs((int)gray[(yy + v + 1) * w + x] - c0) <= tau) ++v;
+        }
+        armU[i] = (uint8_t)u;
+        armD[i] = (uint8_t)v;
+    }
+    __syncthreads();
+    if (tid >= nthr) return;
+    const int ci = tid / W2, k = tid - ci * W2;
+    const int x = xb + ci;
+    if (x >= w) return;
+
+    const int ystart = max(0, y0 - lmax);
+    int r_next = ystart;
+    uint32_t ps = 0, pc = 0;
+    ring_s[(ystart % RS) * nthr + tid] = 0;
+    ring_c[(ystart % RS) * nthr + tid] = 0;
+    for (int y = y0; y < y1; ++y) {
+        const int need = min(h, y + lmax + 1);
+        while (r_next < need) {
+            const uint32_t v = tin[((size_t)r_next * w + x) * W2 + k];
+            const uint32_t inval = __vcmpeq2(v, kInvalidWord);
+            ps = __vadd2(ps, v & ~inval);
+            pc = __vadd2(pc, 0x00010001u & ~inval);
+            ++r_next;
+            const int slot = (r_next % RS) * nthr + tid;
+            ring_s[slot] = ps;
+            ring_c[slot] = pc;
+        }
+        const int ai = ci * kSeg + (y - y0);
+        const int a = y - armU[ai], b = y + armD[ai] + 1;
+        const uint32_t s = __vsub2(ring_s[(b % RS) * nthr + tid], ring_s[(a % RS) * nthr + tid]);
+        const uint32_t n = __vsub2(ring_c[(b % RS) * nthr + tid], ring_c[(a % RS) * nthr + tid]);
+        const int lo = rmin[y * w + x], hi = rmax[y * w + x];
+        uint32_t word = 0;
+#pragma unroll
+        for (int hs = 0; hs < 2; ++hs) {
+            const int di = 2 * k + hs;
+            const int d = d0 + di;
+            const uint32_t sh = (s >> (16 * hs)) & 0xFFFFu, nh = (n >> (16 * hs)) & 0xFFFFu;
+            uint32_t q = kInvalidCost;
+            if (di < D && d >= lo && d < hi && nh > 0) q = div_by_magic(sh, nh, magic[nh]);
+            word |= q << (16 * hs);
+        }
+        cout[((size_t)y * w + x) * W2 + k] = word;
+    }
+}
+
+// Horizontal pass over a volume (aggregation iterations after the first).  A CTA owns one row
+// and a run of `cols` pixels... implemented as the transpose of the vertical kernel: one thread
+// per (row, word) sliding along x.
+__global__ void cross_h_kernel(int w, int h, int d0, int D, int Dp, int lmax, int tau,
+                               const uint8_t* __restrict__ gray, const int16_t* __restrict__ rmin,
+                               const int16_t* __restrict__ rmax, const uint32_t* __restrict__ vin,
+                               uint32_t* __restrict__ vout, const uint32_t* __restrict__ magic) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int W2 = Dp / 2;
+    const int RS = 2 * lmax + 2;
+    const int nthr = W2;
+    uint32_t* ring_s = reinterpret_cast<uint32_t*>(smem);
+    uint32_t* ring_c = ring_s + (size_t)RS * nthr;
+    const int y = blockIdx.y;
+    const int x0 = blockIdx.x * kSeg, x1 = min(w, x0 + kSeg);
+    const int k = threadIdx.x;
+    if (k >= W2) return;
+    const int xstart = max(0, x0 - lmax);
+    int r_next = xstart;
+    uint32_t ps = 0, pc = 0;
+    ring_s[(xstart % RS) * nthr + k] = 0;
+    ring_c[(xstart % RS) * nthr + k] = 0;
+    const uint8_t* g = gray + (size_t)y * w;
+    for (int x = x0; x < x1; ++x) {
+        const int need = min(w, x + lmax + 1);
+        while (r_next < need) {
+            const uint32_t v = vin[((size_t)y * w + r_next) * W2 + k];
+            const uint32_t inval = __vcmpeq2(v, kInvalidWord);
+            ps = __vadd2(ps, v & ~inval);
+            pc = __vadd2(pc, 0x00010001u & ~inval);
+            ++r_next;
+            const int slot = (r_next % RS) * nthr + k;
+            ring_s[slot] = ps;
+            ring_c[slot] = pc;
+        }
+        const int c0 = g[x];
+        int l = 0, r = 0;
+        while (l < lmax && x - l - 1 >= 0 && abs((int)g[x - l - 1] - c0) <= tau) ++l;
+        while (r < lmax && x + r + 1 < w && abs((int)g[x + r + 1] - c0) <= tau) ++r;
+        const int a = x - l, b = x + r + 1;
+        const uint32_t s = __vsub2(ring_s[(b % RS) * nthr + k], ring_s[(a % RS) * nthr + k]);
+        const uint32_t n = __vsub2(ring_c[(b % RS) * nthr + k], ring_c[(a % RS) * nthr + k]);
+        const int lo = rmin[y * w + x], hi = rmax[y * w + x];
+        uint32_t word = 0;
+#pragma unroll
+        for (int hs = 0; hs < 2; ++hs) {
+            const int di = 2 * k + hs;
+            const int d = d0 + di;
+            const uint32_t sh = (s >> (16 * hs)) & 0xFFFFu, nh = (n >> (16 * hs)) & 0xFFFFu;
+            uint32_t q = kInvalidCost;
+            if (di < D && d >= lo && d < hi && nh > 0) q = div_by_magic(sh, nh, magic[nh]);
+            word |= q << (16 * hs);
+        }
+        vout[((size_t)y * w + x) * W2 + k] = word;
+    }
+}
+}  // namespace
+
+cudaError_t launch_cross_v(int w, int h, int d0, int D, int Dp, int lmax, int tau, const uint8_t* gray,
+                           const int16_t* rmin, const int16_t* rmax, const uint32_t* tin, uint32_t* cout,
+                           const uint32_t* magic, cudaStream_t s) {
+    const int W2 = Dp / 2;
+    const int cols = W2 >= 128 ? 1 : 128 / W2;
+    const int nthr = W2 * cols;
+    const int RS = 2 * lmax + 2;
+    const size_t smem = (size_t)RS * nthr * 8 + (size_t)cols * kSeg * 2;
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(cross_v_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    dim3 grid((w + cols - 1) / cols, (h + kSeg - 1) / kSeg);
+    cross_v_kernel<<<grid, round_up(nthr, 32), smem, s>>>(w, h, d0, D, Dp, lmax, tau, cols, gray, rmin, rmax,
+                                                          tin, cout, magic);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cross_h(int w, int h, int d0, int D, int Dp, int lmax, int tau, const uint8_t* gray,
+                           const int16_t* rmin, const int16_t* rmax, const uint32_t* vin, uint32_t* vout,
+                           const uint32_t* magic, cudaStream_t s) {
+    const int W2 = Dp / 2;
+    const int RS = 2 * lmax + 2;
+    const size_t smem = (size_t)RS * W2 * 8;
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(cross_h_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    dim3 grid((w + kSeg - 1) / kSeg, h);
+    cross_h_kernel<<<grid, round_up(W2, 32), smem, s>>>(w, h, d0, D, Dp, lmax, tau, gray, rmin, rmax, vin, vout,
+                                                        magic);
+    return cudaGetLastError();
+}
+
+size_t cross_v_smem_bytes(int Dp, int lmax) {
+    const int W2 = Dp / 2;
+    const int cols = W2 >= 128 ? 1 : 128 / W2;
+    return (size_t)(2 * lmax + 2) * W2 * cols * 8 + (size_t)cols * kSeg * 2;
+}
+
+}  // namespace apgcu

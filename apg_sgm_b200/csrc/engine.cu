@@ -1,0 +1,722 @@
+// Device pipeline orchestration (see engine.h).
+#include "engine.h"
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+
+namespace apgcu {
+
+namespace {
+std::atomic<unsigned long long> g_launches{0};
+
+inline size_t a256(size_t v) { return (v + 255) & ~size_t(255); }
+
+// Default per-pixel search range (PriorEstimator::estimate, src/prior_estimator.cpp:414-424 with
+// SearchRange::set_pixel clamping, include/apg_sgm/search_range.hpp:29-35).
+__global__ void default_range_kernel(int w, int h, int d0, int dmax, int16_t* rmin, int16_t* rmax) {
+    const int n = w * h;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int x = i % w;
+        int lo = d0, hi = min(dmax, x + 1);
+        lo = max(lo, d0);
+        hi = min(hi, dmax);
+        if (hi < lo) hi = lo;
+        rmin[i] = (int16_t)lo;
+        rmax[i] = (int16_t)hi;
+    }
+}
+
+__global__ void fill_u32_kernel(uint32_t* p, size_t n, uint32_t v) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) p[i] = v;
+}
+
+bool u16_path_ok(const apg_pipeline_config_t& c) {
+    // can_use_u16_sgm_accumulator (include/apg_sgm/sgm_optimizer.hpp:9-18) plus headroom for
+    // the saturating path arithmetic: m' + P2 and every path value stay below 0xFFFF.
+    const long long p2max = std::max<long long>(c.P2_base, (long long)c.P1 + 1);
+    const long long path_max = (long long)c.cost_max + p2max;
+    const int npath = c.paths == 8 ? 8 : 4;
+    if ((long long)npath * path_max >= 65535) return false;
+    if (path_max + p2max >= 65535) return false;
+    if (!c.piecewise_p2 && c.adaptive_penalties && c.p2_alpha < 0.f) return false;
+    return true;
+}
+}  // namespace
+
+void count_launches(unsigned n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+unsigned long long launch_count() { return g_launches.load(); }
+
+cudaError_t launch_default_range(int w, int h, int d0, int dmax, int16_t* rmin, int16_t* rmax, cudaStream_t s) {
+    const int n = w * h;
+    const int blocks = std::min((n + 255) / 256, 148 * 8);
+    default_range_kernel<<<blocks, 256, 0, s>>>(w, h, d0, dmax, rmin, rmax);
+    return cudaGetLastError();
+}
+
+int Engine::validate_config(const apg_pipeline_config_t& c, std::string& msg) {
+    // validate_config, src/pipeline.cpp:171-213
+    if (c.max_disparity <= c.min_disparity) {
+        msg = "max_disparity must be strictly greater than min_disparity";
+        return kInvalidDisparityRange;
+    }
+    if (c.cost_max < 0 || c.cost_max > 65535) {
+        msg = "cost_max out of valid uint16 representation range [0, 65535]";
+        return kInvalidConfig;
+    }
+    if (c.P1 < 0) { msg = "SGM P1 penalty must be non-negative"; return kInvalidConfig; }
+    if (c.P2_base <= c.P1) { msg = "SGM P2_base must be strictly greater than P1"; return kInvalidConfig; }
+    if (c.grad_t1 < 0 || c.grad_t2 < c.grad_t1) {
+        msg = "SGM gradient thresholds must satisfy 0 <= grad_t1 <= grad_t2";
+        return kInvalidConfig;
+    }
+    if (c.prior_enable && c.prior_search_radius < 0) { msg = "prior search_radius must be non-negative"; return kInvalidConfig; }
+    if (c.refine_enable && c.refine_iterations < 0) { msg = "refine iterations must be non-negative"; return kInvalidConfig; }
+    // Limits of the device kernels (documented in the library header).
+    const int D = c.max_disparity - c.min_disparity;
+    if (D > 512) { msg = "disparity range above 512 is not supported by the CUDA backend"; return kUnsupportedBackend; }
+    if (c.min_disparity < -32768 || c.max_disparity > 32767) { msg = "disparity bounds must fit int16"; return kInvalidConfig; }
+    if (!u16_path_ok(c)) {
+        msg = "SGM penalties/cost_max exceed the 16-bit path range of the CUDA backend";
+        return kUnsupportedBackend;
+    }
+    if (c.agg_enable) {
+        const int lmax = std::max(1, c.max_arm_length);
+        if (lmax > 127 || (long long)(2 * lmax + 1) * c.cost_max >= 65536) {
+            msg = "cross arm length x cost_max exceeds the 16-bit window range of the CUDA backend";
+            return kUnsupportedBackend;
+        }
+        if (cost_kernel_smem_bytes(D, round_up(D, 64), lmax, true, c.census_type == APG_CENSUS_9X7) > 227 * 1024 ||
+            cross_v_smem_bytes(round_up(D, 64), lmax) > 227 * 1024) {
+            msg = "cross arm length too large for on-chip staging";
+            return kUnsupportedBackend;
+        }
+    }
+    if (c.median_radius > 15) { msg = "median radius above 15 is not supported"; return kUnsupportedBackend; }
+    return kOk;
+}
+
+Layout Engine::make_layout(const apg_pipeline_config_t& c, int w, int h, int ch, int debug) {
+    Layout L;
+    L.w = w; L.h = h; L.ch = ch;
+    L.D = c.max_disparity - c.min_disparity;
+    L.Dp = round_up(L.D, 64);
+    L.cross = c.agg_enable != 0;
+    L.fused_fast = !L.cross && c.census_type == APG_CENSUS_SYMMETRIC_9X7 && !c.use_ad && !c.use_grad &&
+                   !(debug & 4);
+    L.raw_cost = (debug & 1) != 0;
+    const size_t n = (size_t)w * h;
+    const size_t csz = c.census_type == APG_CENSUS_9X7 ? 8 : 4;
+    const size_t vol = n * (size_t)L.Dp * 2;
+    size_t o = 0;
+    auto take = [&](size_t bytes) { const size_t r = o; o = a256(o + bytes); return r; };
+    L.in_left = take(n * ch);
+    L.in_right = take(n * ch);
+    L.lgray = take(n); L.lgx = take(n); L.lgy = take(n);
+    L.rgray = take(n); L.rgx = take(n); L.rgy = take(n);
+    L.cl = take(n * csz); L.cr = take(n * csz);
+    L.rmin = take(n * 2); L.rmax = take(n * 2);
+    L.rkey = take(n * 4);
+    L.disp_right = take(n * 4); L.disp_wta = take(n * 4); L.best = take(n * 4); L.second = take(n * 4);
+    L.confidence = take(n * 4); L.disp_ref = take(n * 4); L.disp_lr = take(n * 4); L.disp_fill = take(n * 4);
+    L.disp_out = take(n * 4); L.d_prior = take(n * 4);
+    L.reliable = take(n); L.reason_conf = take(n); L.reason = take(n);
+    // volumes: Balanced/HQ: A = cross-H output then path sum, B = aggregated cost.
+    //          Fast fused: A = path sum only.  Fast non-fused: A = raw cost, B = path sum.
+    L.volA = take(vol);
+    L.volB = (L.cross || !L.fused_fast) ? take(vol) : 0;
+    L.volS = L.cross ? L.volA : (L.fused_fast ? L.volA : L.volB);
+    L.volRaw = L.raw_cost ? take(vol) : 0;
+    L.lut = take(kLutSize * 4);
+    L.qlut = take(65 * 2);
+    L.magic = take(256 * 4);
+    if (c.prior_enable) {
+        const int cell = 16;
+        L.gw = (w + cell - 1) / cell; L.gh = (h + cell - 1) / cell; L.n_cells = L.gw * L.gh;
+        const int hard_max = std::max(0, c.prior_max_supports);
+        L.max_cand = std::max(8, (hard_max * 2 + L.n_cells - 1) / std::max(1, L.n_cells));
+        L.pr_cand = take((size_t)L.n_cells * L.max_cand * 16);
+        L.pr_ncand = take((size_t)L.n_cells * 4);
+        L.pr_taken = take((size_t)L.n_cells * 4 * 4);
+        L.pr_grid = take((size_t)L.n_cells * 4 * 10);
+        L.pr_maps = take(n * 4 * 4);
+        L.pr_scratch = take((size_t)L.n_cells * L.max_cand * 8 * 2);
+        L.pr_count = take(64);
+    }
+    if (c.refine_enable) {
+        L.rf_prefix = take(n * 4 + 4);
+        L.rf_draws = take(n * 4 + 4);
+        L.rf_scan_tmp_bytes = refine_scan_temp_bytes((int)n);
+        L.rf_scan_tmp = take(L.rf_scan_tmp_bytes);
+        L.rf_count = take(16);
+    }
+    L.total = o;
+    return L;
+}
+
+Engine::Engine(const apg_pipeline_config_t& cfg, int device, cudaStream_t stream) : cfg_(cfg), device_(device) {
+    cudaSetDevice(device_);
+    if (stream) {
+        stream_ = stream;
+    } else {
+        cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking);
+        own_stream_ = true;
+    }
+    for (auto& e : ev_) cudaEventCreate(&e);
+    for (auto& e : pev_) cudaEventCreate(&e);
+    // Cost LUTs on the host with std::exp, exactly as DiscreteCostLut (src/discrete_cost_lut.hpp:20-35).
+    lut_host_.assign(kLutSize, 0.f);
+    const float lc = std::max(cfg_.lambda_census, 1e-3f);
+    const float la = std::max(cfg_.lambda_ad, 1e-3f);
+    const float lg = std::max(cfg_.lambda_grad, 1e-3f);
+    for (int i = 0; i <= 64; ++i) lut_host_[kLutCensus + i] = 1.f - std::exp(-static_cast<float>(i) / lc);
+    if (cfg_.use_ad)
+        for (int i = 0; i < 256; ++i) lut_host_[kLutAd + i] = cfg_.eta_ad * (1.f - std::exp(-static_cast<float>(i) / la));
+    if (cfg_.use_grad)
+        for (int i = 0; i < 511; ++i) lut_host_[kLutGrad + i] = cfg_.mu_grad * (1.f - std::exp(-static_cast<float>(i) / lg));
+    const float norm = 1.f + (cfg_.use_ad ? cfg_.eta_ad : 0.f) + (cfg_.use_grad ? cfg_.mu_grad : 0.f);
+    const float scale = static_cast<float>(cfg_.cost_max) / std::max(norm, 1e-6f);
+    qlut_host_.assign(65, 0);
+    for (int i = 0; i <= 64; ++i) {
+        const int q = static_cast<int>(lut_host_[kLutCensus + i] * scale + 0.5f);
+        qlut_host_[i] = static_cast<uint16_t>(std::min(std::max(q, 0), cfg_.cost_max));
+    }
+}
+
+Engine::~Engine() {
+    release();
+    for (auto& e : ev_) if (e) cudaEventDestroy(e);
+    for (auto& e : pev_) if (e) cudaEventDestroy(e);
+    if (own_stream_ && stream_) cudaStreamDestroy(stream_);
+}
+
+void Engine::release() {
+    if (arena_) {
+        cudaStreamSynchronize(stream_);
+        cudaFree(arena_);
+        arena_ = nullptr;
+        arena_bytes_ = 0;
+    }
+    if (pin_) {
+        cudaFreeHost(pin_);
+        pin_ = nullptr;
+        pinned_bytes_ = 0;
+    }
+    lay_ = Layout();
+}
+
+int Engine::cuda_fail(cudaError_t e, const char* where) {
+    err_ = std::string("CUDA error in ") + where + ": " + cudaGetErrorString(e);
+    return e == cudaErrorMemoryAllocation ? kAllocationFailure : kInternalError;
+}
+
+CostCtx Engine::cost_ctx() const {
+    CostCtx c;
+    c.w = lay_.w; c.h = lay_.h; c.d0 = cfg_.min_disparity; c.D = lay_.D; c.Dp = lay_.Dp;
+    c.census64 = cfg_.census_type == APG_CENSUS_9X7;
+    c.use_ad = cfg_.use_ad; c.use_grad = cfg_.use_grad; c.cost_max = cfg_.cost_max;
+    const float norm = 1.f + (cfg_.use_ad ? cfg_.eta_ad : 0.f) + (cfg_.use_grad ? cfg_.mu_grad : 0.f);
+    c.scale = static_cast<float>(cfg_.cost_max) / std::max(norm, 1e-6f);
+    c.lut = ptr<float>(lay_.lut);
+    c.lgray = ptr<uint8_t>(lay_.lgray); c.lgx = ptr<uint8_t>(lay_.lgx); c.lgy = ptr<uint8_t>(lay_.lgy);
+    c.rgray = ptr<uint8_t>(lay_.rgray); c.rgx = ptr<uint8_t>(lay_.rgx); c.rgy = ptr<uint8_t>(lay_.rgy);
+    c.cl = ptr<uint32_t>(lay_.cl); c.cr = ptr<uint32_t>(lay_.cr);
+    c.cl64 = ptr<unsigned long long>(lay_.cl); c.cr64 = ptr<unsigned long long>(lay_.cr);
+    c.rmin = ptr<int16_t>(lay_.rmin); c.rmax = ptr<int16_t>(lay_.rmax);
+    return c;
+}
+
+int Engine::prepare(int w, int h, int ch) {
+    const Layout L = make_layout(cfg_, w, h, ch, debug_);
+    if (arena_ && arena_bytes_ >= L.total && lay_.w == w && lay_.h == h && lay_.ch == ch &&
+        lay_.raw_cost == L.raw_cost && lay_.fused_fast == L.fused_fast) {
+        return kOk;
+    }
+    if (arena_ && arena_bytes_ >= L.total) {
+        lay_ = L;  // capacity retained (BoundedReuse large -> small)
+    } else {
+        if (arena_) {
+            cudaStreamSynchronize(stream_);
+            cudaFree(arena_);
+            arena_ = nullptr;
+            arena_bytes_ = 0;
+        }
+        cudaError_t e = cudaMalloc(&arena_, L.total);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            arena_ = nullptr;
+            return fail(kAllocationFailure, "device workspace allocation failed (" + std::to_string(L.total) + " bytes)");
+        }
+        arena_bytes_ = L.total;
+        lay_ = L;
+    }
+    // constant tables
+    cudaError_t e = cudaMemcpyAsync(ptr<float>(lay_.lut), lut_host_.data(), kLutSize * 4, cudaMemcpyHostToDevice, stream_);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(ptr<uint16_t>(lay_.qlut), qlut_host_.data(), 65 * 2, cudaMemcpyHostToDevice, stream_);
+    if (e == cudaSuccess) {
+        uint32_t magic[256];
+        for (int d = 0; d < 256; ++d) magic[d] = div_magic(d);
+        e = cudaMemcpyAsync(ptr<uint32_t>(lay_.magic), magic, sizeof(magic), cudaMemcpyHostToDevice, stream_);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);  // magic[] lives on the stack
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "table upload");
+    return kOk;
+}
+
+int Engine::process_host(const uint8_t* left, const uint8_t* right, int w, int h, int stride, int ch, float* disp,
+                         float* conf, uint8_t* reason, uint8_t* reliable) {
+    cudaSetDevice(device_);
+    int rc = prepare(w, h, ch);
+    if (rc) return rc;
+    const size_t n = (size_t)w * h;
+    const size_t in_bytes = n * ch;
+    const size_t need = 2 * in_bytes + n * 4 * 2 + n * 2;
+    if (!pin_ || pinned_bytes_ < need) {
+        if (pin_) cudaFreeHost(pin_);
+        pin_ = nullptr;
+        pinned_bytes_ = 0;
+        if (cudaMallocHost(&pin_, need) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(kAllocationFailure, "pinned host staging allocation failed");
+        }
+        pinned_bytes_ = need;
+    }
+    unsigned char* pl = pin_;
+    unsigned char* pr = pin_ + in_bytes;
+    float* pdisp = reinterpret_cast<float*>(pin_ + 2 * in_bytes);
+    float* pconf = pdisp + n;
+    uint8_t* preason = reinterpret_cast<uint8_t*>(pconf + n);
+    uint8_t* prel = preason + n;
+    const size_t row = (size_t)w * ch;
+    for (int y = 0; y < h; ++y) {
+        std::memcpy(pl + y * row, left + (size_t)y * stride, row);
+        std::memcpy(pr + y * row, right + (size_t)y * stride, row);
+    }
+    cudaError_t e = cudaMemcpyAsync(ptr<uint8_t>(lay_.in_left), pl, in_bytes, cudaMemcpyHostToDevice, stream_);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(ptr<uint8_t>(lay_.in_right), pr, in_bytes, cudaMemcpyHostToDevice, stream_);
+    if (e != cudaSuccess) return cuda_fail(e, "input upload");
+    rc = run(ptr<uint8_t>(lay_.in_left), (int)row, ptr<uint8_t>(lay_.in_right), (int)row, ch, nullptr, nullptr, nullptr,
+             nullptr);
+    if (rc) return rc;
+    e = cudaMemcpyAsync(pdisp, ptr<float>(lay_.disp_out), n * 4, cudaMemcpyDeviceToHost, stream_);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(pconf, ptr<float>(lay_.confidence), n * 4, cudaMemcpyDeviceToHost, stream_);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(preason, ptr<uint8_t>(lay_.reason), n, cudaMemcpyDeviceToHost, stream_);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(prel, ptr<uint8_t>(lay_.reliable), n, cudaMemcpyDeviceToHost, stream_);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+    if (e != cudaSuccess) return cuda_fail(e, "output download");
+    if (disp) std::memcpy(disp, pdisp, n * 4);
+    if (conf) std::memcpy(conf, pconf, n * 4);
+    if (reason) std::memcpy(reason, preason, n);
+    if (reliable) std::memcpy(reliable, prel, n);
+    return kOk;
+}
+
+int Engine::process_device(const uint8_t* dl, const uint8_t* dr, int w, int h, int stride, int ch, float* d_disp,
+                           float* d_conf, uint8_t* d_reason, uint8_t* d_reliable) {
+    cudaSetDevice(device_);
+    int rc = prepare(w, h, ch);
+    if (rc) return rc;
+    return run(dl, stride, dr, stride, ch, d_disp, d_conf, d_reason, d_reliable);
+}
+
+int Engine::sync() {
+    cudaError_t e = cudaStreamSynchronize(stream_);
+    return e == cudaSuccess ? kOk : cuda_fail(e, "stream synchronize");
+}
+
+int Engine::run(const uint8_t* dl, int lstride, const uint8_t* dr, int rstride, int ch, float* d_disp, float* d_conf,
+                uint8_t* d_reason, uint8_t* d_reliable) {
+    const Layout& L = lay_;
+    const int w = L.w, h = L.h, D = L.D, Dp = L.Dp, d0 = cfg_.min_disparity;
+    const size_t n = (size_t)w * h;
+    cudaStream_t s = stream_;
+    unsigned launches = 0;
+    cudaError_t e = cudaSuccess;
+    const bool prof = (debug_ & 8) != 0;
+    nprof_ = 0;
+    if (prof) cudaEventRecord(pev_[0], s);
+#define RUN(expr, what)                                  \
+    do {                                                 \
+        e = (expr);                                      \
+        if (e != cudaSuccess) return cuda_fail(e, what); \
+        ++launches;                                      \
+        if (prof) prof_mark(what);                       \
+    } while (0)
+#define RUNC(expr, what)                                 \
+    do {                                                 \
+        e = (expr);                                      \
+        if (e != cudaSuccess) return cuda_fail(e, what); \
+        if (prof) prof_mark("copy");                     \
+    } while (0)
+    const int c64 = cfg_.census_type == APG_CENSUS_9X7;
+    cudaEventRecord(ev_[0], s);
+    RUN(launch_aux(dl, lstride, ch, w, h, c64, ptr<uint8_t>(L.lgray), ptr<uint8_t>(L.lgx), ptr<uint8_t>(L.lgy),
+                   ptr<uint32_t>(L.cl), ptr<unsigned long long>(L.cl), s), "aux(left)");
+    RUN(launch_aux(dr, rstride, ch, w, h, c64, ptr<uint8_t>(L.rgray), ptr<uint8_t>(L.rgx), ptr<uint8_t>(L.rgy),
+                   ptr<uint32_t>(L.cr), ptr<unsigned long long>(L.cr), s), "aux(right)");
+    cudaEventRecord(ev_[1], s);
+    RUN(launch_default_range(w, h, d0, cfg_.max_disparity, ptr<int16_t>(L.rmin), ptr<int16_t>(L.rmax), s), "range");
+    const CostCtx cc = cost_ctx();
+    support_count_ = 0;
+    if (cfg_.prior_enable) {
+        e = launch_prior(cfg_, cc, L, arena_, s, &launches);
+        if (e != cudaSuccess) return cuda_fail(e, "prior");
+        if (prof) prof_mark("prior");
+    } else if (debug_) {
+        // no prior: d_prior is -1 everywhere (read only by the stage dump)
+        fill_u32_kernel<<<std::min((int)((n + 255) / 256), 148 * 8), 256, 0, s>>>(ptr<uint32_t>(L.d_prior), n, 0xBF800000u);
+        ++launches;
+    }
+    cudaEventRecord(ev_[2], s);
+    // cost (+ cross-H, + right argmin)
+    RUNC(cudaMemsetAsync(ptr<uint32_t>(L.rkey), 0xFF, n * 4, s), "rkey init");
+    const int lmax = std::max(1, cfg_.max_arm_length);
+    const uint32_t* magic = ptr<uint32_t>(L.magic);
+    if (L.raw_cost) RUN(launch_cost(cc, 0, lmax, cfg_.color_threshold, ptr<uint32_t>(L.volRaw), ptr<uint32_t>(L.rkey), magic, s), "cost(raw)");
+    const uint32_t* sgm_src = nullptr;
+    if (L.cross) {
+        RUN(launch_cost(cc, 1, lmax, cfg_.color_threshold, ptr<uint32_t>(L.volA), ptr<uint32_t>(L.rkey), magic, s), "cost+crossH");
+    } else if (L.fused_fast) {
+        if (!L.raw_cost) RUN(launch_cost(cc, 2, lmax, 0, nullptr, ptr<uint32_t>(L.rkey), magic, s), "right argmin");
+    } else {
+        RUN(launch_cost(cc, 0, lmax, 0, ptr<uint32_t>(L.volA), ptr<uint32_t>(L.rkey), magic, s), "cost");
+        sgm_src = ptr<uint32_t>(L.volA);
+    }
+    cudaEventRecord(ev_[3], s);
+    RUN(launch_right_wta_finalize(cc, ptr<uint32_t>(L.rkey), cfg_.subpixel, ptr<float>(L.disp_right), s), "right wta");
+    cudaEventRecord(ev_[4], s);
+    if (L.cross) {
+        const int tau = cfg_.color_threshold;
+        RUN(launch_cross_v(w, h, d0, D, Dp, lmax, tau, ptr<uint8_t>(L.lgray), ptr<int16_t>(L.rmin), ptr<int16_t>(L.rmax),
+                           ptr<uint32_t>(L.volA), ptr<uint32_t>(L.volB), magic, s), "crossV");
+        const int iters = std::max(1, cfg_.agg_iterations);
+        for (int it = 1; it < iters; ++it) {
+            RUN(launch_cross_h(w, h, d0, D, Dp, lmax, tau, ptr<uint8_t>(L.lgray), ptr<int16_t>(L.rmin), ptr<int16_t>(L.rmax),
+                               ptr<uint32_t>(L.volB), ptr<uint32_t>(L.volA), magic, s), "crossH");
+            RUN(launch_cross_v(w, h, d0, D, Dp, lmax, tau, ptr<uint8_t>(L.lgray), ptr<int16_t>(L.rmin), ptr<int16_t>(L.rmax),
+                               ptr<uint32_t>(L.volA), ptr<uint32_t>(L.volB), magic, s), "crossV");
+        }
+        sgm_src = ptr<uint32_t>(L.volB);
+    }
+    cudaEventRecord(ev_[5], s);
+    // SGM sweeps: horizontal, diagonal, then vertical; the last one carries the WTA.
+    static const int order4[4][2] = {{1, 0}, {-1, 0}, {0, 1}, {0, -1}};
+    static const int order8[8][2] = {{1, 0}, {-1, 0}, {1, 1}, {1, -1}, {-1, 1}, {-1, -1}, {0, 1}, {0, -1}};
+    const int npath = cfg_.paths == 8 ? 8 : 4;
+    SgmPathLaunch pl;
+    pl.w = w; pl.h = h; pl.d0 = d0; pl.D = D; pl.Dp = Dp;
+    pl.pen = SgmPen{cfg_.P1, cfg_.P2_base, cfg_.adaptive_penalties, cfg_.piecewise_p2, cfg_.grad_t1, cfg_.grad_t2,
+                    cfg_.p2_alpha};
+    pl.gray = ptr<uint8_t>(L.lgray);
+    pl.cvol = sgm_src;
+    pl.cl = ptr<uint32_t>(L.cl); pl.cr = ptr<uint32_t>(L.cr); pl.qlut = ptr<uint16_t>(L.qlut);
+    pl.rmin = ptr<int16_t>(L.rmin); pl.rmax = ptr<int16_t>(L.rmax);
+    pl.S = ptr<uint32_t>(L.volS);
+    pl.disp = ptr<float>(L.disp_wta); pl.best = ptr<float>(L.best); pl.second = ptr<float>(L.second);
+    pl.subpixel = cfg_.subpixel;
+    pl.store_final = (debug_ & 2) != 0;
+    for (int p = 0; p < npath; ++p) {
+        pl.dx = npath == 8 ? order8[p][0] : order4[p][0];
+        pl.dy = npath == 8 ? order8[p][1] : order4[p][1];
+        pl.mode = p == 0 ? 0 : (p == npath - 1 ? 2 : 1);
+        static const char* kSgmNames[3] = {"sgm_first", "sgm_accum", "sgm_last_wta"};
+        RUN(launch_sgm_path(pl, s), kSgmNames[pl.mode]);
+    }
+    cudaEventRecord(ev_[6], s);
+    // confidence (+ LR when nothing runs between them)
+    const bool refine = cfg_.refine_enable && cfg_.refine_iterations > 0;
+    ConfLrArgs ca;
+    ca.w = w; ca.h = h;
+    ca.disp = ptr<float>(L.disp_wta); ca.disp_right = ptr<float>(L.disp_right);
+    ca.best = ptr<float>(L.best); ca.second = ptr<float>(L.second);
+    ca.lgx = ptr<uint8_t>(L.lgx); ca.lgy = ptr<uint8_t>(L.lgy);
+    ca.uniqueness_ratio = cfg_.conf_uniqueness_ratio; ca.min_texture = cfg_.conf_min_texture;
+    ca.reliable_threshold = cfg_.conf_reliable_threshold; ca.conf_lr_max_diff = cfg_.conf_lr_max_diff;
+    ca.confidence = ptr<float>(L.confidence);
+    ca.reliable = ptr<uint8_t>(L.reliable);
+    ca.reason = ptr<uint8_t>(L.reason);
+    ca.fuse_lr = refine ? 0 : 1;
+    ca.lr_check = cfg_.lr_check;
+    ca.post_lr_max_diff = cfg_.post_lr_max_diff;
+    ca.disp_out = ptr<float>(L.disp_lr);
+    RUN(launch_conf_lr(ca, s), "confidence");
+    if (debug_) RUNC(cudaMemcpyAsync(ptr<uint8_t>(L.reason_conf), ptr<uint8_t>(L.reason), n, cudaMemcpyDeviceToDevice, s), "dbg");
+    cudaEventRecord(ev_[7], s);
+    const float* post_in = ptr<float>(L.disp_lr);
+    if (refine) {
+        RUNC(cudaMemcpyAsync(ptr<float>(L.disp_ref), ptr<float>(L.disp_wta), n * 4, cudaMemcpyDeviceToDevice, s), "refine copy");
+        const int rc = run_refine(ptr<float>(L.disp_ref));
+        if (rc) return rc;
+        if (prof) prof_mark("refine");
+        cudaEventRecord(ev_[8], s);
+        if (cfg_.lr_check) {
+            RUN(launch_lr(w, h, cfg_.post_lr_max_diff, ptr<float>(L.disp_right), ptr<float>(L.disp_ref), ptr<float>(L.disp_lr),
+                          ptr<uint8_t>(L.reason), s), "lr");
+        } else {
+            post_in = ptr<float>(L.disp_ref);
+        }
+    } else {
+        cudaEventRecord(ev_[8], s);
+    }
+    RUN(launch_fill(w, h, cfg_.max_fill_gap, post_in, ptr<uint8_t>(L.reason), ptr<uint8_t>(L.lgray),
+                    cfg_.prior_enable ? ptr<float>(L.d_prior) : nullptr, ptr<float>(L.disp_fill), s), "fill");
+    float* final_out = d_disp ? d_disp : ptr<float>(L.disp_out);
+    if (cfg_.median_radius > 0) {
+        RUN(launch_median(w, h, cfg_.median_radius, ptr<float>(L.disp_fill), final_out, s), "median");
+    } else {
+        RUNC(cudaMemcpyAsync(final_out, ptr<float>(L.disp_fill), n * 4, cudaMemcpyDeviceToDevice, s), "copy");
+    }
+    if (d_reason) RUNC(cudaMemcpyAsync(d_reason, ptr<uint8_t>(L.reason), n, cudaMemcpyDeviceToDevice, s), "reason out");
+    if (d_conf) RUNC(cudaMemcpyAsync(d_conf, ptr<float>(L.confidence), n * 4, cudaMemcpyDeviceToDevice, s), "conf out");
+    if (d_reliable) RUNC(cudaMemcpyAsync(d_reliable, ptr<uint8_t>(L.reliable), n, cudaMemcpyDeviceToDevice, s), "rel out");
+    if (d_disp && d_disp != ptr<float>(L.disp_out) && debug_)
+        RUNC(cudaMemcpyAsync(ptr<float>(L.disp_out), d_disp, n * 4, cudaMemcpyDeviceToDevice, s), "dbg");
+    cudaEventRecord(ev_[9], s);
+    have_times_ = true;
+    count_launches(launches);
+#undef RUN
+#undef RUNC
+    return kOk;
+}
+
+void Engine::prof_mark(const char* name) {
+    if (nprof_ >= kMaxProf) return;
+    pname_[nprof_] = name;
+    cudaEventRecord(pev_[nprof_ + 1], stream_);
+    ++nprof_;
+}
+
+int Engine::launch_profile(int max, const char** names, float* ms) const {
+    if (nprof_ == 0) return 0;
+    cudaEventSynchronize(pev_[nprof_]);
+    const int n = nprof_ < max ? nprof_ : max;
+    for (int i = 0; i < n; ++i) {
+        float t = 0.f;
+        cudaEventElapsedTime(&t, pev_[i], pev_[i + 1]);
+        if (names) names[i] = pname_[i];
+        if (ms) ms[i] = t;
+    }
+    return n;
+}
+
+int Engine::run_refine(float* work) {
+    // detail::refine_scalar (src/refiner.cpp:42-100): one mt19937(12345) stream, a fresh
+    // uniform_int_distribution(-r, r) per iteration, draws consumed in the pass's raster order.
+    std::mt19937 rng(12345);
+    const Layout& L = lay_;
+    const CostCtx cc = cost_ctx();
+    std::vector<int> draws;
+    unsigned launches = 0;
+    for (int it = 0; it < cfg_.refine_iterations; ++it) {
+        const int fwd = (it % 2) == 0;
+        const int radius = std::max(1, cfg_.refine_random_radius >> it);
+        int* d_cnt = reinterpret_cast<int*>(arena_ + L.rf_count);
+        cudaError_t e = launch_refine_count(L, arena_, work, fwd, d_cnt, stream_, &launches);
+        if (e != cudaSuccess) return cuda_fail(e, "refine count");
+        int cnt = 0;
+        e = cudaMemcpyAsync(&cnt, d_cnt, 4, cudaMemcpyDeviceToHost, stream_);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+        if (e != cudaSuccess) return cuda_fail(e, "refine count read");
+        std::uniform_int_distribution<int> dist(-radius, radius);
+        draws.resize(std::max(cnt, 1));
+        for (int i = 0; i < cnt; ++i) draws[i] = dist(rng);
+        if (cnt > 0) {
+            e = cudaMemcpyAsync(reinterpret_cast<int*>(arena_ + L.rf_draws), draws.data(), (size_t)cnt * 4,
+                                cudaMemcpyHostToDevice, stream_);
+            if (e != cudaSuccess) return cuda_fail(e, "refine draws upload");
+        }
+        e = launch_refine_pass(cfg_, cc, L, arena_, work, fwd, stream_, &launches);
+        if (e != cudaSuccess) return cuda_fail(e, "refine pass");
+        // the draws vector is reused by the next pass: wait until this upload is consumed
+        e = cudaStreamSynchronize(stream_);
+        if (e != cudaSuccess) return cuda_fail(e, "refine pass sync");
+    }
+    count_launches(launches);
+    return kOk;
+}
+
+void Engine::stage_times(double* ms) const {
+    for (int i = 0; i < 11; ++i) ms[i] = 0.0;
+    if (!have_times_) return;
+    cudaEventSynchronize(ev_[9]);
+    auto el = [&](int a, int b) {
+        float t = 0.f;
+        cudaEventElapsedTime(&t, ev_[a], ev_[b]);
+        return (double)t;
+    };
+    ms[0] = el(0, 1);   // aux
+    ms[1] = el(1, 2);   // prior / range
+    ms[2] = el(2, 3);   // cost (+cross-H, +right argmin)
+    ms[3] = el(4, 5);   // cross (vertical)
+    ms[4] = el(3, 4);   // right WTA
+    ms[5] = el(5, 6);   // sgm (WTA fused into the last sweep)
+    ms[6] = 0.0;        // wta: fused into the last SGM sweep
+    ms[7] = el(6, 7);   // confidence (+LR when fused)
+    ms[8] = el(7, 8);   // refine
+    ms[9] = el(8, 9);   // post
+    ms[10] = el(0, 9);  // total device time
+}
+
+int Engine::dump(int what, void* dst, size_t bytes) {
+    if (!arena_) return fail(kInternalError, "nothing processed yet");
+    const Layout& L = lay_;
+    const size_t n = (size_t)L.w * L.h;
+    const size_t csz = cfg_.census_type == APG_CENSUS_9X7 ? 8 : 4;
+    size_t off = 0, sz = 0;
+    bool vol = false;
+    switch (what) {
+        case 0: off = L.lgray; sz = n; break;
+        case 1: off = L.lgx; sz = n; break;
+        case 2: off = L.lgy; sz = n; break;
+        case 3: off = L.rgray; sz = n; break;
+        case 4: off = L.rgx; sz = n; break;
+        case 5: off = L.rgy; sz = n; break;
+        case 6: off = L.cl; sz = n * csz; break;
+        case 7: off = L.cr; sz = n * csz; break;
+        case 8: off = L.rmin; sz = n * 2; break;
+        case 9: off = L.rmax; sz = n * 2; break;
+        case 10: if (!L.raw_cost) return fail(kInternalError, "raw cost not materialised"); off = L.volRaw; vol = true; break;
+        case 11: if (!L.cross) return fail(kInternalError, "no aggregated volume"); off = L.volB; vol = true; break;
+        case 12: if (!(debug_ & 2)) return fail(kInternalError, "path sum not kept"); off = L.volS; vol = true; break;
+        case 13: off = L.disp_wta; sz = n * 4; break;
+        case 14: off = L.best; sz = n * 4; break;
+        case 15: off = L.second; sz = n * 4; break;
+        case 16: off = L.disp_right; sz = n * 4; break;
+        case 17: off = L.confidence; sz = n * 4; break;
+        case 18: off = L.reliable; sz = n; break;
+        case 19: off = L.reason_conf; sz = n; break;
+        case 20: off = L.disp_ref; sz = n * 4; break;
+        case 21: off = L.disp_lr; sz = n * 4; break;
+        case 22: off = L.reason; sz = n; break;
+        case 23: off = L.disp_fill; sz = n * 4; break;
+        case 24: off = L.disp_out; sz = n * 4; break;
+        case 25: off = L.d_prior; sz = n * 4; break;
+        default: return fail(kInternalError, "unknown dump id");
+    }
+    cudaError_t e;
+    if (vol) {
+        // strip the disparity padding: D u16 of every Dp-long pixel run
+        if (bytes < n * L.D * 2) return fail(kInternalError, "dump buffer too small");
+        e = cudaMemcpy2DAsync(dst, L.D * 2, arena_ + off, L.Dp * 2, L.D * 2, n, cudaMemcpyDeviceToHost, stream_);
+    } else {
+        if (bytes < sz) return fail(kInternalError, "dump buffer too small");
+        e = cudaMemcpyAsync(dst, arena_ + off, sz, cudaMemcpyDeviceToHost, stream_);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+    return e == cudaSuccess ? kOk : cuda_fail(e, "dump");
+}
+
+}  // namespace apgcu
+
+// ------------------------------------------------------------------------------------------------
+// Extended C-ABI (include/apg_sgm_cuda.h)
+// ------------------------------------------------------------------------------------------------
+#include "../../include/apg_sgm_cuda.h"
+
+struct apgcu_engine_s {
+    apgcu::Engine* eng;
+    std::string err;
+};
+
+extern "C" {
+
+apgcu_engine_t apgcu_engine_create(const apg_pipeline_config_t* cfg, int device, void* stream) {
+    if (!cfg) return nullptr;
+    try {
+        std::string msg;
+        if (apgcu::Engine::validate_config(*cfg, msg) != apgcu::kOk) return nullptr;
+        auto* h = new apgcu_engine_s;
+        h->eng = new apgcu::Engine(*cfg, device, static_cast<cudaStream_t>(stream));
+        return h;
+    } catch (...) {
+        return nullptr;
+    }
+}
+
+void apgcu_engine_destroy(apgcu_engine_t e) {
+    if (!e) return;
+    delete e->eng;
+    delete e;
+}
+
+const char* apgcu_engine_last_error(apgcu_engine_t e) { return e ? e->eng->last_error().c_str() : "Invalid engine handle"; }
+
+int apgcu_engine_set_debug(apgcu_engine_t e, int flags) {
+    if (!e) return apgcu::kInternalError;
+    e->eng->set_debug(flags);
+    return 0;
+}
+
+static int check_views(const uint8_t* l, const uint8_t* r, int w, int h, int stride, int ch) {
+    if (!l || !r || w <= 0 || h <= 0) return apgcu::kEmptyInput;
+    if (ch != 1 && ch != 3 && ch != 4) return apgcu::kSizeMismatch;
+    if (stride < w * ch) return apgcu::kSizeMismatch;
+    return 0;
+}
+
+int apgcu_engine_process(apgcu_engine_t e, const uint8_t* left, const uint8_t* right, int width, int height, int stride,
+                         int channels, float* disparity, float* confidence, uint8_t* invalid_reason,
+                         uint8_t* reliable_mask) {
+    if (!e) return apgcu::kInternalError;
+    if (int v = check_views(left, right, width, height, stride, channels)) return v;
+    try {
+        return e->eng->process_host(left, right, width, height, stride, channels, disparity, confidence, invalid_reason,
+                                    reliable_mask);
+    } catch (const std::bad_alloc&) {
+        return apgcu::kAllocationFailure;
+    } catch (...) {
+        return apgcu::kInternalError;
+    }
+}
+
+int apgcu_engine_process_device(apgcu_engine_t e, const uint8_t* d_left, const uint8_t* d_right, int width, int height,
+                                int stride, int channels, float* d_disparity, float* d_confidence,
+                                uint8_t* d_invalid_reason, uint8_t* d_reliable_mask) {
+    if (!e) return apgcu::kInternalError;
+    if (int v = check_views(d_left, d_right, width, height, stride, channels)) return v;
+    try {
+        return e->eng->process_device(d_left, d_right, width, height, stride, channels, d_disparity, d_confidence,
+                                      d_invalid_reason, d_reliable_mask);
+    } catch (...) {
+        return apgcu::kInternalError;
+    }
+}
+
+int apgcu_engine_sync(apgcu_engine_t e) { return e ? e->eng->sync() : apgcu::kInternalError; }
+
+int apgcu_engine_dump(apgcu_engine_t e, int what, void* host_dst, size_t bytes) {
+    if (!e || !host_dst) return apgcu::kInternalError;
+    return e->eng->dump(what, host_dst, bytes);
+}
+
+int apgcu_engine_stage_times(apgcu_engine_t e, double* ms11) {
+    if (!e || !ms11) return apgcu::kInternalError;
+    e->eng->stage_times(ms11);
+    return 0;
+}
+
+size_t apgcu_engine_allocated_bytes(apgcu_engine_t e) { return e ? e->eng->allocated_bytes() : 0; }
+
+size_t apgcu_workspace_bytes(const apg_pipeline_config_t* cfg, int width, int height) {
+    if (!cfg || width <= 0 || height <= 0) return 0;
+    return apgcu::Engine::make_layout(*cfg, width, height, 3, 0).total;
+}
+
+void apgcu_engine_release(apgcu_engine_t e) {
+    if (e) e->eng->release();
+}
+
+void* apgcu_engine_stream(apgcu_engine_t e) { return e ? static_cast<void*>(e->eng->stream()) : nullptr; }
+
+void apgcu_config_from_mode(int mode, int max_disparity, apg_pipeline_config_t* out) {
+    if (out) *out = apg_config_from_mode(mode, max_disparity);
+}
+
+unsigned long long apgcu_kernel_launch_count(void) { return apgcu::launch_count(); }
+
+int apgcu_engine_launch_profile(apgcu_engine_t e, int max, const char** names, float* ms) {
+    return e ? e->eng->launch_profile(max, names, ms) : 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,130 @@
+// Device pipeline for one stereo pair at a time: workspace arena, stage orchestration, timing.
+//
+// Mirrors StereoMatcher::compute_impl (src/pipeline.cpp:435-719): aux -> search range / prior ->
+// cost (+cross-H, +right argmin) -> right-WTA -> cross-V -> SGM sweeps (+WTA) -> confidence ->
+// refine -> LR -> fill -> median.  Everything between the input upload and the output download
+// runs on one CUDA stream with no host synchronisation, except the HighQuality refiner, which
+// needs one device->host read of the per-pass draw count (the draws come from the C++ standard
+// library's mt19937 / uniform_int_distribution, exactly like the reference).
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <random>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/apg_sgm/pipeline_config.h"
+#include "kernels.h"
+
+namespace apgcu {
+
+enum Status : int {
+    kOk = 0, kEmptyInput = 1, kSizeMismatch = 2, kInvalidDisparityRange = 3, kInvalidConfig = 4,
+    kUnsupportedBackend = 5, kResourceLimitExceeded = 6, kAllocationFailure = 7, kInternalError = 8
+};
+
+// Frame-size-dependent layout of the device arena.
+struct Layout {
+    int w = 0, h = 0, ch = 0, D = 0, Dp = 0;
+    bool fused_fast = false;  // Fast path: costs recomputed inside the SGM sweeps, no volume
+    bool cross = false;
+    bool raw_cost = false;    // debug: materialise the raw volume
+    size_t total = 0;
+    // offsets
+    size_t in_left, in_right;
+    size_t lgray, lgx, lgy, rgray, rgx, rgy;
+    size_t cl, cr;
+    size_t rmin, rmax, rkey;
+    size_t disp_right, disp_wta, best, second, confidence, disp_ref, disp_lr, disp_fill, disp_out, d_prior;
+    size_t reliable, reason_conf, reason;
+    size_t volA, volB, volS, volRaw;
+    size_t lut, qlut, magic;
+    // HighQuality prior / refine
+    size_t pr_cand, pr_ncand, pr_taken, pr_grid, pr_maps, pr_scratch, pr_count;
+    size_t rf_prefix, rf_draws, rf_scan_tmp, rf_count;
+    size_t rf_scan_tmp_bytes = 0;
+    int n_cells = 0, gw = 0, gh = 0, max_cand = 0;
+};
+
+class Engine {
+public:
+    Engine(const apg_pipeline_config_t& cfg, int device, cudaStream_t stream);
+    ~Engine();
+
+    int process_host(const uint8_t* left, const uint8_t* right, int w, int h, int stride, int ch,
+                     float* disp, float* conf, uint8_t* reason, uint8_t* reliable);
+    int process_device(const uint8_t* dl, const uint8_t* dr, int w, int h, int stride, int ch,
+                       float* d_disp, float* d_conf, uint8_t* d_reason, uint8_t* d_reliable);
+    int sync();
+    int dump(int what, void* dst, size_t bytes);
+    void stage_times(double* ms11) const;
+    size_t allocated_bytes() const { return arena_bytes_ + pinned_bytes_; }
+    void release();
+    cudaStream_t stream() const { return stream_; }
+    const std::string& last_error() const { return err_; }
+    void set_debug(int f) { debug_ = f; }
+    int debug() const { return debug_; }
+    const apg_pipeline_config_t& config() const { return cfg_; }
+    int device() const { return device_; }
+
+    // Validation shared with the session layer (src/pipeline.cpp:171-232 + device limits).
+    static int validate_config(const apg_pipeline_config_t& c, std::string& msg);
+    static Layout make_layout(const apg_pipeline_config_t& c, int w, int h, int ch, int debug);
+
+private:
+    int prepare(int w, int h, int ch);
+    int run(const uint8_t* dl, int lstride, const uint8_t* dr, int rstride, int ch, float* d_disp, float* d_conf,
+            uint8_t* d_reason, uint8_t* d_reliable);
+    int run_prior();
+    int run_refine(float* work);
+    int fail(int code, const std::string& m) { err_ = m; return code; }
+    int cuda_fail(cudaError_t e, const char* where);
+    template <typename T> T* ptr(size_t off) const { return reinterpret_cast<T*>(arena_ + off); }
+    CostCtx cost_ctx() const;
+
+    apg_pipeline_config_t cfg_;
+    int device_ = 0;
+    int debug_ = 0;
+    cudaStream_t stream_ = nullptr;
+    bool own_stream_ = false;
+    unsigned char* arena_ = nullptr;
+    size_t arena_bytes_ = 0;
+    Layout lay_;
+    // host staging (pinned)
+    unsigned char* pin_ = nullptr;
+    size_t pinned_bytes_ = 0;
+    std::vector<float> lut_host_;
+    std::vector<uint16_t> qlut_host_;
+    cudaEvent_t ev_[12] = {};
+    bool have_times_ = false;
+    // per-launch profile (APGCU_DEBUG_PROFILE): event after every launch, on the engine stream
+    static constexpr int kMaxProf = 64;
+    cudaEvent_t pev_[kMaxProf + 1] = {};
+    const char* pname_[kMaxProf] = {};
+    int nprof_ = 0;
+    void prof_mark(const char* name);
+
+public:
+    int launch_profile(int max, const char** names, float* ms) const;
+
+private:
+    int support_count_ = 0;
+    std::string err_;
+};
+
+// Process-wide launch counter (reported by bench.py as gpu_launches).
+void count_launches(unsigned n);
+
+// prior.cu / refine.cu
+cudaError_t launch_prior(const apg_pipeline_config_t& cfg, const CostCtx& c, const Layout& L, unsigned char* arena,
+                         cudaStream_t s, unsigned* launches);
+cudaError_t launch_refine_count(const Layout& L, unsigned char* arena, const float* work, int fwd, int* d_count,
+                                cudaStream_t s, unsigned* launches);
+cudaError_t launch_refine_pass(const apg_pipeline_config_t& cfg, const CostCtx& c, const Layout& L,
+                               unsigned char* arena, float* work, int fwd, cudaStream_t s, unsigned* launches);
+size_t refine_scan_temp_bytes(int n);
+
+}  // namespace apgcu

@@ -1,0 +1,82 @@
+// Host-side launch interface of the apg-sgm sm_100a kernels (internal to the library).
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace apgcu {
+
+// aux.cu
+cudaError_t launch_aux(const uint8_t* src, int stride, int ch, int w, int h, int census64, uint8_t* gray,
+                       uint8_t* gx, uint8_t* gy, uint32_t* census, unsigned long long* census_wide,
+                       cudaStream_t s);
+
+// cost.cu: mode 0 raw volume, 1 cross-H volume, 2 right argmin only; all update rkey.
+cudaError_t launch_cost(const CostCtx& c, int mode, int lmax, int tau, uint32_t* vol, uint32_t* rkey,
+                        const uint32_t* magic, cudaStream_t s);
+size_t cost_kernel_smem_bytes(int D, int Dp, int lmax, bool cross, bool census64);
+cudaError_t launch_right_wta_finalize(const CostCtx& c, const uint32_t* rkey, int subpixel, float* disp_right,
+                                      cudaStream_t s);
+
+// cross.cu
+cudaError_t launch_cross_v(int w, int h, int d0, int D, int Dp, int lmax, int tau, const uint8_t* gray,
+                           const int16_t* rmin, const int16_t* rmax, const uint32_t* tin, uint32_t* cout,
+                           const uint32_t* magic, cudaStream_t s);
+cudaError_t launch_cross_h(int w, int h, int d0, int D, int Dp, int lmax, int tau, const uint8_t* gray,
+                           const int16_t* rmin, const int16_t* rmax, const uint32_t* vin, uint32_t* vout,
+                           const uint32_t* magic, cudaStream_t s);
+size_t cross_v_smem_bytes(int Dp, int lmax);
+
+// sgm.cu
+struct SgmPathLaunch {
+    int w, h, d0, D, Dp;
+    int dx, dy;
+    int mode;  // 0 first (store), 1 accumulate, 2 last (accumulate + WTA)
+    SgmPen pen;
+    const uint8_t* gray;
+    const uint32_t* cvol;  // nullptr -> census source (cl, cr, qlut)
+    const uint32_t* cl;
+    const uint32_t* cr;
+    const uint16_t* qlut;
+    const int16_t* rmin;
+    const int16_t* rmax;
+    uint32_t* S;
+    float* disp;
+    float* best;
+    float* second;
+    int subpixel;
+    int store_final;  // last sweep: also write the final sum (stage dumps)
+};
+cudaError_t launch_sgm_path(const SgmPathLaunch& l, cudaStream_t s);
+
+// post.cu
+struct ConfLrArgs {
+    int w, h;
+    const float* disp;
+    const float* disp_right;
+    const float* best;
+    const float* second;
+    const uint8_t* lgx;
+    const uint8_t* lgy;
+    float uniqueness_ratio, min_texture, reliable_threshold;
+    int conf_lr_max_diff;
+    float* confidence;
+    uint8_t* reliable;
+    uint8_t* reason;
+    int fuse_lr, lr_check, post_lr_max_diff;
+    float* disp_out;
+};
+cudaError_t launch_conf_lr(const ConfLrArgs& a, cudaStream_t s);
+cudaError_t launch_lr(int w, int h, int lr_max_diff, const float* dr, const float* din, float* dout,
+                      uint8_t* reason, cudaStream_t s);
+cudaError_t launch_fill(int w, int h, int gap, const float* in, const uint8_t* reason, const uint8_t* gray,
+                        const float* d_prior, float* out, cudaStream_t s);
+cudaError_t launch_median(int w, int h, int r, const float* in, float* out, cudaStream_t s);
+
+// range.cu (default range, HQ prior, refine)
+cudaError_t launch_default_range(int w, int h, int d0, int dmax, int16_t* rmin, int16_t* rmax, cudaStream_t s);
+
+}  // namespace apgcu

@@ -1,0 +1,357 @@
+#!/usr/bin/env python
+"""Benchmark of the apg-sgm B200 engine (one JSON line on rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--workload NAME]
+
+A step is one stereo pair through the whole dense-matching pipeline (aux, cost + right-image
+WTA, SGM sweeps + WTA, confidence / LR / fill / median).  `value` is W*H*D per second over all
+ranks with the pair already resident in HBM and the L2 flushed between steps; `e2e` is the same
+metric through the public session API (apg_session_process) with host buffers, the
+host->device and device->host copies inside every step.  Multi-GPU runs are independent
+replicas (the pipeline has no exchange step): every rank processes its own pairs, the device
+time is the max over ranks.  `--impl reference` times the reference's own CPU implementation
+(oracle/_ref, its AVX2/OpenMP Packed backend) on the host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOADS = {
+    # name: (mode, PairSpec args, label)
+    "fast720": (0, (1280, 720, 128, 12, 0, 120, 0.0), "fast_1280x720_d128"),
+    "balanced640": (1, (640, 480, 64, 8, 4, 60, 0.0), "balanced_640x480_d64"),
+    "hq1080": (2, (1920, 1080, 256, 16, 0, 240, 0.2), "highquality_1920x1080_d256"),
+    "kitti1242": (1, (1242, 375, 192, 12, 0, 180, 0.0), "balanced_1242x375_d192"),
+}
+MODE_NAMES = {0: "Fast", 1: "Balanced", 2: "HighQuality"}
+METRIC = "W*H*D/s at 720p D=128 (Fast, bit-exact)"
+
+
+def _peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def _profile_traffic(kernel: str, workload: str):
+    """dram read+write bytes per launch from the committed ncu summary, if one exists."""
+    f = ROOT / "profiles" / f"{kernel}_{workload}.txt"
+    if not f.exists():
+        return None
+    for line in f.read_text().splitlines():
+        if line.startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].strip())
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def _algorithmic_bytes(name: str, w: int, h: int, D: int, Dp: int) -> float:
+    """Bytes a launch of `name` must move by design (roofline section)."""
+    n = w * h
+    return {
+        "sgm_first": n * D * 2.0,            # write the path sum
+        "sgm_accum": n * D * 4.0,            # read + write the path sum
+        "sgm_last_wta": n * D * 2.0 + n * 12,  # read the path sum, write disparity/best/second
+        "cost+crossH": n * D * 2.0,          # write the horizontally aggregated volume
+        "crossV": n * D * 4.0,               # read T, write C
+        "cost": n * D * 2.0,
+    }.get(name, 0.0)
+
+
+def run_reference(args, wl):
+    """The reference CPU path (oracle/_ref) on the host cores, rank 0 only."""
+    from oracle import oracle as O
+    from apg_sgm_b200 import synthetic as S
+    mode, spec, label = wl
+    spec = S.PairSpec(*spec)
+    L, R, _ = S.make_pair(spec, S.SEED_BASE)
+    if not O.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libapg_ref.so not built"}))
+        return
+    cfg = O.config(mode, spec.max_disparity, volume_backend=2)  # Packed: the AVX2/OpenMP path
+    sess = O.RefSession(cfg, bounded_reuse=True)
+    for _ in range(args.warmup):
+        sess.process(L, R)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        r = sess.process(L, R)
+        times.append(time.perf_counter() - t0)
+        assert r["status"] == 0
+    vox = spec.width * spec.height * spec.max_disparity
+    total = sum(times)
+    value = vox * args.steps / total
+    cores = O.ref_threads()
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "voxels/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": "synthetic",
+        "config": {"workload": label, "mode": MODE_NAMES[mode], "width": spec.width, "height": spec.height,
+                   "max_disparity": spec.max_disparity, "backend": "Packed (AVX2/OpenMP)"},
+        "cpu_baseline": {"value": value, "unit": "voxels/s", "cores": cores, "kind": "reference",
+                         "sample": f"{args.steps} pairs {spec.width}x{spec.height} D{spec.max_disparity} "
+                                   f"{MODE_NAMES[mode]}, reference StereoSession Packed backend"},
+        "e2e": {"value": value, "unit": "voxels/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def cpu_baseline(spec, mode, L, R, gpu_out):
+    """Time the reference (Packed, all host cores) on pair 0 and check the GPU output against it."""
+    from oracle import oracle as O
+    vox = spec.width * spec.height * spec.max_disparity
+    if O.ref_available():
+        cfg = O.config(mode, spec.max_disparity, volume_backend=2)
+        sess = O.RefSession(cfg, bounded_reuse=True)
+        for _ in range(2):
+            ref = sess.process(L, R)
+        ts = []
+        for _ in range(5):
+            t0 = time.perf_counter()
+            ref = sess.process(L, R)
+            ts.append(time.perf_counter() - t0)
+        med = statistics.median(ts)
+        cfg_d = O.config(mode, spec.max_disparity, volume_backend=1)  # Auto==Dense for Fast/Balanced
+        sd = O.RefSession(cfg_d, bounded_reuse=True)
+        sd.process(L, R)
+        t0 = time.perf_counter()
+        sd.process(L, R)
+        dense_s = time.perf_counter() - t0
+        parity = all(np.array_equal(np.ascontiguousarray(gpu_out[k]).view(np.uint8),
+                                    np.ascontiguousarray(ref[k]).view(np.uint8))
+                     for k in ("disparity", "confidence", "invalid_reason", "reliable_mask"))
+        return {"value": vox / med, "unit": "voxels/s", "cores": O.ref_threads(), "kind": "reference",
+                "sample": f"pair 0 ({spec.width}x{spec.height} D{spec.max_disparity} {MODE_NAMES[mode]}), "
+                          f"reference Packed backend, 2 warm-up + median of 5",
+                "ms_per_pair": med * 1000, "dense_backend_ms_per_pair": dense_s * 1000,
+                "stage_ms": ref["stage_ms"]}, parity
+    cfg = O.config(mode, spec.max_disparity)
+    t0 = time.perf_counter()
+    o = O.pipeline(cfg, L, R)
+    dt = time.perf_counter() - t0
+    parity = all(np.array_equal(np.ascontiguousarray(gpu_out[k]).view(np.uint8),
+                                np.ascontiguousarray(o[k]).view(np.uint8))
+                 for k in ("disparity", "confidence", "invalid_reason", "reliable_mask"))
+    return {"value": vox / dt, "unit": "voxels/s", "cores": os.cpu_count(), "kind": "port",
+            "sample": "pair 0, C oracle, 1 run"}, parity
+
+
+def run_b200(args, wl):
+    import torch
+    import apg_sgm_b200 as apg
+    from apg_sgm_b200 import synthetic as S
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+
+    mode, spec_args, label = wl
+    spec = S.PairSpec(*spec_args)
+    w, h, D = spec.width, spec.height, spec.max_disparity
+    Dp = (D + 63) // 64 * 64
+    npairs = 2
+    pairs = [S.make_pair(spec, S.SEED_BASE + rank * npairs + i)[:2] for i in range(npairs)]
+    cfg = apg.config_from_mode(mode, D)
+    eng = apg.Engine(cfg, device=local)
+    es = torch.cuda.ExternalStream(eng.stream, device=dev)
+    d_in = [(torch.from_numpy(l).to(dev), torch.from_numpy(r).to(dev)) for l, r in pairs]
+    d_disp = torch.empty((h, w), dtype=torch.float32, device=dev)
+    d_conf = torch.empty((h, w), dtype=torch.float32, device=dev)
+    d_reason = torch.empty((h, w), dtype=torch.uint8, device=dev)
+    d_rel = torch.empty((h, w), dtype=torch.uint8, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    torch.cuda.synchronize()
+
+    def step(i):
+        l, r = d_in[i % npairs]
+        eng.process_device(l.data_ptr(), r.data_ptr(), w, h, w, 1, d_disp.data_ptr(), d_conf.data_ptr(),
+                           d_reason.data_ptr(), d_rel.data_ptr())
+
+    for i in range(max(args.warmup, 3)):
+        step(i)
+    eng.sync()
+    eng.set_debug(apg.DEBUG_PROFILE)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    per_kernel = {}
+    sampler = ClockSampler(local)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    launches0 = apg.kernel_launch_count()
+    with torch.cuda.stream(es):
+        for k in range(args.steps):
+            flush.zero_()  # L2 flush outside the timed step
+            starts[k].record(es)
+            step(k)
+            ends[k].record(es)
+            for name, ms in eng.launch_profile():  # syncs on this step's last launch
+                per_kernel.setdefault(name, []).append(ms)
+    torch.cuda.synchronize()
+    launches = apg.kernel_launch_count() - launches0
+    clocks = sampler.stop()
+    eng.set_debug(0)
+    dev_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+    t = torch.tensor([dev_ms], dtype=torch.float64, device=dev)
+    if dist:
+        dist.barrier()
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    max_ms = float(t.item())
+    vox = w * h * D
+    value = vox * args.steps * world / (max_ms / 1000.0)
+
+    # end to end through the public session API (host buffers, copies inside every step)
+    sess = apg.StereoSession(mode=MODE_NAMES[mode].lower() if mode != 2 else "high_quality", max_disparity=D,
+                             memory_policy="bounded_reuse")
+    for i in range(max(args.warmup, 3)):
+        sess.process(*pairs[i % npairs])
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        res = sess.process(*pairs[k % npairs])
+        _ = float(res.disparity[0, 0])  # the step's result is on the host
+    e2e_s = time.perf_counter() - t0
+    te = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+    if dist:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = vox * args.steps * world / float(te.item())
+
+    # dominant kernel and its roofline
+    peak, peak_kind = _peaks()
+    totals = {k: sum(v) for k, v in per_kernel.items() if k != "copy"}
+    top = max(totals, key=totals.get)
+    top_avg_ms = statistics.mean(per_kernel[top])
+    alg = _algorithmic_bytes(top, w, h, D, Dp)
+    achieved = alg / (top_avg_ms / 1000.0) / 1e9
+    prof_total = sum(totals.values())
+    roofline = {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_kind": peak_kind,
+                "traffic": _profile_traffic(top, label), "algorithmic_bytes_per_launch": alg,
+                "avg_launch_ms": top_avg_ms,
+                "kernel_shares": {k: round(v / prof_total, 4) for k, v in sorted(totals.items(), key=lambda x: -x[1])},
+                "kernel_avg_ms": {k: round(statistics.mean(per_kernel[k]), 5) for k in totals}}
+
+    out = {
+        "metric": METRIC, "value": value, "unit": "voxels/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u16", "data": "synthetic",
+        "config": {"workload": label, "mode": MODE_NAMES[mode], "width": w, "height": h, "max_disparity": D,
+                   "pairs_per_step": 1, "distinct_pairs": npairs, "l2": "flushed between steps (256 MiB write)",
+                   "parallelism": f"replicas x{world}"},
+        "e2e": {"value": e2e_value, "unit": "voxels/s", "h2d_bytes_per_step": 2 * w * h,
+                "d2h_bytes_per_step": w * h * 10, "api": "apg_session_process (BoundedReuse)"},
+        "gpu_launches": launches,
+        "roofline": roofline,
+        "clocks": clocks,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        gpu0 = eng.process(*pairs[0])
+        cb, parity = cpu_baseline(spec, mode, pairs[0][0], pairs[0][1], gpu0)
+        out["cpu_baseline"] = cb
+        out["parity_vs_cpu_baseline"] = "bit-exact" if parity else "MISMATCH"
+    if rank == 0:
+        print(json.dumps(out))
+    del sess
+    eng.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="fast720")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    wl = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        if int(os.environ.get("RANK", "0")) == 0:
+            run_reference(args, wl)
+        return
+    run_b200(args, wl)
+
+
+if __name__ == "__main__":
+    main()

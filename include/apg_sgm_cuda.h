@@ -1,0 +1,114 @@
+/* apg-sgm B200 engine: extended C-ABI.
+ *
+ * The reference-compatible session API lives in apg_sgm/c_api.h and is implemented by the same
+ * library (libapg_sgm_b200.so).  This header adds the entry points a host needs beyond that API:
+ * an engine over an explicit configuration record, device-pointer processing on a caller stream,
+ * stage dumps for parity checking, the batched form and the served form.
+ *
+ * Every function is extern "C" with plain pointers and sizes; no exception crosses the ABI.
+ * Status codes are the reference's apg_status_code_t values (0 = OK).
+ */
+#ifndef APG_SGM_CUDA_H
+#define APG_SGM_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "apg_sgm/c_api.h"
+#include "apg_sgm/pipeline_config.h"
+
+#if defined(__GNUC__) && __GNUC__ >= 4
+#define APGCU_API __attribute__((visibility("default")))
+#else
+#define APGCU_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct apgcu_engine_s* apgcu_engine_t;
+
+/* Intermediates that apgcu_engine_dump can copy out after a process call. */
+enum {
+    APGCU_DUMP_LEFT_GRAY = 0, APGCU_DUMP_LEFT_GX, APGCU_DUMP_LEFT_GY,
+    APGCU_DUMP_RIGHT_GRAY, APGCU_DUMP_RIGHT_GX, APGCU_DUMP_RIGHT_GY,  /* u8  W*H */
+    APGCU_DUMP_CENSUS_LEFT, APGCU_DUMP_CENSUS_RIGHT,                  /* u32 W*H (u64 for 9x7) */
+    APGCU_DUMP_RANGE_MIN, APGCU_DUMP_RANGE_MAX,                        /* i16 W*H */
+    APGCU_DUMP_COST_RAW,        /* u16 W*H*D  (needs APGCU_DEBUG_RAW_COST) */
+    APGCU_DUMP_COST_AGG,        /* u16 W*H*D  (cross-aggregated volume; Balanced/HQ) */
+    APGCU_DUMP_SGM_SUM,         /* u16 W*H*D  (needs APGCU_DEBUG_KEEP_SUM) */
+    APGCU_DUMP_DISP_WTA, APGCU_DUMP_BEST, APGCU_DUMP_SECOND, APGCU_DUMP_DISP_RIGHT,
+    APGCU_DUMP_CONFIDENCE, APGCU_DUMP_RELIABLE, APGCU_DUMP_REASON_CONF,
+    APGCU_DUMP_DISP_REFINED, APGCU_DUMP_DISP_LR, APGCU_DUMP_REASON, APGCU_DUMP_DISP_FILL,
+    APGCU_DUMP_DISPARITY, APGCU_DUMP_D_PRIOR,
+    APGCU_DUMP_COUNT
+};
+
+/* Debug flags (apgcu_engine_set_debug). */
+#define APGCU_DEBUG_RAW_COST 1   /* also materialise the raw cost volume */
+#define APGCU_DEBUG_KEEP_SUM 2   /* also store the final path sum */
+#define APGCU_DEBUG_NO_FUSION 4  /* Fast mode: read a stored volume instead of recomputing costs */
+#define APGCU_DEBUG_PROFILE 8    /* record a CUDA event after every launch (apgcu_engine_launch_profile) */
+
+/* Engine on CUDA device `device`.  stream may be NULL (the engine creates its own) or a
+ * cudaStream_t the caller keeps alive for the engine's lifetime.  Returns NULL on failure. */
+APGCU_API apgcu_engine_t apgcu_engine_create(const apg_pipeline_config_t* cfg, int device, void* stream);
+APGCU_API void apgcu_engine_destroy(apgcu_engine_t e);
+APGCU_API const char* apgcu_engine_last_error(apgcu_engine_t e);
+APGCU_API int apgcu_engine_set_debug(apgcu_engine_t e, int flags);
+
+/* One pair from HOST memory (strided, 1 or 3 channels); outputs are host arrays of W*H.
+ * Copies in and out are part of the call.  Any output pointer may be NULL. */
+APGCU_API int apgcu_engine_process(apgcu_engine_t e, const uint8_t* left, const uint8_t* right, int width,
+                                   int height, int stride, int channels, float* disparity, float* confidence,
+                                   uint8_t* invalid_reason, uint8_t* reliable_mask);
+
+/* One pair already resident in DEVICE memory; outputs are device arrays.  Enqueued on the
+ * engine stream; returns after enqueueing (call apgcu_engine_sync to wait). */
+APGCU_API int apgcu_engine_process_device(apgcu_engine_t e, const uint8_t* d_left, const uint8_t* d_right,
+                                          int width, int height, int stride, int channels, float* d_disparity,
+                                          float* d_confidence, uint8_t* d_invalid_reason,
+                                          uint8_t* d_reliable_mask);
+APGCU_API int apgcu_engine_sync(apgcu_engine_t e);
+
+/* Copy intermediate `what` (APGCU_DUMP_*) of the last processed pair to host memory. */
+APGCU_API int apgcu_engine_dump(apgcu_engine_t e, int what, void* host_dst, size_t bytes);
+
+/* Per-stage device times of the last pair (ms): aux, prior, cost, cross, right_wta, sgm, wta,
+ * confidence, refine, post, total -- the reference StageTiming fields in declaration order. */
+APGCU_API int apgcu_engine_stage_times(apgcu_engine_t e, double* ms11);
+
+/* Per-launch device times of the last pair (needs APGCU_DEBUG_PROFILE): up to max entries of
+ * (static kernel name, ms); returns the number written. */
+APGCU_API int apgcu_engine_launch_profile(apgcu_engine_t e, int max, const char** names, float* ms);
+
+/* Bytes of device workspace the engine holds now, and would need for a W x H pair. */
+APGCU_API size_t apgcu_engine_allocated_bytes(apgcu_engine_t e);
+APGCU_API size_t apgcu_workspace_bytes(const apg_pipeline_config_t* cfg, int width, int height);
+APGCU_API void apgcu_engine_release(apgcu_engine_t e);
+
+/* Stream the engine enqueues on (a cudaStream_t). */
+APGCU_API void* apgcu_engine_stream(apgcu_engine_t e);
+
+/* PipelineConfig::from_mode (src/config.cpp:5-45) into *out. */
+APGCU_API void apgcu_config_from_mode(int mode, int max_disparity, apg_pipeline_config_t* out);
+
+/* Session over a full configuration record (the reference's C++ StereoSession(PipelineConfig,
+ * ExecutionOptions) constructor, include/apg_sgm/session.hpp:19-23); processed with
+ * apg_session_process like any other session. */
+APGCU_API apg_session_t apgcu_session_create_config(const apg_pipeline_config_t* cfg, int memory_policy,
+                                                    size_t max_retained_bytes);
+/* PipelineStats of the last frame: stage_ms11 as apgcu_engine_stage_times; counters4 =
+ * {frame_allocation_count, frame_reuse_count, peak_workspace_bytes, retained_workspace_bytes}. */
+APGCU_API int apgcu_session_get_stats(apg_session_t s, double* stage_ms11, size_t* counters4);
+/* Workspace bytes the budget gate compares against max_retained_bytes for a W x H x C frame. */
+APGCU_API size_t apgcu_session_estimate_bytes(apg_session_t s, int width, int height, int channels);
+
+/* Number of kernels the library has launched in this process (all engines). */
+APGCU_API unsigned long long apgcu_kernel_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* APG_SGM_CUDA_H */

@@ -1,0 +1,169 @@
+"""GPU parity: every stage of the CUDA engine against the CPU oracle, bit for bit.
+
+The oracle (oracle/apg_oracle.c) is pinned to the reference by tests/test_oracle_pins.py.
+Integer stages (aux planes, census, ranges, cost volumes, path sums, masks) and float stages
+(sub-pixel disparities, confidence, fill, median) are all required to be bit-identical:
+tolerance 0, max |delta| = 0.
+"""
+import numpy as np
+import pytest
+
+from helpers import pattern, same_bits, synth, to_oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def _cases():
+    F, B, H = 0, 1, 2
+    return [
+        # name, mode, (w, h, dmax, dmin), input kind, overrides, debug flags
+        ("fast_160x120_d32", F, (160, 120, 32, 0), "synth", {}, 0),
+        ("fast_nofusion_160x120_d32", F, (160, 120, 32, 0), "synth", {}, 4),
+        ("balanced_97x61_d24", B, (97, 61, 24, 0), "synth", {}, 0),
+        ("balanced_160x120_d64", B, (160, 120, 64, 0), "synth", {}, 0),
+        ("balanced_100x80_d70", B, (100, 80, 70, 0), "synth", {}, 0),
+        ("hq_200x150_d48", H, (200, 150, 48, 0), "synth_patch", {}, 0),
+        ("hq_160x120_d32", H, (160, 120, 32, 0), "synth_patch", {}, 0),
+        ("negative_range_48x36", B, (48, 36, 8, -4), "noise", {}, 0),
+        ("rgb_fast_64x48", F, (64, 48, 16, 0), "rgb", {}, 0),
+        ("rgb_balanced_64x48", B, (64, 48, 16, 0), "rgb", {}, 0),
+        ("census9x7_balanced_96x64", B, (96, 64, 32, 0), "synth", {"census_type": 0}, 0),
+        ("census9x7_fast_96x64", F, (96, 64, 32, 0), "synth", {"census_type": 0}, 0),
+        ("path8_balanced_120x90_d40", B, (120, 90, 40, 0), "synth", {"paths": 8}, 0),
+        ("fast_260x40_d200", F, (260, 40, 200, 0), "synth", {}, 0),
+        ("balanced_agg2_80x60", B, (80, 60, 24, 0), "synth", {"agg_iterations": 2}, 0),
+        ("balanced_continuous_p2", B, (80, 60, 24, 0), "synth", {"piecewise_p2": 0}, 0),
+        ("balanced_min8_max40", B, (120, 60, 40, 8), "synth", {}, 0),
+        ("balanced_no_subpixel", B, (80, 60, 24, 0), "synth", {"subpixel": 0}, 0),
+        ("balanced_median_r2_nolr", B, (80, 60, 24, 0), "synth", {"median_radius": 2, "lr_check": 0}, 0),
+        ("balanced_median_off", B, (80, 60, 24, 0), "synth", {"median_radius": 0}, 0),
+        ("checker_odd_33x27", B, (33, 27, 16, 0), "checker", {}, 0),
+        ("row_33x1", B, (33, 1, 16, 0), "noise", {}, 0),
+        ("column_1x33", B, (1, 33, 16, 0), "noise", {}, 0),
+        ("pixel_1x1", F, (1, 1, 16, 0), "noise", {}, 0),
+        ("hq_d256_300x100", H, (300, 100, 256, 0), "synth_patch", {}, 0),
+    ]
+
+
+def _inputs(kind, w, h, dmax, dmin):
+    if kind == "synth":
+        return synth(w, h, dmax, cells=6, lo=max(dmin, 0), hi=max(dmin, 0) + max(1, (dmax - max(dmin, 0)) * 7 // 8))
+    if kind == "synth_patch":
+        return synth(w, h, dmax, cells=6, lo=0, hi=dmax * 7 // 8, patch=0.2)
+    if kind == "rgb":
+        l = pattern(w, h, 3, "noise")
+        r = np.roll(l, -3, axis=1)
+        return l, r
+    l = pattern(w, h, 1, kind)
+    return l, np.roll(l, -2, axis=1)
+
+
+CASES = _cases()
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c[0] for c in CASES])
+def test_stage_parity(case, O, apg):
+    name, mode, (w, h, dmax, dmin), kind, over, dbg = case
+    cfg = apg.config_from_mode(mode, dmax, dmin, **over)
+    L, R = _inputs(kind, w, h, dmax, dmin)
+    eng = apg.Engine(cfg, debug=apg.DEBUG_RAW_COST | apg.DEBUG_KEEP_SUM | dbg)
+    gpu = eng.process(L, R)
+    ocfg = to_oracle(O, cfg)
+    ora = O.pipeline(ocfg, L, R, stages=True)
+    assert ora["status"] == 0
+    aux = O.aux(L, R)
+
+    checks = [
+        ("left_gray", aux["left"]["gray"]), ("left_gx", aux["left"]["gx"]), ("left_gy", aux["left"]["gy"]),
+        ("right_gray", aux["right"]["gray"]), ("right_gx", aux["right"]["gx"]), ("right_gy", aux["right"]["gy"]),
+        ("census_left", aux["left"]["census" if cfg.census_type == 1 else "census64"]),
+        ("census_right", aux["right"]["census" if cfg.census_type == 1 else "census64"]),
+        ("range_min", ora["range_min"]), ("range_max", ora["range_max"]),
+        ("cost_raw", ora["cost_raw"]),
+    ]
+    if cfg.agg_enable:
+        checks.append(("cost_agg", ora["cost_agg"]))
+    s32 = ora["sgm_sum"]
+    assert int(s32[s32 != 0xFFFFFFFF].max(initial=0)) < 0xFFFF
+    checks.append(("sgm_sum", np.where(s32 == 0xFFFFFFFF, 0xFFFF, s32).astype(np.uint16)))
+    checks += [("disp_wta", ora["disp_wta"]), ("best", ora["best"]), ("second", ora["second"]),
+               ("disp_right", ora["disp_right"])]
+    if cfg.prior_enable:
+        checks.append(("d_prior", ora["d_prior"]))
+    if cfg.refine_enable:
+        checks.append(("disp_refined", ora["disp_refined"]))
+    if cfg.lr_check:
+        checks.append(("disp_lr", ora["disp_lr"]))
+    checks += [("disp_fill", ora["disp_fill"]), ("disparity", ora["disparity"])]
+    for stage, want in checks:
+        got = eng.dump(stage)
+        if not same_bits(got, want):
+            bad = np.argwhere(got != want)
+            i = tuple(bad[0]) if len(bad) else None
+            pytest.fail(f"{name}: stage {stage} differs at {len(bad)} positions; first {i}: gpu={got[i] if i else None} "
+                        f"oracle={want[i] if i else None}")
+    # final outputs of the host-copy path
+    for k in ("disparity", "confidence", "invalid_reason", "reliable_mask"):
+        assert same_bits(gpu[k], ora[k]), f"{name}: final {k} differs"
+    assert np.all(np.isfinite(gpu["disparity"]))
+    neg = gpu["disparity"][gpu["disparity"] < 0]
+    assert np.all(neg == -1.0)
+    assert np.all((gpu["confidence"] >= 0) & (gpu["confidence"] <= 1))
+
+
+def test_fast_fused_equals_unfused(apg):
+    L, R = synth(200, 100, 48)
+    cfg = apg.config_from_mode(0, 48)
+    a = apg.Engine(cfg).process(L, R)
+    b = apg.Engine(cfg, debug=apg.DEBUG_NO_FUSION).process(L, R)
+    for k in a:
+        assert same_bits(a[k], b[k]), k
+
+
+GOLDEN = {  # tests/test_api_contract.cpp:243-257 of the reference (w, h, invalid, reliable, disp, conf, inv, rel)
+    "Odd_Checkerboard": (33, 27, 0, 612, 0x1710451f7eab215, 0xe61822cc0fbe3a38, 0x22081e533cd30004, 0x9ade9d63e4fcae7b),
+    "Color_Noise": (32, 24, 0, 720, 0x7e8e0fa784351325, 0x5860e8f479cbe0fd, 0x82f55cc1fd68a695, 0x9db48cb5d76242b5),
+    "Negative_Disp_Range": (48, 36, 0, 178, 0x1d8e1d22713fcee9, 0x77f3c5cdbc782a05, 0x8ec5011cb7fb425, 0x3563e2187fb4a965),
+}
+
+
+@pytest.mark.parametrize("mode", [0, 1, 2])
+@pytest.mark.parametrize("tag", ["Odd_Checkerboard", "Color_Noise"])
+def test_golden_fingerprints_gpu(tag, mode, O, apg):
+    if tag == "Odd_Checkerboard":
+        img = pattern(33, 27, 1, "checker")
+    else:
+        img = pattern(32, 24, 3, "noise")
+    cfg = apg.config_from_mode(mode, 16)
+    out = apg.Engine(cfg).process(img, img)
+    w, h, inv, rel, dh, ch, ih, rh = GOLDEN[tag]
+    assert out["disparity"].shape == (h, w)
+    assert int((out["disparity"] < 0).sum()) == inv
+    assert int(out["reliable_mask"].sum()) == rel
+    assert O.fnv1a64(out["disparity"]) == dh
+    assert O.fnv1a64(out["confidence"]) == ch
+    assert O.fnv1a64(out["invalid_reason"]) == ih
+    assert O.fnv1a64(out["reliable_mask"]) == rh
+
+
+def test_golden_negative_range_gpu(O, apg):
+    img = pattern(48, 36, 1, "noise")
+    cfg = apg.config_from_mode(1, 8, -4)
+    out = apg.Engine(cfg).process(img, img)
+    w, h, inv, rel, dh, ch, ih, rh = GOLDEN["Negative_Disp_Range"]
+    assert O.fnv1a64(out["disparity"]) == dh
+    assert O.fnv1a64(out["confidence"]) == ch
+    assert O.fnv1a64(out["invalid_reason"]) == ih
+    assert O.fnv1a64(out["reliable_mask"]) == rh
+
+
+@pytest.mark.parametrize("mode,spec", [(1, (640, 480, 64, 8, 4, 60)), (0, (1280, 720, 128, 12, 0, 120))])
+def test_baseline_workloads_match_oracle(mode, spec, O, apg):
+    """The benchmark workloads themselves (640x480 D64 Balanced, 1280x720 D128 Fast)."""
+    from apg_sgm_b200 import synthetic as S
+    L, R, _ = S.make_pair(S.PairSpec(*spec), S.SEED_BASE)
+    cfg = apg.config_from_mode(mode, spec[2])
+    gpu = apg.Engine(cfg).process(L, R)
+    ora = O.pipeline(to_oracle(O, cfg), L, R)
+    for k in ("disparity", "confidence", "invalid_reason", "reliable_mask"):
+        assert same_bits(gpu[k], ora[k]), k
