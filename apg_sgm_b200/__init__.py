@@ -445,6 +445,11 @@ class Engine:
     def set_debug(self, flags: int):
         lib().apgcu_engine_set_debug(self._h, int(flags))
 
+    def set_tuning(self, key: str, value: int):
+        rc = lib().apgcu_engine_set_tuning(self._h, key.encode(), int(value))
+        if rc != 0:
+            raise ValueError(f"invalid tuning {key}={value}")
+
     @property
     def allocated_bytes(self) -> int:
         return int(lib().apgcu_engine_allocated_bytes(self._h))

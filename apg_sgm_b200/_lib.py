@@ -84,6 +84,7 @@ _SIGS = {
     "apgcu_engine_destroy": (None, [C.c_void_p]),
     "apgcu_engine_last_error": (C.c_char_p, [C.c_void_p]),
     "apgcu_engine_set_debug": (C.c_int, [C.c_void_p, C.c_int]),
+    "apgcu_engine_set_tuning": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int]),
     "apgcu_engine_process": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int,
                                        C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "apgcu_engine_process_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int,

@@ -32,6 +32,7 @@ struct CostCtx {
     int use_ad, use_grad, cost_max;
     float scale;       // cost_max / (1 + eta + mu), src/cost_computer.cpp:154-155
     const float* lut;  // kLutSize floats built on the host with std::exp
+    const uint16_t* qlut;  // 65 quantised census-only costs (same float ops, done on the host)
     const uint8_t *lgray, *lgx, *lgy, *rgray, *rgx, *rgy;
     const uint32_t *cl, *cr;
     const unsigned long long *cl64, *cr64;

@@ -45,7 +45,7 @@ __host__ __device__ inline void cost_smem_layout(int txc, int ha, int D, int Dp,
     *off_lut = o; o = align16(o + kLutSize * 4);
     *off_left = o; o = align16(o + (size_t)nx * (csz + 3 + 4));   // census, gray, gx, gy, rmin, rmax
     *off_right = o; o = align16(o + (size_t)nr * (csz + 3));      // census, gray, gx, gy
-    *off_cost = o; o = align16(o + (size_t)nx * Dp * 2);
+    *off_cost = o; o = align16(o + (size_t)nx * (Dp + 2) * 2);  // row stride Dp+2: conflict-free diagonals
     *off_pre = o;
     if (cross) o = align16(o + (size_t)(nx + 1) * (Dp / 2) * 8);
     *total = o;
@@ -62,6 +62,7 @@ __global__ void __launch_bounds__(256) cost_kernel(CostCtx c, int txc, int ha, i
     const int nx = txc + 2 * ha;
     const int nr = nx + c.D - 1;
     const int W2 = c.Dp / 2;  // 32-bit words per pixel
+    const int CS = W2 + 1;    // staged cost row stride in words (odd: diagonal reads hit distinct banks)
     float* s_lut = reinterpret_cast<float*>(smem + o_lut);
     const size_t csz = C64 ? 8 : 4;
     unsigned char* L = smem + o_left;
@@ -75,7 +76,9 @@ __global__ void __launch_bounds__(256) cost_kernel(CostCtx c, int txc, int ha, i
     const int row = y * c.w;
     const int tid = threadIdx.x, nt = blockDim.x;
 
+    __shared__ uint16_t s_q[65];
     for (int i = tid; i < kLutSize; i += nt) s_lut[i] = c.lut[i];
+    for (int i = tid; i < 65; i += nt) s_q[i] = c.qlut[i];
     // left aux (census, gray, gx, gy, rmin, rmax) for x in [xbase, xbase+nx)
     for (int i = tid; i < nx; i += nt) {
         const int x = xbase + i;
@@ -125,6 +128,12 @@ __global__ void __launch_bounds__(256) cost_kernel(CostCtx c, int txc, int ha, i
                     int pop;
                     if (C64) pop = __popcll(clv64 ^ reinterpret_cast<const unsigned long long*>(Rg)[ri]);
                     else pop = __popc(clv ^ reinterpret_cast<const uint32_t*>(Rg)[ri]);
+                    if (!c.use_ad && !c.use_grad) {
+                        // census-only cost: the host pre-quantised LUT (same float ops)
+                        q = s_q[pop];
+                        word = hsel == 0 ? ((word & 0xFFFF0000u) | q) : ((word & 0x0000FFFFu) | (q << 16));
+                        continue;
+                    }
                     float v = s_lut[kLutCensus + pop];
                     if (c.use_ad) v = __fadd_rn(v, s_lut[kLutAd + abs(gl - (int)Rg[nr * csz + ri])]);
                     if (c.use_grad) {
@@ -138,7 +147,7 @@ __global__ void __launch_bounds__(256) cost_kernel(CostCtx c, int txc, int ha, i
                 word = hsel == 0 ? ((word & 0xFFFF0000u) | q) : ((word & 0x0000FFFFu) | (q << 16));
             }
         }
-        s_cost[i] = word;
+        s_cost[xi * CS + k] = word;
     }
     __syncthreads();
 
@@ -155,7 +164,7 @@ __global__ void __launch_bounds__(256) cost_kernel(CostCtx c, int txc, int ha, i
             uint32_t best = kInvalidWord;
             for (int di = di_lo; di < di_hi; ++di) {
                 const int xi = xr + c.d0 + di - xbase;
-                const uint32_t v = s_c16[xi * c.Dp + di];
+                const uint32_t v = s_c16[xi * (c.Dp + 2) + di];
                 if (v != kInvalidCost) {
                     const uint32_t key = (v << 16) | (uint32_t)di;
                     best = key < best ? key : best;
@@ -170,7 +179,7 @@ __global__ void __launch_bounds__(256) cost_kernel(CostCtx c, int txc, int ha, i
             for (int i = tid; i < txc * W2; i += nt) {
                 const int xi = i / W2, k = i - xi * W2;
                 const int x = x0 + xi;
-                if (x < c.w) out_vol[((size_t)row + x) * W2 + k] = s_cost[(xi + ha) * W2 + k];
+                if (x < c.w) out_vol[((size_t)row + x) * W2 + k] = s_cost[(xi + ha) * CS + k];
             }
         }
         return;
@@ -184,7 +193,7 @@ __global__ void __launch_bounds__(256) cost_kernel(CostCtx c, int txc, int ha, i
         s_psum[k] = 0;
         s_pcnt[k] = 0;
         for (int xi = 0; xi < nx; ++xi) {
-            const uint32_t v = s_cost[xi * W2 + k];
+            const uint32_t v = s_cost[xi * CS + k];
             const uint32_t inval = __vcmpeq2(v, kInvalidWord);  // 0xFFFF per invalid half
             ps = __vadd2(ps, v & ~inval);
             pc = __vadd2(pc, 0x00010001u & ~inval);

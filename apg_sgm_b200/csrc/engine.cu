@@ -38,8 +38,10 @@ bool u16_path_ok(const apg_pipeline_config_t& c) {
     const long long p2max = std::max<long long>(c.P2_base, (long long)c.P1 + 1);
     const long long path_max = (long long)c.cost_max + p2max;
     const int npath = c.paths == 8 ? 8 : 4;
-    if ((long long)npath * path_max >= 65535) return false;
-    if (path_max + p2max >= 65535) return false;
+    // Path values use 0x7FFF as "invalid": valid sums must stay below it and an invalid value
+    // plus P2 and P1 must not wrap 16 bits.
+    if ((long long)npath * path_max >= 0x7FFF) return false;
+    if (p2max + c.P1 >= 0x7FFF) return false;
     if (!c.piecewise_p2 && c.adaptive_penalties && c.p2_alpha < 0.f) return false;
     return true;
 }
@@ -104,7 +106,7 @@ Layout Engine::make_layout(const apg_pipeline_config_t& c, int w, int h, int ch,
     L.Dp = round_up(L.D, 64);
     L.cross = c.agg_enable != 0;
     L.fused_fast = !L.cross && c.census_type == APG_CENSUS_SYMMETRIC_9X7 && !c.use_ad && !c.use_grad &&
-                   !(debug & 4);
+                   !c.prior_enable && !(debug & 4);
     L.raw_cost = (debug & 1) != 0;
     const size_t n = (size_t)w * h;
     const size_t csz = c.census_type == APG_CENSUS_9X7 ? 8 : 4;
@@ -122,11 +124,13 @@ Layout Engine::make_layout(const apg_pipeline_config_t& c, int w, int h, int ch,
     L.confidence = take(n * 4); L.disp_ref = take(n * 4); L.disp_lr = take(n * 4); L.disp_fill = take(n * 4);
     L.disp_out = take(n * 4); L.d_prior = take(n * 4);
     L.reliable = take(n); L.reason_conf = take(n); L.reason = take(n);
-    // volumes: Balanced/HQ: A = cross-H output then path sum, B = aggregated cost.
-    //          Fast fused: A = path sum only.  Fast non-fused: A = raw cost, B = path sum.
+    // volA: cross-H output T (Balanced/HQ), raw cost (Fast without fusion) or the first path-sum
+    // buffer (fused Fast); volB: aggregated cost.  The first SGM phase writes one buffer per
+    // direction (3 for Path4, 7 for Path8); buffer 0 reuses volA whenever volA is dead by then.
     L.volA = take(vol);
-    L.volB = (L.cross || !L.fused_fast) ? take(vol) : 0;
-    L.volS = L.cross ? L.volA : (L.fused_fast ? L.volA : L.volB);
+    L.volB = L.cross ? take(vol) : 0;
+    L.nsbuf = (c.paths == 8 ? 8 : 4) - 1;
+    for (int i = 0; i < L.nsbuf; ++i) L.sbuf[i] = (i == 0 && (L.cross || L.fused_fast)) ? L.volA : take(vol);
     L.volRaw = L.raw_cost ? take(vol) : 0;
     L.lut = take(kLutSize * 4);
     L.qlut = take(65 * 2);
@@ -219,6 +223,7 @@ CostCtx Engine::cost_ctx() const {
     const float norm = 1.f + (cfg_.use_ad ? cfg_.eta_ad : 0.f) + (cfg_.use_grad ? cfg_.mu_grad : 0.f);
     c.scale = static_cast<float>(cfg_.cost_max) / std::max(norm, 1e-6f);
     c.lut = ptr<float>(lay_.lut);
+    c.qlut = ptr<uint16_t>(lay_.qlut);
     c.lgray = ptr<uint8_t>(lay_.lgray); c.lgx = ptr<uint8_t>(lay_.lgx); c.lgy = ptr<uint8_t>(lay_.lgy);
     c.rgray = ptr<uint8_t>(lay_.rgray); c.rgx = ptr<uint8_t>(lay_.rgx); c.rgy = ptr<uint8_t>(lay_.rgy);
     c.cl = ptr<uint32_t>(lay_.cl); c.cr = ptr<uint32_t>(lay_.cr);
@@ -400,29 +405,31 @@ int Engine::run(const uint8_t* dl, int lstride, const uint8_t* dr, int rstride, 
         sgm_src = ptr<uint32_t>(L.volB);
     }
     cudaEventRecord(ev_[5], s);
-    // SGM sweeps: horizontal, diagonal, then vertical; the last one carries the WTA.
-    static const int order4[4][2] = {{1, 0}, {-1, 0}, {0, 1}, {0, -1}};
-    static const int order8[8][2] = {{1, 0}, {-1, 0}, {1, 1}, {1, -1}, {-1, 1}, {-1, -1}, {0, 1}, {0, -1}};
-    const int npath = cfg_.paths == 8 ? 8 : 4;
-    SgmPathLaunch pl;
+    // SGM: every sweep but the last in one launch (each direction into its own buffer), then the
+    // last sweep adds them (Path8: folded into one buffer first) and runs the WTA.  The sum over
+    // directions is order-free, so this changes no value.
+    static const int first4[3][2] = {{1, 0}, {-1, 0}, {0, 1}};
+    static const int first8[7][2] = {{1, 0}, {-1, 0}, {0, 1}, {1, 1}, {1, -1}, {-1, 1}, {-1, -1}};
+    SgmLaunch pl;
     pl.w = w; pl.h = h; pl.d0 = d0; pl.D = D; pl.Dp = Dp;
     pl.pen = SgmPen{cfg_.P1, cfg_.P2_base, cfg_.adaptive_penalties, cfg_.piecewise_p2, cfg_.grad_t1, cfg_.grad_t2,
                     cfg_.p2_alpha};
     pl.gray = ptr<uint8_t>(L.lgray);
     pl.cvol = sgm_src;
     pl.cl = ptr<uint32_t>(L.cl); pl.cr = ptr<uint32_t>(L.cr); pl.qlut = ptr<uint16_t>(L.qlut);
-    pl.rmin = ptr<int16_t>(L.rmin); pl.rmax = ptr<int16_t>(L.rmax);
-    pl.S = ptr<uint32_t>(L.volS);
     pl.disp = ptr<float>(L.disp_wta); pl.best = ptr<float>(L.best); pl.second = ptr<float>(L.second);
     pl.subpixel = cfg_.subpixel;
     pl.store_final = (debug_ & 2) != 0;
-    for (int p = 0; p < npath; ++p) {
-        pl.dx = npath == 8 ? order8[p][0] : order4[p][0];
-        pl.dy = npath == 8 ? order8[p][1] : order4[p][1];
-        pl.mode = p == 0 ? 0 : (p == npath - 1 ? 2 : 1);
-        static const char* kSgmNames[3] = {"sgm_first", "sgm_accum", "sgm_last_wta"};
-        RUN(launch_sgm_path(pl, s), kSgmNames[pl.mode]);
+    pl.lanes = sgm_lanes_;
+    uint32_t* sb[7];
+    for (int i = 0; i < L.nsbuf; ++i) sb[i] = ptr<uint32_t>(L.sbuf[i]);
+    RUN(launch_sgm_first(pl, L.nsbuf, L.nsbuf == 7 ? first8 : first4, sb, s), "sgm_first");
+    int nin = L.nsbuf;
+    if (L.nsbuf == 7) {
+        RUN(launch_sgm_sum7(sb, n * (size_t)(Dp / 2), s), "sgm_sum7");
+        nin = 1;
     }
+    RUN(launch_sgm_last(pl, 0, -1, nin, sb, s), "sgm_last_wta");
     cudaEventRecord(ev_[6], s);
     // confidence (+ LR when nothing runs between them)
     const bool refine = cfg_.refine_enable && cfg_.refine_iterations > 0;
@@ -578,7 +585,7 @@ int Engine::dump(int what, void* dst, size_t bytes) {
         case 9: off = L.rmax; sz = n * 2; break;
         case 10: if (!L.raw_cost) return fail(kInternalError, "raw cost not materialised"); off = L.volRaw; vol = true; break;
         case 11: if (!L.cross) return fail(kInternalError, "no aggregated volume"); off = L.volB; vol = true; break;
-        case 12: if (!(debug_ & 2)) return fail(kInternalError, "path sum not kept"); off = L.volS; vol = true; break;
+        case 12: if (!(debug_ & 2)) return fail(kInternalError, "path sum not kept"); off = L.sbuf[0]; vol = true; break;
         case 13: off = L.disp_wta; sz = n * 4; break;
         case 14: off = L.best; sz = n * 4; break;
         case 15: off = L.second; sz = n * 4; break;
@@ -641,6 +648,16 @@ void apgcu_engine_destroy(apgcu_engine_t e) {
 }
 
 const char* apgcu_engine_last_error(apgcu_engine_t e) { return e ? e->eng->last_error().c_str() : "Invalid engine handle"; }
+
+int apgcu_engine_set_tuning(apgcu_engine_t e, const char* key, int value) {
+    if (!e || !key) return apgcu::kInternalError;
+    if (std::strcmp(key, "sgm_lanes") == 0) {
+        if (value != 0 && value != 8 && value != 16 && value != 32) return apgcu::kInvalidConfig;
+        e->eng->set_sgm_lanes(value);
+        return 0;
+    }
+    return apgcu::kInvalidConfig;
+}
 
 int apgcu_engine_set_debug(apgcu_engine_t e, int flags) {
     if (!e) return apgcu::kInternalError;

@@ -40,7 +40,9 @@ struct Layout {
     size_t rmin, rmax, rkey;
     size_t disp_right, disp_wta, best, second, confidence, disp_ref, disp_lr, disp_fill, disp_out, d_prior;
     size_t reliable, reason_conf, reason;
-    size_t volA, volB, volS, volRaw;
+    size_t volA, volB, volRaw;
+    size_t sbuf[7] = {};
+    int nsbuf = 0;
     size_t lut, qlut, magic;
     // HighQuality prior / refine
     size_t pr_cand, pr_ncand, pr_taken, pr_grid, pr_maps, pr_scratch, pr_count;
@@ -66,6 +68,7 @@ public:
     cudaStream_t stream() const { return stream_; }
     const std::string& last_error() const { return err_; }
     void set_debug(int f) { debug_ = f; }
+    void set_sgm_lanes(int t) { sgm_lanes_ = t; }
     int debug() const { return debug_; }
     const apg_pipeline_config_t& config() const { return cfg_; }
     int device() const { return device_; }
@@ -88,6 +91,7 @@ private:
     apg_pipeline_config_t cfg_;
     int device_ = 0;
     int debug_ = 0;
+    int sgm_lanes_ = 0;
     cudaStream_t stream_ = nullptr;
     bool own_stream_ = false;
     unsigned char* arena_ = nullptr;

@@ -31,26 +31,29 @@ cudaError_t launch_cross_h(int w, int h, int d0, int D, int Dp, int lmax, int ta
 size_t cross_v_smem_bytes(int Dp, int lmax);
 
 // sgm.cu
-struct SgmPathLaunch {
+struct SgmLaunch {
     int w, h, d0, D, Dp;
-    int dx, dy;
-    int mode;  // 0 first (store), 1 accumulate, 2 last (accumulate + WTA)
     SgmPen pen;
     const uint8_t* gray;
-    const uint32_t* cvol;  // nullptr -> census source (cl, cr, qlut)
+    const uint32_t* cvol;  // nullptr -> census source (cl, cr, qlut; default search range only)
     const uint32_t* cl;
     const uint32_t* cr;
     const uint16_t* qlut;
-    const int16_t* rmin;
-    const int16_t* rmax;
-    uint32_t* S;
     float* disp;
     float* best;
     float* second;
     int subpixel;
-    int store_final;  // last sweep: also write the final sum (stage dumps)
+    int store_final;  // last sweep: also write the final sum into in[0] (stage dumps)
+    int lanes;        // lanes per scanline chain (8, 16, 32; 0 = default for Dp)
 };
-cudaError_t launch_sgm_path(const SgmPathLaunch& l, cudaStream_t s);
+// First phase: ndir directions in one launch, direction i writing its path values to out[i].
+cudaError_t launch_sgm_first(const SgmLaunch& l, int ndir, const int (*dirs)[2], uint32_t* const* out,
+                             cudaStream_t s);
+// Last sweep (dx, dy): adds the nin (1 or 3) partial sums in[] and writes the WTA maps.
+cudaError_t launch_sgm_last(const SgmLaunch& l, int dx, int dy, int nin, const uint32_t* const* in, cudaStream_t s);
+// bufs[0] += bufs[1..6] (saturating u16 lanes), `words` 32-bit words each.
+cudaError_t launch_sgm_sum7(uint32_t* const* bufs, size_t words, cudaStream_t s);
+int sgm_lanes_for(int Dp, int requested);
 
 // post.cu
 struct ConfLrArgs {

@@ -1,39 +1,56 @@
-// Semi-global matching path sweeps with the path sum accumulated in HBM and the
-// winner-take-all fused into the last sweep.
+// Semi-global matching path sweeps with the path sum in HBM and the winner-take-all fused into
+// the last sweep.
 //
 // Restates SgmOptimizer::optimize / aggregate_path / process_pixel
 // (src/sgm_optimizer.cpp:21-81, 186-274) and wta_impl (:436-555):
 //   L(p,d) = C(p,d) + min(L'(d), L'(d-1)+P1, L'(d+1)+P1, m'+P2) - m',  m' = min_k L'(k),
 //   L = C at the first pixel of a scanline or when no L' entry is valid, L = INF and S = sentinel
-//   where C is invalid; S = sum over the 4 or 8 directions.
+//   where C is invalid; S = sum over the 4 or 8 directions (an order-free integer sum).
 //
-// Design (one warp per scanline: a row, a column or a diagonal ray):
-//   * the disparity axis, padded to Dp = 64*K, is spread over the 32 lanes; lane l holds K
-//     32-bit words = 2K consecutive disparities as packed uint16x2;
-//   * L' stays in registers between steps; L'(d-1) and L'(d+1) come from funnel shifts inside a
-//     lane plus one __shfl_up / __shfl_down across lanes; m' is one __reduce_min_sync;
-//   * INF is 0xFFFF and every add that can meet INF saturates (__vaddus2), so the reference's
-//     "skip invalid predecessor" tests become plain SIMD min/add;
-//   * S uses 16-bit lanes (the host only takes this path when npath*(cost_max+max(P2,P1+1)) <
-//     65535, can_use_u16_sgm_accumulator, include/apg_sgm/sgm_optimizer.hpp:9-18), and the
-//     sentinel 0xFFFF is sticky through the saturating add;
-//   * cost source: the (aggregated) u16 volume, or, in the fused Fast path, the census planes:
-//     C = qlut[popc(cl(x,y) ^ cr(x-d,y))] recomputed per step, so no cost volume exists;
-//   * the last sweep adds its L to S, keeps the sum in registers and does the reference WTA
-//     (first minimum, second minimum outside |d-best|<=1, legacy parabola) with two warp
-//     min-reductions, so the final S never goes back to HBM.
-// Bound: HBM (S read+write 4 B per voxel per middle sweep) and the per-step latency of the
-// shuffle/reduce chain; enough scanlines run concurrently to cover the latter at 720p.
+// Design:
+//   * the directions whose sweeps do not need another's result run together in ONE launch
+//     (left->right, right->left, top->bottom; plus the four diagonals for 8 paths), each chain
+//     writing its own path-sum buffer, so a pair puts 3-7x more chains in flight than a sweep at a
+//     time; the last sweep (bottom->top) adds the partial sums (Path8: folded into one buffer
+//     first) and runs the WTA.  HBM traffic equals sweep-by-sweep accumulation (Path4: 3 writes +
+//     3 reads of 2 B per voxel = 12 B per voxel);
+//   * a chain (one scanline of one direction) runs on a sub-group of T = 8, 16 or 32 lanes; a
+//     warp carries 32/T scanlines in one instruction stream.  Lane j of a group owns 2K
+//     consecutive disparities packed as K uint16x2 words, Dp = 2*K*T;
+//   * L' stays in registers; L'(d-1) / L'(d+1) come from funnel shifts inside a lane plus one
+//     group shuffle each way; m' is one group __reduce_min_sync;
+//   * min-plus arithmetic uses the DPX instructions (__viaddmin_u16x2 = min(a+b, c) per
+//     halfword): best = min(L', min(L'(d-1), L'(d+1)) + P1, m'+P2) is three SIMD ops.
+//     Invalid entries are 0x7FFF: larger than any valid path value (<= cost_max + P2), small
+//     enough that 0x7FFF + P2 + P1 never wraps, so the reference's "skip invalid predecessor"
+//     tests need no masks.  An invalid cost gives L in [0x7FFF, 0x7FFF+P2]; path sums add with
+//     unsigned saturation, so a voxel is invalid iff its sum is >= 0x7FFF (valid sums stay below
+//     npath*(cost_max+P2) < 0x7FFF, checked on the host);
+//   * cost source: the (aggregated) u16 volume, or in the fused Fast path the census planes,
+//     C = qlut[popc(cl(x,y) ^ cr(x-d,y))].  Along a row the right descriptors of a lane slide by
+//     one disparity per step, so a horizontal sweep keeps them in a register ring and takes one
+//     new descriptor per step from the neighbouring lane (shuffle) or, at the group edge, from
+//     memory;
+//   * every load (costs or descriptors, path sums, gray) runs PF steps ahead in a register ring;
+//   * the last sweep adds its L to S, keeps the final sum in registers and runs the reference WTA
+//     (first minimum, second minimum outside |d-best| <= 1, legacy parabola) with two group
+//     min-reductions, so the final sum never returns to HBM.
+// Bound: HBM (S written once, read-modify-written by the middle sweeps, read by the last) and, on
+// the longest scanline, the per-step latency of the shuffle / DPX / reduce chain.
 #include "common.cuh"
 #include "kernels.h"
+
+#include <algorithm>
 
 namespace apgcu {
 
 namespace {
 
-constexpr int kWarps = 4;
+constexpr uint32_t kInf = 0x7FFFu;
+constexpr uint32_t kInf2 = 0x7FFF7FFFu;
 
-enum Mode { kFirst = 0, kAccum = 1, kLast = 2 };
+enum Mode { kFirst = 0, kLast = 2 };
+constexpr int kMaxDirs = 8;
 
 __device__ __forceinline__ uint32_t min_halves(uint32_t v) {
     const uint32_t lo = v & 0xFFFFu, hi = v >> 16;
@@ -41,61 +58,68 @@ __device__ __forceinline__ uint32_t min_halves(uint32_t v) {
 }
 
 template <int K>
-__device__ __forceinline__ void load_words(const uint32_t* __restrict__ base, uint32_t (&v)[K]) {
-    if constexpr (K == 1) {
-        v[0] = __ldg(base);
-    } else if constexpr (K == 2) {
-        const uint2 t = __ldg(reinterpret_cast<const uint2*>(base));
-        v[0] = t.x; v[1] = t.y;
-    } else if constexpr (K == 4) {
-        const uint4 t = __ldg(reinterpret_cast<const uint4*>(base));
-        v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+__device__ __forceinline__ void ld_nc(const uint32_t* __restrict__ base, uint32_t (&v)[K]) {
+    if constexpr (K % 4 == 0) {
+#pragma unroll
+        for (int k = 0; k < K; k += 4) {
+            const uint4 t = __ldg(reinterpret_cast<const uint4*>(base + k));
+            v[k] = t.x; v[k + 1] = t.y; v[k + 2] = t.z; v[k + 3] = t.w;
+        }
+    } else if constexpr (K % 2 == 0) {
+#pragma unroll
+        for (int k = 0; k < K; k += 2) {
+            const uint2 t = __ldg(reinterpret_cast<const uint2*>(base + k));
+            v[k] = t.x; v[k + 1] = t.y;
+        }
     } else {
 #pragma unroll
         for (int k = 0; k < K; ++k) v[k] = __ldg(base + k);
     }
 }
 
+// Path sums: L2-coherent, L1-bypassing (.cg); each sum word is touched by one thread per launch.
 template <int K>
-__device__ __forceinline__ void load_words_rw(const uint32_t* base, uint32_t (&v)[K]) {
-    if constexpr (K == 2) {
-        const uint2 t = *reinterpret_cast<const uint2*>(base);
-        v[0] = t.x; v[1] = t.y;
-    } else if constexpr (K == 4) {
-        const uint4 t = *reinterpret_cast<const uint4*>(base);
-        v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+__device__ __forceinline__ void ld_cg(const uint32_t* base, uint32_t (&v)[K]) {
+    if constexpr (K % 4 == 0) {
+#pragma unroll
+        for (int k = 0; k < K; k += 4) {
+            const uint4 t = __ldcg(reinterpret_cast<const uint4*>(base + k));
+            v[k] = t.x; v[k + 1] = t.y; v[k + 2] = t.z; v[k + 3] = t.w;
+        }
+    } else if constexpr (K % 2 == 0) {
+#pragma unroll
+        for (int k = 0; k < K; k += 2) {
+            const uint2 t = __ldcg(reinterpret_cast<const uint2*>(base + k));
+            v[k] = t.x; v[k + 1] = t.y;
+        }
     } else {
 #pragma unroll
-        for (int k = 0; k < K; ++k) v[k] = base[k];
+        for (int k = 0; k < K; ++k) v[k] = __ldcg(base + k);
     }
 }
 
 template <int K>
-__device__ __forceinline__ void store_words(uint32_t* base, const uint32_t (&v)[K]) {
-    if constexpr (K == 2) {
-        *reinterpret_cast<uint2*>(base) = make_uint2(v[0], v[1]);
-    } else if constexpr (K == 4) {
-        *reinterpret_cast<uint4*>(base) = make_uint4(v[0], v[1], v[2], v[3]);
+__device__ __forceinline__ void st_cg(uint32_t* base, const uint32_t (&v)[K]) {
+    if constexpr (K % 4 == 0) {
+#pragma unroll
+        for (int k = 0; k < K; k += 4) __stcg(reinterpret_cast<uint4*>(base + k), make_uint4(v[k], v[k + 1], v[k + 2], v[k + 3]));
+    } else if constexpr (K % 2 == 0) {
+#pragma unroll
+        for (int k = 0; k < K; k += 2) __stcg(reinterpret_cast<uint2*>(base + k), make_uint2(v[k], v[k + 1]));
     } else {
 #pragma unroll
-        for (int k = 0; k < K; ++k) base[k] = v[k];
+        for (int k = 0; k < K; ++k) __stcg(base + k, v[k]);
     }
 }
 
 struct SgmArgs {
-    int w, h, d0, D, Dp;
-    int dx, dy;
+    int w, h, d0, D, Dp, dmax;
     SgmPen pen;
-    const uint8_t* gray;            // left gray (P2 adaptation)
-    const uint32_t* cvol;           // cost volume words (VOL source)
-    // census source (fused Fast path)
+    const uint8_t* gray;
+    const uint32_t* cvol;
     const uint32_t* cl;
     const uint32_t* cr;
-    const uint16_t* qlut;           // 65 quantised census costs
-    const int16_t* rmin;
-    const int16_t* rmax;
-    uint32_t* S;                    // path sum words
-    // WTA outputs (last sweep)
+    const uint16_t* qlut;
     float* disp;
     float* best;
     float* second;
@@ -103,219 +127,491 @@ struct SgmArgs {
     int store_final;
 };
 
-// Scanline s of direction (dx, dy): first pixel and length.
-__device__ __forceinline__ void scan_start(const SgmArgs& a, int s, int& x, int& y, int& len) {
-    if (a.dy == 0) {
-        y = s; x = a.dx > 0 ? 0 : a.w - 1; len = a.w;
-    } else if (a.dx == 0) {
-        x = s; y = a.dy > 0 ? 0 : a.h - 1; len = a.h;
+// Directions of one launch; warps [warp_begin[i], warp_begin[i+1]) run direction i.
+struct DirTable {
+    int n;
+    int dx[kMaxDirs], dy[kMaxDirs], nscan[kMaxDirs];
+    int warp_begin[kMaxDirs + 1];
+    uint32_t* out[kMaxDirs];       // first phase: each direction's own path-sum buffer
+    const uint32_t* in[kMaxDirs];  // last sweep: the partial sums to add
+    int nin;
+};
+
+// Scanline s of direction (dx, dy): first pixel and length (0 when s is past the last one).
+__device__ __forceinline__ void scan_start(const SgmArgs& a, int dx, int dy, int s, int nscan, int& x, int& y,
+                                           int& len) {
+    x = 0; y = 0; len = 0;
+    if (s >= nscan) return;
+    if (dy == 0) {
+        y = s; x = dx > 0 ? 0 : a.w - 1; len = a.w;
+    } else if (dx == 0) {
+        x = s; y = dy > 0 ? 0 : a.h - 1; len = a.h;
     } else {
-        // ray s: start pixel whose predecessor (x-dx, y-dy) is outside (as the reference's
-        // packed ray enumeration, src/sgm_optimizer.cpp:325-365)
-        if (s < a.w) { x = s; y = a.dy > 0 ? 0 : a.h - 1; }
-        else { x = a.dx > 0 ? 0 : a.w - 1; y = a.dy > 0 ? (s - a.w + 1) : (a.h - 1 - (s - a.w + 1)); }
-        const int rx = a.dx > 0 ? a.w - x : x + 1;
-        const int ry = a.dy > 0 ? a.h - y : y + 1;
+        // ray s: start pixel whose predecessor (x-dx, y-dy) is outside the image (the reference's
+        // ray enumeration, src/sgm_optimizer.cpp:325-365)
+        if (s < a.w) { x = s; y = dy > 0 ? 0 : a.h - 1; }
+        else { x = dx > 0 ? 0 : a.w - 1; y = dy > 0 ? (s - a.w + 1) : (a.h - 1 - (s - a.w + 1)); }
+        const int rx = dx > 0 ? a.w - x : x + 1;
+        const int ry = dy > 0 ? a.h - y : y + 1;
         len = rx < ry ? rx : ry;
     }
 }
 
-template <int K, int MODE, bool CENSUS>
-__global__ void __launch_bounds__(kWarps * 32) sgm_path_kernel(SgmArgs a, int nscan) {
+// Data of one future step, loaded ahead of use.
+template <int K, bool CENSUS, int HDIR, int NB>
+struct Slot {
+    static constexpr int NC = CENSUS ? (HDIR != 0 ? 1 : 2 * K) : K;
+    uint32_t c[NC];          // volume: cost words; census: right descriptors (sliding: the new one)
+    uint32_t s[NB > 0 ? NB : 1][K];  // partial path sums to add (last sweep)
+    uint32_t clv;            // census: left descriptor
+    int g;                   // left gray
+};
+
+template <int K, int T, bool CENSUS, int HDIR, int NB>
+__device__ __forceinline__ void fetch(const SgmArgs& a, const DirTable& tab, int j, int p, int x,
+                                      Slot<K, CENSUS, HDIR, NB>& sl) {
+    const int W2 = a.Dp / 2;
+    sl.g = __ldg(a.gray + p);
+    if (CENSUS) {
+        sl.clv = __ldg(a.cl + p);
+        const int row = p - x;
+        if (HDIR > 0) {
+            // the one descriptor entering the ring at this step: disparity d0 (lane 0 of the group)
+            const int xr = x - a.d0;
+            sl.c[0] = (j == 0 && xr >= 0 && xr < a.w) ? __ldg(a.cr + row + xr) : 0u;
+        } else if (HDIR < 0) {
+            // entering at the top: disparity d0 + Dp - 1 (last lane of the group)
+            const int xr = x - (a.d0 + a.Dp - 1);
+            sl.c[0] = (j == T - 1 && xr >= 0 && xr < a.w) ? __ldg(a.cr + row + xr) : 0u;
+        } else {
+#pragma unroll
+            for (int i = 0; i < 2 * K; ++i) {
+                const int xr = x - (a.d0 + 2 * K * j + i);
+                sl.c[i] = (xr >= 0 && xr < a.w) ? __ldg(a.cr + row + xr) : 0u;
+            }
+        }
+    } else {
+        ld_nc<K>(a.cvol + (size_t)p * W2 + j * K, reinterpret_cast<uint32_t(&)[K]>(sl.c));
+    }
+#pragma unroll
+    for (int b = 0; b < NB; ++b) ld_cg<K>(tab.in[b] + (size_t)p * W2 + j * K, sl.s[b]);
+}
+
+// Winner-take-all on the final sums of the group's pixel p (wta_impl, src/sgm_optimizer.cpp:465-536).
+template <int K, int T>
+__device__ __forceinline__ void wta(const SgmArgs& a, unsigned gmask, int j, int p, const uint32_t (&sv)[K]) {
+    uint32_t kmin = kInvalidWord;
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+#pragma unroll
+        for (int hs = 0; hs < 2; ++hs) {
+            const uint32_t v = (sv[k] >> (16 * hs)) & 0xFFFFu;
+            const uint32_t di = 2 * (j * K + k) + hs;
+            const uint32_t key = v >= kInf ? kInvalidWord : ((v << 16) | di);
+            kmin = key < kmin ? key : kmin;
+        }
+    const uint32_t bkey = __reduce_min_sync(gmask, kmin);
+    float dval = -1.f, fb = __int_as_float(0x7f800000), fs = __int_as_float(0x7f800000);
+    // The reference marks "no winner" with best_d = -1 and tests best_d < 0, so a negative
+    // winning disparity also yields -1 / +inf / +inf (:490-495).
+    if (bkey != kInvalidWord && a.d0 + (int)(bkey & 0xFFFFu) >= 0) {
+        const int bdi = (int)(bkey & 0xFFFFu);
+        uint32_t smin = kInf;
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+#pragma unroll
+            for (int hs = 0; hs < 2; ++hs) {
+                const int di = 2 * (j * K + k) + hs;
+                const uint32_t v = (sv[k] >> (16 * hs)) & 0xFFFFu;
+                if (abs(di - bdi) > 1 && v < smin) smin = v;
+            }
+        const uint32_t sec = __reduce_min_sync(gmask, smin);
+        const int wm = (bdi - 1) >> 1, wp = (bdi + 1) >> 1;
+        uint32_t selm = 0, selp = 0;
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            if (j * K + k == wm) selm = sv[k];
+            if (j * K + k == wp) selp = sv[k];
+        }
+        const uint32_t vm_w = __shfl_sync(gmask, selm, bdi >= 1 ? wm / K : 0, T);
+        const uint32_t vp_w = __shfl_sync(gmask, selp, wp / K < T ? wp / K : T - 1, T);
+        if (j == 0) {
+            const uint32_t bv = bkey >> 16;
+            dval = (float)(a.d0 + bdi);
+            if (a.subpixel && bdi > 0 && bdi + 1 < a.D) {
+                const uint32_t cm = (vm_w >> (16 * ((bdi - 1) & 1))) & 0xFFFFu;
+                const uint32_t cp = (vp_w >> (16 * ((bdi + 1) & 1))) & 0xFFFFu;
+                if (cm < kInf && cp < kInf) dval = __fadd_rn(dval, legacy_delta((float)cm, (float)bv, (float)cp));
+            }
+            fb = (float)bv;
+            fs = sec >= kInf ? __int_as_float(0x7f800000) : (float)sec;
+        }
+    }
+    if (j == 0) {
+        a.disp[p] = dval;
+        a.best[p] = fb;
+        a.second[p] = fs;
+    }
+}
+
+
+// Sliding census ring: logical entry i (disparity d0 + 2Kj + i) of rotation R lives in register
+// (i - R) mod 2K when the row is walked left to right, (i + R) mod 2K right to left.
+template <int K, int HDIR>
+__device__ __forceinline__ constexpr int ring_idx(int i, int R) {
+    return HDIR > 0 ? ((i - R) % (2 * K) + 2 * K) % (2 * K) : (i + R) % (2 * K);
+}
+
+// One scanline chain of direction (dx, dy) on this lane group.  MODE kFirst writes the chain's L
+// to `out`; MODE kLast adds the NB partial sums of `tab.in`, then runs the WTA.
+template <int T, int K, int MODE, bool CENSUS, int HDIR, int PF, int U, int NB>
+__device__ __forceinline__ void run_chain(const SgmArgs& a, const DirTable& tab, const uint16_t* s_q, int dx,
+                                          int dy, int s, int nscan, uint32_t* out) {
+    const int lane = threadIdx.x & 31;
+    const int grp = lane / T, j = lane % T;
+    const unsigned gmask = T == 32 ? 0xffffffffu : (((1u << T) - 1u) << (grp * T));
+    int x0, y0, len;
+    scan_start(a, dx, dy, s, nscan, x0, y0, len);
+    const int maxlen = __reduce_max_sync(0xffffffffu, len);
+    if (maxlen == 0) return;
+    const int W2 = a.Dp / 2;
+    const int step = dy * a.w + dx;
+    const int p0 = y0 * a.w + x0;
+    const uint32_t p1x2 = (uint32_t)a.pen.P1 * 0x00010001u;
+    const int dl0 = a.d0 + 2 * K * j;  // lowest disparity of this lane
+
+    Slot<K, CENSUS, HDIR, NB> ring[PF];
+#pragma unroll
+    for (int u = 0; u < PF; ++u)
+        if (u < len) fetch<K, T, CENSUS, HDIR, NB>(a, tab, j, p0 + u * step, x0 + u * dx, ring[u]);
+
+    // sliding census registers (horizontal census sweeps): descriptors of the first pixel
+    uint32_t cw[CENSUS && HDIR != 0 ? 2 * K : 1];
+    if (CENSUS && HDIR != 0) {
+#pragma unroll
+        for (int i = 0; i < 2 * K; ++i) {
+            const int xr = x0 - (dl0 + i);
+            cw[i] = (len > 0 && xr >= 0 && xr < a.w) ? __ldg(a.cr + y0 * a.w + xr) : 0u;
+        }
+    }
+
+    uint32_t L[K];
+    uint32_t m = kInf;
+    int prev_g = 0;
+#pragma unroll
+    for (int k = 0; k < K; ++k) L[k] = kInf2;
+
+    for (int t0 = 0; t0 < maxlen; t0 += U) {
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int t = t0 + u;
+            if (t >= maxlen) break;
+            if (t < len) {
+                Slot<K, CENSUS, HDIR, NB>& sl = ring[u % PF];
+                const int p = p0 + t * step;
+                const int x = x0 + t * dx;
+                // ---- matching costs of this pixel
+                uint32_t c[K];
+                if (CENSUS) {
+                    // valid disparities: d0 <= d <= min(x, dmax-1) and x - d < w (the default
+                    // range [d0, min(dmax, x+1)) of PriorEstimator::estimate)
+                    const int dlo = x - a.w + 1, dhi = min(x, a.dmax - 1);
+                    const bool all_ok = dl0 >= dlo && dl0 + 2 * K - 1 <= dhi;
+#pragma unroll
+                    for (int k = 0; k < K; ++k) {
+                        uint32_t q2[2];
+#pragma unroll
+                        for (int hs = 0; hs < 2; ++hs) {
+                            const int i = 2 * k + hs;
+                            const uint32_t desc = HDIR != 0 ? cw[ring_idx<K, HDIR>(i, u % (2 * K))] : sl.c[i];
+                            const uint32_t q = s_q[__popc(sl.clv ^ desc)];
+                            q2[hs] = (all_ok || (dl0 + i >= dlo && dl0 + i <= dhi)) ? q : kInf;
+                        }
+                        c[k] = __byte_perm(q2[0], q2[1], 0x5410);
+                    }
+                } else {
+#pragma unroll
+                    for (int k = 0; k < K; ++k) c[k] = __vminu2(sl.c[k], kInf2);  // 0xFFFF -> 0x7FFF
+                }
+                // ---- recurrence (process_pixel, src/sgm_optimizer.cpp:44-80)
+                if (t == 0 || m >= kInf) {
+#pragma unroll
+                    for (int k = 0; k < K; ++k) L[k] = c[k];
+                } else {
+                    const int P2 = adaptive_p2(a.pen, sl.g - prev_g);
+                    const uint32_t mp2 = (m + (uint32_t)P2) * 0x00010001u;
+                    const uint32_t m2 = m * 0x00010001u;
+                    uint32_t up = __shfl_up_sync(gmask, L[K - 1], 1, T);
+                    uint32_t dn = __shfl_down_sync(gmask, L[0], 1, T);
+                    if (j == 0) up = kInf2;
+                    if (j == T - 1) dn = kInf2;
+                    uint32_t Ln[K];
+#pragma unroll
+                    for (int k = 0; k < K; ++k) {
+                        const uint32_t lo_nb = k == 0 ? up : L[k - 1];
+                        const uint32_t hi_nb = k == K - 1 ? dn : L[k + 1];
+                        const uint32_t lm = __byte_perm(lo_nb, L[k], 0x5432);  // (L[k] << 16) | (lo_nb >> 16)
+                        const uint32_t lp = __byte_perm(L[k], hi_nb, 0x5432);  // (hi_nb << 16) | (L[k] >> 16)
+                        const uint32_t b = __vminu2(L[k], __viaddmin_u16x2(__vminu2(lm, lp), p1x2, mp2));
+                        Ln[k] = __vadd2(c[k], __vsub2(b, m2));
+                    }
+#pragma unroll
+                    for (int k = 0; k < K; ++k) L[k] = Ln[k];
+                }
+                uint32_t mm;
+                if constexpr (K == 1) {
+                    mm = min_halves(L[0]);
+                } else {
+                    uint32_t acc = __vminu2(L[0], L[1]);
+#pragma unroll
+                    for (int k = 2; k < K; k += 2) acc = k + 1 < K ? __vimin3_u16x2(acc, L[k], L[k + 1]) : __vminu2(acc, L[k]);
+                    mm = min_halves(acc);
+                }
+                m = __reduce_min_sync(gmask, mm);
+                prev_g = sl.g;
+                // ---- path sum
+                if (MODE == kFirst) {
+                    st_cg<K>(out + (size_t)p * W2 + j * K, L);
+                } else {
+                    uint32_t sv[K];
+#pragma unroll
+                    for (int k = 0; k < K; ++k) {
+                        uint32_t v = L[k];
+#pragma unroll
+                        for (int b = 0; b < NB; ++b) v = __vaddus2(v, sl.s[b][k]);
+                        sv[k] = v;
+                    }
+                    if (a.store_final) {
+                        uint32_t o[K];
+#pragma unroll
+                        for (int k = 0; k < K; ++k) o[k] = sv[k] | __vcmpgeu2(sv[k], kInf2);
+                        st_cg<K>(const_cast<uint32_t*>(tab.in[0]) + (size_t)p * W2 + j * K, o);
+                    }
+                    wta<K, T>(a, gmask, j, p, sv);
+                }
+            }
+            // ---- slide the census ring to the next pixel and refill this prefetch slot
+            if (CENSUS && HDIR != 0) {
+                const int R = u % (2 * K), Rn = (u + 1) % (2 * K);
+                // the entry leaving the ring at this step becomes the neighbour's entering entry
+                const uint32_t leaving = HDIR > 0 ? cw[ring_idx<K, HDIR>(2 * K - 1, R)] : cw[ring_idx<K, HDIR>(0, R)];
+                const uint32_t from_nb = HDIR > 0 ? __shfl_up_sync(gmask, leaving, 1, T) : __shfl_down_sync(gmask, leaving, 1, T);
+                if (t + 1 < len) {
+                    const bool edge = HDIR > 0 ? (j == 0) : (j == T - 1);
+                    const uint32_t entering = edge ? ring[(u + 1) % PF].c[0] : from_nb;
+                    if (HDIR > 0) cw[ring_idx<K, HDIR>(0, Rn)] = entering;
+                    else cw[ring_idx<K, HDIR>(2 * K - 1, Rn)] = entering;
+                }
+            }
+            {
+                const int tn = t + PF;
+                if (tn < len) fetch<K, T, CENSUS, HDIR, NB>(a, tab, j, p0 + tn * step, x0 + tn * dx, ring[u % PF]);
+            }
+        }
+    }
+}
+
+// prefetch depth PF divides the unroll U; the census ring needs U to be a multiple of 2K
+template <int K, bool CENSUS, int HDIR>
+struct Unroll {
+    static constexpr int U = (CENSUS && HDIR != 0) ? (2 * K < 4 ? 4 : 2 * K) : 4;
+    static constexpr int PF = (U % 4 == 0) ? 4 : 2;
+};
+
+__device__ __forceinline__ int find_dir(const DirTable& tab, int warp) {
+    int d = 0;
+#pragma unroll
+    for (int i = 1; i < kMaxDirs; ++i)
+        if (i < tab.n && warp >= tab.warp_begin[i]) d = i;
+    return d;
+}
+
+// First phase: every direction of the table at once, each chain writing its own sum buffer.
+template <int T, int K, bool CENSUS>
+__global__ void __launch_bounds__(128) sgm_first_kernel(SgmArgs a, DirTable tab) {
     __shared__ uint16_t s_q[65];
     if (CENSUS) {
         for (int i = threadIdx.x; i < 65; i += blockDim.x) s_q[i] = a.qlut[i];
         __syncthreads();
     }
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int s = blockIdx.x * kWarps + warp;
-    if (s >= nscan) return;
-    int x, y, len;
-    scan_start(a, s, x, y, len);
-    const int W2 = a.Dp / 2;
-    const int step_p = a.dy * a.w + a.dx;
-    int p = y * a.w + x;
-
-    uint32_t L[K];
-    uint32_t m = 0xFFFFu;
-    int prev_g = 0;
-    const uint32_t p1x2 = (uint32_t)a.pen.P1 * 0x00010001u;
-
-    for (int t = 0; t < len; ++t, p += step_p, x += a.dx) {
-        uint32_t c[K];
-        if (CENSUS) {
-            const uint32_t clv = __ldg(a.cl + p);
-            const int lo = __ldg(a.rmin + p), hi = __ldg(a.rmax + p);
-            const int row = p - x;
-#pragma unroll
-            for (int k = 0; k < K; ++k) {
-                uint32_t wv = 0;
-#pragma unroll
-                for (int hs = 0; hs < 2; ++hs) {
-                    const int di = 2 * (lane * K + k) + hs;
-                    const int d = a.d0 + di;
-                    const int xr = x - d;
-                    uint32_t q = kInvalidCost;
-                    if (di < a.D && d >= lo && d < hi && xr >= 0 && xr < a.w)
-                        q = s_q[__popc(clv ^ __ldg(a.cr + row + xr))];
-                    wv |= q << (16 * hs);
-                }
-                c[k] = wv;
-            }
+    constexpr int C = 32 / T;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (warp >= tab.warp_begin[tab.n]) return;
+    const int d = find_dir(tab, warp);
+    const int dx = tab.dx[d], dy = tab.dy[d];
+    const int s = (warp - tab.warp_begin[d]) * C + (threadIdx.x & 31) / T;
+    if (CENSUS && dy == 0) {
+        if (dx > 0) {
+            using UR = Unroll<K, true, 1>;
+            run_chain<T, K, kFirst, true, 1, UR::PF, UR::U, 0>(a, tab, s_q, dx, dy, s, tab.nscan[d], tab.out[d]);
         } else {
-            load_words<K>(a.cvol + (size_t)p * W2 + lane * K, c);
+            using UR = Unroll<K, true, -1>;
+            run_chain<T, K, kFirst, true, -1, UR::PF, UR::U, 0>(a, tab, s_q, dx, dy, s, tab.nscan[d], tab.out[d]);
         }
-        const int g = __ldg(a.gray + p);
-
-        uint32_t Ln[K];
-        if (t == 0 || m == 0xFFFFu) {
-#pragma unroll
-            for (int k = 0; k < K; ++k) Ln[k] = c[k];
-        } else {
-            const int P2 = adaptive_p2(a.pen, g - prev_g);
-            const uint32_t mp2 = min(m + (uint32_t)P2, 0xFFFFu) * 0x00010001u;
-            const uint32_t m2 = m * 0x00010001u;
-            uint32_t up = __shfl_up_sync(0xffffffffu, L[K - 1], 1);
-            uint32_t dn = __shfl_down_sync(0xffffffffu, L[0], 1);
-            if (lane == 0) up = 0xFFFFFFFFu;
-            if (lane == 31) dn = 0xFFFFFFFFu;
-#pragma unroll
-            for (int k = 0; k < K; ++k) {
-                const uint32_t lo_nb = k == 0 ? up : L[k - 1];
-                const uint32_t hi_nb = k == K - 1 ? dn : L[k + 1];
-                const uint32_t lm = __funnelshift_l(lo_nb, L[k], 16);  // (L[k] << 16) | (lo_nb >> 16)
-                const uint32_t lp = __funnelshift_r(L[k], hi_nb, 16);  // (L[k] >> 16) | (hi_nb << 16)
-                uint32_t bst = __vminu2(L[k], __vaddus2(__vminu2(lm, lp), p1x2));
-                bst = __vminu2(bst, mp2);
-                uint32_t v = __vadd2(c[k], __vsub2(bst, m2));
-                v |= __vcmpeq2(c[k], 0xFFFFFFFFu);
-                Ln[k] = v;
-            }
-        }
-        uint32_t lm_min = 0xFFFFu;
-#pragma unroll
-        for (int k = 0; k < K; ++k) {
-            L[k] = Ln[k];
-            lm_min = min(lm_min, min_halves(Ln[k]));
-        }
-        m = __reduce_min_sync(0xffffffffu, lm_min);
-        prev_g = g;
-
-        uint32_t* sp = a.S + (size_t)p * W2 + lane * K;
-        if (MODE == kFirst) {
-            store_words<K>(sp, Ln);
-        } else {
-            uint32_t sv[K];
-            load_words_rw<K>(sp, sv);
-#pragma unroll
-            for (int k = 0; k < K; ++k) sv[k] = __vaddus2(sv[k], Ln[k]);
-            if (MODE == kAccum) {
-                store_words<K>(sp, sv);
-            } else {
-                if (a.store_final) store_words<K>(sp, sv);
-                // winner-take-all on the final sum (wta_impl, src/sgm_optimizer.cpp:465-536)
-                uint32_t kmin = kInvalidWord;
-#pragma unroll
-                for (int k = 0; k < K; ++k) {
-#pragma unroll
-                    for (int hs = 0; hs < 2; ++hs) {
-                        const uint32_t v = (sv[k] >> (16 * hs)) & 0xFFFFu;
-                        const uint32_t di = 2 * (lane * K + k) + hs;
-                        const uint32_t key = v == 0xFFFFu ? kInvalidWord : ((v << 16) | di);
-                        kmin = key < kmin ? key : kmin;
-                    }
-                }
-                const uint32_t bkey = __reduce_min_sync(0xffffffffu, kmin);
-                float dval = -1.f, fb = __int_as_float(0x7f800000), fs = __int_as_float(0x7f800000);
-                // The reference marks "no winner" with best_d = -1 and tests best_d < 0, so a
-                // negative winning disparity also yields -1 / +inf / +inf (:490-495).
-                if (bkey != kInvalidWord && a.d0 + (int)(bkey & 0xFFFFu) >= 0) {
-                    const int bdi = (int)(bkey & 0xFFFFu);
-                    uint32_t smin = 0xFFFFu;
-#pragma unroll
-                    for (int k = 0; k < K; ++k) {
-#pragma unroll
-                        for (int hs = 0; hs < 2; ++hs) {
-                            const int di = 2 * (lane * K + k) + hs;
-                            const uint32_t v = (sv[k] >> (16 * hs)) & 0xFFFFu;
-                            if (abs(di - bdi) > 1 && v < smin) smin = v;
-                        }
-                    }
-                    const uint32_t sec = __reduce_min_sync(0xffffffffu, smin);
-                    // neighbours of the minimum for the parabola
-                    const int wm = (bdi - 1) >> 1, wp = (bdi + 1) >> 1;  // word indices
-                    uint32_t selm = 0, selp = 0;
-#pragma unroll
-                    for (int k = 0; k < K; ++k) {
-                        if (lane * K + k == wm) selm = sv[k];
-                        if (lane * K + k == wp) selp = sv[k];
-                    }
-                    const uint32_t vm_w = __shfl_sync(0xffffffffu, selm, bdi >= 1 ? wm / K : 0);
-                    const uint32_t vp_w = __shfl_sync(0xffffffffu, selp, wp / K < 32 ? wp / K : 31);
-                    if (lane == 0) {
-                        const uint32_t bv = bkey >> 16;
-                        dval = (float)(a.d0 + bdi);
-                        if (a.subpixel && bdi > 0 && bdi + 1 < a.D) {
-                            const uint32_t cm = (vm_w >> (16 * ((bdi - 1) & 1))) & 0xFFFFu;
-                            const uint32_t cp = (vp_w >> (16 * ((bdi + 1) & 1))) & 0xFFFFu;
-                            if (cm != 0xFFFFu && cp != 0xFFFFu)
-                                dval = __fadd_rn(dval, legacy_delta((float)cm, (float)bv, (float)cp));
-                        }
-                        fb = (float)bv;
-                        fs = sec == 0xFFFFu ? __int_as_float(0x7f800000) : (float)sec;
-                    }
-                }
-                if (lane == 0) {
-                    a.disp[p] = dval;
-                    a.best[p] = fb;
-                    a.second[p] = fs;
-                }
-            }
-        }
-        y += a.dy;
+    } else {
+        using UR = Unroll<K, CENSUS, 0>;
+        run_chain<T, K, kFirst, CENSUS, 0, UR::PF, UR::U, 0>(a, tab, s_q, dx, dy, s, tab.nscan[d], tab.out[d]);
     }
 }
 
-template <int K, int MODE>
-cudaError_t launch_k(const SgmArgs& a, bool census, cudaStream_t st) {
-    int nscan;
-    if (a.dy == 0) nscan = a.h;
-    else if (a.dx == 0) nscan = a.w;
-    else nscan = a.w + a.h - 1;
-    const int blocks = (nscan + kWarps - 1) / kWarps;
-    if (census) sgm_path_kernel<K, MODE, true><<<blocks, kWarps * 32, 0, st>>>(a, nscan);
-    else sgm_path_kernel<K, MODE, false><<<blocks, kWarps * 32, 0, st>>>(a, nscan);
+// Last sweep (one direction): add the NB partial sums and run the WTA.
+template <int T, int K, bool CENSUS, int NB>
+__global__ void __launch_bounds__(128) sgm_last_kernel(SgmArgs a, DirTable tab) {
+    __shared__ uint16_t s_q[65];
+    if (CENSUS) {
+        for (int i = threadIdx.x; i < 65; i += blockDim.x) s_q[i] = a.qlut[i];
+        __syncthreads();
+    }
+    constexpr int C = 32 / T;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int s = warp * C + (threadIdx.x & 31) / T;
+    using UR = Unroll<K, CENSUS, 0>;
+    run_chain<T, K, kLast, CENSUS, 0, UR::PF, UR::U, NB>(a, tab, s_q, tab.dx[0], tab.dy[0], s, tab.nscan[0], nullptr);
+}
+
+// Path8: fold the seven first-phase buffers into the first one (saturating per halfword).
+__global__ void sgm_sum_kernel(uint4* __restrict__ dst, const uint4* __restrict__ b1, const uint4* __restrict__ b2,
+                               const uint4* __restrict__ b3, const uint4* __restrict__ b4,
+                               const uint4* __restrict__ b5, const uint4* __restrict__ b6, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        uint4 v = __ldcg(dst + i);
+        const uint4* src[6] = {b1, b2, b3, b4, b5, b6};
+#pragma unroll
+        for (int b = 0; b < 6; ++b) {
+            const uint4 t = __ldcs(src[b] + i);
+            v.x = __vaddus2(v.x, t.x); v.y = __vaddus2(v.y, t.y);
+            v.z = __vaddus2(v.z, t.z); v.w = __vaddus2(v.w, t.w);
+        }
+        __stcg(dst + i, v);
+    }
+}
+
+int nscan_of(const SgmArgs& a, int dx, int dy) {
+    if (dy == 0) return a.h;
+    if (dx == 0) return a.w;
+    return a.w + a.h - 1;
+}
+
+template <int T, int K>
+cudaError_t launch_first_tk(const SgmArgs& a, DirTable tab, bool census, cudaStream_t st) {
+    constexpr int C = 32 / T;
+    tab.warp_begin[0] = 0;
+    for (int i = 0; i < tab.n; ++i) {
+        tab.nscan[i] = nscan_of(a, tab.dx[i], tab.dy[i]);
+        tab.warp_begin[i + 1] = tab.warp_begin[i] + (tab.nscan[i] + C - 1) / C;
+    }
+    const int blocks = (tab.warp_begin[tab.n] + 3) / 4;
+    if (census) sgm_first_kernel<T, K, true><<<blocks, 128, 0, st>>>(a, tab);
+    else sgm_first_kernel<T, K, false><<<blocks, 128, 0, st>>>(a, tab);
     return cudaGetLastError();
 }
 
-template <int K>
-cudaError_t launch_mode(const SgmArgs& a, int mode, bool census, cudaStream_t st) {
-    if (mode == kFirst) return launch_k<K, kFirst>(a, census, st);
-    if (mode == kAccum) return launch_k<K, kAccum>(a, census, st);
-    return launch_k<K, kLast>(a, census, st);
+template <int T, int K>
+cudaError_t launch_last_tk(const SgmArgs& a, DirTable tab, bool census, cudaStream_t st) {
+    constexpr int C = 32 / T;
+    tab.nscan[0] = nscan_of(a, tab.dx[0], tab.dy[0]);
+    const int warps = (tab.nscan[0] + C - 1) / C;
+    const int blocks = (warps + 3) / 4;
+#define APGCU_LAST(NB)                                                                            \
+    if (tab.nin == NB) {                                                                          \
+        if (census) sgm_last_kernel<T, K, true, NB><<<blocks, 128, 0, st>>>(a, tab);              \
+        else sgm_last_kernel<T, K, false, NB><<<blocks, 128, 0, st>>>(a, tab);                    \
+        return cudaGetLastError();                                                                \
+    }
+    APGCU_LAST(1)
+    APGCU_LAST(3)
+#undef APGCU_LAST
+    return cudaErrorInvalidValue;
+}
+
+template <bool FIRST>
+cudaError_t dispatch(const SgmArgs& a, const DirTable& tab, bool census, int T, cudaStream_t st) {
+#define APGCU_TK(TT, KK) return FIRST ? launch_first_tk<TT, KK>(a, tab, census, st) : launch_last_tk<TT, KK>(a, tab, census, st)
+    if (T == 8) {
+        if (a.Dp == 64) APGCU_TK(8, 4);
+        if (a.Dp == 128) APGCU_TK(8, 8);
+        return cudaErrorInvalidValue;
+    }
+    if (T == 16) {
+        switch (a.Dp / 32) {
+            case 2: APGCU_TK(16, 2);
+            case 4: APGCU_TK(16, 4);
+            case 6: APGCU_TK(16, 6);
+            case 8: APGCU_TK(16, 8);
+            default: return cudaErrorInvalidValue;
+        }
+    }
+    switch (a.Dp / 64) {
+        case 1: APGCU_TK(32, 1);
+        case 2: APGCU_TK(32, 2);
+        case 3: APGCU_TK(32, 3);
+        case 4: APGCU_TK(32, 4);
+        case 5: APGCU_TK(32, 5);
+        case 6: APGCU_TK(32, 6);
+        case 7: APGCU_TK(32, 7);
+        case 8: APGCU_TK(32, 8);
+        default: return cudaErrorInvalidValue;
+    }
+#undef APGCU_TK
+}
+
+SgmArgs make_args(const SgmLaunch& l) {
+    SgmArgs a;
+    a.w = l.w; a.h = l.h; a.d0 = l.d0; a.D = l.D; a.Dp = l.Dp; a.dmax = l.d0 + l.D;
+    a.pen = l.pen; a.gray = l.gray; a.cvol = l.cvol; a.cl = l.cl; a.cr = l.cr; a.qlut = l.qlut;
+    a.disp = l.disp; a.best = l.best; a.second = l.second;
+    a.subpixel = l.subpixel;
+    a.store_final = l.store_final;
+    return a;
 }
 
 }  // namespace
 
-cudaError_t launch_sgm_path(const SgmPathLaunch& l, cudaStream_t st) {
-    SgmArgs a;
-    a.w = l.w; a.h = l.h; a.d0 = l.d0; a.D = l.D; a.Dp = l.Dp; a.dx = l.dx; a.dy = l.dy;
-    a.pen = l.pen; a.gray = l.gray; a.cvol = l.cvol; a.cl = l.cl; a.cr = l.cr; a.qlut = l.qlut;
-    a.rmin = l.rmin; a.rmax = l.rmax; a.S = l.S; a.disp = l.disp; a.best = l.best; a.second = l.second;
-    a.subpixel = l.subpixel;
-    a.store_final = l.store_final;
-    const bool census = l.cvol == nullptr;
-    switch (l.Dp / 64) {
-        case 1: return launch_mode<1>(a, l.mode, census, st);
-        case 2: return launch_mode<2>(a, l.mode, census, st);
-        case 3: return launch_mode<3>(a, l.mode, census, st);
-        case 4: return launch_mode<4>(a, l.mode, census, st);
-        case 5: return launch_mode<5>(a, l.mode, census, st);
-        case 6: return launch_mode<6>(a, l.mode, census, st);
-        case 7: return launch_mode<7>(a, l.mode, census, st);
-        case 8: return launch_mode<8>(a, l.mode, census, st);
-        default: return cudaErrorInvalidValue;
+int sgm_lanes_for(int Dp, int requested) {
+    // lanes per chain: 32 by default (one warp per chain, K = Dp/64 words per lane): the sweeps are
+    // bound by the serial recurrence, and a full warp per chain halves each step's dependent
+    // instruction count against 16 lanes (measured 1.9 vs 2.6 ms per 720p pair at D 128); 16 or
+    // 8 (Dp 64 / 128 only) on request
+    if (requested == 8 && (Dp == 64 || Dp == 128)) return 8;
+    if (requested == 16 && Dp <= 256) return 16;
+    return 32;
+}
+
+cudaError_t launch_sgm_first(const SgmLaunch& l, int ndir, const int (*dirs)[2], uint32_t* const* out,
+                             cudaStream_t st) {
+    if (ndir < 1 || ndir > kMaxDirs) return cudaErrorInvalidValue;
+    const SgmArgs a = make_args(l);
+    DirTable tab = {};
+    tab.n = ndir;
+    for (int i = 0; i < ndir; ++i) {
+        tab.dx[i] = dirs[i][0];
+        tab.dy[i] = dirs[i][1];
+        tab.out[i] = out[i];
     }
+    return dispatch<true>(a, tab, l.cvol == nullptr, sgm_lanes_for(l.Dp, l.lanes), st);
+}
+
+cudaError_t launch_sgm_last(const SgmLaunch& l, int dx, int dy, int nin, const uint32_t* const* in,
+                            cudaStream_t st) {
+    if (nin < 1 || nin > kMaxDirs) return cudaErrorInvalidValue;
+    const SgmArgs a = make_args(l);
+    DirTable tab = {};
+    tab.n = 1;
+    tab.dx[0] = dx;
+    tab.dy[0] = dy;
+    tab.nin = nin;
+    for (int i = 0; i < nin; ++i) tab.in[i] = in[i];
+    return dispatch<false>(a, tab, l.cvol == nullptr, sgm_lanes_for(l.Dp, l.lanes), st);
+}
+
+cudaError_t launch_sgm_sum7(uint32_t* const* bufs, size_t words, cudaStream_t st) {
+    const size_t n = words / 4;
+    const int blocks = (int)std::min<size_t>((n + 255) / 256, 148 * 16);
+    sgm_sum_kernel<<<blocks, 256, 0, st>>>(reinterpret_cast<uint4*>(bufs[0]), reinterpret_cast<const uint4*>(bufs[1]),
+                                           reinterpret_cast<const uint4*>(bufs[2]), reinterpret_cast<const uint4*>(bufs[3]),
+                                           reinterpret_cast<const uint4*>(bufs[4]), reinterpret_cast<const uint4*>(bufs[5]),
+                                           reinterpret_cast<const uint4*>(bufs[6]), n);
+    return cudaGetLastError();
 }
 
 }  // namespace apgcu

@@ -37,7 +37,10 @@ WORKLOADS = {
     "kitti1242": (1, (1242, 375, 192, 12, 0, 180, 0.0), "balanced_1242x375_d192"),
 }
 MODE_NAMES = {0: "Fast", 1: "Balanced", 2: "HighQuality"}
-METRIC = "W*H*D/s at 720p D=128 (Fast, bit-exact)"
+
+
+def metric_name(mode: int, w: int, h: int, D: int) -> str:
+    return f"W*H*D/s at {w}x{h} D={D} ({MODE_NAMES[mode]}, bit-exact)"
 
 
 def _peaks():
@@ -63,7 +66,7 @@ def _profile_traffic(kernel: str, workload: str):
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+    """nvidia-smi clocks / throttle reasons sampled every 50 ms during the timed region."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -78,7 +81,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self._t = threading.Thread(target=self._read, daemon=True)
             self._t.start()
         except FileNotFoundError:
@@ -87,6 +90,13 @@ class ClockSampler:
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
+
+    def wait_first(self, timeout: float = 5.0):
+        """Block until nvidia-smi has printed its first sample, so the timed region is covered."""
+        t0 = time.time()
+        while self.proc and not self.lines and time.time() - t0 < timeout:
+            time.sleep(0.01)
+        self.lines.clear()
 
     def stop(self):
         if not self.proc:
@@ -114,16 +124,20 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def _algorithmic_bytes(name: str, w: int, h: int, D: int, Dp: int) -> float:
-    """Bytes a launch of `name` must move by design (roofline section)."""
+def _algorithmic_bytes(name: str, w: int, h: int, D: int, volume_source: bool, npath: int = 4) -> float:
+    """Bytes a launch of `name` must move by design (roofline section).  Path sums
+    and volumes are u16 per voxel; a volume-fed sweep reads the cost volume once."""
     n = w * h
+    vol = n * D * 2.0 if volume_source else 0.0
+    nfirst = npath - 1
+    nin = 1 if npath == 8 else nfirst
     return {
-        "sgm_first": n * D * 2.0,            # write the path sum
-        "sgm_accum": n * D * 4.0,            # read + write the path sum
-        "sgm_last_wta": n * D * 2.0 + n * 12,  # read the path sum, write disparity/best/second
-        "cost+crossH": n * D * 2.0,          # write the horizontally aggregated volume
-        "crossV": n * D * 4.0,               # read T, write C
-        "cost": n * D * 2.0,
+        "sgm_first": nfirst * (n * D * 2.0 + vol),    # every first-phase sweep writes its own sums
+        "sgm_sum7": n * D * 16.0,                     # Path8: read 7 buffers, write 1
+        "sgm_last_wta": nin * n * D * 2.0 + vol + n * 12,  # read the partial sums, write the WTA maps
+        "cost+crossH": n * D * 2.0,                   # write the horizontally aggregated volume
+        "crossV": n * D * 4.0,                        # read T, write C
+        "cost": n * D * 2.0,                          # write the raw volume
     }.get(name, 0.0)
 
 
@@ -152,7 +166,7 @@ def run_reference(args, wl):
     value = vox * args.steps / total
     cores = O.ref_threads()
     print(json.dumps({
-        "impl": "reference", "metric": METRIC, "value": value, "unit": "voxels/s", "n_gpus": args.gpus,
+        "impl": "reference", "metric": metric_name(mode, spec.width, spec.height, spec.max_disparity), "value": value, "unit": "voxels/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": "synthetic",
         "config": {"workload": label, "mode": MODE_NAMES[mode], "width": spec.width, "height": spec.height,
@@ -246,15 +260,14 @@ def run_b200(args, wl):
     for i in range(max(args.warmup, 3)):
         step(i)
     eng.sync()
-    eng.set_debug(apg.DEBUG_PROFILE)
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    per_kernel = {}
     sampler = ClockSampler(local)
+    sampler.start()
+    sampler.wait_first()
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    sampler.start()
     launches0 = apg.kernel_launch_count()
     with torch.cuda.stream(es):
         for k in range(args.steps):
@@ -262,11 +275,20 @@ def run_b200(args, wl):
             starts[k].record(es)
             step(k)
             ends[k].record(es)
-            for name, ms in eng.launch_profile():  # syncs on this step's last launch
-                per_kernel.setdefault(name, []).append(ms)
     torch.cuda.synchronize()
     launches = apg.kernel_launch_count() - launches0
     clocks = sampler.stop()
+
+    # per-launch device times (a separate pass: the event after every launch is not in the timing)
+    eng.set_debug(apg.DEBUG_PROFILE)
+    per_kernel = {}
+    with torch.cuda.stream(es):
+        for k in range(min(args.steps, 20)):
+            flush.zero_()
+            step(k)
+            for name, ms in eng.launch_profile():  # syncs on this step's last launch
+                per_kernel.setdefault(name, []).append(ms)
+    torch.cuda.synchronize()
     eng.set_debug(0)
     dev_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
     t = torch.tensor([dev_ms], dtype=torch.float64, device=dev)
@@ -299,7 +321,7 @@ def run_b200(args, wl):
     totals = {k: sum(v) for k, v in per_kernel.items() if k != "copy"}
     top = max(totals, key=totals.get)
     top_avg_ms = statistics.mean(per_kernel[top])
-    alg = _algorithmic_bytes(top, w, h, D, Dp)
+    alg = _algorithmic_bytes(top, w, h, D, volume_source=(mode != 0), npath=cfg.paths)
     achieved = alg / (top_avg_ms / 1000.0) / 1e9
     prof_total = sum(totals.values())
     roofline = {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -310,7 +332,7 @@ def run_b200(args, wl):
                 "kernel_avg_ms": {k: round(statistics.mean(per_kernel[k]), 5) for k in totals}}
 
     out = {
-        "metric": METRIC, "value": value, "unit": "voxels/s", "n_gpus": world, "steps": args.steps,
+        "metric": metric_name(mode, w, h, D), "value": value, "unit": "voxels/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u16", "data": "synthetic",
         "config": {"workload": label, "mode": MODE_NAMES[mode], "width": w, "height": h, "max_disparity": D,
@@ -339,7 +361,7 @@ def run_b200(args, wl):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="fast720")

@@ -58,6 +58,11 @@ APGCU_API void apgcu_engine_destroy(apgcu_engine_t e);
 APGCU_API const char* apgcu_engine_last_error(apgcu_engine_t e);
 APGCU_API int apgcu_engine_set_debug(apgcu_engine_t e, int flags);
 
+/* Kernel tuning knobs (results never change, only speed):
+ *   "sgm_lanes": lanes per SGM scanline chain, 8 / 16 / 32 (0 = default, 32).
+ * Returns 0, or APG_STATUS_INVALID_CONFIG for an unknown key or value. */
+APGCU_API int apgcu_engine_set_tuning(apgcu_engine_t e, const char* key, int value);
+
 /* One pair from HOST memory (strided, 1 or 3 channels); outputs are host arrays of W*H.
  * Copies in and out are part of the call.  Any output pointer may be NULL. */
 APGCU_API int apgcu_engine_process(apgcu_engine_t e, const uint8_t* left, const uint8_t* right, int width,
