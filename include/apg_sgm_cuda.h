@@ -113,6 +113,38 @@ APGCU_API size_t apgcu_session_estimate_bytes(apg_session_t s, int width, int he
 /* Number of kernels the library has launched in this process (all engines). */
 APGCU_API unsigned long long apgcu_kernel_launch_count(void);
 
+/* Right-image winner-take-all over a caller's cost volume, allocating nothing.
+ *
+ * No counterpart in the reference: it exposes as one call the right-image WTA that the reference
+ * runs inside its pipeline (wta_right_from_left_volume, src/pipeline.cpp:24-84, internal) and that
+ * the engine fuses into its cost kernel.  It is for callers that must not allocate device memory
+ * on their hot path -- a host that runs under a fixed device-memory budget it accounts itself, or
+ * whose allocator would synchronise the device -- and so cannot hold an engine workspace.  The
+ * call makes no cudaMalloc, cudaFree or other allocating call: its per-pixel keys live in a
+ * static device array of APGCU_NOALLOC_MAX_PIXELS u32 (8 MiB), cleared by the call itself.
+ *
+ * d_cost: u16 volume on the current device, C(x, y, d) at d_cost[(y*width + x)*pitch + d -
+ * min_disparity] for d in [min_disparity, min_disparity + num_disparities), 0xFFFF = invalid.
+ * d_disparity_right: float width*height on the same device; -1 where no valid disparity.
+ * subpixel: nonzero applies the legacy parabola.  stream: a cudaStream_t, or NULL.
+ * Enqueued only; synchronise the stream before reading the result.
+ *
+ * The first call on each device looks up the array's device address (cudaGetSymbolAddress) with
+ * that device current; make that first call before any stream capture.  All calls on one device
+ * share the array: calls that overlap in time on one device race and must be serialised by the
+ * caller.
+ *
+ * Returns APG_STATUS_OK; APG_STATUS_EMPTY_INPUT for a NULL pointer or a non-positive size;
+ * APG_STATUS_INVALID_DISPARITY_RANGE for num_disparities outside [1,
+ * APGCU_NOALLOC_MAX_DISPARITIES]; APG_STATUS_SIZE_MISMATCH for pitch < num_disparities;
+ * APG_STATUS_RESOURCE_LIMIT_EXCEEDED when width*height > APGCU_NOALLOC_MAX_PIXELS or height > 65535
+ * (nothing is launched); APG_STATUS_UNSUPPORTED_BACKEND / APG_STATUS_INTERNAL_ERROR for CUDA failures. */
+#define APGCU_NOALLOC_MAX_PIXELS (1 << 21)
+#define APGCU_NOALLOC_MAX_DISPARITIES 1024
+APGCU_API int apgcu_right_wta_noalloc(const uint16_t* d_cost, int width, int height, int min_disparity,
+                                      int num_disparities, int pitch, int subpixel, float* d_disparity_right,
+                                      void* stream);
+
 #ifdef __cplusplus
 }
 #endif
