@@ -1,6 +1,6 @@
 // Matching-cost volume, fused with the horizontal Cross-arm pass and the right-image WTA.
 //
-// Restates, in one kernel over (row y, 64- or 32-pixel column tile):
+// Restates, in one kernel over (row y, 128- or 64-pixel column tile):
 //   * CostComputer::compute_volume (src/cost_computer.cpp:139-203; LUT form :205-268):
 //     census Hamming + AD + gradient terms from host-built LUTs, quantised to u16;
 //   * the horizontal half of CostAggregator::aggregate_hv (src/cost_aggregator.cpp:65-105):
@@ -26,145 +26,181 @@ namespace apgcu {
 
 namespace {
 
-struct CostSmem {
-    int nx;        // TXc + 2*HA staged left pixels
-    int nr;        // staged right pixels
-    size_t bytes;
-};
+// Staged per-pixel descriptor: census bits and the three 8-bit planes packed as
+// gray | gx << 8 | gy << 16, so one __vabsdiffu4 yields |dgray|, |dgx|, |dgy|.
+template <bool C64> struct Aux;
+template <> struct __align__(8) Aux<false> { uint32_t c; uint32_t g; };
+template <> struct __align__(16) Aux<true> { unsigned long long c; uint32_t g; uint32_t pad; };
 
 __host__ __device__ inline size_t align16(size_t v) { return (v + 15) & ~size_t(15); }
 
-template <bool C64>
-__host__ __device__ inline void cost_smem_layout(int txc, int ha, int D, int Dp, bool cross,
-                                                 size_t* off_lut, size_t* off_left, size_t* off_right,
-                                                 size_t* off_cost, size_t* off_pre, size_t* total) {
-    const int nx = txc + 2 * ha;
-    const int nr = nx + D - 1;
-    const size_t csz = C64 ? 8 : 4;
+// Threads per block: a multiple of the words per pixel W2 (up to 256), so a thread keeps one word
+// index k for the whole kernel and walks pixels with a fixed stride.
+__host__ __device__ inline int cost_threads(int W2) { return W2 <= 256 ? W2 * (256 / W2) : 256; }
+
+struct CostLayout {
+    int txc, ha, nx, nr, segs;
+    size_t lut, magic, arm, left, right, rng, cost, cnt, seg, total;
+};
+
+__host__ __device__ inline CostLayout cost_layout(int txc, int ha, int D, int Dp, bool cross, bool prior, bool c64) {
+    CostLayout l;
+    const int W2 = Dp / 2, CS = W2 + 1;
+    const int nt = cost_threads(W2);
+    l.txc = txc; l.ha = ha;
+    l.nx = txc + 2 * ha;
+    l.nr = l.nx + D - 1;
+    l.segs = W2 <= nt ? nt / W2 : 1;
+    const size_t asz = c64 ? 16 : 8;
     size_t o = 0;
-    *off_lut = o; o = align16(o + kLutSize * 4);
-    *off_left = o; o = align16(o + (size_t)nx * (csz + 3 + 4));   // census, gray, gx, gy, rmin, rmax
-    *off_right = o; o = align16(o + (size_t)nr * (csz + 3));      // census, gray, gx, gy
-    *off_cost = o; o = align16(o + (size_t)nx * (Dp + 2) * 2);  // row stride Dp+2: conflict-free diagonals
-    *off_pre = o;
-    if (cross) o = align16(o + (size_t)(nx + 1) * (Dp / 2) * 8);
-    *total = o;
+    l.lut = o; o = align16(o + kLutSize * 4);
+    l.magic = o; o = align16(o + (cross ? (2 * ha + 2) * 4 : 0));
+    l.arm = o; o = align16(o + (cross ? txc * 4 : 0));
+    l.left = o; o = align16(o + l.nx * asz);
+    l.right = o; o = align16(o + l.nr * asz);
+    l.rng = o; o = align16(o + (prior ? l.nx * 4 : 0));
+    l.cost = o; o = align16(o + (size_t)l.nx * CS * 4);  // odd word stride: diagonals hit distinct banks
+    l.cnt = o; o = align16(o + (cross && prior ? (size_t)l.nx * W2 * 4 : 0));
+    l.seg = o; o = align16(o + (cross ? (size_t)l.segs * W2 * 4 * 2 : 0));
+    l.total = o;
+    return l;
 }
 
-template <bool C64, bool CROSS, bool STORE, bool RWTA>
+// Visit every (staged pixel xi < nrows, word k) pair of the block once.
+template <typename F>
+__device__ __forceinline__ void for_each_word(int nrows, int W2, int nt, F&& body) {
+    const int tid = threadIdx.x;
+    if (W2 <= nt) {
+        const int k = tid % W2, rstep = nt / W2;
+        for (int xi = tid / W2; xi < nrows; xi += rstep) body(xi, k);
+    } else {
+        for (int xi = 0; xi < nrows; ++xi)
+            for (int k = tid; k < W2; k += nt) body(xi, k);
+    }
+}
+
+// One block per (row y, tile of txc columns); the tile's raw costs over [x0 - ha, x0 + txc + ha)
+// are built in shared memory, then (RWTA) folded into the right-image argmin keys, then (CROSS)
+// turned into in-place prefix sums over x and queried over each pixel's horizontal arm.
+template <bool C64, bool CROSS, bool STORE, bool RWTA, bool PRIOR, bool QLUT>
 __global__ void __launch_bounds__(256) cost_kernel(CostCtx c, int txc, int ha, int lmax, int tau,
                                                    uint32_t* __restrict__ out_vol,
                                                    uint32_t* __restrict__ rkey,
                                                    const uint32_t* __restrict__ magic) {
     extern __shared__ __align__(16) unsigned char smem[];
-    size_t o_lut, o_left, o_right, o_cost, o_pre, total;
-    cost_smem_layout<C64>(txc, ha, c.D, c.Dp, CROSS, &o_lut, &o_left, &o_right, &o_cost, &o_pre, &total);
-    const int nx = txc + 2 * ha;
-    const int nr = nx + c.D - 1;
-    const int W2 = c.Dp / 2;  // 32-bit words per pixel
-    const int CS = W2 + 1;    // staged cost row stride in words (odd: diagonal reads hit distinct banks)
-    float* s_lut = reinterpret_cast<float*>(smem + o_lut);
-    const size_t csz = C64 ? 8 : 4;
-    unsigned char* L = smem + o_left;
-    unsigned char* Rg = smem + o_right;
-    uint32_t* s_cost = reinterpret_cast<uint32_t*>(smem + o_cost);
+    const CostLayout ly = cost_layout(txc, ha, c.D, c.Dp, CROSS, PRIOR, C64);
+    const int nx = ly.nx, nr = ly.nr;
+    const int W2 = c.Dp / 2;
+    const int CS = W2 + 1;
+    const int nt = blockDim.x, tid = threadIdx.x;
+    float* s_lut = reinterpret_cast<float*>(smem + ly.lut);
+    uint32_t* s_magic = reinterpret_cast<uint32_t*>(smem + ly.magic);
+    uint32_t* s_arm = reinterpret_cast<uint32_t*>(smem + ly.arm);
+    Aux<C64>* s_left = reinterpret_cast<Aux<C64>*>(smem + ly.left);
+    Aux<C64>* s_right = reinterpret_cast<Aux<C64>*>(smem + ly.right);
+    uint32_t* s_rng = reinterpret_cast<uint32_t*>(smem + ly.rng);
+    uint32_t* s_cost = reinterpret_cast<uint32_t*>(smem + ly.cost);
+    uint32_t* s_cnt = reinterpret_cast<uint32_t*>(smem + ly.cnt);
+    uint32_t* s_seg = reinterpret_cast<uint32_t*>(smem + ly.seg);
+    __shared__ uint16_t s_q[65];
 
     const int y = blockIdx.y;
     const int x0 = blockIdx.x * txc;
-    const int xbase = x0 - ha;                  // staged left pixel 0
-    const int rbase = xbase - (c.d0 + c.D - 1); // staged right pixel 0
+    const int xbase = x0 - ha;                   // staged left pixel 0
+    const int rbase = xbase - (c.d0 + c.D - 1);  // staged right pixel 0
     const int row = y * c.w;
-    const int tid = threadIdx.x, nt = blockDim.x;
 
-    __shared__ uint16_t s_q[65];
-    for (int i = tid; i < kLutSize; i += nt) s_lut[i] = c.lut[i];
-    for (int i = tid; i < 65; i += nt) s_q[i] = c.qlut[i];
-    // left aux (census, gray, gx, gy, rmin, rmax) for x in [xbase, xbase+nx)
+    if (QLUT) {
+        for (int i = tid; i < 65; i += nt) s_q[i] = c.qlut[i];
+    } else {
+        for (int i = tid; i < kLutSize; i += nt) s_lut[i] = c.lut[i];
+    }
+    if (CROSS)
+        for (int i = tid; i < 2 * ha + 2; i += nt) s_magic[i] = magic[i];
     for (int i = tid; i < nx; i += nt) {
         const int x = xbase + i;
         const bool in = x >= 0 && x < c.w;
-        if (C64) reinterpret_cast<unsigned long long*>(L)[i] = in ? c.cl64[row + x] : 0ull;
-        else reinterpret_cast<uint32_t*>(L)[i] = in ? c.cl[row + x] : 0u;
-        L[nx * csz + i] = in ? c.lgray[row + x] : 0;
-        L[nx * (csz + 1) + i] = in ? c.lgx[row + x] : 0;
-        L[nx * (csz + 2) + i] = in ? c.lgy[row + x] : 0;
-        int16_t* rm = reinterpret_cast<int16_t*>(L + nx * (csz + 3));
-        rm[i] = in ? c.rmin[row + x] : (int16_t)0;
-        rm[nx + i] = in ? c.rmax[row + x] : (int16_t)0;  // empty range outside the image
+        Aux<C64> a{};
+        if (in) {
+            if constexpr (C64) a.c = c.cl64[row + x];
+            else a.c = c.cl[row + x];
+            a.g = (uint32_t)c.lgray[row + x] | ((uint32_t)c.lgx[row + x] << 8) | ((uint32_t)c.lgy[row + x] << 16);
+        }
+        s_left[i] = a;
+        if (PRIOR)  // empty range outside the image
+            s_rng[i] = in ? ((uint32_t)(uint16_t)c.rmin[row + x] | ((uint32_t)(uint16_t)c.rmax[row + x] << 16)) : 0u;
     }
     for (int i = tid; i < nr; i += nt) {
         const int xr = rbase + i;
-        const bool in = xr >= 0 && xr < c.w;
-        if (C64) reinterpret_cast<unsigned long long*>(Rg)[i] = in ? c.cr64[row + xr] : 0ull;
-        else reinterpret_cast<uint32_t*>(Rg)[i] = in ? c.cr[row + xr] : 0u;
-        Rg[nr * csz + i] = in ? c.rgray[row + xr] : 0;
-        Rg[nr * (csz + 1) + i] = in ? c.rgx[row + xr] : 0;
-        Rg[nr * (csz + 2) + i] = in ? c.rgy[row + xr] : 0;
+        Aux<C64> a{};
+        if (xr >= 0 && xr < c.w) {
+            if constexpr (C64) a.c = c.cr64[row + xr];
+            else a.c = c.cr[row + xr];
+            a.g = (uint32_t)c.rgray[row + xr] | ((uint32_t)c.rgx[row + xr] << 8) | ((uint32_t)c.rgy[row + xr] << 16);
+        }
+        s_right[i] = a;
     }
     __syncthreads();
 
-    const int16_t* s_rmin = reinterpret_cast<const int16_t*>(L + nx * (csz + 3));
-    const int16_t* s_rmax = s_rmin + nx;
-    // raw costs for every staged left pixel and disparity pair
-    for (int i = tid; i < nx * W2; i += nt) {
-        const int xi = i / W2, k = i - xi * W2;
+    // ---- raw quantised costs C(x, d) of the staged pixels (CostComputer::compute_volume,
+    // src/cost_computer.cpp:247-264), invalid = 0xFFFF
+    for_each_word(nx, W2, nt, [&](int xi, int k) {
         const int x = xbase + xi;
         uint32_t word = kInvalidWord;
         if (x >= 0 && x < c.w) {
-            const int lo = s_rmin[xi], hi = s_rmax[xi];
-            uint32_t clv = 0;
-            unsigned long long clv64 = 0;
-            if (C64) clv64 = reinterpret_cast<const unsigned long long*>(L)[xi];
-            else clv = reinterpret_cast<const uint32_t*>(L)[xi];
-            const int gl = L[nx * csz + xi], gxl = L[nx * (csz + 1) + xi], gyl = L[nx * (csz + 2) + xi];
+            const Aux<C64> la = s_left[xi];
+            int lo = 0, hi = 0;
+            if (PRIOR) {
+                const uint32_t rg = s_rng[xi];
+                lo = (int16_t)(rg & 0xFFFFu);
+                hi = (int16_t)(rg >> 16);
+            }
+            word = 0;
 #pragma unroll
-            for (int hsel = 0; hsel < 2; ++hsel) {
-                const int di = 2 * k + hsel;
+            for (int hs = 0; hs < 2; ++hs) {
+                const int di = 2 * k + hs;
                 const int d = c.d0 + di;
                 const int xr = x - d;
                 uint32_t q = kInvalidCost;
-                if (di < c.D && d >= lo && d < hi && xr >= 0 && xr < c.w) {
-                    const int ri = xr - rbase;
+                // default range [d0, min(dmax, x+1)) and x - d inside the image
+                bool ok = di < c.D && xr >= 0 && xr < c.w;
+                if (PRIOR) ok = ok && d >= lo && d < hi;
+                if (ok) {
+                    const Aux<C64> ra = s_right[xi - di + c.D - 1];
                     int pop;
-                    if (C64) pop = __popcll(clv64 ^ reinterpret_cast<const unsigned long long*>(Rg)[ri]);
-                    else pop = __popc(clv ^ reinterpret_cast<const uint32_t*>(Rg)[ri]);
-                    if (!c.use_ad && !c.use_grad) {
-                        // census-only cost: the host pre-quantised LUT (same float ops)
-                        q = s_q[pop];
-                        word = hsel == 0 ? ((word & 0xFFFF0000u) | q) : ((word & 0x0000FFFFu) | (q << 16));
-                        continue;
+                    if constexpr (C64) pop = __popcll(la.c ^ ra.c);
+                    else pop = __popc(la.c ^ ra.c);
+                    if (QLUT) {
+                        q = s_q[pop];  // census-only: the host pre-quantised LUT (same float ops)
+                    } else {
+                        float v = s_lut[kLutCensus + pop];
+                        const uint32_t ad = __vabsdiffu4(la.g, ra.g);
+                        if (c.use_ad) v = __fadd_rn(v, s_lut[kLutAd + (ad & 0xFFu)]);
+                        if (c.use_grad) v = __fadd_rn(v, s_lut[kLutGrad + ((ad >> 8) & 0xFFu) + (ad >> 16)]);
+                        int qi = __float2int_rz(__fadd_rn(__fmul_rn(v, c.scale), 0.5f));
+                        qi = qi < 0 ? 0 : (qi > c.cost_max ? c.cost_max : qi);
+                        q = (uint32_t)qi;
                     }
-                    float v = s_lut[kLutCensus + pop];
-                    if (c.use_ad) v = __fadd_rn(v, s_lut[kLutAd + abs(gl - (int)Rg[nr * csz + ri])]);
-                    if (c.use_grad) {
-                        const int g = abs(gxl - (int)Rg[nr * (csz + 1) + ri]) + abs(gyl - (int)Rg[nr * (csz + 2) + ri]);
-                        v = __fadd_rn(v, s_lut[kLutGrad + g]);
-                    }
-                    int qi = __float2int_rz(__fadd_rn(__fmul_rn(v, c.scale), 0.5f));
-                    qi = qi < 0 ? 0 : (qi > c.cost_max ? c.cost_max : qi);
-                    q = (uint32_t)qi;
                 }
-                word = hsel == 0 ? ((word & 0xFFFF0000u) | q) : ((word & 0x0000FFFFu) | (q << 16));
+                word |= q << (16 * hs);
             }
         }
         s_cost[xi * CS + k] = word;
-    }
+    });
     __syncthreads();
 
-    const uint16_t* s_c16 = reinterpret_cast<const uint16_t*>(s_cost);
     if (RWTA) {
-        // right pixels receiving a contribution from this tile's own (non-halo) columns
+        // right pixels receiving a contribution from this tile's own (non-halo) columns: the
+        // first minimum over d of C(xr + d, d) (src/pipeline.cpp:38-53) as key cost<<16 | d-d0
+        const uint16_t* s_c16 = reinterpret_cast<const uint16_t*>(s_cost);
         const int xe = min(x0 + txc, c.w);
-        const int r_lo = x0 - c.d0 - c.D + 1, r_hi = xe - c.d0;
+        const int r_lo = max(0, x0 - c.d0 - c.D + 1), r_hi = min(c.w, xe - c.d0);
         for (int xr = r_lo + tid; xr < r_hi; xr += nt) {
-            if (xr < 0 || xr >= c.w) continue;
-            int di_lo = x0 - xr - c.d0, di_hi = xe - xr - c.d0;
-            di_lo = max(di_lo, 0);
-            di_hi = min(di_hi, c.D);
+            const int di_lo = max(x0 - xr - c.d0, 0), di_hi = min(xe - xr - c.d0, c.D);
             uint32_t best = kInvalidWord;
+            const int xi0 = xr + c.d0 - xbase;  // staged column of di = 0
             for (int di = di_lo; di < di_hi; ++di) {
-                const int xi = xr + c.d0 + di - xbase;
-                const uint32_t v = s_c16[xi * (c.Dp + 2) + di];
+                const uint32_t v = s_c16[(xi0 + di) * (2 * CS) + di];
                 if (v != kInvalidCost) {
                     const uint32_t key = (v << 16) | (uint32_t)di;
                     best = key < best ? key : best;
@@ -176,87 +212,149 @@ __global__ void __launch_bounds__(256) cost_kernel(CostCtx c, int txc, int ha, i
 
     if (!CROSS) {
         if (STORE) {
-            for (int i = tid; i < txc * W2; i += nt) {
-                const int xi = i / W2, k = i - xi * W2;
+            for_each_word(txc, W2, nt, [&](int xi, int k) {
                 const int x = x0 + xi;
-                if (x < c.w) out_vol[((size_t)row + x) * W2 + k] = s_cost[(xi + ha) * CS + k];
-            }
+                if (x < c.w) out_vol[((size_t)row + x) * W2 + k] = s_cost[xi * CS + k];
+            });
         }
         return;
     }
 
-    // prefix over staged x of (sum, count) in 16-bit lanes
-    uint32_t* s_psum = reinterpret_cast<uint32_t*>(smem + o_pre);
-    uint32_t* s_pcnt = s_psum + (size_t)(nx + 1) * W2;
-    for (int k = tid; k < W2; k += nt) {
+    // ---- horizontal half of CostAggregator::aggregate_hv (src/cost_aggregator.cpp:65-105)
+    if (RWTA) __syncthreads();  // the argmin above still reads the raw costs
+    // arms of the tile's pixels (build_cross_arms, src/cost_aggregator.cpp:17-63)
+    for (int i = tid; i < txc; i += nt) {
+        const int x = x0 + i;
+        if (x >= c.w) continue;
+        const int sxi = i + ha;
+        const int c0 = (int)(s_left[sxi].g & 0xFFu);
+        int l = 0, r = 0;
+        while (l < lmax && x - l - 1 >= 0 && abs((int)(s_left[sxi - l - 1].g & 0xFFu) - c0) <= tau) ++l;
+        while (r < lmax && x + r + 1 < c.w && abs((int)(s_left[sxi + r + 1].g & 0xFFu) - c0) <= tau) ++r;
+        s_arm[i] = (uint32_t)l | ((uint32_t)r << 16);
+    }
+    // inclusive prefix over staged x of the valid costs (and, with per-pixel ranges, of the valid
+    // counts), in 16-bit lanes: each word column is cut into `segs` segments scanned in parallel
+    const int segs = ly.segs;
+    const int seglen = (nx + segs - 1) / segs;
+    uint32_t* s_segc = s_seg + segs * W2;
+    for (int col = tid; col < W2 * segs; col += nt) {
+        const int k = col % W2, sg = col / W2;
+        const int a = sg * seglen, b = min(nx, a + seglen);
         uint32_t ps = 0, pc = 0;
-        s_psum[k] = 0;
-        s_pcnt[k] = 0;
-        for (int xi = 0; xi < nx; ++xi) {
+        for (int xi = a; xi < b; ++xi) {
             const uint32_t v = s_cost[xi * CS + k];
             const uint32_t inval = __vcmpeq2(v, kInvalidWord);  // 0xFFFF per invalid half
             ps = __vadd2(ps, v & ~inval);
-            pc = __vadd2(pc, 0x00010001u & ~inval);
-            s_psum[(xi + 1) * W2 + k] = ps;
-            s_pcnt[(xi + 1) * W2 + k] = pc;
+            s_cost[xi * CS + k] = ps;
+            if (PRIOR) {
+                pc = __vadd2(pc, 0x00010001u & ~inval);
+                s_cnt[xi * W2 + k] = pc;
+            }
         }
+        s_seg[sg * W2 + k] = ps;
+        if (PRIOR) s_segc[sg * W2 + k] = pc;
     }
     __syncthreads();
+    if (segs > 1) {
+        for (int col = tid; col < W2 * segs; col += nt) {
+            const int k = col % W2, sg = col / W2;
+            if (sg == 0) continue;
+            uint32_t os = 0, oc = 0;
+            for (int j = 0; j < sg; ++j) {
+                os = __vadd2(os, s_seg[j * W2 + k]);
+                if (PRIOR) oc = __vadd2(oc, s_segc[j * W2 + k]);
+            }
+            const int a = sg * seglen, b = min(nx, a + seglen);
+            for (int xi = a; xi < b; ++xi) {
+                s_cost[xi * CS + k] = __vadd2(s_cost[xi * CS + k], os);
+                if (PRIOR) s_cnt[xi * W2 + k] = __vadd2(s_cnt[xi * W2 + k], oc);
+            }
+        }
+        __syncthreads();
+    }
 
-    // query: one (tile pixel, word) per thread-iteration
-    for (int i = tid; i < txc * W2; i += nt) {
-        const int xi = i / W2, k = i - xi * W2;
+    // T(x, d) = floor(window sum / window count) over [x - L(x), x + R(x)]; the window stays inside
+    // the image.  A window difference is exact: the true sum is below 2^16.
+    for_each_word(txc, W2, nt, [&](int xi, int k) {
         const int x = x0 + xi;
-        if (x >= c.w) continue;
+        if (x >= c.w) return;
         const int sxi = xi + ha;
-        // arms L and R of build_cross_arms from the staged gray row
-        const int c0 = L[nx * csz + sxi];
-        int l = 0, r = 0;
-        while (l < lmax && x - l - 1 >= 0 && abs((int)L[nx * csz + sxi - l - 1] - c0) <= tau) ++l;
-        while (r < lmax && x + r + 1 < c.w && abs((int)L[nx * csz + sxi + r + 1] - c0) <= tau) ++r;
-        const int a = sxi - l, b = sxi + r + 1;
-        const uint32_t s = __vsub2(s_psum[b * W2 + k], s_psum[a * W2 + k]);
-        const uint32_t n = __vsub2(s_pcnt[b * W2 + k], s_pcnt[a * W2 + k]);
-        const int lo = s_rmin[sxi], hi = s_rmax[sxi];
+        const uint32_t arm = s_arm[xi];
+        const int l = (int)(arm & 0xFFFFu), r = (int)(arm >> 16);
+        const int a = sxi - l, b = sxi + r;  // inclusive staged window
+        const uint32_t s = __vsub2(s_cost[b * CS + k], a > 0 ? s_cost[(a - 1) * CS + k] : 0u);
+        uint32_t n2 = 0;
+        int lo = 0, hi = 0;
+        if (PRIOR) {
+            n2 = __vsub2(s_cnt[b * W2 + k], a > 0 ? s_cnt[(a - 1) * W2 + k] : 0u);
+            const uint32_t rg = s_rng[sxi];
+            lo = (int16_t)(rg & 0xFFFFu);
+            hi = (int16_t)(rg >> 16);
+        }
         uint32_t word = 0;
 #pragma unroll
-        for (int hsel = 0; hsel < 2; ++hsel) {
-            const int di = 2 * k + hsel;
+        for (int hs = 0; hs < 2; ++hs) {
+            const int di = 2 * k + hs;
             const int d = c.d0 + di;
-            const uint32_t sh = (s >> (16 * hsel)) & 0xFFFFu, nh = (n >> (16 * hsel)) & 0xFFFFu;
-            uint32_t q = kInvalidCost;
-            if (di < c.D && d >= lo && d < hi && nh > 0) q = div_by_magic(sh, nh, magic[nh]);
-            word |= q << (16 * hsel);
+            const uint32_t sh = (s >> (16 * hs)) & 0xFFFFu;
+            int nh;
+            bool ok;
+            if (PRIOR) {
+                nh = (int)((n2 >> (16 * hs)) & 0xFFFFu);
+                ok = di < c.D && d >= lo && d < hi && nh > 0;
+            } else {
+                // valid x' in the window: d <= x' <= w - 1 + d
+                nh = min(x + r, c.w - 1 + d) - max(x - l, d) + 1;
+                ok = di < c.D && d <= x && nh > 0;
+            }
+            const uint32_t q = ok ? div_by_magic(sh, (uint32_t)nh, s_magic[nh]) : kInvalidCost;
+            word |= q << (16 * hs);
         }
         out_vol[((size_t)row + x) * W2 + k] = word;
-    }
+    });
 }
 
-template <bool C64, bool CROSS, bool STORE, bool RWTA>
-cudaError_t launch_cost_t(const CostCtx& c, int lmax, int tau, uint32_t* vol, uint32_t* rkey,
+template <bool C64, bool CROSS, bool STORE, bool RWTA, bool PRIOR, bool QLUT>
+cudaError_t launch_cost_t(const CostCtx& c, int txc, int lmax, int tau, uint32_t* vol, uint32_t* rkey,
                           const uint32_t* magic, cudaStream_t s) {
-    const int txc = c.Dp <= 128 ? 64 : 32;
     const int ha = CROSS ? lmax : 0;
-    size_t a, b, d, e, f, total;
-    cost_smem_layout<C64>(txc, ha, c.D, c.Dp, CROSS, &a, &b, &d, &e, &f, &total);
-    auto kern = cost_kernel<C64, CROSS, STORE, RWTA>;
-    if (total > 48 * 1024) {
-        cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)total);
+    const CostLayout ly = cost_layout(txc, ha, c.D, c.Dp, CROSS, PRIOR, C64);
+    auto kern = cost_kernel<C64, CROSS, STORE, RWTA, PRIOR, QLUT>;
+    if (ly.total > 48 * 1024) {
+        cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ly.total);
         if (err != cudaSuccess) return err;
     }
     dim3 grid((c.w + txc - 1) / txc, c.h);
-    kern<<<grid, 256, total, s>>>(c, txc, ha, lmax, tau, vol, rkey, magic);
+    kern<<<grid, cost_threads(c.Dp / 2), ly.total, s>>>(c, txc, ha, lmax, tau, vol, rkey, magic);
     return cudaGetLastError();
+}
+
+// Tile width: 128 columns where the staged costs fit comfortably (halo overhead 2*lmax/txc), else 64.
+int cost_tile(int Dp) { return Dp <= 128 ? 128 : 64; }
+
+template <bool C64, bool PRIOR>
+cudaError_t launch_cost_m(const CostCtx& c, int mode, int lmax, int tau, uint32_t* vol, uint32_t* rkey,
+                          const uint32_t* magic, cudaStream_t s) {
+    const int txc = cost_tile(c.Dp);
+    const bool qlut = !c.use_ad && !c.use_grad;
+    if (mode == 1) {
+        return qlut ? launch_cost_t<C64, true, true, true, PRIOR, true>(c, txc, lmax, tau, vol, rkey, magic, s)
+                    : launch_cost_t<C64, true, true, true, PRIOR, false>(c, txc, lmax, tau, vol, rkey, magic, s);
+    }
+    if (mode == 0) {
+        return qlut ? launch_cost_t<C64, false, true, true, PRIOR, true>(c, txc, lmax, tau, vol, rkey, magic, s)
+                    : launch_cost_t<C64, false, true, true, PRIOR, false>(c, txc, lmax, tau, vol, rkey, magic, s);
+    }
+    return qlut ? launch_cost_t<C64, false, false, true, PRIOR, true>(c, txc, lmax, tau, vol, rkey, magic, s)
+                : launch_cost_t<C64, false, false, true, PRIOR, false>(c, txc, lmax, tau, vol, rkey, magic, s);
 }
 
 }  // namespace
 
 size_t cost_kernel_smem_bytes(int D, int Dp, int lmax, bool cross, bool census64) {
-    const int txc = Dp <= 128 ? 64 : 32;
-    size_t a, b, d, e, f, total;
-    if (census64) cost_smem_layout<true>(txc, cross ? lmax : 0, D, Dp, cross, &a, &b, &d, &e, &f, &total);
-    else cost_smem_layout<false>(txc, cross ? lmax : 0, D, Dp, cross, &a, &b, &d, &e, &f, &total);
-    return total;
+    // the largest variant: per-pixel ranges (count prefix) included
+    return cost_layout(cost_tile(Dp), cross ? lmax : 0, D, Dp, cross, true, census64).total;
 }
 
 cudaError_t launch_cost(const CostCtx& c, int mode, int lmax, int tau, uint32_t* vol, uint32_t* rkey,
@@ -264,13 +362,11 @@ cudaError_t launch_cost(const CostCtx& c, int mode, int lmax, int tau, uint32_t*
     // mode: 0 = raw volume + right argmin, 1 = cross-H volume + right argmin,
     //       2 = right argmin only (fused Fast path)
     if (c.census64) {
-        if (mode == 0) return launch_cost_t<true, false, true, true>(c, lmax, tau, vol, rkey, magic, s);
-        if (mode == 1) return launch_cost_t<true, true, true, true>(c, lmax, tau, vol, rkey, magic, s);
-        return launch_cost_t<true, false, false, true>(c, lmax, tau, vol, rkey, magic, s);
+        return c.prior_ranges ? launch_cost_m<true, true>(c, mode, lmax, tau, vol, rkey, magic, s)
+                              : launch_cost_m<true, false>(c, mode, lmax, tau, vol, rkey, magic, s);
     }
-    if (mode == 0) return launch_cost_t<false, false, true, true>(c, lmax, tau, vol, rkey, magic, s);
-    if (mode == 1) return launch_cost_t<false, true, true, true>(c, lmax, tau, vol, rkey, magic, s);
-    return launch_cost_t<false, false, false, true>(c, lmax, tau, vol, rkey, magic, s);
+    return c.prior_ranges ? launch_cost_m<false, true>(c, mode, lmax, tau, vol, rkey, magic, s)
+                          : launch_cost_m<false, false>(c, mode, lmax, tau, vol, rkey, magic, s);
 }
 
 // disparity_right from the per-right-pixel argmin keys: legacy sub-pixel on the raw costs of the

@@ -229,6 +229,7 @@ CostCtx Engine::cost_ctx() const {
     c.cl = ptr<uint32_t>(lay_.cl); c.cr = ptr<uint32_t>(lay_.cr);
     c.cl64 = ptr<unsigned long long>(lay_.cl); c.cr64 = ptr<unsigned long long>(lay_.cr);
     c.rmin = ptr<int16_t>(lay_.rmin); c.rmax = ptr<int16_t>(lay_.rmax);
+    c.prior_ranges = cfg_.prior_enable ? 1 : 0;
     return c;
 }
 
