@@ -411,11 +411,209 @@ __device__ __forceinline__ void run_chain(const SgmArgs& a, const DirTable& tab,
     }
 }
 
-// prefetch depth PF divides the unroll U; the census ring needs U to be a multiple of 2K
-template <int K, bool CENSUS, int HDIR>
+// ---- volume-fed chains: loads staged through shared memory with cp.async
+//
+// A register ring cannot keep loads for many future steps independently in flight: completion is
+// tracked per warp by a handful of scoreboards, so loads issued for different steps end up waiting
+// for one another and each step pays a full HBM latency.  cp.async groups are tracked per step
+// instead: step t's group is committed PF steps before use, and cp.async.wait_group(PF-1) waits for
+// exactly that group.  Each lane copies its own words into a per-warp ring slot
+// [cost: 32 lanes x K][partial sums: NB x 32 x K][gray word: 32], so the reads back are
+// conflict-free and need no barrier (a lane reads only what it copied).
+
+__device__ __forceinline__ void cp_async4(uint32_t* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async8(uint32_t* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async16(uint32_t* dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// K words of one lane; the source is 4K-byte aligned (pixel slices are Dp*2 bytes, lanes 4K bytes).
+template <int K>
+__device__ __forceinline__ void cp_words(uint32_t* dst, const uint32_t* src) {
+    if constexpr (K % 4 == 0) {
+#pragma unroll
+        for (int k = 0; k < K; k += 4) cp_async16(dst + k, src + k);
+    } else if constexpr (K % 2 == 0) {
+#pragma unroll
+        for (int k = 0; k < K; k += 2) cp_async8(dst + k, src + k);
+    } else {
+#pragma unroll
+        for (int k = 0; k < K; ++k) cp_async4(dst + k, src + k);
+    }
+}
+
+template <int K>
+__device__ __forceinline__ void lds_words(const uint32_t* src, uint32_t (&v)[K]) {
+    if constexpr (K % 4 == 0) {
+#pragma unroll
+        for (int k = 0; k < K; k += 4) {
+            const uint4 t = *reinterpret_cast<const uint4*>(src + k);
+            v[k] = t.x; v[k + 1] = t.y; v[k + 2] = t.z; v[k + 3] = t.w;
+        }
+    } else if constexpr (K % 2 == 0) {
+#pragma unroll
+        for (int k = 0; k < K; k += 2) {
+            const uint2 t = *reinterpret_cast<const uint2*>(src + k);
+            v[k] = t.x; v[k + 1] = t.y;
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < K; ++k) v[k] = src[k];
+    }
+}
+
+template <int K, int NB>
+__host__ __device__ constexpr int vol_slot_words() { return (K + NB * K + 1) * 32; }
+
+// One volume-fed scanline chain (same recurrence and WTA as run_chain; loads via cp.async).
+template <int T, int K, int MODE, int PF, int NB>
+__device__ __forceinline__ void run_chain_vol(const SgmArgs& a, const DirTable& tab, uint32_t* s_ring, int dx,
+                                              int dy, int s, int nscan, uint32_t* out) {
+    static_assert((PF & (PF - 1)) == 0, "PF must be a power of two");
+    constexpr int SW = vol_slot_words<K, NB>();
+    const int lane = threadIdx.x & 31;
+    const int grp = lane / T, j = lane % T;
+    const unsigned gmask = T == 32 ? 0xffffffffu : (((1u << T) - 1u) << (grp * T));
+    int x0, y0, len;
+    scan_start(a, dx, dy, s, nscan, x0, y0, len);
+    const int maxlen = __reduce_max_sync(0xffffffffu, len);
+    if (maxlen == 0) return;
+    const int W2 = a.Dp / 2;
+    const int step = dy * a.w + dx;
+    const int p0 = y0 * a.w + x0;
+    const uint32_t p1x2 = (uint32_t)a.pen.P1 * 0x00010001u;
+
+    // loads of step t into slot t % PF; every step commits one group (empty past the end)
+    auto issue = [&](int t) {
+        if (t < len) {
+            uint32_t* sl = s_ring + (t & (PF - 1)) * SW;
+            const int p = p0 + t * step;
+            cp_words<K>(sl + lane * K, a.cvol + (size_t)p * W2 + j * K);
+#pragma unroll
+            for (int b = 0; b < NB; ++b) cp_words<K>(sl + 32 * K * (1 + b) + lane * K, tab.in[b] + (size_t)p * W2 + j * K);
+            cp_async4(sl + 32 * K * (1 + NB) + lane, a.gray + (p & ~3));
+        }
+        cp_commit();
+    };
+#pragma unroll
+    for (int t = 0; t < PF; ++t) issue(t);
+
+    uint32_t L[K];
+    uint32_t m = kInf;
+    int prev_g = 0;
+#pragma unroll
+    for (int k = 0; k < K; ++k) L[k] = kInf2;
+
+#pragma unroll 2
+    for (int t = 0; t < maxlen; ++t) {
+        cp_wait<PF - 1>();
+        if (t < len) {
+            const uint32_t* sl = s_ring + (t & (PF - 1)) * SW;
+            const int p = p0 + t * step;
+            uint32_t c[K];
+            lds_words<K>(sl + lane * K, c);
+#pragma unroll
+            for (int k = 0; k < K; ++k) c[k] = __vminu2(c[k], kInf2);  // 0xFFFF -> 0x7FFF
+            const int g = (int)((sl[32 * K * (1 + NB) + lane] >> (8 * (p & 3))) & 0xFFu);
+            if (t == 0 || m >= kInf) {
+#pragma unroll
+                for (int k = 0; k < K; ++k) L[k] = c[k];
+            } else {
+                const int P2 = adaptive_p2(a.pen, g - prev_g);
+                const uint32_t mp2 = (m + (uint32_t)P2) * 0x00010001u;
+                const uint32_t m2 = m * 0x00010001u;
+                uint32_t up = __shfl_up_sync(gmask, L[K - 1], 1, T);
+                uint32_t dn = __shfl_down_sync(gmask, L[0], 1, T);
+                if (j == 0) up = kInf2;
+                if (j == T - 1) dn = kInf2;
+                uint32_t Ln[K];
+#pragma unroll
+                for (int k = 0; k < K; ++k) {
+                    const uint32_t lo_nb = k == 0 ? up : L[k - 1];
+                    const uint32_t hi_nb = k == K - 1 ? dn : L[k + 1];
+                    const uint32_t lm = __byte_perm(lo_nb, L[k], 0x5432);
+                    const uint32_t lp = __byte_perm(L[k], hi_nb, 0x5432);
+                    const uint32_t b = __vminu2(L[k], __viaddmin_u16x2(__vminu2(lm, lp), p1x2, mp2));
+                    Ln[k] = __vadd2(c[k], __vsub2(b, m2));
+                }
+#pragma unroll
+                for (int k = 0; k < K; ++k) L[k] = Ln[k];
+            }
+            uint32_t mm;
+            if constexpr (K == 1) {
+                mm = min_halves(L[0]);
+            } else {
+                uint32_t acc = __vminu2(L[0], L[1]);
+#pragma unroll
+                for (int k = 2; k < K; k += 2) acc = k + 1 < K ? __vimin3_u16x2(acc, L[k], L[k + 1]) : __vminu2(acc, L[k]);
+                mm = min_halves(acc);
+            }
+            m = __reduce_min_sync(gmask, mm);
+            prev_g = g;
+            if (MODE == kFirst) {
+                st_cg<K>(out + (size_t)p * W2 + j * K, L);
+            } else {
+                uint32_t sv[K];
+#pragma unroll
+                for (int k = 0; k < K; ++k) sv[k] = L[k];
+#pragma unroll
+                for (int b = 0; b < NB; ++b) {
+                    uint32_t sb[K];
+                    lds_words<K>(sl + 32 * K * (1 + b) + lane * K, sb);
+#pragma unroll
+                    for (int k = 0; k < K; ++k) sv[k] = __vaddus2(sv[k], sb[k]);
+                }
+                if (a.store_final) {
+                    uint32_t o[K];
+#pragma unroll
+                    for (int k = 0; k < K; ++k) o[k] = sv[k] | __vcmpgeu2(sv[k], kInf2);
+                    st_cg<K>(const_cast<uint32_t*>(tab.in[0]) + (size_t)p * W2 + j * K, o);
+                }
+                wta<K, T>(a, gmask, j, p, sv);
+            }
+        }
+        // the slot just read is refilled only after its values were consumed above
+        issue(t + PF);
+    }
+    cp_wait<0>();
+}
+
+// Prefetch depth PF (steps of loads in flight per chain) and unroll U (a multiple of PF, so ring
+// slots are compile-time registers; the sliding census ring also needs a multiple of 2K).  A
+// volume-fed sweep has few chains per SM, so it keeps many steps in flight to cover the HBM
+// latency under load; the census-fed sweeps load little per step.
+#ifndef APGCU_SGM_PF_VOLUME_FIRST
+#define APGCU_SGM_PF_VOLUME_FIRST 8
+#endif
+#ifndef APGCU_SGM_PF_VOLUME_LAST
+#define APGCU_SGM_PF_VOLUME_LAST 8
+#endif
+#ifndef APGCU_SGM_PF_CENSUS
+#define APGCU_SGM_PF_CENSUS 4
+#endif
+constexpr int kVolPfFirst = APGCU_SGM_PF_VOLUME_FIRST;
+constexpr int kVolPfLast = APGCU_SGM_PF_VOLUME_LAST;
+constexpr int multiple_of_both(int pf, int k2) {
+    int u = pf;
+    while (u % k2) u += pf;
+    return u;
+}
+template <int K, bool CENSUS, int HDIR, int MODE>
 struct Unroll {
-    static constexpr int U = (CENSUS && HDIR != 0) ? (2 * K < 4 ? 4 : 2 * K) : 4;
-    static constexpr int PF = (U % 4 == 0) ? 4 : 2;
+    static constexpr int PF0 = CENSUS ? APGCU_SGM_PF_CENSUS
+                                      : (MODE == kFirst ? APGCU_SGM_PF_VOLUME_FIRST : APGCU_SGM_PF_VOLUME_LAST);
+    static constexpr int PF = (CENSUS && HDIR != 0 && multiple_of_both(PF0, 2 * K) > 16) ? 4 : PF0;
+    static constexpr int U = (CENSUS && HDIR != 0) ? multiple_of_both(PF, 2 * K) : PF;
 };
 
 __device__ __forceinline__ int find_dir(const DirTable& tab, int warp) {
@@ -440,16 +638,22 @@ __global__ void __launch_bounds__(128) sgm_first_kernel(SgmArgs a, DirTable tab)
     const int d = find_dir(tab, warp);
     const int dx = tab.dx[d], dy = tab.dy[d];
     const int s = (warp - tab.warp_begin[d]) * C + (threadIdx.x & 31) / T;
+    if constexpr (!CENSUS) {
+        extern __shared__ __align__(16) uint32_t s_dyn[];
+        uint32_t* ring = s_dyn + (threadIdx.x >> 5) * kVolPfFirst * vol_slot_words<K, 0>();
+        run_chain_vol<T, K, kFirst, kVolPfFirst, 0>(a, tab, ring, dx, dy, s, tab.nscan[d], tab.out[d]);
+        return;
+    }
     if (CENSUS && dy == 0) {
         if (dx > 0) {
-            using UR = Unroll<K, true, 1>;
+            using UR = Unroll<K, true, 1, kFirst>;
             run_chain<T, K, kFirst, true, 1, UR::PF, UR::U, 0>(a, tab, s_q, dx, dy, s, tab.nscan[d], tab.out[d]);
         } else {
-            using UR = Unroll<K, true, -1>;
+            using UR = Unroll<K, true, -1, kFirst>;
             run_chain<T, K, kFirst, true, -1, UR::PF, UR::U, 0>(a, tab, s_q, dx, dy, s, tab.nscan[d], tab.out[d]);
         }
     } else {
-        using UR = Unroll<K, CENSUS, 0>;
+        using UR = Unroll<K, CENSUS, 0, kFirst>;
         run_chain<T, K, kFirst, CENSUS, 0, UR::PF, UR::U, 0>(a, tab, s_q, dx, dy, s, tab.nscan[d], tab.out[d]);
     }
 }
@@ -465,7 +669,13 @@ __global__ void __launch_bounds__(128) sgm_last_kernel(SgmArgs a, DirTable tab) 
     constexpr int C = 32 / T;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int s = warp * C + (threadIdx.x & 31) / T;
-    using UR = Unroll<K, CENSUS, 0>;
+    if constexpr (!CENSUS) {
+        extern __shared__ __align__(16) uint32_t s_dyn[];
+        uint32_t* ring = s_dyn + (threadIdx.x >> 5) * kVolPfLast * vol_slot_words<K, NB>();
+        run_chain_vol<T, K, kLast, kVolPfLast, NB>(a, tab, ring, tab.dx[0], tab.dy[0], s, tab.nscan[0], nullptr);
+        return;
+    }
+    using UR = Unroll<K, CENSUS, 0, kLast>;
     run_chain<T, K, kLast, CENSUS, 0, UR::PF, UR::U, NB>(a, tab, s_q, tab.dx[0], tab.dy[0], s, tab.nscan[0], nullptr);
 }
 
@@ -501,8 +711,17 @@ cudaError_t launch_first_tk(const SgmArgs& a, DirTable tab, bool census, cudaStr
         tab.warp_begin[i + 1] = tab.warp_begin[i] + (tab.nscan[i] + C - 1) / C;
     }
     const int blocks = (tab.warp_begin[tab.n] + 3) / 4;
-    if (census) sgm_first_kernel<T, K, true><<<blocks, 128, 0, st>>>(a, tab);
-    else sgm_first_kernel<T, K, false><<<blocks, 128, 0, st>>>(a, tab);
+    if (census) {
+        sgm_first_kernel<T, K, true><<<blocks, 128, 0, st>>>(a, tab);
+    } else {
+        const size_t smem = (size_t)4 * kVolPfFirst * vol_slot_words<K, 0>() * 4;
+        auto kern = sgm_first_kernel<T, K, false>;
+        if (smem > 48 * 1024) {
+            const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return e;
+        }
+        kern<<<blocks, 128, smem, st>>>(a, tab);
+    }
     return cudaGetLastError();
 }
 
@@ -512,11 +731,21 @@ cudaError_t launch_last_tk(const SgmArgs& a, DirTable tab, bool census, cudaStre
     tab.nscan[0] = nscan_of(a, tab.dx[0], tab.dy[0]);
     const int warps = (tab.nscan[0] + C - 1) / C;
     const int blocks = (warps + 3) / 4;
-#define APGCU_LAST(NB)                                                                            \
-    if (tab.nin == NB) {                                                                          \
-        if (census) sgm_last_kernel<T, K, true, NB><<<blocks, 128, 0, st>>>(a, tab);              \
-        else sgm_last_kernel<T, K, false, NB><<<blocks, 128, 0, st>>>(a, tab);                    \
-        return cudaGetLastError();                                                                \
+#define APGCU_LAST(NB)                                                                               \
+    if (tab.nin == NB) {                                                                             \
+        if (census) {                                                                                \
+            sgm_last_kernel<T, K, true, NB><<<blocks, 128, 0, st>>>(a, tab);                         \
+        } else {                                                                                     \
+            const size_t smem = (size_t)4 * kVolPfLast * vol_slot_words<K, NB>() * 4;               \
+            auto kern = sgm_last_kernel<T, K, false, NB>;                                            \
+            if (smem > 48 * 1024) {                                                                  \
+                const cudaError_t e =                                                                \
+                    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
+                if (e != cudaSuccess) return e;                                                      \
+            }                                                                                        \
+            kern<<<blocks, 128, smem, st>>>(a, tab);                                                 \
+        }                                                                                            \
+        return cudaGetLastError();                                                                   \
     }
     APGCU_LAST(1)
     APGCU_LAST(3)
