@@ -105,8 +105,11 @@ Layout Engine::make_layout(const apg_pipeline_config_t& c, int w, int h, int ch,
     L.D = c.max_disparity - c.min_disparity;
     L.Dp = round_up(L.D, 64);
     L.cross = c.agg_enable != 0;
+    // Fast census-only path: by default the raw volume is stored once and the sweeps read it (the
+    // volume-fed sweeps are the faster ones); on request the sweeps recompute the census costs
+    // instead and no volume is allocated (kLayoutFastFused)
     L.fused_fast = !L.cross && c.census_type == APG_CENSUS_SYMMETRIC_9X7 && !c.use_ad && !c.use_grad &&
-                   !c.prior_enable && !(debug & 4);
+                   !c.prior_enable && (debug & kLayoutFastFused) && !(debug & 4);
     L.raw_cost = (debug & 1) != 0;
     const size_t n = (size_t)w * h;
     const size_t csz = c.census_type == APG_CENSUS_9X7 ? 8 : 4;
@@ -234,7 +237,7 @@ CostCtx Engine::cost_ctx() const {
 }
 
 int Engine::prepare(int w, int h, int ch) {
-    const Layout L = make_layout(cfg_, w, h, ch, debug_);
+    const Layout L = make_layout(cfg_, w, h, ch, debug_ | (fast_fused_ ? kLayoutFastFused : 0));
     if (arena_ && arena_bytes_ >= L.total && lay_.w == w && lay_.h == h && lay_.ch == ch &&
         lay_.raw_cost == L.raw_cost && lay_.fused_fast == L.fused_fast) {
         return kOk;
@@ -655,6 +658,11 @@ int apgcu_engine_set_tuning(apgcu_engine_t e, const char* key, int value) {
     if (std::strcmp(key, "sgm_lanes") == 0) {
         if (value != 0 && value != 8 && value != 16 && value != 32) return apgcu::kInvalidConfig;
         e->eng->set_sgm_lanes(value);
+        return 0;
+    }
+    if (std::strcmp(key, "fast_fused") == 0) {
+        if (value != 0 && value != 1) return apgcu::kInvalidConfig;
+        e->eng->set_fast_fused(value != 0);
         return 0;
     }
     return apgcu::kInvalidConfig;

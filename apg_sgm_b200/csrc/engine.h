@@ -26,6 +26,9 @@ enum Status : int {
     kUnsupportedBackend = 5, kResourceLimitExceeded = 6, kAllocationFailure = 7, kInternalError = 8
 };
 
+// Layout request bit beside the debug flags: Fast census-only sweeps recompute their costs.
+constexpr int kLayoutFastFused = 1 << 16;
+
 // Frame-size-dependent layout of the device arena.
 struct Layout {
     int w = 0, h = 0, ch = 0, D = 0, Dp = 0;
@@ -69,6 +72,7 @@ public:
     const std::string& last_error() const { return err_; }
     void set_debug(int f) { debug_ = f; }
     void set_sgm_lanes(int t) { sgm_lanes_ = t; }
+    void set_fast_fused(bool on) { fast_fused_ = on; }
     int debug() const { return debug_; }
     const apg_pipeline_config_t& config() const { return cfg_; }
     int device() const { return device_; }
@@ -92,6 +96,7 @@ private:
     int device_ = 0;
     int debug_ = 0;
     int sgm_lanes_ = 0;
+    bool fast_fused_ = false;
     cudaStream_t stream_ = nullptr;
     bool own_stream_ = false;
     unsigned char* arena_ = nullptr;

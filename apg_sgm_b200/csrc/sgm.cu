@@ -473,13 +473,16 @@ __device__ __forceinline__ void lds_words(const uint32_t* src, uint32_t (&v)[K])
 }
 
 template <int K, int NB>
-__host__ __device__ constexpr int vol_slot_words() { return (K + NB * K + 1) * 32; }
+__host__ __device__ constexpr int vol_slot_words() { return (K + NB * K) * 32; }
 
 // One volume-fed scanline chain (same recurrence and WTA as run_chain; loads via cp.async).
+// Steps run in blocks of T: at the start of a block lane j loads the gray level of step t0 + j
+// (prefetched one block ahead) and computes that step's adaptive P2, so a step costs one shuffle
+// for P2 instead of a load and the P2 arithmetic.  Addresses advance by a 32-bit word offset.
 template <int T, int K, int MODE, int PF, int NB>
 __device__ __forceinline__ void run_chain_vol(const SgmArgs& a, const DirTable& tab, uint32_t* s_ring, int dx,
                                               int dy, int s, int nscan, uint32_t* out) {
-    static_assert((PF & (PF - 1)) == 0, "PF must be a power of two");
+    static_assert((PF & (PF - 1)) == 0 && T % PF == 0, "PF: a power of two dividing T");
     constexpr int SW = vol_slot_words<K, NB>();
     const int lane = threadIdx.x & 31;
     const int grp = lane / T, j = lane % T;
@@ -492,98 +495,122 @@ __device__ __forceinline__ void run_chain_vol(const SgmArgs& a, const DirTable& 
     const int step = dy * a.w + dx;
     const int p0 = y0 * a.w + x0;
     const uint32_t p1x2 = (uint32_t)a.pen.P1 * 0x00010001u;
+    const uint32_t dstep = (uint32_t)(step * W2);  // word offset per step (wraps for negative steps)
 
-    // loads of step t into slot t % PF; every step commits one group (empty past the end)
-    auto issue = [&](int t) {
+    // loads of step t (word offset off) into slot t % PF; every step commits one group
+    auto issue = [&](int t, uint32_t off) {
         if (t < len) {
             uint32_t* sl = s_ring + (t & (PF - 1)) * SW;
-            const int p = p0 + t * step;
-            cp_words<K>(sl + lane * K, a.cvol + (size_t)p * W2 + j * K);
+            cp_words<K>(sl + lane * K, a.cvol + off);
 #pragma unroll
-            for (int b = 0; b < NB; ++b) cp_words<K>(sl + 32 * K * (1 + b) + lane * K, tab.in[b] + (size_t)p * W2 + j * K);
-            cp_async4(sl + 32 * K * (1 + NB) + lane, a.gray + (p & ~3));
+            for (int b = 0; b < NB; ++b) cp_words<K>(sl + 32 * K * (1 + b) + lane * K, tab.in[b] + off);
         }
         cp_commit();
     };
+    const uint32_t off0 = (uint32_t)p0 * (uint32_t)W2 + (uint32_t)(j * K);
+    uint32_t ioff = off0;  // offset of the next step to issue
 #pragma unroll
-    for (int t = 0; t < PF; ++t) issue(t);
+    for (int t = 0; t < PF; ++t) {
+        issue(t, ioff);
+        ioff += dstep;
+    }
+    uint32_t off = off0;  // offset of the current step
 
     uint32_t L[K];
     uint32_t m = kInf;
-    int prev_g = 0;
 #pragma unroll
     for (int k = 0; k < K; ++k) L[k] = kInf2;
+    int gnext = j < len ? (int)__ldg(a.gray + p0 + j * step) : 0;
+    int gcarry = 0;
 
-#pragma unroll 2
-    for (int t = 0; t < maxlen; ++t) {
-        cp_wait<PF - 1>();
-        if (t < len) {
-            const uint32_t* sl = s_ring + (t & (PF - 1)) * SW;
-            const int p = p0 + t * step;
-            uint32_t c[K];
-            lds_words<K>(sl + lane * K, c);
+    for (int t0 = 0; t0 < maxlen; t0 += T) {
+        // P2 of the steps [t0, t0 + T): lane j holds step t0 + j
+        const int gcur = gnext;
+        {
+            const int tn = t0 + T + j;
+            gnext = tn < len ? (int)__ldg(a.gray + p0 + tn * step) : 0;
+        }
+        int gprev = __shfl_up_sync(gmask, gcur, 1, T);
+        if (j == 0) gprev = gcarry;
+        gcarry = __shfl_sync(gmask, gcur, T - 1, T);
+        const int p2v = adaptive_p2(a.pen, gcur - gprev);
+
+        for (int u0 = 0; u0 < T; u0 += PF) {
+            if (t0 + u0 >= maxlen) break;
 #pragma unroll
-            for (int k = 0; k < K; ++k) c[k] = __vminu2(c[k], kInf2);  // 0xFFFF -> 0x7FFF
-            const int g = (int)((sl[32 * K * (1 + NB) + lane] >> (8 * (p & 3))) & 0xFFu);
-            if (t == 0 || m >= kInf) {
+            for (int v = 0; v < PF; ++v) {
+                const int t = t0 + u0 + v;
+                if (t >= maxlen) break;
+                cp_wait<PF - 1>();
+                const int P2 = __shfl_sync(gmask, p2v, u0 + v, T);
+                if (t < len) {
+                    const uint32_t* sl = s_ring + v * SW;
+                    uint32_t c[K];
+                    lds_words<K>(sl + lane * K, c);
 #pragma unroll
-                for (int k = 0; k < K; ++k) L[k] = c[k];
-            } else {
-                const int P2 = adaptive_p2(a.pen, g - prev_g);
-                const uint32_t mp2 = (m + (uint32_t)P2) * 0x00010001u;
-                const uint32_t m2 = m * 0x00010001u;
-                uint32_t up = __shfl_up_sync(gmask, L[K - 1], 1, T);
-                uint32_t dn = __shfl_down_sync(gmask, L[0], 1, T);
-                if (j == 0) up = kInf2;
-                if (j == T - 1) dn = kInf2;
-                uint32_t Ln[K];
+                    for (int k = 0; k < K; ++k) c[k] = __vminu2(c[k], kInf2);  // 0xFFFF -> 0x7FFF
+                    if (t == 0 || m >= kInf) {
 #pragma unroll
-                for (int k = 0; k < K; ++k) {
-                    const uint32_t lo_nb = k == 0 ? up : L[k - 1];
-                    const uint32_t hi_nb = k == K - 1 ? dn : L[k + 1];
-                    const uint32_t lm = __byte_perm(lo_nb, L[k], 0x5432);
-                    const uint32_t lp = __byte_perm(L[k], hi_nb, 0x5432);
-                    const uint32_t b = __vminu2(L[k], __viaddmin_u16x2(__vminu2(lm, lp), p1x2, mp2));
-                    Ln[k] = __vadd2(c[k], __vsub2(b, m2));
+                        for (int k = 0; k < K; ++k) L[k] = c[k];
+                    } else {
+                        const uint32_t mp2 = (m + (uint32_t)P2) * 0x00010001u;
+                        const uint32_t m2 = m * 0x00010001u;
+                        uint32_t up = __shfl_up_sync(gmask, L[K - 1], 1, T);
+                        uint32_t dn = __shfl_down_sync(gmask, L[0], 1, T);
+                        if (j == 0) up = kInf2;
+                        if (j == T - 1) dn = kInf2;
+                        uint32_t Ln[K];
+#pragma unroll
+                        for (int k = 0; k < K; ++k) {
+                            const uint32_t lo_nb = k == 0 ? up : L[k - 1];
+                            const uint32_t hi_nb = k == K - 1 ? dn : L[k + 1];
+                            const uint32_t lm = __byte_perm(lo_nb, L[k], 0x5432);
+                            const uint32_t lp = __byte_perm(L[k], hi_nb, 0x5432);
+                            const uint32_t b = __vminu2(L[k], __viaddmin_u16x2(__vminu2(lm, lp), p1x2, mp2));
+                            Ln[k] = __vadd2(c[k], __vsub2(b, m2));
+                        }
+#pragma unroll
+                        for (int k = 0; k < K; ++k) L[k] = Ln[k];
+                    }
+                    uint32_t mm;
+                    if constexpr (K == 1) {
+                        mm = min_halves(L[0]);
+                    } else {
+                        uint32_t acc = __vminu2(L[0], L[1]);
+#pragma unroll
+                        for (int k = 2; k < K; k += 2)
+                            acc = k + 1 < K ? __vimin3_u16x2(acc, L[k], L[k + 1]) : __vminu2(acc, L[k]);
+                        mm = min_halves(acc);
+                    }
+                    m = __reduce_min_sync(gmask, mm);
+                    if (MODE == kFirst) {
+                        st_cg<K>(out + off, L);
+                    } else {
+                        uint32_t sv[K];
+#pragma unroll
+                        for (int k = 0; k < K; ++k) sv[k] = L[k];
+#pragma unroll
+                        for (int b = 0; b < NB; ++b) {
+                            uint32_t sb[K];
+                            lds_words<K>(sl + 32 * K * (1 + b) + lane * K, sb);
+#pragma unroll
+                            for (int k = 0; k < K; ++k) sv[k] = __vaddus2(sv[k], sb[k]);
+                        }
+                        if (a.store_final) {
+                            uint32_t o[K];
+#pragma unroll
+                            for (int k = 0; k < K; ++k) o[k] = sv[k] | __vcmpgeu2(sv[k], kInf2);
+                            st_cg<K>(const_cast<uint32_t*>(tab.in[0]) + off, o);
+                        }
+                        wta<K, T>(a, gmask, j, p0 + t * step, sv);
+                    }
                 }
-#pragma unroll
-                for (int k = 0; k < K; ++k) L[k] = Ln[k];
-            }
-            uint32_t mm;
-            if constexpr (K == 1) {
-                mm = min_halves(L[0]);
-            } else {
-                uint32_t acc = __vminu2(L[0], L[1]);
-#pragma unroll
-                for (int k = 2; k < K; k += 2) acc = k + 1 < K ? __vimin3_u16x2(acc, L[k], L[k + 1]) : __vminu2(acc, L[k]);
-                mm = min_halves(acc);
-            }
-            m = __reduce_min_sync(gmask, mm);
-            prev_g = g;
-            if (MODE == kFirst) {
-                st_cg<K>(out + (size_t)p * W2 + j * K, L);
-            } else {
-                uint32_t sv[K];
-#pragma unroll
-                for (int k = 0; k < K; ++k) sv[k] = L[k];
-#pragma unroll
-                for (int b = 0; b < NB; ++b) {
-                    uint32_t sb[K];
-                    lds_words<K>(sl + 32 * K * (1 + b) + lane * K, sb);
-#pragma unroll
-                    for (int k = 0; k < K; ++k) sv[k] = __vaddus2(sv[k], sb[k]);
-                }
-                if (a.store_final) {
-                    uint32_t o[K];
-#pragma unroll
-                    for (int k = 0; k < K; ++k) o[k] = sv[k] | __vcmpgeu2(sv[k], kInf2);
-                    st_cg<K>(const_cast<uint32_t*>(tab.in[0]) + (size_t)p * W2 + j * K, o);
-                }
-                wta<K, T>(a, gmask, j, p, sv);
+                // the slot just read is refilled only after its values were consumed above
+                issue(t + PF, ioff);
+                ioff += dstep;
+                off += dstep;
             }
         }
-        // the slot just read is refilled only after its values were consumed above
-        issue(t + PF);
     }
     cp_wait<0>();
 }

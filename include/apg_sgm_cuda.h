@@ -59,7 +59,9 @@ APGCU_API const char* apgcu_engine_last_error(apgcu_engine_t e);
 APGCU_API int apgcu_engine_set_debug(apgcu_engine_t e, int flags);
 
 /* Kernel tuning knobs (results never change, only speed):
- *   "sgm_lanes": lanes per SGM scanline chain, 8 / 16 / 32 (0 = default, 32).
+ *   "sgm_lanes": lanes per SGM scanline chain, 8 / 16 / 32 (0 = default, 32);
+ *   "fast_fused": 1 = census-only Fast mode recomputes its costs inside the SGM sweeps and stores no
+ *                 cost volume (less memory, slower); 0 = store the volume once (default).
  * Returns 0, or APG_STATUS_INVALID_CONFIG for an unknown key or value. */
 APGCU_API int apgcu_engine_set_tuning(apgcu_engine_t e, const char* key, int value);
 

@@ -111,11 +111,15 @@ def test_stage_parity(case, O, apg):
     assert np.all((gpu["confidence"] >= 0) & (gpu["confidence"] <= 1))
 
 
-def test_fast_fused_equals_unfused(apg):
-    L, R = synth(200, 100, 48)
-    cfg = apg.config_from_mode(0, 48)
-    a = apg.Engine(cfg).process(L, R)
-    b = apg.Engine(cfg, debug=apg.DEBUG_NO_FUSION).process(L, R)
+@pytest.mark.parametrize("w,h,dmax", [(200, 100, 48), (333, 90, 128)])
+def test_fast_fused_equals_unfused(apg, w, h, dmax):
+    """The census-fused Fast sweeps (tuning fast_fused=1) equal the volume-fed default."""
+    L, R = synth(w, h, dmax)
+    cfg = apg.config_from_mode(0, dmax)
+    fused = apg.Engine(cfg)
+    fused.set_tuning("fast_fused", 1)
+    a = fused.process(L, R)
+    b = apg.Engine(cfg).process(L, R)
     for k in a:
         assert same_bits(a[k], b[k]), k
 

@@ -187,7 +187,7 @@ def test_workspace_estimates():
     wf = apg.workspace_bytes(fast, 1280, 720)
     wb = apg.workspace_bytes(bal, 1280, 720)
     vol = 1280 * 720 * 128 * 2
-    assert 3 * vol <= wf < 4 * vol      # Fast: three first-phase path-sum buffers, no cost volume
+    assert 4 * vol <= wf < 5 * vol      # Fast: the census cost volume and three first-phase path sums
     assert 4 * vol <= wb < 5 * vol      # Balanced: cross tmp (= first sum buffer), aggregated cost, 2 more sums
     assert apg.workspace_bytes(fast, 640, 480) < wf
 
