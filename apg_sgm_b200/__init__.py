@@ -96,6 +96,9 @@ class PipelineStats:
         self.unreliable_ratio = 0.0
         self.refine_changed_ratio = 0.0
         self.lr_fail_ratio = 0.0
+        self.valid_pixels = self.reliable_pixels = self.unreliable_pixels = 0
+        self.refine_changed_pixels = self.lr_fail_pixels = self.prior_support_count = 0
+        self.mean_search_width = self.mean_geometry_width = 0.0
         self.effective_threads = 0
         self.requested_threads = 0
         self.requested_backend = "Auto"
@@ -256,37 +259,47 @@ class StereoSession:
 
             def grab(fn, ctype, dtype):
                 p = fn(self._res, C.byref(w), C.byref(h))
-                return np.ctypeslib.as_array(C.cast(p, C.POINTER(ctype)), shape=(n,)).astype(dtype).reshape(
-                    h.value, w.value)
+                return np.ctypeslib.as_array(C.cast(p, C.POINTER(ctype)), shape=(n,)).reshape(h.value, w.value).copy()
 
             disp = grab(L.apg_result_get_disparity, C.c_float, np.float32)
             conf = grab(L.apg_result_get_confidence, C.c_float, np.float32)
             rel = grab(L.apg_result_get_reliable_mask, C.c_uint8, np.uint8)
             reason = grab(L.apg_result_get_invalid_reason, C.c_uint8, np.uint8)
-            stats = self._stats(disp, rel, reason)
+            stats = self._stats(disp.shape[1], disp.shape[0])
         return StereoResult(disp, conf, rel, reason, stats)
 
     compute = process
 
-    def _stats(self, disp, rel, reason) -> PipelineStats:
+    def _stats(self, w: int, h: int) -> PipelineStats:
+        """PipelineStats of the last frame; the pixel counters come from the device
+        (apgcu_session_get_frame_counts), the ratios are float32 divisions as in
+        src/pipeline.cpp:701-707."""
         ms = (C.c_double * 11)()
         cnt = (C.c_size_t * 4)()
+        fc = (C.c_ulonglong * 8)()
         lib().apgcu_session_get_stats(self._h, ms, cnt)
+        lib().apgcu_session_get_frame_counts(self._h, fc)
         s = PipelineStats()
         s.timing = StageTiming(list(ms))
         s.frame_allocation_count = s.allocation_count = int(cnt[0])
         s.frame_reuse_count = s.reuse_count = int(cnt[1])
         s.peak_workspace_bytes = int(cnt[2])
         s.retained_workspace_bytes = int(cnt[3])
-        n = disp.size
+        n = w * h
         D = self._cfg.D
         s.cost_bytes = n * D * 2
-        s.estimated_peak_bytes = int(lib().apgcu_session_estimate_bytes(self._h, disp.shape[1], disp.shape[0], 1))
-        s.valid_disparity_ratio = float((disp >= 0).sum()) / n if n else 0.0
-        rel_n = int((rel != 0).sum())
-        s.reliable_ratio = rel_n / n if n else 0.0
-        s.unreliable_ratio = (n - rel_n) / n if n else 0.0
-        s.lr_fail_ratio = float(np.isin(reason, (1, 2)).sum()) / n if n else 0.0
+        s.estimated_peak_bytes = int(lib().apgcu_session_estimate_bytes(self._h, w, h, 1))
+        (s.valid_pixels, s.reliable_pixels, s.unreliable_pixels, s.refine_changed_pixels, s.lr_fail_pixels,
+         s.prior_support_count) = (int(v) for v in fc[:6])
+        s.mean_search_width = fc[6] / n if n else 0.0
+        s.mean_geometry_width = fc[7] / n if n else 0.0
+        if n:
+            nf = np.float32(n)
+            s.valid_disparity_ratio = float(np.float32(s.valid_pixels) / nf)
+            s.reliable_ratio = float(np.float32(s.reliable_pixels) / nf)
+            s.unreliable_ratio = float(np.float32(s.unreliable_pixels) / nf)
+            s.refine_changed_ratio = float(np.float32(s.refine_changed_pixels) / nf)
+            s.lr_fail_ratio = float(np.float32(s.lr_fail_pixels) / nf)
         s.requested_threads = s.effective_threads = int(self._cfg.num_threads)
         s.requested_backend = self._requested_backend
         s.resolved_backend = "CUDA"

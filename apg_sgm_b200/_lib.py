@@ -100,6 +100,7 @@ _SIGS = {
     "apgcu_session_create_config": (C.c_void_p, [C.POINTER(PipelineConfig), C.c_int, C.c_size_t]),
     "apgcu_session_get_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_size_t)]),
     "apgcu_session_estimate_bytes": (C.c_size_t, [C.c_void_p, C.c_int, C.c_int, C.c_int]),
+    "apgcu_session_get_frame_counts": (C.c_int, [C.c_void_p, C.POINTER(C.c_ulonglong)]),
     "apgcu_kernel_launch_count": (C.c_ulonglong, []),
     "apgcu_engine_launch_profile": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_char_p), C.POINTER(C.c_float)]),
     "apgcu_right_wta_noalloc": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,

@@ -138,6 +138,7 @@ Layout Engine::make_layout(const apg_pipeline_config_t& c, int w, int h, int ch,
     L.lut = take(kLutSize * 4);
     L.qlut = take(65 * 2);
     L.magic = take(256 * 4);
+    L.stats = take(64);
     if (c.prior_enable) {
         const int cell = 16;
         L.gw = (w + cell - 1) / cell; L.gh = (h + cell - 1) / cell; L.n_cells = L.gw * L.gh;
@@ -274,13 +275,14 @@ int Engine::prepare(int w, int h, int ch) {
 }
 
 int Engine::process_host(const uint8_t* left, const uint8_t* right, int w, int h, int stride, int ch, float* disp,
-                         float* conf, uint8_t* reason, uint8_t* reliable) {
+                         float* conf, uint8_t* reason, uint8_t* reliable, bool outputs_pinned) {
     cudaSetDevice(device_);
     int rc = prepare(w, h, ch);
     if (rc) return rc;
     const size_t n = (size_t)w * h;
     const size_t in_bytes = n * ch;
-    const size_t need = 2 * in_bytes + n * 4 * 2 + n * 2;
+    const size_t out_bytes = outputs_pinned ? 0 : n * 4 * 2 + n * 2;
+    const size_t need = 2 * in_bytes + out_bytes;
     if (!pin_ || pinned_bytes_ < need) {
         if (pin_) cudaFreeHost(pin_);
         pin_ = nullptr;
@@ -293,10 +295,10 @@ int Engine::process_host(const uint8_t* left, const uint8_t* right, int w, int h
     }
     unsigned char* pl = pin_;
     unsigned char* pr = pin_ + in_bytes;
-    float* pdisp = reinterpret_cast<float*>(pin_ + 2 * in_bytes);
-    float* pconf = pdisp + n;
-    uint8_t* preason = reinterpret_cast<uint8_t*>(pconf + n);
-    uint8_t* prel = preason + n;
+    float* pdisp = outputs_pinned ? disp : reinterpret_cast<float*>(pin_ + 2 * in_bytes);
+    float* pconf = outputs_pinned ? conf : pdisp + n;
+    uint8_t* preason = outputs_pinned ? reason : reinterpret_cast<uint8_t*>(pconf + n);
+    uint8_t* prel = outputs_pinned ? reliable : preason + n;
     const size_t row = (size_t)w * ch;
     for (int y = 0; y < h; ++y) {
         std::memcpy(pl + y * row, left + (size_t)y * stride, row);
@@ -308,16 +310,36 @@ int Engine::process_host(const uint8_t* left, const uint8_t* right, int w, int h
     rc = run(ptr<uint8_t>(lay_.in_left), (int)row, ptr<uint8_t>(lay_.in_right), (int)row, ch, nullptr, nullptr, nullptr,
              nullptr);
     if (rc) return rc;
-    e = cudaMemcpyAsync(pdisp, ptr<float>(lay_.disp_out), n * 4, cudaMemcpyDeviceToHost, stream_);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(pconf, ptr<float>(lay_.confidence), n * 4, cudaMemcpyDeviceToHost, stream_);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(preason, ptr<uint8_t>(lay_.reason), n, cudaMemcpyDeviceToHost, stream_);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(prel, ptr<uint8_t>(lay_.reliable), n, cudaMemcpyDeviceToHost, stream_);
+    e = cudaSuccess;
+    if (pdisp) e = cudaMemcpyAsync(pdisp, ptr<float>(lay_.disp_out), n * 4, cudaMemcpyDeviceToHost, stream_);
+    if (e == cudaSuccess && pconf) e = cudaMemcpyAsync(pconf, ptr<float>(lay_.confidence), n * 4, cudaMemcpyDeviceToHost, stream_);
+    if (e == cudaSuccess && preason) e = cudaMemcpyAsync(preason, ptr<uint8_t>(lay_.reason), n, cudaMemcpyDeviceToHost, stream_);
+    if (e == cudaSuccess && prel) e = cudaMemcpyAsync(prel, ptr<uint8_t>(lay_.reliable), n, cudaMemcpyDeviceToHost, stream_);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(counts_, ptr<unsigned long long>(lay_.stats), sizeof(counts_),
+                                              cudaMemcpyDeviceToHost, stream_);
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
     if (e != cudaSuccess) return cuda_fail(e, "output download");
-    if (disp) std::memcpy(disp, pdisp, n * 4);
-    if (conf) std::memcpy(conf, pconf, n * 4);
-    if (reason) std::memcpy(reason, preason, n);
-    if (reliable) std::memcpy(reliable, prel, n);
+    counts_fresh_ = true;
+    if (!outputs_pinned) {
+        if (disp) std::memcpy(disp, pdisp, n * 4);
+        if (conf) std::memcpy(conf, pconf, n * 4);
+        if (reason) std::memcpy(reason, preason, n);
+        if (reliable) std::memcpy(reliable, prel, n);
+    }
+    return kOk;
+}
+
+int Engine::frame_counts(unsigned long long* out6) {
+    if (!arena_) return fail(kInternalError, "no frame has been processed");
+    if (!counts_fresh_) {
+        cudaSetDevice(device_);
+        cudaError_t e = cudaMemcpyAsync(counts_, ptr<unsigned long long>(lay_.stats), sizeof(counts_),
+                                        cudaMemcpyDeviceToHost, stream_);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+        if (e != cudaSuccess) return cuda_fail(e, "frame counters");
+        counts_fresh_ = true;
+    }
+    std::memcpy(out6, counts_, 6 * sizeof(unsigned long long));
     return kOk;
 }
 
@@ -326,6 +348,7 @@ int Engine::process_device(const uint8_t* dl, const uint8_t* dr, int w, int h, i
     cudaSetDevice(device_);
     int rc = prepare(w, h, ch);
     if (rc) return rc;
+    counts_fresh_ = false;
     return run(dl, stride, dr, stride, ch, d_disp, d_conf, d_reason, d_reliable);
 }
 
@@ -483,6 +506,14 @@ int Engine::run(const uint8_t* dl, int lstride, const uint8_t* dr, int rstride, 
     if (d_reliable) RUNC(cudaMemcpyAsync(d_reliable, ptr<uint8_t>(L.reliable), n, cudaMemcpyDeviceToDevice, s), "rel out");
     if (d_disp && d_disp != ptr<float>(L.disp_out) && debug_)
         RUNC(cudaMemcpyAsync(ptr<float>(L.disp_out), d_disp, n * 4, cudaMemcpyDeviceToDevice, s), "dbg");
+    // PipelineStats counters (src/pipeline.cpp:650-707); refine_changed compares the WTA map with
+    // the refined one, prior_support_count is the prior's selected-support count
+    unsigned long long* st = ptr<unsigned long long>(L.stats);
+    RUNC(cudaMemsetAsync(st, 0, 64, s), "stats init");
+    RUN(launch_frame_stats((int)n, final_out, ptr<uint8_t>(L.reliable), ptr<uint8_t>(L.reason),
+                           refine ? ptr<float>(L.disp_wta) : nullptr, refine ? ptr<float>(L.disp_ref) : nullptr,
+                           ptr<int16_t>(L.rmin), ptr<int16_t>(L.rmax), st, s), "frame stats");
+    if (cfg_.prior_enable) RUNC(cudaMemcpyAsync(st + 5, arena_ + L.pr_count, 4, cudaMemcpyDeviceToDevice, s), "support count");
     cudaEventRecord(ev_[9], s);
     have_times_ = true;
     count_launches(launches);

@@ -50,6 +50,7 @@ struct Layout {
     // HighQuality prior / refine
     size_t pr_cand, pr_ncand, pr_taken, pr_grid, pr_maps, pr_scratch, pr_count;
     size_t rf_prefix, rf_draws, rf_scan_tmp, rf_count;
+    size_t stats = 0;  // u64 frame counters (launch_frame_stats) + prior support count
     size_t rf_scan_tmp_bytes = 0;
     int n_cells = 0, gw = 0, gh = 0, max_cand = 0;
 };
@@ -59,8 +60,13 @@ public:
     Engine(const apg_pipeline_config_t& cfg, int device, cudaStream_t stream);
     ~Engine();
 
+    // outputs_pinned: the four host outputs are page-locked, so the device copies land in them
+    // directly (otherwise they go through the engine's pinned staging)
     int process_host(const uint8_t* left, const uint8_t* right, int w, int h, int stride, int ch,
-                     float* disp, float* conf, uint8_t* reason, uint8_t* reliable);
+                     float* disp, float* conf, uint8_t* reason, uint8_t* reliable, bool outputs_pinned = false);
+    // Frame counters of the last pair: valid, reliable, lr_fail, refine_changed, sum of range
+    // widths, prior support count.  Waits for the engine stream.
+    int frame_counts(unsigned long long* out6);
     int process_device(const uint8_t* dl, const uint8_t* dr, int w, int h, int stride, int ch,
                        float* d_disp, float* d_conf, uint8_t* d_reason, uint8_t* d_reliable);
     int sync();
@@ -121,6 +127,8 @@ public:
 
 private:
     int support_count_ = 0;
+    unsigned long long counts_[8] = {};  // frame counters copied with the host outputs
+    bool counts_fresh_ = false;
     std::string err_;
 };
 

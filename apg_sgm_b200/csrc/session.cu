@@ -9,7 +9,9 @@
 //     BoundedReuse keeps it (capacity is retained when a smaller frame follows a larger one) and
 //     re-checks the budget after the frame;
 //   * frame_count / total_time_ms advance only on success; results are owned host copies.
+#include <algorithm>
 #include <chrono>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <new>
@@ -42,21 +44,60 @@ struct apg_session_s {
     int last_w = 0, last_h = 0, last_dmax = 0;
     size_t frame_alloc = 0, frame_reuse = 0;
     double stage_ms[11] = {};
+    unsigned long long counts[6] = {};  // Engine::frame_counts of the last frame
+    int frame_w = 0, frame_h = 0;        // its size
     size_t peak_bytes = 0;
     std::mutex mu;
     ~apg_session_s() { delete eng; }
 };
 
+// Result maps live in one page-locked host buffer owned by the result object and reused across
+// frames, so the engine's device-to-host copies land in them directly.
 struct apg_result_s {
     int w = 0, h = 0;
-    std::vector<float> disparity, confidence;
-    std::vector<uint8_t> invalid_reason, reliable_mask;
+    bool has = false;
+    float* disparity = nullptr;
+    float* confidence = nullptr;
+    uint8_t* invalid_reason = nullptr;
+    uint8_t* reliable_mask = nullptr;
+    unsigned char* buf = nullptr;
+    size_t cap = 0;
+    bool pinned = false;
+    bool ensure(size_t n) {
+        const size_t need = n * 10;
+        if (cap < need) {
+            release();
+            void* p = nullptr;
+            if (cudaMallocHost(&p, need) == cudaSuccess) {
+                pinned = true;
+            } else {
+                cudaGetLastError();
+                p = std::malloc(need);
+                pinned = false;
+                if (!p) return false;
+            }
+            buf = static_cast<unsigned char*>(p);
+            cap = need;
+        }
+        disparity = reinterpret_cast<float*>(buf);
+        confidence = disparity + n;
+        invalid_reason = reinterpret_cast<uint8_t*>(confidence + n);
+        reliable_mask = invalid_reason + n;
+        return true;
+    }
+    void release() {
+        if (buf) {
+            if (pinned) cudaFreeHost(buf);
+            else std::free(buf);
+        }
+        buf = nullptr;
+        cap = 0;
+    }
     void clear() {
         w = h = 0;
-        disparity.clear(); confidence.clear(); invalid_reason.clear(); reliable_mask.clear();
-        disparity.shrink_to_fit(); confidence.shrink_to_fit();
-        invalid_reason.shrink_to_fit(); reliable_mask.shrink_to_fit();
+        has = false;
     }
+    ~apg_result_s() { release(); }
 };
 
 namespace {
@@ -193,12 +234,11 @@ int apg_session_process(apg_session_t s, const apg_image_view_t* left, const apg
         const bool was_reuse = s->opt.memory_policy == APG_MEMORY_BOUNDED_REUSE && w == s->last_w && h == s->last_h &&
                                s->cfg.max_disparity == s->last_dmax && s->eng->allocated_bytes() > 0;
         const size_t n = (size_t)w * h;
-        result->w = w;
-        result->h = h;
-        result->disparity.resize(n);
-        result->confidence.resize(n);
-        result->invalid_reason.resize(n);
-        result->reliable_mask.resize(n);
+        if (!result->ensure(n)) {
+            result->clear();
+            s->last_error = "Memory allocation failure";
+            return APG_STATUS_ALLOCATION_FAILURE;
+        }
         // the engine reads the two views with one common stride: repack only if they differ
         const uint8_t* lp = left->data;
         const uint8_t* rp = right->data;
@@ -215,14 +255,20 @@ int apg_session_process(apg_session_t s, const apg_image_view_t* left, const apg
             rp = repack.data() + row * h;
             stride = (int)row;
         }
-        rc = s->eng->process_host(lp, rp, w, h, stride, ch, result->disparity.data(), result->confidence.data(),
-                                  result->invalid_reason.data(), result->reliable_mask.data());
+        rc = s->eng->process_host(lp, rp, w, h, stride, ch, result->disparity, result->confidence,
+                                  result->invalid_reason, result->reliable_mask, result->pinned);
+        if (rc == APG_STATUS_OK) rc = s->eng->frame_counts(s->counts);
         if (rc != APG_STATUS_OK) {
             s->last_error = s->eng->last_error();
             result->clear();
             if (s->opt.memory_policy == APG_MEMORY_RELEASE_PER_FRAME) s->eng->release();
             return rc;
         }
+        result->w = w;
+        result->h = h;
+        result->has = true;
+        s->frame_w = w;
+        s->frame_h = h;
         s->eng->stage_times(s->stage_ms);
         s->peak_bytes = std::max(s->peak_bytes, s->eng->allocated_bytes());
         if (was_reuse) ++s->frame_reuse;
@@ -258,14 +304,14 @@ int apg_session_process(apg_session_t s, const apg_image_view_t* left, const apg
 
 #define APG_RESULT_GETTER(name, field, T)                                  \
     const T* name(apg_result_t r, int* width, int* height) {               \
-        if (!r || r->field.empty()) {                                      \
+        if (!r || !r->has) {                                               \
             if (width) *width = 0;                                         \
             if (height) *height = 0;                                       \
             return nullptr;                                                \
         }                                                                  \
         if (width) *width = r->w;                                          \
         if (height) *height = r->h;                                        \
-        return r->field.data();                                            \
+        return r->field;                                                   \
     }
 APG_RESULT_GETTER(apg_result_get_disparity, disparity, float)
 APG_RESULT_GETTER(apg_result_get_confidence, confidence, float)
@@ -328,6 +374,27 @@ APGCU_API int apgcu_session_get_stats(apg_session_t s, double* stage_ms11, size_
         counters4[2] = s->peak_bytes;
         counters4[3] = s->eng ? s->eng->allocated_bytes() : 0;
     }
+    return APG_STATUS_OK;
+}
+
+APGCU_API int apgcu_session_get_frame_counts(apg_session_t s, unsigned long long* counts8) {
+    if (!s || !counts8) return APG_STATUS_INTERNAL_ERROR;
+    const unsigned long long* c = s->counts;
+    const unsigned long long n = (unsigned long long)s->frame_w * (unsigned long long)s->frame_h;
+    counts8[0] = c[0];                     // valid_pixels
+    counts8[1] = c[1];                     // reliable_pixels
+    counts8[2] = n >= c[1] ? n - c[1] : 0; // unreliable_pixels
+    counts8[3] = c[3];                     // refine_changed_pixels
+    counts8[4] = c[2];                     // lr_fail_pixels
+    counts8[5] = c[5];                     // prior_support_count
+    counts8[6] = c[4];                     // sum over pixels of the search range width
+    // sum over pixels of the geometric width max(min(dmax, x+1) - dmin, 0) (src/pipeline.cpp:659-661)
+    unsigned long long g = 0;
+    for (int x = 0; x < s->frame_w; ++x) {
+        const int hi = std::min(s->cfg.max_disparity, x + 1);
+        g += hi > s->cfg.min_disparity ? (unsigned long long)(hi - s->cfg.min_disparity) : 0ull;
+    }
+    counts8[7] = g * (unsigned long long)s->frame_h;
     return APG_STATUS_OK;
 }
 

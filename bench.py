@@ -300,22 +300,51 @@ def run_b200(args, wl):
     vox = w * h * D
     value = vox * args.steps * world / (max_ms / 1000.0)
 
-    # end to end through the public session API (host buffers, copies inside every step)
-    sess = apg.StereoSession(mode=MODE_NAMES[mode].lower() if mode != 2 else "high_quality", max_disparity=D,
-                             memory_policy="bounded_reuse")
+    # end to end through the public C API (apg_session_process, src/c_api.cpp's entry point): host
+    # images in, host result maps out, the copies inside every step
+    import ctypes as C
+    from apg_sgm_b200 import _lib
+    lib = _lib.lib()
+    opts = _lib.SessionOptions()
+    opts.struct_size = C.sizeof(opts)
+    opts.quality_mode, opts.memory_policy, opts.max_disparity, opts.backend = mode, 1, D, 3
+    sess_c = lib.apg_session_create_ex(C.byref(opts))
+    res_c = lib.apg_result_create()
+    views = [(_lib.ImageView(l.ctypes.data, w, h, w, 1), _lib.ImageView(r.ctypes.data, w, h, w, 1)) for l, r in pairs]
+    rw, rh = C.c_int(), C.c_int()
+
+    def e2e_step(i):
+        lv, rv = views[i % npairs]
+        rc = lib.apg_session_process(sess_c, C.byref(lv), C.byref(rv), res_c)
+        if rc != 0:
+            raise RuntimeError(lib.apg_session_get_last_error(sess_c).decode())
+        return C.cast(lib.apg_result_get_disparity(res_c, C.byref(rw), C.byref(rh)), C.POINTER(C.c_float))[0]
+
     for i in range(max(args.warmup, 3)):
-        sess.process(*pairs[i % npairs])
+        e2e_step(i)
     if dist:
         dist.barrier()
     t0 = time.perf_counter()
     for k in range(args.steps):
-        res = sess.process(*pairs[k % npairs])
-        _ = float(res.disparity[0, 0])  # the step's result is on the host
+        e2e_step(k)
     e2e_s = time.perf_counter() - t0
     te = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
     if dist:
         dist.all_reduce(te, op=dist.ReduceOp.MAX)
     e2e_value = vox * args.steps * world / float(te.item())
+    lib.apg_result_destroy(res_c)
+    lib.apg_session_destroy(sess_c)
+
+    # the same through the Python binding (StereoSession.process returns fresh numpy arrays)
+    sess = apg.StereoSession(mode=MODE_NAMES[mode].lower() if mode != 2 else "high_quality", max_disparity=D,
+                             memory_policy="bounded_reuse")
+    for i in range(max(args.warmup, 3)):
+        sess.process(*pairs[i % npairs])
+    npy = max(3, min(args.steps, 50))
+    t0 = time.perf_counter()
+    for k in range(npy):
+        sess.process(*pairs[k % npairs])
+    py_value = vox * npy / (time.perf_counter() - t0)
 
     # dominant kernel and its roofline
     peak, peak_kind = _peaks()
@@ -340,7 +369,8 @@ def run_b200(args, wl):
                    "pairs_per_step": 1, "distinct_pairs": npairs, "l2": "flushed between steps (256 MiB write)",
                    "parallelism": f"replicas x{world}"},
         "e2e": {"value": e2e_value, "unit": "voxels/s", "h2d_bytes_per_step": 2 * w * h,
-                "d2h_bytes_per_step": w * h * 10, "api": "apg_session_process (BoundedReuse)"},
+                "d2h_bytes_per_step": w * h * 10 + 64, "api": "apg_session_process (C API, BoundedReuse)",
+                "python_binding_value": py_value},
         "gpu_launches": launches,
         "roofline": roofline,
         "clocks": clocks,

@@ -109,6 +109,10 @@ APGCU_API apg_session_t apgcu_session_create_config(const apg_pipeline_config_t*
 /* PipelineStats of the last frame: stage_ms11 as apgcu_engine_stage_times; counters4 =
  * {frame_allocation_count, frame_reuse_count, peak_workspace_bytes, retained_workspace_bytes}. */
 APGCU_API int apgcu_session_get_stats(apg_session_t s, double* stage_ms11, size_t* counters4);
+/* Frame counters of the last frame (PipelineStats, src/pipeline.cpp:650-707), computed on the device:
+ * counts8 = {valid_pixels, reliable_pixels, unreliable_pixels, refine_changed_pixels, lr_fail_pixels,
+ * prior_support_count, sum of search-range widths, sum of geometric range widths}. */
+APGCU_API int apgcu_session_get_frame_counts(apg_session_t s, unsigned long long* counts8);
 /* Workspace bytes the budget gate compares against max_retained_bytes for a W x H x C frame. */
 APGCU_API size_t apgcu_session_estimate_bytes(apg_session_t s, int width, int height, int channels);
 

@@ -90,7 +90,7 @@ def ref_lib():
         _ref.ref_session_create.restype = C.c_void_p
         _ref.ref_session_create.argtypes = [C.POINTER(PipelineConfig), C.c_int]
         _ref.ref_session_destroy.argtypes = [C.c_void_p]
-        _ref.ref_session_process.argtypes = [C.c_void_p] + [C.c_void_p] * 2 + [C.c_int] * 4 + [C.c_void_p] * 5
+        _ref.ref_session_process.argtypes = [C.c_void_p] + [C.c_void_p] * 2 + [C.c_int] * 4 + [C.c_void_p] * 6
         _ref.ref_max_threads.restype = C.c_int
     return _ref
 
@@ -271,12 +271,17 @@ class RefSession:
         out = {"disparity": np.empty((h, w), np.float32), "confidence": np.empty((h, w), np.float32),
                "invalid_reason": np.empty((h, w), np.uint8), "reliable_mask": np.empty((h, w), np.uint8)}
         st = np.zeros(11, np.float64)
+        fs = np.zeros(13, np.float64)
         rc = ref_lib().ref_session_process(self._h, _p(L), _p(R), w, h, stride, ch,
                                            _p(out["disparity"]), _p(out["confidence"]),
-                                           _p(out["invalid_reason"]), _p(out["reliable_mask"]), _p(st))
+                                           _p(out["invalid_reason"]), _p(out["reliable_mask"]), _p(st), _p(fs))
         out["status"] = rc
         out["stage_ms"] = dict(zip(["aux", "prior", "cost", "cross", "right_wta", "sgm", "wta",
                                     "confidence", "refine", "post", "total"], st.tolist()))
+        out["stats"] = dict(zip(["valid_pixels", "reliable_pixels", "unreliable_pixels", "refine_changed_pixels",
+                                 "lr_fail_pixels", "prior_support_count", "mean_search_width",
+                                 "mean_geometry_width", "valid_disparity_ratio", "reliable_ratio",
+                                 "unreliable_ratio", "refine_changed_ratio", "lr_fail_ratio"], fs.tolist()))
         return out
 
     def close(self):

@@ -269,10 +269,12 @@ void* ref_session_create(const apg_pipeline_config_t* ccfg, int bounded_reuse) {
 void ref_session_destroy(void* s) { delete static_cast<StereoSession*>(s); }
 
 // StereoSession::process_status (include/apg_sgm/session.hpp:26-41) on a borrowed strided view.
-// stage_ms (nullable) receives the 11 StageTiming fields in declaration order.
+// stage_ms (nullable) receives the 11 StageTiming fields in declaration order; stats13 (nullable)
+// the PipelineStats frame counters: valid, reliable, unreliable, refine_changed and lr_fail pixels,
+// prior_support_count, mean_search_width, mean_geometry_width, then the five ratios.
 int ref_session_process(void* s, const uint8_t* left, const uint8_t* right, int w, int h, int stride,
                         int ch, float* disp, float* conf, uint8_t* reason, uint8_t* reliable,
-                        double* stage_ms) {
+                        double* stage_ms, double* stats13) {
     auto* ss = static_cast<StereoSession*>(s);
     StereoResult res;
     PipelineStats st;
@@ -289,6 +291,14 @@ int ref_session_process(void* s, const uint8_t* left, const uint8_t* right, int 
         const double v[11] = {t.aux_ms, t.prior_ms, t.cost_ms, t.cross_ms, t.right_wta_ms, t.sgm_ms,
                               t.wta_ms, t.confidence_ms, t.refine_ms, t.post_ms, t.total_ms};
         std::memcpy(stage_ms, v, sizeof(v));
+    }
+    if (stats13) {
+        const double v[13] = {(double)st.valid_pixels, (double)st.reliable_pixels, (double)st.unreliable_pixels,
+                              (double)st.refine_changed_pixels, (double)st.lr_fail_pixels,
+                              (double)st.prior_support_count, st.mean_search_width, st.mean_geometry_width,
+                              st.valid_disparity_ratio, st.reliable_ratio, st.unreliable_ratio,
+                              st.refine_changed_ratio, st.lr_fail_ratio};
+        std::memcpy(stats13, v, sizeof(v));
     }
     return 0;
 }

@@ -171,3 +171,25 @@ def test_baseline_workloads_match_oracle(mode, spec, O, apg):
     ora = O.pipeline(to_oracle(O, cfg), L, R)
     for k in ("disparity", "confidence", "invalid_reason", "reliable_mask"):
         assert same_bits(gpu[k], ora[k]), k
+
+
+@pytest.mark.parametrize("mode,w,h,dmax", [(0, 160, 96, 64), (1, 150, 90, 48), (2, 128, 96, 64)])
+def test_session_frame_stats_match_reference(apg, O, mode, w, h, dmax):
+    """PipelineStats counters and ratios of the session equal the reference session's
+    (src/pipeline.cpp:650-707): counted on the device, float32 ratios."""
+    if not O.ref_available():
+        pytest.skip("oracle/_ref not built")
+    L, R = synth(w, h, dmax, patch=0.2 if mode == 2 else 0.0, seed=11)
+    name = {0: "fast", 1: "balanced", 2: "high_quality"}[mode]
+    sess = apg.StereoSession(mode=name, max_disparity=dmax, memory_policy="bounded_reuse")
+    res = sess.process(L, R)
+    ref = O.RefSession(O.config(mode, dmax, volume_backend=2)).process(L, R)
+    assert ref["status"] == 0
+    for k in ("disparity", "confidence", "invalid_reason", "reliable_mask"):
+        assert same_bits(getattr(res, k), ref[k]), k
+    st, rs = res.stats, ref["stats"]
+    for k in ("valid_pixels", "reliable_pixels", "unreliable_pixels", "refine_changed_pixels", "prior_support_count"):
+        assert getattr(st, k) == int(rs[k]), (k, getattr(st, k), rs[k])
+    for k in ("valid_disparity_ratio", "reliable_ratio", "unreliable_ratio", "refine_changed_ratio", "lr_fail_ratio",
+              "mean_search_width", "mean_geometry_width"):
+        assert getattr(st, k) == rs[k], (k, getattr(st, k), rs[k])
