@@ -186,35 +186,43 @@ __global__ void median_kernel(int w, int h, int r, const float* __restrict__ in,
 // Frame counters of PipelineStats (src/pipeline.cpp:650-707): out[0] valid (disparity >= 0),
 // out[1] reliable (mask != 0), out[2] lr_fail (reason Occlusion or Mismatch), out[3] refine_changed
 // (before and after both >= 0 and |after - before| > 1e-4), out[4] sum over pixels of the search
-// range width max(hi - lo, 0).  One 64-bit atomic per warp and counter; out[] starts at zero.
-__global__ void frame_stats_kernel(int n, const float* __restrict__ disp, const uint8_t* __restrict__ reliable,
-                                   const uint8_t* __restrict__ reason, const float* __restrict__ before,
-                                   const float* __restrict__ after, const int16_t* __restrict__ rmin,
-                                   const int16_t* __restrict__ rmax, unsigned long long* __restrict__ out) {
-    uint32_t c0 = 0, c1 = 0, c2 = 0, c3 = 0, c4 = 0;
+// range width max(hi - lo, 0).  Warp and block reductions, then one 64-bit atomic per block and
+// counter (a few hundred blocks: same-address atomics serialise at L2); out[] starts at zero.
+__global__ void __launch_bounds__(256) frame_stats_kernel(int n, const float* __restrict__ disp,
+                                                          const uint8_t* __restrict__ reliable,
+                                                          const uint8_t* __restrict__ reason,
+                                                          const float* __restrict__ before,
+                                                          const float* __restrict__ after,
+                                                          const int16_t* __restrict__ rmin,
+                                                          const int16_t* __restrict__ rmax,
+                                                          unsigned long long* __restrict__ out) {
+    unsigned long long c[5] = {0, 0, 0, 0, 0};
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
-        c0 += disp[p] >= 0.f;
-        c1 += reliable[p] != 0;
+        c[0] += disp[p] >= 0.f;
+        c[1] += reliable[p] != 0;
         const uint8_t r = reason[p];
-        c2 += (r == kOcclusion || r == kMismatch);
+        c[2] += (r == kOcclusion || r == kMismatch);
         if (before) {
             const float db = before[p], da = after[p];
-            c3 += (db >= 0.f && da >= 0.f && fabsf(__fsub_rn(da, db)) > 1e-4f);
+            c[3] += (db >= 0.f && da >= 0.f && fabsf(__fsub_rn(da, db)) > 1e-4f);
         }
         const int wd = (int)rmax[p] - (int)rmin[p];
-        c4 += wd > 0 ? (uint32_t)wd : 0u;
+        c[4] += wd > 0 ? (unsigned)wd : 0u;
     }
-    c0 = __reduce_add_sync(0xffffffffu, c0);
-    c1 = __reduce_add_sync(0xffffffffu, c1);
-    c2 = __reduce_add_sync(0xffffffffu, c2);
-    c3 = __reduce_add_sync(0xffffffffu, c3);
-    c4 = __reduce_add_sync(0xffffffffu, c4);
-    if ((threadIdx.x & 31) == 0) {
-        atomicAdd(out + 0, (unsigned long long)c0);
-        atomicAdd(out + 1, (unsigned long long)c1);
-        atomicAdd(out + 2, (unsigned long long)c2);
-        atomicAdd(out + 3, (unsigned long long)c3);
-        atomicAdd(out + 4, (unsigned long long)c4);
+    __shared__ unsigned long long s_c[5][8];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int i = 0; i < 5; ++i) {
+        unsigned long long v = c[i];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) s_c[i][wid] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 5) {
+        unsigned long long v = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += s_c[threadIdx.x][w];
+        atomicAdd(out + threadIdx.x, v);
     }
 }
 
@@ -250,7 +258,8 @@ cudaError_t launch_median(int w, int h, int r, const float* in, float* out, cuda
 cudaError_t launch_frame_stats(int n, const float* disp, const uint8_t* reliable, const uint8_t* reason,
                                const float* before, const float* after, const int16_t* rmin, const int16_t* rmax,
                                unsigned long long* out5, cudaStream_t s) {
-    frame_stats_kernel<<<grid_for(n), 256, 0, s>>>(n, disp, reliable, reason, before, after, rmin, rmax, out5);
+    const int blocks = (n + 255) / 256 < 148 * 2 ? (n + 255) / 256 : 148 * 2;
+    frame_stats_kernel<<<blocks, 256, 0, s>>>(n, disp, reliable, reason, before, after, rmin, rmax, out5);
     return cudaGetLastError();
 }
 

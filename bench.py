@@ -54,7 +54,7 @@ def _peaks():
 
 def _profile_traffic(kernel: str, workload: str):
     """dram read+write bytes per launch from the committed ncu summary, if one exists."""
-    f = ROOT / "profiles" / f"{kernel}_{workload}.txt"
+    f = ROOT / "profiles" / f"{kernel.replace('+', '_')}_{workload}.txt"
     if not f.exists():
         return None
     for line in f.read_text().splitlines():
