@@ -11,6 +11,8 @@
 #include "common.cuh"
 #include "kernels.h"
 
+#include <type_traits>
+
 namespace apgcu {
 
 namespace {
@@ -88,6 +90,116 @@ __global__ void cross_v_kernel(int w, int h, int d0, int D, int Dp, int lmax, in
     }
 }
 
+// Vertical pass when every pixel has the default range [d0, min(dmax, x+1)) and d0 >= 0: then
+// T(x, y', d) is valid exactly when d <= x, for every row y', so the window count is the window
+// length and no count prefix is needed; lanes with d > x hold the invalid marker in every row and
+// their (wrapped) sums are never used.  Each thread keeps its column's prefix sums in a power-of-two shared
+// ring and loads its input words kB rows at a time, one batch ahead of use (register double
+// buffer), so kB loads per thread are in flight; the gray column segment is staged in shared
+// memory for the arms.
+constexpr int kB = 16;
+
+template <int RS>
+__global__ void __launch_bounds__(128) cross_v_default_kernel(int w, int h, int d0, int D, int Dp, int lmax, int tau,
+                                                              int cols, const uint8_t* __restrict__ gray,
+                                                              const uint32_t* __restrict__ tin,
+                                                              uint32_t* __restrict__ cout,
+                                                              const uint32_t* __restrict__ magic) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int W2 = Dp / 2;
+    const int nthr = W2 * cols;
+    uint32_t* ring = reinterpret_cast<uint32_t*>(smem);                      // [RS][nthr]
+    uint32_t* s_magic = ring + (size_t)RS * nthr;                              // [2*lmax+2]
+    uint8_t* s_gray = reinterpret_cast<uint8_t*>(s_magic + 2 * lmax + 2);     // [cols][kSeg + 2*lmax]
+    uint8_t* armU = s_gray + cols * (kSeg + 2 * lmax);                         // [cols][kSeg]
+    uint8_t* armD = armU + cols * kSeg;
+    const int xb = blockIdx.x * cols;
+    const int y0 = blockIdx.y * kSeg;
+    const int y1 = min(h, y0 + kSeg);
+    const int tid = threadIdx.x;
+    const int gs = kSeg + 2 * lmax;  // staged gray rows [y0 - lmax, y0 + kSeg + lmax)
+
+    for (int i = tid; i < 2 * lmax + 2; i += blockDim.x) s_magic[i] = magic[i];
+    for (int i = tid; i < cols * gs; i += blockDim.x) {
+        const int r = i / cols, ci = i - r * cols;
+        const int yy = y0 - lmax + r, x = xb + ci;
+        s_gray[ci * gs + r] = (x < w && yy >= 0 && yy < h) ? gray[yy * w + x] : 0;
+    }
+    __syncthreads();
+    for (int i = tid; i < cols * kSeg; i += blockDim.x) {
+        const int ci = i / kSeg, r = i - ci * kSeg;
+        const int yy = y0 + r, x = xb + ci;
+        int u = 0, v = 0;
+        if (x < w && yy < h) {
+            const uint8_t* g = s_gray + ci * gs + lmax + r;  // g[0] = gray(x, yy)
+            const int c0 = g[0];
+            while (u < lmax && yy - u - 1 >= 0 && abs((int)g[-u - 1] - c0) <= tau) ++u;
+            while (v < lmax && yy + v + 1 < h && abs((int)g[v + 1] - c0) <= tau) ++v;
+        }
+        armU[i] = (uint8_t)u;
+        armD[i] = (uint8_t)v;
+    }
+    __syncthreads();
+    if (tid >= nthr) return;
+    const int ci = tid / W2, k = tid - ci * W2;
+    const int x = xb + ci;
+    if (x >= w) return;
+    // output lanes that can be valid: d < dmax and d <= x
+    bool lane_ok[2];
+#pragma unroll
+    for (int hs = 0; hs < 2; ++hs) lane_ok[hs] = (2 * k + hs < D) && (d0 + 2 * k + hs <= x);
+
+    const int ystart = max(0, y0 - lmax);
+    const int yend = min(h, y1 + lmax);  // rows read: [ystart, yend)
+    // ring slot of prefix P(r) (sum over rows [ystart, r]) is (r - ystart + 1) & (RS - 1); slot 0 = P(ystart - 1) = 0
+    ring[tid] = 0;
+    const size_t rowstride = (size_t)w * W2;
+    const uint32_t* src = tin + ((size_t)ystart * w + x) * W2 + k;
+    uint32_t cur[kB], nxt[kB];
+#pragma unroll
+    for (int i = 0; i < kB; ++i) cur[i] = ystart + i < yend ? __ldcs(src + i * rowstride) : 0u;
+#pragma unroll
+    for (int i = 0; i < kB; ++i) nxt[i] = ystart + kB + i < yend ? __ldcs(src + (kB + i) * rowstride) : 0u;
+    int pushed = ystart;  // next row to add to the ring
+    uint32_t ps = 0;
+    uint32_t* dst = cout + ((size_t)y0 * w + x) * W2 + k;
+    for (int y = y0; y < y1; ++y) {
+        const int need = min(h, y + lmax + 1);
+        while (pushed < need) {
+            // add the buffered batch (rows [pushed, pushed + kB)) and load the one after next
+#pragma unroll
+            for (int i = 0; i < kB; ++i) {
+                if (pushed + i < yend) {
+                    ps = __vadd2(ps, cur[i]);
+                    ring[((pushed + i - ystart + 1) & (RS - 1)) * nthr + tid] = ps;
+                }
+            }
+            pushed += kB;
+#pragma unroll
+            for (int i = 0; i < kB; ++i) cur[i] = nxt[i];
+            const int base = pushed + kB;
+#pragma unroll
+            for (int i = 0; i < kB; ++i)
+                nxt[i] = base + i < yend ? __ldcs(src + (size_t)(base + i - ystart) * rowstride) : 0u;
+        }
+        const int ai = ci * kSeg + (y - y0);
+        const int a = y - armU[ai], b = y + armD[ai];  // inclusive window
+        const uint32_t sum = __vsub2(ring[((b - ystart + 1) & (RS - 1)) * nthr + tid],
+                                     ring[((a - ystart) & (RS - 1)) * nthr + tid]);
+        const int len = b - a + 1;
+        const uint32_t mg = s_magic[len];
+        uint32_t word = 0;
+#pragma unroll
+        for (int hs = 0; hs < 2; ++hs) {
+            const uint32_t sh = (sum >> (16 * hs)) & 0xFFFFu;
+            const uint32_t q = lane_ok[hs] ? div_by_magic(sh, (uint32_t)len, mg) : kInvalidCost;
+            word |= q << (16 * hs);
+        }
+        __stcs(dst, word);
+        dst += rowstride;
+    }
+}
+
 // Horizontal pass over a volume (aggregation iterations after the first).  A CTA owns one row
 // and a run of `cols` pixels... implemented as the transpose of the vertical kernel: one thread
 // per (row, word) sliding along x.
@@ -148,10 +260,31 @@ __global__ void cross_h_kernel(int w, int h, int d0, int D, int Dp, int lmax, in
 
 cudaError_t launch_cross_v(int w, int h, int d0, int D, int Dp, int lmax, int tau, const uint8_t* gray,
                            const int16_t* rmin, const int16_t* rmax, const uint32_t* tin, uint32_t* cout,
-                           const uint32_t* magic, cudaStream_t s) {
+                           const uint32_t* magic, bool default_ranges, cudaStream_t s) {
     const int W2 = Dp / 2;
     const int cols = W2 >= 128 ? 1 : 128 / W2;
     const int nthr = W2 * cols;
+    // fast path: default ranges, non-negative disparities, and a ring holding the 2*lmax+2 window
+    // prefixes plus a loaded batch
+    if (default_ranges && d0 >= 0 && nthr <= 128) {
+        const int span = 2 * lmax + 2 + 2 * kB;
+        const size_t extra = (size_t)(2 * lmax + 2) * 4 + (size_t)cols * (kSeg + 2 * lmax) + (size_t)cols * kSeg * 2;
+        auto go = [&](auto rs_tag) -> cudaError_t {
+            constexpr int RS = decltype(rs_tag)::value;
+            const size_t smem = (size_t)RS * nthr * 4 + extra;
+            auto kern = cross_v_default_kernel<RS>;
+            if (smem > 48 * 1024) {
+                cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                if (e != cudaSuccess) return e;
+            }
+            dim3 grid((w + cols - 1) / cols, (h + kSeg - 1) / kSeg);
+            kern<<<grid, 128, smem, s>>>(w, h, d0, D, Dp, lmax, tau, cols, gray, tin, cout, magic);
+            return cudaGetLastError();
+        };
+        if (span <= 64) return go(std::integral_constant<int, 64>());
+        if (span <= 128) return go(std::integral_constant<int, 128>());
+        if (span <= 256) return go(std::integral_constant<int, 256>());
+    }
     const int RS = 2 * lmax + 2;
     const size_t smem = (size_t)RS * nthr * 8 + (size_t)cols * kSeg * 2;
     if (smem > 48 * 1024) {

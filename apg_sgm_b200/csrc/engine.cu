@@ -421,13 +421,13 @@ int Engine::run(const uint8_t* dl, int lstride, const uint8_t* dr, int rstride, 
     if (L.cross) {
         const int tau = cfg_.color_threshold;
         RUN(launch_cross_v(w, h, d0, D, Dp, lmax, tau, ptr<uint8_t>(L.lgray), ptr<int16_t>(L.rmin), ptr<int16_t>(L.rmax),
-                           ptr<uint32_t>(L.volA), ptr<uint32_t>(L.volB), magic, s), "crossV");
+                           ptr<uint32_t>(L.volA), ptr<uint32_t>(L.volB), magic, !cfg_.prior_enable, s), "crossV");
         const int iters = std::max(1, cfg_.agg_iterations);
         for (int it = 1; it < iters; ++it) {
             RUN(launch_cross_h(w, h, d0, D, Dp, lmax, tau, ptr<uint8_t>(L.lgray), ptr<int16_t>(L.rmin), ptr<int16_t>(L.rmax),
                                ptr<uint32_t>(L.volB), ptr<uint32_t>(L.volA), magic, s), "crossH");
             RUN(launch_cross_v(w, h, d0, D, Dp, lmax, tau, ptr<uint8_t>(L.lgray), ptr<int16_t>(L.rmin), ptr<int16_t>(L.rmax),
-                               ptr<uint32_t>(L.volA), ptr<uint32_t>(L.volB), magic, s), "crossV");
+                               ptr<uint32_t>(L.volA), ptr<uint32_t>(L.volB), magic, !cfg_.prior_enable, s), "crossV");
         }
         sgm_src = ptr<uint32_t>(L.volB);
     }

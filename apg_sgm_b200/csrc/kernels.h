@@ -24,7 +24,7 @@ cudaError_t launch_right_wta_finalize(const CostCtx& c, const uint32_t* rkey, in
 // cross.cu
 cudaError_t launch_cross_v(int w, int h, int d0, int D, int Dp, int lmax, int tau, const uint8_t* gray,
                            const int16_t* rmin, const int16_t* rmax, const uint32_t* tin, uint32_t* cout,
-                           const uint32_t* magic, cudaStream_t s);
+                           const uint32_t* magic, bool default_ranges, cudaStream_t s);
 cudaError_t launch_cross_h(int w, int h, int d0, int D, int Dp, int lmax, int tau, const uint8_t* gray,
                            const int16_t* rmin, const int16_t* rmax, const uint32_t* vin, uint32_t* vout,
                            const uint32_t* magic, cudaStream_t s);
