@@ -475,13 +475,64 @@ __device__ __forceinline__ void lds_words(const uint32_t* src, uint32_t (&v)[K])
 template <int K, int NB>
 __host__ __device__ constexpr int vol_slot_words() { return (K + NB * K) * 32; }
 
+// Words per warp of the last sweep's WTA buffer: 32 pixels x (Dp/2 + 1) words (odd row stride, so
+// one lane per row reads without bank conflicts).
+template <int K, int T>
+__host__ __device__ constexpr int wta_buf_words() { return 32 * (K * T + 1); }
+
+// Winner-take-all of one pixel from its final sums, W2 u16x2 words in shared memory, run by one
+// lane (wta_impl, src/sgm_optimizer.cpp:465-536): the first minimum, the second minimum outside
+// |d - best| <= 1, the legacy parabola.  Sums >= 0x7FFF are invalid.  A negative winning
+// disparity reads as "none" like the reference's best_d < 0 test (:490-495).
+__device__ __forceinline__ void wta_row(const SgmArgs& a, const uint32_t* row, int W2, int p) {
+    uint32_t m2 = 0xFFFFFFFFu;
+    for (int k = 0; k < W2; ++k) m2 = __vminu2(m2, row[k]);
+    const uint32_t m = min_halves(m2);
+    float dval = -1.f, fb = __int_as_float(0x7f800000), fs = __int_as_float(0x7f800000);
+    if (m < kInf) {
+        const uint32_t mm = m * 0x00010001u;
+        int bdi = 0;
+        for (int k = 0; k < W2; ++k) {
+            const uint32_t eq = __vcmpeq2(row[k], mm);
+            if (eq) {
+                bdi = 2 * k + ((eq & 0xFFFFu) ? 0 : 1);
+                break;
+            }
+        }
+        if (a.d0 + bdi >= 0) {
+            const int k0 = (bdi - 1) >> 1, k1 = (bdi + 1) >> 1;  // words touching [bdi-1, bdi+1]
+            uint32_t s2 = 0xFFFFFFFFu;
+            for (int k = 0; k < W2; ++k) {
+                uint32_t v = row[k];
+                if (k >= k0 && k <= k1) {
+                    if (abs(2 * k - bdi) <= 1) v |= 0x0000FFFFu;
+                    if (abs(2 * k + 1 - bdi) <= 1) v |= 0xFFFF0000u;
+                }
+                s2 = __vminu2(s2, v);
+            }
+            const uint32_t sec = min_halves(s2);
+            dval = (float)(a.d0 + bdi);
+            if (a.subpixel && bdi > 0 && bdi + 1 < a.D) {
+                const uint16_t* r16 = reinterpret_cast<const uint16_t*>(row);
+                const uint32_t cm = r16[bdi - 1], cp = r16[bdi + 1];
+                if (cm < kInf && cp < kInf) dval = __fadd_rn(dval, legacy_delta((float)cm, (float)m, (float)cp));
+            }
+            fb = (float)m;
+            fs = sec >= kInf ? __int_as_float(0x7f800000) : (float)sec;
+        }
+    }
+    a.disp[p] = dval;
+    a.best[p] = fb;
+    a.second[p] = fs;
+}
+
 // One volume-fed scanline chain (same recurrence and WTA as run_chain; loads via cp.async).
 // Steps run in blocks of T: at the start of a block lane j loads the gray level of step t0 + j
 // (prefetched one block ahead) and computes that step's adaptive P2, so a step costs one shuffle
 // for P2 instead of a load and the P2 arithmetic.  Addresses advance by a 32-bit word offset.
 template <int T, int K, int MODE, int PF, int NB>
-__device__ __forceinline__ void run_chain_vol(const SgmArgs& a, const DirTable& tab, uint32_t* s_ring, int dx,
-                                              int dy, int s, int nscan, uint32_t* out) {
+__device__ __forceinline__ void run_chain_vol(const SgmArgs& a, const DirTable& tab, uint32_t* s_ring,
+                                              uint32_t* s_wta, int dx, int dy, int s, int nscan, uint32_t* out) {
     static_assert((PF & (PF - 1)) == 0 && T % PF == 0, "PF: a power of two dividing T");
     constexpr int SW = vol_slot_words<K, NB>();
     const int lane = threadIdx.x & 31;
@@ -602,7 +653,10 @@ __device__ __forceinline__ void run_chain_vol(const SgmArgs& a, const DirTable& 
                             for (int k = 0; k < K; ++k) o[k] = sv[k] | __vcmpgeu2(sv[k], kInf2);
                             st_cg<K>(const_cast<uint32_t*>(tab.in[0]) + off, o);
                         }
-                        wta<K, T>(a, gmask, j, p0 + t * step, sv);
+                        // final sums of this step's pixel into row (t - t0) of the group's WTA buffer
+                        uint32_t* wr = s_wta + grp * T * (K * T + 1) + (u0 + v) * (K * T + 1) + j * K;
+#pragma unroll
+                        for (int k = 0; k < K; ++k) wr[k] = sv[k];
                     }
                 }
                 // the slot just read is refilled only after its values were consumed above
@@ -610,6 +664,13 @@ __device__ __forceinline__ void run_chain_vol(const SgmArgs& a, const DirTable& 
                 ioff += dstep;
                 off += dstep;
             }
+        }
+        if (MODE == kLast) {
+            // the block's T pixels: lane j of the group runs the WTA of pixel t0 + j of its chain
+            __syncwarp();
+            if (t0 + j < len)
+                wta_row(a, s_wta + grp * T * (K * T + 1) + j * (K * T + 1), K * T, p0 + (t0 + j) * step);
+            __syncwarp();
         }
     }
     cp_wait<0>();
@@ -630,6 +691,13 @@ __device__ __forceinline__ void run_chain_vol(const SgmArgs& a, const DirTable& 
 #endif
 constexpr int kVolPfFirst = APGCU_SGM_PF_VOLUME_FIRST;
 constexpr int kVolPfLast = APGCU_SGM_PF_VOLUME_LAST;
+// Ring depth of the last sweep: the configured depth while 4 warps' rings and WTA buffers fit in
+// 200 KB of shared memory, else 4 (large disparity ranges).
+template <int K, int T, int NB>
+__host__ __device__ constexpr int last_pf() {
+    return (kVolPfLast * vol_slot_words<K, NB>() + wta_buf_words<K, T>()) * 4 * 4 <= 200 * 1024 ? kVolPfLast : 4;
+}
+
 constexpr int multiple_of_both(int pf, int k2) {
     int u = pf;
     while (u % k2) u += pf;
@@ -668,7 +736,7 @@ __global__ void __launch_bounds__(128) sgm_first_kernel(SgmArgs a, DirTable tab)
     if constexpr (!CENSUS) {
         extern __shared__ __align__(16) uint32_t s_dyn[];
         uint32_t* ring = s_dyn + (threadIdx.x >> 5) * kVolPfFirst * vol_slot_words<K, 0>();
-        run_chain_vol<T, K, kFirst, kVolPfFirst, 0>(a, tab, ring, dx, dy, s, tab.nscan[d], tab.out[d]);
+        run_chain_vol<T, K, kFirst, kVolPfFirst, 0>(a, tab, ring, nullptr, dx, dy, s, tab.nscan[d], tab.out[d]);
         return;
     }
     if (CENSUS && dy == 0) {
@@ -698,8 +766,11 @@ __global__ void __launch_bounds__(128) sgm_last_kernel(SgmArgs a, DirTable tab) 
     const int s = warp * C + (threadIdx.x & 31) / T;
     if constexpr (!CENSUS) {
         extern __shared__ __align__(16) uint32_t s_dyn[];
-        uint32_t* ring = s_dyn + (threadIdx.x >> 5) * kVolPfLast * vol_slot_words<K, NB>();
-        run_chain_vol<T, K, kLast, kVolPfLast, NB>(a, tab, ring, tab.dx[0], tab.dy[0], s, tab.nscan[0], nullptr);
+        constexpr int PF = last_pf<K, T, NB>();
+        constexpr int per_warp = PF * vol_slot_words<K, NB>() + wta_buf_words<K, T>();
+        uint32_t* ring = s_dyn + (threadIdx.x >> 5) * per_warp;
+        run_chain_vol<T, K, kLast, PF, NB>(a, tab, ring, ring + PF * vol_slot_words<K, NB>(), tab.dx[0], tab.dy[0],
+                                           s, tab.nscan[0], nullptr);
         return;
     }
     using UR = Unroll<K, CENSUS, 0, kLast>;
@@ -763,7 +834,7 @@ cudaError_t launch_last_tk(const SgmArgs& a, DirTable tab, bool census, cudaStre
         if (census) {                                                                                \
             sgm_last_kernel<T, K, true, NB><<<blocks, 128, 0, st>>>(a, tab);                         \
         } else {                                                                                     \
-            const size_t smem = (size_t)4 * kVolPfLast * vol_slot_words<K, NB>() * 4;               \
+            const size_t smem = (size_t)4 * (last_pf<K, T, NB>() * vol_slot_words<K, NB>() + wta_buf_words<K, T>()) * 4; \
             auto kern = sgm_last_kernel<T, K, false, NB>;                                            \
             if (smem > 48 * 1024) {                                                                  \
                 const cudaError_t e =                                                                \
