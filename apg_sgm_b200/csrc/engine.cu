@@ -357,17 +357,6 @@ int Engine::sync() {
     return e == cudaSuccess ? kOk : cuda_fail(e, "stream synchronize");
 }
 
-int Engine::run(const uint8_t* dl, int lstride, const uint8_t* dr, int rstride, int ch, float* d_disp, float* d_conf,
-                uint8_t* d_reason, uint8_t* d_reliable) {
-    const Layout& L = lay_;
-    const int w = L.w, h = L.h, D = L.D, Dp = L.Dp, d0 = cfg_.min_disparity;
-    const size_t n = (size_t)w * h;
-    cudaStream_t s = stream_;
-    unsigned launches = 0;
-    cudaError_t e = cudaSuccess;
-    const bool prof = (debug_ & 8) != 0;
-    nprof_ = 0;
-    if (prof) cudaEventRecord(pev_[0], s);
 #define RUN(expr, what)                                  \
     do {                                                 \
         e = (expr);                                      \
@@ -381,6 +370,26 @@ int Engine::run(const uint8_t* dl, int lstride, const uint8_t* dr, int rstride, 
         if (e != cudaSuccess) return cuda_fail(e, what); \
         if (prof) prof_mark("copy");                     \
     } while (0)
+
+int Engine::run(const uint8_t* dl, int lstride, const uint8_t* dr, int rstride, int ch, float* d_disp, float* d_conf,
+                uint8_t* d_reason, uint8_t* d_reliable) {
+    nprof_ = 0;
+    if (debug_ & 8) cudaEventRecord(pev_[0], stream_);
+    int rc = run_pre(dl, lstride, dr, rstride, ch);
+    if (rc == kOk) rc = run_sgm();
+    if (rc == kOk) rc = run_post(d_disp, d_conf, d_reason, d_reliable);
+    return rc;
+}
+
+int Engine::run_pre(const uint8_t* dl, int lstride, const uint8_t* dr, int rstride, int ch) {
+    const Layout& L = lay_;
+    const int w = L.w, h = L.h, D = L.D, Dp = L.Dp, d0 = cfg_.min_disparity;
+    const size_t n = (size_t)w * h;
+    cudaStream_t s = stream_;
+    unsigned launches = 0;
+    cudaError_t e = cudaSuccess;
+    const bool prof = (debug_ & 8) != 0;
+    (void)D; (void)Dp; (void)d0; (void)n; (void)w; (void)h;
     const int c64 = cfg_.census_type == APG_CENSUS_9X7;
     cudaEventRecord(ev_[0], s);
     RUN(launch_aux(dl, lstride, ch, w, h, c64, ptr<uint8_t>(L.lgray), ptr<uint8_t>(L.lgx), ptr<uint8_t>(L.lgy),
@@ -432,6 +441,20 @@ int Engine::run(const uint8_t* dl, int lstride, const uint8_t* dr, int rstride, 
         sgm_src = ptr<uint32_t>(L.volB);
     }
     cudaEventRecord(ev_[5], s);
+    sgm_src_ = sgm_src;
+    count_launches(launches);
+    return kOk;
+}
+
+int Engine::run_sgm() {
+    const Layout& L = lay_;
+    const int w = L.w, h = L.h, D = L.D, Dp = L.Dp, d0 = cfg_.min_disparity;
+    const size_t n = (size_t)w * h;
+    cudaStream_t s = stream_;
+    unsigned launches = 0;
+    cudaError_t e = cudaSuccess;
+    const bool prof = (debug_ & 8) != 0;
+    (void)D; (void)Dp; (void)d0; (void)n; (void)w; (void)h;
     // SGM: every sweep but the last in one launch (each direction into its own buffer), then the
     // last sweep adds them (Path8: folded into one buffer first) and runs the WTA.  The sum over
     // directions is order-free, so this changes no value.
@@ -442,7 +465,7 @@ int Engine::run(const uint8_t* dl, int lstride, const uint8_t* dr, int rstride, 
     pl.pen = SgmPen{cfg_.P1, cfg_.P2_base, cfg_.adaptive_penalties, cfg_.piecewise_p2, cfg_.grad_t1, cfg_.grad_t2,
                     cfg_.p2_alpha};
     pl.gray = ptr<uint8_t>(L.lgray);
-    pl.cvol = sgm_src;
+    pl.cvol = sgm_src_;
     pl.cl = ptr<uint32_t>(L.cl); pl.cr = ptr<uint32_t>(L.cr); pl.qlut = ptr<uint16_t>(L.qlut);
     pl.disp = ptr<float>(L.disp_wta); pl.best = ptr<float>(L.best); pl.second = ptr<float>(L.second);
     pl.subpixel = cfg_.subpixel;
@@ -458,6 +481,19 @@ int Engine::run(const uint8_t* dl, int lstride, const uint8_t* dr, int rstride, 
     }
     RUN(launch_sgm_last(pl, 0, -1, nin, sb, s), "sgm_last_wta");
     cudaEventRecord(ev_[6], s);
+    count_launches(launches);
+    return kOk;
+}
+
+int Engine::run_post(float* d_disp, float* d_conf, uint8_t* d_reason, uint8_t* d_reliable) {
+    const Layout& L = lay_;
+    const int w = L.w, h = L.h, D = L.D, Dp = L.Dp, d0 = cfg_.min_disparity;
+    const size_t n = (size_t)w * h;
+    cudaStream_t s = stream_;
+    unsigned launches = 0;
+    cudaError_t e = cudaSuccess;
+    const bool prof = (debug_ & 8) != 0;
+    (void)D; (void)Dp; (void)d0; (void)n; (void)w; (void)h;
     // confidence (+ LR when nothing runs between them)
     const bool refine = cfg_.refine_enable && cfg_.refine_iterations > 0;
     ConfLrArgs ca;
@@ -517,10 +553,11 @@ int Engine::run(const uint8_t* dl, int lstride, const uint8_t* dr, int rstride, 
     cudaEventRecord(ev_[9], s);
     have_times_ = true;
     count_launches(launches);
-#undef RUN
-#undef RUNC
     return kOk;
 }
+
+#undef RUN
+#undef RUNC
 
 void Engine::prof_mark(const char* name) {
     if (nprof_ >= kMaxProf) return;

@@ -91,6 +91,10 @@ private:
     int prepare(int w, int h, int ch);
     int run(const uint8_t* dl, int lstride, const uint8_t* dr, int rstride, int ch, float* d_disp, float* d_conf,
             uint8_t* d_reason, uint8_t* d_reliable);
+    // the three phases of run(): aux .. cross-V, the SGM sweeps + WTA, confidence .. frame counters
+    int run_pre(const uint8_t* dl, int lstride, const uint8_t* dr, int rstride, int ch);
+    int run_sgm();
+    int run_post(float* d_disp, float* d_conf, uint8_t* d_reason, uint8_t* d_reliable);
     int run_prior();
     int run_refine(float* work);
     int fail(int code, const std::string& m) { err_ = m; return code; }
@@ -128,6 +132,7 @@ public:
 private:
     int support_count_ = 0;
     unsigned long long counts_[8] = {};  // frame counters copied with the host outputs
+    const uint32_t* sgm_src_ = nullptr;  // volume the SGM sweeps read (set by run_pre)
     bool counts_fresh_ = false;
     std::string err_;
 };

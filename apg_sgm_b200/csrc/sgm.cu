@@ -531,7 +531,7 @@ __device__ __forceinline__ void wta_row(const SgmArgs& a, const uint32_t* row, i
 // (prefetched one block ahead) and computes that step's adaptive P2, so a step costs one shuffle
 // for P2 instead of a load and the P2 arithmetic.  Addresses advance by a 32-bit word offset.
 template <int T, int K, int MODE, int PF, int NB>
-__device__ __forceinline__ void run_chain_vol(const SgmArgs& a, const DirTable& tab, uint32_t* s_ring,
+__device__ __forceinline__ void run_chain_vol(const SgmArgs& a, const uint32_t* const* in, uint32_t* s_ring,
                                               uint32_t* s_wta, int dx, int dy, int s, int nscan, uint32_t* out) {
     static_assert((PF & (PF - 1)) == 0 && T % PF == 0, "PF: a power of two dividing T");
     constexpr int SW = vol_slot_words<K, NB>();
@@ -554,7 +554,7 @@ __device__ __forceinline__ void run_chain_vol(const SgmArgs& a, const DirTable& 
             uint32_t* sl = s_ring + (t & (PF - 1)) * SW;
             cp_words<K>(sl + lane * K, a.cvol + off);
 #pragma unroll
-            for (int b = 0; b < NB; ++b) cp_words<K>(sl + 32 * K * (1 + b) + lane * K, tab.in[b] + off);
+            for (int b = 0; b < NB; ++b) cp_words<K>(sl + 32 * K * (1 + b) + lane * K, in[b] + off);
         }
         cp_commit();
     };
@@ -651,7 +651,7 @@ __device__ __forceinline__ void run_chain_vol(const SgmArgs& a, const DirTable& 
                             uint32_t o[K];
 #pragma unroll
                             for (int k = 0; k < K; ++k) o[k] = sv[k] | __vcmpgeu2(sv[k], kInf2);
-                            st_cg<K>(const_cast<uint32_t*>(tab.in[0]) + off, o);
+                            st_cg<K>(const_cast<uint32_t*>(in[0]) + off, o);
                         }
                         // final sums of this step's pixel into row (t - t0) of the group's WTA buffer
                         uint32_t* wr = s_wta + grp * T * (K * T + 1) + (u0 + v) * (K * T + 1) + j * K;
@@ -736,7 +736,7 @@ __global__ void __launch_bounds__(128) sgm_first_kernel(SgmArgs a, DirTable tab)
     if constexpr (!CENSUS) {
         extern __shared__ __align__(16) uint32_t s_dyn[];
         uint32_t* ring = s_dyn + (threadIdx.x >> 5) * kVolPfFirst * vol_slot_words<K, 0>();
-        run_chain_vol<T, K, kFirst, kVolPfFirst, 0>(a, tab, ring, nullptr, dx, dy, s, tab.nscan[d], tab.out[d]);
+        run_chain_vol<T, K, kFirst, kVolPfFirst, 0>(a, tab.in, ring, nullptr, dx, dy, s, tab.nscan[d], tab.out[d]);
         return;
     }
     if (CENSUS && dy == 0) {
@@ -769,7 +769,7 @@ __global__ void __launch_bounds__(128) sgm_last_kernel(SgmArgs a, DirTable tab) 
         constexpr int PF = last_pf<K, T, NB>();
         constexpr int per_warp = PF * vol_slot_words<K, NB>() + wta_buf_words<K, T>();
         uint32_t* ring = s_dyn + (threadIdx.x >> 5) * per_warp;
-        run_chain_vol<T, K, kLast, PF, NB>(a, tab, ring, ring + PF * vol_slot_words<K, NB>(), tab.dx[0], tab.dy[0],
+        run_chain_vol<T, K, kLast, PF, NB>(a, tab.in, ring, ring + PF * vol_slot_words<K, NB>(), tab.dx[0], tab.dy[0],
                                            s, tab.nscan[0], nullptr);
         return;
     }
