@@ -15,6 +15,7 @@ import threading
 
 import numpy as np
 
+from . import _lib as _lib_mod
 from ._lib import ImageView, PipelineConfig, SessionOptions, lib
 
 __version__ = "1.0.0"
@@ -497,3 +498,81 @@ def workspace_bytes(config: PipelineConfig, width: int, height: int) -> int:
 __all__ = ["QualityMode", "VolumeBackend", "MemoryPolicy", "StatusCode", "InvalidReason", "StageTiming",
            "PipelineStats", "StereoResult", "StereoSession", "PipelineConfig", "config_from_mode", "Engine",
            "kernel_launch_count", "workspace_bytes", "__version__"]
+
+
+class Batch:
+    """Batched form (apgcu_batch_*): many pairs of uneven sizes and disparity ranges per call.
+
+    Pairs of equal size and range form a bucket; a bucket's pairs run their per-pixel stages
+    concurrently and share one persistent SGM launch per phase, replayed from a cached CUDA graph.
+    Each pair's outputs equal those of Engine.process for that pair alone."""
+
+    def __init__(self, config: PipelineConfig, device: int = 0, **options):
+        err = _validate_config(config)
+        if err:
+            raise RuntimeError(err)
+        self.config = config
+        self._h = lib().apgcu_batch_create(C.byref(config), int(device))
+        if not self._h:
+            raise RuntimeError("apgcu_batch_create failed")
+        for k, v in options.items():
+            self.set_option(k, v)
+
+    def set_option(self, key: str, value: int):
+        if lib().apgcu_batch_set_option(self._h, key.encode(), int(value)) != 0:
+            raise ValueError(f"invalid batch option {key}={value}")
+
+    def process(self, pairs) -> list:
+        """pairs: iterable of (left, right) or (left, right, max_disparity) host arrays.  Returns one
+        dict of disparity / confidence / invalid_reason / reliable_mask per pair."""
+        keep, outs = [], []
+        arr = (_lib_mod.Pair * len(pairs))()
+        for i, p in enumerate(pairs):
+            left, right = p[0], p[1]
+            dmax = int(p[2]) if len(p) > 2 else 0
+            lv, la = _image_view(left, "left")
+            rv, ra = _image_view(right, "right")
+            if lv.stride != rv.stride:
+                la, ra = np.ascontiguousarray(la), np.ascontiguousarray(ra)
+                lv, rv = _image_view(la, "left")[0], _image_view(ra, "right")[0]
+            h, w = lv.height, lv.width
+            o = {"disparity": np.empty((h, w), np.float32), "confidence": np.empty((h, w), np.float32),
+                 "invalid_reason": np.empty((h, w), np.uint8), "reliable_mask": np.empty((h, w), np.uint8)}
+            keep += [la, ra]
+            outs.append(o)
+            arr[i] = _lib_mod.Pair(lv.data, rv.data, w, h, lv.stride, lv.channels, dmax,
+                                   o["disparity"].ctypes.data, o["confidence"].ctypes.data,
+                                   o["invalid_reason"].ctypes.data, o["reliable_mask"].ctypes.data)
+        rc = lib().apgcu_batch_process(self._h, len(pairs), arr, 0)
+        if rc != 0:
+            raise RuntimeError(f"batch processing failed [{rc}]: {self.last_error}")
+        return outs
+
+    def process_device(self, pairs) -> None:
+        """pairs: list of _lib.Pair records holding device pointers (inputs and outputs)."""
+        arr = (_lib_mod.Pair * len(pairs))(*pairs)
+        rc = lib().apgcu_batch_process(self._h, len(pairs), arr, 1)
+        if rc != 0:
+            raise RuntimeError(f"batch processing failed [{rc}]: {self.last_error}")
+
+    @property
+    def last_error(self) -> str:
+        return lib().apgcu_batch_last_error(self._h).decode()
+
+    @property
+    def allocated_bytes(self) -> int:
+        return int(lib().apgcu_batch_allocated_bytes(self._h))
+
+    def release(self):
+        lib().apgcu_batch_release(self._h)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().apgcu_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -58,6 +58,14 @@ class SessionOptions(C.Structure):
                 ("min_disparity", C.c_int), ("max_disparity", C.c_int)]
 
 
+class Pair(C.Structure):
+    """apgcu_pair_t (include/apg_sgm_cuda.h): one pair of a batch."""
+    _fields_ = [("left", C.c_void_p), ("right", C.c_void_p), ("width", C.c_int), ("height", C.c_int),
+                ("stride", C.c_int), ("channels", C.c_int), ("max_disparity", C.c_int),
+                ("disparity", C.c_void_p), ("confidence", C.c_void_p), ("invalid_reason", C.c_void_p),
+                ("reliable_mask", C.c_void_p)]
+
+
 _lib = None
 
 _SIGS = {
@@ -103,6 +111,13 @@ _SIGS = {
     "apgcu_session_get_frame_counts": (C.c_int, [C.c_void_p, C.POINTER(C.c_ulonglong)]),
     "apgcu_kernel_launch_count": (C.c_ulonglong, []),
     "apgcu_engine_launch_profile": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_char_p), C.POINTER(C.c_float)]),
+    "apgcu_batch_create": (C.c_void_p, [C.POINTER(PipelineConfig), C.c_int]),
+    "apgcu_batch_destroy": (None, [C.c_void_p]),
+    "apgcu_batch_last_error": (C.c_char_p, [C.c_void_p]),
+    "apgcu_batch_process": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(Pair), C.c_int]),
+    "apgcu_batch_set_option": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int]),
+    "apgcu_batch_allocated_bytes": (C.c_size_t, [C.c_void_p]),
+    "apgcu_batch_release": (None, [C.c_void_p]),
     "apgcu_right_wta_noalloc": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                           C.c_void_p, C.c_void_p]),
 }

@@ -446,6 +446,101 @@ int Engine::run_pre(const uint8_t* dl, int lstride, const uint8_t* dr, int rstri
     return kOk;
 }
 
+int Engine::sgm_launch(SgmLaunch* out, uint32_t** sbufs) const {
+    const Layout& L = lay_;
+    SgmLaunch& pl = *out;
+    pl.w = L.w; pl.h = L.h; pl.d0 = cfg_.min_disparity; pl.D = L.D; pl.Dp = L.Dp;
+    pl.pen = SgmPen{cfg_.P1, cfg_.P2_base, cfg_.adaptive_penalties, cfg_.piecewise_p2, cfg_.grad_t1, cfg_.grad_t2,
+                    cfg_.p2_alpha};
+    pl.gray = ptr<uint8_t>(L.lgray);
+    // the volume run_pre leaves for the sweeps: cross-aggregated (volB), raw (volA), or none when
+    // the Fast sweeps recompute their census costs
+    pl.cvol = L.cross ? ptr<uint32_t>(L.volB) : (L.fused_fast ? nullptr : ptr<uint32_t>(L.volA));
+    pl.cl = ptr<uint32_t>(L.cl); pl.cr = ptr<uint32_t>(L.cr); pl.qlut = ptr<uint16_t>(L.qlut);
+    pl.disp = ptr<float>(L.disp_wta); pl.best = ptr<float>(L.best); pl.second = ptr<float>(L.second);
+    pl.subpixel = cfg_.subpixel;
+    pl.store_final = (debug_ & 2) != 0;
+    pl.lanes = sgm_lanes_;
+    for (int i = 0; i < L.nsbuf; ++i) sbufs[i] = ptr<uint32_t>(L.sbuf[i]);
+    return L.nsbuf;
+}
+
+int Engine::ensure_pinned(size_t need) {
+    if (pin_ && pinned_bytes_ >= need) return kOk;
+    if (pin_) {
+        cudaStreamSynchronize(stream_);
+        cudaFreeHost(pin_);
+    }
+    pin_ = nullptr;
+    pinned_bytes_ = 0;
+    if (cudaMallocHost(&pin_, need) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(kAllocationFailure, "pinned host staging allocation failed");
+    }
+    pinned_bytes_ = need;
+    return kOk;
+}
+
+int Engine::upload(const uint8_t* left, const uint8_t* right, int w, int h, int stride, int ch, bool device,
+                   cudaStream_t s) {
+    cudaSetDevice(device_);
+    int rc = prepare(w, h, ch);
+    if (rc) return rc;
+    const size_t n = (size_t)w * h, row = (size_t)w * ch, in_bytes = n * ch;
+    cudaError_t e;
+    if (device) {
+        e = cudaMemcpy2DAsync(ptr<uint8_t>(lay_.in_left), row, left, stride, row, h, cudaMemcpyDeviceToDevice, s);
+        if (e == cudaSuccess)
+            e = cudaMemcpy2DAsync(ptr<uint8_t>(lay_.in_right), row, right, stride, row, h, cudaMemcpyDeviceToDevice, s);
+    } else {
+        rc = ensure_pinned(2 * in_bytes + n * 10 + 64);
+        if (rc) return rc;
+        for (int y = 0; y < h; ++y) {
+            std::memcpy(pin_ + y * row, left + (size_t)y * stride, row);
+            std::memcpy(pin_ + in_bytes + y * row, right + (size_t)y * stride, row);
+        }
+        e = cudaMemcpyAsync(ptr<uint8_t>(lay_.in_left), pin_, in_bytes, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(ptr<uint8_t>(lay_.in_right), pin_ + in_bytes, in_bytes, cudaMemcpyHostToDevice, s);
+    }
+    return e == cudaSuccess ? kOk : cuda_fail(e, "input upload");
+}
+
+int Engine::enqueue_pre() {
+    counts_fresh_ = false;
+    const int row = lay_.w * lay_.ch;
+    return run_pre(ptr<uint8_t>(lay_.in_left), row, ptr<uint8_t>(lay_.in_right), row, lay_.ch);
+}
+
+int Engine::enqueue_post() { return run_post(nullptr, nullptr, nullptr, nullptr); }
+
+int Engine::download(float* disp, float* conf, uint8_t* reason, uint8_t* reliable, bool device, cudaStream_t s) {
+    const size_t n = (size_t)lay_.w * lay_.h;
+    const size_t in_bytes = n * lay_.ch;
+    const cudaMemcpyKind kind = device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    if (!device && (!pin_ || pinned_bytes_ < 2 * in_bytes + n * 10)) return fail(kInternalError, "no host staging");
+    unsigned char* st = device ? nullptr : pin_ + 2 * in_bytes;  // host staging: disparity, confidence, reason, reliable, counters
+    float* pd = device ? disp : reinterpret_cast<float*>(st);
+    float* pc = device ? conf : reinterpret_cast<float*>(st + n * 4);
+    uint8_t* pr = device ? reason : st + n * 8;
+    uint8_t* pm = device ? reliable : st + n * 9;
+    cudaError_t e = cudaSuccess;
+    if (disp) e = cudaMemcpyAsync(pd, ptr<float>(lay_.disp_out), n * 4, kind, s);
+    if (e == cudaSuccess && conf) e = cudaMemcpyAsync(pc, ptr<float>(lay_.confidence), n * 4, kind, s);
+    if (e == cudaSuccess && reason) e = cudaMemcpyAsync(pr, ptr<uint8_t>(lay_.reason), n, kind, s);
+    if (e == cudaSuccess && reliable) e = cudaMemcpyAsync(pm, ptr<uint8_t>(lay_.reliable), n, kind, s);
+    return e == cudaSuccess ? kOk : cuda_fail(e, "output download");
+}
+
+void Engine::finish_download(float* disp, float* conf, uint8_t* reason, uint8_t* reliable) const {
+    const size_t n = (size_t)lay_.w * lay_.h;
+    const unsigned char* st = pin_ + 2 * n * lay_.ch;
+    if (disp) std::memcpy(disp, st, n * 4);
+    if (conf) std::memcpy(conf, st + n * 4, n * 4);
+    if (reason) std::memcpy(reason, st + n * 8, n);
+    if (reliable) std::memcpy(reliable, st + n * 9, n);
+}
+
 int Engine::run_sgm() {
     const Layout& L = lay_;
     const int w = L.w, h = L.h, D = L.D, Dp = L.Dp, d0 = cfg_.min_disparity;
@@ -461,18 +556,8 @@ int Engine::run_sgm() {
     static const int first4[3][2] = {{1, 0}, {-1, 0}, {0, 1}};
     static const int first8[7][2] = {{1, 0}, {-1, 0}, {0, 1}, {1, 1}, {1, -1}, {-1, 1}, {-1, -1}};
     SgmLaunch pl;
-    pl.w = w; pl.h = h; pl.d0 = d0; pl.D = D; pl.Dp = Dp;
-    pl.pen = SgmPen{cfg_.P1, cfg_.P2_base, cfg_.adaptive_penalties, cfg_.piecewise_p2, cfg_.grad_t1, cfg_.grad_t2,
-                    cfg_.p2_alpha};
-    pl.gray = ptr<uint8_t>(L.lgray);
-    pl.cvol = sgm_src_;
-    pl.cl = ptr<uint32_t>(L.cl); pl.cr = ptr<uint32_t>(L.cr); pl.qlut = ptr<uint16_t>(L.qlut);
-    pl.disp = ptr<float>(L.disp_wta); pl.best = ptr<float>(L.best); pl.second = ptr<float>(L.second);
-    pl.subpixel = cfg_.subpixel;
-    pl.store_final = (debug_ & 2) != 0;
-    pl.lanes = sgm_lanes_;
     uint32_t* sb[7];
-    for (int i = 0; i < L.nsbuf; ++i) sb[i] = ptr<uint32_t>(L.sbuf[i]);
+    sgm_launch(&pl, sb);
     RUN(launch_sgm_first(pl, L.nsbuf, L.nsbuf == 7 ? first8 : first4, sb, s), "sgm_first");
     int nin = L.nsbuf;
     if (L.nsbuf == 7) {

@@ -64,6 +64,19 @@ public:
     // directly (otherwise they go through the engine's pinned staging)
     int process_host(const uint8_t* left, const uint8_t* right, int w, int h, int stride, int ch,
                      float* disp, float* conf, uint8_t* reason, uint8_t* reliable, bool outputs_pinned = false);
+    // Batch hooks.  upload: copy a pair (host or device memory) into the engine's input buffers on
+    // stream s; enqueue_pre / enqueue_post: the phases before and after the SGM on the engine's own
+    // stream; sgm_launch: the SGM arguments and path-sum buffers (returns their count); download:
+    // outputs to device pointers, or to the pinned staging that finish_download copies out.
+    int upload(const uint8_t* left, const uint8_t* right, int w, int h, int stride, int ch, bool device,
+               cudaStream_t s);
+    int enqueue_pre();
+    int sgm_launch(SgmLaunch* out, uint32_t** sbufs) const;
+    int enqueue_post();
+    int enqueue_sgm() { return run_sgm(); }
+    int download(float* disp, float* conf, uint8_t* reason, uint8_t* reliable, bool device, cudaStream_t s);
+    void finish_download(float* disp, float* conf, uint8_t* reason, uint8_t* reliable) const;
+    bool refine_enabled() const { return cfg_.refine_enable && cfg_.refine_iterations > 0; }
     // Frame counters of the last pair: valid, reliable, lr_fail, refine_changed, sum of range
     // widths, prior support count.  Waits for the engine stream.
     int frame_counts(unsigned long long* out6);
@@ -98,6 +111,7 @@ private:
     int run_prior();
     int run_refine(float* work);
     int fail(int code, const std::string& m) { err_ = m; return code; }
+    int ensure_pinned(size_t need);
     int cuda_fail(cudaError_t e, const char* where);
     template <typename T> T* ptr(size_t off) const { return reinterpret_cast<T*>(arena_ + off); }
     CostCtx cost_ctx() const;

@@ -5,6 +5,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include <vector>
+
 #include "common.cuh"
 
 namespace apgcu {
@@ -54,6 +56,25 @@ cudaError_t launch_sgm_last(const SgmLaunch& l, int dx, int dy, int nin, const u
 // bufs[0] += bufs[1..6] (saturating u16 lanes), `words` 32-bit words each.
 cudaError_t launch_sgm_sum7(uint32_t* const* bufs, size_t words, cudaStream_t s);
 int sgm_lanes_for(int Dp, int requested);
+
+// Batches: the SGM of many pairs with the same Dp (64, 128, 192 or 256), volume-fed, in two
+// persistent launches (every pair's first-phase directions, then every pair's last sweep + WTA).
+struct SgmBatchPlan {
+    int npairs = 0, nsbuf = 0, Dp = 0, lanes = 32;
+    int nseg_first = 0, total_first = 0, nseg_last = 0, total_last = 0;
+    size_t words = 0;  // 32-bit words of one pair's path-sum buffer
+    void* dev = nullptr;
+    size_t off_first = 0, off_last = 0, off_queue = 0;
+    std::vector<uint32_t*> sums;  // npairs x nsbuf path-sum buffers
+};
+bool sgm_batch_supported(int Dp);
+// pl[i]: pair i's launch arguments; sbufs[i*nsbuf + d]: its path-sum buffers (nsbuf 3 or 7);
+// lanes: 16 or 32 lanes per chain.  Uploads the work tables (synchronous).
+cudaError_t sgm_batch_plan_create(const SgmLaunch* pl, uint32_t* const* sbufs, int npairs, int nsbuf, int lanes,
+                                  SgmBatchPlan* plan);
+void sgm_batch_plan_destroy(SgmBatchPlan* plan);
+// max_blocks_per_sm caps the persistent grid (0 = as many as fit).
+cudaError_t launch_sgm_batch(const SgmBatchPlan& plan, int max_blocks_per_sm, cudaStream_t s);
 
 // post.cu
 struct ConfLrArgs {

@@ -41,6 +41,8 @@
 #include "kernels.h"
 
 #include <algorithm>
+#include <cstring>
+#include <vector>
 
 namespace apgcu {
 
@@ -882,6 +884,115 @@ cudaError_t dispatch(const SgmArgs& a, const DirTable& tab, bool census, int T, 
 #undef APGCU_TK
 }
 
+// ---- batches: the chains of many pairs in one persistent launch
+//
+// A launch covers one phase (the first-phase directions, or the last sweep) of every pair of a
+// batch with the same Dp.  Its work queue is the list of warp units: a unit is 32/T consecutive
+// scanlines of one (pair, direction) segment; segments are ordered longest chains first, so the
+// tail of the launch is short.  Warps take units from a global counter until the queue is empty.
+struct BatchPair {
+    SgmArgs a;
+    uint32_t* out[kMaxDirs];       // first phase: one path-sum buffer per direction
+    const uint32_t* in[kMaxDirs];  // last sweep: the partial sums to add
+};
+struct BatchSeg {
+    int begin;  // first unit of the segment
+    int pair, dir, dx, dy, nscan;
+};
+
+template <int T, int K, int MODE, int PF, int NB>
+__global__ void __launch_bounds__(128) sgm_batch_kernel(const BatchPair* __restrict__ pairs,
+                                                        const BatchSeg* __restrict__ segs, int nseg, int total,
+                                                        int* __restrict__ queue) {
+    extern __shared__ __align__(16) uint32_t s_dyn[];
+    constexpr int ring_words = PF * vol_slot_words<K, NB>();
+    constexpr int per_warp = ring_words + (MODE == kLast ? wta_buf_words<K, T>() : 0);
+    BatchSeg* s_seg = reinterpret_cast<BatchSeg*>(s_dyn + 4 * per_warp);
+    for (int i = threadIdx.x; i < nseg; i += blockDim.x) s_seg[i] = segs[i];
+    __syncthreads();
+    uint32_t* ring = s_dyn + (threadIdx.x >> 5) * per_warp;
+    const int lane = threadIdx.x & 31;
+    constexpr int C = 32 / T;
+    for (;;) {
+        int unit = 0;
+        if (lane == 0) unit = atomicAdd(queue, 1);
+        unit = __shfl_sync(0xffffffffu, unit, 0);
+        if (unit >= total) break;
+        int lo = 0, hi = nseg - 1;  // the last segment whose first unit is <= unit
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (s_seg[mid].begin <= unit) lo = mid;
+            else hi = mid - 1;
+        }
+        const BatchSeg sg = s_seg[lo];
+        const BatchPair* bp = pairs + sg.pair;
+        const int scan = (unit - sg.begin) * C + lane / T;
+        run_chain_vol<T, K, MODE, PF, NB>(bp->a, bp->in, ring, ring + ring_words, sg.dx, sg.dy, scan, sg.nscan,
+                                          MODE == kFirst ? bp->out[sg.dir] : nullptr);
+    }
+}
+
+template <int T, int K, int MODE, int NB>
+constexpr int batch_pf() {
+    return MODE == kFirst ? kVolPfFirst : last_pf<K, T, NB>();
+}
+
+template <int T, int K, int MODE, int NB>
+size_t batch_smem(int nseg) {
+    constexpr int PF = batch_pf<T, K, MODE, NB>();
+    constexpr int per_warp = PF * vol_slot_words<K, NB>() + (MODE == kLast ? wta_buf_words<K, T>() : 0);
+    return (size_t)4 * per_warp * 4 + (size_t)nseg * sizeof(BatchSeg);
+}
+
+template <int T, int K, int MODE, int NB>
+cudaError_t launch_batch_tk(const BatchPair* pairs, const BatchSeg* segs, int nseg, int total, int* queue,
+                            int max_blocks_per_sm, cudaStream_t st) {
+    constexpr int PF = batch_pf<T, K, MODE, NB>();
+    auto kern = sgm_batch_kernel<T, K, MODE, PF, NB>;
+    const size_t smem = batch_smem<T, K, MODE, NB>(nseg);
+    if (smem > 48 * 1024) {
+        const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    int dev = 0, nsm = 148, occ = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, 128, smem);
+    if (e != cudaSuccess) return e;
+    if (occ < 1) return cudaErrorInvalidConfiguration;
+    if (max_blocks_per_sm > 0 && occ > max_blocks_per_sm) occ = max_blocks_per_sm;
+    int blocks = nsm * occ;
+    const int need = (total + 3) / 4;
+    if (blocks > need) blocks = need;
+    if (blocks < 1) blocks = 1;
+    kern<<<blocks, 128, smem, st>>>(pairs, segs, nseg, total, queue);
+    return cudaGetLastError();
+}
+
+template <int MODE, int NB>
+cudaError_t launch_batch_dispatch(int T, int Dp, const BatchPair* pairs, const BatchSeg* segs, int nseg, int total,
+                                  int* queue, int max_blocks_per_sm, cudaStream_t st) {
+#define APGCU_BTK(TT, KK) \
+    return launch_batch_tk<TT, KK, MODE, NB>(pairs, segs, nseg, total, queue, max_blocks_per_sm, st)
+    if (T == 16) {
+        switch (Dp) {
+            case 64: APGCU_BTK(16, 2);
+            case 128: APGCU_BTK(16, 4);
+            case 192: APGCU_BTK(16, 6);
+            case 256: APGCU_BTK(16, 8);
+            default: return cudaErrorInvalidValue;
+        }
+    }
+    switch (Dp) {
+        case 64: APGCU_BTK(32, 1);
+        case 128: APGCU_BTK(32, 2);
+        case 192: APGCU_BTK(32, 3);
+        case 256: APGCU_BTK(32, 4);
+        default: return cudaErrorInvalidValue;
+    }
+#undef APGCU_BTK
+}
+
 SgmArgs make_args(const SgmLaunch& l) {
     SgmArgs a;
     a.w = l.w; a.h = l.h; a.d0 = l.d0; a.D = l.D; a.Dp = l.Dp; a.dmax = l.d0 + l.D;
@@ -941,4 +1052,123 @@ cudaError_t launch_sgm_sum7(uint32_t* const* bufs, size_t words, cudaStream_t st
     return cudaGetLastError();
 }
 
+// ---- batch plan (host)
+
+bool sgm_batch_supported(int Dp) { return Dp == 64 || Dp == 128 || Dp == 192 || Dp == 256; }
+
+cudaError_t sgm_batch_plan_create(const SgmLaunch* pl, uint32_t* const* sbufs, int npairs, int nsbuf, int lanes,
+                                  SgmBatchPlan* plan) {
+    *plan = SgmBatchPlan();
+    if (npairs < 1 || (nsbuf != 3 && nsbuf != 7)) return cudaErrorInvalidValue;
+    const int Dp = pl[0].Dp;
+    if (!sgm_batch_supported(Dp)) return cudaErrorInvalidValue;
+    for (int i = 0; i < npairs; ++i)
+        if (pl[i].Dp != Dp || !pl[i].cvol) return cudaErrorInvalidValue;
+    const int T = lanes == 16 ? 16 : 32;
+    const int C = 32 / T;
+    static const int first4[3][2] = {{1, 0}, {-1, 0}, {0, 1}};
+    static const int first8[7][2] = {{1, 0}, {-1, 0}, {0, 1}, {1, 1}, {1, -1}, {-1, 1}, {-1, -1}};
+    std::vector<BatchPair> pairs(npairs);
+    struct S { BatchSeg g; int len; };
+    std::vector<S> first, last;
+    for (int i = 0; i < npairs; ++i) {
+        BatchPair& bp = pairs[i];
+        std::memset(&bp, 0, sizeof(bp));
+        bp.a = make_args(pl[i]);
+        for (int d = 0; d < nsbuf; ++d) {
+            bp.out[d] = sbufs[i * nsbuf + d];
+            bp.in[d] = sbufs[i * nsbuf + d];
+        }
+        for (int d = 0; d < nsbuf; ++d) {
+            const int dx = nsbuf == 7 ? first8[d][0] : first4[d][0];
+            const int dy = nsbuf == 7 ? first8[d][1] : first4[d][1];
+            S sg;
+            sg.g.pair = i; sg.g.dir = d; sg.g.dx = dx; sg.g.dy = dy;
+            sg.g.nscan = nscan_of(bp.a, dx, dy);
+            sg.len = dy == 0 ? bp.a.w : (dx == 0 ? bp.a.h : std::min(bp.a.w, bp.a.h));
+            first.push_back(sg);
+        }
+        S sl;
+        sl.g.pair = i; sl.g.dir = 0; sl.g.dx = 0; sl.g.dy = -1;
+        sl.g.nscan = nscan_of(bp.a, 0, -1);
+        sl.len = bp.a.h;
+        last.push_back(sl);
+    }
+    // longest chains first; stable, so a pair's segments stay together among equals
+    auto order = [](const S& x, const S& y) { return x.len > y.len; };
+    std::stable_sort(first.begin(), first.end(), order);
+    std::stable_sort(last.begin(), last.end(), order);
+    auto units = [&](std::vector<S>& v, int* total) {
+        int u = 0;
+        for (auto& x : v) {
+            x.g.begin = u;
+            u += (x.g.nscan + C - 1) / C;
+        }
+        *total = u;
+    };
+    units(first, &plan->total_first);
+    units(last, &plan->total_last);
+    plan->nseg_first = (int)first.size();
+    plan->nseg_last = (int)last.size();
+    plan->npairs = npairs;
+    plan->nsbuf = nsbuf;
+    plan->Dp = Dp;
+    plan->lanes = T;
+    plan->words = (size_t)pl[0].w * pl[0].h * (Dp / 2);
+    // device tables: pairs | first segments | last segments | 2 queue counters
+    const size_t b_pairs = sizeof(BatchPair) * npairs;
+    const size_t b_first = sizeof(BatchSeg) * first.size();
+    const size_t b_last = sizeof(BatchSeg) * last.size();
+    plan->off_first = (b_pairs + 255) & ~size_t(255);
+    plan->off_last = (plan->off_first + b_first + 255) & ~size_t(255);
+    plan->off_queue = (plan->off_last + b_last + 255) & ~size_t(255);
+    const size_t total = plan->off_queue + 256;
+    std::vector<unsigned char> host(total, 0);
+    std::memcpy(host.data(), pairs.data(), b_pairs);
+    for (size_t i = 0; i < first.size(); ++i)
+        std::memcpy(host.data() + plan->off_first + i * sizeof(BatchSeg), &first[i].g, sizeof(BatchSeg));
+    for (size_t i = 0; i < last.size(); ++i)
+        std::memcpy(host.data() + plan->off_last + i * sizeof(BatchSeg), &last[i].g, sizeof(BatchSeg));
+    cudaError_t e = cudaMalloc(&plan->dev, total);
+    if (e != cudaSuccess) {
+        plan->dev = nullptr;
+        return e;
+    }
+    e = cudaMemcpy(plan->dev, host.data(), total, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) sgm_batch_plan_destroy(plan);
+    // the sum buffers of every pair, for the Path8 fold
+    plan->sums.assign(sbufs, sbufs + (size_t)npairs * nsbuf);
+    return e;
+}
+
+void sgm_batch_plan_destroy(SgmBatchPlan* plan) {
+    if (plan->dev) cudaFree(plan->dev);
+    *plan = SgmBatchPlan();
+}
+
+cudaError_t launch_sgm_batch(const SgmBatchPlan& plan, int max_blocks_per_sm, cudaStream_t st) {
+    unsigned char* base = static_cast<unsigned char*>(plan.dev);
+    const BatchPair* pairs = reinterpret_cast<const BatchPair*>(base);
+    int* queue = reinterpret_cast<int*>(base + plan.off_queue);
+    cudaError_t e = cudaMemsetAsync(queue, 0, 2 * sizeof(int), st);
+    if (e != cudaSuccess) return e;
+    e = launch_batch_dispatch<kFirst, 0>(plan.lanes, plan.Dp, pairs,
+                                         reinterpret_cast<const BatchSeg*>(base + plan.off_first), plan.nseg_first,
+                                         plan.total_first, queue, max_blocks_per_sm, st);
+    if (e != cudaSuccess) return e;
+    if (plan.nsbuf == 7) {
+        for (int i = 0; i < plan.npairs; ++i) {
+            e = launch_sgm_sum7(plan.sums.data() + (size_t)i * 7, plan.words, st);
+            if (e != cudaSuccess) return e;
+        }
+        return launch_batch_dispatch<kLast, 1>(plan.lanes, plan.Dp, pairs,
+                                               reinterpret_cast<const BatchSeg*>(base + plan.off_last), plan.nseg_last,
+                                               plan.total_last, queue + 1, max_blocks_per_sm, st);
+    }
+    return launch_batch_dispatch<kLast, 3>(plan.lanes, plan.Dp, pairs,
+                                           reinterpret_cast<const BatchSeg*>(base + plan.off_last), plan.nseg_last,
+                                           plan.total_last, queue + 1, max_blocks_per_sm, st);
+}
+
 }  // namespace apgcu
+

@@ -119,6 +119,40 @@ APGCU_API size_t apgcu_session_estimate_bytes(apg_session_t s, int width, int he
 /* Number of kernels the library has launched in this process (all engines). */
 APGCU_API unsigned long long apgcu_kernel_launch_count(void);
 
+/* ---- Batched form: many pairs of uneven sizes per call.
+ *
+ * No counterpart in the reference (which processes one pair per call): pairs are grouped into
+ * buckets of equal size and disparity range; each bucket's pairs run their per-pixel stages on
+ * their own streams and share one persistent SGM launch per phase (a work queue of (pair,
+ * direction, scanline) units); the per-bucket sequence is a cached CUDA graph; lanes per scanline
+ * and the persistent-grid cap are autotuned per bucket.  Every pair's outputs equal what
+ * apgcu_engine_process gives for it alone. */
+typedef struct apgcu_batch_s* apgcu_batch_t;
+typedef struct {
+    const uint8_t* left;        /* host or device memory, as the call's device_buffers says */
+    const uint8_t* right;
+    int width, height, stride, channels;
+    int max_disparity;          /* this pair's range end (0: the batch configuration's) */
+    float* disparity;           /* outputs, W*H each; any may be NULL */
+    float* confidence;
+    uint8_t* invalid_reason;
+    uint8_t* reliable_mask;
+} apgcu_pair_t;
+
+/* Batch over a configuration record (its max_disparity is the default range end). NULL if the
+ * configuration is invalid. */
+APGCU_API apgcu_batch_t apgcu_batch_create(const apg_pipeline_config_t* cfg, int device);
+APGCU_API void apgcu_batch_destroy(apgcu_batch_t b);
+APGCU_API const char* apgcu_batch_last_error(apgcu_batch_t b);
+/* Processes npairs pairs and returns when every output is written.  device_buffers != 0: inputs
+ * and outputs are device pointers on the batch's device. */
+APGCU_API int apgcu_batch_process(apgcu_batch_t b, int npairs, const apgcu_pair_t* pairs, int device_buffers);
+/* Options (results never change): "graphs" 0/1, "batched_sgm" 0/1, "autotune" 0/1,
+ * "sgm_lanes" 0/16/32 (0 = autotuned), "max_blocks_per_sm" -1 (autotuned) / 0 (occupancy) / N. */
+APGCU_API int apgcu_batch_set_option(apgcu_batch_t b, const char* key, int value);
+APGCU_API size_t apgcu_batch_allocated_bytes(apgcu_batch_t b);
+APGCU_API void apgcu_batch_release(apgcu_batch_t b);
+
 /* Right-image winner-take-all over a caller's cost volume, allocating nothing.
  *
  * No counterpart in the reference: it exposes as one call the right-image WTA that the reference
