@@ -563,6 +563,11 @@ class Batch:
     def allocated_bytes(self) -> int:
         return int(lib().apgcu_batch_allocated_bytes(self._h))
 
+    @property
+    def last_time_ms(self) -> float:
+        """Device time of the last call (start event to the latest bucket end)."""
+        return float(lib().apgcu_batch_last_time_ms(self._h))
+
     def release(self):
         lib().apgcu_batch_release(self._h)
 

@@ -117,6 +117,7 @@ _SIGS = {
     "apgcu_batch_process": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(Pair), C.c_int]),
     "apgcu_batch_set_option": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int]),
     "apgcu_batch_allocated_bytes": (C.c_size_t, [C.c_void_p]),
+    "apgcu_batch_last_time_ms": (C.c_float, [C.c_void_p]),
     "apgcu_batch_release": (None, [C.c_void_p]),
     "apgcu_right_wta_noalloc": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                           C.c_void_p, C.c_void_p]),

@@ -62,6 +62,8 @@ struct Bucket {
     std::vector<cudaEvent_t> joined;
     std::map<int, SgmBatchPlan> plans;        // by pair count (graphs hold their device tables)
     std::map<int, cudaGraphExec_t> graphs;    // by pair count
+    std::map<int, unsigned long long> graph_launches;  // kernels per replay
+    cudaEvent_t done = nullptr;               // end of the bucket's last call (timing)
     Tuning tune;
     bool tuned = false;
 };
@@ -114,6 +116,7 @@ public:
     int process(int n, const apgcu_pair_t* pairs, bool device_buffers);
     int set_option(const char* key, int value);
     size_t allocated_bytes() const;
+    float last_time_ms() const { return last_ms_; }
     void release();
     const std::string& last_error() const { return err_; }
 
@@ -134,9 +137,13 @@ private:
     bool use_graphs_ = true;
     bool use_batched_sgm_ = true;
     bool autotune_ = true;
+    bool graph_capture_ = false;  // inside a capture: launches are counted at replay
     int forced_lanes_ = 0;
     int forced_max_blocks_ = -1;
     std::map<BucketKey, std::unique_ptr<Bucket>> buckets_;
+    cudaStream_t start_stream_ = nullptr;
+    cudaEvent_t start_ = nullptr;
+    float last_ms_ = 0.f;
     std::string err_;
 };
 
@@ -156,7 +163,8 @@ int Batch::ensure_slots(Bucket& b, int m) {
     if (!b.stream) {
         if (cudaStreamCreateWithFlags(&b.stream, cudaStreamNonBlocking) != cudaSuccess ||
             cudaEventCreateWithFlags(&b.fork, cudaEventDisableTiming) != cudaSuccess ||
-            cudaEventCreateWithFlags(&b.sgm_done, cudaEventDisableTiming) != cudaSuccess) {
+            cudaEventCreateWithFlags(&b.sgm_done, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreate(&b.done) != cudaSuccess) {
             cudaGetLastError();
             return fail(kInternalError, "batch stream creation failed");
         }
@@ -225,6 +233,7 @@ int Batch::enqueue(Bucket& b, int m, bool batched_sgm) {
     }
     if (!batched_sgm) return kOk;
     cudaError_t ce = launch_sgm_batch(b.plans.at(m), b.tune.max_blocks_per_sm, b.stream);
+    if (!graph_capture_) count_launches(2);
     if (ce != cudaSuccess) return fail(kInternalError, std::string("batched SGM: ") + cudaGetErrorString(ce));
     cudaEventRecord(b.sgm_done, b.stream);
     for (int k = 0; k < m; ++k) {
@@ -249,8 +258,12 @@ int Batch::run_bucket(Bucket& b, int m, bool batched_sgm) {
             cudaGetLastError();
             return enqueue(b, m, batched_sgm);
         }
+        graph_capture_ = true;
+        const unsigned long long before = launch_count();
         const int rc = enqueue(b, m, batched_sgm);
+        const unsigned long long captured = launch_count() - before;
         const cudaError_t ce = cudaStreamEndCapture(b.stream, &g);
+        graph_capture_ = false;
         if (rc != kOk || ce != cudaSuccess) {
             cudaGetLastError();
             if (g) cudaGraphDestroy(g);
@@ -265,6 +278,10 @@ int Batch::run_bucket(Bucket& b, int m, bool batched_sgm) {
             return fail(kInternalError, std::string("batch graph instantiate: ") + cudaGetErrorString(ie));
         }
         it = b.graphs.emplace(m, ex).first;
+        b.graph_launches[m] = captured + (batched_sgm ? 2 : 0);
+        count_launches(0);
+    } else {
+        count_launches((unsigned)b.graph_launches[m]);
     }
     const cudaError_t le = cudaGraphLaunch(it->second, b.stream);
     if (le != cudaSuccess) return fail(kInternalError, std::string("batch graph launch: ") + cudaGetErrorString(le));
@@ -320,8 +337,14 @@ int Batch::autotune(Bucket& b, const apgcu_pair_t& sample, bool device_buffers) 
         cudaEventRecord(t1, b.stream);
         cudaEventSynchronize(t1);
         float total = 0.f;
-        cudaEventElapsedTime(&total, t0, t1);
+        if (cudaEventElapsedTime(&total, t0, t1) != cudaSuccess) {
+            cudaGetLastError();
+            total = 1e30f;
+        }
         if (rc) break;
+        if (std::getenv("APGCU_TUNE_LOG"))
+            std::fprintf(stderr, "apgcu tune %s lanes %d max_blocks %d: %.3f ms (2 runs, rc %d)\n", key.c_str(),
+                         t.sgm_lanes, t.max_blocks_per_sm, total, rc);
         if (total < best_ms) {
             best_ms = total;
             best = t;
@@ -361,25 +384,37 @@ int Batch::process(int n, const apgcu_pair_t* pairs, bool device_buffers) {
         if (rc) return fail(rc, "pair " + std::to_string(i) + ": " + msg);
         groups[BucketKey{p.width, p.height, p.channels, c.max_disparity}].push_back(i);
     }
-    // per bucket: tune (first time), upload, run (graph), download
+    // per bucket: tune (first time), upload, run (graph), download; every bucket stream starts
+    // after one start event, so the call's device time is the latest bucket end minus it
+    if (!start_stream_) {
+        if (cudaStreamCreateWithFlags(&start_stream_, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreate(&start_) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(kInternalError, "batch timing stream creation failed");
+        }
+    }
+    for (auto& g : groups) {
+        Bucket& b = bucket_for(g.first);
+        if (b.tuned) continue;
+        if (autotune_ && use_batched_sgm_) {
+            const int rc = autotune(b, pairs[g.second[0]], device_buffers);
+            if (rc) return rc;
+        }
+        b.tuned = true;
+        if (forced_lanes_) b.tune.sgm_lanes = forced_lanes_;
+        if (forced_max_blocks_ >= 0) b.tune.max_blocks_per_sm = forced_max_blocks_;
+        for (auto& sl : b.slots) sl->set_sgm_lanes(b.tune.sgm_lanes);
+        drop_plans(b);
+    }
+    cudaEventRecord(start_, start_stream_);
     std::vector<std::pair<Bucket*, const std::vector<int>*>> order;
     for (auto& g : groups) {
         Bucket& b = bucket_for(g.first);
         const std::vector<int>& idx = g.second;
         const int m = (int)idx.size();
-        if (!b.tuned) {
-            if (autotune_ && use_batched_sgm_) {
-                const int rc = autotune(b, pairs[idx[0]], device_buffers);
-                if (rc) return rc;
-            } else {
-                b.tuned = true;
-            }
-            if (forced_lanes_) b.tune.sgm_lanes = forced_lanes_;
-            if (forced_max_blocks_ >= 0) b.tune.max_blocks_per_sm = forced_max_blocks_;
-            for (auto& s : b.slots) s->set_sgm_lanes(b.tune.sgm_lanes);
-        }
         int rc = ensure_slots(b, m);
         if (rc) return rc;
+        cudaStreamWaitEvent(b.stream, start_, 0);
         for (int k = 0; k < m; ++k) {
             const apgcu_pair_t& p = pairs[idx[k]];
             rc = b.slots[k]->upload(p.left, p.right, p.width, p.height, p.stride, p.channels, device_buffers, b.stream);
@@ -402,11 +437,18 @@ int Batch::process(int n, const apgcu_pair_t* pairs, bool device_buffers) {
                                       b.stream);
             if (rc) return fail(rc, b.slots[k]->last_error());
         }
+        cudaEventRecord(b.done, b.stream);
         order.emplace_back(&b, &idx);
     }
     for (auto& o : order) {
         const cudaError_t e = cudaStreamSynchronize(o.first->stream);
         if (e != cudaSuccess) return fail(kInternalError, std::string("batch: ") + cudaGetErrorString(e));
+    }
+    last_ms_ = 0.f;
+    for (auto& o : order) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, start_, o.first->done) == cudaSuccess) last_ms_ = std::max(last_ms_, ms);
+        else cudaGetLastError();
     }
     if (!device_buffers) {
         for (auto& o : order) {
@@ -458,9 +500,14 @@ void Batch::release() {
         for (auto ev : b.joined) cudaEventDestroy(ev);
         if (b.fork) cudaEventDestroy(b.fork);
         if (b.sgm_done) cudaEventDestroy(b.sgm_done);
+        if (b.done) cudaEventDestroy(b.done);
         if (b.stream) cudaStreamDestroy(b.stream);
     }
     buckets_.clear();
+    if (start_) cudaEventDestroy(start_);
+    if (start_stream_) cudaStreamDestroy(start_stream_);
+    start_ = nullptr;
+    start_stream_ = nullptr;
 }
 
 }  // namespace apgcu
@@ -509,6 +556,8 @@ APGCU_API int apgcu_batch_set_option(apgcu_batch_t b, const char* key, int value
 }
 
 APGCU_API size_t apgcu_batch_allocated_bytes(apgcu_batch_t b) { return b ? b->b->allocated_bytes() : 0; }
+
+APGCU_API float apgcu_batch_last_time_ms(apgcu_batch_t b) { return b ? b->b->last_time_ms() : 0.f; }
 
 APGCU_API void apgcu_batch_release(apgcu_batch_t b) {
     if (b) b->b->release();

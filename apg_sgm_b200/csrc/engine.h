@@ -153,6 +153,7 @@ private:
 
 // Process-wide launch counter (reported by bench.py as gpu_launches).
 void count_launches(unsigned n);
+unsigned long long launch_count();
 
 // prior.cu / refine.cu
 cudaError_t launch_prior(const apg_pipeline_config_t& cfg, const CostCtx& c, const Layout& L, unsigned char* arena,

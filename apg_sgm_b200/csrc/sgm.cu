@@ -926,9 +926,15 @@ __global__ void __launch_bounds__(128) sgm_batch_kernel(const BatchPair* __restr
         }
         const BatchSeg sg = s_seg[lo];
         const BatchPair* bp = pairs + sg.pair;
+        // private copies: the chain stores through pointers, and arguments read through a global
+        // reference would have to be reloaded after every store
+        const SgmArgs a = bp->a;
+        const uint32_t* in[NB > 0 ? NB : 1];
+#pragma unroll
+        for (int b = 0; b < NB; ++b) in[b] = bp->in[b];
+        uint32_t* out = MODE == kFirst ? bp->out[sg.dir] : nullptr;
         const int scan = (unit - sg.begin) * C + lane / T;
-        run_chain_vol<T, K, MODE, PF, NB>(bp->a, bp->in, ring, ring + ring_words, sg.dx, sg.dy, scan, sg.nscan,
-                                          MODE == kFirst ? bp->out[sg.dir] : nullptr);
+        run_chain_vol<T, K, MODE, PF, NB>(a, in, ring, ring + ring_words, sg.dx, sg.dy, scan, sg.nscan, out);
     }
 }
 

@@ -179,6 +179,40 @@ def run_reference(args, wl):
     }))
 
 
+def run_reference_batched(args):
+    """The reference's Packed CPU path over the 64-pair batch, pair after pair; a step is one
+    bounded sample: one pair of each size, scaled by the batch's pair counts."""
+    from oracle import oracle as O
+    from apg_sgm_b200 import synthetic as S
+    specs = S.batched_mix()
+    if not O.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libapg_ref.so not built"}))
+        return
+    vox = sum(sp.width * sp.height * sp.max_disparity for sp in specs)
+    sample = {i: S.make_pair(specs[i], S.SEED_BASE + i)[:2] for i in (0, 24, 48)}
+    sess = {i: O.RefSession(O.config(1, specs[i].max_disparity, volume_backend=2)) for i in sample}
+    weight = {0: 24, 24: 24, 48: 16}
+    for _ in range(args.warmup):
+        for i in sample:
+            sess[i].process(*sample[i])
+    total = 0.0
+    for _ in range(args.steps):
+        for i in sample:
+            t0 = time.perf_counter()
+            sess[i].process(*sample[i])
+            total += (time.perf_counter() - t0) * weight[i]
+    value = vox * args.steps / total
+    print(json.dumps({
+        "impl": "reference", "metric": "W*H*D/s, 64-pair uneven batch (Balanced, bit-exact)", "value": value,
+        "unit": "voxels/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000 * total / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u16", "data": "synthetic", "config": {"workload": "batched_balanced_64_uneven", "pairs": 64},
+        "cpu_baseline": {"value": value, "unit": "voxels/s", "cores": O.ref_threads(), "kind": "reference",
+                         "sample": "per step one pair of each size, scaled by the pair counts"},
+        "e2e": {"value": value, "unit": "voxels/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
 def cpu_baseline(spec, mode, L, R, gpu_out):
     """Time the reference (Packed, all host cores) on pair 0 and check the GPU output against it."""
     from oracle import oracle as O
@@ -389,15 +423,186 @@ def run_b200(args, wl):
         dist.destroy_process_group()
 
 
+def run_batched(args):
+    """The 64-pair uneven Balanced batch (24x 640x480 D64, 24x 1242x375 D192, 16x 1280x720 D128)
+    through the batched form, against the same 64 pairs as sequential plain launches on one
+    stream.  A step is the whole batch; inputs resident in HBM, L2 flushed between steps."""
+    import ctypes as C
+    import torch
+    import apg_sgm_b200 as apg
+    from apg_sgm_b200 import _lib, synthetic as S
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    specs = S.batched_mix()
+    host = [S.make_pair(sp, S.SEED_BASE + rank * len(specs) + i)[:2] for i, sp in enumerate(specs)]
+    vox = sum(sp.width * sp.height * sp.max_disparity for sp in specs)
+    npairs = len(specs)
+    d_in = [(torch.from_numpy(l).to(dev), torch.from_numpy(r).to(dev)) for l, r in host]
+
+    def outs():
+        return [{"disparity": torch.empty((sp.height, sp.width), dtype=torch.float32, device=dev),
+                 "confidence": torch.empty((sp.height, sp.width), dtype=torch.float32, device=dev),
+                 "invalid_reason": torch.empty((sp.height, sp.width), dtype=torch.uint8, device=dev),
+                 "reliable_mask": torch.empty((sp.height, sp.width), dtype=torch.uint8, device=dev)}
+                for sp in specs]
+
+    o_plain, o_batch = outs(), outs()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    cfg = apg.config_from_mode(1, 128)
+    # plain: one engine per size, all on one stream, the pairs one after another
+    stream = torch.cuda.Stream(device=dev)
+    engines = {}
+    for sp in specs:
+        if sp.max_disparity not in engines:
+            engines[sp.max_disparity] = apg.Engine(apg.config_from_mode(1, sp.max_disparity), device=local,
+                                                   stream=stream.cuda_stream)
+
+    def plain_step():
+        for sp, (l, r), o in zip(specs, d_in, o_plain):
+            engines[sp.max_disparity].process_device(l.data_ptr(), r.data_ptr(), sp.width, sp.height, sp.width, 1,
+                                                     o["disparity"].data_ptr(), o["confidence"].data_ptr(),
+                                                     o["invalid_reason"].data_ptr(), o["reliable_mask"].data_ptr())
+
+    batch = apg.Batch(cfg, device=local)
+    recs = [_lib.Pair(l.data_ptr(), r.data_ptr(), sp.width, sp.height, sp.width, 1, sp.max_disparity,
+                      o["disparity"].data_ptr(), o["confidence"].data_ptr(), o["invalid_reason"].data_ptr(),
+                      o["reliable_mask"].data_ptr()) for sp, (l, r), o in zip(specs, d_in, o_batch)]
+
+    # warm-up (the batched form tunes and captures its graphs here)
+    for _ in range(max(args.warmup, 3)):
+        with torch.cuda.stream(stream):
+            plain_step()
+        stream.synchronize()
+        batch.process_device(recs)
+    torch.cuda.synchronize()
+    identical = all(torch.equal(a[k].view(torch.uint8), b[k].view(torch.uint8))
+                    for a, b in zip(o_plain, o_batch) for k in a)
+
+    # plain, timed on its stream
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    for k in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            ev[k][0].record(stream)
+            plain_step()
+            ev[k][1].record(stream)
+    torch.cuda.synchronize()
+    plain_ms = sum(a.elapsed_time(b) for a, b in ev)
+
+    # batched: device time of every call (start event to the latest bucket end)
+    sampler = ClockSampler(local)
+    sampler.start()
+    sampler.wait_first()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = apg.kernel_launch_count()
+    batch_ms = 0.0
+    for k in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        batch.process_device(recs)
+        batch_ms += batch.last_time_ms
+    torch.cuda.synchronize()
+    launches = apg.kernel_launch_count() - launches0
+    clocks = sampler.stop()
+    t = torch.tensor([batch_ms, plain_ms], dtype=torch.float64, device=dev)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    batch_ms, plain_ms = float(t[0]), float(t[1])
+    value = vox * args.steps * world / (batch_ms / 1000.0)
+    plain_value = vox * args.steps * world / (plain_ms / 1000.0)
+
+    # end to end: host images in, host maps out, through apgcu_batch_process
+    e2e_steps = max(3, min(args.steps, 20))
+    for _ in range(2):
+        batch.process([(l, r, sp.max_disparity) for sp, (l, r) in zip(specs, host)])
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        batch.process([(l, r, sp.max_disparity) for sp, (l, r) in zip(specs, host)])
+    e2e_s = time.perf_counter() - t0
+    e2e_value = vox * e2e_steps * world / e2e_s
+    h2d = sum(2 * sp.width * sp.height for sp in specs)
+    d2h = sum(10 * sp.width * sp.height for sp in specs)
+
+    peak, peak_kind = _peaks()
+    # the whole pipeline against the stage-boundary byte model (36 B per voxel for Balanced)
+    achieved = 36.0 * vox / (batch_ms / args.steps / 1000.0) / 1e9
+    out = {
+        "metric": "W*H*D/s, 64-pair uneven batch (Balanced, bit-exact)", "value": value, "unit": "voxels/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": batch_ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": "synthetic",
+        "config": {"workload": "batched_balanced_64_uneven", "pairs": npairs,
+                   "sizes": "24x 640x480 D64, 24x 1242x375 D192, 16x 1280x720 D128", "voxels_per_step": vox,
+                   "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}"},
+        "pairs_per_s": npairs * args.steps * world / (batch_ms / 1000.0),
+        "plain": {"value": plain_value, "ms_per_step": plain_ms / args.steps,
+                  "pairs_per_s": npairs * args.steps * world / (plain_ms / 1000.0),
+                  "how": "the 64 pairs as sequential single-pair launches on one stream"},
+        "speedup_vs_plain": plain_ms / batch_ms,
+        "identical_to_plain": bool(identical),
+        "e2e": {"value": e2e_value, "unit": "voxels/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "api": "apgcu_batch_process (host buffers)"},
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "kernel": "pipeline (36 B/voxel stage-boundary model)", "achieved": achieved,
+                     "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None},
+        "clocks": clocks,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import oracle as O
+        if O.ref_available():
+            # the reference on one pair of each size, scaled to the batch by pair counts
+            tot = 0.0
+            for i in (0, 24, 48):
+                sp = specs[i]
+                sess = O.RefSession(O.config(1, sp.max_disparity, volume_backend=2))
+                sess.process(*host[i])
+                t0 = time.perf_counter()
+                sess.process(*host[i])
+                tot += (time.perf_counter() - t0) * {0: 24, 24: 24, 48: 16}[i]
+            out["cpu_baseline"] = {"value": vox / tot, "unit": "voxels/s", "cores": O.ref_threads(),
+                                   "kind": "reference",
+                                   "sample": "one pair of each size through the reference Packed backend, "
+                                             "scaled by the batch's pair counts"}
+    if rank == 0:
+        print(json.dumps(out))
+    batch.close()
+    for e in engines.values():
+        e.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="fast720")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batched"], default="fast720")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
+    if args.workload == "batched":
+        if args.impl == "reference":
+            if int(os.environ.get("RANK", "0")) == 0:
+                run_reference_batched(args)
+            return
+        run_batched(args)
+        return
     wl = WORKLOADS[args.workload]
     if args.impl == "reference":
         if int(os.environ.get("RANK", "0")) == 0:

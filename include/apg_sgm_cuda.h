@@ -151,6 +151,9 @@ APGCU_API int apgcu_batch_process(apgcu_batch_t b, int npairs, const apgcu_pair_
  * "sgm_lanes" 0/16/32 (0 = autotuned), "max_blocks_per_sm" -1 (autotuned) / 0 (occupancy) / N. */
 APGCU_API int apgcu_batch_set_option(apgcu_batch_t b, const char* key, int value);
 APGCU_API size_t apgcu_batch_allocated_bytes(apgcu_batch_t b);
+/* Device time of the last apgcu_batch_process (ms): from one start event every bucket waits on to
+ * the latest bucket end, copies included. */
+APGCU_API float apgcu_batch_last_time_ms(apgcu_batch_t b);
 APGCU_API void apgcu_batch_release(apgcu_batch_t b);
 
 /* Right-image winner-take-all over a caller's cost volume, allocating nothing.
