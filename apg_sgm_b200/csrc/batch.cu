@@ -13,7 +13,7 @@
 // replayed; inputs are copied into the slots' fixed input buffers before the replay and the
 // outputs copied out after it.  Buckets run on their own streams, concurrently.
 //
-// Tuning (tile shape of the cost kernel, lanes per SGM scanline, persistent-grid cap) is chosen
+// Tuning (tile width of the cost kernel, lanes per SGM scanline, persistent-grid cap) is chosen
 // per (W, D) bucket by an autotuner that times the candidates on the bucket's first pair and
 // caches the winner (in memory, and in a text file when APGCU_TUNE_CACHE names one).
 //
@@ -49,8 +49,9 @@ struct BucketKey {
 };
 
 struct Tuning {
-    int sgm_lanes = 32;      // lanes per scanline chain (32 = one warp per scanline, 16 = half a warp)
+    int sgm_lanes = 32;         // lanes per scanline chain (32 = one warp per scanline, 16 = half a warp)
     int max_blocks_per_sm = 0;  // cap of the persistent SGM grid (0 = occupancy limit)
+    int cost_tile = 0;          // columns per block of the cost kernel (0 = the default for Dp)
 };
 
 struct Bucket {
@@ -90,7 +91,7 @@ void tune_load_locked() {
         std::istringstream in(line);
         int mode, w, h, D;
         Tuning t;
-        if (in >> mode >> w >> h >> D >> t.sgm_lanes >> t.max_blocks_per_sm) {
+        if (in >> mode >> w >> h >> D >> t.sgm_lanes >> t.max_blocks_per_sm >> t.cost_tile) {
             std::ostringstream k;
             k << mode << " " << w << " " << h << " " << D;
             g_tune[k.str()] = t;
@@ -103,7 +104,7 @@ void tune_store_locked(const std::string& key, const Tuning& t) {
     const char* path = std::getenv("APGCU_TUNE_CACHE");
     if (!path) return;
     std::ofstream f(path, std::ios::app);
-    f << key << " " << t.sgm_lanes << " " << t.max_blocks_per_sm << "\n";
+    f << key << " " << t.sgm_lanes << " " << t.max_blocks_per_sm << " " << t.cost_tile << "\n";
 }
 
 }  // namespace
@@ -140,6 +141,7 @@ private:
     bool graph_capture_ = false;  // inside a capture: launches are counted at replay
     int forced_lanes_ = 0;
     int forced_max_blocks_ = -1;
+    int forced_tile_ = -1;
     std::map<BucketKey, std::unique_ptr<Bucket>> buckets_;
     cudaStream_t start_stream_ = nullptr;
     cudaEvent_t start_ = nullptr;
@@ -177,6 +179,7 @@ int Batch::ensure_slots(Bucket& b, int m) {
             return fail(kAllocationFailure, "engine creation failed");
         }
         e->set_sgm_lanes(b.tune.sgm_lanes);
+        e->set_cost_tile(b.tune.cost_tile);
         b.slots.push_back(std::move(e));
         cudaEvent_t ev;
         if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
@@ -304,14 +307,17 @@ int Batch::autotune(Bucket& b, const apgcu_pair_t& sample, bool device_buffers) 
     }
     const int Dp = round_up(b.key.dmax - b.cfg.min_disparity, 64);
     std::vector<Tuning> cand;
-    for (int lanes : {32, 16})
-        for (int mb : {0, 2}) {
-            if (lanes == 16 && Dp > 256) continue;
-            Tuning t;
-            t.sgm_lanes = lanes;
-            t.max_blocks_per_sm = mb;
-            cand.push_back(t);
-        }
+    const int alt_tile = Dp <= 128 ? 256 : 128;
+    for (int tile : {0, alt_tile})
+        for (int lanes : {32, 16})
+            for (int mb : {0, 2}) {
+                if (lanes == 16 && Dp > 256) continue;
+                Tuning t;
+                t.sgm_lanes = lanes;
+                t.max_blocks_per_sm = mb;
+                t.cost_tile = tile;
+                cand.push_back(t);
+            }
     int rc = ensure_slots(b, 1);
     if (rc) return rc;
     Engine& e = *b.slots[0];
@@ -326,6 +332,7 @@ int Batch::autotune(Bucket& b, const apgcu_pair_t& sample, bool device_buffers) 
     for (const Tuning& t : cand) {
         b.tune = t;
         e.set_sgm_lanes(t.sgm_lanes);
+        e.set_cost_tile(t.cost_tile);
         drop_plans(b);
         rc = ensure_plan(b, 1);
         if (rc) break;
@@ -343,8 +350,8 @@ int Batch::autotune(Bucket& b, const apgcu_pair_t& sample, bool device_buffers) 
         }
         if (rc) break;
         if (std::getenv("APGCU_TUNE_LOG"))
-            std::fprintf(stderr, "apgcu tune %s lanes %d max_blocks %d: %.3f ms (2 runs, rc %d)\n", key.c_str(),
-                         t.sgm_lanes, t.max_blocks_per_sm, total, rc);
+            std::fprintf(stderr, "apgcu tune %s lanes %d max_blocks %d cost_tile %d: %.3f ms (2 runs, rc %d)\n",
+                         key.c_str(), t.sgm_lanes, t.max_blocks_per_sm, t.cost_tile, total, rc);
         if (total < best_ms) {
             best_ms = total;
             best = t;
@@ -356,7 +363,10 @@ int Batch::autotune(Bucket& b, const apgcu_pair_t& sample, bool device_buffers) 
     if (rc) return rc;
     b.tune = best;
     b.tuned = true;
-    for (auto& s : b.slots) s->set_sgm_lanes(best.sgm_lanes);
+    for (auto& s : b.slots) {
+        s->set_sgm_lanes(best.sgm_lanes);
+        s->set_cost_tile(best.cost_tile);
+    }
     drop_plans(b);
     std::lock_guard<std::mutex> lk(g_tune_mu);
     tune_store_locked(key, best);
@@ -403,7 +413,11 @@ int Batch::process(int n, const apgcu_pair_t* pairs, bool device_buffers) {
         b.tuned = true;
         if (forced_lanes_) b.tune.sgm_lanes = forced_lanes_;
         if (forced_max_blocks_ >= 0) b.tune.max_blocks_per_sm = forced_max_blocks_;
-        for (auto& sl : b.slots) sl->set_sgm_lanes(b.tune.sgm_lanes);
+        if (forced_tile_ >= 0) b.tune.cost_tile = forced_tile_;
+        for (auto& sl : b.slots) {
+            sl->set_sgm_lanes(b.tune.sgm_lanes);
+            sl->set_cost_tile(b.tune.cost_tile);
+        }
         drop_plans(b);
     }
     cudaEventRecord(start_, start_stream_);
@@ -470,6 +484,9 @@ int Batch::set_option(const char* key, int value) {
     else if (k == "sgm_lanes") {
         if (value != 0 && value != 16 && value != 32) return kInvalidConfig;
         forced_lanes_ = value;
+    } else if (k == "cost_tile") {
+        if (value != 0 && value != 64 && value != 128 && value != 256) return kInvalidConfig;
+        forced_tile_ = value;
     } else if (k == "max_blocks_per_sm") {
         if (value < -1 || value > 64) return kInvalidConfig;
         forced_max_blocks_ = value;

@@ -38,6 +38,7 @@ struct CostCtx {
     const unsigned long long *cl64, *cr64;
     const int16_t *rmin, *rmax;
     int prior_ranges;  // 0: every pixel has the default range [d0, min(dmax, x+1)); 1: rmin/rmax vary
+    int tile;          // cost kernel tile width (64, 128, 256; 0 = default for Dp)
 };
 
 // Quantised cost of left (x, y) against right (xr, y) from LUTs held in shared memory.

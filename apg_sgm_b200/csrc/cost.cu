@@ -156,6 +156,9 @@ __global__ void __launch_bounds__(256) cost_kernel(CostCtx c, int txc, int ha, i
                 hi = (int16_t)(rg >> 16);
             }
             word = 0;
+            // both disparities of the word valid (the common case): no per-voxel range tests
+            const int dw = c.d0 + 2 * k;
+            const bool word_ok = !PRIOR && 2 * k + 1 < c.D && x - (dw + 1) >= 0 && x - dw < c.w;
 #pragma unroll
             for (int hs = 0; hs < 2; ++hs) {
                 const int di = 2 * k + hs;
@@ -163,7 +166,7 @@ __global__ void __launch_bounds__(256) cost_kernel(CostCtx c, int txc, int ha, i
                 const int xr = x - d;
                 uint32_t q = kInvalidCost;
                 // default range [d0, min(dmax, x+1)) and x - d inside the image
-                bool ok = di < c.D && xr >= 0 && xr < c.w;
+                bool ok = word_ok || (di < c.D && xr >= 0 && xr < c.w);
                 if (PRIOR) ok = ok && d >= lo && d < hi;
                 if (ok) {
                     const Aux<C64> ra = s_right[xi - di + c.D - 1];
@@ -293,6 +296,14 @@ __global__ void __launch_bounds__(256) cost_kernel(CostCtx c, int txc, int ha, i
             hi = (int16_t)(rg >> 16);
         }
         uint32_t word = 0;
+        const int dw = c.d0 + 2 * k;
+        if (!PRIOR && 2 * k + 1 < c.D && x - l >= dw + 1 && x + r <= c.w - 1 + dw) {
+            // both windows lie where the word's disparities are valid: the count is the window length
+            const uint32_t len = (uint32_t)(l + r + 1), mg = s_magic[len];
+            word = div_by_magic(s & 0xFFFFu, len, mg) | (div_by_magic(s >> 16, len, mg) << 16);
+            out_vol[((size_t)row + x) * W2 + k] = word;
+            return;
+        }
 #pragma unroll
         for (int hs = 0; hs < 2; ++hs) {
             const int di = 2 * k + hs;
@@ -333,10 +344,19 @@ cudaError_t launch_cost_t(const CostCtx& c, int txc, int lmax, int tau, uint32_t
 // Tile width: 128 columns where the staged costs fit comfortably (halo overhead 2*lmax/txc), else 64.
 int cost_tile(int Dp) { return Dp <= 128 ? 128 : 64; }
 
+// The requested tile width when its shared memory fits, else the default.
+int cost_tile_for(const CostCtx& c, int ha, bool cross, bool prior) {
+    const int req = c.tile;
+    if (req == 64 || req == 128 || req == 256) {
+        if (cost_layout(req, ha, c.D, c.Dp, cross, prior, c.census64 != 0).total <= 200 * 1024) return req;
+    }
+    return cost_tile(c.Dp);
+}
+
 template <bool C64, bool PRIOR>
 cudaError_t launch_cost_m(const CostCtx& c, int mode, int lmax, int tau, uint32_t* vol, uint32_t* rkey,
                           const uint32_t* magic, cudaStream_t s) {
-    const int txc = cost_tile(c.Dp);
+    const int txc = cost_tile_for(c, mode == 1 ? lmax : 0, mode == 1, PRIOR);
     const bool qlut = !c.use_ad && !c.use_grad;
     if (mode == 1) {
         return qlut ? launch_cost_t<C64, true, true, true, PRIOR, true>(c, txc, lmax, tau, vol, rkey, magic, s)

@@ -234,6 +234,7 @@ CostCtx Engine::cost_ctx() const {
     c.cl64 = ptr<unsigned long long>(lay_.cl); c.cr64 = ptr<unsigned long long>(lay_.cr);
     c.rmin = ptr<int16_t>(lay_.rmin); c.rmax = ptr<int16_t>(lay_.rmax);
     c.prior_ranges = cfg_.prior_enable ? 1 : 0;
+    c.tile = cost_tile_;
     return c;
 }
 
@@ -811,6 +812,11 @@ int apgcu_engine_set_tuning(apgcu_engine_t e, const char* key, int value) {
     if (std::strcmp(key, "sgm_lanes") == 0) {
         if (value != 0 && value != 8 && value != 16 && value != 32) return apgcu::kInvalidConfig;
         e->eng->set_sgm_lanes(value);
+        return 0;
+    }
+    if (std::strcmp(key, "cost_tile") == 0) {
+        if (value != 0 && value != 64 && value != 128 && value != 256) return apgcu::kInvalidConfig;
+        e->eng->set_cost_tile(value);
         return 0;
     }
     if (std::strcmp(key, "fast_fused") == 0) {

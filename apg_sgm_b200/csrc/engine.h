@@ -92,6 +92,7 @@ public:
     void set_debug(int f) { debug_ = f; }
     void set_sgm_lanes(int t) { sgm_lanes_ = t; }
     void set_fast_fused(bool on) { fast_fused_ = on; }
+    void set_cost_tile(int t) { cost_tile_ = t; }
     int debug() const { return debug_; }
     const apg_pipeline_config_t& config() const { return cfg_; }
     int device() const { return device_; }
@@ -121,6 +122,7 @@ private:
     int debug_ = 0;
     int sgm_lanes_ = 0;
     bool fast_fused_ = false;
+    int cost_tile_ = 0;
     cudaStream_t stream_ = nullptr;
     bool own_stream_ = false;
     unsigned char* arena_ = nullptr;

@@ -60,6 +60,7 @@ APGCU_API int apgcu_engine_set_debug(apgcu_engine_t e, int flags);
 
 /* Kernel tuning knobs (results never change, only speed):
  *   "sgm_lanes": lanes per SGM scanline chain, 8 / 16 / 32 (0 = default, 32);
+ *   "cost_tile": columns per block of the cost kernel, 64 / 128 / 256 (0 = default for the range);
  *   "fast_fused": 1 = census-only Fast mode recomputes its costs inside the SGM sweeps and stores no
  *                 cost volume (less memory, slower); 0 = store the volume once (default).
  * Returns 0, or APG_STATUS_INVALID_CONFIG for an unknown key or value. */
@@ -148,7 +149,8 @@ APGCU_API const char* apgcu_batch_last_error(apgcu_batch_t b);
  * and outputs are device pointers on the batch's device. */
 APGCU_API int apgcu_batch_process(apgcu_batch_t b, int npairs, const apgcu_pair_t* pairs, int device_buffers);
 /* Options (results never change): "graphs" 0/1, "batched_sgm" 0/1, "autotune" 0/1,
- * "sgm_lanes" 0/16/32 (0 = autotuned), "max_blocks_per_sm" -1 (autotuned) / 0 (occupancy) / N. */
+ * "sgm_lanes" 0/16/32 (0 = autotuned), "max_blocks_per_sm" -1 (autotuned) / 0 (occupancy) / N,
+ * "cost_tile" 0 (autotuned) / 64 / 128 / 256. */
 APGCU_API int apgcu_batch_set_option(apgcu_batch_t b, const char* key, int value);
 APGCU_API size_t apgcu_batch_allocated_bytes(apgcu_batch_t b);
 /* Device time of the last apgcu_batch_process (ms): from one start event every bucket waits on to

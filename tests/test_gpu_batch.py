@@ -56,7 +56,7 @@ def test_batch_equals_single_pairs_and_replays(apg, mode):
 
 
 @pytest.mark.parametrize("opts", [{"graphs": 0}, {"batched_sgm": 0}, {"sgm_lanes": 16},
-                                  {"max_blocks_per_sm": 1, "autotune": 0}])
+                                  {"max_blocks_per_sm": 1, "autotune": 0}, {"cost_tile": 256}, {"cost_tile": 64}])
 def test_batch_options_change_no_result(apg, opts):
     pairs = _pairs(300, mix=[(160, 96, 64, 2), (200, 120, 128, 2)])
     b = apg.Batch(apg.config_from_mode(1, 128), **opts)

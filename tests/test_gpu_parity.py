@@ -193,3 +193,16 @@ def test_session_frame_stats_match_reference(apg, O, mode, w, h, dmax):
     for k in ("valid_disparity_ratio", "reliable_ratio", "unreliable_ratio", "refine_changed_ratio", "lr_fail_ratio",
               "mean_search_width", "mean_geometry_width"):
         assert getattr(st, k) == rs[k], (k, getattr(st, k), rs[k])
+
+
+@pytest.mark.parametrize("mode,tile", [(1, 64), (1, 256), (0, 256), (2, 128)])
+def test_cost_tile_changes_no_result(apg, mode, tile):
+    """The cost kernel's tile width (tuning key cost_tile) changes no output."""
+    L, R = synth(300, 90, 96, patch=0.2 if mode == 2 else 0.0, seed=21)
+    cfg = apg.config_from_mode(mode, 96)
+    a = apg.Engine(cfg).process(L, R)
+    e = apg.Engine(cfg)
+    e.set_tuning("cost_tile", tile)
+    b = e.process(L, R)
+    for k in a:
+        assert same_bits(a[k], b[k]), k
