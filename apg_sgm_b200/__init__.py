@@ -581,3 +581,70 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+_MODE_VALUE = {"fast": 0, "balanced": 1, "high_quality": 2, "hq": 2}
+
+
+class Server:
+    """Served form (apgcu_server_*): a request loop with continuous batching.
+
+    `slots` requests run at once, each on a device-resident engine of its (mode, size, range)
+    borrowed from a pool; engine workspaces are admitted against an HBM budget.  submit() returns
+    at once; wait() returns the outputs and the submission-to-completion latency in ms."""
+
+    def __init__(self, device: int = 0, hbm_budget_gb: float = 120.0, slots: int = 4):
+        self._h = lib().apgcu_server_create(int(device), int(hbm_budget_gb * (1 << 30)), int(slots))
+        if not self._h:
+            raise RuntimeError("apgcu_server_create failed (no CUDA device?)")
+        self._pending = {}
+
+    def submit(self, left, right, mode=QualityMode.Balanced, max_disparity=128, min_disparity=0,
+               outputs: bool = True) -> int:
+        lv, la = _image_view(left, "left")
+        rv, ra = _image_view(right, "right")
+        if lv.stride != rv.stride:
+            la, ra = np.ascontiguousarray(la), np.ascontiguousarray(ra)
+            lv, rv = _image_view(la, "left")[0], _image_view(ra, "right")[0]
+        h, w = lv.height, lv.width
+        o = None
+        if outputs:
+            o = {"disparity": np.empty((h, w), np.float32), "confidence": np.empty((h, w), np.float32),
+                 "invalid_reason": np.empty((h, w), np.uint8), "reliable_mask": np.empty((h, w), np.uint8)}
+        ptr = (lambda k: o[k].ctypes.data) if o else (lambda k: None)
+        req = _lib_mod.Request(int(_MODE_VALUE.get(mode, mode)), int(min_disparity), int(max_disparity),
+                               lv.data, rv.data, w, h, lv.stride, lv.channels, ptr("disparity"), ptr("confidence"),
+                               ptr("invalid_reason"), ptr("reliable_mask"))
+        t = C.c_ulonglong()
+        rc = lib().apgcu_server_submit(self._h, C.byref(req), C.byref(t))
+        if rc != 0:
+            raise RuntimeError(f"submit failed [{rc}]")
+        self._pending[t.value] = (la, ra, o)
+        return t.value
+
+    def wait(self, ticket: int):
+        lat = C.c_double()
+        rc = lib().apgcu_server_wait(self._h, int(ticket), C.byref(lat))
+        _, _, o = self._pending.pop(ticket)
+        if rc != 0:
+            raise RuntimeError(f"request failed [{rc}]: {lib().apgcu_server_last_error(self._h).decode()}")
+        return o, lat.value
+
+    def stats(self) -> dict:
+        c = (C.c_ulonglong * 4)()
+        b = (C.c_size_t * 2)()
+        lib().apgcu_server_stats(self._h, c, b)
+        return {"completed": c[0], "failed": c[1], "evictions": c[2], "peak_in_flight": c[3],
+                "reserved_bytes": b[0], "peak_reserved_bytes": b[1],
+                "budget_bytes": int(lib().apgcu_server_budget(self._h))}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().apgcu_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -66,6 +66,14 @@ class Pair(C.Structure):
                 ("reliable_mask", C.c_void_p)]
 
 
+class Request(C.Structure):
+    """apgcu_request_t (include/apg_sgm_cuda.h): one request to the server."""
+    _fields_ = [("mode", C.c_int), ("min_disparity", C.c_int), ("max_disparity", C.c_int),
+                ("left", C.c_void_p), ("right", C.c_void_p), ("width", C.c_int), ("height", C.c_int),
+                ("stride", C.c_int), ("channels", C.c_int), ("disparity", C.c_void_p), ("confidence", C.c_void_p),
+                ("invalid_reason", C.c_void_p), ("reliable_mask", C.c_void_p)]
+
+
 _lib = None
 
 _SIGS = {
@@ -119,6 +127,13 @@ _SIGS = {
     "apgcu_batch_allocated_bytes": (C.c_size_t, [C.c_void_p]),
     "apgcu_batch_last_time_ms": (C.c_float, [C.c_void_p]),
     "apgcu_batch_release": (None, [C.c_void_p]),
+    "apgcu_server_create": (C.c_void_p, [C.c_int, C.c_size_t, C.c_int]),
+    "apgcu_server_destroy": (None, [C.c_void_p]),
+    "apgcu_server_submit": (C.c_int, [C.c_void_p, C.POINTER(Request), C.POINTER(C.c_ulonglong)]),
+    "apgcu_server_wait": (C.c_int, [C.c_void_p, C.c_ulonglong, C.POINTER(C.c_double)]),
+    "apgcu_server_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_ulonglong), C.POINTER(C.c_size_t)]),
+    "apgcu_server_budget": (C.c_size_t, [C.c_void_p]),
+    "apgcu_server_last_error": (C.c_char_p, [C.c_void_p]),
     "apgcu_right_wta_noalloc": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                           C.c_void_p, C.c_void_p]),
 }

@@ -158,6 +158,41 @@ APGCU_API size_t apgcu_batch_allocated_bytes(apgcu_batch_t b);
 APGCU_API float apgcu_batch_last_time_ms(apgcu_batch_t b);
 APGCU_API void apgcu_batch_release(apgcu_batch_t b);
 
+/* ---- Served form: a request loop with continuous batching.
+ *
+ * No counterpart in the reference.  `slots` worker threads take requests in arrival order; each
+ * borrows a device-resident engine of the request's (mode, size, range) from a pool (or creates
+ * one), runs it on the engine's own stream and returns it, so requests that arrive while others
+ * are on the GPU are admitted as slots and memory free up and overlap on the device.  Engine
+ * workspaces are admitted against an HBM budget (min of hbm_budget_bytes and the device's free
+ * memory less 2 GiB); idle engines of other buckets are released to make room.  Each result
+ * equals the single-pair engine's output for that pair. */
+typedef struct apgcu_server_s* apgcu_server_t;
+typedef struct {
+    int mode;                   /* APG_QUALITY_FAST / BALANCED / HIGH_QUALITY */
+    int min_disparity, max_disparity;
+    const uint8_t* left;        /* host memory, valid until the request completes */
+    const uint8_t* right;
+    int width, height, stride, channels;
+    float* disparity;           /* host outputs, W*H each; any may be NULL */
+    float* confidence;
+    uint8_t* invalid_reason;
+    uint8_t* reliable_mask;
+} apgcu_request_t;
+
+APGCU_API apgcu_server_t apgcu_server_create(int device, size_t hbm_budget_bytes, int slots);
+/* Finishes queued requests' in-flight work, then stops the workers. */
+APGCU_API void apgcu_server_destroy(apgcu_server_t s);
+/* Queues a request (returns at once); *ticket identifies it. */
+APGCU_API int apgcu_server_submit(apgcu_server_t s, const apgcu_request_t* r, unsigned long long* ticket);
+/* Blocks until the request completes; returns its status; *latency_ms = submission to completion. */
+APGCU_API int apgcu_server_wait(apgcu_server_t s, unsigned long long ticket, double* latency_ms);
+/* counts4 = {completed, failed, engine evictions, peak requests in flight};
+ * bytes2 = {reserved workspace bytes now, peak reserved}. */
+APGCU_API int apgcu_server_stats(apgcu_server_t s, unsigned long long* counts4, size_t* bytes2);
+APGCU_API size_t apgcu_server_budget(apgcu_server_t s);
+APGCU_API const char* apgcu_server_last_error(apgcu_server_t s);
+
 /* Right-image winner-take-all over a caller's cost volume, allocating nothing.
  *
  * No counterpart in the reference: it exposes as one call the right-image WTA that the reference

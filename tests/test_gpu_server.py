@@ -1,0 +1,81 @@
+"""Served form (apgcu_server_*): each result is the same alone and in the mix.
+
+A burst of requests of four sizes and three quality modes, in shuffled order, is served with
+several slots (their work overlaps on the device); every output must equal, bit for bit, the
+single-pair engine's output for that pair.  A small HBM budget forces engine evictions without
+changing any result, and a request larger than the whole budget is refused.
+"""
+import numpy as np
+import pytest
+
+from helpers import same_bits, synth
+
+pytestmark = pytest.mark.gpu
+
+KEYS = ("disparity", "confidence", "invalid_reason", "reliable_mask")
+SIZES = [(160, 96, 64), (200, 120, 128), (256, 64, 192), (192, 108, 256)]
+
+
+def _pool():
+    pool = []
+    for i, (w, h, dmax) in enumerate(SIZES):
+        for mode in (1, 0, 2):
+            L, R = synth(w, h, dmax, cells=5, lo=0, hi=dmax - 8, patch=0.2 if mode == 2 else 0.0, seed=60 + i)
+            pool.append((mode, dmax, L, R))
+    return pool
+
+
+def _alone(apg, pool):
+    want = []
+    for mode, dmax, L, R in pool:
+        e = apg.Engine(apg.config_from_mode(mode, dmax))
+        want.append(e.process(L, R))
+        e.close()
+    return want
+
+
+def _serve(apg, pool, order, **kw):
+    srv = apg.Server(**kw)
+    tickets = [(i, srv.submit(pool[i][2], pool[i][3], mode=pool[i][0], max_disparity=pool[i][1])) for i in order]
+    got = []
+    for i, t in tickets:
+        o, lat = srv.wait(t)
+        assert lat > 0
+        got.append((i, o))
+    st = srv.stats()
+    srv.close()
+    return got, st
+
+
+def test_served_results_equal_alone(apg):
+    pool = _pool()
+    want = _alone(apg, pool)
+    order = np.random.default_rng(7).permutation(np.repeat(np.arange(len(pool)), 3))
+    got, st = _serve(apg, pool, order, slots=4)
+    for i, o in got:
+        for k in KEYS:
+            assert same_bits(o[k], want[i][k]), (i, k)
+    assert st["completed"] == len(order) and st["failed"] == 0
+    assert st["peak_in_flight"] >= 2
+
+
+def test_served_small_budget_evicts_and_matches(apg):
+    pool = _pool()
+    want = _alone(apg, pool)
+    biggest = max(apg.workspace_bytes(apg.config_from_mode(m, d), L.shape[1], L.shape[0]) for m, d, L, _ in pool)
+    order = np.random.default_rng(8).permutation(np.repeat(np.arange(len(pool)), 2))
+    got, st = _serve(apg, pool, order, slots=3, hbm_budget_gb=1.5 * biggest / (1 << 30))
+    for i, o in got:
+        for k in KEYS:
+            assert same_bits(o[k], want[i][k]), (i, k)
+    assert st["evictions"] > 0
+    assert st["peak_reserved_bytes"] <= st["budget_bytes"]
+
+
+def test_served_request_beyond_budget_is_refused(apg):
+    L, R = synth(320, 240, 128)
+    srv = apg.Server(slots=1, hbm_budget_gb=1e-3)
+    t = srv.submit(L, R, mode=1, max_disparity=128)
+    with pytest.raises(RuntimeError, match=r"\[6\].*budget"):
+        srv.wait(t)
+    srv.close()
