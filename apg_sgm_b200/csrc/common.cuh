@@ -125,6 +125,25 @@ __device__ __forceinline__ int adaptive_p2(const SgmPen& p, int dI) {
     return P2 > floor_p2 ? P2 : floor_p2;
 }
 
+// Lets `kern` launch with as much dynamic shared memory as the device allows it (the opt-in
+// maximum less the function's static shared memory).  The attribute is per function and shared by
+// every host thread, so it is always set to that same per-function maximum, never to one launch's
+// size: a thread launching with more shared memory than another thread's last setting would
+// otherwise be refused.  Occupancy follows each launch's actual size.
+template <typename F>
+inline cudaError_t allow_dynamic_smem(F kern, size_t smem) {
+    if (smem <= 48 * 1024) return cudaSuccess;
+    int dev = 0, optin = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaFuncAttributes fa;
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, kern);
+    if (e != cudaSuccess) return e;
+    const int limit = optin - (int)fa.sharedSizeBytes;
+    if ((long long)smem > limit) return cudaErrorInvalidValue;
+    return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, limit);
+}
+
 #define APGCU_CHECK(expr)                                                    \
     do {                                                                     \
         cudaError_t _e = (expr);                                             \

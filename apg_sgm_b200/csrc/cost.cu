@@ -332,8 +332,8 @@ cudaError_t launch_cost_t(const CostCtx& c, int txc, int lmax, int tau, uint32_t
     const int ha = CROSS ? lmax : 0;
     const CostLayout ly = cost_layout(txc, ha, c.D, c.Dp, CROSS, PRIOR, C64);
     auto kern = cost_kernel<C64, CROSS, STORE, RWTA, PRIOR, QLUT>;
-    if (ly.total > 48 * 1024) {
-        cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ly.total);
+    {
+        const cudaError_t err = allow_dynamic_smem(kern, ly.total);
         if (err != cudaSuccess) return err;
     }
     dim3 grid((c.w + txc - 1) / txc, c.h);

@@ -273,8 +273,8 @@ cudaError_t launch_cross_v(int w, int h, int d0, int D, int Dp, int lmax, int ta
             constexpr int RS = decltype(rs_tag)::value;
             const size_t smem = (size_t)RS * nthr * 4 + extra;
             auto kern = cross_v_default_kernel<RS>;
-            if (smem > 48 * 1024) {
-                cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            {
+                const cudaError_t e = allow_dynamic_smem(kern, smem);
                 if (e != cudaSuccess) return e;
             }
             dim3 grid((w + cols - 1) / cols, (h + kSeg - 1) / kSeg);
@@ -287,8 +287,8 @@ cudaError_t launch_cross_v(int w, int h, int d0, int D, int Dp, int lmax, int ta
     }
     const int RS = 2 * lmax + 2;
     const size_t smem = (size_t)RS * nthr * 8 + (size_t)cols * kSeg * 2;
-    if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(cross_v_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    {
+        const cudaError_t e = allow_dynamic_smem(cross_v_kernel, smem);
         if (e != cudaSuccess) return e;
     }
     dim3 grid((w + cols - 1) / cols, (h + kSeg - 1) / kSeg);
@@ -303,8 +303,8 @@ cudaError_t launch_cross_h(int w, int h, int d0, int D, int Dp, int lmax, int ta
     const int W2 = Dp / 2;
     const int RS = 2 * lmax + 2;
     const size_t smem = (size_t)RS * W2 * 8;
-    if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(cross_h_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    {
+        const cudaError_t e = allow_dynamic_smem(cross_h_kernel, smem);
         if (e != cudaSuccess) return e;
     }
     dim3 grid((w + kSeg - 1) / kSeg, h);

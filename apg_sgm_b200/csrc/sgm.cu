@@ -816,8 +816,8 @@ cudaError_t launch_first_tk(const SgmArgs& a, DirTable tab, bool census, cudaStr
     } else {
         const size_t smem = (size_t)4 * kVolPfFirst * vol_slot_words<K, 0>() * 4;
         auto kern = sgm_first_kernel<T, K, false>;
-        if (smem > 48 * 1024) {
-            const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        {
+            const cudaError_t e = allow_dynamic_smem(kern, smem);
             if (e != cudaSuccess) return e;
         }
         kern<<<blocks, 128, smem, st>>>(a, tab);
@@ -838,9 +838,8 @@ cudaError_t launch_last_tk(const SgmArgs& a, DirTable tab, bool census, cudaStre
         } else {                                                                                     \
             const size_t smem = (size_t)4 * (last_pf<K, T, NB>() * vol_slot_words<K, NB>() + wta_buf_words<K, T>()) * 4; \
             auto kern = sgm_last_kernel<T, K, false, NB>;                                            \
-            if (smem > 48 * 1024) {                                                                  \
-                const cudaError_t e =                                                                \
-                    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
+            {                                                                                        \
+                const cudaError_t e = allow_dynamic_smem(kern, smem);                                \
                 if (e != cudaSuccess) return e;                                                      \
             }                                                                                        \
             kern<<<blocks, 128, smem, st>>>(a, tab);                                                 \
@@ -956,8 +955,8 @@ cudaError_t launch_batch_tk(const BatchPair* pairs, const BatchSeg* segs, int ns
     constexpr int PF = batch_pf<T, K, MODE, NB>();
     auto kern = sgm_batch_kernel<T, K, MODE, PF, NB>;
     const size_t smem = batch_smem<T, K, MODE, NB>(nseg);
-    if (smem > 48 * 1024) {
-        const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    {
+        const cudaError_t e = allow_dynamic_smem(kern, smem);
         if (e != cudaSuccess) return e;
     }
     int dev = 0, nsm = 148, occ = 1;

@@ -179,6 +179,102 @@ def run_reference(args, wl):
     }))
 
 
+SERVED_SIZES = [(640, 480, 64, 8, 4, 60), (1242, 375, 192, 12, 0, 180), (1280, 720, 128, 12, 0, 120),
+                (1920, 1080, 256, 16, 0, 240)]
+
+
+def _served_stream(n, rate, seed):
+    """n requests: (arrival s, size index, mode, pool slot); Poisson arrivals at `rate` pairs/s
+    (rate 0: all at t = 0); sizes uniform over the four shapes; modes 70/20/10 Balanced/Fast/HQ."""
+    rng = np.random.default_rng(seed)
+    gaps = rng.exponential(1.0 / rate, n) if rate > 0 else np.zeros(n)
+    t = np.cumsum(gaps) - (gaps[0] if rate > 0 else 0.0)
+    size = rng.integers(0, len(SERVED_SIZES), n)
+    mode = rng.choice([1, 0, 2], size=n, p=[0.7, 0.2, 0.1])
+    slot = rng.integers(0, 2, n)
+    return list(zip(t.tolist(), size.tolist(), mode.tolist(), slot.tolist()))
+
+
+def _serve_stream(apg, pool, stream, slots):
+    """Submits every request at its arrival time (a submitter thread) and collects latencies."""
+    import threading as th
+    srv = apg.Server(slots=slots, hbm_budget_gb=120.0)
+    tickets = [None] * len(stream)
+    lat = [0.0] * len(stream)
+    t0 = time.perf_counter()
+
+    def submitter():
+        for i, (ta, si, mode, sl) in enumerate(stream):
+            d = t0 + ta - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            L, R = pool[(si, mode, sl)]
+            tickets[i] = srv.submit(L, R, mode=mode, max_disparity=SERVED_SIZES[si][2])
+
+    th_sub = th.Thread(target=submitter)
+    th_sub.start()
+    for i in range(len(stream)):
+        while tickets[i] is None:
+            time.sleep(0.0005)
+        _, lat[i] = srv.wait(tickets[i])
+    t_end = time.perf_counter()
+    th_sub.join()
+    st = srv.stats()
+    srv.close()
+    lat = np.array(lat)
+    span = t_end - t0
+    return {"pairs_per_s": len(stream) / span, "p50_ms": float(np.percentile(lat, 50)),
+            "p95_ms": float(np.percentile(lat, 95)), "p99_ms": float(np.percentile(lat, 99)),
+            "mean_ms": float(lat.mean()), "span_s": span, "peak_in_flight": st["peak_in_flight"],
+            "evictions": st["evictions"], "peak_reserved_gb": st["peak_reserved_bytes"] / 2 ** 30}
+
+
+def run_served(args):
+    """The served stream: requests of four sizes and three modes with Poisson arrivals, through
+    the served form (args.slots slots, continuous batching) and through the serial plain path
+    (one slot) on the same arrival stream; plus a saturation burst for each."""
+    import apg_sgm_b200 as apg
+    from apg_sgm_b200 import synthetic as S
+    pool = {}
+    for si, (w, h, D, cells, lo, hi) in enumerate(SERVED_SIZES):
+        for mode in (0, 1, 2):
+            for sl in range(2):
+                spec = S.PairSpec(w, h, D, cells, lo, hi, 0.2 if mode == 2 else 0.0)
+                pool[(si, mode, sl)] = S.make_pair(spec, S.SEED_BASE + 1000 + si * 10 + mode * 2 + sl)[:2]
+    rates = [float(r) for r in args.rates.split(",")]
+    per_rate = max(1, args.requests // len(rates))
+    warm = _served_stream(48, 0, 1)
+    _serve_stream(apg, pool, warm, args.slots)  # engines, modules, pinned staging
+    results = []
+    for k, rate in enumerate(rates):
+        stream = _served_stream(per_rate, rate, 100 + k)
+        served = _serve_stream(apg, pool, stream, args.slots)
+        serial = _serve_stream(apg, pool, stream, 1)
+        results.append({"rate": rate, "requests": per_rate, "served": served, "serial": serial})
+    burst = _served_stream(min(per_rate, 1000), 0, 999)
+    cap_served = _serve_stream(apg, pool, burst, args.slots)
+    cap_serial = _serve_stream(apg, pool, burst, 1)
+    mean_vox = float(np.mean([w * h * D for w, h, D, *_ in SERVED_SIZES]))
+    top = results[-1]
+    print(json.dumps({
+        "metric": "served pairs/s with p50/p95/p99 latency (mixed sizes and modes, bit-exact)",
+        "value": cap_served["pairs_per_s"], "unit": "pairs/s", "n_gpus": 1, "steps": per_rate * len(rates),
+        "warmup": len(warm), "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u16",
+        "data": "synthetic",
+        "config": {"workload": "served_mixed_stream", "sizes": "640x480 D64, 1242x375 D192, 1280x720 D128, "
+                   "1920x1080 D256", "modes": "70% Balanced, 20% Fast, 10% HighQuality", "arrivals": "Poisson",
+                   "rates": rates, "slots": args.slots, "hbm_budget_gb": 120, "pool_pairs": len(pool)},
+        "capacity": {"served_pairs_per_s": cap_served["pairs_per_s"], "serial_pairs_per_s": cap_serial["pairs_per_s"],
+                     "speedup": cap_served["pairs_per_s"] / cap_serial["pairs_per_s"],
+                     "served_voxels_per_s": cap_served["pairs_per_s"] * mean_vox, "burst_requests": len(burst),
+                     "served": cap_served, "serial": cap_serial},
+        "rates": results,
+        "latency_ms_at_top_rate": {"p50": top["served"]["p50_ms"], "p95": top["served"]["p95_ms"],
+                                   "p99": top["served"]["p99_ms"]},
+        "e2e": {"value": cap_served["pairs_per_s"], "unit": "pairs/s", "api": "apgcu_server_submit/wait (host buffers)"},
+    }))
+
+
 def run_reference_batched(args):
     """The reference's Packed CPU path over the 64-pair batch, pair after pair; a step is one
     bounded sample: one pair of each size, scaled by the batch's pair counts."""
@@ -593,9 +689,21 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batched"], default="fast720")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batched", "served"], default="fast720")
+    ap.add_argument("--requests", type=int, default=10000, help="served: total requests over the rates")
+    ap.add_argument("--rates", default="50,100,200,400", help="served: Poisson arrival rates, pairs/s")
+    ap.add_argument("--slots", type=int, default=4, help="served: requests in flight")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
+    if args.workload == "served":
+        if args.impl == "reference":
+            if int(os.environ.get("RANK", "0")) == 0:
+                print(json.dumps({"impl": "reference", "unavailable": "the served form has no reference counterpart; "
+                                  "the reference CPU path is timed by the batched and single-pair workloads"}))
+            return
+        if int(os.environ.get("RANK", "0")) == 0:
+            run_served(args)
+        return
     if args.workload == "batched":
         if args.impl == "reference":
             if int(os.environ.get("RANK", "0")) == 0:
