@@ -75,6 +75,10 @@ int Engine::validate_config(const apg_pipeline_config_t& c, std::string& msg) {
     }
     if (c.prior_enable && c.prior_search_radius < 0) { msg = "prior search_radius must be non-negative"; return kInvalidConfig; }
     if (c.refine_enable && c.refine_iterations < 0) { msg = "refine iterations must be non-negative"; return kInvalidConfig; }
+    if (c.refine_enable && c.refine_iterations > kRefineMaxIter) {
+        msg = "refine iterations above 63 are not supported by the CUDA backend";
+        return kUnsupportedBackend;
+    }
     // Limits of the device kernels (documented in the library header).
     const int D = c.max_disparity - c.min_disparity;
     if (D > 512) { msg = "disparity range above 512 is not supported by the CUDA backend"; return kUnsupportedBackend; }
@@ -154,10 +158,11 @@ Layout Engine::make_layout(const apg_pipeline_config_t& c, int w, int h, int ch,
     }
     if (c.refine_enable) {
         L.rf_prefix = take(n * 4 + 4);
-        L.rf_draws = take(n * 4 + 4);
         L.rf_scan_tmp_bytes = refine_scan_temp_bytes((int)n);
         L.rf_scan_tmp = take(L.rf_scan_tmp_bytes);
-        L.rf_count = take(16);
+        L.rf_state = take((size_t)(kRefineProgWord + refine_band_count(h)) * 4);
+        L.rf_pack = take(refine_pack_bytes((int)n, c.census_type == APG_CENSUS_9X7));
+        L.rf_steps = take(refine_steps_bytes((int)n));
     }
     L.total = o;
     return L;
@@ -194,6 +199,7 @@ Engine::Engine(const apg_pipeline_config_t& cfg, int device, cudaStream_t stream
 
 Engine::~Engine() {
     release();
+    if (refine_err_host_) cudaFreeHost(refine_err_host_);
     for (auto& e : ev_) if (e) cudaEventDestroy(e);
     for (auto& e : pev_) if (e) cudaEventDestroy(e);
     if (own_stream_ && stream_) cudaStreamDestroy(stream_);
@@ -211,6 +217,7 @@ void Engine::release() {
         pin_ = nullptr;
         pinned_bytes_ = 0;
     }
+    rtab_.release();
     lay_ = Layout();
 }
 
@@ -320,6 +327,8 @@ int Engine::process_host(const uint8_t* left, const uint8_t* right, int w, int h
                                               cudaMemcpyDeviceToHost, stream_);
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
     if (e != cudaSuccess) return cuda_fail(e, "output download");
+    rc = check_refine();
+    if (rc) return rc;
     counts_fresh_ = true;
     if (!outputs_pinned) {
         if (disp) std::memcpy(disp, pdisp, n * 4);
@@ -355,7 +364,8 @@ int Engine::process_device(const uint8_t* dl, const uint8_t* dr, int w, int h, i
 
 int Engine::sync() {
     cudaError_t e = cudaStreamSynchronize(stream_);
-    return e == cudaSuccess ? kOk : cuda_fail(e, "stream synchronize");
+    if (e != cudaSuccess) return cuda_fail(e, "stream synchronize");
+    return check_refine();
 }
 
 #define RUN(expr, what)                                  \
@@ -667,37 +677,51 @@ int Engine::launch_profile(int max, const char** names, float* ms) const {
 
 int Engine::run_refine(float* work) {
     // detail::refine_scalar (src/refiner.cpp:42-100): one mt19937(12345) stream, a fresh
-    // uniform_int_distribution(-r, r) per iteration, draws consumed in the pass's raster order.
-    std::mt19937 rng(12345);
+    // uniform_int_distribution(-r, r) per iteration, draws consumed in the pass's raster order
+    // (the draw tables and the on-device stream positions of refine.cu); no host synchronisation.
     const Layout& L = lay_;
-    const CostCtx cc = cost_ctx();
-    std::vector<int> draws;
-    unsigned launches = 0;
-    for (int it = 0; it < cfg_.refine_iterations; ++it) {
-        const int fwd = (it % 2) == 0;
-        const int radius = std::max(1, cfg_.refine_random_radius >> it);
-        int* d_cnt = reinterpret_cast<int*>(arena_ + L.rf_count);
-        cudaError_t e = launch_refine_count(L, arena_, work, fwd, d_cnt, stream_, &launches);
-        if (e != cudaSuccess) return cuda_fail(e, "refine count");
-        int cnt = 0;
-        e = cudaMemcpyAsync(&cnt, d_cnt, 4, cudaMemcpyDeviceToHost, stream_);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
-        if (e != cudaSuccess) return cuda_fail(e, "refine count read");
-        std::uniform_int_distribution<int> dist(-radius, radius);
-        draws.resize(std::max(cnt, 1));
-        for (int i = 0; i < cnt; ++i) draws[i] = dist(rng);
-        if (cnt > 0) {
-            e = cudaMemcpyAsync(reinterpret_cast<int*>(arena_ + L.rf_draws), draws.data(), (size_t)cnt * 4,
-                                cudaMemcpyHostToDevice, stream_);
-            if (e != cudaSuccess) return cuda_fail(e, "refine draws upload");
+    const int n = L.w * L.h;
+    const int iters = cfg_.refine_iterations;
+    if (!rtab_.dev || rtab_.iters != iters || rtab_.n_built < n || rtab_.radius_built != cfg_.refine_random_radius) {
+        cudaStreamSynchronize(stream_);
+        if (rtab_.build(iters, cfg_.refine_random_radius, n) != 0) {
+            rtab_.release();
+            cudaGetLastError();
+            return fail(kAllocationFailure, "refine draw tables could not be built");
         }
-        e = launch_refine_pass(cfg_, cc, L, arena_, work, fwd, stream_, &launches);
-        if (e != cudaSuccess) return cuda_fail(e, "refine pass");
-        // the draws vector is reused by the next pass: wait until this upload is consumed
-        e = cudaStreamSynchronize(stream_);
-        if (e != cudaSuccess) return cuda_fail(e, "refine pass sync");
     }
+    if (!refine_err_host_) {
+        if (cudaMallocHost(&refine_err_host_, sizeof(int)) != cudaSuccess) {
+            cudaGetLastError();
+            refine_err_host_ = nullptr;
+            return fail(kAllocationFailure, "pinned refine flag allocation failed");
+        }
+        *refine_err_host_ = 0;
+    }
+    const CostCtx cc = cost_ctx();
+    unsigned launches = 0;
+    unsigned char* state = arena_ + L.rf_state;
+    cudaError_t e = cudaMemsetAsync(state, 0, (size_t)(kRefineProgWord + refine_band_count(L.h)) * 4, stream_);
+    if (e == cudaSuccess) e = launch_refine_pack(cc, L, arena_, stream_, &launches);
+    for (int it = 0; it < iters && e == cudaSuccess; ++it) {
+        e = launch_refine_count(L, arena_, work, (it % 2) == 0, stream_, &launches);
+        if (e == cudaSuccess) e = launch_refine_pass(cc, L, arena_, rtab_, it, work, stream_, &launches);
+    }
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(refine_err_host_, state + kRefineErrWord * 4, sizeof(int), cudaMemcpyDeviceToHost, stream_);
+    if (e != cudaSuccess) return cuda_fail(e, "refine");
+    refine_pending_ = true;
     count_launches(launches);
+    return kOk;
+}
+
+int Engine::check_refine() {
+    if (!refine_pending_) return kOk;
+    refine_pending_ = false;
+    if (refine_err_host_ && *refine_err_host_) {
+        *refine_err_host_ = 0;
+        return fail(kInternalError, "refine: a wavefront wait timed out");
+    }
     return kOk;
 }
 

@@ -49,11 +49,30 @@ struct Layout {
     size_t lut, qlut, magic;
     // HighQuality prior / refine
     size_t pr_cand, pr_ncand, pr_taken, pr_grid, pr_maps, pr_scratch, pr_count;
-    size_t rf_prefix, rf_draws, rf_scan_tmp, rf_count;
+    size_t rf_prefix, rf_scan_tmp, rf_state, rf_pack, rf_steps;  // refine: draw-index prefix, scan scratch,
+                                                                   // pass state, packed images, pixel records
     size_t stats = 0;  // u64 frame counters (launch_frame_stats) + prior support count
     size_t rf_scan_tmp_bytes = 0;
     int n_cells = 0, gw = 0, gh = 0, max_cand = 0;
 };
+
+// Refine pass state (u32 words at Layout::rf_state): pass start positions, error flag, progress.
+constexpr int kRefineMaxIter = 63;
+constexpr int kRefineErrWord = 64;
+constexpr int kRefineProgWord = 80;
+
+// Per-engine device copies of the refiner's draw tables (see refine.cu).
+struct RefineTables {
+    void* dev = nullptr;
+    size_t bytes = 0;
+    int iters = 0, n_built = 0, radius_built = 0;
+    int16_t* value[kRefineMaxIter] = {};
+    unsigned* rejected[kRefineMaxIter] = {};
+    int nrej[kRefineMaxIter] = {};
+    int build(int iterations, int base_radius, int n);  // 0 on success
+    void release();
+};
+int refine_band_count(int h);
 
 class Engine {
 public:
@@ -85,7 +104,7 @@ public:
     int sync();
     int dump(int what, void* dst, size_t bytes);
     void stage_times(double* ms11) const;
-    size_t allocated_bytes() const { return arena_bytes_ + pinned_bytes_; }
+    size_t allocated_bytes() const { return arena_bytes_ + pinned_bytes_ + rtab_.bytes; }
     void release();
     cudaStream_t stream() const { return stream_; }
     const std::string& last_error() const { return err_; }
@@ -111,6 +130,7 @@ private:
     int run_post(float* d_disp, float* d_conf, uint8_t* d_reason, uint8_t* d_reliable);
     int run_prior();
     int run_refine(float* work);
+    int check_refine();  // after a synchronisation: the refine error flag of the last frame
     int fail(int code, const std::string& m) { err_ = m; return code; }
     int ensure_pinned(size_t need);
     int cuda_fail(cudaError_t e, const char* where);
@@ -149,6 +169,9 @@ private:
     int support_count_ = 0;
     unsigned long long counts_[8] = {};  // frame counters copied with the host outputs
     const uint32_t* sgm_src_ = nullptr;  // volume the SGM sweeps read (set by run_pre)
+    RefineTables rtab_;                   // refine draw tables (HighQuality)
+    int* refine_err_host_ = nullptr;      // pinned copy of the refine error flag
+    bool refine_pending_ = false;
     bool counts_fresh_ = false;
     std::string err_;
 };
@@ -157,13 +180,18 @@ private:
 void count_launches(unsigned n);
 unsigned long long launch_count();
 
+
 // prior.cu / refine.cu
 cudaError_t launch_prior(const apg_pipeline_config_t& cfg, const CostCtx& c, const Layout& L, unsigned char* arena,
                          cudaStream_t s, unsigned* launches);
-cudaError_t launch_refine_count(const Layout& L, unsigned char* arena, const float* work, int fwd, int* d_count,
+cudaError_t launch_refine_count(const Layout& L, unsigned char* arena, const float* work, int fwd,
                                 cudaStream_t s, unsigned* launches);
-cudaError_t launch_refine_pass(const apg_pipeline_config_t& cfg, const CostCtx& c, const Layout& L,
-                               unsigned char* arena, float* work, int fwd, cudaStream_t s, unsigned* launches);
+cudaError_t launch_refine_pack(const CostCtx& c, const Layout& L, unsigned char* arena, cudaStream_t s,
+                               unsigned* launches);
+size_t refine_pack_bytes(int n, bool c64);
+size_t refine_steps_bytes(int n);
+cudaError_t launch_refine_pass(const CostCtx& c, const Layout& L, unsigned char* arena, const RefineTables& tab,
+                               int it, float* work, cudaStream_t s, unsigned* launches);
 size_t refine_scan_temp_bytes(int n);
 
 }  // namespace apgcu

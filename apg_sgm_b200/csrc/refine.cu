@@ -2,17 +2,33 @@
 //
 // The reference walks the image in raster order (forward on even passes, backward on odd) and
 // updates unreliable pixels in place, so a pixel sees the already-updated values of its causal
-// neighbours (left/up forward, right/down backward).  On the GPU one pass is an anti-diagonal
-// wavefront: 32x32 tiles are launched one tile-diagonal at a time, and inside a tile one warp
-// sweeps the 63 pixel anti-diagonals (lane = tile column).  This preserves exactly the
-// reference's read-after-write order.
+// neighbours (left and up forward, right and down backward).
 //
-// Random draws: the pixel that consumes a draw is unreliable, has a non-empty range and holds a
-// non-negative value at the start of the pass (a pass reads a pixel before writing it), so the
-// draw index of every pixel is an exclusive prefix count of those pixels in the pass's raster
-// order, computed before the pass.  The draws themselves are produced on the host by
-// std::mt19937 / std::uniform_int_distribution, the reference's own generator.
+// Schedule: a pass is one launch of refine_band_kernel.  A warp owns a band of 32 consecutive
+// (pass-order) rows, lane i row i, and walks the columns with lane i one column behind lane i-1:
+// at step t lane i updates column t - i, so its up neighbour is what lane i-1 produced at step
+// t-1 (one shuffle) and its left neighbour is its own previous value.  The first row of a band
+// reads the row above from global memory once the band above has published, through a progress
+// counter, that its last row is final that far; the bands therefore run as a wavefront about 40
+// columns apart and a pass takes about w + h steps.  Every wait is bounded: on timeout the band
+// sets an error flag (read by the host) and stops.  This is exactly the reference's
+// read-after-write order.
+//
+// Random draws: a pixel consumes a draw when it is unreliable, has a non-empty range and holds a
+// non-negative value at the start of the pass, so its draw index is an exclusive prefix count of
+// such pixels in the pass's raster order.  The reference takes draws from one std::mt19937(12345)
+// stream through a fresh std::uniform_int_distribution<int>(-r, r) per pass.  A draw maps one
+// accepted engine output to a value and skips rejected outputs, each a function of that single
+// output, so per radius the value of every output of the (fixed) stream and the rare rejected
+// indices are tabulated once, on the host, by the standard library itself: pass `it` then takes
+// the q-th accepted output at or after its start position P_it, and P_{it+1} follows on the device
+// from the pass's count.  No host work or synchronisation remains per frame.
+#include <algorithm>
 #include <cub/device/device_scan.cuh>
+#include <map>
+#include <mutex>
+#include <random>
+#include <vector>
 
 #include "engine.h"
 
@@ -20,7 +36,9 @@ namespace apgcu {
 
 namespace {
 
-constexpr int kTile = 32;
+constexpr int kBand = 32;
+constexpr int kPublish = 8;      // steps between progress publications
+constexpr int kMaxRejected = 64;  // rejected outputs tabulated per radius (expected: none)
 
 __global__ void refine_flags_kernel(int w, int h, const uint8_t* __restrict__ reliable, const int16_t* __restrict__ rmin,
                                     const int16_t* __restrict__ rmax, const float* __restrict__ work, int fwd,
@@ -33,57 +51,304 @@ __global__ void refine_flags_kernel(int w, int h, const uint8_t* __restrict__ re
     }
 }
 
-__global__ void copy_total_kernel(const int* prefix, int n, int* out) { *out = prefix[n]; }
+// Raw index of the q-th accepted output at or after P (rejected indices sorted ascending).
+__device__ __forceinline__ unsigned accepted_index(unsigned P, unsigned q, const unsigned* rej, int nrej) {
+    unsigned idx = P + q;
+    for (int k = 0; k < nrej; ++k) {
+        const unsigned r = rej[k];
+        if (r < P) continue;
+        if (r <= idx) ++idx;
+        else break;
+    }
+    return idx;
+}
+
+// Start of pass `it + 1`: the stream position after pass `it`'s count of draws from P[it]; also
+// clears the bands' progress counters for the next pass.
+__global__ void refine_advance_kernel(unsigned* P, int it, const int* count, const unsigned* rej, int nrej,
+                                      int* progress, int nbands) {
+    if (threadIdx.x == 0) {
+        const unsigned c = (unsigned)*count;
+        P[it + 1] = c ? accepted_index(P[it], c - 1, rej, nrej) + 1 : P[it];
+    }
+    for (int b = threadIdx.x; b < nbands; b += blockDim.x) progress[b] = 0;
+}
+
+// Left and right images packed per pixel for the refiner: census (32 bits, or 64 in two words) and
+// gray | gx << 8 | gy << 16, so a candidate's cost needs one load of each side.
+template <bool C64>
+struct RPack;
+template <>
+struct __align__(8) RPack<false> {
+    uint32_t c, g;
+};
+template <>
+struct __align__(16) RPack<true> {
+    unsigned long long c;
+    uint32_t g, pad;
+};
 
 template <bool C64>
-__global__ void __launch_bounds__(32) refine_tile_kernel(CostCtx c, int fwd, int diag, int ntv,
-                                                         const uint8_t* __restrict__ reliable,
-                                                         const int* __restrict__ prefix,
-                                                         const int* __restrict__ draws, float* work) {
+__global__ void refine_pack_kernel(CostCtx c, RPack<C64>* __restrict__ lp, RPack<C64>* __restrict__ rp) {
+    const int n = c.w * c.h;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        RPack<C64> a, b;
+        if constexpr (C64) {
+            a.c = c.cl64[i];
+            b.c = c.cr64[i];
+            a.pad = b.pad = 0;
+        } else {
+            a.c = c.cl[i];
+            b.c = c.cr[i];
+        }
+        a.g = (uint32_t)c.lgray[i] | ((uint32_t)c.lgx[i] << 8) | ((uint32_t)c.lgy[i] << 16);
+        b.g = (uint32_t)c.rgray[i] | ((uint32_t)c.rgx[i] << 8) | ((uint32_t)c.rgy[i] << 16);
+        lp[i] = a;
+        rp[i] = b;
+    }
+}
+
+// The refiner's local cost, local_cost (src/refiner.cpp:14-36), from packed pixels: the same LUT
+// terms added in the same order.
+template <bool C64>
+__device__ __forceinline__ float packed_cost(const CostCtx& c, const float* lut, const RPack<C64>& l,
+                                             const RPack<C64>& r) {
+    int pop;
+    if constexpr (C64) pop = __popcll(l.c ^ r.c);
+    else pop = __popc(l.c ^ r.c);
+    float v = lut[kLutCensus + pop];
+    const uint32_t dd = __vabsdiffu4(l.g, r.g);  // |dgray|, |dgx|, |dgy|
+    if (c.use_ad) v = __fadd_rn(v, lut[kLutAd + (dd & 0xFFu)]);
+    if (c.use_grad) v = __fadd_rn(v, lut[kLutGrad + ((dd >> 8) & 0xFFu) + (dd >> 16)]);
+    return v;
+}
+
+// Everything about one pixel of a pass that does not depend on the wavefront, computed for all
+// pixels at once before the pass and laid out in pass order (index v * w + u): the value at the
+// start of the pass, its range, and the two static candidates -- the current value and the
+// current value plus the pixel's draw -- with their costs.  The band kernel only costs the two
+// dynamic candidates (left and up neighbours) and keeps the reference's candidate order.
+struct __align__(16) RStep {
+    float cur;     // value at the start of the pass
+    float c_cur;   // cost of candidate `cur` (when upd bit 1)
+    float c_draw;  // cost of candidate `cur + draw` (when upd bit 2)
+    int d_pack;    // d_cur (low 16, signed) | d_draw (high 16, signed)
+    int range;     // lo (low 16) | hi (high 16)
+    int upd;       // bit 0: unreliable with a non-empty range; bit 1: cur is a candidate; bit 2: cur + draw is
+    int pad0, pad1;
+};
+
+template <bool C64>
+__device__ __forceinline__ float cand_cost(const CostCtx& c, const float* lut, const RPack<C64>& l,
+                                           const RPack<C64>* __restrict__ rp, int x, int y, int d, int lo, int hi) {
+    const int xr = x - d;
+    if (xr >= 0 && xr < c.w && d >= lo && d < hi) return packed_cost<C64>(c, lut, l, rp[y * c.w + xr]);
+    return 1e6f;
+}
+
+template <bool C64>
+__global__ void refine_prep_kernel(CostCtx c, int fwd, const uint8_t* __restrict__ reliable,
+                                   const int* __restrict__ prefix, const int16_t* __restrict__ draw_value,
+                                   const unsigned* __restrict__ rej, int nrej, const unsigned* __restrict__ P_ptr,
+                                   const RPack<C64>* __restrict__ lp, const RPack<C64>* __restrict__ rp,
+                                   const float* __restrict__ work, RStep* __restrict__ steps) {
     __shared__ float s_lut[kLutSize];
-    for (int i = threadIdx.x; i < kLutSize; i += 32) s_lut[i] = c.lut[i];
-    __syncwarp();
-    const int tu_min = max(0, diag - (ntv - 1));
-    const int tu = tu_min + blockIdx.x, tv = diag - tu;
+    for (int i = threadIdx.x; i < kLutSize; i += blockDim.x) s_lut[i] = c.lut[i];
+    __syncthreads();
     const int w = c.w, h = c.h, n = w * h;
-    const int lu = threadIdx.x;
-    const int u = tu * kTile + lu;
-    for (int s = 0; s < 2 * kTile - 1; ++s) {
-        const int lv = s - lu;
-        const int v = tv * kTile + lv;
-        if (lv >= 0 && lv < kTile && u < w && v < h) {
-            const int x = fwd ? u : w - 1 - u;
-            const int y = fwd ? v : h - 1 - v;
-            const int i = y * w + x;
-            const int lo = c.rmin[i], hi = c.rmax[i];
-            if (!reliable[i] && hi > lo) {
-                const float cur = work[i];
-                float vals[4];
-                int nv = 0;
-                vals[nv++] = cur;
-                if (fwd) {
-                    if (x > 0) vals[nv++] = work[i - 1];
-                    if (y > 0) vals[nv++] = work[i - w];
-                } else {
-                    if (x + 1 < w) vals[nv++] = work[i + 1];
-                    if (y + 1 < h) vals[nv++] = work[i + w];
-                }
-                if (cur >= 0.f) vals[nv++] = __fadd_rn(cur, (float)draws[prefix[fwd ? i : n - 1 - i]]);
-                float best_c = 1e9f;
-                int best_d = cur >= 0.f ? min(max((int)roundf(cur), lo), hi - 1) : lo;
-                for (int j = 0; j < nv; ++j) {
-                    if (vals[j] < 0.f) continue;
-                    const int d = min(max((int)roundf(vals[j]), lo), hi - 1);
-                    const int xr = x - d;
-                    float cc = 1e6f;
-                    if (xr >= 0 && xr < w && d >= lo && d < hi) cc = raw_cost<C64>(c, s_lut, x, y, xr);
-                    if (cc < best_c) { best_c = cc; best_d = d; }
-                }
-                work[i] = (float)best_d;
+    const unsigned P = *P_ptr;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        const int v = j / w, u = j - v * w;
+        const int x = fwd ? u : w - 1 - u;
+        const int y = fwd ? v : h - 1 - v;
+        const int i = y * w + x;
+        RStep st;
+        st.cur = work[i];
+        const int lo = c.rmin[i], hi = c.rmax[i];
+        st.range = (lo & 0xFFFF) | (hi << 16);
+        st.upd = (!reliable[i] && hi > lo) ? 1 : 0;
+        int d_cur = 0, d_draw = 0;
+        st.c_cur = st.c_draw = 1e9f;
+        st.pad0 = st.pad1 = 0;
+        if (st.upd && st.cur >= 0.f) {
+            const RPack<C64> l = lp[i];
+            d_cur = min(max((int)roundf(st.cur), lo), hi - 1);
+            st.c_cur = cand_cost<C64>(c, s_lut, l, rp, x, y, d_cur, lo, hi);
+            st.upd |= 2;
+            const unsigned q = (unsigned)prefix[fwd ? i : n - 1 - i];
+            const float dv = __fadd_rn(st.cur, (float)draw_value[accepted_index(P, q, rej, nrej)]);
+            if (dv >= 0.f) {
+                d_draw = min(max((int)roundf(dv), lo), hi - 1);
+                st.c_draw = cand_cost<C64>(c, s_lut, l, rp, x, y, d_draw, lo, hi);
+                st.upd |= 4;
             }
         }
-        __syncwarp();
+        st.d_pack = (d_cur & 0xFFFF) | (d_draw << 16);
+        steps[j] = st;
     }
+}
+
+constexpr int kRing = 16;  // steps of pixel records in flight per lane
+
+__device__ __forceinline__ void cp16(void* dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
+                 "l"(src)
+                 : "memory");
+}
+
+template <bool C64>
+__global__ void __launch_bounds__(32) refine_band_kernel(CostCtx c, int fwd, const RStep* __restrict__ steps,
+                                                         const RPack<C64>* __restrict__ lp,
+                                                         const RPack<C64>* __restrict__ rp, float* work,
+                                                         int* progress, int* err, int spin_limit) {
+    __shared__ float s_lut[kLutSize];
+    __shared__ __align__(16) RStep s_ring[kRing][32];
+    __shared__ __align__(16) RPack<C64> s_lpk[kRing][32];
+    const int lane = threadIdx.x;
+    for (int i = lane; i < kLutSize; i += 32) s_lut[i] = c.lut[i];
+    __syncwarp();
+    const int band = blockIdx.x;
+    const int w = c.w, h = c.h;
+    const int v = band * kBand + lane;  // pass-order row of this lane
+    const bool row_ok = v < h;
+    volatile int* vprog = progress;
+    // one cp.async group per step: this lane's record (and packed left pixel) of step t
+    auto issue = [&](int t) {
+        const int u = t - lane;
+        if (row_ok && u >= 0 && u < w && t < w + kBand - 1) {
+            const int j = v * w + u;
+            const RStep* src = steps + j;
+            cp16(&s_ring[t % kRing][lane], src);
+            cp16(reinterpret_cast<unsigned char*>(&s_ring[t % kRing][lane]) + 16,
+                 reinterpret_cast<const unsigned char*>(src) + 16);
+            const int x = fwd ? u : w - 1 - u;
+            const int y = fwd ? v : h - 1 - v;
+            if constexpr (C64) {
+                cp16(&s_lpk[t % kRing][lane], lp + y * w + x);
+            } else {
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(
+                                 (unsigned)__cvta_generic_to_shared(&s_lpk[t % kRing][lane])),
+                             "l"(lp + y * w + x)
+                             : "memory");
+            }
+        }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    };
+#pragma unroll 1
+    for (int t = 0; t < kRing; ++t) issue(t);
+    float prev = -1.f;  // value of this lane's previous column (its left neighbour)
+    int ready = band == 0 ? w : 0;  // columns of the row above the band known final
+    bool abort = false;
+    for (int t = 0; t < w + kBand - 1 && !abort; ++t) {
+        if (ready < min(t + 1, w)) {
+            // lane 0 waits until the band above has finished its last row up to column t + kPublish
+            int got = 0;
+            if (lane == 0) {
+                const int target = min(t + kPublish, w);
+                int spins = 0;
+                for (;;) {
+                    got = vprog[band - 1];
+                    if (got >= target) break;
+                    if (++spins > spin_limit || *(volatile int*)err) {
+                        atomicExch(err, 1);
+                        got = -1;
+                        break;
+                    }
+                    __nanosleep(128);
+                }
+                __threadfence();
+            }
+            got = __shfl_sync(0xffffffffu, got, 0);
+            if (got < 0) {
+                abort = true;
+                break;
+            }
+            ready = got;
+        }
+        asm volatile("cp.async.wait_group %0;\n" ::"n"(kRing - 1) : "memory");
+        const float up_lane = __shfl_up_sync(0xffffffffu, prev, 1);
+        const int u = t - lane;
+        if (row_ok && u >= 0 && u < w) {
+            const RStep st = s_ring[t % kRing][lane];
+            float val = st.cur;
+            if (st.upd & 1) {
+                const int x = fwd ? u : w - 1 - u;
+                const int y = fwd ? v : h - 1 - v;
+                const int lo = (int)(short)(st.range & 0xFFFF), hi = st.range >> 16;
+                const int d_cur = (int)(short)(st.d_pack & 0xFFFF), d_draw = st.d_pack >> 16;
+                const bool has_cur = (st.upd & 2) != 0, has_draw = (st.upd & 4) != 0;
+                const RPack<C64> l = s_lpk[t % kRing][lane];
+                // dynamic candidates: left (forward) / right (backward) and up / down
+                float left = -1.f, up = -1.f;
+                if (u > 0) left = prev;
+                if (v > 0) up = lane > 0 ? up_lane : __ldcg(work + (fwd ? y - 1 : y + 1) * w + x);
+                const bool has_l = left >= 0.f, has_u = up >= 0.f;
+                const int dl = has_l ? min(max((int)roundf(left), lo), hi - 1) : 0;
+                const int du = has_u ? min(max((int)roundf(up), lo), hi - 1) : 0;
+                const float cl = has_l ? cand_cost<C64>(c, s_lut, l, rp, x, y, dl, lo, hi) : 0.f;
+                const float cu = has_u ? cand_cost<C64>(c, s_lut, l, rp, x, y, du, lo, hi) : 0.f;
+                // the reference's order: cur, left, up, cur + draw; the first strict minimum wins
+                float best_c = 1e9f;
+                int best_d = st.cur >= 0.f ? d_cur : lo;
+                if (has_cur && st.c_cur < best_c) { best_c = st.c_cur; best_d = d_cur; }
+                if (has_l && cl < best_c) { best_c = cl; best_d = dl; }
+                if (has_u && cu < best_c) { best_c = cu; best_d = du; }
+                if (has_draw && st.c_draw < best_c) { best_c = st.c_draw; best_d = d_draw; }
+                val = (float)best_d;
+                work[y * w + x] = val;
+            }
+            prev = val;
+        }
+        // the slot just read is refilled only after its record was copied out above
+        __syncwarp();
+        issue(t + kRing);
+        // publish how far the band's last row is final (lane 31 is at column t - 31)
+        if ((t % kPublish) == kPublish - 1 && lane == kBand - 1) {
+            __threadfence();
+            vprog[band] = max(0, min(t - (kBand - 1) + 1, w));
+        }
+    }
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    __syncwarp();
+    if (lane == kBand - 1) {
+        __threadfence();
+        vprog[band] = w;  // the whole band is final (or the pass was abandoned: let the next band finish)
+    }
+}
+
+// ---- host: the engine stream, its draw values and rejected indices per radius
+
+struct DrawTable {
+    std::vector<int16_t> value;
+    std::vector<unsigned> rejected;
+};
+
+std::mutex g_rng_mu;
+std::vector<uint32_t> g_raw;          // std::mt19937(12345) outputs, generated on demand
+std::mt19937 g_engine(12345);
+std::map<int, DrawTable> g_tables;   // by radius
+
+// A generator that replays recorded engine outputs, counting how many the distribution takes.
+struct Replay {
+    using result_type = std::mt19937::result_type;
+    const uint32_t* p;
+    int calls = 0;
+    static constexpr result_type min() { return std::mt19937::min(); }
+    static constexpr result_type max() { return std::mt19937::max(); }
+    result_type operator()() { return p[calls++]; }
+};
+
+const DrawTable& draw_table_locked(int radius, size_t length) {
+    while (g_raw.size() < length + 64) g_raw.push_back((uint32_t)g_engine());
+    DrawTable& t = g_tables[radius];
+    std::uniform_int_distribution<int> dist(-radius, radius);
+    for (size_t i = t.value.size(); i < length; ++i) {
+        Replay g{g_raw.data() + i};
+        const int v = dist(g);
+        t.value.push_back((int16_t)v);
+        if (g.calls != 1) t.rejected.push_back((unsigned)i);  // output i is skipped by the distribution
+    }
+    return t;
 }
 
 }  // namespace
@@ -94,7 +359,60 @@ size_t refine_scan_temp_bytes(int n) {
     return bytes;
 }
 
-cudaError_t launch_refine_count(const Layout& L, unsigned char* arena, const float* work, int fwd, int* d_count,
+int refine_band_count(int h) { return (h + kBand - 1) / kBand; }
+
+int RefineTables::build(int iterations, int base_radius, int n) {
+    release();
+    std::vector<const DrawTable*> tabs(iterations);
+    std::vector<size_t> len(iterations);
+    {
+        std::lock_guard<std::mutex> lk(g_rng_mu);
+        for (int it = 0; it < iterations; ++it) {
+            const int radius = std::max(1, base_radius >> it);
+            if (radius > 32767) return 1;
+            // pass `it` starts at most it * n outputs (plus rejections) into the stream
+            len[it] = (size_t)(it + 1) * n + 64;
+            tabs[it] = &draw_table_locked(radius, len[it]);
+            if (tabs[it]->rejected.size() > (size_t)kMaxRejected) return 1;
+        }
+    }
+    iters = iterations;
+    size_t total = 0;
+    for (int it = 0; it < iterations; ++it) total += len[it] * 2 + kMaxRejected * 4 + 256;
+    if (cudaMalloc(&dev, total) != cudaSuccess) {
+        cudaGetLastError();
+        dev = nullptr;
+        return 1;
+    }
+    bytes = total;
+    unsigned char* p = static_cast<unsigned char*>(dev);
+    for (int it = 0; it < iterations; ++it) {
+        const DrawTable& t = *tabs[it];
+        value[it] = reinterpret_cast<int16_t*>(p);
+        if (cudaMemcpy(p, t.value.data(), len[it] * 2, cudaMemcpyHostToDevice) != cudaSuccess) return 1;
+        p += (len[it] * 2 + 255) & ~size_t(255);
+        rejected[it] = reinterpret_cast<unsigned*>(p);
+        size_t nr = 0;
+        for (unsigned r : t.rejected)
+            if (r < len[it]) ++nr;
+        nrej[it] = (int)nr;
+        if (nr && cudaMemcpy(p, t.rejected.data(), nr * 4, cudaMemcpyHostToDevice) != cudaSuccess) return 1;
+        p += kMaxRejected * 4;
+    }
+    n_built = n;
+    radius_built = base_radius;
+    return 0;
+}
+
+void RefineTables::release() {
+    if (dev) cudaFree(dev);
+    dev = nullptr;
+    bytes = 0;
+    iters = 0;
+    n_built = 0;
+}
+
+cudaError_t launch_refine_count(const Layout& L, unsigned char* arena, const float* work, int fwd,
                                 cudaStream_t s, unsigned* launches) {
     const int n = L.w * L.h;
     int* flags = reinterpret_cast<int*>(arena + L.rf_prefix);
@@ -104,27 +422,71 @@ cudaError_t launch_refine_count(const Layout& L, unsigned char* arena, const flo
                                                 reinterpret_cast<const int16_t*>(arena + L.rmax), work, fwd, flags);
     size_t tmp = L.rf_scan_tmp_bytes;
     cudaError_t e = cub::DeviceScan::ExclusiveSum(arena + L.rf_scan_tmp, tmp, flags, flags, n + 1, s);
+    *launches += 2;
     if (e != cudaSuccess) return e;
-    copy_total_kernel<<<1, 1, 0, s>>>(flags, n, d_count);
-    *launches += 3;
     return cudaGetLastError();
 }
 
-cudaError_t launch_refine_pass(const apg_pipeline_config_t& cfg, const CostCtx& c, const Layout& L,
-                               unsigned char* arena, float* work, int fwd, cudaStream_t s, unsigned* launches) {
-    (void)cfg;
-    const int ntu = (L.w + kTile - 1) / kTile, ntv = (L.h + kTile - 1) / kTile;
-    const uint8_t* rel = reinterpret_cast<const uint8_t*>(arena + L.reliable);
-    const int* prefix = reinterpret_cast<const int*>(arena + L.rf_prefix);
-    const int* draws = reinterpret_cast<const int*>(arena + L.rf_draws);
-    for (int dg = 0; dg < ntu + ntv - 1; ++dg) {
-        const int tu_min = max(0, dg - (ntv - 1)), tu_max = min(ntu - 1, dg);
-        const int nb = tu_max - tu_min + 1;
-        if (c.census64) refine_tile_kernel<true><<<nb, 32, 0, s>>>(c, fwd, dg, ntv, rel, prefix, draws, work);
-        else refine_tile_kernel<false><<<nb, 32, 0, s>>>(c, fwd, dg, ntv, rel, prefix, draws, work);
-        ++*launches;
-    }
+cudaError_t launch_refine_pack(const CostCtx& c, const Layout& L, unsigned char* arena, cudaStream_t s,
+                               unsigned* launches) {
+    const int n = L.w * L.h;
+    const int blocks = min((n + 255) / 256, 148 * 8);
+    if (c.census64)
+        refine_pack_kernel<true><<<blocks, 256, 0, s>>>(c, reinterpret_cast<RPack<true>*>(arena + L.rf_pack),
+                                                        reinterpret_cast<RPack<true>*>(arena + L.rf_pack) + n);
+    else
+        refine_pack_kernel<false><<<blocks, 256, 0, s>>>(c, reinterpret_cast<RPack<false>*>(arena + L.rf_pack),
+                                                         reinterpret_cast<RPack<false>*>(arena + L.rf_pack) + n);
+    ++*launches;
     return cudaGetLastError();
 }
+
+size_t refine_pack_bytes(int n, bool c64) { return (size_t)n * 2 * (c64 ? sizeof(RPack<true>) : sizeof(RPack<false>)); }
+
+cudaError_t launch_refine_pass(const CostCtx& c, const Layout& L, unsigned char* arena, const RefineTables& tab,
+                               int it, float* work, cudaStream_t s, unsigned* launches) {
+    const int fwd = (it % 2) == 0;
+    const int n = L.w * L.h;
+    const int nbands = refine_band_count(L.h);
+    const uint8_t* rel = reinterpret_cast<const uint8_t*>(arena + L.reliable);
+    const int* prefix = reinterpret_cast<const int*>(arena + L.rf_prefix);
+    unsigned* P = reinterpret_cast<unsigned*>(arena + L.rf_state);
+    int* err = reinterpret_cast<int*>(arena + L.rf_state) + kRefineErrWord;
+    int* progress = reinterpret_cast<int*>(arena + L.rf_state) + kRefineProgWord;
+    RStep* steps = reinterpret_cast<RStep*>(arena + L.rf_steps);
+    const int blocks = min((n + 255) / 256, 148 * 8);
+    if (c.census64) {
+        const RPack<true>* lpk = reinterpret_cast<const RPack<true>*>(arena + L.rf_pack);
+        refine_prep_kernel<true><<<blocks, 256, 0, s>>>(c, fwd, rel, prefix, tab.value[it], tab.rejected[it], tab.nrej[it],
+                                                        P + it, lpk, lpk + n, work, steps);
+    } else {
+        const RPack<false>* lpk = reinterpret_cast<const RPack<false>*>(arena + L.rf_pack);
+        refine_prep_kernel<false><<<blocks, 256, 0, s>>>(c, fwd, rel, prefix, tab.value[it], tab.rejected[it],
+                                                         tab.nrej[it], P + it, lpk, lpk + n, work, steps);
+    }
+    ++*launches;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    // about a second of waiting at most per wait (spins of ~128 ns sleep plus the poll)
+    int spin_limit = 1 << 23;
+    CostCtx cc = c;
+    const void* lpk = arena + L.rf_pack;
+    const void* rpk = c.census64 ? (const void*)(reinterpret_cast<const RPack<true>*>(lpk) + n)
+                                 : (const void*)(reinterpret_cast<const RPack<false>*>(lpk) + n);
+    const RStep* csteps = steps;
+    int fwd_arg = fwd;
+    void* args[] = {&cc, &fwd_arg, (void*)&csteps, (void*)&lpk, (void*)&rpk, &work, &progress, &err, &spin_limit};
+    const void* kern = c.census64 ? (const void*)refine_band_kernel<true> : (const void*)refine_band_kernel<false>;
+    e = cudaLaunchCooperativeKernel(kern, dim3(nbands), dim3(kBand), args, 0, s);
+    if (e != cudaSuccess) return e;
+    ++*launches;
+    // start of the next pass, and cleared progress counters
+    const int* count = prefix + n;
+    refine_advance_kernel<<<1, 64, 0, s>>>(P, it, count, tab.rejected[it], tab.nrej[it], progress, nbands);
+    ++*launches;
+    return cudaGetLastError();
+}
+
+size_t refine_steps_bytes(int n) { return (size_t)n * sizeof(RStep); }
 
 }  // namespace apgcu

@@ -42,6 +42,12 @@ def _cases():
         ("column_1x33", B, (1, 33, 16, 0), "noise", {}, 0),
         ("pixel_1x1", F, (1, 1, 16, 0), "noise", {}, 0),
         ("hq_d256_300x100", H, (300, 100, 256, 0), "synth_patch", {}, 0),
+        # refiner wavefront edges: a one-row last band, fewer columns than lanes, a negative range,
+        # more passes with a wider random radius
+        ("hq_band_edges_70x33", H, (70, 33, 24, 0), "synth_patch", {}, 0),
+        ("hq_narrow_20x70", H, (20, 70, 16, 0), "synth_patch", {}, 0),
+        ("hq_negative_range_64x48", H, (64, 48, 8, -8), "noise", {}, 0),
+        ("hq_refine_5iter_r7", H, (96, 64, 32, 0), "synth_patch", {"refine_iterations": 5, "refine_random_radius": 7}, 0),
     ]
 
 
