@@ -38,6 +38,7 @@ namespace {
 
 constexpr int kBand = 32;
 constexpr int kPublish = 8;      // steps between progress publications
+constexpr int kUpBatch = 16;     // columns of the row above a band read at once
 constexpr int kMaxRejected = 64;  // rejected outputs tabulated per radius (expected: none)
 
 __global__ void refine_flags_kernel(int w, int h, const uint8_t* __restrict__ reliable, const int16_t* __restrict__ rmin,
@@ -189,6 +190,11 @@ __global__ void refine_prep_kernel(CostCtx c, int fwd, const uint8_t* __restrict
 }
 
 constexpr int kRing = 16;  // steps of pixel records in flight per lane
+constexpr int kAhead = 32; // steps ahead the right-image window is prefetched into L1
+
+__device__ __forceinline__ void prefetch_l1(const void* p) {
+    asm volatile("prefetch.global.L1 [%0];\n" ::"l"(p));
+}
 
 __device__ __forceinline__ void cp16(void* dst, const void* src) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
@@ -236,15 +242,35 @@ __global__ void __launch_bounds__(32) refine_band_kernel(CostCtx c, int fwd, con
     };
 #pragma unroll 1
     for (int t = 0; t < kRing; ++t) issue(t);
+    // the right-image window a lane reads (its row, [x - dmax + 1, x - d0]) slides by one pixel
+    // per step; every lane misses L1 at a different step and the warp waits for the slowest, so
+    // the window's first kAhead steps are prefetched now and its entering edge kAhead steps ahead
+    const int d0 = c.d0, dmax = c.d0 + c.D;
+    const int yrow = fwd ? v : h - 1 - v;
+    const RPack<C64>* rrow = rp + (size_t)(row_ok ? yrow : 0) * w;
+    auto edge = [&](int u) {  // the window pixel entering at column u
+        const int x = fwd ? u : w - 1 - u;
+        return fwd ? x - d0 : x - dmax + 1;
+    };
+    if (row_ok) {
+        for (int k = -c.D; k <= kAhead; k += 8) {
+            const int xr = min(max(edge(k), 0), w - 1);
+            prefetch_l1(rrow + xr);
+        }
+    }
     float prev = -1.f;  // value of this lane's previous column (its left neighbour)
-    int ready = band == 0 ? w : 0;  // columns of the row above the band known final
+    // values of the row above the band for columns [up_base, up_base + kUpBatch): lane k holds
+    // column up_base + k, read together once the band above has published them
+    int up_base = -kUpBatch;
+    float up_vals = -1.f;
+    const int y_above = band > 0 ? (fwd ? band * kBand - 1 : h - band * kBand) : 0;
     bool abort = false;
     for (int t = 0; t < w + kBand - 1 && !abort; ++t) {
-        if (ready < min(t + 1, w)) {
-            // lane 0 waits until the band above has finished its last row up to column t + kPublish
+        if (band > 0 && t < w && t >= up_base + kUpBatch) {
+            // lane 0 waits until the band above has finished its last row up to column t + kUpBatch
             int got = 0;
             if (lane == 0) {
-                const int target = min(t + kPublish, w);
+                const int target = min(t + kUpBatch, w);
                 int spins = 0;
                 for (;;) {
                     got = vprog[band - 1];
@@ -254,18 +280,22 @@ __global__ void __launch_bounds__(32) refine_band_kernel(CostCtx c, int fwd, con
                         got = -1;
                         break;
                     }
-                    __nanosleep(128);
+                    __nanosleep(64);
                 }
-                __threadfence();
             }
             got = __shfl_sync(0xffffffffu, got, 0);
             if (got < 0) {
                 abort = true;
                 break;
             }
-            ready = got;
+            __threadfence();
+            up_base = t;
+            const int col = t + lane;
+            up_vals = (lane < kUpBatch && col < w) ? __ldcg(work + y_above * w + (fwd ? col : w - 1 - col)) : -1.f;
         }
+        const float up_first = __shfl_sync(0xffffffffu, up_vals, (t - up_base) & 31);
         asm volatile("cp.async.wait_group %0;\n" ::"n"(kRing - 1) : "memory");
+        if (row_ok) prefetch_l1(rrow + min(max(edge(t - lane + kAhead), 0), w - 1));
         const float up_lane = __shfl_up_sync(0xffffffffu, prev, 1);
         const int u = t - lane;
         if (row_ok && u >= 0 && u < w) {
@@ -281,7 +311,7 @@ __global__ void __launch_bounds__(32) refine_band_kernel(CostCtx c, int fwd, con
                 // dynamic candidates: left (forward) / right (backward) and up / down
                 float left = -1.f, up = -1.f;
                 if (u > 0) left = prev;
-                if (v > 0) up = lane > 0 ? up_lane : __ldcg(work + (fwd ? y - 1 : y + 1) * w + x);
+                if (v > 0) up = lane > 0 ? up_lane : up_first;
                 const bool has_l = left >= 0.f, has_u = up >= 0.f;
                 const int dl = has_l ? min(max((int)roundf(left), lo), hi - 1) : 0;
                 const int du = has_u ? min(max((int)roundf(up), lo), hi - 1) : 0;
