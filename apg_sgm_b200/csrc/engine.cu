@@ -199,6 +199,9 @@ Engine::Engine(const apg_pipeline_config_t& cfg, int device, cudaStream_t stream
 
 Engine::~Engine() {
     release();
+    if (copy_stream_) cudaStreamDestroy(copy_stream_);
+    if (ev_maps_) cudaEventDestroy(ev_maps_);
+    if (ev_copied_) cudaEventDestroy(ev_copied_);
     if (refine_err_host_) cudaFreeHost(refine_err_host_);
     for (auto& e : ev_) if (e) cudaEventDestroy(e);
     for (auto& e : pev_) if (e) cudaEventDestroy(e);
@@ -308,23 +311,44 @@ int Engine::process_host(const uint8_t* left, const uint8_t* right, int w, int h
     uint8_t* preason = outputs_pinned ? reason : reinterpret_cast<uint8_t*>(pconf + n);
     uint8_t* prel = outputs_pinned ? reliable : preason + n;
     const size_t row = (size_t)w * ch;
-    for (int y = 0; y < h; ++y) {
-        std::memcpy(pl + y * row, left + (size_t)y * stride, row);
-        std::memcpy(pr + y * row, right + (size_t)y * stride, row);
+    if (!copy_stream_) {
+        if (cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&ev_maps_, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&ev_copied_, cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(kInternalError, "copy stream creation failed");
+        }
     }
+    // the left image goes up while the right one is staged
+    for (int y = 0; y < h; ++y) std::memcpy(pl + y * row, left + (size_t)y * stride, row);
     cudaError_t e = cudaMemcpyAsync(ptr<uint8_t>(lay_.in_left), pl, in_bytes, cudaMemcpyHostToDevice, stream_);
+    for (int y = 0; y < h; ++y) std::memcpy(pr + y * row, right + (size_t)y * stride, row);
     if (e == cudaSuccess) e = cudaMemcpyAsync(ptr<uint8_t>(lay_.in_right), pr, in_bytes, cudaMemcpyHostToDevice, stream_);
     if (e != cudaSuccess) return cuda_fail(e, "input upload");
+    early_conf_ = pconf;
+    early_rel_ = prel;
+    early_reason_ = preason;
+    early_issued_ = early_reason_done_ = false;
     rc = run(ptr<uint8_t>(lay_.in_left), (int)row, ptr<uint8_t>(lay_.in_right), (int)row, ch, nullptr, nullptr, nullptr,
              nullptr);
-    if (rc) return rc;
+    early_conf_ = nullptr;
+    early_rel_ = nullptr;
+    early_reason_ = nullptr;
+    if (rc) {
+        cudaStreamSynchronize(copy_stream_);
+        return rc;
+    }
     e = cudaSuccess;
     if (pdisp) e = cudaMemcpyAsync(pdisp, ptr<float>(lay_.disp_out), n * 4, cudaMemcpyDeviceToHost, stream_);
-    if (e == cudaSuccess && pconf) e = cudaMemcpyAsync(pconf, ptr<float>(lay_.confidence), n * 4, cudaMemcpyDeviceToHost, stream_);
-    if (e == cudaSuccess && preason) e = cudaMemcpyAsync(preason, ptr<uint8_t>(lay_.reason), n, cudaMemcpyDeviceToHost, stream_);
-    if (e == cudaSuccess && prel) e = cudaMemcpyAsync(prel, ptr<uint8_t>(lay_.reliable), n, cudaMemcpyDeviceToHost, stream_);
+    if (e == cudaSuccess && pconf && !early_issued_)
+        e = cudaMemcpyAsync(pconf, ptr<float>(lay_.confidence), n * 4, cudaMemcpyDeviceToHost, stream_);
+    if (e == cudaSuccess && preason && !early_reason_done_)
+        e = cudaMemcpyAsync(preason, ptr<uint8_t>(lay_.reason), n, cudaMemcpyDeviceToHost, stream_);
+    if (e == cudaSuccess && prel && !early_issued_)
+        e = cudaMemcpyAsync(prel, ptr<uint8_t>(lay_.reliable), n, cudaMemcpyDeviceToHost, stream_);
     if (e == cudaSuccess) e = cudaMemcpyAsync(counts_, ptr<unsigned long long>(lay_.stats), sizeof(counts_),
                                               cudaMemcpyDeviceToHost, stream_);
+    if (e == cudaSuccess && early_issued_) e = cudaStreamWaitEvent(stream_, ev_copied_, 0);
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
     if (e != cudaSuccess) return cuda_fail(e, "output download");
     rc = check_refine();
@@ -608,6 +632,21 @@ int Engine::run_post(float* d_disp, float* d_conf, uint8_t* d_reason, uint8_t* d
     ca.disp_out = ptr<float>(L.disp_lr);
     RUN(launch_conf_lr(ca, s), "confidence");
     if (debug_) RUNC(cudaMemcpyAsync(ptr<uint8_t>(L.reason_conf), ptr<uint8_t>(L.reason), n, cudaMemcpyDeviceToDevice, s), "dbg");
+    if (early_conf_ || early_rel_ || early_reason_) {
+        // maps that no later stage writes go to the host now, beside fill / median / counters
+        RUNC(cudaEventRecord(ev_maps_, s), "event");
+        RUNC(cudaStreamWaitEvent(copy_stream_, ev_maps_, 0), "event");
+        if (early_conf_)
+            RUNC(cudaMemcpyAsync(early_conf_, ptr<float>(L.confidence), n * 4, cudaMemcpyDeviceToHost, copy_stream_), "conf out");
+        if (early_rel_)
+            RUNC(cudaMemcpyAsync(early_rel_, ptr<uint8_t>(L.reliable), n, cudaMemcpyDeviceToHost, copy_stream_), "rel out");
+        if (early_reason_ && !refine) {
+            RUNC(cudaMemcpyAsync(early_reason_, ptr<uint8_t>(L.reason), n, cudaMemcpyDeviceToHost, copy_stream_), "reason out");
+            early_reason_done_ = true;
+        }
+        RUNC(cudaEventRecord(ev_copied_, copy_stream_), "event");
+        early_issued_ = true;
+    }
     cudaEventRecord(ev_[7], s);
     const float* post_in = ptr<float>(L.disp_lr);
     if (refine) {

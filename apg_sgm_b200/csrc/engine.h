@@ -170,6 +170,14 @@ private:
     unsigned long long counts_[8] = {};  // frame counters copied with the host outputs
     const uint32_t* sgm_src_ = nullptr;  // volume the SGM sweeps read (set by run_pre)
     RefineTables rtab_;                   // refine draw tables (HighQuality)
+    // host path: confidence / reliability (and reason, without refine) are final after the
+    // confidence kernel; their device-to-host copies run on copy_stream_ while the rest finishes
+    cudaStream_t copy_stream_ = nullptr;
+    cudaEvent_t ev_maps_ = nullptr, ev_copied_ = nullptr;
+    float* early_conf_ = nullptr;
+    uint8_t* early_reason_ = nullptr;
+    uint8_t* early_rel_ = nullptr;
+    bool early_issued_ = false, early_reason_done_ = false;
     int* refine_err_host_ = nullptr;      // pinned copy of the refine error flag
     bool refine_pending_ = false;
     bool counts_fresh_ = false;
