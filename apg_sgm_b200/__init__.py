@@ -500,6 +500,21 @@ __all__ = ["QualityMode", "VolumeBackend", "MemoryPolicy", "StatusCode", "Invali
            "kernel_launch_count", "workspace_bytes", "__version__"]
 
 
+
+_OUT_DTYPES = {"disparity": np.float32, "confidence": np.float32, "invalid_reason": np.uint8,
+               "reliable_mask": np.uint8}
+
+
+def _result_arrays(h: int, w: int, out=None) -> dict:
+    """The four result maps of one pair: `out` (caller-owned, checked) or fresh arrays."""
+    if out is None:
+        return {k: np.empty((h, w), dt) for k, dt in _OUT_DTYPES.items()}
+    for k, dt in _OUT_DTYPES.items():
+        a = out[k]
+        if a.shape != (h, w) or a.dtype != dt or not a.flags.c_contiguous or not a.flags.writeable:
+            raise ValueError(f"out[{k!r}] must be a writeable C-contiguous {np.dtype(dt).name} array of shape {(h, w)}")
+    return out
+
 class Batch:
     """Batched form (apgcu_batch_*): many pairs of uneven sizes and disparity ranges per call.
 
@@ -522,9 +537,11 @@ class Batch:
         if lib().apgcu_batch_set_option(self._h, key.encode(), int(value)) != 0:
             raise ValueError(f"invalid batch option {key}={value}")
 
-    def process(self, pairs) -> list:
+    def process(self, pairs, out=None) -> list:
         """pairs: iterable of (left, right) or (left, right, max_disparity) host arrays.  Returns one
-        dict of disparity / confidence / invalid_reason / reliable_mask per pair."""
+        dict of disparity / confidence / invalid_reason / reliable_mask per pair: `out[i]` when a
+        list of caller-owned dicts is given (page-locked ones take the device copies directly),
+        else new arrays."""
         keep, outs = [], []
         arr = (_lib_mod.Pair * len(pairs))()
         for i, p in enumerate(pairs):
@@ -536,8 +553,7 @@ class Batch:
                 la, ra = np.ascontiguousarray(la), np.ascontiguousarray(ra)
                 lv, rv = _image_view(la, "left")[0], _image_view(ra, "right")[0]
             h, w = lv.height, lv.width
-            o = {"disparity": np.empty((h, w), np.float32), "confidence": np.empty((h, w), np.float32),
-                 "invalid_reason": np.empty((h, w), np.uint8), "reliable_mask": np.empty((h, w), np.uint8)}
+            o = _result_arrays(h, w, out[i] if out is not None else None)
             keep += [la, ra]
             outs.append(o)
             arr[i] = _lib_mod.Pair(lv.data, rv.data, w, h, lv.stride, lv.channels, dmax,
@@ -600,17 +616,17 @@ class Server:
         self._pending = {}
 
     def submit(self, left, right, mode=QualityMode.Balanced, max_disparity=128, min_disparity=0,
-               outputs: bool = True) -> int:
+               outputs: bool = True, out: dict = None) -> int:
+        """Queues one pair; `out` (optional) holds caller-owned C-contiguous result arrays (disparity and
+        confidence float32, invalid_reason and reliable_mask uint8, each height x width) that the
+        request writes instead of new ones.  They must stay alive and untouched until wait()."""
         lv, la = _image_view(left, "left")
         rv, ra = _image_view(right, "right")
         if lv.stride != rv.stride:
             la, ra = np.ascontiguousarray(la), np.ascontiguousarray(ra)
             lv, rv = _image_view(la, "left")[0], _image_view(ra, "right")[0]
         h, w = lv.height, lv.width
-        o = None
-        if outputs:
-            o = {"disparity": np.empty((h, w), np.float32), "confidence": np.empty((h, w), np.float32),
-                 "invalid_reason": np.empty((h, w), np.uint8), "reliable_mask": np.empty((h, w), np.uint8)}
+        o = _result_arrays(h, w, out) if (out is not None or outputs) else None
         ptr = (lambda k: o[k].ctypes.data) if o else (lambda k: None)
         req = _lib_mod.Request(int(_MODE_VALUE.get(mode, mode)), int(min_disparity), int(max_disparity),
                                lv.data, rv.data, w, h, lv.stride, lv.channels, ptr("disparity"), ptr("confidence"),
@@ -629,6 +645,16 @@ class Server:
         if rc != 0:
             raise RuntimeError(f"request failed [{rc}]: {lib().apgcu_server_last_error(self._h).decode()}")
         return o, lat.value
+
+    def reserve(self, width: int, height: int, mode=QualityMode.Balanced, max_disparity=128, min_disparity=0,
+                channels: int = 1, count: int = 1):
+        """Warm pool: `count` idle device-resident engines for requests of this mode, size and range."""
+        req = _lib_mod.Request(int(_MODE_VALUE.get(mode, mode)), int(min_disparity), int(max_disparity), None, None,
+                               int(width), int(height), int(width) * int(channels), int(channels),
+                               None, None, None, None)
+        rc = lib().apgcu_server_reserve(self._h, C.byref(req), int(count))
+        if rc != 0:
+            raise RuntimeError(f"reserve failed [{rc}]")
 
     def stats(self) -> dict:
         c = (C.c_ulonglong * 4)()

@@ -133,6 +133,7 @@ _SIGS = {
     "apgcu_server_wait": (C.c_int, [C.c_void_p, C.c_ulonglong, C.POINTER(C.c_double)]),
     "apgcu_server_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_ulonglong), C.POINTER(C.c_size_t)]),
     "apgcu_server_budget": (C.c_size_t, [C.c_void_p]),
+    "apgcu_server_reserve": (C.c_int, [C.c_void_p, C.POINTER(Request), C.c_int]),
     "apgcu_server_last_error": (C.c_char_p, [C.c_void_p]),
     "apgcu_right_wta_noalloc": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                           C.c_void_p, C.c_void_p]),

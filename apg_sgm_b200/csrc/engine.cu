@@ -285,6 +285,18 @@ int Engine::prepare(int w, int h, int ch) {
     return kOk;
 }
 
+// True when p lies in page-locked host memory (cudaMallocHost / cudaHostAlloc / cudaHostRegister),
+// which the copy engines read and write directly.
+static bool host_pinned(const void* p) {
+    if (!p) return false;
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
 int Engine::process_host(const uint8_t* left, const uint8_t* right, int w, int h, int stride, int ch, float* disp,
                          float* conf, uint8_t* reason, uint8_t* reliable, bool outputs_pinned) {
     cudaSetDevice(device_);
@@ -292,9 +304,14 @@ int Engine::process_host(const uint8_t* left, const uint8_t* right, int w, int h
     if (rc) return rc;
     const size_t n = (size_t)w * h;
     const size_t in_bytes = n * ch;
+    // page-locked caller buffers skip the staging copies: inputs go up by DMA from where they lie,
+    // results come down into the caller's arrays
+    const bool inputs_pinned = host_pinned(left) && host_pinned(right);
+    if (!outputs_pinned)
+        outputs_pinned = host_pinned(disp) && host_pinned(conf) && host_pinned(reason) && host_pinned(reliable);
     const size_t out_bytes = outputs_pinned ? 0 : n * 4 * 2 + n * 2;
-    const size_t need = 2 * in_bytes + out_bytes;
-    if (!pin_ || pinned_bytes_ < need) {
+    const size_t need = (inputs_pinned ? 0 : 2 * in_bytes) + out_bytes;
+    if (need && (!pin_ || pinned_bytes_ < need)) {
         if (pin_) cudaFreeHost(pin_);
         pin_ = nullptr;
         pinned_bytes_ = 0;
@@ -304,9 +321,10 @@ int Engine::process_host(const uint8_t* left, const uint8_t* right, int w, int h
         }
         pinned_bytes_ = need;
     }
-    unsigned char* pl = pin_;
-    unsigned char* pr = pin_ + in_bytes;
-    float* pdisp = outputs_pinned ? disp : reinterpret_cast<float*>(pin_ + 2 * in_bytes);
+    unsigned char* pl = inputs_pinned ? nullptr : pin_;
+    unsigned char* pr = inputs_pinned ? nullptr : pin_ + in_bytes;
+    unsigned char* pout = inputs_pinned ? pin_ : pin_ + 2 * in_bytes;
+    float* pdisp = outputs_pinned ? disp : reinterpret_cast<float*>(pout);
     float* pconf = outputs_pinned ? conf : pdisp + n;
     uint8_t* preason = outputs_pinned ? reason : reinterpret_cast<uint8_t*>(pconf + n);
     uint8_t* prel = outputs_pinned ? reliable : preason + n;
@@ -319,11 +337,20 @@ int Engine::process_host(const uint8_t* left, const uint8_t* right, int w, int h
             return fail(kInternalError, "copy stream creation failed");
         }
     }
-    // the left image goes up while the right one is staged
-    for (int y = 0; y < h; ++y) std::memcpy(pl + y * row, left + (size_t)y * stride, row);
-    cudaError_t e = cudaMemcpyAsync(ptr<uint8_t>(lay_.in_left), pl, in_bytes, cudaMemcpyHostToDevice, stream_);
-    for (int y = 0; y < h; ++y) std::memcpy(pr + y * row, right + (size_t)y * stride, row);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(ptr<uint8_t>(lay_.in_right), pr, in_bytes, cudaMemcpyHostToDevice, stream_);
+    cudaError_t e;
+    if (inputs_pinned) {
+        e = cudaMemcpy2DAsync(ptr<uint8_t>(lay_.in_left), row, left, stride, row, h, cudaMemcpyHostToDevice, stream_);
+        if (e == cudaSuccess)
+            e = cudaMemcpy2DAsync(ptr<uint8_t>(lay_.in_right), row, right, stride, row, h, cudaMemcpyHostToDevice,
+                                  stream_);
+    } else {
+        // the left image goes up while the right one is staged
+        for (int y = 0; y < h; ++y) std::memcpy(pl + y * row, left + (size_t)y * stride, row);
+        e = cudaMemcpyAsync(ptr<uint8_t>(lay_.in_left), pl, in_bytes, cudaMemcpyHostToDevice, stream_);
+        for (int y = 0; y < h; ++y) std::memcpy(pr + y * row, right + (size_t)y * stride, row);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(ptr<uint8_t>(lay_.in_right), pr, in_bytes, cudaMemcpyHostToDevice, stream_);
+    }
     if (e != cudaSuccess) return cuda_fail(e, "input upload");
     early_conf_ = pconf;
     early_rel_ = prel;
@@ -527,6 +554,10 @@ int Engine::upload(const uint8_t* left, const uint8_t* right, int w, int h, int 
         e = cudaMemcpy2DAsync(ptr<uint8_t>(lay_.in_left), row, left, stride, row, h, cudaMemcpyDeviceToDevice, s);
         if (e == cudaSuccess)
             e = cudaMemcpy2DAsync(ptr<uint8_t>(lay_.in_right), row, right, stride, row, h, cudaMemcpyDeviceToDevice, s);
+    } else if (host_pinned(left) && host_pinned(right)) {
+        e = cudaMemcpy2DAsync(ptr<uint8_t>(lay_.in_left), row, left, stride, row, h, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess)
+            e = cudaMemcpy2DAsync(ptr<uint8_t>(lay_.in_right), row, right, stride, row, h, cudaMemcpyHostToDevice, s);
     } else {
         rc = ensure_pinned(2 * in_bytes + n * 10 + 64);
         if (rc) return rc;
@@ -553,12 +584,17 @@ int Engine::download(float* disp, float* conf, uint8_t* reason, uint8_t* reliabl
     const size_t n = (size_t)lay_.w * lay_.h;
     const size_t in_bytes = n * lay_.ch;
     const cudaMemcpyKind kind = device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
-    if (!device && (!pin_ || pinned_bytes_ < 2 * in_bytes + n * 10)) return fail(kInternalError, "no host staging");
-    unsigned char* st = device ? nullptr : pin_ + 2 * in_bytes;  // host staging: disparity, confidence, reason, reliable, counters
-    float* pd = device ? disp : reinterpret_cast<float*>(st);
-    float* pc = device ? conf : reinterpret_cast<float*>(st + n * 4);
-    uint8_t* pr = device ? reason : st + n * 8;
-    uint8_t* pm = device ? reliable : st + n * 9;
+    // page-locked host outputs take the copies directly (finish_download then has nothing to do)
+    direct_out_ = device || (host_pinned(disp) && host_pinned(conf) && host_pinned(reason) && host_pinned(reliable));
+    if (!direct_out_) {
+        int rc = ensure_pinned(2 * in_bytes + n * 10 + 64);
+        if (rc) return rc;
+    }
+    unsigned char* st = direct_out_ ? nullptr : pin_ + 2 * in_bytes;  // host staging: disparity, confidence, reason, reliable
+    float* pd = direct_out_ ? disp : reinterpret_cast<float*>(st);
+    float* pc = direct_out_ ? conf : reinterpret_cast<float*>(st + n * 4);
+    uint8_t* pr = direct_out_ ? reason : st + n * 8;
+    uint8_t* pm = direct_out_ ? reliable : st + n * 9;
     cudaError_t e = cudaSuccess;
     if (disp) e = cudaMemcpyAsync(pd, ptr<float>(lay_.disp_out), n * 4, kind, s);
     if (e == cudaSuccess && conf) e = cudaMemcpyAsync(pc, ptr<float>(lay_.confidence), n * 4, kind, s);
@@ -568,6 +604,7 @@ int Engine::download(float* disp, float* conf, uint8_t* reason, uint8_t* reliabl
 }
 
 void Engine::finish_download(float* disp, float* conf, uint8_t* reason, uint8_t* reliable) const {
+    if (direct_out_) return;
     const size_t n = (size_t)lay_.w * lay_.h;
     const unsigned char* st = pin_ + 2 * n * lay_.ch;
     if (disp) std::memcpy(disp, st, n * 4);

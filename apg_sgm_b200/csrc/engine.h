@@ -151,6 +151,7 @@ private:
     // host staging (pinned)
     unsigned char* pin_ = nullptr;
     size_t pinned_bytes_ = 0;
+    bool direct_out_ = false;  // the last download() wrote the caller's page-locked (or device) outputs
     std::vector<float> lut_host_;
     std::vector<uint16_t> qlut_host_;
     cudaEvent_t ev_[12] = {};

@@ -130,6 +130,46 @@ public:
         }
     }
 
+    // Creates `count` idle engines for requests like `r` (its mode, size and range), each warmed by
+    // one blank pair (workspace, staging and tables allocated, kernels loaded), so that the first
+    // requests of a bucket do not pay for them.  Fails when the budget cannot hold them.
+    int reserve(const apgcu_request_t& r, int count) {
+        if (r.width <= 0 || r.height <= 0 || (r.channels != 1 && r.channels != 3 && r.channels != 4)) return kEmptyInput;
+        const apg_pipeline_config_t c = config_of(r);
+        std::string msg;
+        int rc = Engine::validate_config(c, msg);
+        if (rc) return rc;
+        const PoolKey k{r.mode, r.width, r.height, r.channels, c.min_disparity, c.max_disparity};
+        const size_t need = Engine::make_layout(c, k.w, k.h, k.ch, 0).total;
+        std::vector<uint8_t> blank((size_t)r.width * r.height * r.channels, 0);
+        for (int i = 0; i < count; ++i) {
+            {
+                std::lock_guard<std::mutex> lk(mu_);
+                if (reserved_ + need > budget_) return kResourceLimitExceeded;
+                reserved_ += need;
+                peak_reserved_ = std::max(peak_reserved_, reserved_);
+            }
+            Held h;
+            h.bytes = need;
+            cudaSetDevice(device_);
+            try {
+                h.eng = std::make_unique<Engine>(c, device_, nullptr);
+                rc = h.eng->process_host(blank.data(), blank.data(), r.width, r.height, r.width * r.channels,
+                                         r.channels, nullptr, nullptr, nullptr, nullptr);
+            } catch (...) {
+                rc = kAllocationFailure;
+            }
+            std::lock_guard<std::mutex> lk(mu_);
+            if (rc) {
+                reserved_ -= need;
+                return rc;
+            }
+            idle_[k].push_back(std::move(h));
+        }
+        cv_mem_.notify_all();
+        return kOk;
+    }
+
     size_t budget() const { return budget_; }
     std::string last_error() {
         std::lock_guard<std::mutex> lk(mu_);
@@ -313,6 +353,15 @@ APGCU_API int apgcu_server_stats(apgcu_server_t s, unsigned long long* counts4, 
 }
 
 APGCU_API size_t apgcu_server_budget(apgcu_server_t s) { return s ? s->s->budget() : 0; }
+
+APGCU_API int apgcu_server_reserve(apgcu_server_t s, const apgcu_request_t* like, int count) {
+    if (!s || !like) return APG_STATUS_INTERNAL_ERROR;
+    try {
+        return s->s->reserve(*like, count);
+    } catch (...) {
+        return APG_STATUS_INTERNAL_ERROR;
+    }
+}
 
 APGCU_API const char* apgcu_server_last_error(apgcu_server_t s) {
     static thread_local std::string tl;

@@ -191,6 +191,10 @@ APGCU_API int apgcu_server_wait(apgcu_server_t s, unsigned long long ticket, dou
  * bytes2 = {reserved workspace bytes now, peak reserved}. */
 APGCU_API int apgcu_server_stats(apgcu_server_t s, unsigned long long* counts4, size_t* bytes2);
 APGCU_API size_t apgcu_server_budget(apgcu_server_t s);
+/* Warm pool: creates `count` idle engines for requests like *like (its mode, size and range; the
+ * image pointers are not read), each run once on a blank pair, so that later requests of that
+ * bucket find device-resident workspaces.  Counts against the HBM budget. */
+APGCU_API int apgcu_server_reserve(apgcu_server_t s, const apgcu_request_t* like, int count);
 APGCU_API const char* apgcu_server_last_error(apgcu_server_t s);
 
 /* Right-image winner-take-all over a caller's cost volume, allocating nothing.

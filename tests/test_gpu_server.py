@@ -79,3 +79,50 @@ def test_served_request_beyond_budget_is_refused(apg):
     with pytest.raises(RuntimeError, match=r"\[6\].*budget"):
         srv.wait(t)
     srv.close()
+
+
+def test_served_warm_pool_matches(apg):
+    """Engines created ahead by reserve() (warmed on a blank pair) give the same results, and the
+    requests that find them allocate nothing more."""
+    pool = _pool()
+    want = _alone(apg, pool)
+    srv = apg.Server(slots=2)
+    for mode, dmax, L, _ in pool:
+        srv.reserve(L.shape[1], L.shape[0], mode=mode, max_disparity=dmax, count=2)
+    reserved = srv.stats()["reserved_bytes"]
+    order = np.random.default_rng(9).permutation(np.repeat(np.arange(len(pool)), 2))
+    tickets = [(i, srv.submit(pool[i][2], pool[i][3], mode=pool[i][0], max_disparity=pool[i][1])) for i in order]
+    for i, t in tickets:
+        o, _ = srv.wait(t)
+        for k in KEYS:
+            assert same_bits(o[k], want[i][k]), (i, k)
+    st = srv.stats()
+    assert st["reserved_bytes"] == reserved and st["evictions"] == 0
+    srv.close()
+
+
+def test_served_reserve_beyond_budget_is_refused(apg):
+    srv = apg.Server(slots=1, hbm_budget_gb=1e-3)
+    with pytest.raises(RuntimeError, match=r"\[6\]"):
+        srv.reserve(320, 240, mode=1, max_disparity=128)
+    srv.close()
+
+
+def test_served_into_caller_buffers(apg):
+    pool = _pool()[:3]
+    want = _alone(apg, pool)
+    srv = apg.Server(slots=2)
+    outs = []
+    for mode, dmax, L, R in pool:
+        h, w = L.shape
+        o = {"disparity": np.full((h, w), 7, np.float32), "confidence": np.full((h, w), 7, np.float32),
+             "invalid_reason": np.full((h, w), 7, np.uint8), "reliable_mask": np.full((h, w), 7, np.uint8)}
+        outs.append((o, srv.submit(L, R, mode=mode, max_disparity=dmax, out=o)))
+    for i, (o, t) in enumerate(outs):
+        got, _ = srv.wait(t)
+        assert got is o
+        for k in KEYS:
+            assert same_bits(o[k], want[i][k]), (i, k)
+    with pytest.raises(ValueError):
+        srv.submit(pool[0][2], pool[0][3], out={k: np.zeros((1, 1), np.float32) for k in KEYS})
+    srv.close()
