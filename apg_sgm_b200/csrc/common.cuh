@@ -39,6 +39,7 @@ struct CostCtx {
     const int16_t *rmin, *rmax;
     int prior_ranges;  // 0: every pixel has the default range [d0, min(dmax, x+1)); 1: rmin/rmax vary
     int tile;          // cost kernel tile width (64, 128, 256; 0 = default for Dp)
+    int kernel;        // cost kernel: 0 = pixel runs where they apply, 1 = column tiles always
 };
 
 // Quantised cost of left (x, y) against right (xr, y) from LUTs held in shared memory.

@@ -1,0 +1,393 @@
+// Matching-cost volume by pixel runs, fused with the horizontal Cross-arm pass and the
+// right-image argmin: the form used for the 32-bit census with the default disparity ranges
+// (Fast and Balanced).  Results are those of cost.cu's tile kernel, which keeps the forms with
+// per-pixel ranges or the 64-bit census; only the division of the work differs:
+//
+//   * A thread owns one disparity word k (disparities d0+2k and d0+2k+1) and walks a run of
+//     consecutive staged pixels.  The right pixel of (x+1, 2k+1) is the right pixel of (x, 2k), so
+//     each step loads one new right descriptor; the left descriptor is the same for the whole warp
+//     (broadcast loads of four pixels at a time).
+//   * Quantised costs follow CostComputer::compute_volume (src/cost_computer.cpp:247-264): the
+//     census and AD terms come from one table t2[ad][pop] = lut_census[pop] + lut_ad[ad] (the
+//     reference's first float add, done once per entry), then + lut_grad[g], * scale, + 0.5,
+//     truncation and clamp, each float op rounded on its own.  Census-only costs use the host's
+//     pre-quantised table.
+//   * The horizontal prefix over a run (CostAggregator::aggregate_hv's row pass,
+//     src/cost_aggregator.cpp:65-105) is a plain 32-bit running sum of packed words: the
+//     difference of two such sums is exact in each 16-bit half when each half's window sum is
+//     below 2^16, which the host checks for the arm length and cost_max.  Runs are joined at query
+//     time from the per-run totals.
+//   * The right-image argmin (wta_right_from_left_volume, src/pipeline.cpp:24-85): right pixel
+//     r = x - d0 - di receives (x, di) at step x in lane di/2.  Its running minimum key
+//     (cost << 16 | di: lowest cost first, then lowest d) moves one lane up every two steps (a
+//     shuffle), leaves the warp at lane 31 and is merged into rkey with atomicMin, like every
+//     partial minimum; min is idempotent, so a halo pixel seen by two tiles changes nothing.
+//
+// Blocks are persistent: each builds its tables once and then walks (row, column tile) items.
+#include <algorithm>
+
+#include "common.cuh"
+#include "kernels.h"
+
+namespace apgcu {
+
+namespace {
+
+constexpr int kT2Stride = 33;  // t2 row per |dgray|: popcounts 0..32 of a 32-bit census
+
+struct RunGeom {
+    int txc, ha, nx, nr, roff, rl, nrun, wpc, ntx, ntiles;
+    size_t t2, lgt, q, magic, arm, lc, lg, rc, rg, pre, tot, total;
+};
+
+__host__ inline size_t a16(size_t v) { return (v + 15) & ~size_t(15); }
+
+// Staging and table layout of one block.  nx (staged left pixels) and rl (run length) are
+// multiples of 4 (16-byte loads of four left descriptors); roff shifts the staged right row so
+// that each step group's right descriptors start at an even index (8-byte loads).
+// Warps per block: 16 with the aggregation (its staging limits a block to two per SM), else 8.
+RunGeom run_geom(const CostCtx& c, int txc, int ha, bool cross, bool full) {
+    RunGeom g{};
+    const int W2 = c.Dp / 2;
+    g.txc = txc;
+    g.ha = ha;
+    g.wpc = W2 / 32;
+    g.nrun = std::max(1, (cross ? 16 : 8) / g.wpc);
+    g.nx = round_up(txc + 2 * ha, 4);
+    g.rl = round_up((g.nx + g.nrun - 1) / g.nrun, 4);
+    g.roff = (c.D - 1) % 2 == 0 ? 2 : 1;
+    g.nr = round_up(g.nx + c.D - 1 + g.roff, 4);
+    g.ntx = (c.w + txc - 1) / txc;
+    g.ntiles = g.ntx * c.h;
+    const bool stage_g = full || cross;
+    size_t o = 0;
+    g.t2 = o; o = a16(o + (full ? 256 * kT2Stride * 4 : 0));
+    g.lgt = o; o = a16(o + (full ? 511 * 4 : 0));
+    g.q = o; o = a16(o + (full ? 0 : 65 * 4));
+    g.magic = o; o = a16(o + (cross ? (2 * ha + 2) * 4 : 0));
+    g.arm = o; o = a16(o + (cross ? txc * 4 : 0));
+    g.lc = o; o = a16(o + g.nx * 4);
+    g.lg = o; o = a16(o + (stage_g ? g.nx * 4 : 0));
+    g.rc = o; o = a16(o + g.nr * 4);
+    g.rg = o; o = a16(o + (full ? g.nr * 4 : 0));
+    g.pre = o; o = a16(o + (cross ? (size_t)g.nx * W2 * 4 : 0));
+    g.tot = o; o = a16(o + (cross ? (size_t)g.nrun * W2 * 4 : 0));
+    g.total = o;
+    return g;
+}
+
+__device__ __forceinline__ uint32_t pack_g(const uint8_t* gray, const uint8_t* gx, const uint8_t* gy, int i) {
+    return (uint32_t)gray[i] | ((uint32_t)gx[i] << 8) | ((uint32_t)gy[i] << 16);
+}
+
+// Quantised cost of one (left, right) descriptor pair.
+template <bool FULL>
+__device__ __forceinline__ uint32_t run_cost(uint32_t lc, uint32_t lg, uint32_t rc, uint32_t rg, const float* s_t2,
+                                             const float* s_lgt, const uint32_t* s_q, float scale, uint32_t cmax) {
+    const int pop = __popc(lc ^ rc);
+    if constexpr (!FULL) {
+        return s_q[pop];
+    } else {
+        const uint32_t ad = __vabsdiffu4(lg, rg);  // |dgray|, |dgx|, |dgy|
+        const float t = s_t2[(ad & 0xFFu) * kT2Stride + pop];
+        const float v = __fadd_rn(t, s_lgt[__dp4a(ad, 0x00010100u, 0u)]);
+        // truncation saturates below zero, so only the upper clamp remains
+        const uint32_t q = __float2uint_rz(__fadd_rn(__fmul_rn(v, scale), 0.5f));
+        return min(q, cmax);
+    }
+}
+
+// One run of steps for this thread's word.  V: every (x, d) of the run is a valid voxel for
+// every lane of the warp (no per-voxel tests).  W2T: words per pixel when known at compile time.
+template <bool V, bool CROSS, bool STORE, bool FULL, int W2T>
+__device__ __forceinline__ void run_steps(const CostCtx& c, const RunGeom& g, int row, int xbase, int xs, int xe,
+                                          int k, const uint32_t* s_lc, const uint32_t* s_lg, const uint32_t* s_rc,
+                                          const uint32_t* s_rg, const float* s_t2, const float* s_lgt,
+                                          const uint32_t* s_q, uint32_t* s_pre, uint32_t* s_tot, int run,
+                                          uint32_t* __restrict__ out_vol, uint32_t* __restrict__ rkey) {
+    const int lane = threadIdx.x & 31;
+    const int W2 = W2T ? W2T : (c.Dp >> 1);
+    const int di0 = 2 * k;
+    const int dlo = c.d0 + di0;
+    const float scale = c.scale;
+    const uint32_t cmax = (uint32_t)c.cost_max;
+    // words past the range load at the last even disparity of the range (in bounds, and the same
+    // parity as di0, which keeps the 8-byte right loads aligned) and are masked below
+    const int dload = V ? di0 : min(di0, (c.D - 1) & ~1);
+    int ri = xs - dload + c.D - 1 + g.roff;  // staged right descriptor of (xs, dload); even
+    uint32_t pc = s_rc[ri - 1], pg = FULL ? s_rg[ri - 1] : 0u;
+    uint32_t acc_old = kInvalidWord, acc_cur = kInvalidWord, pre = 0;
+    const uint32_t kd0 = (uint32_t)di0, kd1 = kd0 + 1u;
+    const bool v0d = di0 < c.D, v1d = di0 + 1 < c.D;
+    uint32_t* pp = s_pre + xs * W2 + k;                                   // prefix of (xs, k)
+    uint32_t* vp = out_vol + ((size_t)row + (xbase + xs)) * W2 + k;      // volume word of (xs, k)
+    uint32_t* rk = rkey + row + (xbase + xs - dlo - 1);                  // lane 31's leaving pixel (V)
+    for (int xi = xs; xi < xe; xi += 4) {
+        const uint4 lc4 = *reinterpret_cast<const uint4*>(s_lc + xi);
+        uint4 lg4 = make_uint4(0, 0, 0, 0);
+        if (FULL) lg4 = *reinterpret_cast<const uint4*>(s_lg + xi);
+        const uint2 ra = *reinterpret_cast<const uint2*>(s_rc + ri);
+        const uint2 rb = *reinterpret_cast<const uint2*>(s_rc + ri + 2);
+        uint2 ga = make_uint2(0, 0), gb = make_uint2(0, 0);
+        if (FULL) {
+            ga = *reinterpret_cast<const uint2*>(s_rg + ri);
+            gb = *reinterpret_cast<const uint2*>(s_rg + ri + 2);
+        }
+        const uint32_t L[4] = {lc4.x, lc4.y, lc4.z, lc4.w};
+        const uint32_t LG[4] = {lg4.x, lg4.y, lg4.z, lg4.w};
+        const uint32_t R[5] = {pc, ra.x, ra.y, rb.x, rb.y};
+        const uint32_t RG[5] = {pg, ga.x, ga.y, gb.x, gb.y};
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int x = xbase + xi + j;
+            uint32_t q0 = run_cost<FULL>(L[j], LG[j], R[j + 1], RG[j + 1], s_t2, s_lgt, s_q, scale, cmax);
+            uint32_t q1 = run_cost<FULL>(L[j], LG[j], R[j], RG[j], s_t2, s_lgt, s_q, scale, cmax);
+            bool v0 = true, v1 = true;
+            if (!V) {
+                const bool xin = x >= 0 && x < c.w;
+                v0 = xin && v0d && x - dlo >= 0 && x - dlo < c.w;
+                v1 = xin && v1d && x - dlo - 1 >= 0 && x - dlo - 1 < c.w;
+            }
+            // right-image argmin chain
+            const uint32_t key0 = v0 ? ((q0 << 16) | kd0) : kInvalidWord;
+            const uint32_t key1 = v1 ? ((q1 << 16) | kd1) : kInvalidWord;
+            acc_old = min(acc_old, key1);
+            acc_cur = min(acc_cur, key0);
+            const uint32_t in = __shfl_up_sync(0xFFFFFFFFu, acc_old, 1);
+            if (lane == 31) {
+                const int r = x - dlo - 1;  // right pixel whose minimum leaves the warp
+                if (V) atomicMin(rk + j, acc_old);
+                else if (acc_old != kInvalidWord && r >= 0 && r < c.w) atomicMin(rkey + row + r, acc_old);
+            }
+            acc_old = acc_cur;
+            acc_cur = lane ? in : kInvalidWord;
+            if (CROSS) {
+                pre += (v0 ? q0 : 0u) | ((v1 ? q1 : 0u) << 16);
+                pp[j * W2] = pre;
+            } else if (STORE) {
+                // without a halo the staged pixels are the tile's; V runs lie inside the image
+                if (V || (xi + j < g.txc && x < c.w)) {
+                    if (!v0) q0 = kInvalidCost;
+                    if (!v1) q1 = kInvalidCost;
+                    vp[(size_t)j * W2] = q0 | (q1 << 16);
+                }
+            }
+        }
+        pc = rb.y;
+        pg = gb.y;
+        ri += 4;
+        pp += 4 * W2;
+        vp += 4 * (size_t)W2;
+        rk += 4;
+    }
+    if (xe > xs) {
+        // partial minima still held: acc_old (right pixel got di0 at the last step), acc_cur
+        // (got up to di0-1 from the lane below)
+        const int xl = xbase + xe - 1;
+        const int r_old = xl - dlo, r_cur = xl + 1 - dlo;
+        if (acc_old != kInvalidWord && r_old >= 0 && r_old < c.w) atomicMin(rkey + row + r_old, acc_old);
+        if (acc_cur != kInvalidWord && r_cur >= 0 && r_cur < c.w) atomicMin(rkey + row + r_cur, acc_cur);
+    }
+    if (CROSS) s_tot[run * W2 + k] = pre;
+}
+
+// Aggregated word kk at pixel x from its packed window sum s (cost.cu's tile kernel, same rules).
+__device__ __forceinline__ uint32_t agg_word(const CostCtx& c, uint32_t s, int kk, int x, int l, int r,
+                                             const uint32_t* s_magic) {
+    const int dw = c.d0 + 2 * kk;
+    if (2 * kk + 1 < c.D && x - l >= dw + 1 && x + r <= c.w - 1 + dw) {
+        const uint32_t len = (uint32_t)(l + r + 1), mg = s_magic[len];
+        return div_by_magic(s & 0xFFFFu, len, mg) | (div_by_magic(s >> 16, len, mg) << 16);
+    }
+    uint32_t word = 0;
+#pragma unroll
+    for (int hs = 0; hs < 2; ++hs) {
+        const int di = 2 * kk + hs;
+        const int d = c.d0 + di;
+        const uint32_t sh = (s >> (16 * hs)) & 0xFFFFu;
+        const int nh = min(x + r, c.w - 1 + d) - max(x - l, d) + 1;  // valid x' in the window
+        const bool ok = di < c.D && d <= x && nh > 0;
+        const uint32_t q = ok ? div_by_magic(sh, (uint32_t)nh, s_magic[nh]) : kInvalidCost;
+        word |= q << (16 * hs);
+    }
+    return word;
+}
+
+template <bool CROSS, bool STORE, bool FULL, int W2T>
+__global__ void __launch_bounds__(512, CROSS ? 2 : 1) cost_run_kernel(CostCtx c, RunGeom g, int lmax, int tau,
+                                                       uint32_t* __restrict__ out_vol, uint32_t* __restrict__ rkey,
+                                                       const uint32_t* __restrict__ magic) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    float* s_t2 = reinterpret_cast<float*>(smem + g.t2);
+    float* s_lgt = reinterpret_cast<float*>(smem + g.lgt);
+    uint32_t* s_q = reinterpret_cast<uint32_t*>(smem + g.q);
+    uint32_t* s_magic = reinterpret_cast<uint32_t*>(smem + g.magic);
+    uint32_t* s_arm = reinterpret_cast<uint32_t*>(smem + g.arm);
+    uint32_t* s_lc = reinterpret_cast<uint32_t*>(smem + g.lc);
+    uint32_t* s_lg = reinterpret_cast<uint32_t*>(smem + g.lg);
+    uint32_t* s_rc = reinterpret_cast<uint32_t*>(smem + g.rc);
+    uint32_t* s_rg = reinterpret_cast<uint32_t*>(smem + g.rg);
+    uint32_t* s_pre = reinterpret_cast<uint32_t*>(smem + g.pre);
+    uint32_t* s_tot = reinterpret_cast<uint32_t*>(smem + g.tot);
+    const int tid = threadIdx.x, nt = blockDim.x, wi = tid >> 5, lane = tid & 31;
+    const int W2 = W2T ? W2T : (c.Dp >> 1);
+
+    if (FULL) {
+        for (int i = tid; i < 256 * kT2Stride; i += nt) {
+            const int ad = i / kT2Stride, pop = i - ad * kT2Stride;
+            const float lc = c.lut[kLutCensus + pop];
+            s_t2[i] = c.use_ad ? __fadd_rn(lc, c.lut[kLutAd + ad]) : lc;
+        }
+        // without the gradient term, + 0.0f leaves every sum as it is
+        for (int i = tid; i < 511; i += nt) s_lgt[i] = c.use_grad ? c.lut[kLutGrad + i] : 0.0f;
+    } else {
+        for (int i = tid; i < 65; i += nt) s_q[i] = c.qlut[i];
+    }
+    if (CROSS)
+        for (int i = tid; i < 2 * g.ha + 2; i += nt) s_magic[i] = magic[i];
+
+    const int kset = wi % g.wpc, run = wi / g.wpc;
+    const int k = kset * 32 + lane;
+    const int xs = min(run * g.rl, g.nx), xe = min(xs + g.rl, g.nx);
+
+    for (int tile = blockIdx.x; tile < g.ntiles; tile += gridDim.x) {
+        const int y = tile / g.ntx;
+        const int x0 = (tile - y * g.ntx) * g.txc;
+        const int xbase = x0 - g.ha;
+        const int rbase = xbase - (c.d0 + c.D - 1) - g.roff;  // image column of staged right 0
+        const int row = y * c.w;
+        __syncthreads();  // the previous item's readers are done with the staging
+        for (int i = tid; i < g.nx; i += nt) {
+            const int x = xbase + i;
+            const bool in = x >= 0 && x < c.w;
+            s_lc[i] = in ? c.cl[row + x] : 0u;
+            if (FULL || CROSS) s_lg[i] = in ? pack_g(c.lgray, c.lgx, c.lgy, row + x) : 0u;
+        }
+        for (int i = tid; i < g.nr; i += nt) {
+            const int xr = rbase + i;
+            const bool in = xr >= 0 && xr < c.w;
+            s_rc[i] = in ? c.cr[row + xr] : 0u;
+            if (FULL) s_rg[i] = in ? pack_g(c.rgray, c.rgx, c.rgy, row + xr) : 0u;
+        }
+        __syncthreads();
+        if (CROSS) {
+            // arms (build_cross_arms, src/cost_aggregator.cpp:17-63) and the runs each window
+            // spans: l | r << 8 | run(a - 1) << 16 | run(b) << 24 over staged [a, b]
+            for (int i = tid; i < g.txc; i += nt) {
+                const int x = x0 + i;
+                if (x >= c.w) break;
+                const int sxi = i + g.ha;
+                const int c0 = (int)(s_lg[sxi] & 0xFFu);
+                int l = 0, r = 0;
+                while (l < lmax && x - l - 1 >= 0 && abs((int)(s_lg[sxi - l - 1] & 0xFFu) - c0) <= tau) ++l;
+                while (r < lmax && x + r + 1 < c.w && abs((int)(s_lg[sxi + r + 1] & 0xFFu) - c0) <= tau) ++r;
+                const int a = sxi - l, b = sxi + r;
+                const int rlo = a > 0 ? (a - 1) / g.rl : 0, rhi = b / g.rl;
+                s_arm[i] = (uint32_t)l | ((uint32_t)r << 8) | ((uint32_t)rlo << 16) | ((uint32_t)rhi << 24);
+            }
+        }
+        if (k < W2) {
+            const int xa = xbase + xs, xb = xbase + xe - 1;
+            const int dlo = c.d0 + 2 * k;
+            const bool ok = xa >= 0 && xb < c.w && 2 * k + 1 < c.D && xa - dlo - 1 >= 0 && xb - dlo <= c.w - 1;
+            if (__all_sync(0xFFFFFFFFu, ok))
+                run_steps<true, CROSS, STORE, FULL, W2T>(c, g, row, xbase, xs, xe, k, s_lc, s_lg, s_rc, s_rg, s_t2, s_lgt,
+                                                    s_q, s_pre, s_tot, run, out_vol, rkey);
+            else
+                run_steps<false, CROSS, STORE, FULL, W2T>(c, g, row, xbase, xs, xe, k, s_lc, s_lg, s_rc, s_rg, s_t2,
+                                                     s_lgt, s_q, s_pre, s_tot, run, out_vol, rkey);
+        }
+        if (CROSS) {
+            __syncthreads();
+            // T(x, d) = floor(window sum / valid count) over [x - L(x), x + R(x)]; a thread takes
+            // two words of one pixel
+            const int pairs = W2 >> 1;
+            const int p = tid % pairs, k2 = 2 * p;
+            for (int xi = tid / pairs; xi < g.txc; xi += nt / pairs) {
+                const int x = x0 + xi;
+                if (x >= c.w) break;
+                const uint32_t arm = s_arm[xi];
+                const int l = (int)(arm & 0xFFu), r = (int)((arm >> 8) & 0xFFu);
+                const int rlo = (int)((arm >> 16) & 0xFFu), rhi = (int)(arm >> 24);
+                const int sxi = xi + g.ha, a = sxi - l, b = sxi + r;
+                uint2 sb = *reinterpret_cast<const uint2*>(s_pre + b * W2 + k2);
+                const uint2 sa = a > 0 ? *reinterpret_cast<const uint2*>(s_pre + (a - 1) * W2 + k2) : make_uint2(0, 0);
+                for (int j = rlo; j < rhi; ++j) {
+                    const uint2 t = *reinterpret_cast<const uint2*>(s_tot + j * W2 + k2);
+                    sb.x += t.x;
+                    sb.y += t.y;
+                }
+                const uint32_t w0 = agg_word(c, sb.x - sa.x, k2, x, l, r, s_magic);
+                const uint32_t w1 = agg_word(c, sb.y - sa.y, k2 + 1, x, l, r, s_magic);
+                *reinterpret_cast<uint2*>(out_vol + ((size_t)row + x) * W2 + k2) = make_uint2(w0, w1);
+            }
+        }
+    }
+}
+
+template <bool CROSS, bool STORE, bool FULL, int W2T>
+cudaError_t launch_runs_w(const CostCtx& c, int txc, int lmax, int tau, uint32_t* vol, uint32_t* rkey,
+                          const uint32_t* magic, cudaStream_t s) {
+    const RunGeom g = run_geom(c, txc, CROSS ? lmax : 0, CROSS, FULL);
+    const int nt = 32 * g.wpc * g.nrun;
+    auto kern = cost_run_kernel<CROSS, STORE, FULL, W2T>;
+    cudaError_t e = allow_dynamic_smem(kern, g.total);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0, dev = 0, nsm = 0;
+    e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, nt, g.total);
+    if (e != cudaSuccess) return e;
+    const int blocks = std::max(1, std::min(g.ntiles, std::max(1, per_sm) * nsm));
+    kern<<<blocks, nt, g.total, s>>>(c, g, lmax, tau, vol, rkey, magic);
+    return cudaGetLastError();
+}
+
+// Words per pixel as a compile-time constant for the usual disparity paddings.
+template <bool CROSS, bool STORE, bool FULL>
+cudaError_t launch_runs_t(const CostCtx& c, int txc, int lmax, int tau, uint32_t* vol, uint32_t* rkey,
+                          const uint32_t* magic, cudaStream_t s) {
+    switch (c.Dp) {
+        case 64: return launch_runs_w<CROSS, STORE, FULL, 32>(c, txc, lmax, tau, vol, rkey, magic, s);
+        case 128: return launch_runs_w<CROSS, STORE, FULL, 64>(c, txc, lmax, tau, vol, rkey, magic, s);
+        case 192: return launch_runs_w<CROSS, STORE, FULL, 96>(c, txc, lmax, tau, vol, rkey, magic, s);
+        case 256: return launch_runs_w<CROSS, STORE, FULL, 128>(c, txc, lmax, tau, vol, rkey, magic, s);
+        default: return launch_runs_w<CROSS, STORE, FULL, 0>(c, txc, lmax, tau, vol, rkey, magic, s);
+    }
+}
+
+}  // namespace
+
+size_t cost_runs_smem_bytes(const CostCtx& c, int mode, int lmax) {
+    const bool full = c.use_ad || c.use_grad;
+    const int txc = mode == 1 ? (c.Dp <= 128 ? 128 : 64) : 256;
+    return run_geom(c, txc, mode == 1 ? lmax : 0, mode == 1, full).total;
+}
+
+bool cost_runs_supported(const CostCtx& c, int mode, int lmax) {
+    if (c.kernel == 1 || c.census64 || c.prior_ranges) return false;
+    if (c.Dp % 64 != 0 || c.Dp > 512) return false;
+    const bool full = c.use_ad || c.use_grad;
+    if (mode == 2 && full) return false;  // the fused form exists for census-only costs
+    if (mode == 1 && lmax > 127) return false;
+    return cost_runs_smem_bytes(c, mode, lmax) <= 200 * 1024;
+}
+
+cudaError_t launch_cost_runs(const CostCtx& c, int mode, int lmax, int tau, uint32_t* vol, uint32_t* rkey,
+                             const uint32_t* magic, cudaStream_t s) {
+    const bool full = c.use_ad || c.use_grad;
+    if (mode == 1) {
+        int txc = c.Dp <= 128 ? 128 : 64;
+        if ((c.tile == 64 || c.tile == 128 || c.tile == 256) &&
+            run_geom(c, c.tile, lmax, true, full).total <= 200 * 1024)
+            txc = c.tile;
+        return full ? launch_runs_t<true, true, true>(c, txc, lmax, tau, vol, rkey, magic, s)
+                    : launch_runs_t<true, true, false>(c, txc, lmax, tau, vol, rkey, magic, s);
+    }
+    if (mode == 0)
+        return full ? launch_runs_t<false, true, true>(c, 256, lmax, tau, vol, rkey, magic, s)
+                    : launch_runs_t<false, true, false>(c, 256, lmax, tau, vol, rkey, magic, s);
+    return launch_runs_t<false, false, false>(c, 256, lmax, tau, vol, rkey, magic, s);
+}
+
+}  // namespace apgcu

@@ -245,6 +245,7 @@ CostCtx Engine::cost_ctx() const {
     c.rmin = ptr<int16_t>(lay_.rmin); c.rmax = ptr<int16_t>(lay_.rmax);
     c.prior_ranges = cfg_.prior_enable ? 1 : 0;
     c.tile = cost_tile_;
+    c.kernel = cost_kernel_;
     return c;
 }
 
@@ -917,6 +918,11 @@ int apgcu_engine_set_tuning(apgcu_engine_t e, const char* key, int value) {
     if (std::strcmp(key, "cost_tile") == 0) {
         if (value != 0 && value != 64 && value != 128 && value != 256) return apgcu::kInvalidConfig;
         e->eng->set_cost_tile(value);
+        return 0;
+    }
+    if (std::strcmp(key, "cost_kernel") == 0) {
+        if (value != 0 && value != 1) return apgcu::kInvalidConfig;
+        e->eng->set_cost_kernel(value);
         return 0;
     }
     if (std::strcmp(key, "fast_fused") == 0) {

@@ -112,6 +112,7 @@ public:
     void set_sgm_lanes(int t) { sgm_lanes_ = t; }
     void set_fast_fused(bool on) { fast_fused_ = on; }
     void set_cost_tile(int t) { cost_tile_ = t; }
+    void set_cost_kernel(int k) { cost_kernel_ = k; }
     int debug() const { return debug_; }
     const apg_pipeline_config_t& config() const { return cfg_; }
     int device() const { return device_; }
@@ -143,6 +144,7 @@ private:
     int sgm_lanes_ = 0;
     bool fast_fused_ = false;
     int cost_tile_ = 0;
+    int cost_kernel_ = 0;  // 0: pixel-run cost kernel where it applies, 1: column-tile kernel
     cudaStream_t stream_ = nullptr;
     bool own_stream_ = false;
     unsigned char* arena_ = nullptr;

@@ -17,6 +17,12 @@ cudaError_t launch_aux(const uint8_t* src, int stride, int ch, int w, int h, int
                        cudaStream_t s);
 
 // cost.cu: mode 0 raw volume, 1 cross-H volume, 2 right argmin only; all update rkey.
+// Pixel-run form of the cost kernel (32-bit census, default ranges); launch_cost uses it where
+// cost_runs_supported holds.
+bool cost_runs_supported(const CostCtx& c, int mode, int lmax);
+size_t cost_runs_smem_bytes(const CostCtx& c, int mode, int lmax);
+cudaError_t launch_cost_runs(const CostCtx& c, int mode, int lmax, int tau, uint32_t* vol, uint32_t* rkey,
+                             const uint32_t* magic, cudaStream_t s);
 cudaError_t launch_cost(const CostCtx& c, int mode, int lmax, int tau, uint32_t* vol, uint32_t* rkey,
                         const uint32_t* magic, cudaStream_t s);
 size_t cost_kernel_smem_bytes(int D, int Dp, int lmax, bool cross, bool census64);
