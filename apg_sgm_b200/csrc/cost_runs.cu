@@ -1,12 +1,14 @@
 // Matching-cost volume by pixel runs, fused with the horizontal Cross-arm pass and the
 // right-image argmin: the form used for the 32-bit census with the default disparity ranges
-// (Fast and Balanced).  Results are those of cost.cu's tile kernel, which keeps the forms with
-// per-pixel ranges or the 64-bit census; only the division of the work differs:
+// (Fast and Balanced), up to 256 padded disparities.  Results are those of cost.cu's tile kernel,
+// which keeps the forms with per-pixel ranges, the 64-bit census or wider ranges; only the
+// division of the work differs:
 //
-//   * A thread owns one disparity word k (disparities d0+2k and d0+2k+1) and walks a run of
-//     consecutive staged pixels.  The right pixel of (x+1, 2k+1) is the right pixel of (x, 2k), so
-//     each step loads one new right descriptor; the left descriptor is the same for the whole warp
-//     (broadcast loads of four pixels at a time).
+//   * One warp covers the whole disparity range of a run of consecutive staged pixels: lane l owns
+//     the WPL = Dp/64 words k = WPL*l .. WPL*l + WPL-1 (the P = 2*WPL disparities P*l .. P*l+P-1)
+//     and walks the run one pixel per step.  The right pixel of (x+1, di+1) is the right pixel of
+//     (x, di), so each step loads one new right descriptor per lane into a P-entry register window;
+//     the left descriptor is the same for the whole warp (broadcast loads of four pixels at a time).
 //   * Quantised costs follow CostComputer::compute_volume (src/cost_computer.cpp:247-264): the
 //     census and AD terms come from one table t2[ad][pop] = lut_census[pop] + lut_ad[ad] (the
 //     reference's first float add, done once per entry), then + lut_grad[g], * scale, + 0.5,
@@ -18,10 +20,12 @@
 //     below 2^16, which the host checks for the arm length and cost_max.  Runs are joined at query
 //     time from the per-run totals.
 //   * The right-image argmin (wta_right_from_left_volume, src/pipeline.cpp:24-85): right pixel
-//     r = x - d0 - di receives (x, di) at step x in lane di/2.  Its running minimum key
-//     (cost << 16 | di: lowest cost first, then lowest d) moves one lane up every two steps (a
-//     shuffle), leaves the warp at lane 31 and is merged into rkey with atomicMin, like every
-//     partial minimum; min is idempotent, so a halo pixel seen by two tiles changes nothing.
+//     r = x - d0 - di receives (x, di) at step x in lane di/P.  Each lane keeps the running minimum
+//     keys (cost << 16 | di: lowest cost first, then lowest d) of its P right pixels; every step
+//     the oldest moves one lane up (a shuffle), and the one leaving lane 31 -- complete over this
+//     run -- goes to a per-warp buffer that is merged into rkey with atomicMin at the end of the
+//     run, together with the partial minima still held.  min is idempotent, so a halo pixel seen
+//     by two tiles changes nothing.
 //
 // Blocks are persistent: each builds its tables once and then walks (row, column tile) items.
 #include <algorithm>
@@ -36,26 +40,30 @@ namespace {
 constexpr int kT2Stride = 33;  // t2 row per |dgray|: popcounts 0..32 of a 32-bit census
 
 struct RunGeom {
-    int txc, ha, nx, nr, roff, rl, nrun, wpc, ntx, ntiles;
-    size_t t2, lgt, q, magic, arm, lc, lg, rc, rg, pre, tot, total;
+    int txc, ha, nx, nr, roff, rl, nrun, ntx, ntiles;
+    size_t t2, lgt, q, magic, arm, lc, lg, rc, rg, pre, tot, emit, total;
 };
 
-__host__ inline size_t a16(size_t v) { return (v + 15) & ~size_t(15); }
+inline size_t a16(size_t v) { return (v + 15) & ~size_t(15); }
 
-// Staging and table layout of one block.  nx (staged left pixels) and rl (run length) are
-// multiples of 4 (16-byte loads of four left descriptors); roff shifts the staged right row so
-// that each step group's right descriptors start at an even index (8-byte loads).
-// Warps per block: 16 with the aggregation (its staging limits a block to two per SM), else 8.
+inline int run_warps(bool cross) { return cross ? 16 : 8; }
+
+// Staging and table layout of one block for a tile of txc columns with halo ha.  nx (staged left
+// pixels) and rl (run length) are multiples of 4 (16-byte loads of four left descriptors); roff
+// shifts the staged right row so that each step group's right descriptors start at an even index
+// (8-byte loads) and every lane with a disparity inside the range finds its whole window staged.
+// One run per warp.
 RunGeom run_geom(const CostCtx& c, int txc, int ha, bool cross, bool full) {
     RunGeom g{};
     const int W2 = c.Dp / 2;
     g.txc = txc;
     g.ha = ha;
-    g.wpc = W2 / 32;
-    g.nrun = std::max(1, (cross ? 16 : 8) / g.wpc);
+    g.nrun = run_warps(cross);
     g.nx = round_up(txc + 2 * ha, 4);
     g.rl = round_up((g.nx + g.nrun - 1) / g.nrun, 4);
-    g.roff = (c.D - 1) % 2 == 0 ? 2 : 1;
+    // even start for every step group, plus P entries so that a lane holding any disparity of the
+    // range loads its own window without clamping
+    g.roff = ((c.D - 1) % 2 == 0 ? 2 : 1) + c.Dp / 32;
     g.nr = round_up(g.nx + c.D - 1 + g.roff, 4);
     g.ntx = (c.w + txc - 1) / txc;
     g.ntiles = g.ntx * c.h;
@@ -72,6 +80,7 @@ RunGeom run_geom(const CostCtx& c, int txc, int ha, bool cross, bool full) {
     g.rg = o; o = a16(o + (full ? g.nr * 4 : 0));
     g.pre = o; o = a16(o + (cross ? (size_t)g.nx * W2 * 4 : 0));
     g.tot = o; o = a16(o + (cross ? (size_t)g.nrun * W2 * 4 : 0));
+    g.emit = o; o = a16(o + (size_t)g.nrun * g.rl * 4);
     g.total = o;
     return g;
 }
@@ -97,37 +106,55 @@ __device__ __forceinline__ uint32_t run_cost(uint32_t lc, uint32_t lg, uint32_t 
     }
 }
 
-// One run of steps for this thread's word.  V: every (x, d) of the run is a valid voxel for
-// every lane of the warp (no per-voxel tests).  W2T: words per pixel when known at compile time.
-template <bool V, bool CROSS, bool STORE, bool FULL, int W2T>
+template <int N>
+__device__ __forceinline__ void store_words(uint32_t* p, const uint32_t (&w)[N]) {
+    if constexpr (N == 4) {
+        *reinterpret_cast<uint4*>(p) = make_uint4(w[0], w[1], w[2], w[3]);
+    } else if constexpr (N == 2) {
+        *reinterpret_cast<uint2*>(p) = make_uint2(w[0], w[1]);
+    } else {
+#pragma unroll
+        for (int i = 0; i < N; ++i) p[i] = w[i];
+    }
+}
+
+// One run of steps of this lane's P disparities.  V: every (x, d) of the run is a valid voxel for
+// every lane of the warp (no per-voxel tests).
+template <bool V, bool CROSS, bool STORE, bool FULL, int WPL>
 __device__ __forceinline__ void run_steps(const CostCtx& c, const RunGeom& g, int row, int xbase, int xs, int xe,
-                                          int k, const uint32_t* s_lc, const uint32_t* s_lg, const uint32_t* s_rc,
+                                          const uint32_t* s_lc, const uint32_t* s_lg, const uint32_t* s_rc,
                                           const uint32_t* s_rg, const float* s_t2, const float* s_lgt,
-                                          const uint32_t* s_q, uint32_t* s_pre, uint32_t* s_tot, int run,
-                                          uint32_t* __restrict__ out_vol, uint32_t* __restrict__ rkey) {
+                                          const uint32_t* s_q, uint32_t* s_pre, uint32_t* s_tot, uint32_t* s_em,
+                                          int run, uint32_t* __restrict__ out_vol, uint32_t* __restrict__ rkey) {
+    constexpr int P = 2 * WPL;
+    constexpr int W2 = 32 * WPL;
     const int lane = threadIdx.x & 31;
-    const int W2 = W2T ? W2T : (c.Dp >> 1);
-    const int di0 = 2 * k;
-    const int dlo = c.d0 + di0;
+    const int dbase = P * lane;  // first disparity index of this lane
     const float scale = c.scale;
     const uint32_t cmax = (uint32_t)c.cost_max;
-    // words past the range load at the last even disparity of the range (in bounds, and the same
-    // parity as di0, which keeps the 8-byte right loads aligned) and are masked below
-    const int dload = V ? di0 : min(di0, (c.D - 1) & ~1);
-    int ri = xs - dload + c.D - 1 + g.roff;  // staged right descriptor of (xs, dload); even
-    uint32_t pc = s_rc[ri - 1], pg = FULL ? s_rg[ri - 1] : 0u;
-    uint32_t acc_old = kInvalidWord, acc_cur = kInvalidWord, pre = 0;
-    const uint32_t kd0 = (uint32_t)di0, kd1 = kd0 + 1u;
-    const bool v0d = di0 < c.D, v1d = di0 + 1 < c.D;
-    uint32_t* pp = s_pre + xs * W2 + k;                                   // prefix of (xs, k)
-    uint32_t* vp = out_vol + ((size_t)row + (xbase + xs)) * W2 + k;      // volume word of (xs, k)
-    uint32_t* rk = rkey + row + (xbase + xs - dlo - 1);                  // lane 31's leaving pixel (V)
+    // lanes wholly past the range load at the last in-bounds even base (dl + P <= D + roff keeps
+    // every window entry inside the staged row; even keeps the 8-byte loads aligned) and are
+    // masked; a lane with any disparity below D has dbase <= D - 1 < D + roff - P, so keeps its own
+    const int dl = V ? dbase : min(dbase, (c.D + g.roff - P) & ~1);
+    int ri = xs - dl + c.D - 1 + g.roff;  // staged right descriptor of (xs, dl); even
+    uint32_t wc[P], wg[P], acc[P], pre[WPL];
+#pragma unroll
+    for (int j = 0; j < P; ++j) {
+        // before the first step's shift: wc[j] holds the descriptor of (xs - 1, dl + j)
+        wc[j] = j < P - 1 ? s_rc[ri - 1 - j] : 0u;
+        wg[j] = (FULL && j < P - 1) ? s_rg[ri - 1 - j] : 0u;
+        acc[j] = kInvalidWord;
+    }
+#pragma unroll
+    for (int w = 0; w < WPL; ++w) pre[w] = 0;
+    uint32_t* pp = s_pre + xs * W2 + WPL * lane;                             // prefix words of (xs)
+    uint32_t* vp = out_vol + ((size_t)row + (xbase + xs)) * W2 + WPL * lane;  // volume words of (xs)
     for (int xi = xs; xi < xe; xi += 4) {
         const uint4 lc4 = *reinterpret_cast<const uint4*>(s_lc + xi);
         uint4 lg4 = make_uint4(0, 0, 0, 0);
         if (FULL) lg4 = *reinterpret_cast<const uint4*>(s_lg + xi);
-        const uint2 ra = *reinterpret_cast<const uint2*>(s_rc + ri);
-        const uint2 rb = *reinterpret_cast<const uint2*>(s_rc + ri + 2);
+        const uint2 na = *reinterpret_cast<const uint2*>(s_rc + ri);
+        const uint2 nb = *reinterpret_cast<const uint2*>(s_rc + ri + 2);
         uint2 ga = make_uint2(0, 0), gb = make_uint2(0, 0);
         if (FULL) {
             ga = *reinterpret_cast<const uint2*>(s_rg + ri);
@@ -135,60 +162,79 @@ __device__ __forceinline__ void run_steps(const CostCtx& c, const RunGeom& g, in
         }
         const uint32_t L[4] = {lc4.x, lc4.y, lc4.z, lc4.w};
         const uint32_t LG[4] = {lg4.x, lg4.y, lg4.z, lg4.w};
-        const uint32_t R[5] = {pc, ra.x, ra.y, rb.x, rb.y};
-        const uint32_t RG[5] = {pg, ga.x, ga.y, gb.x, gb.y};
+        const uint32_t NC[4] = {na.x, na.y, nb.x, nb.y};
+        const uint32_t NG[4] = {ga.x, ga.y, gb.x, gb.y};
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int x = xbase + xi + j;
-            uint32_t q0 = run_cost<FULL>(L[j], LG[j], R[j + 1], RG[j + 1], s_t2, s_lgt, s_q, scale, cmax);
-            uint32_t q1 = run_cost<FULL>(L[j], LG[j], R[j], RG[j], s_t2, s_lgt, s_q, scale, cmax);
-            bool v0 = true, v1 = true;
-            if (!V) {
-                const bool xin = x >= 0 && x < c.w;
-                v0 = xin && v0d && x - dlo >= 0 && x - dlo < c.w;
-                v1 = xin && v1d && x - dlo - 1 >= 0 && x - dlo - 1 < c.w;
+        for (int s = 0; s < 4; ++s) {
+            const int x = xbase + xi + s;
+#pragma unroll
+            for (int j = P - 1; j > 0; --j) {
+                wc[j] = wc[j - 1];
+                wg[j] = wg[j - 1];
             }
-            // right-image argmin chain
-            const uint32_t key0 = v0 ? ((q0 << 16) | kd0) : kInvalidWord;
-            const uint32_t key1 = v1 ? ((q1 << 16) | kd1) : kInvalidWord;
-            acc_old = min(acc_old, key1);
-            acc_cur = min(acc_cur, key0);
-            const uint32_t in = __shfl_up_sync(0xFFFFFFFFu, acc_old, 1);
-            if (lane == 31) {
-                const int r = x - dlo - 1;  // right pixel whose minimum leaves the warp
-                if (V) atomicMin(rk + j, acc_old);
-                else if (acc_old != kInvalidWord && r >= 0 && r < c.w) atomicMin(rkey + row + r, acc_old);
+            wc[0] = NC[s];
+            wg[0] = NG[s];
+            uint32_t q[P];
+            bool v[P];
+#pragma unroll
+            for (int j = 0; j < P; ++j) {
+                q[j] = run_cost<FULL>(L[s], LG[s], wc[j], wg[j], s_t2, s_lgt, s_q, scale, cmax);
+                v[j] = true;
+                if (!V) {
+                    const int di = dbase + j, xr = x - c.d0 - di;
+                    v[j] = x >= 0 && x < c.w && di < c.D && xr >= 0 && xr < c.w;
+                }
+                const uint32_t key = v[j] ? ((q[j] << 16) | (uint32_t)(dbase + j)) : kInvalidWord;
+                acc[j] = min(acc[j], key);
             }
-            acc_old = acc_cur;
-            acc_cur = lane ? in : kInvalidWord;
+            // the oldest minimum moves one lane up; lane 31's is complete for this run
+            const uint32_t out = acc[P - 1];
+            if (lane == 31) s_em[xi - xs + s] = out;
+            const uint32_t in = __shfl_up_sync(0xFFFFFFFFu, out, 1);
+#pragma unroll
+            for (int j = P - 1; j > 0; --j) acc[j] = acc[j - 1];
+            acc[0] = lane ? in : kInvalidWord;
             if (CROSS) {
-                pre += (v0 ? q0 : 0u) | ((v1 ? q1 : 0u) << 16);
-                pp[j * W2] = pre;
+#pragma unroll
+                for (int w = 0; w < WPL; ++w)
+                    pre[w] += (v[2 * w] ? q[2 * w] : 0u) | ((v[2 * w + 1] ? q[2 * w + 1] : 0u) << 16);
+                store_words<WPL>(pp + s * W2, pre);
             } else if (STORE) {
                 // without a halo the staged pixels are the tile's; V runs lie inside the image
-                if (V || (xi + j < g.txc && x < c.w)) {
-                    if (!v0) q0 = kInvalidCost;
-                    if (!v1) q1 = kInvalidCost;
-                    vp[(size_t)j * W2] = q0 | (q1 << 16);
+                if (V || (xi + s < g.txc && x < c.w)) {
+                    uint32_t wd[WPL];
+#pragma unroll
+                    for (int w = 0; w < WPL; ++w)
+                        wd[w] = (v[2 * w] ? q[2 * w] : kInvalidCost) |
+                                ((v[2 * w + 1] ? q[2 * w + 1] : kInvalidCost) << 16);
+                    store_words<WPL>(vp + (size_t)s * W2, wd);
                 }
             }
         }
-        pc = rb.y;
-        pg = gb.y;
         ri += 4;
         pp += 4 * W2;
         vp += 4 * (size_t)W2;
-        rk += 4;
     }
+    __syncwarp();
     if (xe > xs) {
-        // partial minima still held: acc_old (right pixel got di0 at the last step), acc_cur
-        // (got up to di0-1 from the lane below)
-        const int xl = xbase + xe - 1;
-        const int r_old = xl - dlo, r_cur = xl + 1 - dlo;
-        if (acc_old != kInvalidWord && r_old >= 0 && r_old < c.w) atomicMin(rkey + row + r_old, acc_old);
-        if (acc_cur != kInvalidWord && r_cur >= 0 && r_cur < c.w) atomicMin(rkey + row + r_cur, acc_cur);
+        // minima that left lane 31 at step xs + e: right pixel xbase + xs + e - d0 - (Dp - 1)
+        const int n = xe - xs;
+        const int r0 = xbase + xs - c.d0 - (2 * W2 - 1);
+        for (int e = lane; e < n; e += 32) {
+            const uint32_t m = s_em[e];
+            const int r = r0 + e;
+            if (m != kInvalidWord && r >= 0 && r < c.w) atomicMin(rkey + row + r, m);
+        }
+        // partial minima still held: acc[j] is for right pixel xl + 1 - d0 - dbase - j
+        const int r1 = xbase + xe - c.d0 - dbase;
+#pragma unroll
+        for (int j = 0; j < P; ++j) {
+            const int r = r1 - j;
+            if (acc[j] != kInvalidWord && r >= 0 && r < c.w) atomicMin(rkey + row + r, acc[j]);
+        }
     }
-    if (CROSS) s_tot[run * W2 + k] = pre;
+    __syncwarp();
+    if (CROSS) store_words<WPL>(s_tot + run * W2 + WPL * lane, pre);
 }
 
 // Aggregated word kk at pixel x from its packed window sum s (cost.cu's tile kernel, same rules).
@@ -213,10 +259,12 @@ __device__ __forceinline__ uint32_t agg_word(const CostCtx& c, uint32_t s, int k
     return word;
 }
 
-template <bool CROSS, bool STORE, bool FULL, int W2T>
-__global__ void __launch_bounds__(512, CROSS ? 2 : 1) cost_run_kernel(CostCtx c, RunGeom g, int lmax, int tau,
-                                                       uint32_t* __restrict__ out_vol, uint32_t* __restrict__ rkey,
-                                                       const uint32_t* __restrict__ magic) {
+template <bool CROSS, bool STORE, bool FULL, int WPL>
+__global__ void __launch_bounds__(CROSS ? 512 : 256, CROSS ? 2 : 1)
+    cost_run_kernel(CostCtx c, RunGeom g, int lmax, int tau, uint32_t* __restrict__ out_vol,
+                    uint32_t* __restrict__ rkey, const uint32_t* __restrict__ magic) {
+    constexpr int W2 = 32 * WPL;
+    constexpr int P = 2 * WPL;
     extern __shared__ __align__(16) unsigned char smem[];
     float* s_t2 = reinterpret_cast<float*>(smem + g.t2);
     float* s_lgt = reinterpret_cast<float*>(smem + g.lgt);
@@ -229,8 +277,8 @@ __global__ void __launch_bounds__(512, CROSS ? 2 : 1) cost_run_kernel(CostCtx c,
     uint32_t* s_rg = reinterpret_cast<uint32_t*>(smem + g.rg);
     uint32_t* s_pre = reinterpret_cast<uint32_t*>(smem + g.pre);
     uint32_t* s_tot = reinterpret_cast<uint32_t*>(smem + g.tot);
-    const int tid = threadIdx.x, nt = blockDim.x, wi = tid >> 5, lane = tid & 31;
-    const int W2 = W2T ? W2T : (c.Dp >> 1);
+    const int tid = threadIdx.x, nt = blockDim.x, run = tid >> 5, lane = tid & 31;
+    uint32_t* s_em = reinterpret_cast<uint32_t*>(smem + g.emit) + run * g.rl;
 
     if (FULL) {
         for (int i = tid; i < 256 * kT2Stride; i += nt) {
@@ -246,8 +294,6 @@ __global__ void __launch_bounds__(512, CROSS ? 2 : 1) cost_run_kernel(CostCtx c,
     if (CROSS)
         for (int i = tid; i < 2 * g.ha + 2; i += nt) s_magic[i] = magic[i];
 
-    const int kset = wi % g.wpc, run = wi / g.wpc;
-    const int k = kset * 32 + lane;
     const int xs = min(run * g.rl, g.nx), xe = min(xs + g.rl, g.nx);
 
     for (int tile = blockIdx.x; tile < g.ntiles; tile += gridDim.x) {
@@ -286,22 +332,23 @@ __global__ void __launch_bounds__(512, CROSS ? 2 : 1) cost_run_kernel(CostCtx c,
                 s_arm[i] = (uint32_t)l | ((uint32_t)r << 8) | ((uint32_t)rlo << 16) | ((uint32_t)rhi << 24);
             }
         }
-        if (k < W2) {
+        {
             const int xa = xbase + xs, xb = xbase + xe - 1;
-            const int dlo = c.d0 + 2 * k;
-            const bool ok = xa >= 0 && xb < c.w && 2 * k + 1 < c.D && xa - dlo - 1 >= 0 && xb - dlo <= c.w - 1;
+            const int dlo = c.d0 + P * lane;
+            const bool ok = xa >= 0 && xb < c.w && P * lane + P - 1 < c.D && xa - (dlo + P - 1) >= 0 &&
+                            xb - dlo <= c.w - 1;
             if (__all_sync(0xFFFFFFFFu, ok))
-                run_steps<true, CROSS, STORE, FULL, W2T>(c, g, row, xbase, xs, xe, k, s_lc, s_lg, s_rc, s_rg, s_t2, s_lgt,
-                                                    s_q, s_pre, s_tot, run, out_vol, rkey);
+                run_steps<true, CROSS, STORE, FULL, WPL>(c, g, row, xbase, xs, xe, s_lc, s_lg, s_rc, s_rg, s_t2, s_lgt,
+                                                         s_q, s_pre, s_tot, s_em, run, out_vol, rkey);
             else
-                run_steps<false, CROSS, STORE, FULL, W2T>(c, g, row, xbase, xs, xe, k, s_lc, s_lg, s_rc, s_rg, s_t2,
-                                                     s_lgt, s_q, s_pre, s_tot, run, out_vol, rkey);
+                run_steps<false, CROSS, STORE, FULL, WPL>(c, g, row, xbase, xs, xe, s_lc, s_lg, s_rc, s_rg, s_t2,
+                                                          s_lgt, s_q, s_pre, s_tot, s_em, run, out_vol, rkey);
         }
         if (CROSS) {
             __syncthreads();
             // T(x, d) = floor(window sum / valid count) over [x - L(x), x + R(x)]; a thread takes
             // two words of one pixel
-            const int pairs = W2 >> 1;
+            constexpr int pairs = W2 / 2;
             const int p = tid % pairs, k2 = 2 * p;
             for (int xi = tid / pairs; xi < g.txc; xi += nt / pairs) {
                 const int x = x0 + xi;
@@ -317,20 +364,63 @@ __global__ void __launch_bounds__(512, CROSS ? 2 : 1) cost_run_kernel(CostCtx c,
                     sb.x += t.x;
                     sb.y += t.y;
                 }
-                const uint32_t w0 = agg_word(c, sb.x - sa.x, k2, x, l, r, s_magic);
-                const uint32_t w1 = agg_word(c, sb.y - sa.y, k2 + 1, x, l, r, s_magic);
+                const uint32_t s0 = sb.x - sa.x, s1 = sb.y - sa.y;
+                uint32_t w0, w1;
+                const uint32_t len = (uint32_t)(l + r + 1);
+                // every word of the pixel has its whole window valid (no padded words, x - d inside
+                // the image over the window for every d): one count, no per-word tests
+                if (c.D == c.Dp && len > 1 && x - l >= c.d0 + c.Dp - 1 && x + r <= c.w - 1 + c.d0) {
+                    const uint32_t mg = s_magic[len];
+                    w0 = __byte_perm(__umulhi(s0 & 0xFFFFu, mg), __umulhi(s0 >> 16, mg), 0x5410);
+                    w1 = __byte_perm(__umulhi(s1 & 0xFFFFu, mg), __umulhi(s1 >> 16, mg), 0x5410);
+                } else {
+                    w0 = agg_word(c, s0, k2, x, l, r, s_magic);
+                    w1 = agg_word(c, s1, k2 + 1, x, l, r, s_magic);
+                }
                 *reinterpret_cast<uint2*>(out_vol + ((size_t)row + x) * W2 + k2) = make_uint2(w0, w1);
             }
         }
     }
 }
 
-template <bool CROSS, bool STORE, bool FULL, int W2T>
+// Shared memory one SM gives each of `per_sm` resident blocks.
+size_t smem_per_block(int per_sm) {
+    static size_t sm_total = 0, reserved = 0;
+    if (!sm_total) {
+        int dev = 0, v = 0, r = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess &&
+            cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) == cudaSuccess &&
+            cudaDeviceGetAttribute(&r, cudaDevAttrReservedSharedMemoryPerBlock, dev) == cudaSuccess) {
+            sm_total = (size_t)v;
+            reserved = (size_t)r;
+        } else {
+            cudaGetLastError();
+            return 100 * 1024;
+        }
+    }
+    return sm_total / per_sm - reserved;
+}
+
+// Tile width of the aggregating form: the fewest tiles per row (least halo) whose staging lets two
+// 16-warp blocks share an SM; a requested width (tuning key cost_tile) wins when it fits one block.
+int cross_tile(const CostCtx& c, int lmax, bool full) {
+    if ((c.tile == 64 || c.tile == 128 || c.tile == 256) && run_geom(c, c.tile, lmax, true, full).total <= 200 * 1024)
+        return c.tile;
+    const size_t budget = smem_per_block(2);
+    for (int ntx = 1; ntx <= c.w; ++ntx) {
+        const int txc = round_up((c.w + ntx - 1) / ntx, 4);
+        if (run_geom(c, txc, lmax, true, full).total <= budget) return txc;
+        if (txc <= 32) break;
+    }
+    return 32;
+}
+
+template <bool CROSS, bool STORE, bool FULL, int WPL>
 cudaError_t launch_runs_w(const CostCtx& c, int txc, int lmax, int tau, uint32_t* vol, uint32_t* rkey,
                           const uint32_t* magic, cudaStream_t s) {
     const RunGeom g = run_geom(c, txc, CROSS ? lmax : 0, CROSS, FULL);
-    const int nt = 32 * g.wpc * g.nrun;
-    auto kern = cost_run_kernel<CROSS, STORE, FULL, W2T>;
+    const int nt = 32 * g.nrun;
+    auto kern = cost_run_kernel<CROSS, STORE, FULL, WPL>;
     cudaError_t e = allow_dynamic_smem(kern, g.total);
     if (e != cudaSuccess) return e;
     int per_sm = 0, dev = 0, nsm = 0;
@@ -343,16 +433,15 @@ cudaError_t launch_runs_w(const CostCtx& c, int txc, int lmax, int tau, uint32_t
     return cudaGetLastError();
 }
 
-// Words per pixel as a compile-time constant for the usual disparity paddings.
+// Words per lane as a compile-time constant: one warp spans Dp = 64 * WPL disparities.
 template <bool CROSS, bool STORE, bool FULL>
 cudaError_t launch_runs_t(const CostCtx& c, int txc, int lmax, int tau, uint32_t* vol, uint32_t* rkey,
                           const uint32_t* magic, cudaStream_t s) {
     switch (c.Dp) {
-        case 64: return launch_runs_w<CROSS, STORE, FULL, 32>(c, txc, lmax, tau, vol, rkey, magic, s);
-        case 128: return launch_runs_w<CROSS, STORE, FULL, 64>(c, txc, lmax, tau, vol, rkey, magic, s);
-        case 192: return launch_runs_w<CROSS, STORE, FULL, 96>(c, txc, lmax, tau, vol, rkey, magic, s);
-        case 256: return launch_runs_w<CROSS, STORE, FULL, 128>(c, txc, lmax, tau, vol, rkey, magic, s);
-        default: return launch_runs_w<CROSS, STORE, FULL, 0>(c, txc, lmax, tau, vol, rkey, magic, s);
+        case 64: return launch_runs_w<CROSS, STORE, FULL, 1>(c, txc, lmax, tau, vol, rkey, magic, s);
+        case 128: return launch_runs_w<CROSS, STORE, FULL, 2>(c, txc, lmax, tau, vol, rkey, magic, s);
+        case 192: return launch_runs_w<CROSS, STORE, FULL, 3>(c, txc, lmax, tau, vol, rkey, magic, s);
+        default: return launch_runs_w<CROSS, STORE, FULL, 4>(c, txc, lmax, tau, vol, rkey, magic, s);
     }
 }
 
@@ -360,13 +449,13 @@ cudaError_t launch_runs_t(const CostCtx& c, int txc, int lmax, int tau, uint32_t
 
 size_t cost_runs_smem_bytes(const CostCtx& c, int mode, int lmax) {
     const bool full = c.use_ad || c.use_grad;
-    const int txc = mode == 1 ? (c.Dp <= 128 ? 128 : 64) : 256;
-    return run_geom(c, txc, mode == 1 ? lmax : 0, mode == 1, full).total;
+    if (mode == 1) return run_geom(c, cross_tile(c, lmax, full), lmax, true, full).total;
+    return run_geom(c, 256, 0, false, full).total;
 }
 
 bool cost_runs_supported(const CostCtx& c, int mode, int lmax) {
     if (c.kernel == 1 || c.census64 || c.prior_ranges) return false;
-    if (c.Dp % 64 != 0 || c.Dp > 512) return false;
+    if (c.Dp % 64 != 0 || c.Dp > 256) return false;
     const bool full = c.use_ad || c.use_grad;
     if (mode == 2 && full) return false;  // the fused form exists for census-only costs
     if (mode == 1 && lmax > 127) return false;
@@ -377,10 +466,7 @@ cudaError_t launch_cost_runs(const CostCtx& c, int mode, int lmax, int tau, uint
                              const uint32_t* magic, cudaStream_t s) {
     const bool full = c.use_ad || c.use_grad;
     if (mode == 1) {
-        int txc = c.Dp <= 128 ? 128 : 64;
-        if ((c.tile == 64 || c.tile == 128 || c.tile == 256) &&
-            run_geom(c, c.tile, lmax, true, full).total <= 200 * 1024)
-            txc = c.tile;
+        const int txc = cross_tile(c, lmax, full);
         return full ? launch_runs_t<true, true, true>(c, txc, lmax, tau, vol, rkey, magic, s)
                     : launch_runs_t<true, true, false>(c, txc, lmax, tau, vol, rkey, magic, s);
     }
