@@ -264,10 +264,11 @@ cudaError_t launch_cross_v(int w, int h, int d0, int D, int Dp, int lmax, int ta
     const int W2 = Dp / 2;
     const int cols = W2 >= 128 ? 1 : 128 / W2;
     const int nthr = W2 * cols;
-    // fast path: default ranges, non-negative disparities, and a ring holding the 2*lmax+2 window
-    // prefixes plus a loaded batch
+    // fast path: default ranges, non-negative disparities, and a ring holding the window's prefixes
+    // plus the batch pushed ahead: rows from y - lmax - 1 up to y + lmax + kB - 1 are live, and a
+    // ring of more than 2*lmax + kB slots never overwrites one before its last read
     if (default_ranges && d0 >= 0 && nthr <= 128) {
-        const int span = 2 * lmax + 2 + 2 * kB;
+        const int span = 2 * lmax + kB + 2;
         const size_t extra = (size_t)(2 * lmax + 2) * 4 + (size_t)cols * (kSeg + 2 * lmax) + (size_t)cols * kSeg * 2;
         auto go = [&](auto rs_tag) -> cudaError_t {
             constexpr int RS = decltype(rs_tag)::value;
