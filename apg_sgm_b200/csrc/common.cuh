@@ -42,30 +42,6 @@ struct CostCtx {
     int kernel;        // cost kernel: 0 = pixel runs where they apply, 1 = column tiles always
 };
 
-// Quantised cost of left (x, y) against right (xr, y) from LUTs held in shared memory.
-// Same operation order as src/cost_computer.cpp:247-264; every float op is rounded on its own
-// (no contraction), so the u16 result equals the reference bit for bit.
-template <bool C64>
-__device__ __forceinline__ uint16_t quantised_cost(const CostCtx& c, const float* s_lut, uint32_t cl32,
-                                                   unsigned long long cl64v, int gl, int gxl, int gyl,
-                                                   int row, int xr) {
-    int pop;
-    if (C64) pop = __popcll(cl64v ^ c.cr64[row + xr]);
-    else pop = __popc(cl32 ^ c.cr[row + xr]);
-    float v = s_lut[kLutCensus + pop];
-    if (c.use_ad) {
-        const int ad = abs(gl - (int)c.rgray[row + xr]);
-        v = __fadd_rn(v, s_lut[kLutAd + ad]);
-    }
-    if (c.use_grad) {
-        const int g = abs(gxl - (int)c.rgx[row + xr]) + abs(gyl - (int)c.rgy[row + xr]);
-        v = __fadd_rn(v, s_lut[kLutGrad + g]);
-    }
-    int q = __float2int_rz(__fadd_rn(__fmul_rn(v, c.scale), 0.5f));
-    q = q < 0 ? 0 : (q > c.cost_max ? c.cost_max : q);
-    return (uint16_t)q;
-}
-
 // Unquantised (float) cost, used by the refiner's local cost (src/refiner.cpp:14-36).
 template <bool C64>
 __device__ __forceinline__ float raw_cost(const CostCtx& c, const float* lut, int x, int y, int xr) {

@@ -410,22 +410,32 @@ __global__ void right_wta_finalize_kernel(CostCtx c, const uint32_t* __restrict_
             const int bd = c.d0 + di;
             dv = (float)bd;
             const int y = p / c.w, xr = p - y * c.w;
-            const int xm = xr + bd - 1, x0 = xr + bd, xp = xr + bd + 1;
-            if (subpixel && xm >= 0 && xm < c.w && x0 >= 0 && x0 < c.w && xp >= 0 && xp < c.w && di > 0 &&
-                di + 1 < c.D) {
+            const int xm = xr + bd - 1, xp = xr + bd + 1;
+            if (subpixel && xm >= 0 && xp < c.w && di > 0 && di + 1 < c.D) {
                 const int row = y * c.w;
-                // C(xl, d) is valid iff d is inside range(xl) and xl - d is inside the image;
-                // here xl - d == xr for all three, so only the range test remains.
+                // C(xl, d) is valid iff d is inside range(xl) and xl - d is inside the image; here
+                // xl - d == xr for all three, so only the range test remains, and with the default
+                // ranges it always holds (d >= d0, d < dmax, d <= xl).  The right pixel's
+                // descriptors are the same for the three costs (src/cost_computer.cpp:247-264).
+                const int rg = c.rgray[row + xr], rgx = c.rgx[row + xr], rgy = c.rgy[row + xr];
+                uint32_t rc32 = 0;
+                unsigned long long rc64 = 0;
+                if (C64) rc64 = c.cr64[row + xr];
+                else rc32 = c.cr[row + xr];
                 auto cost_at = [&](int xl, int d, uint32_t& out) -> bool {
-                    if (d < c.rmin[row + xl] || d >= c.rmax[row + xl]) return false;
-                    if (C64) out = quantised_cost<true>(c, s_lut, 0u, c.cl64[row + xl], c.lgray[row + xl],
-                                                        c.lgx[row + xl], c.lgy[row + xl], row, xr);
-                    else out = quantised_cost<false>(c, s_lut, c.cl[row + xl], 0ull, c.lgray[row + xl],
-                                                     c.lgx[row + xl], c.lgy[row + xl], row, xr);
+                    if (c.prior_ranges && (d < c.rmin[row + xl] || d >= c.rmax[row + xl])) return false;
+                    const int pop = C64 ? __popcll(c.cl64[row + xl] ^ rc64) : __popc(c.cl[row + xl] ^ rc32);
+                    float v = s_lut[kLutCensus + pop];
+                    if (c.use_ad) v = __fadd_rn(v, s_lut[kLutAd + abs((int)c.lgray[row + xl] - rg)]);
+                    if (c.use_grad)
+                        v = __fadd_rn(v, s_lut[kLutGrad + abs((int)c.lgx[row + xl] - rgx) + abs((int)c.lgy[row + xl] - rgy)]);
+                    int q = __float2int_rz(__fadd_rn(__fmul_rn(v, c.scale), 0.5f));
+                    q = q < 0 ? 0 : (q > c.cost_max ? c.cost_max : q);
+                    out = (uint32_t)q;
                     return true;
                 };
                 uint32_t cm, c0v, cp;
-                if (cost_at(xm, bd - 1, cm) && cost_at(x0, bd, c0v) && cost_at(xp, bd + 1, cp))
+                if (cost_at(xm, bd - 1, cm) && cost_at(xm + 1, bd, c0v) && cost_at(xp, bd + 1, cp))
                     dv = __fadd_rn(dv, legacy_delta((float)cm, (float)c0v, (float)cp));
             }
         }
@@ -436,7 +446,7 @@ __global__ void right_wta_finalize_kernel(CostCtx c, const uint32_t* __restrict_
 cudaError_t launch_right_wta_finalize(const CostCtx& c, const uint32_t* rkey, int subpixel, float* disp_right,
                                       cudaStream_t s) {
     const int n = c.w * c.h;
-    const int blocks = min((n + 255) / 256, 148 * 8);
+    const int blocks = min((n + 255) / 256, 148 * 4);  // each block stages the LUT once
     if (c.census64) right_wta_finalize_kernel<true><<<blocks, 256, 0, s>>>(c, rkey, subpixel, disp_right);
     else right_wta_finalize_kernel<false><<<blocks, 256, 0, s>>>(c, rkey, subpixel, disp_right);
     return cudaGetLastError();

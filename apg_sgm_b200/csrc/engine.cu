@@ -229,6 +229,29 @@ int Engine::cuda_fail(cudaError_t e, const char* where) {
     return e == cudaErrorMemoryAllocation ? kAllocationFailure : kInternalError;
 }
 
+// The per-pixel range planes are read by the prior and the refiner, the stage dumps, the general
+// vertical aggregation (negative minimum disparity or more than 256 padded disparities) and the
+// aggregation iterations after the first.  Every other consumer -- the cost kernels, the
+// right-image sub-pixel step and the frame counters -- uses the default range
+// [d0, max(min(dmax, x + 1), d0)) in closed form, so without those readers the planes are not
+// written at all.
+bool Engine::range_planes_needed() const {
+    // the stage-dump debug flags keep every intermediate; the launch profile alone changes no work
+    if (cfg_.prior_enable || cfg_.refine_enable || (debug_ & ~8)) return true;
+    return cfg_.agg_enable && (cfg_.agg_iterations > 1 || cfg_.min_disparity < 0 || lay_.Dp > 256);
+}
+
+// Sum over the frame of the default range widths max(min(dmax, x + 1) - d0, 0)
+// (PipelineStats' search-width total for frames without a prior).
+unsigned long long Engine::default_range_width_sum() const {
+    unsigned long long row = 0;
+    for (int x = 0; x < lay_.w; ++x) {
+        const int wd = std::min(cfg_.max_disparity, x + 1) - cfg_.min_disparity;
+        row += wd > 0 ? (unsigned long long)wd : 0ull;
+    }
+    return row * (unsigned long long)lay_.h;
+}
+
 CostCtx Engine::cost_ctx() const {
     CostCtx c;
     c.w = lay_.w; c.h = lay_.h; c.d0 = cfg_.min_disparity; c.D = lay_.D; c.Dp = lay_.Dp;
@@ -460,7 +483,10 @@ int Engine::run_pre(const uint8_t* dl, int lstride, const uint8_t* dr, int rstri
     RUN(launch_aux(dr, rstride, ch, w, h, c64, ptr<uint8_t>(L.rgray), ptr<uint8_t>(L.rgx), ptr<uint8_t>(L.rgy),
                    ptr<uint32_t>(L.cr), ptr<unsigned long long>(L.cr), s), "aux(right)");
     cudaEventRecord(ev_[1], s);
-    RUN(launch_default_range(w, h, d0, cfg_.max_disparity, ptr<int16_t>(L.rmin), ptr<int16_t>(L.rmax), s), "range");
+    ranges_written_ = range_planes_needed();
+    if (ranges_written_)
+        RUN(launch_default_range(w, h, d0, cfg_.max_disparity, ptr<int16_t>(L.rmin), ptr<int16_t>(L.rmax), s),
+            "range");
     const CostCtx cc = cost_ctx();
     support_count_ = 0;
     if (cfg_.prior_enable) {
@@ -719,9 +745,12 @@ int Engine::run_post(float* d_disp, float* d_conf, uint8_t* d_reason, uint8_t* d
     // the refined one, prior_support_count is the prior's selected-support count
     unsigned long long* st = ptr<unsigned long long>(L.stats);
     RUNC(cudaMemsetAsync(st, 0, 64, s), "stats init");
+    const bool planes = range_planes_needed();
     RUN(launch_frame_stats((int)n, final_out, ptr<uint8_t>(L.reliable), ptr<uint8_t>(L.reason),
                            refine ? ptr<float>(L.disp_wta) : nullptr, refine ? ptr<float>(L.disp_ref) : nullptr,
-                           ptr<int16_t>(L.rmin), ptr<int16_t>(L.rmax), st, s), "frame stats");
+                           planes ? ptr<int16_t>(L.rmin) : nullptr, planes ? ptr<int16_t>(L.rmax) : nullptr,
+                           planes ? 0ull : default_range_width_sum(), st, s),
+        "frame stats");
     if (cfg_.prior_enable) RUNC(cudaMemcpyAsync(st + 5, arena_ + L.pr_count, 4, cudaMemcpyDeviceToDevice, s), "support count");
     cudaEventRecord(ev_[9], s);
     have_times_ = true;
@@ -840,8 +869,18 @@ int Engine::dump(int what, void* dst, size_t bytes) {
         case 5: off = L.rgy; sz = n; break;
         case 6: off = L.cl; sz = n * csz; break;
         case 7: off = L.cr; sz = n * csz; break;
-        case 8: off = L.rmin; sz = n * 2; break;
-        case 9: off = L.rmax; sz = n * 2; break;
+        case 8:
+        case 9:
+            off = what == 8 ? L.rmin : L.rmax;
+            sz = n * 2;
+            if (!ranges_written_) {
+                // the frame used the default ranges in closed form: write the planes now
+                const cudaError_t e = launch_default_range(L.w, L.h, cfg_.min_disparity, cfg_.max_disparity,
+                                                           ptr<int16_t>(L.rmin), ptr<int16_t>(L.rmax), stream_);
+                if (e != cudaSuccess) return cuda_fail(e, "range planes");
+                ranges_written_ = true;
+            }
+            break;
         case 10: if (!L.raw_cost) return fail(kInternalError, "raw cost not materialised"); off = L.volRaw; vol = true; break;
         case 11: if (!L.cross) return fail(kInternalError, "no aggregated volume"); off = L.volB; vol = true; break;
         case 12: if (!(debug_ & 2)) return fail(kInternalError, "path sum not kept"); off = L.sbuf[0]; vol = true; break;

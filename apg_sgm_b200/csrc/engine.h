@@ -137,6 +137,8 @@ private:
     int cuda_fail(cudaError_t e, const char* where);
     template <typename T> T* ptr(size_t off) const { return reinterpret_cast<T*>(arena_ + off); }
     CostCtx cost_ctx() const;
+    bool range_planes_needed() const;
+    unsigned long long default_range_width_sum() const;
 
     apg_pipeline_config_t cfg_;
     int device_ = 0;
@@ -153,7 +155,8 @@ private:
     // host staging (pinned)
     unsigned char* pin_ = nullptr;
     size_t pinned_bytes_ = 0;
-    bool direct_out_ = false;  // the last download() wrote the caller's page-locked (or device) outputs
+    bool direct_out_ = false;
+    bool ranges_written_ = false;  // the last frame wrote the range planes (else: default ranges)  // the last download() wrote the caller's page-locked (or device) outputs
     std::vector<float> lut_host_;
     std::vector<uint16_t> qlut_host_;
     cudaEvent_t ev_[12] = {};

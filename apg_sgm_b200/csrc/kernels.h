@@ -107,7 +107,7 @@ cudaError_t launch_fill(int w, int h, int gap, const float* in, const uint8_t* r
 cudaError_t launch_median(int w, int h, int r, const float* in, float* out, cudaStream_t s);
 cudaError_t launch_frame_stats(int n, const float* disp, const uint8_t* reliable, const uint8_t* reason,
                                const float* before, const float* after, const int16_t* rmin, const int16_t* rmax,
-                               unsigned long long* out5, cudaStream_t s);
+                               unsigned long long range_sum, unsigned long long* out5, cudaStream_t s);
 
 // range.cu (default range, HQ prior, refine)
 cudaError_t launch_default_range(int w, int h, int d0, int dmax, int16_t* rmin, int16_t* rmax, cudaStream_t s);

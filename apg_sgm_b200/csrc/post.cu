@@ -5,6 +5,8 @@
 // (src/postprocess.cpp:10-40, 42-168, 255-309).  Every float expression keeps the reference's
 // operation order with explicitly rounded intrinsics (no contraction), so outputs are bit-exact.
 // These kernels touch O(W*H) bytes and are a few microseconds each at 720p.
+#include <algorithm>
+
 #include "common.cuh"
 #include "kernels.h"
 
@@ -183,11 +185,199 @@ __global__ void median_kernel(int w, int h, int r, const float* __restrict__ in,
     }
 }
 
+// The same fill with the neighbour search done by warp ballots: a warp owns 32 consecutive pixels
+// of a row; the walk of the reference (xl = x - 1 down while xl >= max(x - gap, 0) and
+// row[xl] < 0) stops at the nearest "stopper" q, a pixel with !(row[q] < 0), or ends one beyond the
+// gap.  The nearest stopper on each side comes from the segments' stopper masks (this segment,
+// then further ones while some lane's gap reaches them), so each pixel costs a few bit operations
+// instead of a walk.  Everything after the two neighbours is the per-pixel rule above.
+__global__ void fill_ballot_kernel(int w, int h, int gap, const float* __restrict__ in,
+                                   const uint8_t* __restrict__ reason, const uint8_t* __restrict__ gray,
+                                   const float* __restrict__ d_prior, float* __restrict__ out) {
+    const int lane = threadIdx.x & 31;
+    const int nseg = (w + 31) >> 5;
+    const long long total = (long long)nseg * h;
+    const long long wstride = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long sg = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; sg < total; sg += wstride) {
+        const int y = (int)(sg / nseg), s = (int)(sg - (long long)y * nseg);
+        const int x = (s << 5) + lane;
+        const float* row = in + (size_t)y * w;
+        const bool inimg = x < w;
+        const float v = inimg ? row[x] : 0.f;
+        const bool hole = inimg && !(v >= 0.f);
+        if (!__any_sync(0xFFFFFFFFu, hole)) {
+            if (inimg) out[(size_t)y * w + x] = v;
+            continue;
+        }
+        const unsigned stop = __ballot_sync(0xFFFFFFFFu, inimg && !(v < 0.f));
+        // left: largest stopper in [max(x - gap, 0), x - 1]
+        int ql = -1;
+        {
+            const unsigned below = stop & ((1u << lane) - 1u);
+            if (below) ql = (s << 5) + 31 - __clz(below);
+            bool need = hole && !below;
+            for (int k = s - 1; __any_sync(0xFFFFFFFFu, need && (k << 5) + 31 >= x - gap && k >= 0); --k) {
+                const unsigned mk = __ballot_sync(0xFFFFFFFFu, !(row[(k << 5) + lane] < 0.f));
+                if (need && mk) {
+                    ql = (k << 5) + 31 - __clz(mk);
+                    need = false;
+                }
+            }
+        }
+        // right: smallest stopper in [x + 1, min(x + gap, w - 1)]
+        int qr = w;
+        {
+            const unsigned above = lane < 31 ? (stop & ~((2u << lane) - 1u)) : 0u;
+            if (above) qr = (s << 5) + __ffs(above) - 1;
+            bool need = hole && !above;
+            for (int k = s + 1; __any_sync(0xFFFFFFFFu, need && (k << 5) <= x + gap && k < nseg); ++k) {
+                const int xx = (k << 5) + lane;
+                const unsigned mk = __ballot_sync(0xFFFFFFFFu, xx < w && !(row[xx] < 0.f));
+                if (need && mk) {
+                    qr = (k << 5) + __ffs(mk) - 1;
+                    need = false;
+                }
+            }
+        }
+        if (!hole) {
+            if (inimg) out[(size_t)y * w + x] = v;
+            continue;
+        }
+        const int xl = (ql >= 0 && ql >= x - gap) ? ql : max(x - gap - 1, -1);
+        const int xr = (qr < w && qr <= x + gap) ? qr : min(x + gap + 1, w);
+        const float dl = (xl >= 0 && row[xl] >= 0.f) ? row[xl] : -1.f;
+        const float dr = (xr < w && row[xr] >= 0.f) ? row[xr] : -1.f;
+        const size_t i = (size_t)y * w + x;
+        float o = v;
+        if (reason[i] == kOcclusion) {
+            if (dl >= 0.f && dr >= 0.f) o = (dr < dl) ? dr : dl;
+            else if (dl >= 0.f) o = dl;
+            else if (dr >= 0.f) o = dr;
+            out[i] = o;
+            continue;
+        }
+        const int c0 = gray[i];
+        float best_d = -1.f;
+        int best_abs = 999;
+        const int cx[4] = {xl, xr, x, x};
+        const int cy[4] = {y, y, y - 1, y + 1};
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int xx = cx[k], yy = cy[k];
+            if (xx < 0 || yy < 0 || xx >= w || yy >= h) continue;
+            const float dv = in[(size_t)yy * w + xx];
+            if (dv < 0.f) continue;
+            const int ad = abs((int)gray[(size_t)yy * w + xx] - c0);
+            if (ad < best_abs) { best_abs = ad; best_d = dv; }
+        }
+        if (best_d >= 0.f && best_abs <= 18) {
+            o = best_d;
+        } else if (d_prior && d_prior[i] >= 0.f) {
+            o = d_prior[i];
+        } else if (dl >= 0.f && dr >= 0.f) {
+            const float t = __fdiv_rn((float)(x - xl), (float)(xr - xl));
+            o = __fadd_rn(__fmul_rn(dl, __fsub_rn(1.f, t)), __fmul_rn(dr, t));
+        } else if (dl >= 0.f) {
+            o = dl;
+        } else if (dr >= 0.f) {
+            o = dr;
+        }
+        out[i] = o;
+    }
+}
+
+// The 3x3 case (median_radius 1, the default) over a staged 34x10 tile: each thread sorts its nine
+// window values in registers with a 25-exchange sorting network (invalid values, !(v >= 0), as
+// +inf, so the cnt valid ones come first) and takes entry cnt/2 -- the cnt/2-th smallest, as the
+// rank count above.  Equal values are interchangeable except +0 and -0; when the selected value is
+// a zero, the first valid zero in raster order is returned, as the rank count does.
+constexpr int kMedTX = 32, kMedTY = 8;
+
+__device__ __forceinline__ void cswap(float& a, float& b) {
+    const float lo = fminf(a, b), hi = fmaxf(a, b);
+    a = lo;
+    b = hi;
+}
+
+__global__ void __launch_bounds__(kMedTX * kMedTY) median3_kernel(int w, int h, const float* __restrict__ in,
+                                                                  float* __restrict__ out) {
+    __shared__ float t[kMedTY + 2][kMedTX + 2];
+    const int x0 = blockIdx.x * kMedTX, y0 = blockIdx.y * kMedTY;
+    const int tid = threadIdx.y * kMedTX + threadIdx.x;
+    for (int i = tid; i < (kMedTY + 2) * (kMedTX + 2); i += kMedTX * kMedTY) {
+        const int sy = i / (kMedTX + 2), sx = i - sy * (kMedTX + 2);
+        const int yy = y0 + sy - 1, xx = x0 + sx - 1;
+        // outside the image: not part of the window (invalid)
+        t[sy][sx] = (xx >= 0 && xx < w && yy >= 0 && yy < h) ? in[(size_t)yy * w + xx] : -1.f;
+    }
+    __syncthreads();
+    const int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
+    if (x >= w || y >= h) return;
+    float v[9];
+    int cnt = 0;
+#pragma unroll
+    for (int dy = 0; dy < 3; ++dy)
+#pragma unroll
+        for (int dx = 0; dx < 3; ++dx) {
+            const float u = t[threadIdx.y + dy][threadIdx.x + dx];
+            const bool ok = u >= 0.f;
+            cnt += ok;
+            v[dy * 3 + dx] = ok ? u : __int_as_float(0x7f800000);
+        }
+    const float center = t[threadIdx.y + 1][threadIdx.x + 1];
+    if (cnt == 0) {
+        out[(size_t)y * w + x] = center;
+        return;
+    }
+    float s[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) s[i] = v[i];
+    // 9-input sorting network (25 compare-exchanges)
+    cswap(s[0], s[3]); cswap(s[1], s[7]); cswap(s[2], s[5]); cswap(s[4], s[8]);
+    cswap(s[0], s[7]); cswap(s[2], s[4]); cswap(s[3], s[8]); cswap(s[5], s[6]);
+    cswap(s[0], s[2]); cswap(s[1], s[3]); cswap(s[4], s[5]); cswap(s[7], s[8]);
+    cswap(s[1], s[4]); cswap(s[3], s[6]); cswap(s[5], s[7]);
+    cswap(s[0], s[1]); cswap(s[2], s[4]); cswap(s[3], s[5]); cswap(s[6], s[8]);
+    cswap(s[2], s[3]); cswap(s[4], s[5]); cswap(s[6], s[7]);
+    cswap(s[1], s[2]); cswap(s[3], s[4]); cswap(s[5], s[6]);
+    const int k = cnt / 2;
+    float res = s[0];
+#pragma unroll
+    for (int i = 1; i < 9; ++i)
+        if (i == k) res = s[i];
+    if (res == 0.f) {
+        // the sign of the first valid zero in raster order
+#pragma unroll
+        for (int i = 8; i >= 0; --i)
+            if (v[i] == 0.f) res = v[i];
+    }
+    out[(size_t)y * w + x] = res;
+}
+
 // Frame counters of PipelineStats (src/pipeline.cpp:650-707): out[0] valid (disparity >= 0),
 // out[1] reliable (mask != 0), out[2] lr_fail (reason Occlusion or Mismatch), out[3] refine_changed
 // (before and after both >= 0 and |after - before| > 1e-4), out[4] sum over pixels of the search
-// range width max(hi - lo, 0).  Warp and block reductions, then one 64-bit atomic per block and
-// counter (a few hundred blocks: same-address atomics serialise at L2); out[] starts at zero.
+// range width max(hi - lo, 0) -- read from the range planes, or, for the default ranges (rmin
+// null), the host's closed form `range_sum`.  Four pixels per thread and step when the buffers
+// allow 16-byte and 4-byte loads (n4 = n / 4, the tail one pixel at a time), warp
+// and block reductions, then one 64-bit atomic per block and counter (a few hundred blocks:
+// same-address atomics serialise at L2); out[] starts at zero.
+__device__ __forceinline__ void stats_pixel(unsigned long long (&c)[5], float d, uint8_t rel, uint8_t r,
+                                            const float* before, const float* after, const int16_t* rmin,
+                                            const int16_t* rmax, int p) {
+    c[0] += d >= 0.f;
+    c[1] += rel != 0;
+    c[2] += (r == kOcclusion || r == kMismatch);
+    if (before) {
+        const float db = before[p], da = after[p];
+        c[3] += (db >= 0.f && da >= 0.f && fabsf(__fsub_rn(da, db)) > 1e-4f);
+    }
+    if (rmin) {
+        const int wd = (int)rmax[p] - (int)rmin[p];
+        c[4] += wd > 0 ? (unsigned)wd : 0u;
+    }
+}
+
 __global__ void __launch_bounds__(256) frame_stats_kernel(int n, const float* __restrict__ disp,
                                                           const uint8_t* __restrict__ reliable,
                                                           const uint8_t* __restrict__ reason,
@@ -195,20 +385,27 @@ __global__ void __launch_bounds__(256) frame_stats_kernel(int n, const float* __
                                                           const float* __restrict__ after,
                                                           const int16_t* __restrict__ rmin,
                                                           const int16_t* __restrict__ rmax,
+                                                          unsigned long long range_sum, bool vec,
                                                           unsigned long long* __restrict__ out) {
     unsigned long long c[5] = {0, 0, 0, 0, 0};
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
-        c[0] += disp[p] >= 0.f;
-        c[1] += reliable[p] != 0;
-        const uint8_t r = reason[p];
-        c[2] += (r == kOcclusion || r == kMismatch);
-        if (before) {
-            const float db = before[p], da = after[p];
-            c[3] += (db >= 0.f && da >= 0.f && fabsf(__fsub_rn(da, db)) > 1e-4f);
+    const int stride = gridDim.x * blockDim.x;
+    int tail = 0;
+    if (vec) {
+        const int n4 = n / 4;
+        for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n4; q += stride) {
+            const float4 d = reinterpret_cast<const float4*>(disp)[q];
+            const uchar4 rl = reinterpret_cast<const uchar4*>(reliable)[q];
+            const uchar4 rs = reinterpret_cast<const uchar4*>(reason)[q];
+            stats_pixel(c, d.x, rl.x, rs.x, before, after, rmin, rmax, 4 * q);
+            stats_pixel(c, d.y, rl.y, rs.y, before, after, rmin, rmax, 4 * q + 1);
+            stats_pixel(c, d.z, rl.z, rs.z, before, after, rmin, rmax, 4 * q + 2);
+            stats_pixel(c, d.w, rl.w, rs.w, before, after, rmin, rmax, 4 * q + 3);
         }
-        const int wd = (int)rmax[p] - (int)rmin[p];
-        c[4] += wd > 0 ? (unsigned)wd : 0u;
+        tail = 4 * n4;
     }
+    for (int p = tail + blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride)
+        stats_pixel(c, disp[p], reliable[p], reason[p], before, after, rmin, rmax, p);
+    if (blockIdx.x == 0 && threadIdx.x == 0) c[4] += range_sum;
     __shared__ unsigned long long s_c[5][8];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
@@ -246,20 +443,35 @@ cudaError_t launch_lr(int w, int h, int lr_max_diff, const float* dr, const floa
 
 cudaError_t launch_fill(int w, int h, int gap, const float* in, const uint8_t* reason, const uint8_t* gray,
                         const float* d_prior, float* out, cudaStream_t s) {
-    fill_kernel<<<grid_for(w * h), 256, 0, s>>>(w, h, gap, in, reason, gray, d_prior, out);
+    if (gap >= 0) {
+        const long long warps = (long long)((w + 31) / 32) * h;
+        const int blocks = (int)std::min<long long>((warps + 7) / 8, 148 * 16);
+        fill_ballot_kernel<<<blocks, 256, 0, s>>>(w, h, gap, in, reason, gray, d_prior, out);
+    } else {
+        fill_kernel<<<grid_for(w * h), 256, 0, s>>>(w, h, gap, in, reason, gray, d_prior, out);
+    }
     return cudaGetLastError();
 }
 
 cudaError_t launch_median(int w, int h, int r, const float* in, float* out, cudaStream_t s) {
-    median_kernel<<<grid_for(w * h), 256, 0, s>>>(w, h, r, in, out);
+    if (r == 1) {
+        const dim3 grid((w + kMedTX - 1) / kMedTX, (h + kMedTY - 1) / kMedTY), block(kMedTX, kMedTY);
+        median3_kernel<<<grid, block, 0, s>>>(w, h, in, out);
+    } else {
+        median_kernel<<<grid_for(w * h), 256, 0, s>>>(w, h, r, in, out);
+    }
     return cudaGetLastError();
 }
 
 cudaError_t launch_frame_stats(int n, const float* disp, const uint8_t* reliable, const uint8_t* reason,
                                const float* before, const float* after, const int16_t* rmin, const int16_t* rmax,
-                               unsigned long long* out5, cudaStream_t s) {
+                               unsigned long long range_sum, unsigned long long* out5, cudaStream_t s) {
     const int blocks = (n + 255) / 256 < 148 * 2 ? (n + 255) / 256 : 148 * 2;
-    frame_stats_kernel<<<blocks, 256, 0, s>>>(n, disp, reliable, reason, before, after, rmin, rmax, out5);
+    // 16-byte loads of the map and 4-byte loads of the byte planes need those alignments
+    const bool vec = ((reinterpret_cast<uintptr_t>(disp) & 15) | (reinterpret_cast<uintptr_t>(reliable) & 3) |
+                      (reinterpret_cast<uintptr_t>(reason) & 3)) == 0;
+    frame_stats_kernel<<<blocks, 256, 0, s>>>(n, disp, reliable, reason, before, after, rmin, rmax, range_sum, vec,
+                                              out5);
     return cudaGetLastError();
 }
 

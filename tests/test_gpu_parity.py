@@ -212,3 +212,19 @@ def test_cost_tile_changes_no_result(apg, mode, tile):
     b = e.process(L, R)
     for k in a:
         assert same_bits(a[k], b[k]), k
+
+
+@pytest.mark.parametrize("mode,dmin", [(0, 0), (1, 0), (1, 8)])
+def test_range_dump_without_debug(apg, mode, dmin):
+    """Frames without a prior use the default ranges in closed form and skip writing the range
+    planes; a later dump writes them on demand: [d0, max(min(dmax, x + 1), d0)) per column."""
+    w, h, dmax = 150, 20, 64
+    L, R = synth(w, h, dmax, seed=3)
+    e = apg.Engine(apg.config_from_mode(mode, dmax, dmin))
+    e.process(L, R)
+    rmin, rmax = e.dump("range_min"), e.dump("range_max")
+    e.close()
+    x = np.arange(w)
+    want_max = np.maximum(np.minimum(dmax, x + 1), dmin).astype(np.int16)
+    assert (rmin == dmin).all()
+    assert (rmax == want_max[None, :]).all()
