@@ -486,39 +486,62 @@ __host__ __device__ constexpr int wta_buf_words() { return 32 * (K * T + 1); }
 // lane (wta_impl, src/sgm_optimizer.cpp:465-536): the first minimum, the second minimum outside
 // |d - best| <= 1, the legacy parabola.  Sums >= 0x7FFF are invalid.  A negative winning
 // disparity reads as "none" like the reference's best_d < 0 test (:490-495).
-__device__ __forceinline__ void wta_row(const SgmArgs& a, const uint32_t* row, int W2, int p) {
-    uint32_t m2 = 0xFFFFFFFFu;
-    for (int k = 0; k < W2; ++k) m2 = __vminu2(m2, row[k]);
-    const uint32_t m = min_halves(m2);
+template <int W2>
+__device__ __forceinline__ void wta_row(const SgmArgs& a, const uint32_t* row, int p) {
+    // one pass over the row keeps the minimum of each chunk of CS words in registers; the first
+    // index and the second minimum then read at most three chunks again
+    constexpr int CS = W2 / 16 >= 4 ? W2 / 16 : 4;  // words per chunk (W2 is a multiple of 8)
+    constexpr int NC = W2 / CS;
+    uint32_t cmin[NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+        uint32_t v = row[c * CS];
+#pragma unroll
+        for (int i = 1; i < CS; ++i) v = __vminu2(v, row[c * CS + i]);
+        cmin[c] = v;
+    }
+    uint32_t all = cmin[0];
+#pragma unroll
+    for (int c = 1; c < NC; ++c) all = __vminu2(all, cmin[c]);
+    const uint32_t m = min_halves(all);
     float dval = -1.f, fb = __int_as_float(0x7f800000), fs = __int_as_float(0x7f800000);
     if (m < kInf) {
-        const uint32_t mm = m * 0x00010001u;
-        int bdi = 0;
-        for (int k = 0; k < W2; ++k) {
-            const uint32_t eq = __vcmpeq2(row[k], mm);
-            if (eq) {
-                bdi = 2 * k + ((eq & 0xFFFFu) ? 0 : 1);
-                break;
-            }
+        // the first chunk whose minimum is m, then the first halfword equal to m inside it
+        int fc = 0;
+#pragma unroll
+        for (int c = NC - 1; c >= 0; --c)
+            if (min_halves(cmin[c]) == m) fc = c;
+        int bdi = 2 * fc * CS;
+        for (int i = 0; i < CS; ++i) {
+            const uint32_t v = row[fc * CS + i];
+            if ((v & 0xFFFFu) == m) { bdi = 2 * (fc * CS + i); break; }
+            if ((v >> 16) == m) { bdi = 2 * (fc * CS + i) + 1; break; }
         }
         if (a.d0 + bdi >= 0) {
-            const int k0 = (bdi - 1) >> 1, k1 = (bdi + 1) >> 1;  // words touching [bdi-1, bdi+1]
-            uint32_t s2 = 0xFFFFFFFFu;
-            for (int k = 0; k < W2; ++k) {
-                uint32_t v = row[k];
-                if (k >= k0 && k <= k1) {
-                    if (abs(2 * k - bdi) <= 1) v |= 0x0000FFFFu;
-                    if (abs(2 * k + 1 - bdi) <= 1) v |= 0xFFFF0000u;
-                }
-                s2 = __vminu2(s2, v);
-            }
-            const uint32_t sec = min_halves(s2);
+            const uint16_t* r16 = reinterpret_cast<const uint16_t*>(row);
             dval = (float)(a.d0 + bdi);
             if (a.subpixel && bdi > 0 && bdi + 1 < a.D) {
-                const uint16_t* r16 = reinterpret_cast<const uint16_t*>(row);
                 const uint32_t cm = r16[bdi - 1], cp = r16[bdi + 1];
                 if (cm < kInf && cp < kInf) dval = __fadd_rn(dval, legacy_delta((float)cm, (float)m, (float)cp));
             }
+            // second minimum outside |d - best| <= 1: chunks without an excluded halfword keep
+            // their minimum; the (at most two) chunks with one are read again with those masked
+            const int klo = bdi > 0 ? (bdi - 1) >> 1 : 0, khi = min((bdi + 1) >> 1, W2 - 1);
+            const int clo = klo / CS, chi = khi / CS;
+            uint32_t sec2 = 0xFFFFFFFFu;
+#pragma unroll
+            for (int c = 0; c < NC; ++c)
+                if (c != clo && c != chi) sec2 = __vminu2(sec2, cmin[c]);
+            for (int c = clo; c <= chi; ++c) {
+                for (int i = 0; i < CS; ++i) {
+                    const int k = c * CS + i;
+                    uint32_t v = row[k];
+                    if (abs(2 * k - bdi) <= 1) v |= 0x0000FFFFu;
+                    if (abs(2 * k + 1 - bdi) <= 1) v |= 0xFFFF0000u;
+                    sec2 = __vminu2(sec2, v);
+                }
+            }
+            const uint32_t sec = min_halves(sec2);
             fb = (float)m;
             fs = sec >= kInf ? __int_as_float(0x7f800000) : (float)sec;
         }
@@ -671,7 +694,7 @@ __device__ __forceinline__ void run_chain_vol(const SgmArgs& a, const uint32_t* 
             // the block's T pixels: lane j of the group runs the WTA of pixel t0 + j of its chain
             __syncwarp();
             if (t0 + j < len)
-                wta_row(a, s_wta + grp * T * (K * T + 1) + j * (K * T + 1), K * T, p0 + (t0 + j) * step);
+                wta_row<K * T>(a, s_wta + grp * T * (K * T + 1) + j * (K * T + 1), p0 + (t0 + j) * step);
             __syncwarp();
         }
     }
@@ -693,11 +716,18 @@ __device__ __forceinline__ void run_chain_vol(const SgmArgs& a, const uint32_t* 
 #endif
 constexpr int kVolPfFirst = APGCU_SGM_PF_VOLUME_FIRST;
 constexpr int kVolPfLast = APGCU_SGM_PF_VOLUME_LAST;
-// Ring depth of the last sweep: the configured depth while 4 warps' rings and WTA buffers fit in
-// 200 KB of shared memory, else 4 (large disparity ranges).
+// Ring depth of the first phase: the configured depth, at most T (the P2 block of T steps is
+// walked in ring-sized pieces).
+template <int T>
+__host__ __device__ constexpr int first_pf() {
+    return kVolPfFirst < T ? kVolPfFirst : T;
+}
+// Ring depth of the last sweep: the configured depth (at most T) while 4 warps' rings and WTA
+// buffers fit in 200 KB of shared memory, else 4 (large disparity ranges).
 template <int K, int T, int NB>
 __host__ __device__ constexpr int last_pf() {
-    return (kVolPfLast * vol_slot_words<K, NB>() + wta_buf_words<K, T>()) * 4 * 4 <= 200 * 1024 ? kVolPfLast : 4;
+    constexpr int pf = kVolPfLast < T ? kVolPfLast : T;
+    return (pf * vol_slot_words<K, NB>() + wta_buf_words<K, T>()) * 4 * 4 <= 200 * 1024 ? pf : (T < 4 ? T : 4);
 }
 
 constexpr int multiple_of_both(int pf, int k2) {
@@ -737,8 +767,8 @@ __global__ void __launch_bounds__(128) sgm_first_kernel(SgmArgs a, DirTable tab)
     const int s = (warp - tab.warp_begin[d]) * C + (threadIdx.x & 31) / T;
     if constexpr (!CENSUS) {
         extern __shared__ __align__(16) uint32_t s_dyn[];
-        uint32_t* ring = s_dyn + (threadIdx.x >> 5) * kVolPfFirst * vol_slot_words<K, 0>();
-        run_chain_vol<T, K, kFirst, kVolPfFirst, 0>(a, tab.in, ring, nullptr, dx, dy, s, tab.nscan[d], tab.out[d]);
+        uint32_t* ring = s_dyn + (threadIdx.x >> 5) * first_pf<T>() * vol_slot_words<K, 0>();
+        run_chain_vol<T, K, kFirst, first_pf<T>(), 0>(a, tab.in, ring, nullptr, dx, dy, s, tab.nscan[d], tab.out[d]);
         return;
     }
     if (CENSUS && dy == 0) {
@@ -814,7 +844,7 @@ cudaError_t launch_first_tk(const SgmArgs& a, DirTable tab, bool census, cudaStr
     if (census) {
         sgm_first_kernel<T, K, true><<<blocks, 128, 0, st>>>(a, tab);
     } else {
-        const size_t smem = (size_t)4 * kVolPfFirst * vol_slot_words<K, 0>() * 4;
+        const size_t smem = (size_t)4 * first_pf<T>() * vol_slot_words<K, 0>() * 4;
         auto kern = sgm_first_kernel<T, K, false>;
         {
             const cudaError_t e = allow_dynamic_smem(kern, smem);
@@ -939,7 +969,7 @@ __global__ void __launch_bounds__(128) sgm_batch_kernel(const BatchPair* __restr
 
 template <int T, int K, int MODE, int NB>
 constexpr int batch_pf() {
-    return MODE == kFirst ? kVolPfFirst : last_pf<K, T, NB>();
+    return MODE == kFirst ? first_pf<T>() : last_pf<K, T, NB>();
 }
 
 template <int T, int K, int MODE, int NB>
