@@ -200,6 +200,125 @@ __global__ void __launch_bounds__(128) cross_v_default_kernel(int w, int h, int 
     }
 }
 
+// Vertical pass for any ranges (per-pixel ranges of the prior, negative disparities, wide
+// ranges): the batched, power-of-two ring form above plus a prefix of valid counts.  Sums are plain
+// 32-bit running sums of the packed words with invalid halves zeroed, and counts are 16-bit running
+// sums of (valid low half) | (valid high half) << 8: a window difference is exact in every lane
+// because a window's sum is below 2^16 (host-checked for the arm length and cost_max) and its
+// counts are at most 2*lmax + 1 <= 255.  The centre pixel's range is staged with the arms.
+template <int RS>
+__global__ void __launch_bounds__(256) cross_v_count_kernel(int w, int h, int d0, int D, int Dp, int lmax, int tau,
+                                                            int cols, const uint8_t* __restrict__ gray,
+                                                            const int16_t* __restrict__ rmin,
+                                                            const int16_t* __restrict__ rmax,
+                                                            const uint32_t* __restrict__ tin,
+                                                            uint32_t* __restrict__ cout,
+                                                            const uint32_t* __restrict__ magic) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int W2 = Dp / 2;
+    const int nthr = W2 * cols;
+    uint32_t* ring = reinterpret_cast<uint32_t*>(smem);                  // [RS][nthr] sums
+    uint32_t* s_rng = ring + (size_t)RS * nthr;                          // [cols][kSeg] lo | hi << 16
+    uint32_t* s_magic = s_rng + cols * kSeg;                             // [2*lmax+2]
+    uint16_t* ringc = reinterpret_cast<uint16_t*>(s_magic + 2 * lmax + 2);  // [RS][nthr] counts
+    uint8_t* s_gray = reinterpret_cast<uint8_t*>(ringc + (size_t)RS * nthr);  // [cols][kSeg + 2*lmax]
+    uint8_t* armU = s_gray + cols * (kSeg + 2 * lmax);                   // [cols][kSeg]
+    uint8_t* armD = armU + cols * kSeg;
+    const int xb = blockIdx.x * cols;
+    const int y0 = blockIdx.y * kSeg;
+    const int y1 = min(h, y0 + kSeg);
+    const int tid = threadIdx.x;
+    const int gs = kSeg + 2 * lmax;
+
+    for (int i = tid; i < 2 * lmax + 2; i += blockDim.x) s_magic[i] = magic[i];
+    for (int i = tid; i < cols * gs; i += blockDim.x) {
+        const int r = i / cols, ci = i - r * cols;
+        const int yy = y0 - lmax + r, x = xb + ci;
+        s_gray[ci * gs + r] = (x < w && yy >= 0 && yy < h) ? gray[yy * w + x] : 0;
+    }
+    __syncthreads();
+    for (int i = tid; i < cols * kSeg; i += blockDim.x) {
+        const int ci = i / kSeg, r = i - ci * kSeg;
+        const int yy = y0 + r, x = xb + ci;
+        int u = 0, v = 0;
+        uint32_t rg = 0;
+        if (x < w && yy < h) {
+            const uint8_t* g = s_gray + ci * gs + lmax + r;
+            const int c0 = g[0];
+            while (u < lmax && yy - u - 1 >= 0 && abs((int)g[-u - 1] - c0) <= tau) ++u;
+            while (v < lmax && yy + v + 1 < h && abs((int)g[v + 1] - c0) <= tau) ++v;
+            rg = (uint32_t)(uint16_t)rmin[yy * w + x] | ((uint32_t)(uint16_t)rmax[yy * w + x] << 16);
+        }
+        armU[i] = (uint8_t)u;
+        armD[i] = (uint8_t)v;
+        s_rng[i] = rg;
+    }
+    __syncthreads();
+    if (tid >= nthr) return;
+    const int ci = tid / W2, k = tid - ci * W2;
+    const int x = xb + ci;
+    if (x >= w) return;
+
+    const int ystart = max(0, y0 - lmax);
+    const int yend = min(h, y1 + lmax);
+    ring[tid] = 0;
+    ringc[tid] = 0;
+    const size_t rowstride = (size_t)w * W2;
+    const uint32_t* src = tin + ((size_t)ystart * w + x) * W2 + k;
+    uint32_t cur[kB], nxt[kB];
+#pragma unroll
+    for (int i = 0; i < kB; ++i) cur[i] = ystart + i < yend ? __ldcs(src + i * rowstride) : 0u;
+#pragma unroll
+    for (int i = 0; i < kB; ++i) nxt[i] = ystart + kB + i < yend ? __ldcs(src + (kB + i) * rowstride) : 0u;
+    int pushed = ystart;
+    uint32_t ps = 0;
+    uint32_t pc = 0;  // low 16 bits used
+    uint32_t* dst = cout + ((size_t)y0 * w + x) * W2 + k;
+    for (int y = y0; y < y1; ++y) {
+        const int need = min(h, y + lmax + 1);
+        while (pushed < need) {
+#pragma unroll
+            for (int i = 0; i < kB; ++i) {
+                if (pushed + i < yend) {
+                    const uint32_t v = cur[i];
+                    const bool lo_bad = (v & 0xFFFFu) == 0xFFFFu, hi_bad = v >= 0xFFFF0000u;
+                    ps += v & ((lo_bad ? 0u : 0x0000FFFFu) | (hi_bad ? 0u : 0xFFFF0000u));
+                    pc += (lo_bad ? 0u : 1u) + (hi_bad ? 0u : 0x100u);
+                    const int slot = ((pushed + i - ystart + 1) & (RS - 1)) * nthr + tid;
+                    ring[slot] = ps;
+                    ringc[slot] = (uint16_t)pc;
+                }
+            }
+            pushed += kB;
+#pragma unroll
+            for (int i = 0; i < kB; ++i) cur[i] = nxt[i];
+            const int base = pushed + kB;
+#pragma unroll
+            for (int i = 0; i < kB; ++i)
+                nxt[i] = base + i < yend ? __ldcs(src + (size_t)(base + i - ystart) * rowstride) : 0u;
+        }
+        const int ai = ci * kSeg + (y - y0);
+        const int a = y - armU[ai], b = y + armD[ai];  // inclusive window
+        const int sb = ((b - ystart + 1) & (RS - 1)) * nthr + tid, sa = ((a - ystart) & (RS - 1)) * nthr + tid;
+        const uint32_t sum = ring[sb] - ring[sa];
+        const uint32_t cnt = (uint32_t)(uint16_t)(ringc[sb] - ringc[sa]);
+        const uint32_t rg = s_rng[ai];
+        const int lo = (int16_t)(rg & 0xFFFFu), hi = (int16_t)(rg >> 16);
+        uint32_t word = 0;
+#pragma unroll
+        for (int hs = 0; hs < 2; ++hs) {
+            const int di = 2 * k + hs;
+            const int d = d0 + di;
+            const uint32_t sh = (sum >> (16 * hs)) & 0xFFFFu, nh = (cnt >> (8 * hs)) & 0xFFu;
+            uint32_t q = kInvalidCost;
+            if (di < D && d >= lo && d < hi && nh > 0) q = div_by_magic(sh, nh, s_magic[nh]);
+            word |= q << (16 * hs);
+        }
+        __stcs(dst, word);
+        dst += rowstride;
+    }
+}
+
 // Horizontal pass over a volume (aggregation iterations after the first).  A CTA owns one row
 // and a run of `cols` pixels... implemented as the transpose of the vertical kernel: one thread
 // per (row, word) sliding along x.
@@ -285,6 +404,29 @@ cudaError_t launch_cross_v(int w, int h, int d0, int D, int Dp, int lmax, int ta
         if (span <= 64) return go(std::integral_constant<int, 64>());
         if (span <= 128) return go(std::integral_constant<int, 128>());
         if (span <= 256) return go(std::integral_constant<int, 256>());
+    }
+    if (nthr <= 256) {
+        // any ranges: sum and count rings, batched loads
+        const int span = 2 * lmax + kB + 2;
+        const size_t extra = (size_t)cols * kSeg * 4 + (size_t)(2 * lmax + 2) * 4 + (size_t)cols * (kSeg + 2 * lmax) +
+                             (size_t)cols * kSeg * 2;
+        auto go = [&](auto rs_tag) -> cudaError_t {
+            constexpr int RS = decltype(rs_tag)::value;
+            const size_t smem = (size_t)RS * nthr * 6 + extra;
+            auto kern = cross_v_count_kernel<RS>;
+            {
+                const cudaError_t e = allow_dynamic_smem(kern, smem);
+                if (e != cudaSuccess) return e;
+            }
+            dim3 grid((w + cols - 1) / cols, (h + kSeg - 1) / kSeg);
+            kern<<<grid, round_up(nthr, 32), smem, s>>>(w, h, d0, D, Dp, lmax, tau, cols, gray, rmin, rmax, tin, cout,
+                                                        magic);
+            return cudaGetLastError();
+        };
+        auto fits = [&](int rs) { return (size_t)rs * nthr * 6 + extra <= 200 * 1024; };
+        if (span <= 64 && fits(64)) return go(std::integral_constant<int, 64>());
+        if (span <= 128 && fits(128)) return go(std::integral_constant<int, 128>());
+        if (span <= 256 && fits(256)) return go(std::integral_constant<int, 256>());
     }
     const int RS = 2 * lmax + 2;
     const size_t smem = (size_t)RS * nthr * 8 + (size_t)cols * kSeg * 2;
