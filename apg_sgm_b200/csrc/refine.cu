@@ -202,11 +202,16 @@ __device__ __forceinline__ void cp16(void* dst, const void* src) {
                  : "memory");
 }
 
-template <bool C64>
+// WIN: each lane's right-image window ([x - dmax + 1, x - d0] of its row, sliding one pixel per
+// step) lives in shared memory, a ring of wmask + 1 records per lane (a power of two holding the
+// window plus the kRing steps copied ahead); every step copies the entering pixel with the step's
+// record, so the candidates' right pixels are shared-memory loads.  Without WIN they are global
+// loads kept warm in L1 by prefetches.
+template <bool C64, bool WIN>
 __global__ void __launch_bounds__(32) refine_band_kernel(CostCtx c, int fwd, const RStep* __restrict__ steps,
                                                          const RPack<C64>* __restrict__ lp,
                                                          const RPack<C64>* __restrict__ rp, float* work,
-                                                         int* progress, int* err, int spin_limit) {
+                                                         int* progress, int* err, int spin_limit, int wmask) {
     __shared__ float s_lut[kLutSize];
     __shared__ __align__(16) RStep s_ring[kRing][32];
     __shared__ __align__(16) RPack<C64> s_lpk[kRing][32];
@@ -218,46 +223,66 @@ __global__ void __launch_bounds__(32) refine_band_kernel(CostCtx c, int fwd, con
     const int v = band * kBand + lane;  // pass-order row of this lane
     const bool row_ok = v < h;
     volatile int* vprog = progress;
+    // pass-order column u of this lane's row is image column x = xb + xs * u
+    const int xs = fwd ? 1 : -1, xb = fwd ? 0 : w - 1;
+    const int yrow = fwd ? v : h - 1 - v;
+    const size_t rowoff = (size_t)(row_ok ? yrow : 0) * w;
+    const RStep* srow = steps + (size_t)(row_ok ? v : 0) * w;  // this lane's records, pass order
+    const RPack<C64>* lrow = lp + rowoff;                       // this lane's left pixels
+    const RPack<C64>* rrow = rp + rowoff;                       // this lane's right-image row
+    float* wrow = work + rowoff;
+    const int d0 = c.d0, dmax = c.d0 + c.D;
+    const int eoff = fwd ? d0 : dmax - 1;  // entering window pixel of column u: x(u) - eoff
+    extern __shared__ __align__(16) unsigned char s_dyn[];
+    RPack<C64>* s_win = reinterpret_cast<RPack<C64>*>(s_dyn) + lane * (wmask + 2);  // one record of padding
+    auto copy_win = [&](int u) {
+        const int pe = xb + xs * u - eoff;
+        if ((unsigned)pe < (unsigned)w)
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(
+                             (unsigned)__cvta_generic_to_shared(&s_win[pe & wmask])),
+                         "l"(rrow + pe)
+                         : "memory");
+    };
     // one cp.async group per step: this lane's record (and packed left pixel) of step t
     auto issue = [&](int t) {
         const int u = t - lane;
-        if (row_ok && u >= 0 && u < w && t < w + kBand - 1) {
-            const int j = v * w + u;
-            const RStep* src = steps + j;
+        if (row_ok && u >= 0 && u < w) {
+            const RStep* src = srow + u;
             cp16(&s_ring[t % kRing][lane], src);
             cp16(reinterpret_cast<unsigned char*>(&s_ring[t % kRing][lane]) + 16,
                  reinterpret_cast<const unsigned char*>(src) + 16);
-            const int x = fwd ? u : w - 1 - u;
-            const int y = fwd ? v : h - 1 - v;
+            const RPack<C64>* ls = lrow + (xb + xs * u);
             if constexpr (C64) {
-                cp16(&s_lpk[t % kRing][lane], lp + y * w + x);
+                cp16(&s_lpk[t % kRing][lane], ls);
             } else {
                 asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(
                                  (unsigned)__cvta_generic_to_shared(&s_lpk[t % kRing][lane])),
-                             "l"(lp + y * w + x)
+                             "l"(ls)
                              : "memory");
             }
         }
+        // the window pixel entering at this column (also for the columns before the lane's first)
+        if (WIN && row_ok && u < w) copy_win(u);
         asm volatile("cp.async.commit_group;\n" ::: "memory");
     };
+    if constexpr (WIN) {
+        // the rest of the window of the lane's first column: columns -(D - 1) .. -lane - 1
+        if (row_ok)
+            for (int u = -(c.D - 1); u < -lane; ++u) copy_win(u);
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    }
 #pragma unroll 1
     for (int t = 0; t < kRing; ++t) issue(t);
     // the right-image window a lane reads (its row, [x - dmax + 1, x - d0]) slides by one pixel
     // per step; every lane misses L1 at a different step and the warp waits for the slowest, so
     // the window's first kAhead steps are prefetched now and its entering edge kAhead steps ahead
-    const int d0 = c.d0, dmax = c.d0 + c.D;
-    const int yrow = fwd ? v : h - 1 - v;
-    const RPack<C64>* rrow = rp + (size_t)(row_ok ? yrow : 0) * w;
-    auto edge = [&](int u) {  // the window pixel entering at column u
-        const int x = fwd ? u : w - 1 - u;
-        return fwd ? x - d0 : x - dmax + 1;
-    };
-    if (row_ok) {
+    if (!WIN && row_ok) {
         for (int k = -c.D; k <= kAhead; k += 8) {
-            const int xr = min(max(edge(k), 0), w - 1);
+            const int xr = min(max(xb + xs * k - eoff, 0), w - 1);
             prefetch_l1(rrow + xr);
         }
     }
+    int pe = xb + xs * (kAhead - lane) - eoff;  // entering pixel kAhead steps ahead of step t = 0
     float prev = -1.f;  // value of this lane's previous column (its left neighbour)
     // values of the row above the band for columns [up_base, up_base + kUpBatch): lane k holds
     // column up_base + k, read together once the band above has published them
@@ -291,19 +316,19 @@ __global__ void __launch_bounds__(32) refine_band_kernel(CostCtx c, int fwd, con
             __threadfence();
             up_base = t;
             const int col = t + lane;
-            up_vals = (lane < kUpBatch && col < w) ? __ldcg(work + y_above * w + (fwd ? col : w - 1 - col)) : -1.f;
+            up_vals = (lane < kUpBatch && col < w) ? __ldcg(work + y_above * w + (xb + xs * col)) : -1.f;
         }
         const float up_first = __shfl_sync(0xffffffffu, up_vals, (t - up_base) & 31);
         asm volatile("cp.async.wait_group %0;\n" ::"n"(kRing - 1) : "memory");
-        if (row_ok) prefetch_l1(rrow + min(max(edge(t - lane + kAhead), 0), w - 1));
+        if (!WIN && row_ok) prefetch_l1(rrow + min(max(pe, 0), w - 1));
+        pe += xs;
         const float up_lane = __shfl_up_sync(0xffffffffu, prev, 1);
         const int u = t - lane;
         if (row_ok && u >= 0 && u < w) {
             const RStep st = s_ring[t % kRing][lane];
             float val = st.cur;
             if (st.upd & 1) {
-                const int x = fwd ? u : w - 1 - u;
-                const int y = fwd ? v : h - 1 - v;
+                const int x = xb + xs * u;
                 const int lo = (int)(short)(st.range & 0xFFFF), hi = st.range >> 16;
                 const int d_cur = (int)(short)(st.d_pack & 0xFFFF), d_draw = st.d_pack >> 16;
                 const bool has_cur = (st.upd & 2) != 0, has_draw = (st.upd & 4) != 0;
@@ -313,10 +338,16 @@ __global__ void __launch_bounds__(32) refine_band_kernel(CostCtx c, int fwd, con
                 if (u > 0) left = prev;
                 if (v > 0) up = lane > 0 ? up_lane : up_first;
                 const bool has_l = left >= 0.f, has_u = up >= 0.f;
+                // clamped into [lo, hi - 1] (hi > lo for an updated pixel), so only x - d needs a test
                 const int dl = has_l ? min(max((int)roundf(left), lo), hi - 1) : 0;
                 const int du = has_u ? min(max((int)roundf(up), lo), hi - 1) : 0;
-                const float cl = has_l ? cand_cost<C64>(c, s_lut, l, rp, x, y, dl, lo, hi) : 0.f;
-                const float cu = has_u ? cand_cost<C64>(c, s_lut, l, rp, x, y, du, lo, hi) : 0.f;
+                const int xl = x - dl, xu = x - du;
+                const float cl = (has_l && (unsigned)xl < (unsigned)w)
+                                     ? packed_cost<C64>(c, s_lut, l, WIN ? s_win[xl & wmask] : rrow[xl])
+                                     : 1e6f;
+                const float cu = (has_u && (unsigned)xu < (unsigned)w)
+                                     ? packed_cost<C64>(c, s_lut, l, WIN ? s_win[xu & wmask] : rrow[xu])
+                                     : 1e6f;
                 // the reference's order: cur, left, up, cur + draw; the first strict minimum wins
                 float best_c = 1e9f;
                 int best_d = st.cur >= 0.f ? d_cur : lo;
@@ -325,7 +356,7 @@ __global__ void __launch_bounds__(32) refine_band_kernel(CostCtx c, int fwd, con
                 if (has_u && cu < best_c) { best_c = cu; best_d = du; }
                 if (has_draw && st.c_draw < best_c) { best_c = st.c_draw; best_d = d_draw; }
                 val = (float)best_d;
-                work[y * w + x] = val;
+                wrow[x] = val;
             }
             prev = val;
         }
@@ -505,9 +536,32 @@ cudaError_t launch_refine_pass(const CostCtx& c, const Layout& L, unsigned char*
                                  : (const void*)(reinterpret_cast<const RPack<false>*>(lpk) + n);
     const RStep* csteps = steps;
     int fwd_arg = fwd;
-    void* args[] = {&cc, &fwd_arg, (void*)&csteps, (void*)&lpk, (void*)&rpk, &work, &progress, &err, &spin_limit};
-    const void* kern = c.census64 ? (const void*)refine_band_kernel<true> : (const void*)refine_band_kernel<false>;
-    e = cudaLaunchCooperativeKernel(kern, dim3(nbands), dim3(kBand), args, 0, s);
+    // the right-image window in shared memory (32-bit census): a power-of-two ring per lane holding
+    // the D window pixels plus the kRing copied ahead, when every band still fits on the device at once
+    int wmask = 0;
+    size_t wbytes = 0;
+    const void* kern = c.census64 ? (const void*)refine_band_kernel<true, false> : (const void*)refine_band_kernel<false, false>;
+    if (!c.census64) {
+        int rs = 1;
+        while (rs < c.D + kRing) rs <<= 1;
+        const size_t bytes = (size_t)kBand * (rs + 1) * sizeof(RPack<false>);
+        auto wk = refine_band_kernel<false, true>;
+        if (rs <= 512 && allow_dynamic_smem(wk, bytes) == cudaSuccess) {
+            int per_sm = 0, dev = 0, nsm = 0;
+            if (cudaGetDevice(&dev) == cudaSuccess &&
+                cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, wk, kBand, bytes) == cudaSuccess &&
+                per_sm * nsm >= nbands) {
+                wmask = rs - 1;
+                wbytes = bytes;
+                kern = (const void*)wk;
+            }
+        }
+        cudaGetLastError();
+    }
+    void* args[] = {&cc, &fwd_arg, (void*)&csteps, (void*)&lpk, (void*)&rpk, &work, &progress, &err, &spin_limit,
+                    &wmask};
+    e = cudaLaunchCooperativeKernel(kern, dim3(nbands), dim3(kBand), args, wbytes, s);
     if (e != cudaSuccess) return e;
     ++*launches;
     // start of the next pass, and cleared progress counters
