@@ -1,8 +1,7 @@
 // Matching-cost volume by pixel runs, fused with the horizontal Cross-arm pass and the
-// right-image argmin: the form used for the 32-bit census with the default disparity ranges
-// (Fast and Balanced), up to 256 padded disparities.  Results are those of cost.cu's tile kernel,
-// which keeps the forms with per-pixel ranges, the 64-bit census or wider ranges; only the
-// division of the work differs:
+// right-image argmin: the form used for the 32-bit census (Fast, Balanced, and HighQuality with the
+// prior's per-pixel ranges), up to 256 padded disparities.  Results are those of cost.cu's tile
+// kernel, which keeps the 64-bit census and wider ranges; only the division of the work differs:
 //
 //   * One warp covers the whole disparity range of a run of consecutive staged pixels: lane l owns
 //     the WPL = Dp/64 words k = WPL*l .. WPL*l + WPL-1 (the P = 2*WPL disparities P*l .. P*l+P-1)
@@ -19,6 +18,9 @@
 //     difference of two such sums is exact in each 16-bit half when each half's window sum is
 //     below 2^16, which the host checks for the arm length and cost_max.  Runs are joined at query
 //     time from the per-run totals.
+//   * Per-pixel ranges: each staged left pixel carries [lo, hi); a lane turns it into a mask of its
+//     P disparities per step, and the aggregation keeps a second running prefix of valid counts
+//     (two 8-bit counts per word, exact for windows of at most 255 pixels).
 //   * The right-image argmin (wta_right_from_left_volume, src/pipeline.cpp:24-85): right pixel
 //     r = x - d0 - di receives (x, di) at step x in lane di/P.  Each lane keeps the running minimum
 //     keys (cost << 16 | di: lowest cost first, then lowest d) of its P right pixels; every step
@@ -41,7 +43,7 @@ constexpr int kT2Stride = 33;  // t2 row per |dgray|: popcounts 0..32 of a 32-bi
 
 struct RunGeom {
     int txc, ha, nx, nr, roff, rl, nrun, ntx, ntiles;
-    size_t t2, lgt, q, magic, arm, lc, lg, rc, rg, pre, tot, emit, total;
+    size_t t2, lgt, q, magic, arm, lc, lg, rc, rg, rng, pre, cnt, tot, totc, emit, total;
 };
 
 inline size_t a16(size_t v) { return (v + 15) & ~size_t(15); }
@@ -53,7 +55,7 @@ inline int run_warps(bool cross) { return cross ? 16 : 8; }
 // shifts the staged right row so that each step group's right descriptors start at an even index
 // (8-byte loads) and every lane with a disparity inside the range finds its whole window staged.
 // One run per warp.
-RunGeom run_geom(const CostCtx& c, int txc, int ha, bool cross, bool full) {
+RunGeom run_geom(const CostCtx& c, int txc, int ha, bool cross, bool full, bool prior) {
     RunGeom g{};
     const int W2 = c.Dp / 2;
     g.txc = txc;
@@ -78,8 +80,11 @@ RunGeom run_geom(const CostCtx& c, int txc, int ha, bool cross, bool full) {
     g.lg = o; o = a16(o + (stage_g ? g.nx * 4 : 0));
     g.rc = o; o = a16(o + g.nr * 4);
     g.rg = o; o = a16(o + (full ? g.nr * 4 : 0));
+    g.rng = o; o = a16(o + (prior ? g.nx * 4 : 0));                                // lo | hi << 16
     g.pre = o; o = a16(o + (cross ? (size_t)g.nx * W2 * 4 : 0));
+    g.cnt = o; o = a16(o + (cross && prior ? (size_t)g.nx * W2 * 2 : 0));        // valid counts
     g.tot = o; o = a16(o + (cross ? (size_t)g.nrun * W2 * 4 : 0));
+    g.totc = o; o = a16(o + (cross && prior ? (size_t)g.nrun * W2 * 2 : 0));
     g.emit = o; o = a16(o + (size_t)g.nrun * g.rl * 4);
     g.total = o;
     return g;
@@ -118,13 +123,29 @@ __device__ __forceinline__ void store_words(uint32_t* p, const uint32_t (&w)[N])
     }
 }
 
+// WPL 16-bit count words (two 8-bit valid counts each) at p, which is 4-byte aligned for even WPL.
+template <int N>
+__device__ __forceinline__ void store_counts(uint16_t* p, const uint32_t (&c)[N]) {
+    if constexpr (N % 2 == 0) {
+#pragma unroll
+        for (int i = 0; i < N; i += 2)
+            *reinterpret_cast<uint32_t*>(p + i) = (c[i] & 0xFFFFu) | (c[i + 1] << 16);
+    } else {
+#pragma unroll
+        for (int i = 0; i < N; ++i) p[i] = (uint16_t)c[i];
+    }
+}
+
 // One run of steps of this lane's P disparities.  V: every (x, d) of the run is a valid voxel for
 // every lane of the warp (no per-voxel tests).
-template <bool V, bool CROSS, bool STORE, bool FULL, int WPL>
+// PRIOR: every left pixel has its own range [lo, hi) (staged in s_rng); a voxel outside it is
+// invalid, and the aggregation also keeps a prefix of valid counts (s_cnt, s_totc).
+template <bool V, bool CROSS, bool STORE, bool FULL, int WPL, bool PRIOR>
 __device__ __forceinline__ void run_steps(const CostCtx& c, const RunGeom& g, int row, int xbase, int xs, int xe,
                                           const uint32_t* s_lc, const uint32_t* s_lg, const uint32_t* s_rc,
                                           const uint32_t* s_rg, const float* s_t2, const float* s_lgt,
-                                          const uint32_t* s_q, uint32_t* s_pre, uint32_t* s_tot, uint32_t* s_em,
+                                          const uint32_t* s_q, const uint32_t* s_rng, uint32_t* s_pre,
+                                          uint16_t* s_cnt, uint32_t* s_tot, uint16_t* s_totc, uint32_t* s_em,
                                           int run, uint32_t* __restrict__ out_vol, uint32_t* __restrict__ rkey) {
     constexpr int P = 2 * WPL;
     constexpr int W2 = 32 * WPL;
@@ -137,7 +158,7 @@ __device__ __forceinline__ void run_steps(const CostCtx& c, const RunGeom& g, in
     // masked; a lane with any disparity below D has dbase <= D - 1 < D + roff - P, so keeps its own
     const int dl = V ? dbase : min(dbase, (c.D + g.roff - P) & ~1);
     int ri = xs - dl + c.D - 1 + g.roff;  // staged right descriptor of (xs, dl); even
-    uint32_t wc[P], wg[P], acc[P], pre[WPL];
+    uint32_t wc[P], wg[P], acc[P], pre[WPL], cnt[WPL];
 #pragma unroll
     for (int j = 0; j < P; ++j) {
         // before the first step's shift: wc[j] holds the descriptor of (xs - 1, dl + j)
@@ -146,8 +167,9 @@ __device__ __forceinline__ void run_steps(const CostCtx& c, const RunGeom& g, in
         acc[j] = kInvalidWord;
     }
 #pragma unroll
-    for (int w = 0; w < WPL; ++w) pre[w] = 0;
+    for (int w = 0; w < WPL; ++w) pre[w] = cnt[w] = 0;
     uint32_t* pp = s_pre + xs * W2 + WPL * lane;                             // prefix words of (xs)
+    uint16_t* cp = s_cnt + xs * W2 + WPL * lane;                             // count words of (xs)
     uint32_t* vp = out_vol + ((size_t)row + (xbase + xs)) * W2 + WPL * lane;  // volume words of (xs)
     for (int xi = xs; xi < xe; xi += 4) {
         const uint4 lc4 = *reinterpret_cast<const uint4*>(s_lc + xi);
@@ -176,6 +198,14 @@ __device__ __forceinline__ void run_steps(const CostCtx& c, const RunGeom& g, in
             wg[0] = NG[s];
             uint32_t q[P];
             bool v[P];
+            uint32_t rmask = 0xFFFFu;  // this lane's disparities inside the left pixel's range
+            if (PRIOR) {
+                const uint32_t rg = s_rng[xi + s];
+                const int base = c.d0 + dbase;
+                const int a0 = min(max((int)(int16_t)(rg & 0xFFFFu) - base, 0), P);
+                const int a1 = min(max((int)(int16_t)(rg >> 16) - base, 0), P);
+                rmask = ((1u << a1) - 1u) & ~((1u << a0) - 1u);
+            }
 #pragma unroll
             for (int j = 0; j < P; ++j) {
                 q[j] = run_cost<FULL>(L[s], LG[s], wc[j], wg[j], s_t2, s_lgt, s_q, scale, cmax);
@@ -184,6 +214,7 @@ __device__ __forceinline__ void run_steps(const CostCtx& c, const RunGeom& g, in
                     const int di = dbase + j, xr = x - c.d0 - di;
                     v[j] = x >= 0 && x < c.w && di < c.D && xr >= 0 && xr < c.w;
                 }
+                if (PRIOR) v[j] = v[j] && ((rmask >> j) & 1u);
                 const uint32_t key = v[j] ? ((q[j] << 16) | (uint32_t)(dbase + j)) : kInvalidWord;
                 acc[j] = min(acc[j], key);
             }
@@ -199,6 +230,11 @@ __device__ __forceinline__ void run_steps(const CostCtx& c, const RunGeom& g, in
                 for (int w = 0; w < WPL; ++w)
                     pre[w] += (v[2 * w] ? q[2 * w] : 0u) | ((v[2 * w + 1] ? q[2 * w + 1] : 0u) << 16);
                 store_words<WPL>(pp + s * W2, pre);
+                if (PRIOR) {
+#pragma unroll
+                    for (int w = 0; w < WPL; ++w) cnt[w] += (v[2 * w] ? 1u : 0u) + (v[2 * w + 1] ? 0x100u : 0u);
+                    store_counts<WPL>(cp + s * W2, cnt);
+                }
             } else if (STORE) {
                 // without a halo the staged pixels are the tile's; V runs lie inside the image
                 if (V || (xi + s < g.txc && x < c.w)) {
@@ -213,6 +249,7 @@ __device__ __forceinline__ void run_steps(const CostCtx& c, const RunGeom& g, in
         }
         ri += 4;
         pp += 4 * W2;
+        cp += 4 * W2;
         vp += 4 * (size_t)W2;
     }
     __syncwarp();
@@ -235,6 +272,7 @@ __device__ __forceinline__ void run_steps(const CostCtx& c, const RunGeom& g, in
     }
     __syncwarp();
     if (CROSS) store_words<WPL>(s_tot + run * W2 + WPL * lane, pre);
+    if (CROSS && PRIOR) store_counts<WPL>(s_totc + run * W2 + WPL * lane, cnt);
 }
 
 // Aggregated word kk at pixel x from its packed window sum s (cost.cu's tile kernel, same rules).
@@ -259,8 +297,28 @@ __device__ __forceinline__ uint32_t agg_word(const CostCtx& c, uint32_t s, int k
     return word;
 }
 
-template <bool CROSS, bool STORE, bool FULL, int WPL>
-__global__ void __launch_bounds__(CROSS ? 512 : 256, CROSS ? 2 : 1)
+// Aggregated word kk from its window sum s and its two 8-bit valid counts n, with per-pixel ranges
+// (cost.cu's tile kernel, same rule): a half is valid when its disparity is inside the centre
+// pixel's range and its window holds a valid voxel.
+__device__ __forceinline__ uint32_t prior_word(const CostCtx& c, uint32_t s, uint32_t n, int kk, int lo, int hi,
+                                               const uint32_t* s_magic) {
+    uint32_t word = 0;
+#pragma unroll
+    for (int hs = 0; hs < 2; ++hs) {
+        const int di = 2 * kk + hs;
+        const int d = c.d0 + di;
+        const uint32_t sh = (s >> (16 * hs)) & 0xFFFFu, nh = (n >> (8 * hs)) & 0xFFu;
+        const bool ok = di < c.D && d >= lo && d < hi && nh > 0;
+        const uint32_t q = ok ? div_by_magic(sh, nh, s_magic[nh]) : kInvalidCost;
+        word |= q << (16 * hs);
+    }
+    return word;
+}
+
+// With per-pixel ranges and 192 or 256 padded disparities the aggregating block keeps one block per
+// SM (more registers, wider tiles); otherwise two.
+template <bool CROSS, bool STORE, bool FULL, int WPL, bool PRIOR>
+__global__ void __launch_bounds__(CROSS ? 512 : 256, CROSS ? ((PRIOR && WPL > 2) ? 1 : 2) : 1)
     cost_run_kernel(CostCtx c, RunGeom g, int lmax, int tau, uint32_t* __restrict__ out_vol,
                     uint32_t* __restrict__ rkey, const uint32_t* __restrict__ magic) {
     constexpr int W2 = 32 * WPL;
@@ -277,6 +335,9 @@ __global__ void __launch_bounds__(CROSS ? 512 : 256, CROSS ? 2 : 1)
     uint32_t* s_rg = reinterpret_cast<uint32_t*>(smem + g.rg);
     uint32_t* s_pre = reinterpret_cast<uint32_t*>(smem + g.pre);
     uint32_t* s_tot = reinterpret_cast<uint32_t*>(smem + g.tot);
+    uint32_t* s_rng = reinterpret_cast<uint32_t*>(smem + g.rng);
+    uint16_t* s_cnt = reinterpret_cast<uint16_t*>(smem + g.cnt);
+    uint16_t* s_totc = reinterpret_cast<uint16_t*>(smem + g.totc);
     const int tid = threadIdx.x, nt = blockDim.x, run = tid >> 5, lane = tid & 31;
     uint32_t* s_em = reinterpret_cast<uint32_t*>(smem + g.emit) + run * g.rl;
 
@@ -308,6 +369,8 @@ __global__ void __launch_bounds__(CROSS ? 512 : 256, CROSS ? 2 : 1)
             const bool in = x >= 0 && x < c.w;
             s_lc[i] = in ? c.cl[row + x] : 0u;
             if (FULL || CROSS) s_lg[i] = in ? pack_g(c.lgray, c.lgx, c.lgy, row + x) : 0u;
+            // outside the image: an empty range
+            if (PRIOR) s_rng[i] = in ? ((uint32_t)(uint16_t)c.rmin[row + x] | ((uint32_t)(uint16_t)c.rmax[row + x] << 16)) : 0u;
         }
         for (int i = tid; i < g.nr; i += nt) {
             const int xr = rbase + i;
@@ -338,11 +401,13 @@ __global__ void __launch_bounds__(CROSS ? 512 : 256, CROSS ? 2 : 1)
             const bool ok = xa >= 0 && xb < c.w && P * lane + P - 1 < c.D && xa - (dlo + P - 1) >= 0 &&
                             xb - dlo <= c.w - 1;
             if (__all_sync(0xFFFFFFFFu, ok))
-                run_steps<true, CROSS, STORE, FULL, WPL>(c, g, row, xbase, xs, xe, s_lc, s_lg, s_rc, s_rg, s_t2, s_lgt,
-                                                         s_q, s_pre, s_tot, s_em, run, out_vol, rkey);
+                run_steps<true, CROSS, STORE, FULL, WPL, PRIOR>(c, g, row, xbase, xs, xe, s_lc, s_lg, s_rc, s_rg, s_t2,
+                                                                s_lgt, s_q, s_rng, s_pre, s_cnt, s_tot, s_totc, s_em,
+                                                                run, out_vol, rkey);
             else
-                run_steps<false, CROSS, STORE, FULL, WPL>(c, g, row, xbase, xs, xe, s_lc, s_lg, s_rc, s_rg, s_t2,
-                                                          s_lgt, s_q, s_pre, s_tot, s_em, run, out_vol, rkey);
+                run_steps<false, CROSS, STORE, FULL, WPL, PRIOR>(c, g, row, xbase, xs, xe, s_lc, s_lg, s_rc, s_rg,
+                                                                 s_t2, s_lgt, s_q, s_rng, s_pre, s_cnt, s_tot, s_totc,
+                                                                 s_em, run, out_vol, rkey);
         }
         if (CROSS) {
             __syncthreads();
@@ -367,6 +432,26 @@ __global__ void __launch_bounds__(CROSS ? 512 : 256, CROSS ? 2 : 1)
                 const uint32_t s0 = sb.x - sa.x, s1 = sb.y - sa.y;
                 uint32_t w0, w1;
                 const uint32_t len = (uint32_t)(l + r + 1);
+                if constexpr (PRIOR) {
+                    // valid counts of the window from the count prefix (two 8-bit counts per word),
+                    // validity from the centre pixel's range (the tile kernel's rule)
+                    const uint32_t cb = *reinterpret_cast<const uint32_t*>(s_cnt + b * W2 + k2);
+                    const uint32_t ca = a > 0 ? *reinterpret_cast<const uint32_t*>(s_cnt + (a - 1) * W2 + k2) : 0u;
+                    uint32_t tlo = 0, thi = 0;
+                    for (int j = rlo; j < rhi; ++j) {
+                        const uint32_t t = *reinterpret_cast<const uint32_t*>(s_totc + j * W2 + k2);
+                        tlo += t & 0xFFFFu;
+                        thi += t >> 16;
+                    }
+                    const uint32_t n0 = ((cb & 0xFFFFu) - (ca & 0xFFFFu) + tlo) & 0xFFFFu;
+                    const uint32_t n1 = ((cb >> 16) - (ca >> 16) + thi) & 0xFFFFu;
+                    const uint32_t rg = s_rng[sxi];
+                    const int lo = (int)(int16_t)(rg & 0xFFFFu), hi = (int)(int16_t)(rg >> 16);
+                    w0 = prior_word(c, s0, n0, k2, lo, hi, s_magic);
+                    w1 = prior_word(c, s1, n1, k2 + 1, lo, hi, s_magic);
+                    *reinterpret_cast<uint2*>(out_vol + ((size_t)row + x) * W2 + k2) = make_uint2(w0, w1);
+                    continue;
+                }
                 // every word of the pixel has its whole window valid (no padded words, x - d inside
                 // the image over the window for every d): one count, no per-word tests
                 if (c.D == c.Dp && len > 1 && x - l >= c.d0 + c.Dp - 1 && x + r <= c.w - 1 + c.d0) {
@@ -402,25 +487,29 @@ size_t smem_per_block(int per_sm) {
 }
 
 // Tile width of the aggregating form: the fewest tiles per row (least halo) whose staging lets two
-// 16-warp blocks share an SM; a requested width (tuning key cost_tile) wins when it fits one block.
+// 16-warp blocks share an SM (one block for the wide per-pixel-range form); a requested width
+// (tuning key cost_tile) wins when it fits one block.
 int cross_tile(const CostCtx& c, int lmax, bool full) {
-    if ((c.tile == 64 || c.tile == 128 || c.tile == 256) && run_geom(c, c.tile, lmax, true, full).total <= 200 * 1024)
+    const bool prior = c.prior_ranges != 0;
+    if ((c.tile == 64 || c.tile == 128 || c.tile == 256) &&
+        run_geom(c, c.tile, lmax, true, full, prior).total <= 200 * 1024)
         return c.tile;
-    const size_t budget = smem_per_block(2);
+    // one block per SM for the wide per-pixel-range form (see cost_run_kernel), else two
+    const size_t budget = smem_per_block(prior && c.Dp > 128 ? 1 : 2);
     for (int ntx = 1; ntx <= c.w; ++ntx) {
         const int txc = round_up((c.w + ntx - 1) / ntx, 4);
-        if (run_geom(c, txc, lmax, true, full).total <= budget) return txc;
+        if (run_geom(c, txc, lmax, true, full, prior).total <= budget) return txc;
         if (txc <= 32) break;
     }
     return 32;
 }
 
-template <bool CROSS, bool STORE, bool FULL, int WPL>
+template <bool CROSS, bool STORE, bool FULL, int WPL, bool PRIOR>
 cudaError_t launch_runs_w(const CostCtx& c, int txc, int lmax, int tau, uint32_t* vol, uint32_t* rkey,
                           const uint32_t* magic, cudaStream_t s) {
-    const RunGeom g = run_geom(c, txc, CROSS ? lmax : 0, CROSS, FULL);
+    const RunGeom g = run_geom(c, txc, CROSS ? lmax : 0, CROSS, FULL, PRIOR);
     const int nt = 32 * g.nrun;
-    auto kern = cost_run_kernel<CROSS, STORE, FULL, WPL>;
+    auto kern = cost_run_kernel<CROSS, STORE, FULL, WPL, PRIOR>;
     cudaError_t e = allow_dynamic_smem(kern, g.total);
     if (e != cudaSuccess) return e;
     int per_sm = 0, dev = 0, nsm = 0;
@@ -434,32 +523,41 @@ cudaError_t launch_runs_w(const CostCtx& c, int txc, int lmax, int tau, uint32_t
 }
 
 // Words per lane as a compile-time constant: one warp spans Dp = 64 * WPL disparities.
+template <bool CROSS, bool STORE, bool FULL, bool PRIOR>
+cudaError_t launch_runs_p(const CostCtx& c, int txc, int lmax, int tau, uint32_t* vol, uint32_t* rkey,
+                          const uint32_t* magic, cudaStream_t s) {
+    switch (c.Dp) {
+        case 64: return launch_runs_w<CROSS, STORE, FULL, 1, PRIOR>(c, txc, lmax, tau, vol, rkey, magic, s);
+        case 128: return launch_runs_w<CROSS, STORE, FULL, 2, PRIOR>(c, txc, lmax, tau, vol, rkey, magic, s);
+        case 192: return launch_runs_w<CROSS, STORE, FULL, 3, PRIOR>(c, txc, lmax, tau, vol, rkey, magic, s);
+        default: return launch_runs_w<CROSS, STORE, FULL, 4, PRIOR>(c, txc, lmax, tau, vol, rkey, magic, s);
+    }
+}
+
 template <bool CROSS, bool STORE, bool FULL>
 cudaError_t launch_runs_t(const CostCtx& c, int txc, int lmax, int tau, uint32_t* vol, uint32_t* rkey,
                           const uint32_t* magic, cudaStream_t s) {
-    switch (c.Dp) {
-        case 64: return launch_runs_w<CROSS, STORE, FULL, 1>(c, txc, lmax, tau, vol, rkey, magic, s);
-        case 128: return launch_runs_w<CROSS, STORE, FULL, 2>(c, txc, lmax, tau, vol, rkey, magic, s);
-        case 192: return launch_runs_w<CROSS, STORE, FULL, 3>(c, txc, lmax, tau, vol, rkey, magic, s);
-        default: return launch_runs_w<CROSS, STORE, FULL, 4>(c, txc, lmax, tau, vol, rkey, magic, s);
-    }
+    if (c.prior_ranges) return launch_runs_p<CROSS, STORE, FULL, true>(c, txc, lmax, tau, vol, rkey, magic, s);
+    return launch_runs_p<CROSS, STORE, FULL, false>(c, txc, lmax, tau, vol, rkey, magic, s);
 }
 
 }  // namespace
 
 size_t cost_runs_smem_bytes(const CostCtx& c, int mode, int lmax) {
     const bool full = c.use_ad || c.use_grad;
-    if (mode == 1) return run_geom(c, cross_tile(c, lmax, full), lmax, true, full).total;
-    return run_geom(c, 256, 0, false, full).total;
+    const bool prior = c.prior_ranges != 0;
+    if (mode == 1) return run_geom(c, cross_tile(c, lmax, full), lmax, true, full, prior).total;
+    return run_geom(c, 256, 0, false, full, prior).total;
 }
 
 bool cost_runs_supported(const CostCtx& c, int mode, int lmax) {
-    if (c.kernel == 1 || c.census64 || c.prior_ranges) return false;
+    if (c.kernel == 1 || c.census64) return false;
     if (c.Dp % 64 != 0 || c.Dp > 256) return false;
     const bool full = c.use_ad || c.use_grad;
-    if (mode == 2 && full) return false;  // the fused form exists for census-only costs
+    if (mode == 2 && (full || c.prior_ranges)) return false;  // the fused form: census-only, default ranges
     if (mode == 1 && lmax > 127) return false;
-    return cost_runs_smem_bytes(c, mode, lmax) <= 200 * 1024;
+    // the staging must fit the per-block budget the tile width was chosen for
+    return cost_runs_smem_bytes(c, mode, lmax) <= smem_per_block(c.prior_ranges && c.Dp > 128 && mode == 1 ? 1 : 2);
 }
 
 cudaError_t launch_cost_runs(const CostCtx& c, int mode, int lmax, int tau, uint32_t* vol, uint32_t* rkey,

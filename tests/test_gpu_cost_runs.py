@@ -4,8 +4,9 @@ The run form (cost_runs.cu) is the default for the 32-bit census with default ra
 key cost_kernel=1 forces the tile form (cost.cu).  Both must give bit-identical raw volumes, cross-H
 aggregated volumes, right-image disparities and final maps over the shapes that exercise the
 run kernel's edges: odd and padded disparity counts, negative minimum disparity, images narrower
-than a tile or than the disparity range, the three-warp word sets of D=192, D=256, and the cost
-forms (census only, AD only, gradient only, all three; with and without aggregation).  The
+than a tile or than the disparity range, the three-warp word sets of D=192, D=256, the cost
+forms (census only, AD only, gradient only, all three; with and without aggregation) and the
+per-pixel ranges of the HighQuality prior.  The
 stage-parity tests check the same kernels against the oracle.
 """
 import zlib
@@ -36,6 +37,12 @@ CASES = [
     ("fast_odd_d65", 0, 513, 31, 65, 0, {}),
     ("fast_neg_dmin", 0, 130, 30, 32, -32, {}),
     ("fast_full_costs", 0, 200, 40, 64, 0, {"use_ad": True, "use_grad": True}),
+    # per-pixel ranges from the prior (HighQuality): range masks per voxel, count prefixes
+    ("hq_300x90_d96", 2, 300, 90, 96, 0, {}),
+    ("hq_333x40_d256", 2, 333, 40, 256, 0, {}),
+    ("hq_neg_dmin", 2, 160, 48, 40, -24, {}),
+    ("hq_narrow_70x33", 2, 70, 33, 128, 0, {}),
+    ("hq_census_agg", 2, 200, 60, 64, 0, {"use_ad": False, "use_grad": False}),
 ]
 
 
@@ -56,7 +63,7 @@ def _run(apg, cfg, L, R, kernel, fused=False, debug=True):
 def test_runs_equal_tiles(apg, case):
     name, mode, w, h, dmax, dmin, over = case
     cfg = apg.config_from_mode(mode, dmax, dmin, **over)
-    L, R = synth(w, h, max(dmax, 8), seed=zlib.crc32(name.encode()) % 1000)
+    L, R = synth(w, h, max(dmax, 8), patch=0.2 if mode == 2 else 0.0, seed=zlib.crc32(name.encode()) % 1000)
     a, da = _run(apg, cfg, L, R, 0)
     b, db = _run(apg, cfg, L, R, 1)
     for k in a:
