@@ -315,10 +315,10 @@ __device__ __forceinline__ uint32_t prior_word(const CostCtx& c, uint32_t s, uin
     return word;
 }
 
-// With per-pixel ranges and 192 or 256 padded disparities the aggregating block keeps one block per
-// SM (more registers, wider tiles); otherwise two.
+// With 192 or 256 padded disparities the aggregating kernel keeps one block per SM (registers for
+// the wider lane state, wider tiles: less halo); otherwise two.
 template <bool CROSS, bool STORE, bool FULL, int WPL, bool PRIOR>
-__global__ void __launch_bounds__(CROSS ? 512 : 256, CROSS ? ((PRIOR && WPL > 2) ? 1 : 2) : 1)
+__global__ void __launch_bounds__(CROSS ? 512 : 256, CROSS ? (WPL > 2 ? 1 : 2) : 1)
     cost_run_kernel(CostCtx c, RunGeom g, int lmax, int tau, uint32_t* __restrict__ out_vol,
                     uint32_t* __restrict__ rkey, const uint32_t* __restrict__ magic) {
     constexpr int W2 = 32 * WPL;
@@ -487,15 +487,15 @@ size_t smem_per_block(int per_sm) {
 }
 
 // Tile width of the aggregating form: the fewest tiles per row (least halo) whose staging lets two
-// 16-warp blocks share an SM (one block for the wide per-pixel-range form); a requested width
+// 16-warp blocks share an SM (one block for 192 or 256 padded disparities); a requested width
 // (tuning key cost_tile) wins when it fits one block.
 int cross_tile(const CostCtx& c, int lmax, bool full) {
     const bool prior = c.prior_ranges != 0;
     if ((c.tile == 64 || c.tile == 128 || c.tile == 256) &&
         run_geom(c, c.tile, lmax, true, full, prior).total <= 200 * 1024)
         return c.tile;
-    // one block per SM for the wide per-pixel-range form (see cost_run_kernel), else two
-    const size_t budget = smem_per_block(prior && c.Dp > 128 ? 1 : 2);
+    // one block per SM for the wide forms (see cost_run_kernel), else two
+    const size_t budget = smem_per_block(c.Dp > 128 ? 1 : 2);
     for (int ntx = 1; ntx <= c.w; ++ntx) {
         const int txc = round_up((c.w + ntx - 1) / ntx, 4);
         if (run_geom(c, txc, lmax, true, full, prior).total <= budget) return txc;
@@ -557,7 +557,7 @@ bool cost_runs_supported(const CostCtx& c, int mode, int lmax) {
     if (mode == 2 && (full || c.prior_ranges)) return false;  // the fused form: census-only, default ranges
     if (mode == 1 && lmax > 127) return false;
     // the staging must fit the per-block budget the tile width was chosen for
-    return cost_runs_smem_bytes(c, mode, lmax) <= smem_per_block(c.prior_ranges && c.Dp > 128 && mode == 1 ? 1 : 2);
+    return cost_runs_smem_bytes(c, mode, lmax) <= smem_per_block(c.Dp > 128 && mode == 1 ? 1 : 2);
 }
 
 cudaError_t launch_cost_runs(const CostCtx& c, int mode, int lmax, int tau, uint32_t* vol, uint32_t* rkey,
