@@ -2,7 +2,7 @@
 // (src/cost_aggregator.cpp:107-138), and a standalone horizontal pass for the second and later
 // aggregation iterations (:77-105).
 //
-// Vertical kernel: a CTA owns `cols` adjacent pixel columns x and a 128-row segment; each thread
+// Vertical kernel: a CTA owns `cols` adjacent pixel columns x and a 256-row segment; each thread
 // owns one 32-bit word (two disparities) of one column and slides down the segment keeping the
 // column prefix sums (sum and count, 16-bit lanes) of the last 2*Lmax+2 rows in a shared-memory
 // ring, so every input voxel is read once (plus a 2*Lmax row halo per segment) and every output
@@ -16,7 +16,7 @@
 namespace apgcu {
 
 namespace {
-constexpr int kSeg = 128;
+constexpr int kSeg = 256;
 
 __global__ void cross_v_kernel(int w, int h, int d0, int D, int Dp, int lmax, int tau, int cols,
                                const uint8_t* __restrict__ gray, const int16_t* __restrict__ rmin,
