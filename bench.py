@@ -785,7 +785,7 @@ def main():
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batched", "served"], default="fast720")
     ap.add_argument("--requests", type=int, default=10000, help="served: total requests over the rates")
-    ap.add_argument("--rates", default="50,100,200,400", help="served: Poisson arrival rates, pairs/s")
+    ap.add_argument("--rates", default="50,100,200,400,600", help="served: Poisson arrival rates, pairs/s")
     ap.add_argument("--slots", type=int, default=4, help="served: requests in flight")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
