@@ -196,6 +196,11 @@ __device__ __forceinline__ void prefetch_l1(const void* p) {
     asm volatile("prefetch.global.L1 [%0];\n" ::"l"(p));
 }
 
+// Progress counters between bands use the fence forms of release and acquire: the publishing lane
+// fences (acquire-release, device scope) and then stores the counter; the reading band polls the
+// counter and fences before reading the row above.
+__device__ __forceinline__ void fence_acq_rel() { asm volatile("fence.acq_rel.gpu;\n" ::: "memory"); }
+
 __device__ __forceinline__ void cp16(void* dst, const void* src) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
                  "l"(src)
@@ -313,7 +318,7 @@ __global__ void __launch_bounds__(32) refine_band_kernel(CostCtx c, int fwd, con
                 abort = true;
                 break;
             }
-            __threadfence();
+            fence_acq_rel();
             up_base = t;
             const int col = t + lane;
             up_vals = (lane < kUpBatch && col < w) ? __ldcg(work + y_above * w + (xb + xs * col)) : -1.f;
@@ -365,14 +370,14 @@ __global__ void __launch_bounds__(32) refine_band_kernel(CostCtx c, int fwd, con
         issue(t + kRing);
         // publish how far the band's last row is final (lane 31 is at column t - 31)
         if ((t % kPublish) == kPublish - 1 && lane == kBand - 1) {
-            __threadfence();
+            fence_acq_rel();
             vprog[band] = max(0, min(t - (kBand - 1) + 1, w));
         }
     }
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     __syncwarp();
     if (lane == kBand - 1) {
-        __threadfence();
+        fence_acq_rel();
         vprog[band] = w;  // the whole band is final (or the pass was abandoned: let the next band finish)
     }
 }
