@@ -722,12 +722,13 @@ template <int T>
 __host__ __device__ constexpr int first_pf() {
     return kVolPfFirst < T ? kVolPfFirst : T;
 }
-// Ring depth of the last sweep: the configured depth (at most T) while 4 warps' rings and WTA
-// buffers fit in 200 KB of shared memory, else 4 (large disparity ranges).
+// Ring depth of the last sweep: the configured depth (at most T) while a warp's ring and WTA buffer
+// stay within 17 KB of shared memory (about thirteen chains per SM), else 4 (large disparity
+// ranges; the sweep's time does not depend on the depth between 4 and 8, occupancy does).
 template <int K, int T, int NB>
 __host__ __device__ constexpr int last_pf() {
     constexpr int pf = kVolPfLast < T ? kVolPfLast : T;
-    return (pf * vol_slot_words<K, NB>() + wta_buf_words<K, T>()) * 4 * 4 <= 200 * 1024 ? pf : (T < 4 ? T : 4);
+    return (pf * vol_slot_words<K, NB>() + wta_buf_words<K, T>()) * 4 <= 17 * 1024 ? pf : (T < 4 ? T : 4);
 }
 
 constexpr int multiple_of_both(int pf, int k2) {
@@ -866,13 +867,14 @@ cudaError_t launch_last_tk(const SgmArgs& a, DirTable tab, bool census, cudaStre
         if (census) {                                                                                \
             sgm_last_kernel<T, K, true, NB><<<blocks, 128, 0, st>>>(a, tab);                         \
         } else {                                                                                     \
-            const size_t smem = (size_t)4 * (last_pf<K, T, NB>() * vol_slot_words<K, NB>() + wta_buf_words<K, T>()) * 4; \
+            /* one warp per block: shared memory is granted per chain, not per four */              \
+            const size_t smem = (size_t)(last_pf<K, T, NB>() * vol_slot_words<K, NB>() + wta_buf_words<K, T>()) * 4; \
             auto kern = sgm_last_kernel<T, K, false, NB>;                                            \
             {                                                                                        \
                 const cudaError_t e = allow_dynamic_smem(kern, smem);                                \
                 if (e != cudaSuccess) return e;                                                      \
             }                                                                                        \
-            kern<<<blocks, 128, smem, st>>>(a, tab);                                                 \
+            kern<<<warps, 32, smem, st>>>(a, tab);                                                   \
         }                                                                                            \
         return cudaGetLastError();                                                                   \
     }
