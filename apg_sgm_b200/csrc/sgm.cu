@@ -845,13 +845,14 @@ cudaError_t launch_first_tk(const SgmArgs& a, DirTable tab, bool census, cudaStr
     if (census) {
         sgm_first_kernel<T, K, true><<<blocks, 128, 0, st>>>(a, tab);
     } else {
-        const size_t smem = (size_t)4 * first_pf<T>() * vol_slot_words<K, 0>() * 4;
+        // one warp per block: chains of different lengths (directions) end independently
+        const size_t smem = (size_t)first_pf<T>() * vol_slot_words<K, 0>() * 4;
         auto kern = sgm_first_kernel<T, K, false>;
         {
             const cudaError_t e = allow_dynamic_smem(kern, smem);
             if (e != cudaSuccess) return e;
         }
-        kern<<<blocks, 128, smem, st>>>(a, tab);
+        kern<<<tab.warp_begin[tab.n], 32, smem, st>>>(a, tab);
     }
     return cudaGetLastError();
 }
