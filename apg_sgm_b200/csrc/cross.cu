@@ -98,6 +98,7 @@ __global__ void cross_v_kernel(int w, int h, int d0, int D, int Dp, int lmax, in
 // buffer), so kB loads per thread are in flight; the gray column segment is staged in shared
 // memory for the arms.
 constexpr int kB = 16;
+constexpr int kQ = 8;  // output rows computed together (independent windows: their loads overlap)
 
 template <int RS>
 __global__ void __launch_bounds__(128) cross_v_default_kernel(int w, int h, int d0, int D, int Dp, int lmax, int tau,
@@ -163,8 +164,9 @@ __global__ void __launch_bounds__(128) cross_v_default_kernel(int w, int h, int 
     int pushed = ystart;  // next row to add to the ring
     uint32_t ps = 0;
     uint32_t* dst = cout + ((size_t)y0 * w + x) * W2 + k;
-    for (int y = y0; y < y1; ++y) {
-        const int need = min(h, y + lmax + 1);
+    for (int yb = y0; yb < y1; yb += kQ) {
+        // prefixes up to the last window of the chunk's rows, then kQ independent rows
+        const int need = min(h, min(yb + kQ, y1) + lmax);
         while (pushed < need) {
             // add the buffered batch (rows [pushed, pushed + kB)) and load the one after next
 #pragma unroll
@@ -182,21 +184,26 @@ __global__ void __launch_bounds__(128) cross_v_default_kernel(int w, int h, int 
             for (int i = 0; i < kB; ++i)
                 nxt[i] = base + i < yend ? __ldcs(src + (size_t)(base + i - ystart) * rowstride) : 0u;
         }
-        const int ai = ci * kSeg + (y - y0);
-        const int a = y - armU[ai], b = y + armD[ai];  // inclusive window
-        const uint32_t sum = __vsub2(ring[((b - ystart + 1) & (RS - 1)) * nthr + tid],
-                                     ring[((a - ystart) & (RS - 1)) * nthr + tid]);
-        const int len = b - a + 1;
-        const uint32_t mg = s_magic[len];
-        uint32_t word = 0;
 #pragma unroll
-        for (int hs = 0; hs < 2; ++hs) {
-            const uint32_t sh = (sum >> (16 * hs)) & 0xFFFFu;
-            const uint32_t q = lane_ok[hs] ? div_by_magic(sh, (uint32_t)len, mg) : kInvalidCost;
-            word |= q << (16 * hs);
+        for (int i = 0; i < kQ; ++i) {
+            const int y = yb + i;
+            if (y >= y1) break;
+            const int ai = ci * kSeg + (y - y0);
+            const int a = y - armU[ai], b = y + armD[ai];  // inclusive window
+            const uint32_t sum = __vsub2(ring[((b - ystart + 1) & (RS - 1)) * nthr + tid],
+                                         ring[((a - ystart) & (RS - 1)) * nthr + tid]);
+            const int len = b - a + 1;
+            const uint32_t mg = s_magic[len];
+            uint32_t word = 0;
+#pragma unroll
+            for (int hs = 0; hs < 2; ++hs) {
+                const uint32_t sh = (sum >> (16 * hs)) & 0xFFFFu;
+                const uint32_t q = lane_ok[hs] ? div_by_magic(sh, (uint32_t)len, mg) : kInvalidCost;
+                word |= q << (16 * hs);
+            }
+            __stcs(dst + (size_t)i * rowstride, word);
         }
-        __stcs(dst, word);
-        dst += rowstride;
+        dst += (size_t)kQ * rowstride;
     }
 }
 
@@ -274,8 +281,8 @@ __global__ void __launch_bounds__(256) cross_v_count_kernel(int w, int h, int d0
     uint32_t ps = 0;
     uint32_t pc = 0;  // low 16 bits used
     uint32_t* dst = cout + ((size_t)y0 * w + x) * W2 + k;
-    for (int y = y0; y < y1; ++y) {
-        const int need = min(h, y + lmax + 1);
+    for (int yb = y0; yb < y1; yb += kQ) {
+        const int need = min(h, min(yb + kQ, y1) + lmax);
         while (pushed < need) {
 #pragma unroll
             for (int i = 0; i < kB; ++i) {
@@ -297,25 +304,30 @@ __global__ void __launch_bounds__(256) cross_v_count_kernel(int w, int h, int d0
             for (int i = 0; i < kB; ++i)
                 nxt[i] = base + i < yend ? __ldcs(src + (size_t)(base + i - ystart) * rowstride) : 0u;
         }
-        const int ai = ci * kSeg + (y - y0);
-        const int a = y - armU[ai], b = y + armD[ai];  // inclusive window
-        const int sb = ((b - ystart + 1) & (RS - 1)) * nthr + tid, sa = ((a - ystart) & (RS - 1)) * nthr + tid;
-        const uint32_t sum = ring[sb] - ring[sa];
-        const uint32_t cnt = (uint32_t)(uint16_t)(ringc[sb] - ringc[sa]);
-        const uint32_t rg = s_rng[ai];
-        const int lo = (int16_t)(rg & 0xFFFFu), hi = (int16_t)(rg >> 16);
-        uint32_t word = 0;
 #pragma unroll
-        for (int hs = 0; hs < 2; ++hs) {
-            const int di = 2 * k + hs;
-            const int d = d0 + di;
-            const uint32_t sh = (sum >> (16 * hs)) & 0xFFFFu, nh = (cnt >> (8 * hs)) & 0xFFu;
-            uint32_t q = kInvalidCost;
-            if (di < D && d >= lo && d < hi && nh > 0) q = div_by_magic(sh, nh, s_magic[nh]);
-            word |= q << (16 * hs);
+        for (int i = 0; i < kQ; ++i) {
+            const int y = yb + i;
+            if (y >= y1) break;
+            const int ai = ci * kSeg + (y - y0);
+            const int a = y - armU[ai], b = y + armD[ai];  // inclusive window
+            const int sb = ((b - ystart + 1) & (RS - 1)) * nthr + tid, sa = ((a - ystart) & (RS - 1)) * nthr + tid;
+            const uint32_t sum = ring[sb] - ring[sa];
+            const uint32_t cnt = (uint32_t)(uint16_t)(ringc[sb] - ringc[sa]);
+            const uint32_t rg = s_rng[ai];
+            const int lo = (int16_t)(rg & 0xFFFFu), hi = (int16_t)(rg >> 16);
+            uint32_t word = 0;
+#pragma unroll
+            for (int hs = 0; hs < 2; ++hs) {
+                const int di = 2 * k + hs;
+                const int d = d0 + di;
+                const uint32_t sh = (sum >> (16 * hs)) & 0xFFFFu, nh = (cnt >> (8 * hs)) & 0xFFu;
+                uint32_t q = kInvalidCost;
+                if (di < D && d >= lo && d < hi && nh > 0) q = div_by_magic(sh, nh, s_magic[nh]);
+                word |= q << (16 * hs);
+            }
+            __stcs(dst + (size_t)i * rowstride, word);
         }
-        __stcs(dst, word);
-        dst += rowstride;
+        dst += (size_t)kQ * rowstride;
     }
 }
 
@@ -383,11 +395,12 @@ cudaError_t launch_cross_v(int w, int h, int d0, int D, int Dp, int lmax, int ta
     const int W2 = Dp / 2;
     const int cols = W2 >= 128 ? 1 : 128 / W2;
     const int nthr = W2 * cols;
-    // fast path: default ranges, non-negative disparities, and a ring holding the window's prefixes
-    // plus the batch pushed ahead: rows from y - lmax - 1 up to y + lmax + kB - 1 are live, and a
-    // ring of more than 2*lmax + kB slots never overwrites one before its last read
+    // fast path: default ranges, non-negative disparities, and a ring holding the windows' prefixes
+    // of a chunk of kQ rows plus the batch pushed ahead: rows from yb - lmax - 1 up to
+    // yb + kQ + lmax + kB - 2 are live, so a ring of 2*lmax + kB + kQ + 2 slots never overwrites
+    // one before its last read
+    const int span = 2 * lmax + kB + kQ + 2;
     if (default_ranges && d0 >= 0 && nthr <= 128) {
-        const int span = 2 * lmax + kB + 2;
         const size_t extra = (size_t)(2 * lmax + 2) * 4 + (size_t)cols * (kSeg + 2 * lmax) + (size_t)cols * kSeg * 2;
         auto go = [&](auto rs_tag) -> cudaError_t {
             constexpr int RS = decltype(rs_tag)::value;
@@ -407,7 +420,6 @@ cudaError_t launch_cross_v(int w, int h, int d0, int D, int Dp, int lmax, int ta
     }
     if (nthr <= 256) {
         // any ranges: sum and count rings, batched loads
-        const int span = 2 * lmax + kB + 2;
         const size_t extra = (size_t)cols * kSeg * 4 + (size_t)(2 * lmax + 2) * 4 + (size_t)cols * (kSeg + 2 * lmax) +
                              (size_t)cols * kSeg * 2;
         auto go = [&](auto rs_tag) -> cudaError_t {
