@@ -10,6 +10,10 @@
 #pragma once
 
 #include <cstdint>
+#include <map>
+#include <mutex>
+#include <utility>
+
 #include <cuda_runtime.h>
 
 namespace apgcu {
@@ -103,22 +107,40 @@ __device__ __forceinline__ int adaptive_p2(const SgmPen& p, int dI) {
 }
 
 // Lets `kern` launch with as much dynamic shared memory as the device allows it (the opt-in
-// maximum less the function's static shared memory).  The attribute is per function and shared by
-// every host thread, so it is always set to that same per-function maximum, never to one launch's
-// size: a thread launching with more shared memory than another thread's last setting would
-// otherwise be refused.  Occupancy follows each launch's actual size.
+// maximum less the function's static shared memory), and refuses a larger request.  The attribute
+// is per function and shared by every host thread, so it is always set to that same per-function
+// maximum, never to one launch's size: a thread launching with more shared memory than another
+// thread's last setting would otherwise be refused.  It is set once per (function, device) -- also
+// for requests under 48 KB, whose sum with the static size may still exceed the default limit --
+// and remembered.  Occupancy follows each launch's actual size.
 template <typename F>
 inline cudaError_t allow_dynamic_smem(F kern, size_t smem) {
-    if (smem <= 48 * 1024) return cudaSuccess;
-    int dev = 0, optin = 0;
+    int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
-    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    cudaFuncAttributes fa;
-    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, kern);
     if (e != cudaSuccess) return e;
-    const int limit = optin - (int)fa.sharedSizeBytes;
-    if ((long long)smem > limit) return cudaErrorInvalidValue;
-    return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, limit);
+    static std::mutex mu;
+    static std::map<std::pair<const void*, int>, int> limits;
+    const std::pair<const void*, int> key(reinterpret_cast<const void*>(kern), dev);
+    int limit = -1;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        const auto it = limits.find(key);
+        if (it != limits.end()) limit = it->second;
+    }
+    if (limit < 0) {
+        int optin = 0;
+        cudaFuncAttributes fa;
+        e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+        if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, kern);
+        if (e == cudaSuccess) {
+            limit = optin - (int)fa.sharedSizeBytes;
+            e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, limit);
+        }
+        if (e != cudaSuccess) return e;
+        std::lock_guard<std::mutex> lk(mu);
+        limits[key] = limit;
+    }
+    return (long long)smem > limit ? cudaErrorInvalidValue : cudaSuccess;
 }
 
 #define APGCU_CHECK(expr)                                                    \
