@@ -18,12 +18,17 @@ namespace {
 constexpr int TX = 32, TY = 8, HX = 4, HY = 3;
 constexpr int SX = TX + 2 * HX, SY = TY + 2 * HY;
 
+// blockIdx.z selects the image: both images of a pair go through one launch.
 template <bool C64>
-__global__ void __launch_bounds__(TX * TY) aux_kernel(const uint8_t* __restrict__ src, int stride, int ch,
-                                                      int w, int h, uint8_t* __restrict__ gray,
-                                                      uint8_t* __restrict__ gx, uint8_t* __restrict__ gy,
-                                                      uint32_t* __restrict__ census,
-                                                      unsigned long long* __restrict__ census64) {
+__global__ void __launch_bounds__(TX * TY) aux_kernel(AuxImage im0, AuxImage im1, int ch, int w, int h) {
+    const AuxImage& im = blockIdx.z ? im1 : im0;
+    const uint8_t* __restrict__ src = im.src;
+    const int stride = im.stride;
+    uint8_t* __restrict__ gray = im.gray;
+    uint8_t* __restrict__ gx = im.gx;
+    uint8_t* __restrict__ gy = im.gy;
+    uint32_t* __restrict__ census = im.census;
+    unsigned long long* __restrict__ census64 = im.census64;
     __shared__ uint8_t g[SY][SX];
     const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
     const int tid = threadIdx.y * TX + threadIdx.x;
@@ -83,12 +88,11 @@ __global__ void __launch_bounds__(TX * TY) aux_kernel(const uint8_t* __restrict_
 }
 }  // namespace
 
-cudaError_t launch_aux(const uint8_t* src, int stride, int ch, int w, int h, int census64,
-                       uint8_t* gray, uint8_t* gx, uint8_t* gy, uint32_t* census,
-                       unsigned long long* census_wide, cudaStream_t s) {
-    dim3 grid((w + TX - 1) / TX, (h + TY - 1) / TY), block(TX, TY);
-    if (census64) aux_kernel<true><<<grid, block, 0, s>>>(src, stride, ch, w, h, gray, gx, gy, census, census_wide);
-    else aux_kernel<false><<<grid, block, 0, s>>>(src, stride, ch, w, h, gray, gx, gy, census, census_wide);
+cudaError_t launch_aux(const AuxImage& left, const AuxImage& right, int ch, int w, int h, int census64,
+                       cudaStream_t s) {
+    dim3 grid((w + TX - 1) / TX, (h + TY - 1) / TY, 2), block(TX, TY);
+    if (census64) aux_kernel<true><<<grid, block, 0, s>>>(left, right, ch, w, h);
+    else aux_kernel<false><<<grid, block, 0, s>>>(left, right, ch, w, h);
     return cudaGetLastError();
 }
 

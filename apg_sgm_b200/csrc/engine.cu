@@ -478,10 +478,13 @@ int Engine::run_pre(const uint8_t* dl, int lstride, const uint8_t* dr, int rstri
     (void)D; (void)Dp; (void)d0; (void)n; (void)w; (void)h;
     const int c64 = cfg_.census_type == APG_CENSUS_9X7;
     cudaEventRecord(ev_[0], s);
-    RUN(launch_aux(dl, lstride, ch, w, h, c64, ptr<uint8_t>(L.lgray), ptr<uint8_t>(L.lgx), ptr<uint8_t>(L.lgy),
-                   ptr<uint32_t>(L.cl), ptr<unsigned long long>(L.cl), s), "aux(left)");
-    RUN(launch_aux(dr, rstride, ch, w, h, c64, ptr<uint8_t>(L.rgray), ptr<uint8_t>(L.rgx), ptr<uint8_t>(L.rgy),
-                   ptr<uint32_t>(L.cr), ptr<unsigned long long>(L.cr), s), "aux(right)");
+    {
+        const AuxImage li{dl, lstride, ptr<uint8_t>(L.lgray), ptr<uint8_t>(L.lgx), ptr<uint8_t>(L.lgy),
+                          ptr<uint32_t>(L.cl), ptr<unsigned long long>(L.cl)};
+        const AuxImage ri{dr, rstride, ptr<uint8_t>(L.rgray), ptr<uint8_t>(L.rgx), ptr<uint8_t>(L.rgy),
+                          ptr<uint32_t>(L.cr), ptr<unsigned long long>(L.cr)};
+        RUN(launch_aux(li, ri, ch, w, h, c64, s), "aux");
+    }
     cudaEventRecord(ev_[1], s);
     ranges_written_ = range_planes_needed();
     if (ranges_written_)

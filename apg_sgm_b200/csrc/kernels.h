@@ -12,8 +12,15 @@
 namespace apgcu {
 
 // aux.cu
-cudaError_t launch_aux(const uint8_t* src, int stride, int ch, int w, int h, int census64, uint8_t* gray,
-                       uint8_t* gx, uint8_t* gy, uint32_t* census, unsigned long long* census_wide,
+// One image's input and aux planes (gray, |gx|, |gy|, census 32 or 64 bits).
+struct AuxImage {
+    const uint8_t* src;
+    int stride;
+    uint8_t *gray, *gx, *gy;
+    uint32_t* census;
+    unsigned long long* census64;
+};
+cudaError_t launch_aux(const AuxImage& left, const AuxImage& right, int ch, int w, int h, int census64,
                        cudaStream_t s);
 
 // cost.cu: mode 0 raw volume, 1 cross-H volume, 2 right argmin only; all update rkey.

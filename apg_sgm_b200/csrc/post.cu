@@ -196,10 +196,10 @@ __global__ void fill_ballot_kernel(int w, int h, int gap, const float* __restric
                                    const float* __restrict__ d_prior, float* __restrict__ out) {
     const int lane = threadIdx.x & 31;
     const int nseg = (w + 31) >> 5;
-    const long long total = (long long)nseg * h;
-    const long long wstride = ((long long)gridDim.x * blockDim.x) >> 5;
-    for (long long sg = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; sg < total; sg += wstride) {
-        const int y = (int)(sg / nseg), s = (int)(sg - (long long)y * nseg);
+    const int total = nseg * h;  // segments of the frame (w * h / 32 + h, far below 2^31)
+    const int wstride = (gridDim.x * blockDim.x) >> 5;
+    for (int sg = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; sg < total; sg += wstride) {
+        const int y = sg / nseg, s = sg - y * nseg;
         const int x = (s << 5) + lane;
         const float* row = in + (size_t)y * w;
         const bool inimg = x < w;
