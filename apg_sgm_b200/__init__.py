@@ -27,6 +27,14 @@ class QualityMode(enum.IntEnum):
     HighQuality = 2
 
 
+class HierarchicalFallback(enum.IntEnum):
+    """HierarchicalFallback (include/apg_sgm/config.hpp:68-72): the range of a pixel whose 2x2
+    coarse neighbourhood has no valid disparity."""
+    NearestValid = 0
+    FullRange = 1
+    ExpandedRadius = 2
+
+
 class VolumeBackend(enum.IntEnum):
     Auto = 0
     Dense = 1
@@ -182,7 +190,10 @@ def _parse(value, enum_cls, table, what):
     if isinstance(value, str):
         s = value.lower()
         if s not in table:
-            valid = ", ".join(f"'{k}'" for k in dict.fromkeys(table.values()).keys())
+            first = {}
+            for k, v in table.items():
+                first.setdefault(v, k)
+            valid = ", ".join(f"'{k}'" for k in first.values())
             raise ValueError(f"Unrecognized {what} '{s}'. Valid: {valid}")
         return table[s]
     return enum_cls(int(value))
@@ -192,6 +203,9 @@ _MODES = {"fast": QualityMode.Fast, "balanced": QualityMode.Balanced, "high_qual
           "hq": QualityMode.HighQuality, "highquality": QualityMode.HighQuality}
 _BACKENDS = {"auto": VolumeBackend.Auto, "dense": VolumeBackend.Dense, "packed": VolumeBackend.Packed,
              "cuda": VolumeBackend.CUDA}
+_FALLBACKS = {"nearest_valid": HierarchicalFallback.NearestValid, "nearest": HierarchicalFallback.NearestValid,
+              "full_range": HierarchicalFallback.FullRange, "full": HierarchicalFallback.FullRange,
+              "expanded_radius": HierarchicalFallback.ExpandedRadius, "expanded": HierarchicalFallback.ExpandedRadius}
 _POLICIES = {"bounded_reuse": MemoryPolicy.BoundedReuse, "boundedreuse": MemoryPolicy.BoundedReuse,
              "reuse": MemoryPolicy.BoundedReuse, "release_per_frame": MemoryPolicy.ReleasePerFrame,
              "release": MemoryPolicy.ReleasePerFrame, "releaseperframe": MemoryPolicy.ReleasePerFrame}
@@ -204,7 +218,9 @@ class StereoSession:
     (ctypes releases the GIL for the duration of every library call)."""
 
     def __init__(self, mode="balanced", threads=0, max_disparity=128, min_disparity=0, backend="auto",
-                 memory_policy="release_per_frame", max_retained_bytes=0, config: PipelineConfig | None = None):
+                 memory_policy="release_per_frame", max_retained_bytes=0, hierarchical=False, hierarchical_radius=4,
+                 hierarchical_fallback=None, adaptive_radius=False, confidence_threshold=0.5, expanded_radius=8,
+                 config: PipelineConfig | None = None):
         qm = _parse(mode, QualityMode, _MODES, "mode")
         if qm is None:
             qm = QualityMode.Balanced
@@ -224,6 +240,16 @@ class StereoSession:
             cfg = config
         if be is not None:
             cfg.volume_backend = int(be)
+        if hierarchical:
+            # binding.cpp:200-223
+            cfg.hier_enable = 1
+            cfg.hier_radius = int(hierarchical_radius)
+            cfg.hier_adaptive_radius = 1 if adaptive_radius else 0
+            cfg.hier_confidence_threshold = float(confidence_threshold)
+            cfg.hier_expanded_radius = int(expanded_radius)
+            fb = _parse(hierarchical_fallback, HierarchicalFallback, _FALLBACKS, "hierarchical_fallback")
+            if fb is not None:
+                cfg.hier_fallback = int(fb)
         err = _validate_config(cfg)
         if err:
             raise RuntimeError(err)
@@ -332,9 +358,34 @@ class StereoSession:
     def last_error(self):
         return lib().apg_session_get_last_error(self._h).decode()
 
+    @property
+    def hierarchical_enabled(self) -> bool:
+        return bool(self._cfg.hier_enable)
+
+    @property
+    def hierarchical_radius(self) -> int:
+        return int(self._cfg.hier_radius)
+
+    @property
+    def adaptive_radius(self) -> bool:
+        return bool(self._cfg.hier_adaptive_radius)
+
+    @property
+    def hierarchical_telemetry(self) -> dict:
+        """HierarchicalTelemetry of the last frame (src/hierarchical_stereo.hpp:36-42); all zero
+        without hierarchical mode or for frames under 32 x 32."""
+        return _hier_dict(lib().apgcu_session_hier_telemetry, self._h)
+
     def __repr__(self):
-        return (f"<apg_sgm.StereoSession frames={self.frame_count} avg_time_ms={self.average_time_ms} "
-                f"allocated_bytes={self.allocated_bytes}>")
+        # PyStereoSession::repr, binding.cpp:335-351
+        r = (f"<apg_sgm.StereoSession frames={self.frame_count} avg_time_ms={self.average_time_ms} "
+             f"allocated_bytes={self.allocated_bytes}")
+        if self._cfg.hier_enable:
+            r += f" hierarchical=True (R={self._cfg.hier_radius}"
+            if self._cfg.hier_adaptive_radius:
+                r += f", adaptive_R={self._cfg.hier_expanded_radius}@{self._cfg.hier_confidence_threshold:.2f}"
+            r += ")"
+        return r + ">"
 
     def __del__(self):
         try:
@@ -364,7 +415,33 @@ def _validate_config(cfg: PipelineConfig) -> str:
         return "prior search_radius must be non-negative"
     if cfg.refine_enable and cfg.refine_iterations < 0:
         return "refine iterations must be non-negative"
+    if cfg.hier_enable:
+        if cfg.volume_backend == VolumeBackend.Dense:
+            return "hierarchical mode requires Auto or Packed backend"
+        if cfg.hier_radius <= 0:
+            return "hierarchical radius must be strictly positive"
+        if cfg.hier_scale != 2:
+            return "hierarchical scale currently supports only 2"
+        if cfg.hier_adaptive_radius:
+            if cfg.hier_expanded_radius < cfg.hier_radius:
+                return "hierarchical expanded_radius cannot be less than radius"
+            if not (0.0 <= cfg.hier_confidence_threshold <= 1.0):
+                return "hierarchical confidence_threshold must be between 0.0 and 1.0"
     return ""
+
+
+_HIER_KEYS = ("avg_states_per_pixel", "coarse_valid_ratio", "fallback_pixel_ratio", "full_range_pixel_ratio",
+              "coarse_time_ms")
+
+
+def _hier_dict(fn, handle) -> dict:
+    v = (C.c_double * 6)()
+    rc = fn(handle, v)
+    if rc != 0:
+        raise RuntimeError(f"hierarchical telemetry failed [{rc}]")
+    d = dict(zip(_HIER_KEYS, list(v)[:5]))
+    d["coarse_pass"] = bool(v[5])
+    return d
 
 
 DUMPS = ["left_gray", "left_gx", "left_gy", "right_gray", "right_gx", "right_gy", "census_left", "census_right",
@@ -426,6 +503,10 @@ class Engine:
             raise RuntimeError(self.last_error)
 
     @property
+    def hier_telemetry(self) -> dict:
+        """HierarchicalTelemetry of the last pair (apgcu_engine_hier_telemetry)."""
+        return _hier_dict(lib().apgcu_engine_hier_telemetry, self._h)
+
     def stream(self) -> int:
         return int(lib().apgcu_engine_stream(self._h) or 0)
 
@@ -495,7 +576,7 @@ def workspace_bytes(config: PipelineConfig, width: int, height: int) -> int:
     return int(lib().apgcu_workspace_bytes(C.byref(config), int(width), int(height)))
 
 
-__all__ = ["QualityMode", "VolumeBackend", "MemoryPolicy", "StatusCode", "InvalidReason", "StageTiming",
+__all__ = ["QualityMode", "HierarchicalFallback", "VolumeBackend", "MemoryPolicy", "StatusCode", "InvalidReason", "StageTiming",
            "PipelineStats", "StereoResult", "StereoSession", "PipelineConfig", "config_from_mode", "Engine",
            "kernel_launch_count", "workspace_bytes", "__version__"]
 

@@ -35,6 +35,10 @@ class PipelineConfig(C.Structure):
         ("refine_enable", C.c_int), ("refine_iterations", C.c_int), ("refine_random_radius", C.c_int),
         ("subpixel", C.c_int), ("lr_check", C.c_int), ("post_lr_max_diff", C.c_int),
         ("median_radius", C.c_int), ("max_fill_gap", C.c_int),
+        ("hier_enable", C.c_int), ("hier_radius", C.c_int), ("hier_scale", C.c_int), ("hier_fallback", C.c_int),
+        ("hier_coarse_cross_agg", C.c_int), ("hier_coarse_fill_holes", C.c_int),
+        ("hier_adaptive_radius", C.c_int), ("hier_confidence_threshold", C.c_float),
+        ("hier_expanded_radius", C.c_int),
     ]
 
     @property
@@ -117,6 +121,8 @@ _SIGS = {
     "apgcu_session_get_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_size_t)]),
     "apgcu_session_estimate_bytes": (C.c_size_t, [C.c_void_p, C.c_int, C.c_int, C.c_int]),
     "apgcu_session_get_frame_counts": (C.c_int, [C.c_void_p, C.POINTER(C.c_ulonglong)]),
+    "apgcu_session_hier_telemetry": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
+    "apgcu_engine_hier_telemetry": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     "apgcu_kernel_launch_count": (C.c_ulonglong, []),
     "apgcu_engine_launch_profile": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_char_p), C.POINTER(C.c_float)]),
     "apgcu_batch_create": (C.c_void_p, [C.POINTER(PipelineConfig), C.c_int]),

@@ -75,6 +75,22 @@ int Engine::validate_config(const apg_pipeline_config_t& c, std::string& msg) {
     }
     if (c.prior_enable && c.prior_search_radius < 0) { msg = "prior search_radius must be non-negative"; return kInvalidConfig; }
     if (c.refine_enable && c.refine_iterations < 0) { msg = "refine iterations must be non-negative"; return kInvalidConfig; }
+    if (c.hier_enable) {
+        // src/pipeline.cpp:193-210
+        if (c.volume_backend == 1) { msg = "hierarchical mode requires Auto or Packed backend"; return kInvalidConfig; }
+        if (c.hier_radius <= 0) { msg = "hierarchical radius must be strictly positive"; return kInvalidConfig; }
+        if (c.hier_scale != 2) { msg = "hierarchical scale currently supports only 2"; return kInvalidConfig; }
+        if (c.hier_adaptive_radius) {
+            if (c.hier_expanded_radius < c.hier_radius) {
+                msg = "hierarchical expanded_radius cannot be less than radius";
+                return kInvalidConfig;
+            }
+            if (!(c.hier_confidence_threshold >= 0.f && c.hier_confidence_threshold <= 1.f)) {
+                msg = "hierarchical confidence_threshold must be between 0.0 and 1.0";
+                return kInvalidConfig;
+            }
+        }
+    }
     if (c.refine_enable && c.refine_iterations > kRefineMaxIter) {
         msg = "refine iterations above 63 are not supported by the CUDA backend";
         return kUnsupportedBackend;
@@ -100,7 +116,35 @@ int Engine::validate_config(const apg_pipeline_config_t& c, std::string& msg) {
         }
     }
     if (c.median_radius > 15) { msg = "median radius above 15 is not supported"; return kUnsupportedBackend; }
+    if (c.hier_enable) {
+        // the half-size pass runs on the same kernels: its configuration must fit them too
+        std::string m;
+        const int rc = validate_config(coarse_config(c), m);
+        if (rc != kOk) { msg = "hierarchical coarse pass: " + m; return rc; }
+    }
     return kOk;
+}
+
+apg_pipeline_config_t Engine::coarse_config(const apg_pipeline_config_t& c) {
+    apg_pipeline_config_t k = c;
+    k.min_disparity = std::max(0, c.min_disparity / 2);
+    k.max_disparity = std::max(k.min_disparity + 1, (c.max_disparity + 1) / 2);
+    k.prior_enable = 0;
+    k.refine_enable = 0;
+    k.agg_enable = c.hier_coarse_cross_agg;
+    k.volume_backend = 2;
+    k.subpixel = 1;
+    k.lr_check = 1;
+    k.median_radius = 1;
+    k.max_fill_gap = c.hier_coarse_fill_holes ? 16 : 0;
+    k.hier_enable = 0;
+    return k;
+}
+
+size_t Engine::workspace_bytes(const apg_pipeline_config_t& c, int w, int h, int ch, int debug) {
+    size_t t = make_layout(c, w, h, ch, debug).total;
+    if (hier_runs(c, w, h)) t += make_layout(coarse_config(c), w / 2, h / 2, 1, 0).total;
+    return t;
 }
 
 Layout Engine::make_layout(const apg_pipeline_config_t& c, int w, int h, int ch, int debug) {
@@ -113,7 +157,7 @@ Layout Engine::make_layout(const apg_pipeline_config_t& c, int w, int h, int ch,
     // volume-fed sweeps are the faster ones); on request the sweeps recompute the census costs
     // instead and no volume is allocated (kLayoutFastFused)
     L.fused_fast = !L.cross && c.census_type == APG_CENSUS_SYMMETRIC_9X7 && !c.use_ad && !c.use_grad &&
-                   !c.prior_enable && (debug & kLayoutFastFused) && !(debug & 4);
+                   !c.prior_enable && !c.hier_enable && (debug & kLayoutFastFused) && !(debug & 4);
     L.raw_cost = (debug & 1) != 0;
     const size_t n = (size_t)w * h;
     const size_t csz = c.census_type == APG_CENSUS_9X7 ? 8 : 4;
@@ -143,7 +187,13 @@ Layout Engine::make_layout(const apg_pipeline_config_t& c, int w, int h, int ch,
     L.qlut = take(65 * 2);
     L.magic = take(256 * 4);
     L.stats = take(64);
-    if (c.prior_enable) {
+    if (hier_runs(c, w, h)) {
+        const size_t nc = (size_t)(w / 2) * (h / 2);
+        L.hc_left = take(nc);
+        L.hc_right = take(nc);
+    }
+    if (c.hier_enable) L.hstats = take(64);
+    if (c.prior_enable && !c.hier_enable) {
         const int cell = 16;
         L.gw = (w + cell - 1) / cell; L.gh = (h + cell - 1) / cell; L.n_cells = L.gw * L.gh;
         const int hard_max = std::max(0, c.prior_max_supports);
@@ -221,6 +271,7 @@ void Engine::release() {
         pinned_bytes_ = 0;
     }
     rtab_.release();
+    coarse_.reset();
     lay_ = Layout();
 }
 
@@ -237,7 +288,7 @@ int Engine::cuda_fail(cudaError_t e, const char* where) {
 // written at all.
 bool Engine::range_planes_needed() const {
     // the stage-dump debug flags keep every intermediate; the launch profile alone changes no work
-    if (cfg_.prior_enable || cfg_.refine_enable || (debug_ & ~8)) return true;
+    if (ranged() || cfg_.refine_enable || (debug_ & ~8)) return true;
     return cfg_.agg_enable && (cfg_.agg_iterations > 1 || cfg_.min_disparity < 0 || lay_.Dp > 256);
 }
 
@@ -266,13 +317,27 @@ CostCtx Engine::cost_ctx() const {
     c.cl = ptr<uint32_t>(lay_.cl); c.cr = ptr<uint32_t>(lay_.cr);
     c.cl64 = ptr<unsigned long long>(lay_.cl); c.cr64 = ptr<unsigned long long>(lay_.cr);
     c.rmin = ptr<int16_t>(lay_.rmin); c.rmax = ptr<int16_t>(lay_.rmax);
-    c.prior_ranges = cfg_.prior_enable ? 1 : 0;
+    c.prior_ranges = ranged() ? 1 : 0;
     c.tile = cost_tile_;
     c.kernel = cost_kernel_;
     return c;
 }
 
 int Engine::prepare(int w, int h, int ch) {
+    const int rc = prepare_arena(w, h, ch);
+    if (rc != kOk || !hier_runs(cfg_, w, h)) return rc;
+    // hierarchical mode: the half-size engine enqueues on this engine's stream
+    if (!coarse_) {
+        coarse_ = std::make_unique<Engine>(coarse_config(cfg_), device_, stream_);
+        coarse_->skip_fill_ = !cfg_.hier_coarse_fill_holes;
+    }
+    coarse_->cost_kernel_ = cost_kernel_;
+    const int r2 = coarse_->prepare(w / 2, h / 2, 1);
+    if (r2 != kOk) return fail(r2, "hierarchical coarse pass: " + coarse_->last_error());
+    return kOk;
+}
+
+int Engine::prepare_arena(int w, int h, int ch) {
     const Layout L = make_layout(cfg_, w, h, ch, debug_ | (fast_fused_ ? kLayoutFastFused : 0));
     if (arena_ && arena_bytes_ >= L.total && lay_.w == w && lay_.h == h && lay_.ch == ch &&
         lay_.raw_cost == L.raw_cost && lay_.fused_fast == L.fused_fast) {
@@ -486,21 +551,31 @@ int Engine::run_pre(const uint8_t* dl, int lstride, const uint8_t* dr, int rstri
         RUN(launch_aux(li, ri, ch, w, h, c64, s), "aux");
     }
     cudaEventRecord(ev_[1], s);
+    // search ranges: the hierarchical pass (frames of 32 x 32 and more) writes every pixel's
+    // range itself; otherwise the default ranges, narrowed by the prior where it runs
+    hier_ran_ = hier_runs(cfg_, w, h);
     ranges_written_ = range_planes_needed();
-    if (ranges_written_)
+    if (ranges_written_ && !hier_ran_)
         RUN(launch_default_range(w, h, d0, cfg_.max_disparity, ptr<int16_t>(L.rmin), ptr<int16_t>(L.rmax), s),
             "range");
     const CostCtx cc = cost_ctx();
     support_count_ = 0;
-    if (cfg_.prior_enable) {
+    if (hier_ran_) {
+        count_launches(launches);
+        launches = 0;
+        const int rc = run_hier();
+        if (rc != kOk) return rc;
+    } else if (prior_runs()) {
         e = launch_prior(cfg_, cc, L, arena_, s, &launches);
         if (e != cudaSuccess) return cuda_fail(e, "prior");
         if (prof) prof_mark("prior");
-    } else if (debug_) {
-        // no prior: d_prior is -1 everywhere (read only by the stage dump)
+    } else if (debug_ || ranged()) {
+        // no guiding disparity: d_prior is -1 everywhere (read by the fill in hierarchical mode,
+        // otherwise only by the stage dump)
         fill_u32_kernel<<<std::min((int)((n + 255) / 256), 148 * 8), 256, 0, s>>>(ptr<uint32_t>(L.d_prior), n, 0xBF800000u);
         ++launches;
     }
+    if (cfg_.hier_enable && !hier_ran_) RUNC(cudaMemsetAsync(arena_ + L.hstats, 0, 32, s), "hier stats init");
     cudaEventRecord(ev_[2], s);
     // cost (+ cross-H, + right argmin)
     RUNC(cudaMemsetAsync(ptr<uint32_t>(L.rkey), 0xFF, n * 4, s), "rkey init");
@@ -522,13 +597,13 @@ int Engine::run_pre(const uint8_t* dl, int lstride, const uint8_t* dr, int rstri
     if (L.cross) {
         const int tau = cfg_.color_threshold;
         RUN(launch_cross_v(w, h, d0, D, Dp, lmax, tau, ptr<uint8_t>(L.lgray), ptr<int16_t>(L.rmin), ptr<int16_t>(L.rmax),
-                           ptr<uint32_t>(L.volA), ptr<uint32_t>(L.volB), magic, !cfg_.prior_enable, s), "crossV");
+                           ptr<uint32_t>(L.volA), ptr<uint32_t>(L.volB), magic, !ranged(), s), "crossV");
         const int iters = std::max(1, cfg_.agg_iterations);
         for (int it = 1; it < iters; ++it) {
             RUN(launch_cross_h(w, h, d0, D, Dp, lmax, tau, ptr<uint8_t>(L.lgray), ptr<int16_t>(L.rmin), ptr<int16_t>(L.rmax),
                                ptr<uint32_t>(L.volB), ptr<uint32_t>(L.volA), magic, s), "crossH");
             RUN(launch_cross_v(w, h, d0, D, Dp, lmax, tau, ptr<uint8_t>(L.lgray), ptr<int16_t>(L.rmin), ptr<int16_t>(L.rmax),
-                               ptr<uint32_t>(L.volA), ptr<uint32_t>(L.volB), magic, !cfg_.prior_enable, s), "crossV");
+                               ptr<uint32_t>(L.volA), ptr<uint32_t>(L.volB), magic, !ranged(), s), "crossV");
         }
         sgm_src = ptr<uint32_t>(L.volB);
     }
@@ -731,13 +806,19 @@ int Engine::run_post(float* d_disp, float* d_conf, uint8_t* d_reason, uint8_t* d
     } else {
         cudaEventRecord(ev_[8], s);
     }
-    RUN(launch_fill(w, h, cfg_.max_fill_gap, post_in, ptr<uint8_t>(L.reason), ptr<uint8_t>(L.lgray),
-                    cfg_.prior_enable ? ptr<float>(L.d_prior) : nullptr, ptr<float>(L.disp_fill), s), "fill");
+    // the hierarchical coarse pass without coarse_fill_holes calls no fill at all
+    // (src/hierarchical_stereo.cpp:262-265); a zero gap would still fill from the neighbours
+    const float* med_in = post_in;
+    if (!skip_fill_) {
+        RUN(launch_fill(w, h, cfg_.max_fill_gap, post_in, ptr<uint8_t>(L.reason), ptr<uint8_t>(L.lgray),
+                        ranged() ? ptr<float>(L.d_prior) : nullptr, ptr<float>(L.disp_fill), s), "fill");
+        med_in = ptr<float>(L.disp_fill);
+    }
     float* final_out = d_disp ? d_disp : ptr<float>(L.disp_out);
     if (cfg_.median_radius > 0) {
-        RUN(launch_median(w, h, cfg_.median_radius, ptr<float>(L.disp_fill), final_out, s), "median");
+        RUN(launch_median(w, h, cfg_.median_radius, med_in, final_out, s), "median");
     } else {
-        RUNC(cudaMemcpyAsync(final_out, ptr<float>(L.disp_fill), n * 4, cudaMemcpyDeviceToDevice, s), "copy");
+        RUNC(cudaMemcpyAsync(final_out, med_in, n * 4, cudaMemcpyDeviceToDevice, s), "copy");
     }
     if (d_reason) RUNC(cudaMemcpyAsync(d_reason, ptr<uint8_t>(L.reason), n, cudaMemcpyDeviceToDevice, s), "reason out");
     if (d_conf) RUNC(cudaMemcpyAsync(d_conf, ptr<float>(L.confidence), n * 4, cudaMemcpyDeviceToDevice, s), "conf out");
@@ -754,15 +835,64 @@ int Engine::run_post(float* d_disp, float* d_conf, uint8_t* d_reason, uint8_t* d
                            planes ? ptr<int16_t>(L.rmin) : nullptr, planes ? ptr<int16_t>(L.rmax) : nullptr,
                            planes ? 0ull : default_range_width_sum(), st, s),
         "frame stats");
-    if (cfg_.prior_enable) RUNC(cudaMemcpyAsync(st + 5, arena_ + L.pr_count, 4, cudaMemcpyDeviceToDevice, s), "support count");
+    if (prior_runs()) RUNC(cudaMemcpyAsync(st + 5, arena_ + L.pr_count, 4, cudaMemcpyDeviceToDevice, s), "support count");
     cudaEventRecord(ev_[9], s);
     have_times_ = true;
     count_launches(launches);
     return kOk;
 }
 
+// HierarchicalStereo::estimate_search_range (src/hierarchical_stereo.cpp:113-431) after the
+// full-size aux planes: the half-size grays, the whole pipeline over them on the coarse engine
+// (same stream, its outputs stay in its arena), then every full-size pixel's range and guiding
+// disparity from the coarse disparity and confidence.
+int Engine::run_hier() {
+    const Layout& L = lay_;
+    const int w = L.w, h = L.h;
+    cudaStream_t s = stream_;
+    unsigned launches = 0;
+    cudaError_t e = cudaSuccess;
+    const bool prof = (debug_ & 8) != 0;
+    RUN(launch_hier_downsample(ptr<uint8_t>(L.lgray), ptr<uint8_t>(L.rgray), w, h, ptr<uint8_t>(L.hc_left),
+                               ptr<uint8_t>(L.hc_right), s), "hier downsample");
+    count_launches(launches);
+    launches = 0;
+    const int rc = coarse_->run(ptr<uint8_t>(L.hc_left), w / 2, ptr<uint8_t>(L.hc_right), w / 2, 1, nullptr, nullptr,
+                                nullptr, nullptr);
+    if (rc != kOk) return fail(rc, "hierarchical coarse pass: " + coarse_->last_error());
+    if (prof) prof_mark("hier coarse pass");
+    RUNC(cudaMemsetAsync(arena_ + L.hstats, 0, 32, s), "hier stats init");
+    const Layout& K = coarse_->lay_;
+    RUN(launch_hier_range(cfg_, w, h, coarse_->ptr<float>(K.disp_out), coarse_->ptr<float>(K.confidence),
+                          ptr<int16_t>(L.rmin), ptr<int16_t>(L.rmax), ptr<float>(L.d_prior),
+                          ptr<unsigned long long>(L.hstats), s), "hier range");
+    count_launches(launches);
+    return kOk;
+}
+
 #undef RUN
 #undef RUNC
+
+int Engine::hier_telemetry(double* out6) {
+    for (int i = 0; i < 6; ++i) out6[i] = 0.0;
+    if (!arena_ || !cfg_.hier_enable) return kOk;
+    unsigned long long c[4] = {};
+    cudaError_t e = cudaMemcpyAsync(c, arena_ + lay_.hstats, sizeof(c), cudaMemcpyDeviceToHost, stream_);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+    if (e != cudaSuccess) return cuda_fail(e, "hierarchical telemetry");
+    if (!hier_ran_) return kOk;
+    // src/hierarchical_stereo.cpp:413-420: double ratios, three of them stored as float
+    const double n = (double)lay_.w * lay_.h, nc = (double)(lay_.w / 2) * (lay_.h / 2);
+    out6[0] = n > 0 ? (double)(long long)c[3] / n : 0.0;
+    out6[1] = nc > 0 ? (double)(float)((double)c[0] / nc) : 0.0;
+    out6[2] = n > 0 ? (double)(float)((double)c[1] / n) : 0.0;
+    out6[3] = n > 0 ? (double)(float)((double)c[2] / n) : 0.0;
+    float ms = 0.f;
+    if (have_times_ && cudaEventElapsedTime(&ms, ev_[1], ev_[2]) == cudaSuccess) out6[4] = ms;
+    cudaGetLastError();
+    out6[5] = 1.0;
+    return kOk;
+}
 
 void Engine::prof_mark(const char* name) {
     if (nprof_ >= kMaxProf) return;
@@ -1033,7 +1163,12 @@ size_t apgcu_engine_allocated_bytes(apgcu_engine_t e) { return e ? e->eng->alloc
 
 size_t apgcu_workspace_bytes(const apg_pipeline_config_t* cfg, int width, int height) {
     if (!cfg || width <= 0 || height <= 0) return 0;
-    return apgcu::Engine::make_layout(*cfg, width, height, 3, 0).total;
+    return apgcu::Engine::workspace_bytes(*cfg, width, height, 3, 0);
+}
+
+int apgcu_engine_hier_telemetry(apgcu_engine_t e, double* out6) {
+    if (!e || !out6) return apgcu::kInternalError;
+    return e->eng->hier_telemetry(out6);
 }
 
 void apgcu_engine_release(apgcu_engine_t e) {

@@ -10,6 +10,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <memory>
 #include <random>
 #include <string>
 #include <vector>
@@ -52,6 +53,8 @@ struct Layout {
     size_t rf_prefix, rf_scan_tmp, rf_state, rf_pack, rf_steps;  // refine: draw-index prefix, scan scratch,
                                                                    // pass state, packed images, pixel records
     size_t stats = 0;  // u64 frame counters (launch_frame_stats) + prior support count
+    // hierarchical search range: half-size grays of both images, telemetry counters (4 x u64)
+    size_t hc_left = 0, hc_right = 0, hstats = 0;
     size_t rf_scan_tmp_bytes = 0;
     int n_cells = 0, gw = 0, gh = 0, max_cand = 0;
 };
@@ -104,7 +107,14 @@ public:
     int sync();
     int dump(int what, void* dst, size_t bytes);
     void stage_times(double* ms11) const;
-    size_t allocated_bytes() const { return arena_bytes_ + pinned_bytes_ + rtab_.bytes; }
+    size_t allocated_bytes() const {
+        return arena_bytes_ + pinned_bytes_ + rtab_.bytes + (coarse_ ? coarse_->allocated_bytes() : 0);
+    }
+    // HierarchicalTelemetry of the last frame (src/hierarchical_stereo.hpp:36-42) from the device
+    // counters: avg_states_per_pixel, coarse_valid_ratio, fallback_pixel_ratio,
+    // full_range_pixel_ratio, coarse pass device time (ms), 1 if the coarse pass ran.  Waits for
+    // the engine stream.
+    int hier_telemetry(double* out6);
     void release();
     cudaStream_t stream() const { return stream_; }
     const std::string& last_error() const { return err_; }
@@ -120,9 +130,18 @@ public:
     // Validation shared with the session layer (src/pipeline.cpp:171-232 + device limits).
     static int validate_config(const apg_pipeline_config_t& c, std::string& msg);
     static Layout make_layout(const apg_pipeline_config_t& c, int w, int h, int ch, int debug);
+    // Device bytes for a W x H frame: the arena plus, in hierarchical mode, the half-size engine's.
+    static size_t workspace_bytes(const apg_pipeline_config_t& c, int w, int h, int ch, int debug);
+    // The half-size pass's configuration (src/hierarchical_stereo.cpp:172-182).
+    static apg_pipeline_config_t coarse_config(const apg_pipeline_config_t& c);
+    // Hierarchical mode runs its coarse pass for frames of at least 32 x 32 pixels.
+    static bool hier_runs(const apg_pipeline_config_t& c, int w, int h) {
+        return c.hier_enable && w >= 32 && h >= 32;
+    }
 
 private:
     int prepare(int w, int h, int ch);
+    int prepare_arena(int w, int h, int ch);
     int run(const uint8_t* dl, int lstride, const uint8_t* dr, int rstride, int ch, float* d_disp, float* d_conf,
             uint8_t* d_reason, uint8_t* d_reliable);
     // the three phases of run(): aux .. cross-V, the SGM sweeps + WTA, confidence .. frame counters
@@ -130,6 +149,11 @@ private:
     int run_sgm();
     int run_post(float* d_disp, float* d_conf, uint8_t* d_reason, uint8_t* d_reliable);
     int run_prior();
+    int run_hier();
+    // per-pixel ranges: from the prior or from the hierarchical pass (every other frame has the
+    // default range of each pixel); the prior does not run in hierarchical mode
+    bool ranged() const { return cfg_.prior_enable || cfg_.hier_enable; }
+    bool prior_runs() const { return cfg_.prior_enable && !cfg_.hier_enable; }
     int run_refine(float* work);
     int check_refine();  // after a synchronisation: the refine error flag of the last frame
     int fail(int code, const std::string& m) { err_ = m; return code; }
@@ -173,6 +197,9 @@ public:
 
 private:
     int support_count_ = 0;
+    std::unique_ptr<Engine> coarse_;  // hierarchical mode: the half-size engine (same stream)
+    bool skip_fill_ = false;          // coarse engine without coarse_fill_holes: no fill stage
+    bool hier_ran_ = false;           // the last frame ran the coarse pass
     unsigned long long counts_[8] = {};  // frame counters copied with the host outputs
     const uint32_t* sgm_src_ = nullptr;  // volume the SGM sweeps read (set by run_pre)
     RefineTables rtab_;                   // refine draw tables (HighQuality)

@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "apg_sgm/pipeline_config.h"
 
 namespace apgcu {
 
@@ -35,6 +36,13 @@ cudaError_t launch_cost(const CostCtx& c, int mode, int lmax, int tau, uint32_t*
 size_t cost_kernel_smem_bytes(int D, int Dp, int lmax, bool cross, bool census64);
 cudaError_t launch_right_wta_finalize(const CostCtx& c, const uint32_t* rkey, int subpixel, float* disp_right,
                                       cudaStream_t s);
+
+// hier.cu: the hierarchical search range around the half-size pass (Engine::run_hier).
+cudaError_t launch_hier_downsample(const uint8_t* lg, const uint8_t* rg, int w, int h, uint8_t* cl, uint8_t* cr,
+                                   cudaStream_t s);
+cudaError_t launch_hier_range(const apg_pipeline_config_t& c, int w, int h, const float* coarse_disp,
+                              const float* coarse_conf, int16_t* rmin, int16_t* rmax, float* d_prior,
+                              unsigned long long* counts, cudaStream_t s);
 
 // cross.cu
 cudaError_t launch_cross_v(int w, int h, int d0, int D, int Dp, int lmax, int tau, const uint8_t* gray,

@@ -140,7 +140,7 @@ public:
         int rc = Engine::validate_config(c, msg);
         if (rc) return rc;
         const PoolKey k{r.mode, r.width, r.height, r.channels, c.min_disparity, c.max_disparity};
-        const size_t need = Engine::make_layout(c, k.w, k.h, k.ch, 0).total;
+        const size_t need = Engine::workspace_bytes(c, k.w, k.h, k.ch, 0);
         std::vector<uint8_t> blank((size_t)r.width * r.height * r.channels, 0);
         for (int i = 0; i < count; ++i) {
             {
@@ -199,7 +199,7 @@ private:
             it->second.pop_back();
             return h;
         }
-        const size_t need = Engine::make_layout(c, k.w, k.h, k.ch, 0).total;
+        const size_t need = Engine::workspace_bytes(c, k.w, k.h, k.ch, 0);
         if (need > budget_) {
             *code = kResourceLimitExceeded;
             return Held();

@@ -45,6 +45,7 @@ struct apg_session_s {
     size_t frame_alloc = 0, frame_reuse = 0;
     double stage_ms[11] = {};
     unsigned long long counts[6] = {};  // Engine::frame_counts of the last frame
+    double hier[6] = {};                 // Engine::hier_telemetry of the last frame
     int frame_w = 0, frame_h = 0;        // its size
     size_t peak_bytes = 0;
     std::mutex mu;
@@ -136,7 +137,7 @@ int validate_views(const apg_image_view_t* l, const apg_image_view_t* r, std::st
 size_t estimate_bytes(const apg_pipeline_config_t& cfg, int w, int h, int ch) {
     if (w <= 0 || h <= 0) return 0;
     const size_t n = (size_t)w * h;
-    return apgcu::Engine::make_layout(cfg, w, h, ch, 0).total + 2 * n * ch + n * 10;
+    return apgcu::Engine::workspace_bytes(cfg, w, h, ch, 0) + 2 * n * ch + n * 10;
 }
 
 }  // namespace
@@ -258,6 +259,7 @@ int apg_session_process(apg_session_t s, const apg_image_view_t* left, const apg
         rc = s->eng->process_host(lp, rp, w, h, stride, ch, result->disparity, result->confidence,
                                   result->invalid_reason, result->reliable_mask, result->pinned);
         if (rc == APG_STATUS_OK) rc = s->eng->frame_counts(s->counts);
+        if (rc == APG_STATUS_OK) rc = s->eng->hier_telemetry(s->hier);
         if (rc != APG_STATUS_OK) {
             s->last_error = s->eng->last_error();
             result->clear();
@@ -374,6 +376,12 @@ APGCU_API int apgcu_session_get_stats(apg_session_t s, double* stage_ms11, size_
         counters4[2] = s->peak_bytes;
         counters4[3] = s->eng ? s->eng->allocated_bytes() : 0;
     }
+    return APG_STATUS_OK;
+}
+
+APGCU_API int apgcu_session_hier_telemetry(apg_session_t s, double* out6) {
+    if (!s || !out6) return APG_STATUS_INTERNAL_ERROR;
+    std::memcpy(out6, s->hier, sizeof(s->hier));
     return APG_STATUS_OK;
 }
 

@@ -30,19 +30,25 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 WORKLOADS = {
-    # name: (mode, PairSpec args, label)
-    "fast720": (0, (1280, 720, 128, 12, 0, 120, 0.0), "fast_1280x720_d128"),
-    "balanced640": (1, (640, 480, 64, 8, 4, 60, 0.0), "balanced_640x480_d64"),
-    "balanced720": (1, (1280, 720, 128, 12, 0, 120, 0.0), "balanced_1280x720_d128"),
-    "hq1080": (2, (1920, 1080, 256, 16, 0, 240, 0.2), "highquality_1920x1080_d256"),
-    "balanced1080": (1, (1920, 1080, 256, 16, 0, 240, 0.0), "balanced_1920x1080_d256"),
-    "kitti1242": (1, (1242, 375, 192, 12, 0, 180, 0.0), "balanced_1242x375_d192"),
+    # name: (mode, PairSpec args, label, configuration overrides)
+    "fast720": (0, (1280, 720, 128, 12, 0, 120, 0.0), "fast_1280x720_d128", {}),
+    "balanced640": (1, (640, 480, 64, 8, 4, 60, 0.0), "balanced_640x480_d64", {}),
+    "balanced720": (1, (1280, 720, 128, 12, 0, 120, 0.0), "balanced_1280x720_d128", {}),
+    "hq1080": (2, (1920, 1080, 256, 16, 0, 240, 0.2), "highquality_1920x1080_d256", {}),
+    "balanced1080": (1, (1920, 1080, 256, 16, 0, 240, 0.0), "balanced_1920x1080_d256", {}),
+    "kitti1242": (1, (1242, 375, 192, 12, 0, 180, 0.0), "balanced_1242x375_d192", {}),
+    # hierarchical coarse-to-fine search range (HierarchicalConfig defaults: R = 4, NearestValid)
+    "balanced720_hier": (1, (1280, 720, 128, 12, 0, 120, 0.0), "balanced_1280x720_d128_hierarchical",
+                         {"hier_enable": 1}),
+    "hq1080_hier": (2, (1920, 1080, 256, 16, 0, 240, 0.2), "highquality_1920x1080_d256_hierarchical",
+                    {"hier_enable": 1}),
 }
 MODE_NAMES = {0: "Fast", 1: "Balanced", 2: "HighQuality"}
 
 
-def metric_name(mode: int, w: int, h: int, D: int) -> str:
-    return f"W*H*D/s at {w}x{h} D={D} ({MODE_NAMES[mode]}, bit-exact)"
+def metric_name(mode: int, w: int, h: int, D: int, over=None) -> str:
+    kind = f"{MODE_NAMES[mode]}, hierarchical" if (over or {}).get("hier_enable") else MODE_NAMES[mode]
+    return f"W*H*D/s at {w}x{h} D={D} ({kind}, bit-exact)"
 
 
 def _peaks():
@@ -147,13 +153,13 @@ def run_reference(args, wl):
     """The reference CPU path (oracle/_ref) on the host cores, rank 0 only."""
     from oracle import oracle as O
     from apg_sgm_b200 import synthetic as S
-    mode, spec, label = wl
+    mode, spec, label, over = wl
     spec = S.PairSpec(*spec)
     L, R, _ = S.make_pair(spec, S.SEED_BASE)
     if not O.ref_available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libapg_ref.so not built"}))
         return
-    cfg = O.config(mode, spec.max_disparity, volume_backend=2)  # Packed: the AVX2/OpenMP path
+    cfg = O.config(mode, spec.max_disparity, volume_backend=2, **over)  # Packed: the AVX2/OpenMP path
     sess = O.RefSession(cfg, bounded_reuse=True)
     for _ in range(args.warmup):
         sess.process(L, R)
@@ -168,7 +174,8 @@ def run_reference(args, wl):
     value = vox * args.steps / total
     cores = O.ref_threads()
     print(json.dumps({
-        "impl": "reference", "metric": metric_name(mode, spec.width, spec.height, spec.max_disparity), "value": value, "unit": "voxels/s", "n_gpus": args.gpus,
+        "impl": "reference", "metric": metric_name(mode, spec.width, spec.height, spec.max_disparity, over),
+        "value": value, "unit": "voxels/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": "synthetic",
         "config": {"workload": label, "mode": MODE_NAMES[mode], "width": spec.width, "height": spec.height,
@@ -389,12 +396,13 @@ def run_reference_batched(args):
     }))
 
 
-def cpu_baseline(spec, mode, L, R, gpu_out):
+def cpu_baseline(spec, mode, L, R, gpu_out, over=None):
     """Time the reference (Packed, all host cores) on pair 0 and check the GPU output against it."""
     from oracle import oracle as O
+    over = over or {}
     vox = spec.width * spec.height * spec.max_disparity
     if O.ref_available():
-        cfg = O.config(mode, spec.max_disparity, volume_backend=2)
+        cfg = O.config(mode, spec.max_disparity, volume_backend=2, **over)
         sess = O.RefSession(cfg, bounded_reuse=True)
         for _ in range(2):
             ref = sess.process(L, R)
@@ -404,12 +412,14 @@ def cpu_baseline(spec, mode, L, R, gpu_out):
             ref = sess.process(L, R)
             ts.append(time.perf_counter() - t0)
         med = statistics.median(ts)
-        cfg_d = O.config(mode, spec.max_disparity, volume_backend=1)  # Auto==Dense for Fast/Balanced
-        sd = O.RefSession(cfg_d, bounded_reuse=True)
-        sd.process(L, R)
-        t0 = time.perf_counter()
-        sd.process(L, R)
-        dense_s = time.perf_counter() - t0
+        dense_s = float("nan")
+        if not over.get("hier_enable"):  # hierarchical mode rejects the Dense backend
+            cfg_d = O.config(mode, spec.max_disparity, volume_backend=1)  # Auto==Dense for Fast/Balanced
+            sd = O.RefSession(cfg_d, bounded_reuse=True)
+            sd.process(L, R)
+            t0 = time.perf_counter()
+            sd.process(L, R)
+            dense_s = time.perf_counter() - t0
         parity = all(np.array_equal(np.ascontiguousarray(gpu_out[k]).view(np.uint8),
                                     np.ascontiguousarray(ref[k]).view(np.uint8))
                      for k in ("disparity", "confidence", "invalid_reason", "reliable_mask"))
@@ -418,7 +428,7 @@ def cpu_baseline(spec, mode, L, R, gpu_out):
                           f"reference Packed backend, 2 warm-up + median of 5",
                 "ms_per_pair": med * 1000, "dense_backend_ms_per_pair": dense_s * 1000,
                 "stage_ms": ref["stage_ms"]}, parity
-    cfg = O.config(mode, spec.max_disparity)
+    cfg = O.config(mode, spec.max_disparity, **over)
     t0 = time.perf_counter()
     o = O.pipeline(cfg, L, R)
     dt = time.perf_counter() - t0
@@ -446,14 +456,14 @@ def run_b200(args, wl):
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
 
-    mode, spec_args, label = wl
+    mode, spec_args, label, over = wl
     spec = S.PairSpec(*spec_args)
     w, h, D = spec.width, spec.height, spec.max_disparity
     Dp = (D + 63) // 64 * 64
     npairs = 2
     # host images in page-locked memory: the end-to-end leg uploads them from there every step
     pairs = [tuple(_pinned(a) for a in S.make_pair(spec, S.SEED_BASE + rank * npairs + i)[:2]) for i in range(npairs)]
-    cfg = apg.config_from_mode(mode, D)
+    cfg = apg.config_from_mode(mode, D, **over)
     eng = apg.Engine(cfg, device=local)
     es = torch.cuda.ExternalStream(eng.stream, device=dev)
     d_in = [(torch.from_numpy(l).to(dev), torch.from_numpy(r).to(dev)) for l, r in pairs]
@@ -519,7 +529,11 @@ def run_b200(args, wl):
     opts = _lib.SessionOptions()
     opts.struct_size = C.sizeof(opts)
     opts.quality_mode, opts.memory_policy, opts.max_disparity, opts.backend = mode, 1, D, 3
-    sess_c = lib.apg_session_create_ex(C.byref(opts))
+    if over:
+        # options the reference's C API does not carry: the full-configuration session
+        sess_c = lib.apgcu_session_create_config(C.byref(cfg), 1, 0)
+    else:
+        sess_c = lib.apg_session_create_ex(C.byref(opts))
     res_c = lib.apg_result_create()
     views = [(_lib.ImageView(l.ctypes.data, w, h, w, 1), _lib.ImageView(r.ctypes.data, w, h, w, 1)) for l, r in pairs]
     rw, rh = C.c_int(), C.c_int()
@@ -548,7 +562,7 @@ def run_b200(args, wl):
 
     # the same through the Python binding (StereoSession.process returns fresh numpy arrays)
     sess = apg.StereoSession(mode=MODE_NAMES[mode].lower() if mode != 2 else "high_quality", max_disparity=D,
-                             memory_policy="bounded_reuse")
+                             memory_policy="bounded_reuse", hierarchical=bool(over.get("hier_enable")))
     for i in range(max(args.warmup, 3)):
         sess.process(*pairs[i % npairs])
     npy = max(3, min(args.steps, 50))
@@ -582,14 +596,15 @@ def run_b200(args, wl):
                             "the HBM fraction of its 2 B/voxel output is shown for reference")
 
     out = {
-        "metric": metric_name(mode, w, h, D), "value": value, "unit": "voxels/s", "n_gpus": world, "steps": args.steps,
+        "metric": metric_name(mode, w, h, D, over), "value": value, "unit": "voxels/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u16", "data": "synthetic",
         "config": {"workload": label, "mode": MODE_NAMES[mode], "width": w, "height": h, "max_disparity": D,
                    "pairs_per_step": 1, "distinct_pairs": npairs, "l2": "flushed between steps (256 MiB write)",
                    "parallelism": f"replicas x{world}"},
         "e2e": {"value": e2e_value, "unit": "voxels/s", "h2d_bytes_per_step": 2 * w * h,
-                "d2h_bytes_per_step": w * h * 10 + 64, "api": "apg_session_process (C API, BoundedReuse)",
+                "d2h_bytes_per_step": w * h * 10 + 64, "api": "apg_session_process (C API, BoundedReuse)" + (
+                    "; session from apgcu_session_create_config" if over else ""),
                 "python_binding_value": py_value},
         "gpu_launches": launches,
         "roofline": roofline,
@@ -597,7 +612,7 @@ def run_b200(args, wl):
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         gpu0 = eng.process(*pairs[0])
-        cb, parity = cpu_baseline(spec, mode, pairs[0][0], pairs[0][1], gpu0)
+        cb, parity = cpu_baseline(spec, mode, pairs[0][0], pairs[0][1], gpu0, over)
         out["cpu_baseline"] = cb
         out["parity_vs_cpu_baseline"] = "bit-exact" if parity else "MISMATCH"
     if rank == 0:

@@ -4,8 +4,8 @@
  * Every numeric knob of PipelineConfig that the dense-matching path reads is a field here,
  * with the same meaning and units.  apg_config_from_mode() restates
  * PipelineConfig::from_mode (src/config.cpp:5-45) and the member defaults of
- * include/apg_sgm/config.hpp:7-66.  The hierarchical coarse-to-fine mode is not represented:
- * it is an opt-in experiment that no quality preset enables.
+ * include/apg_sgm/config.hpp:7-84, including HierarchicalConfig (the opt-in coarse-to-fine
+ * search range of src/hierarchical_stereo.cpp, which no quality preset enables).
  *
  * It is the configuration record of the CUDA library's extended C-ABI (include/apg_sgm_cuda.h)
  * and is also read by the CPU oracle and the reference shim under oracle/.
@@ -27,6 +27,11 @@ extern "C" {
 /* Census flavours (include/apg_sgm/types.hpp:24-27). */
 #define APG_CENSUS_9X7 0           /* 62-bit plain census, uint64 descriptors */
 #define APG_CENSUS_SYMMETRIC_9X7 1 /* 31-bit symmetric census, uint32 descriptors */
+
+/* HierarchicalFallback (include/apg_sgm/config.hpp:68-72). */
+#define APG_HIER_FALLBACK_NEAREST_VALID 0
+#define APG_HIER_FALLBACK_FULL_RANGE 1
+#define APG_HIER_FALLBACK_EXPANDED_RADIUS 2
 
 typedef struct {
     int mode;          /* APG_MODE_* (informational once the fields below are set) */
@@ -67,6 +72,12 @@ typedef struct {
 
     /* PostParams (config.hpp:60-66) */
     int subpixel, lr_check, post_lr_max_diff, median_radius, max_fill_gap;
+
+    /* HierarchicalConfig (config.hpp:74-84); hier_fallback is APG_HIER_FALLBACK_* */
+    int hier_enable, hier_radius, hier_scale, hier_fallback;
+    int hier_coarse_cross_agg, hier_coarse_fill_holes, hier_adaptive_radius;
+    float hier_confidence_threshold;
+    int hier_expanded_radius;
 } apg_pipeline_config_t;
 
 /* PipelineConfig::from_mode(mode, max_disparity) with min_disparity 0 (src/config.cpp:5-45). */
@@ -91,6 +102,9 @@ static inline apg_pipeline_config_t apg_config_from_mode(int mode, int max_dispa
     c.conf_min_texture = 2.f; c.conf_reliable_threshold = 0.25f;
     c.refine_enable = 0; c.refine_iterations = 3; c.refine_random_radius = 4;
     c.subpixel = 1; c.lr_check = 1; c.post_lr_max_diff = 1; c.median_radius = 1; c.max_fill_gap = 32;
+    c.hier_enable = 0; c.hier_radius = 4; c.hier_scale = 2; c.hier_fallback = APG_HIER_FALLBACK_NEAREST_VALID;
+    c.hier_coarse_cross_agg = 1; c.hier_coarse_fill_holes = 1; c.hier_adaptive_radius = 0;
+    c.hier_confidence_threshold = 0.5f; c.hier_expanded_radius = 8;
     if (mode == APG_MODE_FAST) {
         c.use_ad = 0; c.use_grad = 0; c.agg_enable = 0; c.paths = 4; c.adaptive_penalties = 0;
         c.prior_enable = 0; c.refine_enable = 0; c.subpixel = 1; c.lr_check = 1;

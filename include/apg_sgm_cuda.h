@@ -99,6 +99,12 @@ APGCU_API void apgcu_engine_release(apgcu_engine_t e);
 /* Stream the engine enqueues on (a cudaStream_t). */
 APGCU_API void* apgcu_engine_stream(apgcu_engine_t e);
 
+/* HierarchicalTelemetry of the engine's last pair (src/hierarchical_stereo.hpp:36-42), computed
+ * from device counters: out6 = {avg_states_per_pixel, coarse_valid_ratio, fallback_pixel_ratio,
+ * full_range_pixel_ratio, coarse pass device time in ms, 1 if the coarse pass ran (0 for frames
+ * under 32 x 32 or with hierarchical mode off)}.  Waits for the engine stream. */
+APGCU_API int apgcu_engine_hier_telemetry(apgcu_engine_t e, double* out6);
+
 /* PipelineConfig::from_mode (src/config.cpp:5-45) into *out. */
 APGCU_API void apgcu_config_from_mode(int mode, int max_disparity, apg_pipeline_config_t* out);
 
@@ -114,6 +120,8 @@ APGCU_API int apgcu_session_get_stats(apg_session_t s, double* stage_ms11, size_
  * counts8 = {valid_pixels, reliable_pixels, unreliable_pixels, refine_changed_pixels, lr_fail_pixels,
  * prior_support_count, sum of search-range widths, sum of geometric range widths}. */
 APGCU_API int apgcu_session_get_frame_counts(apg_session_t s, unsigned long long* counts8);
+/* HierarchicalTelemetry of the session's last frame, as apgcu_engine_hier_telemetry. */
+APGCU_API int apgcu_session_hier_telemetry(apg_session_t s, double* out6);
 /* Workspace bytes the budget gate compares against max_retained_bytes for a W x H x C frame. */
 APGCU_API size_t apgcu_session_estimate_bytes(apg_session_t s, int width, int height, int channels);
 

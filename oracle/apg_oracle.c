@@ -978,11 +978,145 @@ static int validate(const apg_pipeline_config_t* c, const uint8_t* l, const uint
     return 0;
 }
 
+/* The coarse configuration of HierarchicalStereo::estimate_search_range,
+ * src/hierarchical_stereo.cpp:172-182: half the disparity bounds, no prior, no refine,
+ * aggregation as coarse_cross_agg, sub-pixel and LR on, median radius 1, fill gap 16 or none. */
+void orc_hier_coarse_config(const apg_pipeline_config_t* cfg, apg_pipeline_config_t* c) {
+    *c = *cfg;
+    c->min_disparity = imax(0, cfg->min_disparity / 2);
+    c->max_disparity = imax(c->min_disparity + 1, (cfg->max_disparity + 1) / 2);
+    c->prior_enable = 0;
+    c->refine_enable = 0;
+    c->agg_enable = cfg->hier_coarse_cross_agg;
+    c->volume_backend = 2;
+    c->subpixel = 1;
+    c->lr_check = 1;
+    c->median_radius = 1;
+    c->max_fill_gap = cfg->hier_coarse_fill_holes ? 16 : 0;
+    c->hier_enable = 0;
+}
+
+static int pipeline_run(const apg_pipeline_config_t* cfg, const uint8_t* left, const uint8_t* right,
+                        int w, int h, int stride, int ch, float* disparity, float* confidence,
+                        uint8_t* invalid_reason, uint8_t* reliable_mask, orc_stages_t* st, int skip_fill);
+
+/* HierarchicalStereo::estimate_search_range, src/hierarchical_stereo.cpp:113-431: a half-size
+ * pass of the whole pipeline (2x2 box-averaged grays, (sum + 2) / 4) and, per full-size pixel,
+ * a range around twice the coarse disparities of its 2x2 coarse neighbourhood, with the
+ * confidence-adaptive radius and the NearestValid / ExpandedRadius / FullRange fallbacks.
+ * d_prior receives the guiding disparity (-1 where none).  counts4 (nullable) receives
+ * {coarse pixels with a valid disparity, fallback pixels, full-range pixels, sum of widths}
+ * (HierarchicalTelemetry's numerators, src/hierarchical_stereo.cpp:413-420).
+ * Returns 0 for frames under 32 pixels in either dimension (default ranges), 1 otherwise. */
+int orc_hier_range(const apg_pipeline_config_t* cfg, int W, int H, const uint8_t* lg, const uint8_t* rg,
+                   int16_t* rmin, int16_t* rmax, float* d_prior, int64_t* counts4,
+                   float* coarse_disp, float* coarse_conf) {
+    if (counts4) counts4[0] = counts4[1] = counts4[2] = counts4[3] = 0;
+    if (W < 32 || H < 32) {
+        orc_range_default(cfg, W, H, rmin, rmax);
+        for (size_t i = 0; i < (size_t)W * H; ++i) d_prior[i] = -1.f;
+        return 0;
+    }
+    const int Wc = W / 2, Hc = H / 2;
+    const size_t nc = (size_t)Wc * Hc;
+    uint8_t* cimg = (uint8_t*)malloc(nc * 2);
+    uint8_t *cl = cimg, *cr = cimg + nc;
+    for (int yc = 0; yc < Hc; ++yc) {
+        const int y0 = yc * 2, y1 = imin(y0 + 1, H - 1);
+        for (int xc = 0; xc < Wc; ++xc) {
+            const int x0 = xc * 2, x1 = imin(x0 + 1, W - 1);
+            const int sl = lg[y0 * W + x0] + lg[y0 * W + x1] + lg[y1 * W + x0] + lg[y1 * W + x1];
+            const int sr = rg[y0 * W + x0] + rg[y0 * W + x1] + rg[y1 * W + x0] + rg[y1 * W + x1];
+            cl[yc * Wc + xc] = (uint8_t)((sl + 2) / 4);
+            cr[yc * Wc + xc] = (uint8_t)((sr + 2) / 4);
+        }
+    }
+    apg_pipeline_config_t cc;
+    orc_hier_coarse_config(cfg, &cc);
+    float* cd = (float*)malloc(nc * 8);
+    float* cf = cd + nc;
+    uint8_t* cm = (uint8_t*)malloc(nc * 2);
+    pipeline_run(&cc, cl, cr, Wc, Hc, Wc, 1, cd, cf, cm, cm + nc, NULL, !cfg->hier_coarse_fill_holes);
+    if (coarse_disp) memcpy(coarse_disp, cd, nc * 4);
+    if (coarse_conf) memcpy(coarse_conf, cf, nc * 4);
+    int64_t nvalid = 0, nfall = 0, nfull = 0, wsum = 0;
+    for (size_t i = 0; i < nc; ++i) nvalid += cd[i] >= 0.f;
+    const int R = cfg->hier_radius;
+    for (int y = 0; y < H; ++y) {
+        for (int x = 0; x < W; ++x) {
+            const int i = y * W + x;
+            const int xc = imax(0, imin(x / 2, Wc - 1)), yc = imax(0, imin(y / 2, Hc - 1));
+            const int xc1 = imin(xc + 1, Wc - 1), yc1 = imin(yc + 1, Hc - 1);
+            const float q[4] = {cd[yc * Wc + xc], cd[yc * Wc + xc1], cd[yc1 * Wc + xc], cd[yc1 * Wc + xc1]};
+            float mn = 1e9f, mx = -1e9f;
+            int nv = 0;
+            for (int k = 0; k < 4; ++k)
+                if (q[k] >= 0.f) {
+                    mn = fminf_ref(mn, q[k]);
+                    mx = fmaxf_ref(mx, q[k]);
+                    ++nv;
+                }
+            const int glo = cfg->min_disparity, ghi = imin(cfg->max_disparity, x + 1);
+            d_prior[i] = -1.f;
+            int lo = glo, hi = ghi;
+            if (nv > 0) {
+                const float dc = q[0] >= 0.f ? q[0] : 0.5f * (mn + mx);
+                const float Dc = 2.0f * dc, Dmn = 2.0f * mn, Dmx = 2.0f * mx;
+                int er = R;
+                if (cfg->hier_adaptive_radius && cf[yc * Wc + xc] < cfg->hier_confidence_threshold)
+                    er = cfg->hier_expanded_radius;
+                lo = imin((int)floorf(Dc) - er, (int)floorf(Dmn) - 1);
+                hi = imax((int)ceilf(Dc) + er + 1, (int)ceilf(Dmx) + 2);
+                lo = imax(lo, glo);
+                hi = imin(hi, ghi);
+                if (hi < lo) hi = lo;
+                d_prior[i] = Dc;
+            } else {
+                ++nfall;
+                if (cfg->hier_fallback != APG_HIER_FALLBACK_FULL_RANGE) {
+                    const int K = 4;
+                    float near = -1.f;
+                    int best = 1000;
+                    for (int sy = imax(0, yc - K); sy <= imin(Hc - 1, yc + K); ++sy)
+                        for (int sx = imax(0, xc - K); sx <= imin(Wc - 1, xc + K); ++sx) {
+                            const float v = cd[sy * Wc + sx];
+                            const int d2 = (sx - xc) * (sx - xc) + (sy - yc) * (sy - yc);
+                            if (v >= 0.f && d2 < best) { best = d2; near = v; }
+                        }
+                    if (near >= 0.f) {
+                        const float Dn = 2.0f * near;
+                        const int re = cfg->hier_fallback == APG_HIER_FALLBACK_EXPANDED_RADIUS ? 2 * R : R + 8;
+                        lo = imax(glo, (int)floorf(Dn) - re);
+                        hi = imin(ghi, (int)ceilf(Dn) + re + 1);
+                        if (hi < lo) hi = lo;
+                        d_prior[i] = Dn;
+                    }
+                }
+            }
+            set_range(cfg, rmin, rmax, i, lo, hi);
+            wsum += hi - lo;  /* the full-range branches add ghi - glo unclamped, as the reference */
+            if (hi - lo == ghi - glo) ++nfull;
+        }
+    }
+    if (counts4) { counts4[0] = nvalid; counts4[1] = nfall; counts4[2] = nfull; counts4[3] = wsum; }
+    free(cimg); free(cd); free(cm);
+    return 1;
+}
+
 /* StereoMatcher::compute_impl, src/pipeline.cpp:435-719, Dense branch. */
 int orc_pipeline(const apg_pipeline_config_t* cfg, const uint8_t* left, const uint8_t* right,
                  int w, int h, int stride, int ch,
                  float* disparity, float* confidence, uint8_t* invalid_reason, uint8_t* reliable_mask,
                  orc_stages_t* st) {
+    return pipeline_run(cfg, left, right, w, h, stride, ch, disparity, confidence, invalid_reason,
+                        reliable_mask, st, 0);
+}
+
+/* skip_fill: the coarse pass of the hierarchical mode calls fill_holes only with a positive gap
+ * (src/hierarchical_stereo.cpp:262-265); a zero gap still fills from the direct neighbours. */
+static int pipeline_run(const apg_pipeline_config_t* cfg, const uint8_t* left, const uint8_t* right,
+                        int w, int h, int stride, int ch, float* disparity, float* confidence,
+                        uint8_t* invalid_reason, uint8_t* reliable_mask, orc_stages_t* st, int skip_fill) {
     const int v = validate(cfg, left, right, w, h, stride, ch);
     if (v) return v;
     const size_t n = (size_t)w * h;
@@ -1008,7 +1142,10 @@ int orc_pipeline(const apg_pipeline_config_t* cfg, const uint8_t* left, const ui
     orc_range_default(cfg, w, h, rmin, rmax);
     for (size_t i = 0; i < n; ++i) d_prior[i] = -1.f;
     int support_count = 0;
-    if (cfg->prior_enable) {
+    if (cfg->hier_enable) {
+        /* the hierarchical range replaces the prior (src/pipeline.cpp:483-499) */
+        orc_hier_range(cfg, w, h, lg, rg, rmin, rmax, d_prior, NULL, NULL, NULL);
+    } else if (cfg->prior_enable) {
         const int cap = cfg->prior_max_supports > 0 ? cfg->prior_max_supports : 1;
         orc_support_t* sup = (orc_support_t*)malloc(sizeof(orc_support_t) * cap);
         support_count = orc_extract_supports(cfg, w, h, lgx, lgy, cl, cr, cl64, cr64, sup, cap);
@@ -1065,7 +1202,10 @@ int orc_pipeline(const apg_pipeline_config_t* cfg, const uint8_t* left, const ui
     orc_lr_check(cfg, w, h, dr, disp, invalid_reason);
     if (st && st->disp_lr) memcpy(st->disp_lr, disp, n * 4);
     float* filled = (float*)malloc(n * 4);
-    orc_fill_holes(cfg, w, h, disp, invalid_reason, lg, d_prior, filled);
+    if (skip_fill)
+        memcpy(filled, disp, n * 4);
+    else
+        orc_fill_holes(cfg, w, h, disp, invalid_reason, lg, d_prior, filled);
     if (st && st->disp_fill) memcpy(st->disp_fill, filled, n * 4);
     orc_median(cfg, w, h, filled, disparity);
     free(filled); free(disp); free(best); free(second); free(dr); free(d_prior);

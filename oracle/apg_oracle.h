@@ -100,6 +100,14 @@ int orc_pipeline(const apg_pipeline_config_t* cfg, const uint8_t* left, const ui
                  float* disparity, float* confidence, uint8_t* invalid_reason, uint8_t* reliable_mask,
                  orc_stages_t* stages);
 
+/* Hierarchical coarse-to-fine search range (src/hierarchical_stereo.cpp:113-431).  lg / rg are
+ * the full-size grays; coarse_disp / coarse_conf (nullable, (W/2)*(H/2)) receive the coarse pass's
+ * final disparity and confidence.  Returns 0 for the small-frame fallback, 1 otherwise. */
+void orc_hier_coarse_config(const apg_pipeline_config_t* cfg, apg_pipeline_config_t* coarse);
+int  orc_hier_range(const apg_pipeline_config_t* cfg, int w, int h, const uint8_t* lg, const uint8_t* rg,
+                    int16_t* rmin, int16_t* rmax, float* d_prior, int64_t* counts4,
+                    float* coarse_disp, float* coarse_conf);
+
 uint64_t orc_fnv1a64(const uint8_t* data, uint64_t n);
 void orc_config_from_mode(int mode, int max_disparity, apg_pipeline_config_t* out);
 

@@ -41,6 +41,10 @@ class PipelineConfig(C.Structure):
         ("refine_enable", C.c_int), ("refine_iterations", C.c_int), ("refine_random_radius", C.c_int),
         ("subpixel", C.c_int), ("lr_check", C.c_int), ("post_lr_max_diff", C.c_int),
         ("median_radius", C.c_int), ("max_fill_gap", C.c_int),
+        ("hier_enable", C.c_int), ("hier_radius", C.c_int), ("hier_scale", C.c_int), ("hier_fallback", C.c_int),
+        ("hier_coarse_cross_agg", C.c_int), ("hier_coarse_fill_holes", C.c_int),
+        ("hier_adaptive_radius", C.c_int), ("hier_confidence_threshold", C.c_float),
+        ("hier_expanded_radius", C.c_int),
     ]
 
     def copy(self) -> "PipelineConfig":
@@ -74,6 +78,7 @@ def lib():
         _orc.orc_rng_create.argtypes = [C.c_uint32]
         _orc.orc_rng_destroy.argtypes = [C.c_void_p]
         _orc.orc_rng_draws.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p]
+        _orc.orc_hier_range.restype = C.c_int
     return _orc
 
 
@@ -104,6 +109,15 @@ def config(mode: int, max_disparity: int = 128, min_disparity: int = 0, **kw) ->
         if not hasattr(c, k):
             raise AttributeError(k)
         setattr(c, k, v)
+    return c
+
+
+def config_from_record(raw: bytes) -> PipelineConfig:
+    """A configuration saved as the raw bytes of apg_pipeline_config_t.  Records shorter than the
+    current struct (saved before the hierarchical fields were appended) keep the from_mode
+    defaults of the fields after them."""
+    c = config(BALANCED, 128)
+    C.memmove(C.addressof(c), raw, min(len(raw), C.sizeof(c)))
     return c
 
 
@@ -167,6 +181,35 @@ def pipeline(cfg: PipelineConfig, left, right, stages: bool = False) -> dict:
         out["support_count"] = st.support_count
     out["status"] = rc
     return out
+
+
+def hier_range(cfg: PipelineConfig, left, right) -> dict:
+    """Oracle hierarchical search range (orc_hier_range): range planes, d_prior, the coarse
+    pass's disparity and confidence, and the telemetry numerators."""
+    a = aux(left, right)
+    h, w = a["left"]["gray"].shape
+    wc, hc = w // 2, h // 2
+    out = {"range_min": np.empty((h, w), np.int16), "range_max": np.empty((h, w), np.int16),
+           "d_prior": np.empty((h, w), np.float32), "coarse_disparity": np.full((max(hc, 1), max(wc, 1)), -1, np.float32),
+           "coarse_confidence": np.zeros((max(hc, 1), max(wc, 1)), np.float32)}
+    cnt = np.zeros(4, np.int64)
+    ran = lib().orc_hier_range(C.byref(cfg), w, h, _p(a["left"]["gray"]), _p(a["right"]["gray"]),
+                               _p(out["range_min"]), _p(out["range_max"]), _p(out["d_prior"]), _p(cnt),
+                               _p(out["coarse_disparity"]), _p(out["coarse_confidence"]))
+    out["ran"] = int(ran)
+    out["coarse_valid"], out["fallback"], out["full_range"], out["width_sum"] = (int(v) for v in cnt)
+    n = w * h
+    out["telemetry"] = {"avg_states_per_pixel": out["width_sum"] / n if n else 0.0,
+                        "coarse_valid_ratio": float(np.float32(out["coarse_valid"] / (wc * hc))) if ran else 0.0,
+                        "fallback_pixel_ratio": float(np.float32(out["fallback"] / n)),
+                        "full_range_pixel_ratio": float(np.float32(out["full_range"] / n))}
+    return out
+
+
+def hier_coarse_config(cfg: PipelineConfig) -> PipelineConfig:
+    c = PipelineConfig()
+    lib().orc_hier_coarse_config(C.byref(cfg), C.byref(c))
+    return c
 
 
 def aux(left, right):
@@ -256,6 +299,26 @@ def ref_dump(cfg: PipelineConfig, left, right) -> dict:
     rc = ref_lib().ref_dump(C.byref(cfg), _p(L), _p(R), w, h, stride, ch, C.byref(d))
     out["status"] = rc
     out["support_count"] = d.support_count
+    return out
+
+
+def ref_hier_dump(cfg: PipelineConfig, left, right) -> dict:
+    """The reference's hierarchical search range (range planes, d_prior, telemetry) and the final
+    maps of its full pipeline with the same configuration (ref_hier_dump in ref_shim.cpp)."""
+    L, w, h, stride, ch = _view(left)
+    R, _, _, _, _ = _view(right)
+    out = {"range_min": np.zeros((h, w), np.int16), "range_max": np.zeros((h, w), np.int16),
+           "d_prior": np.zeros((h, w), np.float32),
+           "disparity": np.zeros((h, w), np.float32), "confidence": np.zeros((h, w), np.float32),
+           "invalid_reason": np.zeros((h, w), np.uint8), "reliable_mask": np.zeros((h, w), np.uint8)}
+    t = np.zeros(5, np.float64)
+    rc = ref_lib().ref_hier_dump(C.byref(cfg), _p(L), _p(R), w, h, stride, ch, _p(out["range_min"]),
+                                 _p(out["range_max"]), _p(out["d_prior"]), _p(t), _p(out["disparity"]),
+                                 _p(out["confidence"]), _p(out["invalid_reason"]), _p(out["reliable_mask"]))
+    out["status"] = rc
+    out["ran"] = int(t[4])
+    out["telemetry"] = dict(zip(["avg_states_per_pixel", "coarse_valid_ratio", "fallback_pixel_ratio",
+                                 "full_range_pixel_ratio"], t[:4].tolist()))
     return out
 
 

@@ -21,9 +21,11 @@
 #include "apg_sgm/refiner.hpp"
 #include "apg_sgm/session.hpp"
 #include "apg_sgm/sgm_optimizer.hpp"
+#include "hierarchical_stereo.hpp"
 
 #include "../include/apg_sgm/pipeline_config.h"
 
+#include <algorithm>
 #include <chrono>
 #include <cstring>
 #include <vector>
@@ -88,6 +90,18 @@ PipelineConfig to_ref(const apg_pipeline_config_t& c) {
     p.post.lr_max_diff = c.post_lr_max_diff;
     p.post.median_radius = c.median_radius;
     p.post.max_fill_gap = c.max_fill_gap;
+    p.hierarchical.enable = c.hier_enable != 0;
+    p.hierarchical.radius = c.hier_radius;
+    p.hierarchical.scale = c.hier_scale;
+    p.hierarchical.fallback = c.hier_fallback == APG_HIER_FALLBACK_FULL_RANGE ? HierarchicalFallback::FullRange
+                              : (c.hier_fallback == APG_HIER_FALLBACK_EXPANDED_RADIUS
+                                     ? HierarchicalFallback::ExpandedRadius
+                                     : HierarchicalFallback::NearestValid);
+    p.hierarchical.coarse_cross_agg = c.hier_coarse_cross_agg != 0;
+    p.hierarchical.coarse_fill_holes = c.hier_coarse_fill_holes != 0;
+    p.hierarchical.adaptive_radius = c.hier_adaptive_radius != 0;
+    p.hierarchical.confidence_threshold = c.hier_confidence_threshold;
+    p.hierarchical.expanded_radius = c.hier_expanded_radius;
     return p;
 }
 
@@ -256,6 +270,49 @@ void ref_winner_take_all(const apg_pipeline_config_t* ccfg, const uint32_t* vol,
     put(disp, d.data(), n);
     put(best, b.data(), n);
     put(second, s.data(), n);
+}
+
+// Hierarchical search range of one pair (HierarchicalStereo::estimate_search_range after
+// CostComputer::compute_aux, src/hierarchical_stereo.cpp:113-431) and the final maps of a full
+// StereoMatcher::compute with the same configuration (Packed backend).  telem5 (nullable):
+// avg_states_per_pixel, coarse_valid_ratio, fallback_pixel_ratio, full_range_pixel_ratio and 1 if
+// the coarse pass ran (0: the small-frame fallback).  d_prior is -1 where the reference leaves it
+// unset.  Returns 0, or the StatusCode of a rejected configuration or input.
+int ref_hier_dump(const apg_pipeline_config_t* ccfg, const uint8_t* left, const uint8_t* right, int w, int h,
+                  int stride, int ch, int16_t* rmin, int16_t* rmax, float* d_prior, double* telem5,
+                  float* disparity, float* confidence, uint8_t* invalid_reason, uint8_t* reliable_mask) {
+    PipelineConfig cfg = to_ref(*ccfg);
+    Status s = validate_config(cfg);
+    if (!s.ok()) return static_cast<int>(s.code);
+    const Image8 L = to_image(left, w, h, stride, ch);
+    const Image8 R = to_image(right, w, h, stride, ch);
+    const size_t n = static_cast<size_t>(w) * h;
+    PipelineBuffers b;
+    CostComputer().compute_aux(L, R, cfg, b);
+    HierarchicalTelemetry t;
+    const bool ran = HierarchicalStereo::estimate_search_range(cfg.hierarchical, cfg, b, &t, nullptr, cfg.num_threads);
+    put(rmin, b.range.dmin.data(), n);
+    put(rmax, b.range.dmax.data(), n);
+    if (d_prior) {
+        if (b.d_prior.empty()) std::fill(d_prior, d_prior + n, -1.f);
+        else put(d_prior, b.d_prior.data(), n);
+    }
+    if (telem5) {
+        const double v[5] = {t.avg_states_per_pixel, t.coarse_valid_ratio, t.fallback_pixel_ratio,
+                             t.full_range_pixel_ratio, ran ? 1.0 : 0.0};
+        std::memcpy(telem5, v, sizeof(v));
+    }
+    StereoMatcher matcher(cfg);
+    PipelineBuffers full;
+    if (!matcher.compute(L, R, full)) {
+        s = validate_inputs(L, R);
+        return s.ok() ? static_cast<int>(StatusCode::InternalError) : static_cast<int>(s.code);
+    }
+    put(disparity, full.disparity.data(), n);
+    put(confidence, full.confidence.data(), n);
+    put(invalid_reason, full.invalid_reason.data(), n);
+    put(reliable_mask, full.reliable_mask.data(), n);
+    return 0;
 }
 
 // Public-API session used for timing the reference CPU path.

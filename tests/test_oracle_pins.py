@@ -84,7 +84,7 @@ def _fixture_cases():
 @pytest.mark.parametrize("case", _fixture_cases())
 def test_oracle_matches_reference_fixtures(case, O):
     z = np.load(FIX)
-    cfg = O.PipelineConfig.from_buffer_copy(z[f"{case}/config"].tobytes())
+    cfg = O.config_from_record(z[f"{case}/config"].tobytes())
     L, R = z[f"{case}/left"], z[f"{case}/right"]
     out = O.pipeline(cfg, L, R, stages=True)
     assert out["status"] == 0
