@@ -502,11 +502,11 @@ class Engine:
         if rc != 0:
             raise RuntimeError(self.last_error)
 
-    @property
     def hier_telemetry(self) -> dict:
         """HierarchicalTelemetry of the last pair (apgcu_engine_hier_telemetry)."""
         return _hier_dict(lib().apgcu_engine_hier_telemetry, self._h)
 
+    @property
     def stream(self) -> int:
         return int(lib().apgcu_engine_stream(self._h) or 0)
 
