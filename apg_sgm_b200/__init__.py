@@ -572,13 +572,72 @@ def kernel_launch_count() -> int:
     return int(lib().apgcu_kernel_launch_count())
 
 
+StereoMetrics = _lib_mod.StereoMetricsRec
+RegionMetrics = _lib_mod.RegionMetricsRec
+
+
+def evaluate_stereo(est, gt, range=None, d_before_refine=None, d_after_refine=None, vis_mask=None,
+                    max_valid_gt: float = 1e5, left_image=None, thresholds=None, stream=None) -> StereoMetrics:
+    """evaluate_stereo (src/metrics.cpp:119-502; the support block is not part of it) on the GPU.
+
+    est, gt: HxW float32 disparity maps; range: (range_min, range_max) int16 planes; the refine
+    maps, vis_mask (uint8, >= 200 = visible) and left_image (HxW or HxWx3 uint8) are optional as in
+    the reference.  thresholds: (boundary_disparity_gradient, low_texture_gradient, max_valid_gt),
+    default QualityThresholds{}.  Either all arrays are numpy (host; copied in) or all are CUDA
+    tensors of the current device (evaluated in place on `stream`, default the current torch
+    stream).  Returns the record (attributes as StereoMetrics; .to_dict())."""
+    arrays = [est, gt, None if range is None else range[0], None if range is None else range[1], d_before_refine,
+              d_after_refine, vis_mask, left_image]
+    present = [a for a in arrays if a is not None]
+    on_device = all(hasattr(a, "is_cuda") and a.is_cuda for a in present)
+    if not on_device and any(hasattr(a, "is_cuda") and a.is_cuda for a in present):
+        raise ValueError("evaluate_stereo: pass all arrays on the host or all on the device")
+    want = [np.float32, np.float32, np.int16, np.int16, np.float32, np.float32, np.uint8, np.uint8]
+    keep, ptrs = [], []
+    h, w = (int(gt.shape[0]), int(gt.shape[1]))
+    for a, dt in zip(arrays, want):
+        if a is None:
+            ptrs.append(None)
+            continue
+        if on_device:
+            import torch
+            tdt = {np.float32: torch.float32, np.int16: torch.int16, np.uint8: torch.uint8}[dt]
+            if a.dtype != tdt:
+                raise TypeError(f"evaluate_stereo: expected {tdt}, got {a.dtype}")
+            a = a.contiguous()
+            keep.append(a)
+            ptrs.append(C.c_void_p(a.data_ptr()))
+        else:
+            a = np.ascontiguousarray(a, dt)
+            keep.append(a)
+            ptrs.append(a.ctypes.data_as(C.c_void_p))
+        if tuple(a.shape[:2]) != (h, w):
+            raise ValueError(f"evaluate_stereo: every map must be {h}x{w}")
+    lch = 0 if left_image is None else (1 if len(left_image.shape) == 2 else int(left_image.shape[2]))
+    thr = None
+    if thresholds is not None:
+        thr = _lib_mod.QualityThresholdsRec(*[float(v) for v in thresholds])
+    if on_device and stream is None:
+        import torch
+        stream = torch.cuda.current_stream().cuda_stream
+    out = StereoMetrics()
+    rc = lib().apgcu_evaluate_stereo(ptrs[0], ptrs[1], w, h, ptrs[2], ptrs[3], ptrs[4], ptrs[5], ptrs[6],
+                                     C.c_float(max_valid_gt), ptrs[7], w * lch, lch,
+                                     C.byref(thr) if thr is not None else None, 1 if on_device else 0,
+                                     C.c_void_p(stream) if stream else None, C.byref(out))
+    if rc != 0:
+        raise RuntimeError(f"evaluate_stereo failed [{rc}]")
+    return out
+
+
 def workspace_bytes(config: PipelineConfig, width: int, height: int) -> int:
     return int(lib().apgcu_workspace_bytes(C.byref(config), int(width), int(height)))
 
 
 __all__ = ["QualityMode", "HierarchicalFallback", "VolumeBackend", "MemoryPolicy", "StatusCode", "InvalidReason", "StageTiming",
            "PipelineStats", "StereoResult", "StereoSession", "PipelineConfig", "config_from_mode", "Engine",
-           "kernel_launch_count", "workspace_bytes", "__version__"]
+           "kernel_launch_count", "workspace_bytes", "evaluate_stereo", "StereoMetrics", "RegionMetrics",
+           "__version__"]
 
 
 

@@ -49,6 +49,49 @@ class PipelineConfig(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+_REGION_FIELDS = ["total_pixels", "valid_est_pixels", "valid_ratio", "epe", "bad_0_5", "bad_1_0", "bad_2_0",
+                  "bad_3_0", "d1"]
+
+
+class RegionMetricsRec(C.Structure):
+    """apg_region_metrics_t (include/apg_sgm/metrics.h): RegionMetrics."""
+    _fields_ = [(k, C.c_int if k in ("total_pixels", "valid_est_pixels") else C.c_float) for k in _REGION_FIELDS]
+
+
+class QualityThresholdsRec(C.Structure):
+    """apg_quality_thresholds_t (include/apg_sgm/metrics.h): QualityThresholds."""
+    _fields_ = [("boundary_disparity_gradient", C.c_float), ("low_texture_gradient", C.c_float),
+                ("max_valid_gt", C.c_float)]
+
+
+_I, _F, _U = C.c_int, C.c_float, C.c_ulonglong
+_STEREO_FIELDS = (
+    [("total_pixels", _I), ("evaluated_pixels", _I), ("valid_pixels", _I), ("valid_ratio", _F), ("epe", _F),
+     ("bad_0_5", _F), ("bad_1_0", _F), ("bad_2_0", _F), ("bad_3_0", _F), ("kitti_d1_all", _F), ("kitti_d1_noc", _F),
+     ("edge_pixels", _I), ("edge_epe", _F), ("nonedge_pixels", _I), ("nonedge_epe", _F), ("lr_fail_ratio", _F),
+     ("has_range", _I), ("range_recall_all", _F), ("range_recall_matchable", _F), ("range_recall_visible", _F),
+     ("range_visible_eval_pixels", _U), ("range_visible_in_pixels", _U), ("range_matchable_eval_pixels", _U),
+     ("range_matchable_in_pixels", _U), ("prior_miss_visible_count", _I), ("prior_miss_edge", _I),
+     ("prior_miss_nonedge", _I), ("prior_miss_edge_ratio", _F), ("prior_miss_nonedge_ratio", _F)]
+    + [(r, RegionMetricsRec) for r in ("reg_all", "reg_noc", "reg_occ", "reg_boundary", "reg_non_boundary",
+                                       "reg_low_texture", "reg_high_texture")]
+    + [("has_refine_stats", _I), ("refine_eval_pixels", _I), ("refine_epe_delta", _F), ("post_epe_delta", _F),
+       ("total_epe_delta", _F), ("refine_improved_ratio", _F), ("refine_worsened_ratio", _F),
+       ("refine_unchanged_ratio", _F), ("refine_changed_ratio", _F)])
+
+
+class StereoMetricsRec(C.Structure):
+    """apg_stereo_metrics_t (include/apg_sgm/metrics.h): StereoMetrics without the support block."""
+    _fields_ = _STEREO_FIELDS
+
+    def to_dict(self) -> dict:
+        d = {}
+        for k, t in self._fields_:
+            v = getattr(self, k)
+            d[k] = {r: getattr(v, r) for r in _REGION_FIELDS} if t is RegionMetricsRec else v
+        return d
+
+
 class ImageView(C.Structure):
     """apg_image_view_t (include/apg_sgm/c_api.h)."""
     _fields_ = [("data", C.c_void_p), ("width", C.c_int), ("height", C.c_int),
@@ -124,6 +167,10 @@ _SIGS = {
     "apgcu_session_hier_telemetry": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     "apgcu_engine_hier_telemetry": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     "apgcu_kernel_launch_count": (C.c_ulonglong, []),
+    "apgcu_evaluate_stereo": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                        C.c_void_p, C.c_void_p, C.c_float, C.c_void_p, C.c_int, C.c_int,
+                                        C.POINTER(QualityThresholdsRec), C.c_int, C.c_void_p,
+                                        C.POINTER(StereoMetricsRec)]),
     "apgcu_engine_launch_profile": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_char_p), C.POINTER(C.c_float)]),
     "apgcu_batch_create": (C.c_void_p, [C.POINTER(PipelineConfig), C.c_int]),
     "apgcu_batch_destroy": (None, [C.c_void_p]),

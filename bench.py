@@ -792,13 +792,157 @@ def run_batched(args):
         dist.destroy_process_group()
 
 
+METRICS_SPEC = (1920, 1080, 256, 16, 0, 240, 0.2)
+METRICS_BYTES_PER_PIXEL = 22  # est 4 + gt 4 + ranges 2+2 + refine maps 4+4 + visibility 1 + left image 1
+
+
+def _metrics_inputs(seed: int):
+    """A 1920x1080 evaluation frame: synthetic ground truth (on a 1/256 grid), an estimate with
+    sub-pixel noise, gross errors and invalid pixels, refine maps, per-pixel ranges, the
+    matchability mask as visibility and the left image."""
+    from apg_sgm_b200 import synthetic as S
+    spec = S.PairSpec(*METRICS_SPEC)
+    L, _, gt = S.make_pair(spec, seed)
+    rng = np.random.default_rng(seed)
+    h, w = gt.shape
+    gt = (np.round(gt.astype(np.float64) * 256) / 256).astype(np.float32)
+    noise = (np.round(rng.normal(0, 0.7, (h, w)) * 65536) / 65536).astype(np.float32)
+    gross = rng.random((h, w)) < 0.05
+    noise[gross] += rng.integers(-20, 20, gross.sum()).astype(np.float32)
+    est = (gt + noise).astype(np.float32)
+    est[rng.random((h, w)) < 0.06] = -1.0
+    before = (gt + 1.5 * noise).astype(np.float32)
+    after = (gt + 1.1 * noise).astype(np.float32)
+    r = rng.integers(2, 12, (h, w))
+    rmin = (np.floor(gt) - r).astype(np.int16)
+    rmax = (np.floor(gt) + r).astype(np.int16)
+    vis = np.where(np.arange(w)[None, :] - np.round(gt) >= 0, 255, 0).astype(np.uint8)
+    return {"est": est, "gt": gt, "rmin": rmin, "rmax": rmax, "before": before, "after": after, "vis": vis,
+            "left": L}
+
+
+def _metrics_call(fn, d):
+    return fn(d["est"], d["gt"], (d["rmin"], d["rmax"]), d["before"], d["after"], d["vis"], 1e5, d["left"])
+
+
+def run_metrics(args):
+    """evaluate_stereo (src/metrics.cpp:119-502) over one 1920x1080 frame with every optional input.
+    value: pixels/s with the inputs resident in HBM (L2 flushed between steps); e2e: the same call
+    on page-locked host arrays (copies inside)."""
+    import torch
+    import apg_sgm_b200 as apg
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    host = {k: _pinned(v) for k, v in _metrics_inputs(11).items()}
+    h, w = host["gt"].shape
+    n = w * h
+    d = {k: torch.from_numpy(v).to(dev) for k, v in host.items()}
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    s = torch.cuda.Stream(device=dev)
+    call = lambda arrs: _metrics_call(lambda *a: apg.evaluate_stereo(*a, stream=s.cuda_stream), arrs)  # noqa: E731
+    torch.cuda.synchronize()
+    for _ in range(max(args.warmup, 3)):
+        call(d)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    sampler = ClockSampler(local)
+    sampler.start()
+    sampler.wait_first()
+    launches0 = apg.kernel_launch_count()
+    with torch.cuda.stream(s):
+        for k in range(args.steps):
+            flush.zero_()
+            starts[k].record(s)
+            m = call(d)
+            ends[k].record(s)
+    torch.cuda.synchronize()
+    launches = apg.kernel_launch_count() - launches0
+    clocks = sampler.stop()
+    times = [a.elapsed_time(b) for a, b in zip(starts, ends)]
+    dev_ms = sum(times)
+    value = n * args.steps / (dev_ms / 1000.0)
+    # e2e: host arrays, copies inside the call
+    for _ in range(3):
+        _metrics_call(apg.evaluate_stereo, host)
+    t0 = time.perf_counter()
+    ne = max(3, min(args.steps, 50))
+    for _ in range(ne):
+        _metrics_call(apg.evaluate_stereo, host)
+    e2e_s = (time.perf_counter() - t0) / ne
+    peak, peak_kind = _peaks()
+    alg = METRICS_BYTES_PER_PIXEL * n
+    med_ms = statistics.median(times)
+    achieved = alg / (med_ms / 1000.0) / 1e9
+    out = {
+        "metric": f"evaluate_stereo pixels/s at {w}x{h} (every optional input)", "value": value, "unit": "pixels/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "metrics_1920x1080", "width": w, "height": h,
+                   "inputs": "est, gt, ranges, refine before/after, visibility, left image",
+                   "l2": "flushed between steps (256 MiB write)"},
+        "e2e": {"value": n / e2e_s, "unit": "pixels/s", "h2d_bytes_per_step": alg,
+                "d2h_bytes_per_step": (76 + 15) * 8, "api": "apgcu_evaluate_stereo, page-locked host arrays"},
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "kernel": "metrics_kernel (+ final reduce, tally copy)", "achieved": achieved,
+                     "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+                     "traffic": None, "algorithmic_bytes_per_launch": alg, "avg_launch_ms": med_ms,
+                     "note": "timed per call (two kernels and the 728-byte tally copy)"},
+        "clocks": clocks,
+    }
+    if not args.no_cpu_baseline:
+        from oracle import oracle as O
+        if O.ref_available():
+            ref = lambda *a: O.evaluate_stereo(*a, reference=True)  # noqa: E731
+            want = _metrics_call(ref, host)
+            ts = []
+            for _ in range(5):
+                t0 = time.perf_counter()
+                _metrics_call(ref, host)
+                ts.append(time.perf_counter() - t0)
+            med = statistics.median(ts)
+            same = all(getattr(m, k) == getattr(want, k) for k, _ in m._fields_ if not k.startswith("reg_"))
+            out["cpu_baseline"] = {"value": n / med, "unit": "pixels/s", "cores": 1, "kind": "reference",
+                                   "sample": f"one {w}x{h} frame through the reference's evaluate_stereo, median of 5",
+                                   "ms_per_frame": med * 1000}
+            out["parity_vs_cpu_baseline"] = "identical record" if same else "MISMATCH"
+    print(json.dumps(out))
+
+
+def run_reference_metrics(args):
+    """The reference's evaluate_stereo on the host for the metrics workload."""
+    from oracle import oracle as O
+    if not O.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libapg_ref.so not built"}))
+        return
+    host = _metrics_inputs(11)
+    h, w = host["gt"].shape
+    ref = lambda *a: O.evaluate_stereo(*a, reference=True)  # noqa: E731
+    for _ in range(args.warmup):
+        _metrics_call(ref, host)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        _metrics_call(ref, host)
+    total = time.perf_counter() - t0
+    value = w * h * args.steps / total
+    print(json.dumps({
+        "impl": "reference", "metric": f"evaluate_stereo pixels/s at {w}x{h} (every optional input)", "value": value,
+        "unit": "pixels/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000 * total / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic", "config": {"workload": "metrics_1920x1080", "width": w, "height": h},
+        "cpu_baseline": {"value": value, "unit": "pixels/s", "cores": 1, "kind": "reference",
+                         "sample": f"{args.steps} frames through the reference's evaluate_stereo (single-threaded)"},
+        "e2e": {"value": value, "unit": "pixels/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batched", "served"], default="fast720")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batched", "served", "metrics1080"], default="fast720")
     ap.add_argument("--requests", type=int, default=10000, help="served: total requests over the rates")
     ap.add_argument("--rates", default="50,100,200,400,600", help="served: Poisson arrival rates, pairs/s")
     ap.add_argument("--slots", type=int, default=4, help="served: requests in flight")
@@ -812,6 +956,10 @@ def main():
             return
         if int(os.environ.get("RANK", "0")) == 0:
             run_served(args)
+        return
+    if args.workload == "metrics1080":
+        if int(os.environ.get("RANK", "0")) == 0:
+            (run_reference_metrics if args.impl == "reference" else run_metrics)(args)
         return
     if args.workload == "batched":
         if args.impl == "reference":

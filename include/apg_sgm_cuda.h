@@ -15,6 +15,7 @@
 #include <stdint.h>
 
 #include "apg_sgm/c_api.h"
+#include "apg_sgm/metrics.h"
 #include "apg_sgm/pipeline_config.h"
 
 #if defined(__GNUC__) && __GNUC__ >= 4
@@ -124,6 +125,23 @@ APGCU_API int apgcu_session_get_frame_counts(apg_session_t s, unsigned long long
 APGCU_API int apgcu_session_hier_telemetry(apg_session_t s, double* out6);
 /* Workspace bytes the budget gate compares against max_retained_bytes for a W x H x C frame. */
 APGCU_API size_t apgcu_session_estimate_bytes(apg_session_t s, int width, int height, int channels);
+
+/* ---- Accuracy metrics (evaluate_stereo, src/metrics.cpp:119-502; the support block is not part
+ * of it).  est / gt: W*H disparity maps; range_min / range_max (int16 W*H, half-open per-pixel
+ * intervals), d_before_refine / d_after_refine, vis_mask (W*H, >= 200 = visible) and left_image
+ * (left_stride bytes per row, 1 or 3 channels: the low-texture split) may each be NULL, as the
+ * reference's optional arguments.  thresholds NULL means QualityThresholds{}.  device_buffers != 0:
+ * every array is device memory on the current device and the call enqueues on `stream` (a
+ * cudaStream_t, NULL = the legacy default stream); otherwise they are host arrays copied in.
+ * Returns when *out is written: counts exact, ratios formed with the reference's float
+ * expressions, sums of errors in double (equal to the reference's whenever its sequential double
+ * sum is exact).  Scratch comes from the stream-ordered allocator. */
+APGCU_API int apgcu_evaluate_stereo(const float* est, const float* gt, int width, int height,
+                                    const int16_t* range_min, const int16_t* range_max,
+                                    const float* d_before_refine, const float* d_after_refine,
+                                    const uint8_t* vis_mask, float max_valid_gt, const uint8_t* left_image,
+                                    int left_stride, int left_channels, const apg_quality_thresholds_t* thresholds,
+                                    int device_buffers, void* stream, apg_stereo_metrics_t* out);
 
 /* Number of kernels the library has launched in this process (all engines). */
 APGCU_API unsigned long long apgcu_kernel_launch_count(void);

@@ -1217,3 +1217,159 @@ static int pipeline_run(const apg_pipeline_config_t* cfg, const uint8_t* left, c
 void orc_config_from_mode(int mode, int max_disparity, apg_pipeline_config_t* out) {
     *out = apg_config_from_mode(mode, max_disparity);
 }
+
+/* evaluate_stereo, src/metrics.cpp:119-502, without the support block: the per-pixel tallies in
+ * raster order (so the double sums are the reference's, rounding included), then
+ * apg_metrics_finalize (include/apg_sgm/metrics.h) for the float ratios.  left (nullable) is the
+ * left image with its row stride and channel count; thr NULL means QualityThresholds{}. */
+static int gt_valid(float g, float mx) { return isfinite(g) && g >= 0.0f && g < mx; }
+
+static float orc_luma(const uint8_t* img, int stride, int ch, int x, int y) {
+    const uint8_t* p = img + (size_t)y * stride + (size_t)x * ch;
+    if (ch == 1) return (float)p[0];
+    return 0.299f * (float)p[0] + 0.587f * (float)p[1] + 0.114f * (float)p[2];
+}
+
+static void region_add(long long* r, double* sum, float e, float g) {
+    const int ok = isfinite(e) && e >= 0.0f;
+    const float diff = ok ? fabsf(e - g) : 1e9f;
+    const int d1 = !ok || (diff > 3.0f && (g > 1e-3f ? (diff / g > 0.05f) : 1));
+    r[0]++;
+    if (d1) r[6]++;
+    if (ok) {
+        r[1]++;
+        *sum += diff;
+        if (diff > 0.5f) r[2]++;
+        if (diff > 1.0f) r[3]++;
+        if (diff > 2.0f) r[4]++;
+        if (diff > 3.0f) r[5]++;
+    }
+}
+
+void orc_evaluate_stereo(const float* est, const float* gt, int w, int h, const int16_t* rmin, const int16_t* rmax,
+                         const float* before, const float* after, const uint8_t* vis, float max_valid_gt,
+                         const uint8_t* left, int left_stride, int left_ch, const apg_quality_thresholds_t* thr,
+                         apg_stereo_metrics_t* out) {
+    static const int dxs[4] = {1, -1, 0, 0}, dys[4] = {0, 0, 1, -1};
+    const apg_quality_thresholds_t T = thr ? *thr : apg_quality_thresholds_default();
+    long long c[APG_MC_COUNT];
+    double sm[APG_MS_COUNT];
+    memset(c, 0, sizeof(c));
+    memset(sm, 0, sizeof(sm));
+    if (w <= 0 || h <= 0) {
+        apg_stereo_metrics_t z;
+        memset(&z, 0, sizeof(z));
+        *out = z;
+        return;
+    }
+    const size_t n = (size_t)w * h;
+    const int has_range = rmin && rmax, has_ref = before && after, has_left = left != NULL;
+    uint8_t* edge = (uint8_t*)calloc(n, 1);
+    uint8_t* low = has_left ? (uint8_t*)calloc(n, 1) : NULL;
+    for (int y = 0; y < h; ++y)
+        for (int x = 0; x < w; ++x) {
+            const float g = gt[(size_t)y * w + x];
+            if (!gt_valid(g, max_valid_gt)) continue;
+            float md = 0.0f;
+            for (int k = 0; k < 4; ++k) {
+                const int nx = x + dxs[k], ny = y + dys[k];
+                if (nx >= 0 && nx < w && ny >= 0 && ny < h) {
+                    const float ng = gt[(size_t)ny * w + nx];
+                    if (isfinite(ng) && ng >= 0.0f && ng < max_valid_gt) md = fmaxf_ref(md, fabsf(g - ng));
+                }
+            }
+            if (md >= T.boundary_disparity_gradient) edge[(size_t)y * w + x] = 1;
+        }
+    if (has_left)
+        for (int y = 0; y < h; ++y)
+            for (int x = 0; x < w; ++x) {
+                const int xp = imax(0, x - 1), xn = imin(w - 1, x + 1), yp = imax(0, y - 1), yn = imin(h - 1, y + 1);
+                const float sx = (x == 0 || x == w - 1) ? 1.0f : 2.0f, sy = (y == 0 || y == h - 1) ? 1.0f : 2.0f;
+                const float dx = (orc_luma(left, left_stride, left_ch, xn, y) - orc_luma(left, left_stride, left_ch, xp, y)) / sx;
+                const float dy = (orc_luma(left, left_stride, left_ch, x, yn) - orc_luma(left, left_stride, left_ch, x, yp)) / sy;
+                if (sqrtf(dx * dx + dy * dy) < T.low_texture_gradient) low[(size_t)y * w + x] = 1;
+            }
+    long long* reg = c + APG_MC_REGION0;
+    for (int y = 0; y < h; ++y)
+        for (int x = 0; x < w; ++x) {
+            const size_t i = (size_t)y * w + x;
+            const float g = gt[i];
+            if (!gt_valid(g, max_valid_gt)) continue;
+            c[APG_MC_EVALUATED]++;
+            const int xr = x - (int)roundf(g);
+            const int matchable = xr >= 0 && xr < w;
+            const int visible = vis ? vis[i] >= 200 : matchable;
+            const int ed = edge[i] != 0;
+            if (has_range) {
+                const int in = g >= (float)rmin[i] && g < (float)rmax[i];
+                c[APG_MC_EVAL_ALL]++;
+                if (in) c[APG_MC_IN_ALL]++;
+                if (matchable) {
+                    c[APG_MC_EVAL_MATCH]++;
+                    if (in) c[APG_MC_IN_MATCH]++;
+                }
+                if (visible) {
+                    c[APG_MC_EVAL_VIS]++;
+                    if (in) c[APG_MC_IN_VIS]++;
+                    else {
+                        c[APG_MC_MISS_VIS]++;
+                        if (ed) c[APG_MC_MISS_EDGE]++;
+                        else c[APG_MC_MISS_NONEDGE]++;
+                    }
+                }
+            }
+            const float e = est[i];
+            const int ok = isfinite(e) && e >= 0.0f;
+            if (!ok) {
+                c[APG_MC_LR_FAIL]++;
+            } else {
+                const float diff = fabsf(e - g);
+                c[APG_MC_VALID]++;
+                sm[APG_MS_EPE] += diff;
+                if (diff > 0.5f) c[APG_MC_C05]++;
+                if (diff > 1.0f) c[APG_MC_C10]++;
+                if (diff > 2.0f) c[APG_MC_C20]++;
+                if (diff > 3.0f) c[APG_MC_C30]++;
+                if (ed) { c[APG_MC_EDGE]++; sm[APG_MS_EDGE] += diff; }
+                else { c[APG_MC_NONEDGE]++; sm[APG_MS_NONEDGE] += diff; }
+            }
+            const int d1 = !ok || (fabsf(e - g) > 3.0f && (g > 1e-3f ? (fabsf(e - g) / g > 0.05f) : 1));
+            if (d1) c[APG_MC_D1_ALL]++;
+            if (visible) {
+                c[APG_MC_EVAL_NOC]++;
+                if (d1) c[APG_MC_D1_NOC]++;
+            }
+            region_add(reg + 0, sm + APG_MS_REGION0 + 0, e, g);
+            if (visible) region_add(reg + 7, sm + APG_MS_REGION0 + 1, e, g);
+            else region_add(reg + 14, sm + APG_MS_REGION0 + 2, e, g);
+            if (ed) region_add(reg + 21, sm + APG_MS_REGION0 + 3, e, g);
+            else region_add(reg + 28, sm + APG_MS_REGION0 + 4, e, g);
+            if (has_left) {
+                if (low[i]) region_add(reg + 35, sm + APG_MS_REGION0 + 5, e, g);
+                else region_add(reg + 42, sm + APG_MS_REGION0 + 6, e, g);
+            }
+            if (has_ref) {
+                const float eb = before[i], ea = after[i];
+                if (isfinite(eb) && eb >= 0.0f && isfinite(ea) && ea >= 0.0f) {
+                    const float db = fabsf(eb - g), da = fabsf(ea - g);
+                    c[APG_MC_REF_EVAL]++;
+                    sm[APG_MS_BEFORE] += db;
+                    sm[APG_MS_AFTER] += da;
+                    if (da < db - 1e-4f) c[APG_MC_REF_IMPROVED]++;
+                    else if (da > db + 1e-4f) c[APG_MC_REF_WORSENED]++;
+                    else c[APG_MC_REF_UNCHANGED]++;
+                    if (fabsf(ea - eb) > 1e-4f) c[APG_MC_REF_CHANGED]++;
+                    if (ok) {
+                        c[APG_MC_TOTAL_EVAL]++;
+                        sm[APG_MS_TOT_BEFORE] += db;
+                        sm[APG_MS_TOT_AFTER] += da;
+                        sm[APG_MS_TOT_FINAL] += fabsf(e - g);
+                    }
+                }
+            }
+        }
+    free(edge);
+    free(low);
+    apg_metrics_finalize(c, sm, w * h, has_range, has_ref, out);
+}
+

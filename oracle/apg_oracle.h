@@ -17,6 +17,7 @@
 
 #include <stdint.h>
 #include "../include/apg_sgm/pipeline_config.h"
+#include "../include/apg_sgm/metrics.h"
 
 #ifdef __cplusplus
 extern "C" {
@@ -107,6 +108,12 @@ void orc_hier_coarse_config(const apg_pipeline_config_t* cfg, apg_pipeline_confi
 int  orc_hier_range(const apg_pipeline_config_t* cfg, int w, int h, const uint8_t* lg, const uint8_t* rg,
                     int16_t* rmin, int16_t* rmax, float* d_prior, int64_t* counts4,
                     float* coarse_disp, float* coarse_conf);
+
+/* Accuracy metrics (src/metrics.cpp:119-502, without supports).  Any nullable input may be NULL. */
+void orc_evaluate_stereo(const float* est, const float* gt, int w, int h, const int16_t* rmin, const int16_t* rmax,
+                         const float* before, const float* after, const uint8_t* vis, float max_valid_gt,
+                         const uint8_t* left, int left_stride, int left_ch, const apg_quality_thresholds_t* thr,
+                         apg_stereo_metrics_t* out);
 
 uint64_t orc_fnv1a64(const uint8_t* data, uint64_t n);
 void orc_config_from_mode(int mode, int max_disparity, apg_pipeline_config_t* out);

@@ -57,6 +57,49 @@ class PipelineConfig(C.Structure):
         return self.max_disparity - self.min_disparity
 
 
+_REGION_FIELDS = ["total_pixels", "valid_est_pixels", "valid_ratio", "epe", "bad_0_5", "bad_1_0", "bad_2_0",
+                  "bad_3_0", "d1"]
+
+
+class RegionMetricsRec(C.Structure):
+    """apg_region_metrics_t (include/apg_sgm/metrics.h): RegionMetrics."""
+    _fields_ = [(k, C.c_int if k in ("total_pixels", "valid_est_pixels") else C.c_float) for k in _REGION_FIELDS]
+
+
+class QualityThresholdsRec(C.Structure):
+    """apg_quality_thresholds_t (include/apg_sgm/metrics.h): QualityThresholds."""
+    _fields_ = [("boundary_disparity_gradient", C.c_float), ("low_texture_gradient", C.c_float),
+                ("max_valid_gt", C.c_float)]
+
+
+_I, _F, _U = C.c_int, C.c_float, C.c_ulonglong
+_STEREO_FIELDS = (
+    [("total_pixels", _I), ("evaluated_pixels", _I), ("valid_pixels", _I), ("valid_ratio", _F), ("epe", _F),
+     ("bad_0_5", _F), ("bad_1_0", _F), ("bad_2_0", _F), ("bad_3_0", _F), ("kitti_d1_all", _F), ("kitti_d1_noc", _F),
+     ("edge_pixels", _I), ("edge_epe", _F), ("nonedge_pixels", _I), ("nonedge_epe", _F), ("lr_fail_ratio", _F),
+     ("has_range", _I), ("range_recall_all", _F), ("range_recall_matchable", _F), ("range_recall_visible", _F),
+     ("range_visible_eval_pixels", _U), ("range_visible_in_pixels", _U), ("range_matchable_eval_pixels", _U),
+     ("range_matchable_in_pixels", _U), ("prior_miss_visible_count", _I), ("prior_miss_edge", _I),
+     ("prior_miss_nonedge", _I), ("prior_miss_edge_ratio", _F), ("prior_miss_nonedge_ratio", _F)]
+    + [(r, RegionMetricsRec) for r in ("reg_all", "reg_noc", "reg_occ", "reg_boundary", "reg_non_boundary",
+                                       "reg_low_texture", "reg_high_texture")]
+    + [("has_refine_stats", _I), ("refine_eval_pixels", _I), ("refine_epe_delta", _F), ("post_epe_delta", _F),
+       ("total_epe_delta", _F), ("refine_improved_ratio", _F), ("refine_worsened_ratio", _F),
+       ("refine_unchanged_ratio", _F), ("refine_changed_ratio", _F)])
+
+
+class StereoMetricsRec(C.Structure):
+    """apg_stereo_metrics_t (include/apg_sgm/metrics.h): StereoMetrics without the support block."""
+    _fields_ = _STEREO_FIELDS
+
+    def to_dict(self) -> dict:
+        d = {}
+        for k, t in self._fields_:
+            v = getattr(self, k)
+            d[k] = {r: getattr(v, r) for r in _REGION_FIELDS} if t is RegionMetricsRec else v
+        return d
+
+
 _orc = None
 _ref = None
 
@@ -319,6 +362,46 @@ def ref_hier_dump(cfg: PipelineConfig, left, right) -> dict:
     out["ran"] = int(t[4])
     out["telemetry"] = dict(zip(["avg_states_per_pixel", "coarse_valid_ratio", "fallback_pixel_ratio",
                                  "full_range_pixel_ratio"], t[:4].tolist()))
+    return out
+
+
+def _metric_args(est, gt, range_, before, after, vis, left):
+    est = np.ascontiguousarray(est, np.float32)
+    gt = np.ascontiguousarray(gt, np.float32)
+    h, w = gt.shape
+    rmin = rmax = None
+    if range_ is not None:
+        rmin, rmax = (np.ascontiguousarray(a, np.int16) for a in range_)
+    if before is not None:
+        before, after = np.ascontiguousarray(before, np.float32), np.ascontiguousarray(after, np.float32)
+    if vis is not None:
+        vis = np.ascontiguousarray(vis, np.uint8)
+    lstride = lch = 0
+    if left is not None:
+        left = np.ascontiguousarray(left, np.uint8)
+        lch = 1 if left.ndim == 2 else left.shape[2]
+        lstride = w * lch
+    keep = (est, gt, rmin, rmax, before, after, vis, left)
+    return keep, w, h, lstride, lch
+
+
+def _thr(thresholds):
+    if thresholds is None:
+        return None
+    t = QualityThresholdsRec()
+    t.boundary_disparity_gradient, t.low_texture_gradient, t.max_valid_gt = thresholds
+    return C.byref(t)
+
+
+def evaluate_stereo(est, gt, range_=None, before=None, after=None, vis=None, max_valid_gt=1e5, left=None,
+                    thresholds=None, reference=False) -> StereoMetricsRec:
+    """evaluate_stereo (src/metrics.cpp:119-502, no supports): the oracle's restatement, or with
+    reference=True the reference build's own function.  thresholds: (boundary, low_texture, max_gt)."""
+    keep, w, h, lstride, lch = _metric_args(est, gt, range_, before, after, vis, left)
+    out = StereoMetricsRec()
+    f = ref_lib().ref_evaluate_stereo if reference else lib().orc_evaluate_stereo
+    f(*[_p(a) for a in keep[:2]], C.c_int(w), C.c_int(h), *[_p(a) for a in keep[2:7]], C.c_float(max_valid_gt),
+      _p(keep[7]), C.c_int(lstride), C.c_int(lch), _thr(thresholds), C.byref(out))
     return out
 
 

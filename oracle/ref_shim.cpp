@@ -21,8 +21,10 @@
 #include "apg_sgm/refiner.hpp"
 #include "apg_sgm/session.hpp"
 #include "apg_sgm/sgm_optimizer.hpp"
+#include "apg_sgm/metrics.hpp"
 #include "hierarchical_stereo.hpp"
 
+#include "../include/apg_sgm/metrics.h"
 #include "../include/apg_sgm/pipeline_config.h"
 
 #include <algorithm>
@@ -313,6 +315,105 @@ int ref_hier_dump(const apg_pipeline_config_t* ccfg, const uint8_t* left, const 
     put(invalid_reason, full.invalid_reason.data(), n);
     put(reliable_mask, full.reliable_mask.data(), n);
     return 0;
+}
+
+static void region_out(const RegionMetrics& r, apg_region_metrics_t* o) {
+    o->total_pixels = r.total_pixels;
+    o->valid_est_pixels = r.valid_est_pixels;
+    o->valid_ratio = r.valid_ratio;
+    o->epe = r.epe;
+    o->bad_0_5 = r.bad_0_5;
+    o->bad_1_0 = r.bad_1_0;
+    o->bad_2_0 = r.bad_2_0;
+    o->bad_3_0 = r.bad_3_0;
+    o->d1 = r.d1;
+}
+
+// The reference's evaluate_stereo (src/metrics.cpp:119-502) on plain buffers; nullable inputs
+// are passed as null pointers, thr NULL means QualityThresholds{}.
+void ref_evaluate_stereo(const float* est, const float* gt, int w, int h, const int16_t* rmin, const int16_t* rmax,
+                         const float* before, const float* after, const uint8_t* vis, float max_valid_gt,
+                         const uint8_t* left, int left_stride, int left_ch, const apg_quality_thresholds_t* thr,
+                         apg_stereo_metrics_t* out) {
+    const size_t n = static_cast<size_t>(w) * h;
+    auto img32 = [&](const float* p) {
+        Image32f im(w, h);
+        std::memcpy(im.data(), p, n * sizeof(float));
+        return im;
+    };
+    const Image32f E = img32(est), G = img32(gt);
+    SearchRange range;
+    if (rmin && rmax) {
+        range.allocate(w, h, 0, 1);
+        std::memcpy(range.dmin.data(), rmin, n * sizeof(int16_t));
+        std::memcpy(range.dmax.data(), rmax, n * sizeof(int16_t));
+    }
+    Image32f B, A;
+    if (before && after) {
+        B = img32(before);
+        A = img32(after);
+    }
+    Image8 V;
+    if (vis) V = to_image(vis, w, h, w, 1);
+    Image8 Lf;
+    if (left) Lf = to_image(left, w, h, left_stride, left_ch);
+    QualityThresholds q;
+    if (thr) {
+        q.boundary_disparity_gradient = thr->boundary_disparity_gradient;
+        q.low_texture_gradient = thr->low_texture_gradient;
+        q.max_valid_gt = thr->max_valid_gt;
+    }
+    const StereoMetrics m = evaluate_stereo(E, G, (rmin && rmax) ? &range : nullptr, (before && after) ? &B : nullptr,
+                                            (before && after) ? &A : nullptr, vis ? &V : nullptr, max_valid_gt,
+                                            nullptr, left ? &Lf : nullptr, q);
+    apg_stereo_metrics_t o;
+    std::memset(&o, 0, sizeof(o));
+    o.total_pixels = m.total_pixels;
+    o.evaluated_pixels = m.evaluated_pixels;
+    o.valid_pixels = m.valid_pixels;
+    o.valid_ratio = m.valid_ratio;
+    o.epe = m.epe;
+    o.bad_0_5 = m.bad_0_5;
+    o.bad_1_0 = m.bad_1_0;
+    o.bad_2_0 = m.bad_2_0;
+    o.bad_3_0 = m.bad_3_0;
+    o.kitti_d1_all = m.kitti_d1_all;
+    o.kitti_d1_noc = m.kitti_d1_noc;
+    o.edge_pixels = m.edge_pixels;
+    o.edge_epe = m.edge_epe;
+    o.nonedge_pixels = m.nonedge_pixels;
+    o.nonedge_epe = m.nonedge_epe;
+    o.lr_fail_ratio = m.lr_fail_ratio;
+    o.has_range = m.has_range ? 1 : 0;
+    o.range_recall_all = m.range_recall_all;
+    o.range_recall_matchable = m.range_recall_matchable;
+    o.range_recall_visible = m.range_recall_visible;
+    o.range_visible_eval_pixels = m.range_visible_eval_pixels;
+    o.range_visible_in_pixels = m.range_visible_in_pixels;
+    o.range_matchable_eval_pixels = m.range_matchable_eval_pixels;
+    o.range_matchable_in_pixels = m.range_matchable_in_pixels;
+    o.prior_miss_visible_count = m.prior_miss_visible_count;
+    o.prior_miss_edge = m.prior_miss_edge;
+    o.prior_miss_nonedge = m.prior_miss_nonedge;
+    o.prior_miss_edge_ratio = m.prior_miss_edge_ratio;
+    o.prior_miss_nonedge_ratio = m.prior_miss_nonedge_ratio;
+    region_out(m.reg_all, &o.reg_all);
+    region_out(m.reg_noc, &o.reg_noc);
+    region_out(m.reg_occ, &o.reg_occ);
+    region_out(m.reg_boundary, &o.reg_boundary);
+    region_out(m.reg_non_boundary, &o.reg_non_boundary);
+    region_out(m.reg_low_texture, &o.reg_low_texture);
+    region_out(m.reg_high_texture, &o.reg_high_texture);
+    o.has_refine_stats = m.has_refine_stats ? 1 : 0;
+    o.refine_eval_pixels = m.refine_eval_pixels;
+    o.refine_epe_delta = m.refine_epe_delta;
+    o.post_epe_delta = m.post_epe_delta;
+    o.total_epe_delta = m.total_epe_delta;
+    o.refine_improved_ratio = m.refine_improved_ratio;
+    o.refine_worsened_ratio = m.refine_worsened_ratio;
+    o.refine_unchanged_ratio = m.refine_unchanged_ratio;
+    o.refine_changed_ratio = m.refine_changed_ratio;
+    *out = o;
 }
 
 // Public-API session used for timing the reference CPU path.
