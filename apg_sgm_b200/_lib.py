@@ -167,6 +167,7 @@ _SIGS = {
     "apgcu_session_hier_telemetry": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     "apgcu_engine_hier_telemetry": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     "apgcu_kernel_launch_count": (C.c_ulonglong, []),
+    "apgcu_metrics_last_kernel_ms": (C.c_float, []),
     "apgcu_evaluate_stereo": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
                                         C.c_void_p, C.c_void_p, C.c_float, C.c_void_p, C.c_int, C.c_int,
                                         C.POINTER(QualityThresholdsRec), C.c_int, C.c_void_p,

@@ -274,6 +274,12 @@ void count_launches(unsigned n);
 // ------------------------------------------------------------------------------------------------
 #include "../../include/apg_sgm_cuda.h"
 
+namespace {
+thread_local float g_metrics_ms = 0.0f;  // device time of this thread's last evaluation's kernels
+}
+
+extern "C" APGCU_API float apgcu_metrics_last_kernel_ms(void) { return g_metrics_ms; }
+
 extern "C" APGCU_API int apgcu_evaluate_stereo(const float* est, const float* gt, int w, int h, const int16_t* rmin,
                                                const int16_t* rmax, const float* before, const float* after,
                                                const uint8_t* vis, float max_valid_gt, const uint8_t* left,
@@ -328,12 +334,16 @@ extern "C" APGCU_API int apgcu_evaluate_stereo(const float* est, const float* gt
     }
     long long* dc = nullptr;
     double* ds = nullptr;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    const bool timed = cudaEventCreate(&ev[0]) == cudaSuccess && cudaEventCreate(&ev[1]) == cudaSuccess;
+    if (timed && e == cudaSuccess) cudaEventRecord(ev[0], s);
     if (e == cudaSuccess)
         e = apgcu::launch_metrics(dE, dG, w, h, has_range ? dR0 : nullptr, has_range ? dR1 : nullptr,
                                   has_ref ? dB : nullptr, has_ref ? dA : nullptr, dV, max_valid_gt, dL, left_stride,
                                   left_ch, T, blk + in_bytes, &dc, &ds, s);
     long long c[APG_MC_COUNT];
     double sm[APG_MS_COUNT];
+    if (timed && e == cudaSuccess) cudaEventRecord(ev[1], s);
     if (e == cudaSuccess) {
         apgcu::count_launches(2);
         e = cudaMemcpyAsync(c, dc, sizeof(c), cudaMemcpyDeviceToHost, s);
@@ -341,6 +351,11 @@ extern "C" APGCU_API int apgcu_evaluate_stereo(const float* est, const float* gt
     if (e == cudaSuccess) e = cudaMemcpyAsync(sm, ds, sizeof(sm), cudaMemcpyDeviceToHost, s);
     cudaFreeAsync(blk, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (timed) {
+        if (e == cudaSuccess) cudaEventElapsedTime(&g_metrics_ms, ev[0], ev[1]);
+        cudaEventDestroy(ev[0]);
+        cudaEventDestroy(ev[1]);
+    }
     if (e != cudaSuccess) {
         cudaGetLastError();
         return APG_STATUS_INTERNAL_ERROR;

@@ -143,6 +143,10 @@ APGCU_API int apgcu_evaluate_stereo(const float* est, const float* gt, int width
                                     int left_stride, int left_channels, const apg_quality_thresholds_t* thresholds,
                                     int device_buffers, void* stream, apg_stereo_metrics_t* out);
 
+/* Device time (ms) of the two kernels of this thread's last apgcu_evaluate_stereo, from events on
+ * its stream around them. */
+APGCU_API float apgcu_metrics_last_kernel_ms(void);
+
 /* Number of kernels the library has launched in this process (all engines). */
 APGCU_API unsigned long long apgcu_kernel_launch_count(void);
 
