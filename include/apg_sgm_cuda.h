@@ -135,7 +135,8 @@ APGCU_API size_t apgcu_session_estimate_bytes(apg_session_t s, int width, int he
  * cudaStream_t, NULL = the legacy default stream); otherwise they are host arrays copied in.
  * Returns when *out is written: counts exact, ratios formed with the reference's float
  * expressions, sums of errors in double (equal to the reference's whenever its sequential double
- * sum is exact).  Scratch comes from the stream-ordered allocator. */
+ * sum is exact).  Scratch (and the device copies of host inputs) comes from a stream-ordered pool the
+ * library owns per device, which keeps its high-water mark between calls. */
 APGCU_API int apgcu_evaluate_stereo(const float* est, const float* gt, int width, int height,
                                     const int16_t* range_min, const int16_t* range_max,
                                     const float* d_before_refine, const float* d_after_refine,
