@@ -630,6 +630,150 @@ def evaluate_stereo(est, gt, range=None, d_before_refine=None, d_after_refine=No
     return out
 
 
+# ---- On-disk formats (src/image.cpp:62-206) ----------------------------------------------------
+
+def _path(p) -> bytes:
+    return str(p).encode()
+
+
+def _io_check(rc: int, what: str, path):
+    if rc != 0:
+        raise OSError(f"{what} failed for {path} [{rc}]")
+
+
+def load_image(path) -> np.ndarray:
+    """load_image: binary PGM (HxW) or PPM (HxWx3) as uint8."""
+    w, h, c = C.c_int(), C.c_int(), C.c_int()
+    _io_check(lib().apgcu_image_info(_path(path), C.byref(w), C.byref(h), C.byref(c)), "load_image", path)
+    a = np.empty((h.value, w.value, c.value) if c.value > 1 else (h.value, w.value), np.uint8)
+    _io_check(lib().apgcu_load_image(_path(path), a.ctypes.data, a.nbytes, C.byref(w), C.byref(h), C.byref(c)),
+              "load_image", path)
+    return a
+
+
+def save_pgm(path, img):
+    a = np.ascontiguousarray(img, np.uint8)
+    if a.ndim != 2:
+        raise ValueError("save_pgm takes a single-channel HxW image")
+    _io_check(lib().apgcu_save_pgm(_path(path), a.ctypes.data, a.shape[1], a.shape[0]), "save_pgm", path)
+
+
+def save_pgm16(path, disp):
+    a = np.ascontiguousarray(disp, np.int16)
+    _io_check(lib().apgcu_save_pgm16(_path(path), a.ctypes.data, a.shape[1], a.shape[0]), "save_pgm16", path)
+
+
+def save_disparity_preview(path, disp, dmax: float):
+    a = np.ascontiguousarray(disp, np.float32)
+    _io_check(lib().apgcu_save_disparity_preview(_path(path), a.ctypes.data, a.shape[1], a.shape[0],
+                                                 C.c_float(dmax)), "save_disparity_preview", path)
+
+
+def load_pfm(path) -> np.ndarray:
+    """load_pfm: HxW float32 (channel 0 of a colour PFM), top row first."""
+    w, h, c = C.c_int(), C.c_int(), C.c_int()
+    _io_check(lib().apgcu_pfm_info(_path(path), C.byref(w), C.byref(h), C.byref(c)), "load_pfm", path)
+    a = np.empty((h.value, w.value), np.float32)
+    _io_check(lib().apgcu_load_pfm(_path(path), a.ctypes.data, a.size, C.byref(w), C.byref(h)), "load_pfm", path)
+    return a
+
+
+def save_pfm(path, img):
+    a = np.ascontiguousarray(img, np.float32)
+    _io_check(lib().apgcu_save_pfm(_path(path), a.ctypes.data, a.shape[1], a.shape[0]), "save_pfm", path)
+
+
+class Loader:
+    """Pair loader (apgcu_loader_*): worker threads read (left, right) image files into page-locked
+    buffers the loader recycles.  wait() lends the pair as numpy views of those buffers, valid until
+    release()."""
+
+    def __init__(self, threads: int = 4):
+        self._h = lib().apgcu_loader_create(int(threads))
+        if not self._h:
+            raise RuntimeError("apgcu_loader_create failed")
+
+    def submit(self, left_path, right_path) -> int:
+        t = C.c_ulonglong()
+        rc = lib().apgcu_loader_submit(self._h, _path(left_path), _path(right_path), C.byref(t))
+        if rc != 0:
+            raise RuntimeError(f"loader submit failed [{rc}]")
+        return t.value
+
+    def wait(self, ticket: int):
+        p = _lib_mod.LoadedPair()
+        rc = lib().apgcu_loader_wait(self._h, int(ticket), C.byref(p))
+        if rc != 0:
+            raise OSError(f"loading pair {ticket} failed [{rc}]")
+        shape = (p.height, p.width, p.channels) if p.channels > 1 else (p.height, p.width)
+        n = p.width * p.height * p.channels
+        views = []
+        for ptr in (p.left, p.right):
+            buf = (C.c_uint8 * n).from_address(ptr)
+            views.append(np.frombuffer(buf, np.uint8).reshape(shape))
+        return views[0], views[1]
+
+    def release(self, ticket: int):
+        lib().apgcu_loader_release(self._h, int(ticket))
+
+    @property
+    def pinned_bytes(self) -> int:
+        return int(lib().apgcu_loader_pinned_bytes(self._h))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().apgcu_loader_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def serve_files(server: "Server", pairs, mode=QualityMode.Balanced, max_disparity=128, min_disparity=0,
+                loader: Loader = None, depth: int = 16, out_pool=None):
+    """Runs (left_path, right_path) pairs through `server`, reading ahead with a Loader: up to
+    `depth` pairs are read or in flight at once, each pair's page-locked images go to the server as
+    they are, and a pair's buffers return to the loader when its request completes.  out_pool
+    (optional): a list of at least `depth` caller-owned result dicts (see Server.submit) reused in
+    turn.  Yields (index, outputs, latency_ms) in submission order."""
+    own = loader is None
+    ld = loader or Loader()
+    pairs = list(pairs)
+    tickets, inflight = {}, []
+    nxt = 0
+    try:
+        while nxt < len(pairs) and len(tickets) < depth:
+            tickets[nxt] = ld.submit(*pairs[nxt])
+            nxt += 1
+        for i in range(len(pairs)):
+            if i in tickets:
+                lt = tickets.pop(i)
+                left, right = ld.wait(lt)
+                out = out_pool[i % len(out_pool)] if out_pool else None
+                inflight.append((i, lt, server.submit(left, right, mode=mode, max_disparity=max_disparity,
+                                                      min_disparity=min_disparity, out=out)))
+            while inflight and (len(inflight) >= depth or i == len(pairs) - 1):
+                j, lt, st = inflight.pop(0)
+                o, lat = server.wait(st)
+                ld.release(lt)
+                if nxt < len(pairs):
+                    tickets[nxt] = ld.submit(*pairs[nxt])
+                    nxt += 1
+                yield j, o, lat
+    finally:
+        for j, lt, st in inflight:
+            try:
+                server.wait(st)
+            except Exception:
+                pass
+            ld.release(lt)
+        if own:
+            ld.close()
+
+
 def workspace_bytes(config: PipelineConfig, width: int, height: int) -> int:
     return int(lib().apgcu_workspace_bytes(C.byref(config), int(width), int(height)))
 
@@ -637,6 +781,8 @@ def workspace_bytes(config: PipelineConfig, width: int, height: int) -> int:
 __all__ = ["QualityMode", "HierarchicalFallback", "VolumeBackend", "MemoryPolicy", "StatusCode", "InvalidReason", "StageTiming",
            "PipelineStats", "StereoResult", "StereoSession", "PipelineConfig", "config_from_mode", "Engine",
            "kernel_launch_count", "workspace_bytes", "evaluate_stereo", "StereoMetrics", "RegionMetrics",
+           "load_image", "save_pgm", "save_pgm16", "save_disparity_preview", "load_pfm", "save_pfm", "Loader",
+           "serve_files",
            "__version__"]
 
 

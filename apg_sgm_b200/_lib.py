@@ -105,6 +105,12 @@ class SessionOptions(C.Structure):
                 ("min_disparity", C.c_int), ("max_disparity", C.c_int)]
 
 
+class LoadedPair(C.Structure):
+    """apgcu_loaded_pair_t (include/apg_sgm_cuda.h): one pair read by the loader."""
+    _fields_ = [("status", C.c_int), ("width", C.c_int), ("height", C.c_int), ("channels", C.c_int),
+                ("left", C.c_void_p), ("right", C.c_void_p)]
+
+
 class Pair(C.Structure):
     """apgcu_pair_t (include/apg_sgm_cuda.h): one pair of a batch."""
     _fields_ = [("left", C.c_void_p), ("right", C.c_void_p), ("width", C.c_int), ("height", C.c_int),
@@ -167,6 +173,21 @@ _SIGS = {
     "apgcu_session_hier_telemetry": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     "apgcu_engine_hier_telemetry": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     "apgcu_kernel_launch_count": (C.c_ulonglong, []),
+    "apgcu_image_info": (C.c_int, [C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "apgcu_load_image": (C.c_int, [C.c_char_p, C.c_void_p, C.c_size_t, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                   C.POINTER(C.c_int)]),
+    "apgcu_save_pgm": (C.c_int, [C.c_char_p, C.c_void_p, C.c_int, C.c_int]),
+    "apgcu_save_pgm16": (C.c_int, [C.c_char_p, C.c_void_p, C.c_int, C.c_int]),
+    "apgcu_save_disparity_preview": (C.c_int, [C.c_char_p, C.c_void_p, C.c_int, C.c_int, C.c_float]),
+    "apgcu_pfm_info": (C.c_int, [C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "apgcu_load_pfm": (C.c_int, [C.c_char_p, C.c_void_p, C.c_size_t, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "apgcu_save_pfm": (C.c_int, [C.c_char_p, C.c_void_p, C.c_int, C.c_int]),
+    "apgcu_loader_create": (C.c_void_p, [C.c_int]),
+    "apgcu_loader_destroy": (None, [C.c_void_p]),
+    "apgcu_loader_submit": (C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p, C.POINTER(C.c_ulonglong)]),
+    "apgcu_loader_wait": (C.c_int, [C.c_void_p, C.c_ulonglong, C.POINTER(LoadedPair)]),
+    "apgcu_loader_release": (C.c_int, [C.c_void_p, C.c_ulonglong]),
+    "apgcu_loader_pinned_bytes": (C.c_size_t, [C.c_void_p]),
     "apgcu_metrics_last_kernel_ms": (C.c_float, []),
     "apgcu_evaluate_stereo": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
                                         C.c_void_p, C.c_void_p, C.c_float, C.c_void_p, C.c_int, C.c_int,

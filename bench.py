@@ -943,13 +943,141 @@ def run_reference_metrics(args):
     }))
 
 
+FILES_SPEC = (1280, 720, 128, 12, 0, 120, 0.0)
+
+
+def _write_file_pairs(apg, n: int, d):
+    """n Balanced 1280x720 D128 pairs as binary PGM files in directory d (synthetic, seeded)."""
+    from apg_sgm_b200 import synthetic as S
+    spec = S.PairSpec(*FILES_SPEC)
+    paths = []
+    for i in range(n):
+        L, R, _ = S.make_pair(spec, S.SEED_BASE + i)
+        lp, rp = os.path.join(d, f"l{i:03d}.pgm"), os.path.join(d, f"r{i:03d}.pgm")
+        apg.save_pgm(lp, L)
+        apg.save_pgm(rp, R)
+        paths.append((lp, rp))
+    return paths
+
+
+def run_files(args):
+    """Pairs served from PGM files: the page-locked Loader reading ahead into the served form
+    (serve_files) against the serial path (load_image, then one engine call per pair).  A step is
+    the whole set of 48 pairs, files in the page cache; host time from the first read to the last
+    result on the host."""
+    import tempfile
+    import torch
+    import apg_sgm_b200 as apg
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    n = 48
+    w, h, D = FILES_SPEC[0], FILES_SPEC[1], FILES_SPEC[2]
+    with tempfile.TemporaryDirectory() as d:
+        paths = _write_file_pairs(apg, n, d)
+        srv = apg.Server(device=local, slots=4)
+        srv.reserve(w, h, mode=1, max_disparity=D, count=4)
+        depth = 16
+        pool = [{k: _pinned(np.zeros((h, w), dt)) for k, dt in (("disparity", np.float32), ("confidence", np.float32),
+                                                                  ("invalid_reason", np.uint8),
+                                                                  ("reliable_mask", np.uint8))} for _ in range(depth)]
+        ld = apg.Loader(threads=4)
+        eng = apg.Engine(apg.config_from_mode(1, D), device=local)
+
+        def served():
+            for _ in apg.serve_files(srv, paths, mode=1, max_disparity=D, loader=ld, depth=depth, out_pool=pool):
+                pass
+
+        def serial():
+            for lp, rp in paths:
+                eng.process(apg.load_image(lp), apg.load_image(rp))
+
+        for _ in range(max(args.warmup, 3) if args.warmup else 1):
+            served()
+            serial()
+        launches0 = apg.kernel_launch_count()
+        t0 = time.perf_counter()
+        steps = max(1, min(args.steps, 5))
+        for _ in range(steps):
+            served()
+        t_served = (time.perf_counter() - t0) / steps
+        launches = apg.kernel_launch_count() - launches0
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            serial()
+        t_serial = (time.perf_counter() - t0) / steps
+        out = {
+            "metric": f"pairs/s from PGM files, {w}x{h} D={D} Balanced", "value": n / t_served, "unit": "pairs/s",
+            "n_gpus": 1, "steps": steps, "warmup": args.warmup, "ms_per_step": t_served * 1000,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": "synthetic",
+            "config": {"workload": "files_48x_balanced_1280x720_d128", "pairs_per_step": n,
+                       "loader_threads": 4, "server_slots": 4, "depth": depth,
+                       "files": "binary PGM in the page cache"},
+            "e2e": {"value": n / t_served, "unit": "pairs/s", "h2d_bytes_per_step": n * 2 * w * h,
+                    "d2h_bytes_per_step": n * w * h * 10, "api": "serve_files (Loader -> Server, page-locked)"},
+            "serial_value": n / t_serial, "served_over_serial": t_serial / t_served,
+            "gpu_launches": launches,
+            "loader_pinned_bytes": ld.pinned_bytes,
+        }
+        if not args.no_cpu_baseline:
+            from oracle import oracle as O
+            if O.ref_available():
+                sess = O.RefSession(O.config(1, D, volume_backend=2), bounded_reuse=True)
+                sample = paths[:4]
+                for lp, rp in sample[:1]:
+                    sess.process(O.ref_load_image(lp)[1], O.ref_load_image(rp)[1])
+                t0 = time.perf_counter()
+                for lp, rp in sample:
+                    sess.process(O.ref_load_image(lp)[1], O.ref_load_image(rp)[1])
+                tr = (time.perf_counter() - t0) / len(sample)
+                out["cpu_baseline"] = {"value": 1.0 / tr, "unit": "pairs/s", "cores": O.ref_threads(),
+                                       "kind": "reference",
+                                       "sample": "4 of the file pairs: the reference's load_image + StereoSession "
+                                                 "(Packed backend), all host threads"}
+        ld.close()
+        eng.close()
+        srv.close()
+        print(json.dumps(out))
+
+
+def run_reference_files(args):
+    """The reference's load_image + StereoSession over a bounded sample of the file pairs."""
+    import tempfile
+    import apg_sgm_b200 as apg  # only to write the input files
+    from oracle import oracle as O
+    if not O.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libapg_ref.so not built"}))
+        return
+    D = FILES_SPEC[2]
+    with tempfile.TemporaryDirectory() as d:
+        paths = _write_file_pairs(apg, 4, d)
+        sess = O.RefSession(O.config(1, D, volume_backend=2), bounded_reuse=True)
+        for _ in range(args.warmup):
+            sess.process(O.ref_load_image(paths[0][0])[1], O.ref_load_image(paths[0][1])[1])
+        t0 = time.perf_counter()
+        for k in range(args.steps):
+            lp, rp = paths[k % len(paths)]
+            sess.process(O.ref_load_image(lp)[1], O.ref_load_image(rp)[1])
+        total = time.perf_counter() - t0
+    value = args.steps / total
+    print(json.dumps({
+        "impl": "reference", "metric": f"pairs/s from PGM files, {FILES_SPEC[0]}x{FILES_SPEC[1]} D={D} Balanced",
+        "value": value, "unit": "pairs/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000 * total / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u16", "data": "synthetic", "config": {"workload": "files_48x_balanced_1280x720_d128"},
+        "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": O.ref_threads(), "kind": "reference",
+                         "sample": f"{args.steps} file pairs through load_image + StereoSession (Packed)"},
+        "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batched", "served", "metrics1080"], default="fast720")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batched", "served", "metrics1080", "files720"],
+                    default="fast720")
     ap.add_argument("--requests", type=int, default=10000, help="served: total requests over the rates")
     ap.add_argument("--rates", default="50,100,200,400,600", help="served: Poisson arrival rates, pairs/s")
     ap.add_argument("--slots", type=int, default=4, help="served: requests in flight")
@@ -963,6 +1091,10 @@ def main():
             return
         if int(os.environ.get("RANK", "0")) == 0:
             run_served(args)
+        return
+    if args.workload == "files720":
+        if int(os.environ.get("RANK", "0")) == 0:
+            (run_reference_files if args.impl == "reference" else run_files)(args)
         return
     if args.workload == "metrics1080":
         if int(os.environ.get("RANK", "0")) == 0:

@@ -148,6 +148,40 @@ APGCU_API int apgcu_evaluate_stereo(const float* est, const float* gt, int width
  * its stream around them. */
 APGCU_API float apgcu_metrics_last_kernel_ms(void);
 
+/* ---- On-disk formats (src/image.cpp:62-206), byte-compatible with the reference's readers and
+ * writers.  Status: 0, APG_STATUS_EMPTY_INPUT (no such file / null argument),
+ * APG_STATUS_INVALID_CONFIG (malformed or short file, unsupported magic, maxval outside 1..255),
+ * APG_STATUS_SIZE_MISMATCH (dst too small: the dimensions are still written). */
+APGCU_API int apgcu_image_info(const char* path, int* width, int* height, int* channels);   /* P5 / P6 */
+APGCU_API int apgcu_load_image(const char* path, uint8_t* dst, size_t dst_bytes, int* width, int* height,
+                               int* channels);                                             /* load_image */
+APGCU_API int apgcu_save_pgm(const char* path, const uint8_t* img, int width, int height); /* save_pgm */
+APGCU_API int apgcu_save_pgm16(const char* path, const int16_t* disp, int width, int height); /* save_pgm16 */
+APGCU_API int apgcu_save_disparity_preview(const char* path, const float* disp, int width, int height,
+                                           float dmax);                                    /* save_disparity_preview */
+APGCU_API int apgcu_pfm_info(const char* path, int* width, int* height, int* channels);
+APGCU_API int apgcu_load_pfm(const char* path, float* dst, size_t dst_floats, int* width, int* height); /* load_pfm */
+APGCU_API int apgcu_save_pfm(const char* path, const float* img, int width, int height);  /* save_pfm */
+
+/* Pair loader (no reference counterpart): `threads` workers read (left, right) image files into
+ * page-locked buffers that the loader recycles, so engines and the server take them by DMA.
+ * submit returns at once with a ticket; wait blocks until that pair is read and lends its two
+ * images (valid until release). */
+typedef struct apgcu_loader_s* apgcu_loader_t;
+typedef struct {
+    int status;                 /* as apgcu_load_image; SIZE_MISMATCH if the two images differ */
+    int width, height, channels;
+    const uint8_t* left;        /* page-locked, width*height*channels bytes, rows contiguous */
+    const uint8_t* right;
+} apgcu_loaded_pair_t;
+APGCU_API apgcu_loader_t apgcu_loader_create(int threads);
+APGCU_API void apgcu_loader_destroy(apgcu_loader_t l);
+APGCU_API int apgcu_loader_submit(apgcu_loader_t l, const char* left_path, const char* right_path,
+                                  unsigned long long* ticket);
+APGCU_API int apgcu_loader_wait(apgcu_loader_t l, unsigned long long ticket, apgcu_loaded_pair_t* out);
+APGCU_API int apgcu_loader_release(apgcu_loader_t l, unsigned long long ticket);
+APGCU_API size_t apgcu_loader_pinned_bytes(apgcu_loader_t l);
+
 /* Number of kernels the library has launched in this process (all engines). */
 APGCU_API unsigned long long apgcu_kernel_launch_count(void);
 

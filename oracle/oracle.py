@@ -405,6 +405,38 @@ def evaluate_stereo(est, gt, range_=None, before=None, after=None, vis=None, max
     return out
 
 
+def ref_load_image(path):
+    """The reference's load_image: (status, array or None); status 1 ok, 0 failed, -1 threw."""
+    w, h, c = C.c_int(), C.c_int(), C.c_int()
+    rc = ref_lib().ref_load_image(str(path).encode(), None, C.c_size_t(0), C.byref(w), C.byref(h), C.byref(c))
+    if rc != 1:
+        return rc, None
+    a = np.empty((h.value, w.value, c.value) if c.value > 1 else (h.value, w.value), np.uint8)
+    ref_lib().ref_load_image(str(path).encode(), _p(a), C.c_size_t(a.nbytes), C.byref(w), C.byref(h), C.byref(c))
+    return 1, a
+
+
+def ref_load_pfm(path):
+    w, h = C.c_int(), C.c_int()
+    rc = ref_lib().ref_load_pfm(str(path).encode(), None, C.c_size_t(0), C.byref(w), C.byref(h))
+    if rc != 1:
+        return rc, None
+    a = np.empty((h.value, w.value), np.float32)
+    ref_lib().ref_load_pfm(str(path).encode(), _p(a), C.c_size_t(a.size), C.byref(w), C.byref(h))
+    return 1, a
+
+
+def ref_save(kind: str, path, arr, dmax: float = 0.0) -> int:
+    """The reference's save_pgm / save_pgm16 / save_disparity_preview / save_pfm."""
+    a = np.ascontiguousarray(arr)
+    h, w = a.shape[:2]
+    f = getattr(ref_lib(), "ref_save_" + kind)
+    args = [str(path).encode(), _p(a), C.c_int(w), C.c_int(h)]
+    if kind == "disparity_preview":
+        args.append(C.c_float(dmax))
+    return int(f(*args))
+
+
 class RefSession:
     """The reference's public StereoSession (BoundedReuse) for timing its CPU path."""
 

@@ -416,6 +416,62 @@ void ref_evaluate_stereo(const float* est, const float* gt, int w, int h, const 
     *out = o;
 }
 
+// The reference's image I/O (src/image.cpp:62-206).  Loads return 1 on success, 0 on failure, -1
+// where the reference throws (std::stoi / std::stof on a malformed header); dims are written on
+// success only.
+int ref_load_image(const char* path, uint8_t* dst, size_t cap, int* w, int* h, int* ch) {
+    try {
+        Image8 im;
+        if (!load_image(path, im)) return 0;
+        *w = im.width();
+        *h = im.height();
+        *ch = im.channels();
+        const size_t n = static_cast<size_t>(im.width()) * im.height() * im.channels();
+        if (dst && cap >= n) std::memcpy(dst, im.data(), n);
+        return 1;
+    } catch (...) {
+        return -1;
+    }
+}
+
+int ref_load_pfm(const char* path, float* dst, size_t cap, int* w, int* h) {
+    try {
+        Image32f im;
+        if (!load_pfm(path, im)) return 0;
+        *w = im.width();
+        *h = im.height();
+        const size_t n = static_cast<size_t>(im.width()) * im.height();
+        if (dst && cap >= n) std::memcpy(dst, im.data(), n * sizeof(float));
+        return 1;
+    } catch (...) {
+        return -1;
+    }
+}
+
+int ref_save_pgm(const char* path, const uint8_t* img, int w, int h) {
+    Image8 im(w, h, 1);
+    std::memcpy(im.data(), img, static_cast<size_t>(w) * h);
+    return save_pgm(path, im) ? 1 : 0;
+}
+
+int ref_save_pgm16(const char* path, const int16_t* d, int w, int h) {
+    Image16s im(w, h);
+    std::memcpy(im.data(), d, static_cast<size_t>(w) * h * sizeof(int16_t));
+    return save_pgm16(path, im) ? 1 : 0;
+}
+
+int ref_save_disparity_preview(const char* path, const float* d, int w, int h, float dmax) {
+    Image32f im(w, h);
+    std::memcpy(im.data(), d, static_cast<size_t>(w) * h * sizeof(float));
+    return save_disparity_preview(path, im, dmax) ? 1 : 0;
+}
+
+int ref_save_pfm(const char* path, const float* d, int w, int h) {
+    Image32f im(w, h);
+    std::memcpy(im.data(), d, static_cast<size_t>(w) * h * sizeof(float));
+    return save_pfm(path, im) ? 1 : 0;
+}
+
 // Public-API session used for timing the reference CPU path.
 void* ref_session_create(const apg_pipeline_config_t* ccfg, int bounded_reuse) {
     ExecutionOptions opt;
