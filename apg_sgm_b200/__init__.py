@@ -774,6 +774,83 @@ def serve_files(server: "Server", pairs, mode=QualityMode.Balanced, max_disparit
             ld.close()
 
 
+# ---- Experimental scopes (src/subpixel_estimator.hpp, src/inpaint_internal.hpp) -----------------
+
+class SubpixelMethod(enum.IntEnum):
+    Legacy = 0
+    CurvGate = 1
+    ConfGate = 2
+    Stabilized = 3
+
+
+class InpaintMethod(enum.IntEnum):
+    Legacy = 0
+    ShadowReclass = 1
+
+
+_SUBPIXEL = {"legacy": SubpixelMethod.Legacy, "a": SubpixelMethod.Legacy, "curv_gate": SubpixelMethod.CurvGate,
+             "curv": SubpixelMethod.CurvGate, "b": SubpixelMethod.CurvGate, "conf_gate": SubpixelMethod.ConfGate,
+             "conf": SubpixelMethod.ConfGate, "c": SubpixelMethod.ConfGate, "stabilized": SubpixelMethod.Stabilized,
+             "stab": SubpixelMethod.Stabilized, "d": SubpixelMethod.Stabilized}
+_INPAINT = {"legacy": InpaintMethod.Legacy, "a": InpaintMethod.Legacy, "shadow_reclass": InpaintMethod.ShadowReclass,
+            "shadow": InpaintMethod.ShadowReclass, "c": InpaintMethod.ShadowReclass}
+
+
+def _get_experimental():
+    sm, sp, im, ig = C.c_int(), C.c_float(), C.c_int(), C.c_int()
+    lib().apgcu_get_experimental(C.byref(sm), C.byref(sp), C.byref(im), C.byref(ig))
+    return sm.value, sp.value, im.value, ig.value
+
+
+class ExperimentalSubpixelScope:
+    """ExperimentalSubpixelScope (src/subpixel_estimator.hpp:130-155): within the `with` block, every
+    frame this thread runs uses `method` (parse_subpixel_method's names or SubpixelMethod) with
+    `param` (<= 0: the method's default) for the WTA and right-image sub-pixel step; the previous
+    scope returns on exit.  The telemetry counters are not part of this library."""
+
+    def __init__(self, method=SubpixelMethod.Legacy, param: float = 0.0, collect_telemetry: bool = False):
+        if collect_telemetry:
+            raise NotImplementedError("sub-pixel telemetry is not part of the CUDA backend")
+        m = _parse(method, SubpixelMethod, _SUBPIXEL, "subpixel method")
+        self.method, self.param = (SubpixelMethod.Legacy if m is None else m), float(param)
+
+    def __enter__(self):
+        self._prev = _get_experimental()
+        _, _, im, ig = self._prev
+        lib().apgcu_set_experimental(int(self.method), C.c_float(self.param), im, ig)
+        return self
+
+    def __exit__(self, *exc):
+        sm, sp, _, _ = self._prev
+        _, _, im, ig = _get_experimental()
+        lib().apgcu_set_experimental(sm, C.c_float(sp), im, ig)
+        return False
+
+
+class ExperimentalInpaintScope:
+    """ExperimentalInpaintScope (src/inpaint_internal.hpp, src/postprocess.cpp:42-53): within the
+    `with` block every frame this thread runs fills holes with `method` (Legacy or ShadowReclass)
+    and `max_gap` (Legacy at 32 keeps the configuration's max_fill_gap)."""
+
+    def __init__(self, method=InpaintMethod.Legacy, max_gap: int = 32, collect_telemetry: bool = False):
+        if collect_telemetry:
+            raise NotImplementedError("inpaint telemetry is not part of the CUDA backend")
+        m = _parse(method, InpaintMethod, _INPAINT, "inpaint method")
+        self.method, self.max_gap = (InpaintMethod.Legacy if m is None else m), int(max_gap)
+
+    def __enter__(self):
+        self._prev = _get_experimental()
+        sm, sp, _, _ = self._prev
+        lib().apgcu_set_experimental(sm, C.c_float(sp), int(self.method), self.max_gap)
+        return self
+
+    def __exit__(self, *exc):
+        _, _, im, ig = self._prev
+        sm, sp, _, _ = _get_experimental()
+        lib().apgcu_set_experimental(sm, C.c_float(sp), im, ig)
+        return False
+
+
 def workspace_bytes(config: PipelineConfig, width: int, height: int) -> int:
     return int(lib().apgcu_workspace_bytes(C.byref(config), int(width), int(height)))
 
@@ -782,7 +859,7 @@ __all__ = ["QualityMode", "HierarchicalFallback", "VolumeBackend", "MemoryPolicy
            "PipelineStats", "StereoResult", "StereoSession", "PipelineConfig", "config_from_mode", "Engine",
            "kernel_launch_count", "workspace_bytes", "evaluate_stereo", "StereoMetrics", "RegionMetrics",
            "load_image", "save_pgm", "save_pgm16", "save_disparity_preview", "load_pfm", "save_pfm", "Loader",
-           "serve_files",
+           "serve_files", "SubpixelMethod", "InpaintMethod", "ExperimentalSubpixelScope", "ExperimentalInpaintScope",
            "__version__"]
 
 

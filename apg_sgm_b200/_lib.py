@@ -173,6 +173,9 @@ _SIGS = {
     "apgcu_session_hier_telemetry": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     "apgcu_engine_hier_telemetry": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     "apgcu_kernel_launch_count": (C.c_ulonglong, []),
+    "apgcu_set_experimental": (C.c_int, [C.c_int, C.c_float, C.c_int, C.c_int]),
+    "apgcu_get_experimental": (None, [C.POINTER(C.c_int), C.POINTER(C.c_float), C.POINTER(C.c_int),
+                                      C.POINTER(C.c_int)]),
     "apgcu_image_info": (C.c_int, [C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "apgcu_load_image": (C.c_int, [C.c_char_p, C.c_void_p, C.c_size_t, C.POINTER(C.c_int), C.POINTER(C.c_int),
                                    C.POINTER(C.c_int)]),

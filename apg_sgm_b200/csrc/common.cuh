@@ -42,6 +42,8 @@ struct CostCtx {
     const unsigned long long *cl64, *cr64;
     const int16_t *rmin, *rmax;
     int prior_ranges;  // 0: every pixel has the default range [d0, min(dmax, x+1)); 1: rmin/rmax vary
+    int sp_method = 0;     // sub-pixel method of the right-image WTA (subpixel_delta), 0 = Legacy
+    float sp_param = 0.0f;
     int tile;          // cost kernel tile width (64, 128, 256; 0 = default for Dp)
     int kernel;        // cost kernel: 0 = pixel runs where they apply, 1 = column tiles always
 };
@@ -74,6 +76,30 @@ __device__ __forceinline__ float legacy_delta(float cm, float c0, float cp) {
         return delta;
     }
     return 0.0f;
+}
+
+// SubpixelEstimator::compute_delta without telemetry (src/subpixel_estimator.cpp:58-119), the
+// method an ExperimentalSubpixelScope selects: 0 Legacy, 1 CurvGate (denominator >= param, 4 by
+// default, on a convex triple), 2 ConfGate (uniqueness >= param, 0.05 by default, on a convex
+// triple), 3 Stabilized (denominator + param, 4 by default, when the centre is a minimum).
+// Inputs are integer-valued floats; uniq is the WTA's (second - best) / max(best, 1), 1 elsewhere.
+__device__ __forceinline__ float subpixel_delta(float cm, float c0, float cp, int method, float param, float uniq) {
+    if (method == 0) return legacy_delta(cm, c0, cp);
+    const float denom = __fadd_rn(__fsub_rn(cm, __fmul_rn(2.0f, c0)), cp);
+    const bool non_convex = c0 >= cm || c0 >= cp || denom <= 1e-6f;
+    float den = denom;
+    bool apply;
+    if (method == 1) {
+        apply = !non_convex && denom >= (param > 0.0f ? param : 4.0f);
+    } else if (method == 2) {
+        apply = !non_convex && uniq >= (param > 0.0f ? param : 0.05f);
+    } else {
+        apply = c0 <= cm && c0 <= cp && denom > 0.0f;
+        den = __fadd_rn(denom, param > 0.0f ? param : 4.0f);
+    }
+    if (!apply) return 0.0f;
+    const float raw = __fdiv_rn(__fmul_rn(0.5f, __fsub_rn(cm, cp)), den);
+    return raw < -0.5f ? -0.5f : (0.5f < raw ? 0.5f : raw);
 }
 
 // Exact q = n / d for n < 2^16 and 1 <= d < 2^16 with one high multiply:

@@ -436,7 +436,7 @@ __global__ void right_wta_finalize_kernel(CostCtx c, const uint32_t* __restrict_
                 };
                 uint32_t cm, c0v, cp;
                 if (cost_at(xm, bd - 1, cm) && cost_at(xm + 1, bd, c0v) && cost_at(xp, bd + 1, cp))
-                    dv = __fadd_rn(dv, legacy_delta((float)cm, (float)c0v, (float)cp));
+                    dv = __fadd_rn(dv, subpixel_delta((float)cm, (float)c0v, (float)cp, c.sp_method, c.sp_param, 1.0f));
             }
         }
         disp_right[p] = dv;

@@ -48,6 +48,11 @@ bool u16_path_ok(const apg_pipeline_config_t& c) {
 }  // namespace
 
 void count_launches(unsigned n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+ExperimentalScope& experimental_scope() {
+    static thread_local ExperimentalScope s;
+    return s;
+}
 unsigned long long launch_count() { return g_launches.load(); }
 
 cudaError_t launch_default_range(int w, int h, int d0, int dmax, int16_t* rmin, int16_t* rmax, cudaStream_t s) {
@@ -318,6 +323,8 @@ CostCtx Engine::cost_ctx() const {
     c.cl64 = ptr<unsigned long long>(lay_.cl); c.cr64 = ptr<unsigned long long>(lay_.cr);
     c.rmin = ptr<int16_t>(lay_.rmin); c.rmax = ptr<int16_t>(lay_.rmax);
     c.prior_ranges = ranged() ? 1 : 0;
+    c.sp_method = scope_.sp_method;
+    c.sp_param = scope_.sp_param;
     c.tile = cost_tile_;
     c.kernel = cost_kernel_;
     return c;
@@ -542,6 +549,7 @@ int Engine::run_pre(const uint8_t* dl, int lstride, const uint8_t* dr, int rstri
     const bool prof = (debug_ & 8) != 0;
     (void)D; (void)Dp; (void)d0; (void)n; (void)w; (void)h;
     const int c64 = cfg_.census_type == APG_CENSUS_9X7;
+    scope_ = experimental_scope();
     cudaEventRecord(ev_[0], s);
     {
         const AuxImage li{dl, lstride, ptr<uint8_t>(L.lgray), ptr<uint8_t>(L.lgx), ptr<uint8_t>(L.lgy),
@@ -626,6 +634,8 @@ int Engine::sgm_launch(SgmLaunch* out, uint32_t** sbufs) const {
     pl.cl = ptr<uint32_t>(L.cl); pl.cr = ptr<uint32_t>(L.cr); pl.qlut = ptr<uint16_t>(L.qlut);
     pl.disp = ptr<float>(L.disp_wta); pl.best = ptr<float>(L.best); pl.second = ptr<float>(L.second);
     pl.subpixel = cfg_.subpixel;
+    pl.sp_method = scope_.sp_method;
+    pl.sp_param = scope_.sp_param;
     pl.store_final = (debug_ & 2) != 0;
     pl.lanes = sgm_lanes_;
     for (int i = 0; i < L.nsbuf; ++i) sbufs[i] = ptr<uint32_t>(L.sbuf[i]);
@@ -810,7 +820,10 @@ int Engine::run_post(float* d_disp, float* d_conf, uint8_t* d_reason, uint8_t* d
     // (src/hierarchical_stereo.cpp:262-265); a zero gap would still fill from the neighbours
     const float* med_in = post_in;
     if (!skip_fill_) {
-        RUN(launch_fill(w, h, cfg_.max_fill_gap, post_in, ptr<uint8_t>(L.reason), ptr<uint8_t>(L.lgray),
+        // the inpaint scope's gap replaces max_fill_gap unless it is Legacy at its default 32
+        // (src/postprocess.cpp:45-48)
+        const int gap = (scope_.ip_method == 0 && scope_.ip_gap == 32) ? cfg_.max_fill_gap : scope_.ip_gap;
+        RUN(launch_fill(w, h, gap, scope_.ip_method == 1, post_in, ptr<uint8_t>(L.reason), ptr<uint8_t>(L.lgray),
                         ranged() ? ptr<float>(L.d_prior) : nullptr, ptr<float>(L.disp_fill), s), "fill");
         med_in = ptr<float>(L.disp_fill);
     }
@@ -1164,6 +1177,25 @@ size_t apgcu_engine_allocated_bytes(apgcu_engine_t e) { return e ? e->eng->alloc
 size_t apgcu_workspace_bytes(const apg_pipeline_config_t* cfg, int width, int height) {
     if (!cfg || width <= 0 || height <= 0) return 0;
     return apgcu::Engine::workspace_bytes(*cfg, width, height, 3, 0);
+}
+
+int apgcu_set_experimental(int subpixel_method, float subpixel_param, int inpaint_method, int inpaint_gap) {
+    if (subpixel_method < 0 || subpixel_method > 3 || inpaint_method < 0 || inpaint_method > 1)
+        return apgcu::kInvalidConfig;
+    apgcu::ExperimentalScope& s = apgcu::experimental_scope();
+    s.sp_method = subpixel_method;
+    s.sp_param = subpixel_param;
+    s.ip_method = inpaint_method;
+    s.ip_gap = inpaint_gap;
+    return 0;
+}
+
+void apgcu_get_experimental(int* subpixel_method, float* subpixel_param, int* inpaint_method, int* inpaint_gap) {
+    const apgcu::ExperimentalScope& s = apgcu::experimental_scope();
+    if (subpixel_method) *subpixel_method = s.sp_method;
+    if (subpixel_param) *subpixel_param = s.sp_param;
+    if (inpaint_method) *inpaint_method = s.ip_method;
+    if (inpaint_gap) *inpaint_gap = s.ip_gap;
 }
 
 int apgcu_engine_hier_telemetry(apgcu_engine_t e, double* out6) {

@@ -59,6 +59,18 @@ struct Layout {
     int n_cells = 0, gw = 0, gh = 0, max_cand = 0;
 };
 
+// The experimental scopes of the calling thread (ExperimentalSubpixelScope,
+// src/subpixel_estimator.cpp:7-57; ExperimentalInpaintScope, src/postprocess.cpp:42-53): the
+// sub-pixel method (0 Legacy, 1 CurvGate, 2 ConfGate, 3 Stabilized) with its parameter, and the
+// inpaint method (0 Legacy, 1 ShadowReclass) with its gap.  An engine reads them once per frame.
+struct ExperimentalScope {
+    int sp_method = 0;
+    float sp_param = 0.0f;
+    int ip_method = 0;
+    int ip_gap = 32;
+};
+ExperimentalScope& experimental_scope();
+
 // Refine pass state (u32 words at Layout::rf_state): pass start positions, error flag, progress.
 constexpr int kRefineMaxIter = 63;
 constexpr int kRefineErrWord = 64;
@@ -198,6 +210,7 @@ public:
 private:
     int support_count_ = 0;
     std::unique_ptr<Engine> coarse_;  // hierarchical mode: the half-size engine (same stream)
+    ExperimentalScope scope_;         // the calling thread's experimental scopes, read per frame
     bool skip_fill_ = false;          // coarse engine without coarse_fill_holes: no fill stage
     bool hier_ran_ = false;           // the last frame ran the coarse pass
     unsigned long long counts_[8] = {};  // frame counters copied with the host outputs

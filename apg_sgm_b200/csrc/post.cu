@@ -97,10 +97,18 @@ __global__ void lr_kernel(int w, int h, int lr_max_diff, const float* __restrict
     }
 }
 
-// Legacy hole fill, src/postprocess.cpp:87-168.  Reads the pre-fill map, writes a copy.
-__global__ void fill_kernel(int w, int h, int gap, const float* __restrict__ in, const uint8_t* __restrict__ reason,
-                            const uint8_t* __restrict__ gray, const float* __restrict__ d_prior,
-                            float* __restrict__ out) {
+// ShadowReclass (src/postprocess.cpp:170-192): a mismatch hole between two valid neighbours at least
+// 4 px apart is a depth step's shadow and is filled like an occlusion.
+__device__ __forceinline__ bool occlusion_like(uint8_t r, int shadow, float dl, float dr) {
+    return r == kOcclusion ||
+           (shadow && r == kMismatch && dl >= 0.f && dr >= 0.f && fabsf(__fsub_rn(dr, dl)) >= 4.0f);
+}
+
+// Legacy hole fill, src/postprocess.cpp:87-168 (shadow != 0: the ShadowReclass inpaint,
+// :170-239).  Reads the pre-fill map, writes a copy.
+__global__ void fill_kernel(int w, int h, int gap, int shadow, const float* __restrict__ in,
+                            const uint8_t* __restrict__ reason, const uint8_t* __restrict__ gray,
+                            const float* __restrict__ d_prior, float* __restrict__ out) {
     const int n = w * h;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const float v = in[i];
@@ -114,7 +122,7 @@ __global__ void fill_kernel(int w, int h, int gap, const float* __restrict__ in,
         const float dl = (xl >= 0 && row[xl] >= 0.f) ? row[xl] : -1.f;
         const float dr = (xr < w && row[xr] >= 0.f) ? row[xr] : -1.f;
         float o = v;
-        if (reason[i] == kOcclusion) {
+        if (occlusion_like(reason[i], shadow, dl, dr)) {
             if (dl >= 0.f && dr >= 0.f) o = (dr < dl) ? dr : dl;
             else if (dl >= 0.f) o = dl;
             else if (dr >= 0.f) o = dr;
@@ -191,7 +199,7 @@ __global__ void median_kernel(int w, int h, int r, const float* __restrict__ in,
 // gap.  The nearest stopper on each side comes from the segments' stopper masks (this segment,
 // then further ones while some lane's gap reaches them), so each pixel costs a few bit operations
 // instead of a walk.  Everything after the two neighbours is the per-pixel rule above.
-__global__ void fill_ballot_kernel(int w, int h, int gap, const float* __restrict__ in,
+__global__ void fill_ballot_kernel(int w, int h, int gap, int shadow, const float* __restrict__ in,
                                    const uint8_t* __restrict__ reason, const uint8_t* __restrict__ gray,
                                    const float* __restrict__ d_prior, float* __restrict__ out) {
     const int lane = threadIdx.x & 31;
@@ -249,7 +257,7 @@ __global__ void fill_ballot_kernel(int w, int h, int gap, const float* __restric
         const float dr = (xr < w && row[xr] >= 0.f) ? row[xr] : -1.f;
         const size_t i = (size_t)y * w + x;
         float o = v;
-        if (reason[i] == kOcclusion) {
+        if (occlusion_like(reason[i], shadow, dl, dr)) {
             if (dl >= 0.f && dr >= 0.f) o = (dr < dl) ? dr : dl;
             else if (dl >= 0.f) o = dl;
             else if (dr >= 0.f) o = dr;
@@ -441,14 +449,14 @@ cudaError_t launch_lr(int w, int h, int lr_max_diff, const float* dr, const floa
     return cudaGetLastError();
 }
 
-cudaError_t launch_fill(int w, int h, int gap, const float* in, const uint8_t* reason, const uint8_t* gray,
-                        const float* d_prior, float* out, cudaStream_t s) {
+cudaError_t launch_fill(int w, int h, int gap, int shadow, const float* in, const uint8_t* reason,
+                        const uint8_t* gray, const float* d_prior, float* out, cudaStream_t s) {
     if (gap >= 0) {
         const long long warps = (long long)((w + 31) / 32) * h;
         const int blocks = (int)std::min<long long>((warps + 7) / 8, 148 * 16);
-        fill_ballot_kernel<<<blocks, 256, 0, s>>>(w, h, gap, in, reason, gray, d_prior, out);
+        fill_ballot_kernel<<<blocks, 256, 0, s>>>(w, h, gap, shadow, in, reason, gray, d_prior, out);
     } else {
-        fill_kernel<<<grid_for(w * h), 256, 0, s>>>(w, h, gap, in, reason, gray, d_prior, out);
+        fill_kernel<<<grid_for(w * h), 256, 0, s>>>(w, h, gap, shadow, in, reason, gray, d_prior, out);
     }
     return cudaGetLastError();
 }

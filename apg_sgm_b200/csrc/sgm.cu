@@ -126,6 +126,8 @@ struct SgmArgs {
     float* best;
     float* second;
     int subpixel;
+    int sp_method;
+    float sp_param;
     int store_final;
 };
 
@@ -243,7 +245,11 @@ __device__ __forceinline__ void wta(const SgmArgs& a, unsigned gmask, int j, int
             if (a.subpixel && bdi > 0 && bdi + 1 < a.D) {
                 const uint32_t cm = (vm_w >> (16 * ((bdi - 1) & 1))) & 0xFFFFu;
                 const uint32_t cp = (vp_w >> (16 * ((bdi + 1) & 1))) & 0xFFFFu;
-                if (cm < kInf && cp < kInf) dval = __fadd_rn(dval, legacy_delta((float)cm, (float)bv, (float)cp));
+                if (cm < kInf && cp < kInf) {
+                    // WTA uniqueness (src/sgm_optimizer.cpp:520-525): (second - best) / max(best, 1)
+                    const float u = sec >= kInf ? 1.0f : __fdiv_rn((float)(sec - bv), (float)max(bv, 1u));
+                    dval = __fadd_rn(dval, subpixel_delta((float)cm, (float)bv, (float)cp, a.sp_method, a.sp_param, u));
+                }
             }
             fb = (float)bv;
             fs = sec >= kInf ? __int_as_float(0x7f800000) : (float)sec;
@@ -520,10 +526,6 @@ __device__ __forceinline__ void wta_row(const SgmArgs& a, const uint32_t* row, i
         if (a.d0 + bdi >= 0) {
             const uint16_t* r16 = reinterpret_cast<const uint16_t*>(row);
             dval = (float)(a.d0 + bdi);
-            if (a.subpixel && bdi > 0 && bdi + 1 < a.D) {
-                const uint32_t cm = r16[bdi - 1], cp = r16[bdi + 1];
-                if (cm < kInf && cp < kInf) dval = __fadd_rn(dval, legacy_delta((float)cm, (float)m, (float)cp));
-            }
             // second minimum outside |d - best| <= 1: chunks without an excluded halfword keep
             // their minimum; the (at most two) chunks with one are read again with those masked
             const int klo = bdi > 0 ? (bdi - 1) >> 1 : 0, khi = min((bdi + 1) >> 1, W2 - 1);
@@ -542,6 +544,14 @@ __device__ __forceinline__ void wta_row(const SgmArgs& a, const uint32_t* row, i
                 }
             }
             const uint32_t sec = min_halves(sec2);
+            if (a.subpixel && bdi > 0 && bdi + 1 < a.D) {
+                const uint32_t cm = r16[bdi - 1], cp = r16[bdi + 1];
+                if (cm < kInf && cp < kInf) {
+                    // WTA uniqueness (src/sgm_optimizer.cpp:520-525): (second - best) / max(best, 1)
+                    const float u = sec >= kInf ? 1.0f : __fdiv_rn((float)(sec - m), (float)max(m, 1u));
+                    dval = __fadd_rn(dval, subpixel_delta((float)cm, (float)m, (float)cp, a.sp_method, a.sp_param, u));
+                }
+            }
             fb = (float)m;
             fs = sec >= kInf ? __int_as_float(0x7f800000) : (float)sec;
         }
@@ -1037,6 +1047,8 @@ SgmArgs make_args(const SgmLaunch& l) {
     a.pen = l.pen; a.gray = l.gray; a.cvol = l.cvol; a.cl = l.cl; a.cr = l.cr; a.qlut = l.qlut;
     a.disp = l.disp; a.best = l.best; a.second = l.second;
     a.subpixel = l.subpixel;
+    a.sp_method = l.sp_method;
+    a.sp_param = l.sp_param;
     a.store_final = l.store_final;
     return a;
 }

@@ -106,6 +106,18 @@ APGCU_API void* apgcu_engine_stream(apgcu_engine_t e);
  * under 32 x 32 or with hierarchical mode off)}.  Waits for the engine stream. */
 APGCU_API int apgcu_engine_hier_telemetry(apgcu_engine_t e, double* out6);
 
+/* Experimental scopes of the CALLING THREAD (ExperimentalSubpixelScope, src/subpixel_estimator.hpp;
+ * ExperimentalInpaintScope, src/inpaint_internal.hpp), read by every engine, session and batch call
+ * made on that thread when it starts a frame: subpixel_method 0 Legacy, 1 CurvGate, 2 ConfGate,
+ * 3 Stabilized with its parameter (<= 0: the method's default); inpaint_method 0 Legacy,
+ * 1 ShadowReclass with its gap (Legacy at 32 keeps the configuration's max_fill_gap).  Defaults
+ * (0, 0, 0, 32) reproduce the reference without scopes.  The scopes' telemetry counters are not
+ * part of this library; the allocation-free right-image WTA always uses Legacy.  Returns 0 or
+ * APG_STATUS_INVALID_CONFIG for an unknown method. */
+APGCU_API int apgcu_set_experimental(int subpixel_method, float subpixel_param, int inpaint_method, int inpaint_gap);
+APGCU_API void apgcu_get_experimental(int* subpixel_method, float* subpixel_param, int* inpaint_method,
+                                      int* inpaint_gap);
+
 /* PipelineConfig::from_mode (src/config.cpp:5-45) into *out. */
 APGCU_API void apgcu_config_from_mode(int mode, int max_disparity, apg_pipeline_config_t* out);
 

@@ -377,7 +377,39 @@ static float legacy_delta(float cm, float c0, float cp) {
     return 0.0f;
 }
 
-/* wta_impl<uint32_t>, src/sgm_optimizer.cpp:436-555 (Legacy subpixel, no telemetry). */
+/* Experimental scopes (ExperimentalSubpixelScope, src/subpixel_estimator.cpp:7-57;
+ * ExperimentalInpaintScope, src/postprocess.cpp:42-53), process-wide in the oracle. */
+static int g_sp_method = 0, g_ip_method = 0, g_ip_gap = 32;
+static float g_sp_param = 0.0f;
+
+void orc_set_experimental(int sp_method, float sp_param, int ip_method, int ip_gap) {
+    g_sp_method = sp_method;
+    g_sp_param = sp_param;
+    g_ip_method = ip_method;
+    g_ip_gap = ip_gap;
+}
+
+/* SubpixelEstimator::compute_delta without telemetry, src/subpixel_estimator.cpp:58-119. */
+static float sp_delta(float cm, float c0, float cp, float uniq) {
+    if (g_sp_method == 0) return legacy_delta(cm, c0, cp);
+    const float denom = cm - 2.0f * c0 + cp;
+    const int non_convex = c0 >= cm || c0 >= cp || denom <= 1e-6f;
+    float raw;
+    if (g_sp_method == 1) {
+        if (non_convex || !(denom >= (g_sp_param > 0.0f ? g_sp_param : 4.0f))) return 0.0f;
+        raw = 0.5f * (cm - cp) / denom;
+    } else if (g_sp_method == 2) {
+        if (non_convex || !(uniq >= (g_sp_param > 0.0f ? g_sp_param : 0.05f))) return 0.0f;
+        raw = 0.5f * (cm - cp) / denom;
+    } else {
+        if (!(c0 <= cm && c0 <= cp && denom > 0.0f)) return 0.0f;
+        raw = 0.5f * (cm - cp) / (denom + (g_sp_param > 0.0f ? g_sp_param : 4.0f));
+    }
+    return raw < -0.5f ? -0.5f : (0.5f < raw ? 0.5f : raw);
+}
+
+/* wta_impl<uint32_t>, src/sgm_optimizer.cpp:436-555 (sub-pixel step as the scope selects, no
+ * telemetry). */
 void orc_wta(const apg_pipeline_config_t* cfg, const uint32_t* acc, const int16_t* rmin,
              const int16_t* rmax, int w, int h, float* disp, float* best_out, float* second_out) {
     const int d0 = cfg->min_disparity, D = cfg->max_disparity - cfg->min_disparity;
@@ -414,8 +446,11 @@ void orc_wta(const apg_pipeline_config_t* cfg, const uint32_t* acc, const int16_
                 const int di = best_d - d0;
                 if (di > 0 && di + 1 < D) {
                     const uint32_t cm = s[di - 1], c0 = s[di], cp = s[di + 1];
-                    if (cm != ORC_INVALID_COST32 && cp != ORC_INVALID_COST32)
-                        dval += legacy_delta((float)cm, (float)c0, (float)cp);
+                    if (cm != ORC_INVALID_COST32 && cp != ORC_INVALID_COST32) {
+                        float u = 1.0f;
+                        if (second < UINT64_MAX) u = (float)(second - best) / (float)(best > 1 ? best : 1);
+                        dval += sp_delta((float)cm, (float)c0, (float)cp, u);
+                    }
                 }
             }
             disp[i] = dval;
@@ -450,7 +485,7 @@ void orc_wta_right(const apg_pipeline_config_t* cfg, const uint16_t* vol, int w,
                         const uint16_t c0 = vol[((size_t)y * w + x0) * D + di];
                         const uint16_t cp = vol[((size_t)y * w + xp) * D + di + 1];
                         if (cm != ORC_INVALID_COST && c0 != ORC_INVALID_COST && cp != ORC_INVALID_COST)
-                            dval += legacy_delta((float)cm, (float)c0, (float)cp);
+                            dval += sp_delta((float)cm, (float)c0, (float)cp, 1.0f);
                     }
                 }
             }
@@ -585,7 +620,8 @@ void orc_lr_check(const apg_pipeline_config_t* cfg, int w, int h, const float* d
 /* PostProcessor::fill_holes, Legacy route, src/postprocess.cpp:42-168 and :252. */
 void orc_fill_holes(const apg_pipeline_config_t* cfg, int w, int h, const float* in,
                     const uint8_t* reason, const uint8_t* lgray, const float* d_prior, float* out) {
-    const int gap = cfg->max_fill_gap;
+    /* the inpaint scope's gap replaces max_fill_gap unless it is Legacy at 32 (postprocess.cpp:45-48) */
+    const int gap = (g_ip_method == 0 && g_ip_gap == 32) ? cfg->max_fill_gap : g_ip_gap;
     memcpy(out, in, sizeof(float) * (size_t)w * h);
     for (int y = 0; y < h; ++y) {
         for (int x = 0; x < w; ++x) {
@@ -597,7 +633,11 @@ void orc_fill_holes(const apg_pipeline_config_t* cfg, int w, int h, const float*
             while (xr < w && xr <= x + gap && in[y * w + xr] < 0.f) ++xr;
             const float dl = (xl >= 0 && in[y * w + xl] >= 0.f) ? in[y * w + xl] : -1.f;
             const float dr = (xr < w && in[y * w + xr] >= 0.f) ? in[y * w + xr] : -1.f;
-            if (reason[i] == ORC_OCCLUSION) {
+            /* ShadowReclass (postprocess.cpp:170-192): a mismatch between valid neighbours >= 4 px
+             * apart is filled like an occlusion */
+            const int shadow = g_ip_method == 1 && reason[i] == ORC_MISMATCH && dl >= 0.f && dr >= 0.f &&
+                               fabsf(dr - dl) >= 4.0f;
+            if (reason[i] == ORC_OCCLUSION || shadow) {
                 if (dl >= 0.f && dr >= 0.f) out[i] = fminf_ref(dl, dr);
                 else if (dl >= 0.f) out[i] = dl;
                 else if (dr >= 0.f) out[i] = dr;

@@ -437,6 +437,16 @@ def ref_save(kind: str, path, arr, dmax: float = 0.0) -> int:
     return int(f(*args))
 
 
+def set_experimental(sp_method: int = 0, sp_param: float = 0.0, ip_method: int = 0, ip_gap: int = 32,
+                     reference: bool = False):
+    """The experimental scopes (sub-pixel method/param, inpaint method/gap) of the oracle, or with
+    reference=True the reference's own scopes on the calling thread."""
+    if reference:
+        ref_lib().ref_set_experimental(C.c_int(sp_method), C.c_float(sp_param), C.c_int(ip_method), C.c_int(ip_gap))
+    else:
+        lib().orc_set_experimental(C.c_int(sp_method), C.c_float(sp_param), C.c_int(ip_method), C.c_int(ip_gap))
+
+
 class RefSession:
     """The reference's public StereoSession (BoundedReuse) for timing its CPU path."""
 

@@ -23,6 +23,8 @@
 #include "apg_sgm/sgm_optimizer.hpp"
 #include "apg_sgm/metrics.hpp"
 #include "hierarchical_stereo.hpp"
+#include "inpaint_internal.hpp"
+#include "subpixel_estimator.hpp"
 
 #include "../include/apg_sgm/metrics.h"
 #include "../include/apg_sgm/pipeline_config.h"
@@ -30,6 +32,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cstring>
+#include <memory>
 #include <vector>
 
 #if defined(_OPENMP)
@@ -470,6 +473,18 @@ int ref_save_pfm(const char* path, const float* d, int w, int h) {
     Image32f im(w, h);
     std::memcpy(im.data(), d, static_cast<size_t>(w) * h * sizeof(float));
     return save_pfm(path, im) ? 1 : 0;
+}
+
+// The reference's experimental scopes on the calling thread, kept open until the next call
+// (defaults 0, 0, 0, 32 restore the reference's production behaviour).
+static std::unique_ptr<ExperimentalInpaintScope> g_ip_scope;
+static std::unique_ptr<ExperimentalSubpixelScope> g_sp_scope;
+
+void ref_set_experimental(int sp_method, float sp_param, int ip_method, int ip_gap) {
+    g_ip_scope.reset();
+    g_sp_scope.reset();
+    g_sp_scope.reset(new ExperimentalSubpixelScope(static_cast<SubpixelMethod>(sp_method), sp_param, false));
+    g_ip_scope.reset(new ExperimentalInpaintScope(static_cast<InpaintMethod>(ip_method), ip_gap, false));
 }
 
 // Public-API session used for timing the reference CPU path.
