@@ -67,6 +67,7 @@ struct Bucket {
     cudaEvent_t done = nullptr;               // end of the bucket's last call (timing)
     Tuning tune;
     bool tuned = false;
+    ExperimentalScope scope;  // the experimental scopes the bucket's plans and graphs were built under
 };
 
 // process-wide tuning cache, keyed "mode W H D"
@@ -434,6 +435,14 @@ int Batch::process(int n, const apgcu_pair_t* pairs, bool device_buffers) {
             rc = b.slots[k]->upload(p.left, p.right, p.width, p.height, p.stride, p.channels, device_buffers, b.stream);
             if (rc) return fail(rc, b.slots[k]->last_error());
         }
+        // plans and graphs hold the kernels' arguments, the experimental scopes among them: a call
+        // under other scopes than the cached ones rebuilds them
+        const ExperimentalScope cur = experimental_scope();
+        if (!same_scope(cur, b.scope)) {
+            drop_plans(b);
+            b.scope = cur;
+        }
+        for (int k = 0; k < m; ++k) b.slots[k]->capture_scope();
         const int Dp = round_up(b.key.dmax - b.cfg.min_disparity, 64);
         SgmLaunch probe;
         uint32_t* s7[7];

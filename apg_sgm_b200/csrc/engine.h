@@ -70,6 +70,10 @@ struct ExperimentalScope {
     int ip_gap = 32;
 };
 ExperimentalScope& experimental_scope();
+inline bool same_scope(const ExperimentalScope& a, const ExperimentalScope& b) {
+    return a.sp_method == b.sp_method && a.sp_param == b.sp_param && a.ip_method == b.ip_method &&
+           a.ip_gap == b.ip_gap;
+}
 
 // Refine pass state (u32 words at Layout::rf_state): pass start positions, error flag, progress.
 constexpr int kRefineMaxIter = 63;
@@ -135,6 +139,9 @@ public:
     void set_fast_fused(bool on) { fast_fused_ = on; }
     void set_cost_tile(int t) { cost_tile_ = t; }
     void set_cost_kernel(int k) { cost_kernel_ = k; }
+    // takes the calling thread's experimental scopes now (run_pre does so for every frame; the
+    // batched form needs them before it builds SGM plans from sgm_launch)
+    void capture_scope() { scope_ = experimental_scope(); }
     int debug() const { return debug_; }
     const apg_pipeline_config_t& config() const { return cfg_; }
     int device() const { return device_; }
