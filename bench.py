@@ -46,6 +46,21 @@ WORKLOADS = {
 MODE_NAMES = {0: "Fast", 1: "Balanced", 2: "HighQuality"}
 
 
+_SP_NAMES = {"legacy": 0, "curv_gate": 1, "conf_gate": 2, "stabilized": 3}
+_IP_NAMES = {"legacy": 0, "shadow_reclass": 1}
+
+
+def _scope_of(args):
+    """(sp_method, sp_param, ip_method, ip_gap) from --subpixel NAME[:PARAM] and --inpaint NAME[:GAP]."""
+    sp, _, spp = args.subpixel.partition(":")
+    ip, _, ipg = args.inpaint.partition(":")
+    return _SP_NAMES[sp], float(spp or 0.0), _IP_NAMES[ip], int(ipg or 32)
+
+
+def _scope_label(args) -> dict:
+    return {} if _scope_of(args) == (0, 0.0, 0, 32) else {"subpixel": args.subpixel, "inpaint": args.inpaint}
+
+
 def metric_name(mode: int, w: int, h: int, D: int, over=None) -> str:
     kind = f"{MODE_NAMES[mode]}, hierarchical" if (over or {}).get("hier_enable") else MODE_NAMES[mode]
     return f"W*H*D/s at {w}x{h} D={D} ({kind}, bit-exact)"
@@ -160,6 +175,7 @@ def run_reference(args, wl):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libapg_ref.so not built"}))
         return
     cfg = O.config(mode, spec.max_disparity, volume_backend=2, **over)  # Packed: the AVX2/OpenMP path
+    O.set_experimental(*_scope_of(args), reference=True)  # the reference's scopes on this thread
     sess = O.RefSession(cfg, bounded_reuse=True)
     for _ in range(args.warmup):
         sess.process(L, R)
@@ -179,7 +195,7 @@ def run_reference(args, wl):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": "synthetic",
         "config": {"workload": label, "mode": MODE_NAMES[mode], "width": spec.width, "height": spec.height,
-                   "max_disparity": spec.max_disparity, "backend": "Packed (AVX2/OpenMP)"},
+                   "max_disparity": spec.max_disparity, "backend": "Packed (AVX2/OpenMP)", **_scope_label(args)},
         "cpu_baseline": {"value": value, "unit": "voxels/s", "cores": cores, "kind": "reference",
                          "sample": f"{args.steps} pairs {spec.width}x{spec.height} D{spec.max_disparity} "
                                    f"{MODE_NAMES[mode]}, reference StereoSession Packed backend"},
@@ -459,6 +475,10 @@ def run_b200(args, wl):
     mode, spec_args, label, over = wl
     spec = S.PairSpec(*spec_args)
     w, h, D = spec.width, spec.height, spec.max_disparity
+    # experimental scopes (ExperimentalSubpixelScope / ExperimentalInpaintScope) of this thread: every
+    # frame below, device, e2e and Python binding alike, runs under them
+    from apg_sgm_b200 import _lib as _scope_lib
+    _scope_lib.lib().apgcu_set_experimental(*_scope_of(args))
     Dp = (D + 63) // 64 * 64
     npairs = 2
     # host images in page-locked memory: the end-to-end leg uploads them from there every step
@@ -601,7 +621,7 @@ def run_b200(args, wl):
         "vs_baseline": None, "dtype": "u16", "data": "synthetic",
         "config": {"workload": label, "mode": MODE_NAMES[mode], "width": w, "height": h, "max_disparity": D,
                    "pairs_per_step": 1, "distinct_pairs": npairs, "l2": "flushed between steps (256 MiB write)",
-                   "parallelism": f"replicas x{world}"},
+                   "parallelism": f"replicas x{world}", **_scope_label(args)},
         "e2e": {"value": e2e_value, "unit": "voxels/s", "h2d_bytes_per_step": 2 * w * h,
                 "d2h_bytes_per_step": w * h * 10 + 64, "api": "apg_session_process (C API, BoundedReuse)" + (
                     "; session from apgcu_session_create_config" if over else ""),
@@ -612,6 +632,10 @@ def run_b200(args, wl):
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         gpu0 = eng.process(*pairs[0])
+        from oracle import oracle as O
+        if O.ref_available():
+            O.set_experimental(*_scope_of(args), reference=True)
+        O.set_experimental(*_scope_of(args))
         cb, parity = cpu_baseline(spec, mode, pairs[0][0], pairs[0][1], gpu0, over)
         out["cpu_baseline"] = cb
         out["parity_vs_cpu_baseline"] = "bit-exact" if parity else "MISMATCH"
@@ -1082,6 +1106,11 @@ def main():
     ap.add_argument("--rates", default="50,100,200,400,600", help="served: Poisson arrival rates, pairs/s")
     ap.add_argument("--slots", type=int, default=4, help="served: requests in flight")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--subpixel", default="legacy",
+                    help="ExperimentalSubpixelScope for the single-pair workloads: legacy | curv_gate | conf_gate | "
+                         "stabilized, optionally :PARAM")
+    ap.add_argument("--inpaint", default="legacy",
+                    help="ExperimentalInpaintScope for the single-pair workloads: legacy | shadow_reclass, optionally :GAP")
     args = ap.parse_args()
     if args.workload == "served":
         if args.impl == "reference":
