@@ -314,7 +314,7 @@ def main(argv=None) -> int:
                     help="accepted for compatibility: every backend runs the CUDA engine")
     ap.add_argument("--packed", action="store_true", help="accepted for compatibility")
     ap.add_argument("--hierarchical", action="store_true")
-    ap.add_argument("--hierarchical-radius", type=int, default=4)
+    ap.add_argument("--hierarchical-radius", type=int, default=8)  # the runner's default (not the config's 4)
     ap.add_argument("--hierarchical-fallback", default="nearest_valid", choices=sorted(_FB_PARSE))
     ap.add_argument("--hierarchical-no-cross", action="store_true")
     ap.add_argument("--hierarchical-no-fill", action="store_true")
@@ -322,12 +322,14 @@ def main(argv=None) -> int:
     ap.add_argument("--hierarchical-confidence-threshold", type=float, default=0.5)
     ap.add_argument("--hierarchical-expanded-radius", type=int, default=8)
     ap.add_argument("--subpixel-method", default="legacy", choices=sorted(_SP_PARSE))
-    ap.add_argument("--subpixel-param", type=float, default=0.0)
+    ap.add_argument("--subpixel-param", type=float, default=None)
     ap.add_argument("--inpaint-method", default="legacy", choices=sorted(_IP_PARSE))
     ap.add_argument("--inpaint-gap", type=lambda v: max(1, int(v)), default=32)
     for flag in ("--verify-backends", "--subpixel-telem", "--inpaint-telem"):
         ap.add_argument(flag, action="store_true", help="not part of the CUDA backend")
     args = ap.parse_args(argv)
+    if args.subpixel_param is None:  # the method's default parameter (apps/benchmark_stereo.cpp:265-273)
+        args.subpixel_param = {1: 4.0, 2: 0.05, 3: 4.0}.get(_SP_PARSE[args.subpixel_method], 0.0)
     for flag in ("verify_backends", "subpixel_telem", "inpaint_telem"):
         if getattr(args, flag):
             print(f"Error: --{flag.replace('_', '-')} is not part of the CUDA backend", file=sys.stderr)

@@ -33,7 +33,9 @@ def _manifest(apg, d):
 
 
 @pytest.mark.parametrize("extra", [[], ["--subpixel-method", "conf_gate", "--inpaint-method", "shadow_reclass",
-                                        "--inpaint-gap", "12"]], ids=["default", "scopes"])
+                                        "--inpaint-gap", "12"],
+                                   ["--hierarchical", "--hierarchical-adaptive", "--hierarchical-fallback", "expanded"]],
+                         ids=["default", "scopes", "hierarchical"])
 def test_runner_matches_reference_runner(O, apg, tmp_path, extra):
     exe = O.HERE / "_ref" / "benchmark_stereo"
     if not exe.exists():
