@@ -502,6 +502,17 @@ class Engine:
         if rc != 0:
             raise RuntimeError(self.last_error)
 
+    def supports(self):
+        """The prior's selected supports of the last pair in the reference's order
+        (PipelineBuffers::supports): x, y (int32), disparity, confidence (float32) arrays."""
+        n = lib().apgcu_engine_supports(self._h, None, None, None, None, 0)
+        if n < 0:
+            raise RuntimeError(self.last_error)
+        x, y = np.empty(n, np.int32), np.empty(n, np.int32)
+        d, c = np.empty(n, np.float32), np.empty(n, np.float32)
+        lib().apgcu_engine_supports(self._h, x.ctypes.data, y.ctypes.data, d.ctypes.data, c.ctypes.data, n)
+        return x, y, d, c
+
     def hier_telemetry(self) -> dict:
         """HierarchicalTelemetry of the last pair (apgcu_engine_hier_telemetry)."""
         return _hier_dict(lib().apgcu_engine_hier_telemetry, self._h)
@@ -851,6 +862,25 @@ class ExperimentalInpaintScope:
         return False
 
 
+SupportMetrics = _lib_mod.SupportMetricsRec
+
+
+def evaluate_supports(supports, gt, vis_mask=None, max_valid_gt: float = 1e5, cell_size: int = 16) -> SupportMetrics:
+    """evaluate_supports (src/metrics.cpp:8-124) on the GPU: supports = (x, y, disparity[, ...])
+    arrays (Engine.supports()), gt HxW float32, vis_mask HxW uint8 (>= 200 visible) or None."""
+    x, y, d = (np.ascontiguousarray(a, t) for a, t in zip(supports[:3], (np.int32, np.int32, np.float32)))
+    gt = np.ascontiguousarray(gt, np.float32)
+    h, w = gt.shape
+    vis = None if vis_mask is None else np.ascontiguousarray(vis_mask, np.uint8)
+    out = SupportMetrics()
+    rc = lib().apgcu_evaluate_supports(x.ctypes.data, y.ctypes.data, d.ctypes.data, len(x), gt.ctypes.data, w, h,
+                                       None if vis is None else vis.ctypes.data, C.c_float(max_valid_gt),
+                                       int(cell_size), 0, None, C.byref(out))
+    if rc != 0:
+        raise RuntimeError(f"evaluate_supports failed [{rc}]")
+    return out
+
+
 def workspace_bytes(config: PipelineConfig, width: int, height: int) -> int:
     return int(lib().apgcu_workspace_bytes(C.byref(config), int(width), int(height)))
 
@@ -858,7 +888,7 @@ def workspace_bytes(config: PipelineConfig, width: int, height: int) -> int:
 __all__ = ["QualityMode", "HierarchicalFallback", "VolumeBackend", "MemoryPolicy", "StatusCode", "InvalidReason", "StageTiming",
            "PipelineStats", "StereoResult", "StereoSession", "PipelineConfig", "config_from_mode", "Engine",
            "kernel_launch_count", "workspace_bytes", "evaluate_stereo", "StereoMetrics", "RegionMetrics",
-           "load_image", "save_pgm", "save_pgm16", "save_disparity_preview", "load_pfm", "save_pfm", "Loader",
+           "evaluate_supports", "SupportMetrics", "load_image", "save_pgm", "save_pgm16", "save_disparity_preview", "load_pfm", "save_pfm", "Loader",
            "serve_files", "SubpixelMethod", "InpaintMethod", "ExperimentalSubpixelScope", "ExperimentalInpaintScope",
            "__version__"]
 

@@ -92,6 +92,21 @@ class StereoMetricsRec(C.Structure):
         return d
 
 
+_SUPPORT_INT = ["total", "gt_valid", "visible", "correct_05", "correct_1", "correct_2", "visible_correct_05",
+                "visible_correct_1", "visible_correct_2", "visible_gt_cells", "correct_visible_cells"]
+_SUPPORT_FLOAT = ["precision_05", "precision_1", "precision_2", "precision_all_05", "precision_all_1",
+                  "precision_all_2", "precision_vis_05", "precision_vis_1", "precision_vis_2", "mean_abs_error",
+                  "mae_all", "mae_visible", "grid_recall_1", "grid_coverage", "support_grid_recall_vis_1"]
+
+
+class SupportMetricsRec(C.Structure):
+    """apg_support_metrics_t (include/apg_sgm/metrics.h): SupportMetrics."""
+    _fields_ = [(k, C.c_int) for k in _SUPPORT_INT] + [(k, C.c_float) for k in _SUPPORT_FLOAT]
+
+    def to_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class ImageView(C.Structure):
     """apg_image_view_t (include/apg_sgm/c_api.h)."""
     _fields_ = [("data", C.c_void_p), ("width", C.c_int), ("height", C.c_int),
@@ -173,6 +188,10 @@ _SIGS = {
     "apgcu_session_hier_telemetry": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     "apgcu_engine_hier_telemetry": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     "apgcu_kernel_launch_count": (C.c_ulonglong, []),
+    "apgcu_evaluate_supports": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int,
+                                          C.c_void_p, C.c_float, C.c_int, C.c_int, C.c_void_p,
+                                          C.POINTER(SupportMetricsRec)]),
+    "apgcu_engine_supports": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
     "apgcu_set_experimental": (C.c_int, [C.c_int, C.c_float, C.c_int, C.c_int]),
     "apgcu_get_experimental": (None, [C.POINTER(C.c_int), C.POINTER(C.c_float), C.POINTER(C.c_int),
                                       C.POINTER(C.c_int)]),

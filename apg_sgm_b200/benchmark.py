@@ -10,10 +10,10 @@ starting with '#' are skipped, relative paths are taken from the manifest's dire
 (make_ablation_config, src/ablation.cpp) the pair runs `--warmup` times, then `--repeat` timed
 times through a BoundedReuse session; the median run by host time is reported, its accuracy
 scored against the ground truth with evaluate_stereo on the GPU.  The CSV has the reference's
-columns in the reference's order and number formats.  Columns this backend does not compute are
-written as the reference writes them when it does not collect them: the support-match metrics (the
-reference fills them for the prior presets with ground truth; here they stay zero) and the
-sub-pixel / inpaint telemetry counters.  `backend` is `cuda`.
+columns in the reference's order and number formats, the prior presets' support-match block from
+the engine's supports (evaluate_supports on the GPU).  The sub-pixel / inpaint telemetry counters
+are not computed by this backend and are written as the reference writes them when it does not
+collect them.  `backend` is `cuda`.
 """
 from __future__ import annotations
 
@@ -27,7 +27,7 @@ from pathlib import Path
 import numpy as np
 
 from . import (ExperimentalInpaintScope, ExperimentalSubpixelScope, StereoSession, config_from_mode, evaluate_stereo,
-               load_image, load_pfm, save_disparity_preview, save_pfm, save_pgm)
+               evaluate_supports, load_image, load_pfm, save_disparity_preview, save_pfm, save_pgm)
 from ._lib import PipelineConfig
 
 ABLATIONS = ["A", "B", "C", "D", "E", "F", "G"]
@@ -217,7 +217,7 @@ def run(args) -> int:
                 samples.sort(key=lambda s: s[0])
                 total_ms, res, htel = samples[args.repeat // 2]
                 st = res.stats
-                m = None
+                m = sm = None
                 if has_gt:
                     # the frame's ranges and refine maps come from an engine run of the same pair
                     from . import Engine
@@ -226,9 +226,12 @@ def run(args) -> int:
                     rng = (e.dump("range_min"), e.dump("range_max")) if (cfg.prior_enable or args.hierarchical) else None
                     before = e.dump("disp_wta") if cfg.refine_enable else None
                     after = e.dump("disp_refined") if cfg.refine_enable else None
+                    sup = e.supports() if cfg.prior_enable else None
                     e.close()
                     m = evaluate_stereo(res.disparity, gt, rng, before, after, vis, 1e5, left)
-            rows.append(_row(args, c, aid, cfg, w, h, m, st, total_ms, htel, sp_method, ip_method))
+                    if sup is not None and len(sup[0]) > 0:  # has_supports: the prior's list is not empty
+                        sm = evaluate_supports(sup, gt, vis, 1e5)
+            rows.append(_row(args, c, aid, cfg, w, h, m, sm, st, total_ms, htel, sp_method, ip_method))
             z = m if m is not None else None
             print(f"[{aid}] {_DESC[aid]:32s} | EPE: {(z.epe if z else -1.0):6.3f} | "
                   f"Bad2.0: {(z.bad_2_0 if z else -1.0):5.1f}% | D1-all: {(z.kitti_d1_all if z else -1.0):5.1f}% | "
@@ -248,7 +251,7 @@ def run(args) -> int:
     return 0
 
 
-def _row(args, c, aid, cfg, w, h, m, st, total_ms, htel, sp_method, ip_method) -> str:
+def _row(args, c, aid, cfg, w, h, m, sm, st, total_ms, htel, sp_method, ip_method) -> str:
     has = m is not None
     z = lambda k: getattr(m, k) if has else 0.0  # noqa: E731
     cost = "Census+AD+Grad" if (cfg.use_ad or cfg.use_grad) else "Census"
@@ -268,7 +271,17 @@ def _row(args, c, aid, cfg, w, h, m, st, total_ms, htel, sp_method, ip_method) -
               f"{_f(np.float32(m.prior_miss_nonedge_ratio) * np.float32(100.0), 2)},")
     else:
         r += "N/A,N/A,N/A,0,0,0,0,0,0.00,0.00,"
-    r += f"{st.prior_support_count},0.0,0.0,0.0,0.0,0.0,0.0,0.0,0,0,0,0,0,0,0,0,0,0,0.0,0.0,0.0,"
+    if cfg.prior_enable and has and sm is not None:
+        r += (f"{st.prior_support_count},"
+              + ",".join(_f(getattr(sm, k), 4) for k in ("precision_all_05", "precision_all_1", "precision_all_2",
+                                                         "precision_vis_1", "precision_vis_05", "precision_vis_1",
+                                                         "precision_vis_2")) + ","
+              + ",".join(str(getattr(sm, k)) for k in ("gt_valid", "visible", "correct_05", "correct_1", "correct_2",
+                                                       "visible_correct_05", "visible_correct_1", "visible_correct_2",
+                                                       "visible_gt_cells", "correct_visible_cells")) + ","
+              + ",".join(_f(getattr(sm, k), 4) for k in ("mae_all", "mae_visible", "grid_recall_1")) + ",")
+    else:
+        r += f"{st.prior_support_count},0.0,0.0,0.0,0.0,0.0,0.0,0.0,0,0,0,0,0,0,0,0,0,0,0.0,0.0,0.0,"
     D = cfg.max_disparity - cfg.min_disparity
     geom = 1.0 - st.mean_geometry_width / D if D > 0 else 0.0
     incr = (1.0 - st.mean_search_width / st.mean_geometry_width) if st.mean_geometry_width > 0 else 0.0

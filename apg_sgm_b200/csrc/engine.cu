@@ -886,6 +886,49 @@ int Engine::run_hier() {
 #undef RUN
 #undef RUNC
 
+int Engine::supports(std::vector<SupportOut>& out) {
+    out.clear();
+    if (!arena_ || !prior_runs() || lay_.n_cells == 0) return kOk;
+    const int nc = lay_.n_cells, mc = lay_.max_cand;
+    std::vector<int> ncand(nc), taken(nc);
+    std::vector<SupportOut> cand((size_t)nc * mc);
+    static_assert(sizeof(SupportOut) == 16, "device Support record: int x, y; float d, conf");
+    cudaError_t e = cudaMemcpyAsync(ncand.data(), arena_ + lay_.pr_ncand, nc * 4, cudaMemcpyDeviceToHost, stream_);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(taken.data(), arena_ + lay_.pr_taken, nc * 4, cudaMemcpyDeviceToHost, stream_);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(cand.data(), arena_ + lay_.pr_cand, cand.size() * 16, cudaMemcpyDeviceToHost, stream_);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+    if (e != cudaSuccess) return cuda_fail(e, "supports");
+    // the selection order of extract_supports: pass 1 (each non-empty cell's base quota), then
+    // round-robin rounds; or, with more non-empty cells than the budget, one per sampled cell
+    std::vector<int> ne;
+    for (int ci = 0; ci < nc; ++ci)
+        if (ncand[ci] > 0) ne.push_back(ci);
+    const int hard_max = cfg_.prior_max_supports;
+    auto emit = [&](int ci, int k) { out.push_back(cand[(size_t)ci * mc + k]); };
+    if ((int)ne.size() <= hard_max) {
+        const int bq = std::max(1, hard_max / std::max(1, (int)ne.size()));
+        std::vector<int> q1(nc, 0);
+        for (int ci : ne) {
+            q1[ci] = std::min(std::min(bq, ncand[ci]), taken[ci]);
+            for (int k = 0; k < q1[ci]; ++k) emit(ci, k);
+        }
+        for (int r = 0;; ++r) {
+            bool any = false;
+            for (int ci : ne)
+                if (taken[ci] > q1[ci] + r) {
+                    emit(ci, q1[ci] + r);
+                    any = true;
+                }
+            if (!any) break;
+        }
+    } else {
+        for (int ci : ne)
+            if (taken[ci] > 0) emit(ci, 0);
+    }
+    return kOk;
+}
+
 int Engine::hier_telemetry(double* out6) {
     for (int i = 0; i < 6; ++i) out6[i] = 0.0;
     if (!arena_ || !cfg_.hier_enable) return kOk;
@@ -1196,6 +1239,20 @@ void apgcu_get_experimental(int* subpixel_method, float* subpixel_param, int* in
     if (subpixel_param) *subpixel_param = s.sp_param;
     if (inpaint_method) *inpaint_method = s.ip_method;
     if (inpaint_gap) *inpaint_gap = s.ip_gap;
+}
+
+int apgcu_engine_supports(apgcu_engine_t e, int* x, int* y, float* disparity, float* confidence, int cap) {
+    if (!e) return -1;
+    std::vector<apgcu::Engine::SupportOut> s;
+    if (e->eng->supports(s) != apgcu::kOk) return -1;
+    const int n = (int)s.size();
+    for (int i = 0; i < n && i < cap; ++i) {
+        if (x) x[i] = s[i].x;
+        if (y) y[i] = s[i].y;
+        if (disparity) disparity[i] = s[i].d;
+        if (confidence) confidence[i] = s[i].conf;
+    }
+    return n;
 }
 
 int apgcu_engine_hier_telemetry(apgcu_engine_t e, double* out6) {

@@ -131,6 +131,11 @@ public:
     // full_range_pixel_ratio, coarse pass device time (ms), 1 if the coarse pass ran.  Waits for
     // the engine stream.
     int hier_telemetry(double* out6);
+    // The prior's selected supports of the last frame in the reference's order
+    // (PipelineBuffers::supports, src/prior_estimator.cpp:112-165): x, y, disparity, confidence.
+    // Waits for the engine stream; empty without a prior.
+    struct SupportOut { int x, y; float d, conf; };
+    int supports(std::vector<SupportOut>& out);
     void release();
     cudaStream_t stream() const { return stream_; }
     const std::string& last_error() const { return err_; }

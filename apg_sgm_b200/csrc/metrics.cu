@@ -341,6 +341,104 @@ cudaError_t launch_metrics(const float* est, const float* gt, int w, int h, cons
     return cudaGetLastError();
 }
 
+// ---- evaluate_supports (src/metrics.cpp:8-124) -------------------------------------------------
+
+namespace {
+
+__device__ __forceinline__ bool support_visible(const float* gt, const uint8_t* vis, int w, int i, int x, float g) {
+    const int xr = x - (int)roundf(g);
+    return vis ? vis[i] >= 200 : (xr >= 0 && xr < w);
+}
+
+// Cells holding a visible ground-truth pixel.
+__global__ void support_cells_kernel(const float* __restrict__ gt, const uint8_t* __restrict__ vis, int w, int h,
+                                     float max_gt, int cell, int gw, uint8_t* __restrict__ vis_cell) {
+    const int n = w * h;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float g = gt[i];
+        if (!gt_ok(g, max_gt)) continue;
+        const int y = i / w, x = i - y * w;
+        if (support_visible(gt, vis, w, i, x, g)) vis_cell[(y / cell) * gw + x / cell] = 1;
+    }
+}
+
+// One block: the supports' tallies (thread-strided, then a fixed tree), cells with a correct
+// visible support, then the cell counts.  out_c: 10 counts, out_s: 2 sums.
+__global__ void __launch_bounds__(256) support_eval_kernel(const int* __restrict__ sx, const int* __restrict__ sy,
+                                                           const float* __restrict__ sd, int ns,
+                                                           const float* __restrict__ gt,
+                                                           const uint8_t* __restrict__ vis, int w, int h,
+                                                           float max_gt, int cell, int gw, int n_cells,
+                                                           const uint8_t* __restrict__ vis_cell,
+                                                           uint8_t* __restrict__ ok_cell, long long* out_c,
+                                                           double* out_s) {
+    unsigned c[8] = {};
+    double s0 = 0.0, s1 = 0.0;
+    for (int k = threadIdx.x; k < ns; k += blockDim.x) {
+        const int x = sx[k], y = sy[k];
+        if (x < 0 || x >= w || y < 0 || y >= h) continue;
+        const int i = y * w + x;
+        const float g = gt[i];
+        if (!gt_ok(g, max_gt)) continue;
+        const bool v = support_visible(gt, vis, w, i, x, g);
+        const float err = fabsf(__fsub_rn(sd[k], g));
+        c[0] += 1;
+        c[1] += v;
+        s0 += err;
+        if (v) s1 += err;
+        c[2] += err <= 0.5f;
+        c[3] += err <= 1.0f;
+        c[4] += err <= 2.0f;
+        c[5] += v && err <= 0.5f;
+        c[6] += v && err <= 1.0f;
+        c[7] += v && err <= 2.0f;
+        if (v && err <= 1.0f) {
+            const int gx = x / cell, gy = y / cell;
+            ok_cell[gy * gw + gx] = 1;
+        }
+    }
+    __shared__ unsigned sc[8][8];
+    __shared__ double ss[2][8];
+    __shared__ unsigned cells[2][8];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const unsigned t = __reduce_add_sync(0xffffffffu, c[k]);
+        if (lane == 0) sc[k][warp] = t;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        s0 += __shfl_down_sync(0xffffffffu, s0, o);
+        s1 += __shfl_down_sync(0xffffffffu, s1, o);
+    }
+    if (lane == 0) { ss[0][warp] = s0; ss[1][warp] = s1; }
+    __syncthreads();  // every ok_cell store is done
+    unsigned nv = 0, nok = 0;
+    for (int ci = threadIdx.x; ci < n_cells; ci += blockDim.x) {
+        nv += vis_cell[ci];
+        nok += vis_cell[ci] && ok_cell[ci];
+    }
+    nv = __reduce_add_sync(0xffffffffu, nv);
+    nok = __reduce_add_sync(0xffffffffu, nok);
+    if (lane == 0) { cells[0][warp] = nv; cells[1][warp] = nok; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < 8; ++k) {
+            long long t = 0;
+            for (int wp = 0; wp < 8; ++wp) t += sc[k][wp];
+            out_c[k] = t;
+        }
+        long long a = 0, b = 0;
+        double d0 = 0.0, d1 = 0.0;
+        for (int wp = 0; wp < 8; ++wp) { a += cells[0][wp]; b += cells[1][wp]; d0 += ss[0][wp]; d1 += ss[1][wp]; }
+        out_c[8] = a;
+        out_c[9] = b;
+        out_s[0] = d0;
+        out_s[1] = d1;
+    }
+}
+
+}  // namespace
+
 void count_launches(unsigned n);
 
 }  // namespace apgcu
@@ -476,3 +574,73 @@ extern "C" APGCU_API int apgcu_evaluate_stereo(const float* est, const float* gt
     apg_metrics_finalize(c, sm, w * h, has_range, has_ref, out);
     return APG_STATUS_OK;
 }
+
+extern "C" APGCU_API int apgcu_evaluate_supports(const int* sx, const int* sy, const float* sd, int n_supports,
+                                                 const float* gt, int w, int h, const uint8_t* vis, float max_valid_gt,
+                                                 int cell_size, int device_buffers, void* stream,
+                                                 apg_support_metrics_t* out) {
+    if (!out) return APG_STATUS_INTERNAL_ERROR;
+    std::memset(out, 0, sizeof(*out));
+    out->total = n_supports;
+    if (n_supports <= 0 || w <= 0 || h <= 0) return APG_STATUS_OK;  // no supports or no ground truth
+    if (!sx || !sy || !sd || !gt) return APG_STATUS_EMPTY_INPUT;
+    if (cell_size <= 0) return APG_STATUS_INVALID_CONFIG;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const size_t n = (size_t)w * h;
+    const int gw = (w + cell_size - 1) / cell_size, gh = (h + cell_size - 1) / cell_size, n_cells = gw * gh;
+    auto a256 = [](size_t v) { return (v + 255) & ~(size_t)255; };
+    const size_t in_bytes = device_buffers ? 0 : 3 * a256((size_t)n_supports * 4) + a256(n * 4) + (vis ? a256(n) : 0);
+    const size_t scratch = 2 * a256((size_t)n_cells) + 256;
+    unsigned char* blk = nullptr;
+    cudaMemPool_t pool = nullptr;
+    cudaError_t e = metrics_pool(&pool);
+    if (e == cudaSuccess) e = cudaMallocFromPoolAsync(reinterpret_cast<void**>(&blk), in_bytes + scratch, pool, s);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return APG_STATUS_ALLOCATION_FAILURE;
+    }
+    const int *dx = sx, *dy = sy;
+    const float *dd = sd, *dg = gt;
+    const uint8_t* dv = vis;
+    size_t o = 0;
+    auto up = [&](const void* src, size_t bytes) -> void* {
+        void* d = blk + o;
+        o += a256(bytes);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(d, src, bytes, cudaMemcpyHostToDevice, s);
+        return d;
+    };
+    if (!device_buffers) {
+        dx = static_cast<const int*>(up(sx, (size_t)n_supports * 4));
+        dy = static_cast<const int*>(up(sy, (size_t)n_supports * 4));
+        dd = static_cast<const float*>(up(sd, (size_t)n_supports * 4));
+        dg = static_cast<const float*>(up(gt, n * 4));
+        if (vis) dv = static_cast<const uint8_t*>(up(vis, n));
+    }
+    unsigned char* sc = blk + in_bytes;
+    uint8_t* vis_cell = sc;
+    uint8_t* ok_cell = sc + a256((size_t)n_cells);
+    long long* dc = reinterpret_cast<long long*>(sc + 2 * a256((size_t)n_cells));
+    double* ds = reinterpret_cast<double*>(dc + 10);
+    if (e == cudaSuccess) e = cudaMemsetAsync(sc, 0, 2 * a256((size_t)n_cells), s);
+    if (e == cudaSuccess) {
+        const int blocks = (int)std::min<size_t>((n + 255) / 256, 148 * 4);
+        apgcu::support_cells_kernel<<<blocks, 256, 0, s>>>(dg, dv, w, h, max_valid_gt, cell_size, gw, vis_cell);
+        apgcu::support_eval_kernel<<<1, 256, 0, s>>>(dx, dy, dd, n_supports, dg, dv, w, h, max_valid_gt, cell_size, gw,
+                                                     n_cells, vis_cell, ok_cell, dc, ds);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) apgcu::count_launches(2);
+    }
+    long long c[10];
+    double sm[2];
+    if (e == cudaSuccess) e = cudaMemcpyAsync(c, dc, sizeof(c), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(sm, ds, sizeof(sm), cudaMemcpyDeviceToHost, s);
+    cudaFreeAsync(blk, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return APG_STATUS_INTERNAL_ERROR;
+    }
+    apg_support_finalize(n_supports, c, sm, out);
+    return APG_STATUS_OK;
+}
+

@@ -1,5 +1,6 @@
-/* Plain-C mirror of the reference's accuracy metrics records (include/apg_sgm/metrics.hpp:46-125 of
- * the reference: RegionMetrics, QualityThresholds, StereoMetrics without the support block),
+/* Plain-C mirror of the reference's accuracy metrics records (include/apg_sgm/metrics.hpp:11-125 of
+ * the reference: SupportMetrics, RegionMetrics, QualityThresholds, and StereoMetrics, whose
+ * support block is evaluated separately by evaluate_supports),
  * shared by the CUDA library's evaluate entry point (include/apg_sgm_cuda.h), the CPU oracle and
  * the reference shim under oracle/.  Field names and meanings are the reference's; counts of
  * pixels are int as there, the four range pixel counts size_t-wide (unsigned long long).
@@ -51,6 +52,57 @@ typedef struct {
     float refine_epe_delta, post_epe_delta, total_epe_delta;
     float refine_improved_ratio, refine_worsened_ratio, refine_unchanged_ratio, refine_changed_ratio;
 } apg_stereo_metrics_t;
+
+/* SupportMetrics (metrics.hpp:11-44): the prior's support matches against the ground truth. */
+typedef struct {
+    int total, gt_valid, visible, correct_05, correct_1, correct_2;
+    int visible_correct_05, visible_correct_1, visible_correct_2, visible_gt_cells, correct_visible_cells;
+    float precision_05, precision_1, precision_2;
+    float precision_all_05, precision_all_1, precision_all_2;
+    float precision_vis_05, precision_vis_1, precision_vis_2;
+    float mean_abs_error, mae_all, mae_visible;
+    float grid_recall_1, grid_coverage, support_grid_recall_vis_1;
+} apg_support_metrics_t;
+
+/* SupportMetrics from its tallies (src/metrics.cpp:92-124): c = {gt_valid, visible, correct_05,
+ * correct_1, correct_2, visible_correct_05, visible_correct_1, visible_correct_2, visible_gt_cells,
+ * correct_visible_cells}, s = {sum of errors, sum of visible errors}. */
+static inline void apg_support_finalize(int total, const long long* c, const double* s, apg_support_metrics_t* m) {
+    apg_support_metrics_t z = {0};
+    *m = z;
+    m->total = total;
+    m->gt_valid = (int)c[0];
+    m->visible = (int)c[1];
+    m->correct_05 = (int)c[2];
+    m->correct_1 = (int)c[3];
+    m->correct_2 = (int)c[4];
+    m->visible_correct_05 = (int)c[5];
+    m->visible_correct_1 = (int)c[6];
+    m->visible_correct_2 = (int)c[7];
+    if (m->gt_valid > 0) {
+        m->precision_all_05 = (float)m->correct_05 / (float)m->gt_valid;
+        m->precision_all_1 = (float)m->correct_1 / (float)m->gt_valid;
+        m->precision_all_2 = (float)m->correct_2 / (float)m->gt_valid;
+        m->precision_05 = m->precision_all_05;
+        m->precision_1 = m->precision_all_1;
+        m->precision_2 = m->precision_all_2;
+        m->mae_all = (float)(s[0] / m->gt_valid);
+        m->mean_abs_error = m->mae_all;
+    }
+    if (m->visible > 0) {
+        m->precision_vis_05 = (float)m->visible_correct_05 / (float)m->visible;
+        m->precision_vis_1 = (float)m->visible_correct_1 / (float)m->visible;
+        m->precision_vis_2 = (float)m->visible_correct_2 / (float)m->visible;
+        m->mae_visible = (float)(s[1] / m->visible);
+    }
+    m->visible_gt_cells = (int)c[8];
+    m->correct_visible_cells = (int)c[9];
+    if (c[8] > 0) {
+        m->grid_recall_1 = (float)(int)c[9] / (float)(int)c[8];
+        m->grid_coverage = m->grid_recall_1;
+        m->support_grid_recall_vis_1 = m->grid_recall_1;
+    }
+}
 
 /* QualityThresholds{} defaults. */
 static inline apg_quality_thresholds_t apg_quality_thresholds_default(void) {

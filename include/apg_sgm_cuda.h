@@ -118,6 +118,11 @@ APGCU_API int apgcu_set_experimental(int subpixel_method, float subpixel_param, 
 APGCU_API void apgcu_get_experimental(int* subpixel_method, float* subpixel_param, int* inpaint_method,
                                       int* inpaint_gap);
 
+/* The prior's selected supports of the engine's last pair, in the reference's order
+ * (PipelineBuffers::supports): up to cap entries written; returns the total count (0 without a
+ * prior, -1 on error).  Waits for the engine stream. */
+APGCU_API int apgcu_engine_supports(apgcu_engine_t e, int* x, int* y, float* disparity, float* confidence, int cap);
+
 /* PipelineConfig::from_mode (src/config.cpp:5-45) into *out. */
 APGCU_API void apgcu_config_from_mode(int mode, int max_disparity, apg_pipeline_config_t* out);
 
@@ -155,6 +160,14 @@ APGCU_API int apgcu_evaluate_stereo(const float* est, const float* gt, int width
                                     const uint8_t* vis_mask, float max_valid_gt, const uint8_t* left_image,
                                     int left_stride, int left_channels, const apg_quality_thresholds_t* thresholds,
                                     int device_buffers, void* stream, apg_stereo_metrics_t* out);
+
+/* evaluate_supports (src/metrics.cpp:8-124): n_supports support matches (x, y, disparity; e.g.
+ * apgcu_engine_supports) against the W x H ground truth gt, vis_mask (nullable, >= 200 = visible),
+ * cells of cell_size pixels (16 in the reference).  Buffers as apgcu_evaluate_stereo's. */
+APGCU_API int apgcu_evaluate_supports(const int* x, const int* y, const float* disparity, int n_supports,
+                                      const float* gt, int width, int height, const uint8_t* vis_mask,
+                                      float max_valid_gt, int cell_size, int device_buffers, void* stream,
+                                      apg_support_metrics_t* out);
 
 /* Device time (ms) of the two kernels of this thread's last apgcu_evaluate_stereo, from events on
  * its stream around them. */

@@ -1413,3 +1413,58 @@ void orc_evaluate_stereo(const float* est, const float* gt, int w, int h, const 
     apg_metrics_finalize(c, sm, w * h, has_range, has_ref, out);
 }
 
+/* evaluate_supports, src/metrics.cpp:8-124: the supports in their order (so the double sums are the
+ * reference's), cells of cell_size pixels. */
+void orc_evaluate_supports(const orc_support_t* sp, int ns, const float* gt, int w, int h, const uint8_t* vis,
+                           float max_valid_gt, int cell_size, apg_support_metrics_t* out) {
+    long long c[10];
+    double s[2] = {0.0, 0.0};
+    memset(c, 0, sizeof(c));
+    if (ns <= 0 || w <= 0 || h <= 0) {
+        apg_support_metrics_t z;
+        memset(&z, 0, sizeof(z));
+        z.total = ns;
+        *out = z;
+        return;
+    }
+    const int gw = (w + cell_size - 1) / cell_size, gh = (h + cell_size - 1) / cell_size, nc = gw * gh;
+    uint8_t* vc = (uint8_t*)calloc((size_t)nc * 2, 1);
+    uint8_t* oc = vc + nc;
+    for (int y = 0; y < h; ++y)
+        for (int x = 0; x < w; ++x) {
+            const float g = gt[(size_t)y * w + x];
+            if (!gt_valid(g, max_valid_gt)) continue;
+            const int xr = x - (int)roundf(g);
+            const int v = vis ? vis[(size_t)y * w + x] >= 200 : (xr >= 0 && xr < w);
+            if (v && x / cell_size < gw && y / cell_size < gh) vc[(y / cell_size) * gw + x / cell_size] = 1;
+        }
+    for (int k = 0; k < ns; ++k) {
+        const int x = sp[k].x, y = sp[k].y;
+        if (x < 0 || x >= w || y < 0 || y >= h) continue;
+        const float g = gt[(size_t)y * w + x];
+        if (!gt_valid(g, max_valid_gt)) continue;
+        c[0]++;
+        const int xr = x - (int)roundf(g);
+        const int v = vis ? vis[(size_t)y * w + x] >= 200 : (xr >= 0 && xr < w);
+        if (v) c[1]++;
+        const float err = fabsf(sp[k].disparity - g);
+        s[0] += err;
+        if (v) s[1] += err;
+        if (err <= 0.5f) { c[2]++; if (v) c[5]++; }
+        if (err <= 1.0f) {
+            c[3]++;
+            if (v) {
+                c[6]++;
+                if (x / cell_size < gw && y / cell_size < gh) oc[(y / cell_size) * gw + x / cell_size] = 1;
+            }
+        }
+        if (err <= 2.0f) { c[4]++; if (v) c[7]++; }
+    }
+    for (int i = 0; i < nc; ++i) {
+        c[8] += vc[i];
+        c[9] += vc[i] && oc[i];
+    }
+    free(vc);
+    apg_support_finalize(ns, c, s, out);
+}
+

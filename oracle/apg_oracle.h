@@ -115,6 +115,10 @@ void orc_evaluate_stereo(const float* est, const float* gt, int w, int h, const 
                          const uint8_t* left, int left_stride, int left_ch, const apg_quality_thresholds_t* thr,
                          apg_stereo_metrics_t* out);
 
+/* evaluate_supports (src/metrics.cpp:8-124). */
+void orc_evaluate_supports(const orc_support_t* s, int n, const float* gt, int w, int h, const uint8_t* vis,
+                           float max_valid_gt, int cell_size, apg_support_metrics_t* out);
+
 /* Experimental scopes: sub-pixel method 0 Legacy, 1 CurvGate, 2 ConfGate, 3 Stabilized with its
  * parameter; inpaint method 0 Legacy, 1 ShadowReclass with its gap.  Defaults (0, 0, 0, 32). */
 void orc_set_experimental(int sp_method, float sp_param, int ip_method, int ip_gap);

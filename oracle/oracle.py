@@ -100,6 +100,21 @@ class StereoMetricsRec(C.Structure):
         return d
 
 
+_SUPPORT_INT = ["total", "gt_valid", "visible", "correct_05", "correct_1", "correct_2", "visible_correct_05",
+                "visible_correct_1", "visible_correct_2", "visible_gt_cells", "correct_visible_cells"]
+_SUPPORT_FLOAT = ["precision_05", "precision_1", "precision_2", "precision_all_05", "precision_all_1",
+                  "precision_all_2", "precision_vis_05", "precision_vis_1", "precision_vis_2", "mean_abs_error",
+                  "mae_all", "mae_visible", "grid_recall_1", "grid_coverage", "support_grid_recall_vis_1"]
+
+
+class SupportMetricsRec(C.Structure):
+    """apg_support_metrics_t (include/apg_sgm/metrics.h): SupportMetrics."""
+    _fields_ = [(k, C.c_int) for k in _SUPPORT_INT] + [(k, C.c_float) for k in _SUPPORT_FLOAT]
+
+    def to_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 _orc = None
 _ref = None
 
@@ -435,6 +450,41 @@ def ref_save(kind: str, path, arr, dmax: float = 0.0) -> int:
     if kind == "disparity_preview":
         args.append(C.c_float(dmax))
     return int(f(*args))
+
+
+def evaluate_supports(x, y, d, gt, vis=None, max_valid_gt=1e5, cell_size=16, reference=False) -> SupportMetricsRec:
+    """evaluate_supports (src/metrics.cpp:8-124): the oracle's, or with reference=True the reference's."""
+    gt = np.ascontiguousarray(gt, np.float32)
+    h, w = gt.shape
+    out = SupportMetricsRec()
+    if vis is not None:
+        vis = np.ascontiguousarray(vis, np.uint8)
+    if reference:
+        xs, ys, ds = (np.ascontiguousarray(a, t) for a, t in ((x, np.int32), (y, np.int32), (d, np.float32)))
+        ref_lib().ref_evaluate_supports(_p(xs), _p(ys), _p(ds), C.c_int(len(xs)), _p(gt), C.c_int(w), C.c_int(h),
+                                        _p(vis), C.c_float(max_valid_gt), C.c_int(cell_size), C.byref(out))
+    else:
+        n = len(x)
+        sp = np.zeros(n, dtype=[("x", "<i4"), ("y", "<i4"), ("d", "<f4"), ("c", "<f4")])
+        sp["x"], sp["y"], sp["d"] = x, y, d
+        lib().orc_evaluate_supports(_p(sp), C.c_int(n), _p(gt), C.c_int(w), C.c_int(h), _p(vis),
+                                    C.c_float(max_valid_gt), C.c_int(cell_size), C.byref(out))
+    return out
+
+
+def supports(cfg: PipelineConfig, left, right):
+    """The oracle prior's selected supports of a pair, in order: (x, y, disparity, confidence) arrays."""
+    a = aux(left, right)
+    h, w = a["left"]["gray"].shape
+    cap = max(1, cfg.prior_max_supports)
+    sp = np.zeros(cap, dtype=[("x", "<i4"), ("y", "<i4"), ("d", "<f4"), ("c", "<f4")])
+    sym = cfg.census_type == 1
+    n = lib().orc_extract_supports(C.byref(cfg), w, h, _p(a["left"]["gx"]), _p(a["left"]["gy"]),
+                                   _p(a["left"]["census"]) if sym else None, _p(a["right"]["census"]) if sym else None,
+                                   None if sym else _p(a["left"]["census64"]),
+                                   None if sym else _p(a["right"]["census64"]), _p(sp), cap)
+    sp = sp[:n]
+    return sp["x"].copy(), sp["y"].copy(), sp["d"].copy(), sp["c"].copy()
 
 
 def set_experimental(sp_method: int = 0, sp_param: float = 0.0, ip_method: int = 0, ip_gap: int = 32,

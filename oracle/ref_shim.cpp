@@ -487,6 +487,36 @@ void ref_set_experimental(int sp_method, float sp_param, int ip_method, int ip_g
     g_ip_scope.reset(new ExperimentalInpaintScope(static_cast<InpaintMethod>(ip_method), ip_gap, false));
 }
 
+// The reference's evaluate_supports (src/metrics.cpp:8-124) on plain arrays.
+void ref_evaluate_supports(const int* x, const int* y, const float* d, int n, const float* gt, int w, int h,
+                           const uint8_t* vis, float max_valid_gt, int cell_size, apg_support_metrics_t* out) {
+    std::vector<SupportMatch> s(static_cast<size_t>(std::max(n, 0)));
+    for (int i = 0; i < n; ++i) {
+        s[i].x = x[i];
+        s[i].y = y[i];
+        s[i].disparity = d[i];
+    }
+    Image32f G(w, h);
+    std::memcpy(G.data(), gt, static_cast<size_t>(w) * h * sizeof(float));
+    Image8 V;
+    if (vis) V = to_image(vis, w, h, w, 1);
+    const SupportMetrics m = evaluate_supports(s, G, vis ? &V : nullptr, max_valid_gt, cell_size);
+    apg_support_metrics_t o;
+    std::memset(&o, 0, sizeof(o));
+    o.total = m.total; o.gt_valid = m.gt_valid; o.visible = m.visible;
+    o.correct_05 = m.correct_05; o.correct_1 = m.correct_1; o.correct_2 = m.correct_2;
+    o.visible_correct_05 = m.visible_correct_05; o.visible_correct_1 = m.visible_correct_1;
+    o.visible_correct_2 = m.visible_correct_2; o.visible_gt_cells = m.visible_gt_cells;
+    o.correct_visible_cells = m.correct_visible_cells;
+    o.precision_05 = m.precision_05; o.precision_1 = m.precision_1; o.precision_2 = m.precision_2;
+    o.precision_all_05 = m.precision_all_05; o.precision_all_1 = m.precision_all_1; o.precision_all_2 = m.precision_all_2;
+    o.precision_vis_05 = m.precision_vis_05; o.precision_vis_1 = m.precision_vis_1; o.precision_vis_2 = m.precision_vis_2;
+    o.mean_abs_error = m.mean_abs_error; o.mae_all = m.mae_all; o.mae_visible = m.mae_visible;
+    o.grid_recall_1 = m.grid_recall_1; o.grid_coverage = m.grid_coverage;
+    o.support_grid_recall_vis_1 = m.support_grid_recall_vis_1;
+    *out = o;
+}
+
 // Public-API session used for timing the reference CPU path.
 void* ref_session_create(const apg_pipeline_config_t* ccfg, int bounded_reuse) {
     ExecutionOptions opt;

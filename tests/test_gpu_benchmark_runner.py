@@ -1,7 +1,7 @@
 """The manifest benchmark runner against the reference's own runner (apps/benchmark_stereo.cpp,
 built from the reference sources into oracle/_ref/benchmark_stereo) on the same manifest: every
-CSV column except those that measure this machine (times, bytes, thread counts, backend name) and
-the support-match block of the prior presets (not computed by this backend) must be identical."""
+CSV column except those that measure this machine (times, bytes, thread counts, backend name) must
+be identical."""
 import csv
 import subprocess
 
@@ -50,9 +50,7 @@ def test_runner_matches_reference_runner(O, apg, tmp_path, extra):
     ours = list(csv.DictReader(open(tmp_path / "ours.csv")))
     assert len(ref) == len(ours) == 12
     for a, b in zip(ref, ours):
-        prior = a["prior"] == "On" and a["case"] != "nogt"
         for k in a:
-            if k in SKIP or k.startswith("time_") or (prior and k.startswith("support_")) or \
-                    (prior and k == "grid_recall_1"):
+            if k in SKIP or k.startswith("time_"):
                 continue
             assert a[k] == b[k], (a["case"], a["ablation_id"], k, a[k], b[k])

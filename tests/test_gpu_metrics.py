@@ -91,3 +91,26 @@ def test_gpu_metrics_1080p_engine_output(O, apg):
     # a scored map, not a quality target (the synthetic pair has 20% flat patches)
     assert got.valid_pixels > 0 and 0.0 < got.epe < 64.0
     assert got.reg_all.total_pixels == got.evaluated_pixels
+
+
+@pytest.mark.parametrize("w,h,dmax,max_sup", [(320, 240, 64, 4000), (240, 160, 48, 60), (200, 120, 64, 200)])
+def test_engine_supports_and_support_metrics(O, apg, w, h, dmax, max_sup):
+    """The prior's support list (Engine.supports) equals the oracle's extract_supports in order and
+    value -- the stratified budget (max 4000) and the uniform sampling (60 < non-empty cells) -- and
+    evaluate_supports on the GPU equals the oracle's on it."""
+    from helpers import synth, to_oracle
+    cfg = apg.config_from_mode(2, dmax, prior_max_supports=max_sup)
+    L, R = synth(w, h, dmax, patch=0.2, seed=w + max_sup)
+    e = apg.Engine(cfg)
+    e.process(L, R)
+    sx, sy, sd, sc = e.supports()
+    e.close()
+    ox, oy, od, oc = O.supports(to_oracle(O, cfg), L, R)
+    assert len(sx) == len(ox) > 0
+    assert np.array_equal(sx, ox) and np.array_equal(sy, oy)
+    assert np.array_equal(sd.view(np.uint32), od.view(np.uint32)) and np.array_equal(sc.view(np.uint32), oc.view(np.uint32))
+    d = metric_case(w, h, 5)
+    for vis in (None, d["vis"]):
+        got = apg.evaluate_supports((sx, sy, sd), d["gt"], vis)
+        want = O.evaluate_supports(sx, sy, sd, d["gt"], vis)
+        assert got.to_dict() == want.to_dict()

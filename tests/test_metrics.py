@@ -102,3 +102,30 @@ def test_oracle_matches_metric_fixtures(case, O):
     got = run_case(_oracle(O), c)
     want = O.StereoMetricsRec.from_buffer_copy(z[f"{case}/record"].tobytes())
     assert not same_metrics(got, want)
+
+
+SUPPORT_CASES = [(96, 64, 16, 11, True), (75, 41, 7, 12, False), (40, 30, 16, 13, True)]
+
+
+@pytest.mark.parametrize("case", SUPPORT_CASES, ids=[f"{c[0]}x{c[1]}_cell{c[2]}" for c in SUPPORT_CASES])
+def test_support_metrics_oracle_matches_reference(case, O):
+    """evaluate_supports (src/metrics.cpp:8-124): supports inside and outside the frame, on invalid
+    ground truth, visible or not, errors around 0.5 / 1 / 2."""
+    if not O.ref_available():
+        pytest.skip("reference build (oracle/_ref) not present")
+    w, h, cell, seed, with_vis = case
+    d = metric_case(w, h, seed)
+    rng = np.random.default_rng(seed)
+    n = 300
+    x = rng.integers(-3, w + 3, n).astype(np.int32)
+    y = rng.integers(-3, h + 3, n).astype(np.int32)
+    g0 = np.nan_to_num(d["gt"], nan=0.0, posinf=0.0, neginf=0.0)
+    base = g0[np.clip(y, 0, h - 1), np.clip(x, 0, w - 1)]
+    disp = (base + rng.choice(np.array([0.0, 0.5, 0.75, 1.0, 1.5, 2.0, 2.5, 9.0], np.float32), n)).astype(np.float32)
+    vis = d["vis"] if with_vis else None
+    got = O.evaluate_supports(x, y, disp, d["gt"], vis, 1e5, cell)
+    want = O.evaluate_supports(x, y, disp, d["gt"], vis, 1e5, cell, reference=True)
+    assert got.to_dict() == want.to_dict()
+    assert got.gt_valid > 0 and got.visible > 0 and got.correct_1 > 0
+    empty = O.evaluate_supports(x[:0], y[:0], disp[:0], d["gt"], vis, 1e5, cell)
+    assert empty.total == 0 and empty.gt_valid == 0
