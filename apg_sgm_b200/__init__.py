@@ -813,53 +813,159 @@ def _get_experimental():
     return sm.value, sp.value, im.value, ig.value
 
 
+def _get_telemetry_flags():
+    a, b = C.c_int(), C.c_int()
+    lib().apgcu_get_experimental_telemetry(C.byref(a), C.byref(b))
+    return a.value, b.value
+
+
+class SubpixelTelemetry:
+    """SubpixelTelemetry (src/subpixel_estimator.hpp:50-118): this thread's counters."""
+
+    def __init__(self, rec):
+        for k, _ in rec._fields_:
+            v = getattr(rec, k)
+            setattr(self, k, list(v) if k == "delta_buckets" else v)
+
+    def applied_ratio(self) -> float:
+        return self.applied_pixels / self.candidate_pixels if self.candidate_pixels else 0.0
+
+    def clamped_ratio(self) -> float:
+        return self.clamped_count / self.applied_pixels if self.applied_pixels else 0.0
+
+    def mean_abs_delta(self) -> float:
+        return self.sum_abs_delta / self.applied_pixels if self.applied_pixels else 0.0
+
+    def percentile_abs_delta(self, q: float) -> float:
+        if self.applied_pixels == 0:
+            return 0.0
+        import math
+        target = int(math.ceil(float(np.float32(np.float32(q) * np.float32(self.applied_pixels)))))
+        acc = 0
+        for i, c in enumerate(self.delta_buckets):
+            acc += c
+            if acc >= target:
+                return float(np.float32(np.float32(i + 0.5) * np.float32(0.01)))
+        return 0.5
+
+    def p50_abs_delta(self) -> float:
+        return self.percentile_abs_delta(0.50)
+
+    def p95_abs_delta(self) -> float:
+        return self.percentile_abs_delta(0.95)
+
+
+class InpaintTelemetry:
+    """InpaintTelemetry (src/inpaint_internal.hpp:65-163): this thread's counters."""
+
+    _ROUTES = ["none", "occ_both_min", "occ_left_only", "occ_right_only", "mismatch_color_horiz",
+               "mismatch_color_vert", "mismatch_prior", "mismatch_lerp", "mismatch_left_only",
+               "mismatch_right_only", "remained_invalid"]
+
+    def __init__(self, rec):
+        for k, _ in rec._fields_:
+            v = getattr(rec, k)
+            setattr(self, k, list(v) if k in ("route_counts", "run_length_buckets") else v)
+
+    def route(self, name: str) -> int:
+        return self.route_counts[self._ROUTES.index(name)]
+
+    def total_filled_pixels(self) -> int:
+        rem = self.route_counts[10]
+        return self.total_invalid_pixels - rem if self.total_invalid_pixels > rem else 0
+
+    def fill_ratio(self) -> float:
+        return self.total_filled_pixels() / self.total_invalid_pixels if self.total_invalid_pixels else 0.0
+
+    def occ_filled_pixels(self) -> int:
+        return self.route_counts[1] + self.route_counts[2] + self.route_counts[3]
+
+    def occ_unfilled_pixels(self) -> int:
+        a = self.classified_occ_pixels + self.reclassified_shadow_pixels
+        return a - self.occ_filled_pixels() if a > self.occ_filled_pixels() else 0
+
+    def mismatch_native_filled_pixels(self) -> int:
+        return sum(self.route_counts[4:10])
+
+    def mismatch_filled_pixels(self) -> int:
+        return self.mismatch_native_filled_pixels() + self.reclassified_shadow_pixels
+
+    def mismatch_unfilled_pixels(self) -> int:
+        f = self.mismatch_filled_pixels()
+        return self.classified_mismatch_pixels - f if self.classified_mismatch_pixels > f else 0
+
+
+def _telemetry():
+    sp, ip = _lib_mod.SubpixelTelemetryRec(), _lib_mod.InpaintTelemetryRec()
+    lib().apgcu_get_telemetry(C.byref(sp), C.byref(ip))
+    return sp, ip
+
+
 class ExperimentalSubpixelScope:
     """ExperimentalSubpixelScope (src/subpixel_estimator.hpp:130-155): within the `with` block, every
     frame this thread runs uses `method` (parse_subpixel_method's names or SubpixelMethod) with
-    `param` (<= 0: the method's default) for the WTA and right-image sub-pixel step; the previous
-    scope returns on exit.  The telemetry counters are not part of this library."""
+    `param` (<= 0: the method's default) for the WTA and right-image sub-pixel step; with
+    collect_telemetry the WTA's counters accumulate into current_telemetry() (reset on entry).  The
+    previous scope returns on exit."""
 
     def __init__(self, method=SubpixelMethod.Legacy, param: float = 0.0, collect_telemetry: bool = False):
-        if collect_telemetry:
-            raise NotImplementedError("sub-pixel telemetry is not part of the CUDA backend")
         m = _parse(method, SubpixelMethod, _SUBPIXEL, "subpixel method")
         self.method, self.param = (SubpixelMethod.Legacy if m is None else m), float(param)
+        self.collect = bool(collect_telemetry)
 
     def __enter__(self):
         self._prev = _get_experimental()
+        self._prev_tel = _get_telemetry_flags()
         _, _, im, ig = self._prev
         lib().apgcu_set_experimental(int(self.method), C.c_float(self.param), im, ig)
+        lib().apgcu_set_experimental_telemetry(int(self.collect), _get_telemetry_flags()[1])
+        if self.collect:
+            lib().apgcu_reset_telemetry(1, 0)
         return self
 
     def __exit__(self, *exc):
         sm, sp, _, _ = self._prev
         _, _, im, ig = _get_experimental()
         lib().apgcu_set_experimental(sm, C.c_float(sp), im, ig)
+        lib().apgcu_set_experimental_telemetry(self._prev_tel[0], _get_telemetry_flags()[1])
         return False
+
+    @staticmethod
+    def current_telemetry() -> SubpixelTelemetry:
+        return SubpixelTelemetry(_telemetry()[0])
 
 
 class ExperimentalInpaintScope:
     """ExperimentalInpaintScope (src/inpaint_internal.hpp, src/postprocess.cpp:42-53): within the
     `with` block every frame this thread runs fills holes with `method` (Legacy or ShadowReclass)
-    and `max_gap` (Legacy at 32 keeps the configuration's max_fill_gap)."""
+    and `max_gap` (Legacy at 32 keeps the configuration's max_fill_gap); with collect_telemetry the
+    fill's counters accumulate into current_telemetry() (reset on entry)."""
 
     def __init__(self, method=InpaintMethod.Legacy, max_gap: int = 32, collect_telemetry: bool = False):
-        if collect_telemetry:
-            raise NotImplementedError("inpaint telemetry is not part of the CUDA backend")
         m = _parse(method, InpaintMethod, _INPAINT, "inpaint method")
         self.method, self.max_gap = (InpaintMethod.Legacy if m is None else m), int(max_gap)
+        self.collect = bool(collect_telemetry)
 
     def __enter__(self):
         self._prev = _get_experimental()
+        self._prev_tel = _get_telemetry_flags()
         sm, sp, _, _ = self._prev
         lib().apgcu_set_experimental(sm, C.c_float(sp), int(self.method), self.max_gap)
+        lib().apgcu_set_experimental_telemetry(_get_telemetry_flags()[0], int(self.collect))
+        if self.collect:
+            lib().apgcu_reset_telemetry(0, 1)
         return self
 
     def __exit__(self, *exc):
         _, _, im, ig = self._prev
         sm, sp, _, _ = _get_experimental()
         lib().apgcu_set_experimental(sm, C.c_float(sp), im, ig)
+        lib().apgcu_set_experimental_telemetry(_get_telemetry_flags()[0], self._prev_tel[1])
         return False
+
+    @staticmethod
+    def current_telemetry() -> InpaintTelemetry:
+        return InpaintTelemetry(_telemetry()[1])
 
 
 SupportMetrics = _lib_mod.SupportMetricsRec
@@ -890,6 +996,7 @@ __all__ = ["QualityMode", "HierarchicalFallback", "VolumeBackend", "MemoryPolicy
            "kernel_launch_count", "workspace_bytes", "evaluate_stereo", "StereoMetrics", "RegionMetrics",
            "evaluate_supports", "SupportMetrics", "load_image", "save_pgm", "save_pgm16", "save_disparity_preview", "load_pfm", "save_pfm", "Loader",
            "serve_files", "SubpixelMethod", "InpaintMethod", "ExperimentalSubpixelScope", "ExperimentalInpaintScope",
+           "SubpixelTelemetry", "InpaintTelemetry",
            "__version__"]
 
 

@@ -120,6 +120,23 @@ class SessionOptions(C.Structure):
                 ("min_disparity", C.c_int), ("max_disparity", C.c_int)]
 
 
+class SubpixelTelemetryRec(C.Structure):
+    """apg_subpixel_telemetry_t (include/apg_sgm/telemetry.h)."""
+    _fields_ = [("candidate_pixels", C.c_ulonglong), ("applied_pixels", C.c_ulonglong),
+                ("degenerate_count", C.c_ulonglong), ("clamped_count", C.c_ulonglong),
+                ("negative_curvature_count", C.c_ulonglong), ("sum_abs_delta", C.c_double),
+                ("delta_buckets", C.c_ulonglong * 50)]
+
+
+class InpaintTelemetryRec(C.Structure):
+    """apg_inpaint_telemetry_t (include/apg_sgm/telemetry.h)."""
+    _fields_ = [("total_invalid_pixels", C.c_ulonglong), ("classified_occ_pixels", C.c_ulonglong),
+                ("classified_mismatch_pixels", C.c_ulonglong), ("hit_max_gap_pixels", C.c_ulonglong),
+                ("reclassified_shadow_pixels", C.c_ulonglong), ("route_counts", C.c_ulonglong * 11),
+                ("invalid_runs_count", C.c_ulonglong), ("invalid_runs_truncated", C.c_ulonglong),
+                ("run_length_buckets", C.c_ulonglong * 10)]
+
+
 class LoadedPair(C.Structure):
     """apgcu_loaded_pair_t (include/apg_sgm_cuda.h): one pair read by the loader."""
     _fields_ = [("status", C.c_int), ("width", C.c_int), ("height", C.c_int), ("channels", C.c_int),
@@ -193,6 +210,10 @@ _SIGS = {
                                           C.POINTER(SupportMetricsRec)]),
     "apgcu_engine_supports": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
     "apgcu_set_experimental": (C.c_int, [C.c_int, C.c_float, C.c_int, C.c_int]),
+    "apgcu_set_experimental_telemetry": (C.c_int, [C.c_int, C.c_int]),
+    "apgcu_get_experimental_telemetry": (None, [C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "apgcu_get_telemetry": (None, [C.c_void_p, C.c_void_p]),
+    "apgcu_reset_telemetry": (None, [C.c_int, C.c_int]),
     "apgcu_get_experimental": (None, [C.POINTER(C.c_int), C.POINTER(C.c_float), C.POINTER(C.c_int),
                                       C.POINTER(C.c_int)]),
     "apgcu_image_info": (C.c_int, [C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),

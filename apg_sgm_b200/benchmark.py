@@ -11,9 +11,9 @@ starting with '#' are skipped, relative paths are taken from the manifest's dire
 times through a BoundedReuse session; the median run by host time is reported, its accuracy
 scored against the ground truth with evaluate_stereo on the GPU.  The CSV has the reference's
 columns in the reference's order and number formats, the prior presets' support-match block from
-the engine's supports (evaluate_supports on the GPU).  The sub-pixel / inpaint telemetry counters
-are not computed by this backend and are written as the reference writes them when it does not
-collect them.  `backend` is `cuda`.
+the engine's supports (evaluate_supports on the GPU), and the scopes' telemetry columns with
+--subpixel-telem / --inpaint-telem (zeros without, as the reference writes them).  `backend` is
+`cuda`.
 """
 from __future__ import annotations
 
@@ -204,16 +204,18 @@ def run(args) -> int:
                 cfg.hier_confidence_threshold = args.hierarchical_confidence_threshold
                 cfg.hier_expanded_radius = args.hierarchical_expanded_radius
             cfg.max_fill_gap = args.inpaint_gap
-            with ExperimentalSubpixelScope(sp_method, args.subpixel_param), \
-                    ExperimentalInpaintScope(ip_method, args.inpaint_gap):
+            with ExperimentalSubpixelScope(sp_method, args.subpixel_param, args.subpixel_telem), \
+                    ExperimentalInpaintScope(ip_method, args.inpaint_gap, args.inpaint_telem):
                 sess = StereoSession(config=cfg, memory_policy="bounded_reuse")
                 for _ in range(args.warmup):
                     sess.process(left, right)
+                _reset_telemetry(args)  # counters of the timed runs only (benchmark_stereo.cpp:545-550)
                 samples = []
                 for _ in range(args.repeat):
                     t0 = time.perf_counter()
                     res = sess.process(left, right)
                     samples.append(((time.perf_counter() - t0) * 1000.0, res, sess.hierarchical_telemetry))
+                tel = (ExperimentalSubpixelScope.current_telemetry(), ExperimentalInpaintScope.current_telemetry())
                 samples.sort(key=lambda s: s[0])
                 total_ms, res, htel = samples[args.repeat // 2]
                 st = res.stats
@@ -231,7 +233,7 @@ def run(args) -> int:
                     m = evaluate_stereo(res.disparity, gt, rng, before, after, vis, 1e5, left)
                     if sup is not None and len(sup[0]) > 0:  # has_supports: the prior's list is not empty
                         sm = evaluate_supports(sup, gt, vis, 1e5)
-            rows.append(_row(args, c, aid, cfg, w, h, m, sm, st, total_ms, htel, sp_method, ip_method))
+            rows.append(_row(args, c, aid, cfg, w, h, m, sm, st, total_ms, htel, sp_method, ip_method, tel))
             z = m if m is not None else None
             print(f"[{aid}] {_DESC[aid]:32s} | EPE: {(z.epe if z else -1.0):6.3f} | "
                   f"Bad2.0: {(z.bad_2_0 if z else -1.0):5.1f}% | D1-all: {(z.kitti_d1_all if z else -1.0):5.1f}% | "
@@ -251,7 +253,36 @@ def run(args) -> int:
     return 0
 
 
-def _row(args, c, aid, cfg, w, h, m, sm, st, total_ms, htel, sp_method, ip_method) -> str:
+def _reset_telemetry(args):
+    from ._lib import lib
+    lib().apgcu_reset_telemetry(int(args.subpixel_telem), int(args.inpaint_telem))
+
+
+def _per_run(tel, repeat, sp_on, ip_on):
+    """The timed runs' telemetry divided by the repeat count, each counter with integer division
+    and the |delta| sum in double, as benchmark_stereo.cpp:588-600 and 673-688 do."""
+    from . import InpaintTelemetry, SubpixelTelemetry
+    from ._lib import InpaintTelemetryRec, SubpixelTelemetryRec
+    sp, ip = tel
+    if not sp_on:
+        sp = SubpixelTelemetry(SubpixelTelemetryRec())
+    if not ip_on:
+        ip = InpaintTelemetry(InpaintTelemetryRec())
+    if repeat > 1:
+        for k in ("candidate_pixels", "applied_pixels", "degenerate_count", "clamped_count",
+                  "negative_curvature_count"):
+            setattr(sp, k, getattr(sp, k) // repeat)
+        sp.sum_abs_delta = sp.sum_abs_delta / repeat
+        sp.delta_buckets = [v // repeat for v in sp.delta_buckets]
+        for k in ("total_invalid_pixels", "classified_occ_pixels", "classified_mismatch_pixels", "hit_max_gap_pixels",
+                  "reclassified_shadow_pixels", "invalid_runs_count", "invalid_runs_truncated"):
+            setattr(ip, k, getattr(ip, k) // repeat)
+        ip.route_counts = [v // repeat for v in ip.route_counts]
+        ip.run_length_buckets = [v // repeat for v in ip.run_length_buckets]
+    return sp, ip
+
+
+def _row(args, c, aid, cfg, w, h, m, sm, st, total_ms, htel, sp_method, ip_method, tel) -> str:
     has = m is not None
     z = lambda k: getattr(m, k) if has else 0.0  # noqa: E731
     cost = "Census+AD+Grad" if (cfg.use_ad or cfg.use_grad) else "Census"
@@ -309,8 +340,15 @@ def _row(args, c, aid, cfg, w, h, m, sm, st, total_ms, htel, sp_method, ip_metho
     else:
         hv = (st.mean_search_width, 0.0, 0.0, 0.0)
     r += ",".join(_f(v, 4) for v in hv) + ","
-    r += f"{_SP_STR[sp_method]},{_f(args.subpixel_param, 4)},0,0,0.0000,0,0,0.0000,0,0.0000,0.0000,0.0000,"
-    r += f"{_IP_STR[ip_method]},{args.inpaint_gap},0,0,0.0000,0,0,0,0,0,0,0,0,0,0\n"
+    sp, ip = _per_run(tel, args.repeat, args.subpixel_telem, args.inpaint_telem)
+    r += (f"{_SP_STR[sp_method]},{_f(args.subpixel_param, 4)},{sp.candidate_pixels},{sp.applied_pixels},"
+          f"{_f(sp.applied_ratio(), 4)},{sp.degenerate_count},{sp.clamped_count},{_f(sp.clamped_ratio(), 4)},"
+          f"{sp.negative_curvature_count},{_f(sp.mean_abs_delta(), 4)},{_f(sp.p50_abs_delta(), 4)},"
+          f"{_f(sp.p95_abs_delta(), 4)},")
+    rc = ip.route_counts
+    r += (f"{_IP_STR[ip_method]},{args.inpaint_gap},{ip.total_invalid_pixels},{ip.total_filled_pixels()},"
+          f"{_f(ip.fill_ratio(), 4)},{rc[1]},{rc[2]},{rc[3]},{ip.occ_unfilled_pixels()},{rc[7]},{rc[8]},{rc[9]},"
+          f"{ip.mismatch_unfilled_pixels()},{ip.reclassified_shadow_pixels},{ip.hit_max_gap_pixels}\n")
     return r
 
 
@@ -338,15 +376,15 @@ def main(argv=None) -> int:
     ap.add_argument("--subpixel-param", type=float, default=None)
     ap.add_argument("--inpaint-method", default="legacy", choices=sorted(_IP_PARSE))
     ap.add_argument("--inpaint-gap", type=lambda v: max(1, int(v)), default=32)
-    for flag in ("--verify-backends", "--subpixel-telem", "--inpaint-telem"):
-        ap.add_argument(flag, action="store_true", help="not part of the CUDA backend")
+    ap.add_argument("--subpixel-telem", action="store_true")
+    ap.add_argument("--inpaint-telem", action="store_true")
+    ap.add_argument("--verify-backends", action="store_true", help="not part of the CUDA backend (one layout)")
     args = ap.parse_args(argv)
     if args.subpixel_param is None:  # the method's default parameter (apps/benchmark_stereo.cpp:265-273)
         args.subpixel_param = {1: 4.0, 2: 0.05, 3: 4.0}.get(_SP_PARSE[args.subpixel_method], 0.0)
-    for flag in ("verify_backends", "subpixel_telem", "inpaint_telem"):
-        if getattr(args, flag):
-            print(f"Error: --{flag.replace('_', '-')} is not part of the CUDA backend", file=sys.stderr)
-            return 2
+    if args.verify_backends:
+        print("Error: --verify-backends is not part of the CUDA backend", file=sys.stderr)
+        return 2
     return run(args)
 
 

@@ -466,6 +466,11 @@ int Batch::process(int n, const apgcu_pair_t* pairs, bool device_buffers) {
     for (auto& o : order) {
         const cudaError_t e = cudaStreamSynchronize(o.first->stream);
         if (e != cudaSuccess) return fail(kInternalError, std::string("batch: ") + cudaGetErrorString(e));
+        // the experimental scopes' telemetry of the bucket's pairs, into this thread's totals
+        for (size_t k = 0; k < o.second->size(); ++k) {
+            const int rc = o.first->slots[k]->collect_telemetry();
+            if (rc) return fail(rc, o.first->slots[k]->last_error());
+        }
     }
     last_ms_ = 0.f;
     for (auto& o : order) {

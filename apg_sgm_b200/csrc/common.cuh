@@ -16,6 +16,8 @@
 
 #include <cuda_runtime.h>
 
+#include "apg_sgm/telemetry.h"
+
 namespace apgcu {
 
 constexpr uint16_t kInvalidCost = 0xFFFFu;   // types.hpp:44 kInvalidCost
@@ -100,6 +102,45 @@ __device__ __forceinline__ float subpixel_delta(float cm, float c0, float cp, in
     if (!apply) return 0.0f;
     const float raw = __fdiv_rn(__fmul_rn(0.5f, __fsub_rn(cm, cp)), den);
     return raw < -0.5f ? -0.5f : (0.5f < raw ? 0.5f : raw);
+}
+
+// compute_delta with telemetry (src/subpixel_estimator.cpp:58-134): the same delta, and the
+// reference's counters (candidates, non-convex and degenerate triples, applied offsets with their
+// |delta| histogram and sum, clamped raw offsets) added with 64-bit atomics.
+__device__ __forceinline__ float subpixel_delta_tel(float cm, float c0, float cp, int method, float param, float uniq,
+                                                    apg_subpixel_telemetry_t* t) {
+    atomicAdd(&t->candidate_pixels, 1ull);
+    const float denom = __fadd_rn(__fsub_rn(cm, __fmul_rn(2.0f, c0)), cp);
+    const bool non_convex = c0 >= cm || c0 >= cp || denom <= 1e-6f;
+    if (non_convex) {
+        atomicAdd(&t->negative_curvature_count, 1ull);
+        if (fabsf(denom) <= 1e-6f || (cm == c0 && c0 == cp)) atomicAdd(&t->degenerate_count, 1ull);
+    }
+    float den = denom;
+    bool apply;
+    if (method == 0) {
+        apply = fabsf(denom) > 1e-6f;
+    } else if (method == 1) {
+        apply = !non_convex && denom >= (param > 0.0f ? param : 4.0f);
+    } else if (method == 2) {
+        apply = !non_convex && uniq >= (param > 0.0f ? param : 0.05f);
+    } else {
+        apply = c0 <= cm && c0 <= cp && denom > 0.0f;
+        den = __fadd_rn(denom, param > 0.0f ? param : 4.0f);
+    }
+    float raw = 0.0f, delta = 0.0f;
+    if (apply) {
+        raw = __fdiv_rn(__fmul_rn(0.5f, __fsub_rn(cm, cp)), den);
+        delta = raw < -0.5f ? -0.5f : (0.5f < raw ? 0.5f : raw);
+    }
+    if (fabsf(delta) > 1e-5f) {
+        const float a = fabsf(delta);
+        atomicAdd(&t->applied_pixels, 1ull);
+        atomicAdd(&t->sum_abs_delta, (double)a);
+        atomicAdd(&t->delta_buckets[min(49, (int)__fmul_rn(a, 100.0f))], 1ull);
+    }
+    if (fabsf(raw) >= 0.5f) atomicAdd(&t->clamped_count, 1ull);
+    return delta;
 }
 
 // Exact q = n / d for n < 2^16 and 1 <= d < 2^16 with one high multiply:

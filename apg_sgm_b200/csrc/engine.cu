@@ -53,6 +53,11 @@ ExperimentalScope& experimental_scope() {
     static thread_local ExperimentalScope s;
     return s;
 }
+
+TelemetryTotals& telemetry_totals() {
+    static thread_local TelemetryTotals t;
+    return t;
+}
 unsigned long long launch_count() { return g_launches.load(); }
 
 cudaError_t launch_default_range(int w, int h, int d0, int dmax, int16_t* rmin, int16_t* rmax, cudaStream_t s) {
@@ -188,6 +193,7 @@ Layout Engine::make_layout(const apg_pipeline_config_t& c, int w, int h, int ch,
     L.nsbuf = (c.paths == 8 ? 8 : 4) - 1;
     for (int i = 0; i < L.nsbuf; ++i) L.sbuf[i] = (i == 0 && (L.cross || L.fused_fast)) ? L.volA : take(vol);
     L.volRaw = L.raw_cost ? take(vol) : 0;
+    L.tel = take(sizeof(apg_subpixel_telemetry_t) + sizeof(apg_inpaint_telemetry_t));
     L.lut = take(kLutSize * 4);
     L.qlut = take(65 * 2);
     L.magic = take(256 * 4);
@@ -476,6 +482,8 @@ int Engine::process_host(const uint8_t* left, const uint8_t* right, int w, int h
     if (e != cudaSuccess) return cuda_fail(e, "output download");
     rc = check_refine();
     if (rc) return rc;
+    rc = collect_telemetry();
+    if (rc) return rc;
     counts_fresh_ = true;
     if (!outputs_pinned) {
         if (disp) std::memcpy(disp, pdisp, n * 4);
@@ -512,7 +520,46 @@ int Engine::process_device(const uint8_t* dl, const uint8_t* dr, int w, int h, i
 int Engine::sync() {
     cudaError_t e = cudaStreamSynchronize(stream_);
     if (e != cudaSuccess) return cuda_fail(e, "stream synchronize");
-    return check_refine();
+    const int rc = check_refine();
+    return rc ? rc : collect_telemetry();
+}
+
+int Engine::collect_telemetry() {
+    if (coarse_) {
+        const int rc = coarse_->collect_telemetry();
+        if (rc) return fail(rc, coarse_->last_error());
+    }
+    if (!tel_pending_) return kOk;
+    tel_pending_ = false;
+    apg_subpixel_telemetry_t sp;
+    apg_inpaint_telemetry_t ip;
+    cudaError_t e = cudaMemcpyAsync(&sp, arena_ + lay_.tel, sizeof(sp), cudaMemcpyDeviceToHost, stream_);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(&ip, arena_ + lay_.tel + sizeof(sp), sizeof(ip), cudaMemcpyDeviceToHost, stream_);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+    if (e != cudaSuccess) return cuda_fail(e, "telemetry");
+    TelemetryTotals& t = telemetry_totals();
+    if (scope_.sp_telem) {
+        t.sp.candidate_pixels += sp.candidate_pixels;
+        t.sp.applied_pixels += sp.applied_pixels;
+        t.sp.degenerate_count += sp.degenerate_count;
+        t.sp.clamped_count += sp.clamped_count;
+        t.sp.negative_curvature_count += sp.negative_curvature_count;
+        t.sp.sum_abs_delta += sp.sum_abs_delta;
+        for (int i = 0; i < 50; ++i) t.sp.delta_buckets[i] += sp.delta_buckets[i];
+    }
+    if (scope_.ip_telem) {
+        t.ip.total_invalid_pixels += ip.total_invalid_pixels;
+        t.ip.classified_occ_pixels += ip.classified_occ_pixels;
+        t.ip.classified_mismatch_pixels += ip.classified_mismatch_pixels;
+        t.ip.hit_max_gap_pixels += ip.hit_max_gap_pixels;
+        t.ip.reclassified_shadow_pixels += ip.reclassified_shadow_pixels;
+        for (int i = 0; i < 11; ++i) t.ip.route_counts[i] += ip.route_counts[i];
+        t.ip.invalid_runs_count += ip.invalid_runs_count;
+        t.ip.invalid_runs_truncated += ip.invalid_runs_truncated;
+        for (int i = 0; i < 10; ++i) t.ip.run_length_buckets[i] += ip.run_length_buckets[i];
+    }
+    return kOk;
 }
 
 #define RUN(expr, what)                                  \
@@ -551,6 +598,11 @@ int Engine::run_pre(const uint8_t* dl, int lstride, const uint8_t* dr, int rstri
     const int c64 = cfg_.census_type == APG_CENSUS_9X7;
     scope_ = experimental_scope();
     cudaEventRecord(ev_[0], s);
+    if (scope_.sp_telem || scope_.ip_telem) {
+        RUNC(cudaMemsetAsync(arena_ + L.tel, 0, sizeof(apg_subpixel_telemetry_t) + sizeof(apg_inpaint_telemetry_t), s),
+             "telemetry init");
+        tel_pending_ = true;
+    }
     {
         const AuxImage li{dl, lstride, ptr<uint8_t>(L.lgray), ptr<uint8_t>(L.lgx), ptr<uint8_t>(L.lgy),
                           ptr<uint32_t>(L.cl), ptr<unsigned long long>(L.cl)};
@@ -636,6 +688,7 @@ int Engine::sgm_launch(SgmLaunch* out, uint32_t** sbufs) const {
     pl.subpixel = cfg_.subpixel;
     pl.sp_method = scope_.sp_method;
     pl.sp_param = scope_.sp_param;
+    pl.sp_tel = scope_.sp_telem ? ptr<apg_subpixel_telemetry_t>(L.tel) : nullptr;
     pl.store_final = (debug_ & 2) != 0;
     pl.lanes = sgm_lanes_;
     for (int i = 0; i < L.nsbuf; ++i) sbufs[i] = ptr<uint32_t>(L.sbuf[i]);
@@ -823,7 +876,10 @@ int Engine::run_post(float* d_disp, float* d_conf, uint8_t* d_reason, uint8_t* d
         // the inpaint scope's gap replaces max_fill_gap unless it is Legacy at its default 32
         // (src/postprocess.cpp:45-48)
         const int gap = (scope_.ip_method == 0 && scope_.ip_gap == 32) ? cfg_.max_fill_gap : scope_.ip_gap;
-        RUN(launch_fill(w, h, gap, scope_.ip_method == 1, post_in, ptr<uint8_t>(L.reason), ptr<uint8_t>(L.lgray),
+        apg_inpaint_telemetry_t* ipt =
+            scope_.ip_telem ? reinterpret_cast<apg_inpaint_telemetry_t*>(arena_ + L.tel + sizeof(apg_subpixel_telemetry_t))
+                            : nullptr;
+        RUN(launch_fill(w, h, gap, scope_.ip_method == 1, ipt, post_in, ptr<uint8_t>(L.reason), ptr<uint8_t>(L.lgray),
                         ranged() ? ptr<float>(L.d_prior) : nullptr, ptr<float>(L.disp_fill), s), "fill");
         med_in = ptr<float>(L.disp_fill);
     }
@@ -1231,6 +1287,31 @@ int apgcu_set_experimental(int subpixel_method, float subpixel_param, int inpain
     s.ip_method = inpaint_method;
     s.ip_gap = inpaint_gap;
     return 0;
+}
+
+int apgcu_set_experimental_telemetry(int subpixel, int inpaint) {
+    apgcu::ExperimentalScope& s = apgcu::experimental_scope();
+    s.sp_telem = subpixel != 0;
+    s.ip_telem = inpaint != 0;
+    return 0;
+}
+
+void apgcu_get_experimental_telemetry(int* subpixel, int* inpaint) {
+    const apgcu::ExperimentalScope& s = apgcu::experimental_scope();
+    if (subpixel) *subpixel = s.sp_telem;
+    if (inpaint) *inpaint = s.ip_telem;
+}
+
+void apgcu_get_telemetry(apg_subpixel_telemetry_t* sp, apg_inpaint_telemetry_t* ip) {
+    const apgcu::TelemetryTotals& t = apgcu::telemetry_totals();
+    if (sp) *sp = t.sp;
+    if (ip) *ip = t.ip;
+}
+
+void apgcu_reset_telemetry(int subpixel, int inpaint) {
+    apgcu::TelemetryTotals& t = apgcu::telemetry_totals();
+    if (subpixel) t.sp = apg_subpixel_telemetry_t{};
+    if (inpaint) t.ip = apg_inpaint_telemetry_t{};
 }
 
 void apgcu_get_experimental(int* subpixel_method, float* subpixel_param, int* inpaint_method, int* inpaint_gap) {

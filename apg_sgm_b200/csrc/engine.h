@@ -55,6 +55,7 @@ struct Layout {
     size_t stats = 0;  // u64 frame counters (launch_frame_stats) + prior support count
     // hierarchical search range: half-size grays of both images, telemetry counters (4 x u64)
     size_t hc_left = 0, hc_right = 0, hstats = 0;
+    size_t tel = 0;  // scope telemetry of the frame: apg_subpixel_telemetry_t then apg_inpaint_telemetry_t
     size_t rf_scan_tmp_bytes = 0;
     int n_cells = 0, gw = 0, gh = 0, max_cand = 0;
 };
@@ -68,12 +69,20 @@ struct ExperimentalScope {
     float sp_param = 0.0f;
     int ip_method = 0;
     int ip_gap = 32;
+    int sp_telem = 0, ip_telem = 0;  // collect the scopes' telemetry
 };
 ExperimentalScope& experimental_scope();
 inline bool same_scope(const ExperimentalScope& a, const ExperimentalScope& b) {
     return a.sp_method == b.sp_method && a.sp_param == b.sp_param && a.ip_method == b.ip_method &&
-           a.ip_gap == b.ip_gap;
+           a.ip_gap == b.ip_gap && a.sp_telem == b.sp_telem && a.ip_telem == b.ip_telem;
 }
+// The calling thread's accumulated scope telemetry (the reference's thread-local
+// ExperimentalSubpixelScope / ExperimentalInpaintScope::current_telemetry()).
+struct TelemetryTotals {
+    apg_subpixel_telemetry_t sp{};
+    apg_inpaint_telemetry_t ip{};
+};
+TelemetryTotals& telemetry_totals();
 
 // Refine pass state (u32 words at Layout::rf_state): pass start positions, error flag, progress.
 constexpr int kRefineMaxIter = 63;
@@ -147,6 +156,9 @@ public:
     // takes the calling thread's experimental scopes now (run_pre does so for every frame; the
     // batched form needs them before it builds SGM plans from sgm_launch)
     void capture_scope() { scope_ = experimental_scope(); }
+    // adds the last frame's scope telemetry (and the coarse pass's) to the calling thread's totals
+    // once the frame has completed; process_host and sync() call it
+    int collect_telemetry();
     int debug() const { return debug_; }
     const apg_pipeline_config_t& config() const { return cfg_; }
     int device() const { return device_; }
@@ -223,6 +235,7 @@ private:
     int support_count_ = 0;
     std::unique_ptr<Engine> coarse_;  // hierarchical mode: the half-size engine (same stream)
     ExperimentalScope scope_;         // the calling thread's experimental scopes, read per frame
+    bool tel_pending_ = false;        // the last frame counted telemetry not yet collected
     bool skip_fill_ = false;          // coarse engine without coarse_fill_holes: no fill stage
     bool hier_ran_ = false;           // the last frame ran the coarse pass
     unsigned long long counts_[8] = {};  // frame counters copied with the host outputs

@@ -68,6 +68,7 @@ struct SgmLaunch {
     int subpixel;
     int sp_method = 0;    // sub-pixel method of the WTA (subpixel_delta), 0 = Legacy
     float sp_param = 0.0f;
+    apg_subpixel_telemetry_t* sp_tel = nullptr;  // telemetry counters (ExperimentalSubpixelScope), or none
     int store_final;  // last sweep: also write the final sum into in[0] (stage dumps)
     int lanes;        // lanes per scanline chain (8, 16, 32; 0 = default for Dp)
 };
@@ -119,7 +120,8 @@ struct ConfLrArgs {
 cudaError_t launch_conf_lr(const ConfLrArgs& a, cudaStream_t s);
 cudaError_t launch_lr(int w, int h, int lr_max_diff, const float* dr, const float* din, float* dout,
                       uint8_t* reason, cudaStream_t s);
-cudaError_t launch_fill(int w, int h, int gap, int shadow, const float* in, const uint8_t* reason, const uint8_t* gray,
+cudaError_t launch_fill(int w, int h, int gap, int shadow, apg_inpaint_telemetry_t* tel, const float* in,
+                        const uint8_t* reason, const uint8_t* gray,
                         const float* d_prior, float* out, cudaStream_t s);
 cudaError_t launch_median(int w, int h, int r, const float* in, float* out, cudaStream_t s);
 cudaError_t launch_frame_stats(int n, const float* disp, const uint8_t* reliable, const uint8_t* reason,

@@ -105,10 +105,12 @@ __device__ __forceinline__ bool occlusion_like(uint8_t r, int shadow, float dl, 
 }
 
 // Legacy hole fill, src/postprocess.cpp:87-168 (shadow != 0: the ShadowReclass inpaint,
-// :170-239).  Reads the pre-fill map, writes a copy.
-__global__ void fill_kernel(int w, int h, int gap, int shadow, const float* __restrict__ in,
-                            const uint8_t* __restrict__ reason, const uint8_t* __restrict__ gray,
-                            const float* __restrict__ d_prior, float* __restrict__ out) {
+// :170-239).  Reads the pre-fill map, writes a copy.  tel (nullable): the InpaintTelemetry
+// counters of every hole (classification, gap bound hit, fill route, shadow reclassification).
+__global__ void fill_kernel(int w, int h, int gap, int shadow, apg_inpaint_telemetry_t* __restrict__ tel,
+                            const float* __restrict__ in, const uint8_t* __restrict__ reason,
+                            const uint8_t* __restrict__ gray, const float* __restrict__ d_prior,
+                            float* __restrict__ out) {
     const int n = w * h;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const float v = in[i];
@@ -121,41 +123,83 @@ __global__ void fill_kernel(int w, int h, int gap, int shadow, const float* __re
         while (xr < w && xr <= x + gap && row[xr] < 0.f) ++xr;
         const float dl = (xl >= 0 && row[xl] >= 0.f) ? row[xl] : -1.f;
         const float dr = (xr < w && row[xr] >= 0.f) ? row[xr] : -1.f;
+        const uint8_t r = reason[i];
+        if (tel) {
+            atomicAdd(&tel->total_invalid_pixels, 1ull);
+            if (r == kOcclusion) atomicAdd(&tel->classified_occ_pixels, 1ull);
+            else if (r == kMismatch) atomicAdd(&tel->classified_mismatch_pixels, 1ull);
+            if (xl < 0 || x - xl > gap || xr >= w || xr - x > gap) atomicAdd(&tel->hit_max_gap_pixels, 1ull);
+        }
         float o = v;
-        if (occlusion_like(reason[i], shadow, dl, dr)) {
-            if (dl >= 0.f && dr >= 0.f) o = (dr < dl) ? dr : dl;
-            else if (dl >= 0.f) o = dl;
-            else if (dr >= 0.f) o = dr;
-            out[i] = o;
-            continue;
-        }
-        const int c0 = gray[i];
-        float best_d = -1.f;
-        int best_abs = 999;
-        const int cx[4] = {xl, xr, x, x};
-        const int cy[4] = {y, y, y - 1, y + 1};
+        int route;  // FillRoute (src/inpaint_internal.hpp:34-47)
+        if (occlusion_like(r, shadow, dl, dr)) {
+            if (tel && r != kOcclusion) atomicAdd(&tel->reclassified_shadow_pixels, 1ull);
+            if (dl >= 0.f && dr >= 0.f) { o = (dr < dl) ? dr : dl; route = 1; }
+            else if (dl >= 0.f) { o = dl; route = 2; }
+            else if (dr >= 0.f) { o = dr; route = 3; }
+            else route = 10;
+        } else {
+            const int c0 = gray[i];
+            float best_d = -1.f;
+            int best_abs = 999;
+            bool best_vert = false;
+            const int cx[4] = {xl, xr, x, x};
+            const int cy[4] = {y, y, y - 1, y + 1};
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const int xx = cx[k], yy = cy[k];
-            if (xx < 0 || yy < 0 || xx >= w || yy >= h) continue;
-            const float dv = in[(size_t)yy * w + xx];
-            if (dv < 0.f) continue;
-            const int ad = abs((int)gray[(size_t)yy * w + xx] - c0);
-            if (ad < best_abs) { best_abs = ad; best_d = dv; }
+            for (int k = 0; k < 4; ++k) {
+                const int xx = cx[k], yy = cy[k];
+                if (xx < 0 || yy < 0 || xx >= w || yy >= h) continue;
+                const float dv = in[(size_t)yy * w + xx];
+                if (dv < 0.f) continue;
+                const int ad = abs((int)gray[(size_t)yy * w + xx] - c0);
+                if (ad < best_abs) { best_abs = ad; best_d = dv; best_vert = k >= 2; }
+            }
+            if (best_d >= 0.f && best_abs <= 18) {
+                o = best_d;
+                route = best_vert ? 5 : 4;
+            } else if (d_prior && d_prior[i] >= 0.f) {
+                o = d_prior[i];
+                route = 6;
+            } else if (dl >= 0.f && dr >= 0.f) {
+                const float t = __fdiv_rn((float)(x - xl), (float)(xr - xl));
+                o = __fadd_rn(__fmul_rn(dl, __fsub_rn(1.f, t)), __fmul_rn(dr, t));
+                route = 7;
+            } else if (dl >= 0.f) {
+                o = dl;
+                route = 8;
+            } else if (dr >= 0.f) {
+                o = dr;
+                route = 9;
+            } else {
+                route = 10;
+            }
         }
-        if (best_d >= 0.f && best_abs <= 18) {
-            o = best_d;
-        } else if (d_prior && d_prior[i] >= 0.f) {
-            o = d_prior[i];
-        } else if (dl >= 0.f && dr >= 0.f) {
-            const float t = __fdiv_rn((float)(x - xl), (float)(xr - xl));
-            o = __fadd_rn(__fmul_rn(dl, __fsub_rn(1.f, t)), __fmul_rn(dr, t));
-        } else if (dl >= 0.f) {
-            o = dl;
-        } else if (dr >= 0.f) {
-            o = dr;
-        }
+        if (tel) atomicAdd(&tel->route_counts[route], 1ull);
         out[i] = o;
+    }
+}
+
+// InpaintTelemetry's run statistics (src/postprocess.cpp:64-85): each row's runs of invalid
+// pixels, one thread per row.
+__global__ void fill_runs_kernel(int w, int h, int gap, const float* __restrict__ in,
+                                 apg_inpaint_telemetry_t* __restrict__ tel) {
+    for (int y = blockIdx.x * blockDim.x + threadIdx.x; y < h; y += gridDim.x * blockDim.x) {
+        const float* row = in + (size_t)y * w;
+        int len = 0;
+        for (int x = 0; x <= w; ++x) {
+            if (x < w && row[x] < 0.f) {
+                ++len;
+                continue;
+            }
+            if (len > 0) {
+                atomicAdd(&tel->invalid_runs_count, 1ull);
+                if (len > gap) atomicAdd(&tel->invalid_runs_truncated, 1ull);
+                const int b = len < 4 ? 0 : len < 8 ? 1 : len < 16 ? 2 : len < 24 ? 3 : len < 32 ? 4 : len < 48 ? 5
+                                                   : len < 64 ? 6 : len < 96 ? 7 : len < 128 ? 8 : 9;
+                atomicAdd(&tel->run_length_buckets[b], 1ull);
+                len = 0;
+            }
+        }
     }
 }
 
@@ -192,6 +236,7 @@ __global__ void median_kernel(int w, int h, int r, const float* __restrict__ in,
         out[i] = res;
     }
 }
+
 
 // The same fill with the neighbour search done by warp ballots: a warp owns 32 consecutive pixels
 // of a row; the walk of the reference (xl = x - 1 down while xl >= max(x - gap, 0) and
@@ -449,14 +494,20 @@ cudaError_t launch_lr(int w, int h, int lr_max_diff, const float* dr, const floa
     return cudaGetLastError();
 }
 
-cudaError_t launch_fill(int w, int h, int gap, int shadow, const float* in, const uint8_t* reason,
-                        const uint8_t* gray, const float* d_prior, float* out, cudaStream_t s) {
+cudaError_t launch_fill(int w, int h, int gap, int shadow, apg_inpaint_telemetry_t* tel, const float* in,
+                        const uint8_t* reason, const uint8_t* gray, const float* d_prior, float* out, cudaStream_t s) {
+    if (tel) {
+        // telemetry: the per-pixel form (same map) counts every hole, one thread per row the runs
+        fill_runs_kernel<<<(h + 127) / 128, 128, 0, s>>>(w, h, gap, in, tel);
+        fill_kernel<<<grid_for(w * h), 256, 0, s>>>(w, h, gap, shadow, tel, in, reason, gray, d_prior, out);
+        return cudaGetLastError();
+    }
     if (gap >= 0) {
         const long long warps = (long long)((w + 31) / 32) * h;
         const int blocks = (int)std::min<long long>((warps + 7) / 8, 148 * 16);
         fill_ballot_kernel<<<blocks, 256, 0, s>>>(w, h, gap, shadow, in, reason, gray, d_prior, out);
     } else {
-        fill_kernel<<<grid_for(w * h), 256, 0, s>>>(w, h, gap, shadow, in, reason, gray, d_prior, out);
+        fill_kernel<<<grid_for(w * h), 256, 0, s>>>(w, h, gap, shadow, nullptr, in, reason, gray, d_prior, out);
     }
     return cudaGetLastError();
 }

@@ -128,6 +128,7 @@ struct SgmArgs {
     int subpixel;
     int sp_method;
     float sp_param;
+    apg_subpixel_telemetry_t* sp_tel;
     int store_final;
 };
 
@@ -248,7 +249,10 @@ __device__ __forceinline__ void wta(const SgmArgs& a, unsigned gmask, int j, int
                 if (cm < kInf && cp < kInf) {
                     // WTA uniqueness (src/sgm_optimizer.cpp:520-525): (second - best) / max(best, 1)
                     const float u = sec >= kInf ? 1.0f : __fdiv_rn((float)(sec - bv), (float)max(bv, 1u));
-                    dval = __fadd_rn(dval, subpixel_delta((float)cm, (float)bv, (float)cp, a.sp_method, a.sp_param, u));
+                    dval = __fadd_rn(dval, a.sp_tel ? subpixel_delta_tel((float)cm, (float)bv, (float)cp, a.sp_method,
+                                                                         a.sp_param, u, a.sp_tel)
+                                                    : subpixel_delta((float)cm, (float)bv, (float)cp, a.sp_method,
+                                                                     a.sp_param, u));
                 }
             }
             fb = (float)bv;
@@ -549,7 +553,10 @@ __device__ __forceinline__ void wta_row(const SgmArgs& a, const uint32_t* row, i
                 if (cm < kInf && cp < kInf) {
                     // WTA uniqueness (src/sgm_optimizer.cpp:520-525): (second - best) / max(best, 1)
                     const float u = sec >= kInf ? 1.0f : __fdiv_rn((float)(sec - m), (float)max(m, 1u));
-                    dval = __fadd_rn(dval, subpixel_delta((float)cm, (float)m, (float)cp, a.sp_method, a.sp_param, u));
+                    dval = __fadd_rn(dval, a.sp_tel ? subpixel_delta_tel((float)cm, (float)m, (float)cp, a.sp_method,
+                                                                         a.sp_param, u, a.sp_tel)
+                                                    : subpixel_delta((float)cm, (float)m, (float)cp, a.sp_method,
+                                                                     a.sp_param, u));
                 }
             }
             fb = (float)m;
@@ -1049,6 +1056,7 @@ SgmArgs make_args(const SgmLaunch& l) {
     a.subpixel = l.subpixel;
     a.sp_method = l.sp_method;
     a.sp_param = l.sp_param;
+    a.sp_tel = l.sp_tel;
     a.store_final = l.store_final;
     return a;
 }

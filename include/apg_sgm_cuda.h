@@ -17,6 +17,7 @@
 #include "apg_sgm/c_api.h"
 #include "apg_sgm/metrics.h"
 #include "apg_sgm/pipeline_config.h"
+#include "apg_sgm/telemetry.h"
 
 #if defined(__GNUC__) && __GNUC__ >= 4
 #define APGCU_API __attribute__((visibility("default")))
@@ -111,12 +112,20 @@ APGCU_API int apgcu_engine_hier_telemetry(apgcu_engine_t e, double* out6);
  * made on that thread when it starts a frame: subpixel_method 0 Legacy, 1 CurvGate, 2 ConfGate,
  * 3 Stabilized with its parameter (<= 0: the method's default); inpaint_method 0 Legacy,
  * 1 ShadowReclass with its gap (Legacy at 32 keeps the configuration's max_fill_gap).  Defaults
- * (0, 0, 0, 32) reproduce the reference without scopes.  The scopes' telemetry counters are not
- * part of this library; the allocation-free right-image WTA always uses Legacy.  Returns 0 or
- * APG_STATUS_INVALID_CONFIG for an unknown method. */
+ * (0, 0, 0, 32) reproduce the reference without scopes.  The allocation-free right-image WTA
+ * always uses Legacy.  Returns 0 or APG_STATUS_INVALID_CONFIG for an unknown method. */
 APGCU_API int apgcu_set_experimental(int subpixel_method, float subpixel_param, int inpaint_method, int inpaint_gap);
 APGCU_API void apgcu_get_experimental(int* subpixel_method, float* subpixel_param, int* inpaint_method,
                                       int* inpaint_gap);
+/* The scopes' telemetry (collect_telemetry): while on for the calling thread, every frame it runs
+ * adds the WTA's sub-pixel counters and the hole fill's counters (SubpixelTelemetry,
+ * InpaintTelemetry; the hierarchical coarse pass included, as in the reference) to the thread's
+ * totals when the frame completes (apgcu_engine_process, apg_session_process, a batch call, or
+ * apgcu_engine_sync after apgcu_engine_process_device).  get copies the totals, reset clears them. */
+APGCU_API int apgcu_set_experimental_telemetry(int subpixel, int inpaint);
+APGCU_API void apgcu_get_experimental_telemetry(int* subpixel, int* inpaint);
+APGCU_API void apgcu_get_telemetry(apg_subpixel_telemetry_t* subpixel, apg_inpaint_telemetry_t* inpaint);
+APGCU_API void apgcu_reset_telemetry(int subpixel, int inpaint);
 
 /* The prior's selected supports of the engine's last pair, in the reference's order
  * (PipelineBuffers::supports): up to cap entries written; returns the total count (0 without a

@@ -389,6 +389,57 @@ void orc_set_experimental(int sp_method, float sp_param, int ip_method, int ip_g
     g_ip_gap = ip_gap;
 }
 
+static int g_sp_tel = 0, g_ip_tel = 0;
+static apg_subpixel_telemetry_t g_spt;
+static apg_inpaint_telemetry_t g_ipt;
+
+/* Telemetry on/off; switching on clears the totals (the scopes' constructors reset them). */
+void orc_set_telemetry(int subpixel, int inpaint) {
+    g_sp_tel = subpixel;
+    g_ip_tel = inpaint;
+    if (subpixel) memset(&g_spt, 0, sizeof(g_spt));
+    if (inpaint) memset(&g_ipt, 0, sizeof(g_ipt));
+}
+
+void orc_get_telemetry(apg_subpixel_telemetry_t* sp, apg_inpaint_telemetry_t* ip) {
+    if (sp) *sp = g_spt;
+    if (ip) *ip = g_ipt;
+}
+
+/* compute_delta with telemetry, src/subpixel_estimator.cpp:58-134. */
+static float sp_delta_tel(float cm, float c0, float cp, float uniq) {
+    apg_subpixel_telemetry_t* t = &g_spt;
+    t->candidate_pixels++;
+    const float denom = cm - 2.0f * c0 + cp;
+    const int non_convex = c0 >= cm || c0 >= cp || denom <= 1e-6f;
+    if (non_convex) {
+        t->negative_curvature_count++;
+        if (fabsf(denom) <= 1e-6f || (cm == c0 && c0 == cp)) t->degenerate_count++;
+    }
+    float raw = 0.0f, delta = 0.0f;
+    int apply;
+    float den = denom;
+    if (g_sp_method == 0) apply = fabsf(denom) > 1e-6f;
+    else if (g_sp_method == 1) apply = !non_convex && denom >= (g_sp_param > 0.0f ? g_sp_param : 4.0f);
+    else if (g_sp_method == 2) apply = !non_convex && uniq >= (g_sp_param > 0.0f ? g_sp_param : 0.05f);
+    else {
+        apply = c0 <= cm && c0 <= cp && denom > 0.0f;
+        den = denom + (g_sp_param > 0.0f ? g_sp_param : 4.0f);
+    }
+    if (apply) {
+        raw = 0.5f * (cm - cp) / den;
+        delta = raw < -0.5f ? -0.5f : (0.5f < raw ? 0.5f : raw);
+    }
+    if (fabsf(delta) > 1e-5f) {
+        const float a = fabsf(delta);
+        t->applied_pixels++;
+        t->sum_abs_delta += a;
+        t->delta_buckets[imin(49, (int)(a * 100.0f))]++;
+    }
+    if (fabsf(raw) >= 0.5f) t->clamped_count++;
+    return delta;
+}
+
 /* SubpixelEstimator::compute_delta without telemetry, src/subpixel_estimator.cpp:58-119. */
 static float sp_delta(float cm, float c0, float cp, float uniq) {
     if (g_sp_method == 0) return legacy_delta(cm, c0, cp);
@@ -449,7 +500,8 @@ void orc_wta(const apg_pipeline_config_t* cfg, const uint32_t* acc, const int16_
                     if (cm != ORC_INVALID_COST32 && cp != ORC_INVALID_COST32) {
                         float u = 1.0f;
                         if (second < UINT64_MAX) u = (float)(second - best) / (float)(best > 1 ? best : 1);
-                        dval += sp_delta((float)cm, (float)c0, (float)cp, u);
+                        dval += g_sp_tel ? sp_delta_tel((float)cm, (float)c0, (float)cp, u)
+                                         : sp_delta((float)cm, (float)c0, (float)cp, u);
                     }
                 }
             }
@@ -622,8 +674,22 @@ void orc_fill_holes(const apg_pipeline_config_t* cfg, int w, int h, const float*
                     const uint8_t* reason, const uint8_t* lgray, const float* d_prior, float* out) {
     /* the inpaint scope's gap replaces max_fill_gap unless it is Legacy at 32 (postprocess.cpp:45-48) */
     const int gap = (g_ip_method == 0 && g_ip_gap == 32) ? cfg->max_fill_gap : g_ip_gap;
+    apg_inpaint_telemetry_t* t = g_ip_tel ? &g_ipt : NULL;
     memcpy(out, in, sizeof(float) * (size_t)w * h);
     for (int y = 0; y < h; ++y) {
+        if (t) { /* run statistics, postprocess.cpp:64-85 */
+            int len = 0;
+            for (int x = 0; x <= w; ++x) {
+                if (x < w && in[y * w + x] < 0.f) { ++len; continue; }
+                if (len > 0) {
+                    t->invalid_runs_count++;
+                    if (len > gap) t->invalid_runs_truncated++;
+                    t->run_length_buckets[len < 4 ? 0 : len < 8 ? 1 : len < 16 ? 2 : len < 24 ? 3 : len < 32 ? 4
+                                          : len < 48 ? 5 : len < 64 ? 6 : len < 96 ? 7 : len < 128 ? 8 : 9]++;
+                    len = 0;
+                }
+            }
+        }
         for (int x = 0; x < w; ++x) {
             const int i = y * w + x;
             if (in[i] >= 0.f) continue;
@@ -633,19 +699,29 @@ void orc_fill_holes(const apg_pipeline_config_t* cfg, int w, int h, const float*
             while (xr < w && xr <= x + gap && in[y * w + xr] < 0.f) ++xr;
             const float dl = (xl >= 0 && in[y * w + xl] >= 0.f) ? in[y * w + xl] : -1.f;
             const float dr = (xr < w && in[y * w + xr] >= 0.f) ? in[y * w + xr] : -1.f;
+            if (t) {
+                t->total_invalid_pixels++;
+                if (reason[i] == ORC_OCCLUSION) t->classified_occ_pixels++;
+                else if (reason[i] == ORC_MISMATCH) t->classified_mismatch_pixels++;
+                if (xl < 0 || x - xl > gap || xr >= w || xr - x > gap) t->hit_max_gap_pixels++;
+            }
+            int route;
             /* ShadowReclass (postprocess.cpp:170-192): a mismatch between valid neighbours >= 4 px
              * apart is filled like an occlusion */
             const int shadow = g_ip_method == 1 && reason[i] == ORC_MISMATCH && dl >= 0.f && dr >= 0.f &&
                                fabsf(dr - dl) >= 4.0f;
             if (reason[i] == ORC_OCCLUSION || shadow) {
-                if (dl >= 0.f && dr >= 0.f) out[i] = fminf_ref(dl, dr);
-                else if (dl >= 0.f) out[i] = dl;
-                else if (dr >= 0.f) out[i] = dr;
+                if (t && shadow) t->reclassified_shadow_pixels++;
+                if (dl >= 0.f && dr >= 0.f) { out[i] = fminf_ref(dl, dr); route = 1; }
+                else if (dl >= 0.f) { out[i] = dl; route = 2; }
+                else if (dr >= 0.f) { out[i] = dr; route = 3; }
+                else route = 10;
+                if (t) t->route_counts[route]++;
                 continue;
             }
             const int c0 = lgray[i];
             float best_d = -1.f;
-            int best_abs = 999;
+            int best_abs = 999, best_vert = 0;
             const int cx[4] = {xl, xr, x, x};
             const int cy[4] = {y, y, y - 1, y + 1};
             const int en[4] = {1, 1, y > 0, y + 1 < h};
@@ -656,20 +732,28 @@ void orc_fill_holes(const apg_pipeline_config_t* cfg, int w, int h, const float*
                 const float d = in[yy * w + xx];
                 if (d < 0.f) continue;
                 const int ad = abs((int)lgray[yy * w + xx] - c0);
-                if (ad < best_abs) { best_abs = ad; best_d = d; }
+                if (ad < best_abs) { best_abs = ad; best_d = d; best_vert = k >= 2; }
             }
             if (best_d >= 0.f && best_abs <= 18) {
                 out[i] = best_d;
+                route = best_vert ? 5 : 4;
             } else if (d_prior && d_prior[i] >= 0.f) {
                 out[i] = d_prior[i];
+                route = 6;
             } else if (dl >= 0.f && dr >= 0.f) {
-                const float t = (float)(x - xl) / (float)(xr - xl);
-                out[i] = dl * (1.f - t) + dr * t;
+                const float tt = (float)(x - xl) / (float)(xr - xl);
+                out[i] = dl * (1.f - tt) + dr * tt;
+                route = 7;
             } else if (dl >= 0.f) {
                 out[i] = dl;
+                route = 8;
             } else if (dr >= 0.f) {
                 out[i] = dr;
+                route = 9;
+            } else {
+                route = 10;
             }
+            if (t) t->route_counts[route]++;
         }
     }
 }

@@ -18,6 +18,7 @@
 #include <stdint.h>
 #include "../include/apg_sgm/pipeline_config.h"
 #include "../include/apg_sgm/metrics.h"
+#include "../include/apg_sgm/telemetry.h"
 
 #ifdef __cplusplus
 extern "C" {
@@ -122,6 +123,9 @@ void orc_evaluate_supports(const orc_support_t* s, int n, const float* gt, int w
 /* Experimental scopes: sub-pixel method 0 Legacy, 1 CurvGate, 2 ConfGate, 3 Stabilized with its
  * parameter; inpaint method 0 Legacy, 1 ShadowReclass with its gap.  Defaults (0, 0, 0, 32). */
 void orc_set_experimental(int sp_method, float sp_param, int ip_method, int ip_gap);
+/* The scopes' telemetry: on/off, read, reset (the oracle's totals, over every pipeline run). */
+void orc_set_telemetry(int subpixel, int inpaint);
+void orc_get_telemetry(apg_subpixel_telemetry_t* sp, apg_inpaint_telemetry_t* ip);
 
 uint64_t orc_fnv1a64(const uint8_t* data, uint64_t n);
 void orc_config_from_mode(int mode, int max_disparity, apg_pipeline_config_t* out);

@@ -115,6 +115,28 @@ class SupportMetricsRec(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class SubpixelTelemetryRec(C.Structure):
+    """apg_subpixel_telemetry_t (include/apg_sgm/telemetry.h)."""
+    _fields_ = [("candidate_pixels", C.c_ulonglong), ("applied_pixels", C.c_ulonglong),
+                ("degenerate_count", C.c_ulonglong), ("clamped_count", C.c_ulonglong),
+                ("negative_curvature_count", C.c_ulonglong), ("sum_abs_delta", C.c_double),
+                ("delta_buckets", C.c_ulonglong * 50)]
+
+
+class InpaintTelemetryRec(C.Structure):
+    """apg_inpaint_telemetry_t (include/apg_sgm/telemetry.h)."""
+    _fields_ = [("total_invalid_pixels", C.c_ulonglong), ("classified_occ_pixels", C.c_ulonglong),
+                ("classified_mismatch_pixels", C.c_ulonglong), ("hit_max_gap_pixels", C.c_ulonglong),
+                ("reclassified_shadow_pixels", C.c_ulonglong), ("route_counts", C.c_ulonglong * 11),
+                ("invalid_runs_count", C.c_ulonglong), ("invalid_runs_truncated", C.c_ulonglong),
+                ("run_length_buckets", C.c_ulonglong * 10)]
+
+
+def telemetry_dict(rec) -> dict:
+    return {k: (list(getattr(rec, k)) if k in ("delta_buckets", "route_counts", "run_length_buckets")
+                else getattr(rec, k)) for k, _ in rec._fields_}
+
+
 _orc = None
 _ref = None
 
@@ -488,13 +510,23 @@ def supports(cfg: PipelineConfig, left, right):
 
 
 def set_experimental(sp_method: int = 0, sp_param: float = 0.0, ip_method: int = 0, ip_gap: int = 32,
-                     reference: bool = False):
-    """The experimental scopes (sub-pixel method/param, inpaint method/gap) of the oracle, or with
-    reference=True the reference's own scopes on the calling thread."""
+                     reference: bool = False, sp_telemetry: bool = False, ip_telemetry: bool = False):
+    """The experimental scopes (sub-pixel method/param, inpaint method/gap, telemetry on/off: on
+    clears the totals) of the oracle, or with reference=True the reference's own scopes on the
+    calling thread."""
     if reference:
-        ref_lib().ref_set_experimental(C.c_int(sp_method), C.c_float(sp_param), C.c_int(ip_method), C.c_int(ip_gap))
+        ref_lib().ref_set_experimental_tel(C.c_int(sp_method), C.c_float(sp_param), C.c_int(int(sp_telemetry)),
+                                           C.c_int(ip_method), C.c_int(ip_gap), C.c_int(int(ip_telemetry)))
     else:
         lib().orc_set_experimental(C.c_int(sp_method), C.c_float(sp_param), C.c_int(ip_method), C.c_int(ip_gap))
+        lib().orc_set_telemetry(C.c_int(int(sp_telemetry)), C.c_int(int(ip_telemetry)))
+
+
+def get_telemetry(reference: bool = False):
+    """(sub-pixel, inpaint) telemetry totals as dicts: the oracle's or the reference's."""
+    sp, ip = SubpixelTelemetryRec(), InpaintTelemetryRec()
+    (ref_lib().ref_get_telemetry if reference else lib().orc_get_telemetry)(C.byref(sp), C.byref(ip))
+    return telemetry_dict(sp), telemetry_dict(ip)
 
 
 class RefSession:

@@ -27,6 +27,7 @@
 #include "subpixel_estimator.hpp"
 
 #include "../include/apg_sgm/metrics.h"
+#include "../include/apg_sgm/telemetry.h"
 #include "../include/apg_sgm/pipeline_config.h"
 
 #include <algorithm>
@@ -480,11 +481,37 @@ int ref_save_pfm(const char* path, const float* d, int w, int h) {
 static std::unique_ptr<ExperimentalInpaintScope> g_ip_scope;
 static std::unique_ptr<ExperimentalSubpixelScope> g_sp_scope;
 
-void ref_set_experimental(int sp_method, float sp_param, int ip_method, int ip_gap) {
+void ref_set_experimental_tel(int sp_method, float sp_param, int sp_tel, int ip_method, int ip_gap, int ip_tel) {
     g_ip_scope.reset();
     g_sp_scope.reset();
-    g_sp_scope.reset(new ExperimentalSubpixelScope(static_cast<SubpixelMethod>(sp_method), sp_param, false));
-    g_ip_scope.reset(new ExperimentalInpaintScope(static_cast<InpaintMethod>(ip_method), ip_gap, false));
+    g_sp_scope.reset(new ExperimentalSubpixelScope(static_cast<SubpixelMethod>(sp_method), sp_param, sp_tel != 0));
+    g_ip_scope.reset(new ExperimentalInpaintScope(static_cast<InpaintMethod>(ip_method), ip_gap, ip_tel != 0));
+}
+
+void ref_set_experimental(int sp_method, float sp_param, int ip_method, int ip_gap) {
+    ref_set_experimental_tel(sp_method, sp_param, 0, ip_method, ip_gap, 0);
+}
+
+// The reference's telemetry totals of the calling thread (current_telemetry() of both scopes).
+void ref_get_telemetry(apg_subpixel_telemetry_t* sp, apg_inpaint_telemetry_t* ip) {
+    const SubpixelTelemetry& s = ExperimentalSubpixelScope::current_telemetry();
+    sp->candidate_pixels = s.candidate_pixels;
+    sp->applied_pixels = s.applied_pixels;
+    sp->degenerate_count = s.degenerate_count;
+    sp->clamped_count = s.clamped_count;
+    sp->negative_curvature_count = s.negative_curvature_count;
+    sp->sum_abs_delta = s.sum_abs_delta;
+    for (int i = 0; i < 50; ++i) sp->delta_buckets[i] = s.delta_buckets[i];
+    const InpaintTelemetry& t = ExperimentalInpaintScope::current_telemetry();
+    ip->total_invalid_pixels = t.total_invalid_pixels;
+    ip->classified_occ_pixels = t.classified_occ_pixels;
+    ip->classified_mismatch_pixels = t.classified_mismatch_pixels;
+    ip->hit_max_gap_pixels = t.hit_max_gap_pixels;
+    ip->reclassified_shadow_pixels = t.reclassified_shadow_pixels;
+    for (int i = 0; i < 11; ++i) ip->route_counts[i] = t.route_counts[i];
+    ip->invalid_runs_count = t.invalid_runs_count;
+    ip->invalid_runs_truncated = t.invalid_runs_truncated;
+    for (int i = 0; i < 10; ++i) ip->run_length_buckets[i] = t.run_length_buckets[i];
 }
 
 // The reference's evaluate_supports (src/metrics.cpp:8-124) on plain arrays.

@@ -79,5 +79,32 @@ def test_python_scopes_nest_and_are_thread_local(apg):
     assert apg._get_experimental() == (0, 0.0, 0, 32)
     with pytest.raises(ValueError):
         apg.ExperimentalInpaintScope("bogus")
-    with pytest.raises(NotImplementedError):
-        apg.ExperimentalSubpixelScope("legacy", collect_telemetry=True)
+    with apg.ExperimentalSubpixelScope("legacy", collect_telemetry=True):
+        with apg.ExperimentalInpaintScope("legacy", collect_telemetry=True):
+            assert apg._get_telemetry_flags() == (1, 1)
+        assert apg._get_telemetry_flags() == (1, 0)
+        assert apg.ExperimentalSubpixelScope.current_telemetry().candidate_pixels == 0
+    assert apg._get_telemetry_flags() == (0, 0)
+
+
+TEL_CASES = [(1, (2, 0.0, 1, 16), 0), (2, (3, 0.0, 0, 32), 0), (1, (0, 0.0, 0, 32), 1), (0, (1, 6.0, 0, 8), 0)]
+
+
+@pytest.mark.parametrize("case", TEL_CASES, ids=[f"m{m}_sp{s[0]}_ip{s[2]}_h{h}" for m, s, h in TEL_CASES])
+def test_telemetry_oracle_matches_reference(case, O, scoped):
+    """SubpixelTelemetry / InpaintTelemetry of one frame (the reference's own scopes with
+    collect_telemetry, through its StereoSession) against the oracle's, the hierarchical coarse
+    pass included."""
+    if not O.ref_available():
+        pytest.skip("reference build (oracle/_ref) not present")
+    mode, scope, hier = case
+    L, R = synth(96, 64, 32, patch=0.25, seed=21 + mode)
+    O.set_experimental(*scope, sp_telemetry=True, ip_telemetry=True)
+    O.set_experimental(*scope, reference=True, sp_telemetry=True, ip_telemetry=True)
+    O.pipeline(O.config(mode, 32, hier_enable=hier), L, R)
+    s = O.RefSession(O.config(mode, 32, volume_backend=2, hier_enable=hier), bounded_reuse=True)
+    assert s.process(L, R)["status"] == 0
+    (sa, ia), (sb, ib) = O.get_telemetry(), O.get_telemetry(reference=True)
+    assert sa.pop("sum_abs_delta") == pytest.approx(sb.pop("sum_abs_delta"), rel=1e-12)
+    assert sa == sb and ia == ib
+    assert sa["candidate_pixels"] > 0 and ia["total_invalid_pixels"] > 0

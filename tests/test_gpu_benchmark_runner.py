@@ -34,15 +34,18 @@ def _manifest(apg, d):
 
 @pytest.mark.parametrize("extra", [[], ["--subpixel-method", "conf_gate", "--inpaint-method", "shadow_reclass",
                                         "--inpaint-gap", "12"],
-                                   ["--hierarchical", "--hierarchical-adaptive", "--hierarchical-fallback", "expanded"]],
-                         ids=["default", "scopes", "hierarchical"])
+                                   ["--hierarchical", "--hierarchical-adaptive", "--hierarchical-fallback", "expanded"],
+                                   ["--subpixel-method", "stabilized", "--subpixel-telem", "--inpaint-telem",
+                                    "--repeat", "2"]],
+                         ids=["default", "scopes", "hierarchical", "telemetry"])
 def test_runner_matches_reference_runner(O, apg, tmp_path, extra):
     exe = O.HERE / "_ref" / "benchmark_stereo"
     if not exe.exists():
         pytest.skip("reference runner (oracle/_ref/benchmark_stereo) not built")
     from apg_sgm_b200 import benchmark as B
     m = _manifest(apg, tmp_path)
-    args = ["--manifest", str(m), "--ablation", "A,C,E,F", "--warmup", "0", "--repeat", "1"] + extra
+    args = ["--manifest", str(m), "--ablation", "A,C,E,F", "--warmup", "0"] + \
+        (["--repeat", "1"] if "--repeat" not in extra else []) + extra
     r = subprocess.run([str(exe)] + args + ["--output", str(tmp_path / "ref.csv")], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
     assert B.main(args + ["--output", str(tmp_path / "ours.csv")]) == 0

@@ -120,3 +120,47 @@ def test_batch_under_scope_and_default_elsewhere(O, apg, oracle_scope):
         t.join()
     for k in MAPS:
         assert same_bits(res["out"][k], base[k]), k
+
+
+TEL_CASES = [(1, (2, 0.0, 1, 16), 0), (2, (3, 0.0, 0, 32), 0), (1, (0, 0.0, 0, 32), 1), (0, (1, 6.0, 0, 8), 0)]
+
+
+@pytest.mark.parametrize("case", TEL_CASES, ids=[f"m{m}_sp{s[0]}_ip{s[2]}_h{h}" for m, s, h in TEL_CASES])
+def test_telemetry_matches_oracle(case, O, apg, oracle_scope):
+    """The scopes' telemetry counted on the device (WTA sub-pixel step, hole fill, run lengths; the
+    hierarchical coarse pass included) equals the oracle's; two frames accumulate; the batched form
+    collects its pairs'."""
+    mode, (sm, sp, im, ig), hier = case
+    L, R = synth(160, 96, 48, patch=0.25, seed=31 + mode)
+    cfg = apg.config_from_mode(mode, 48, hier_enable=hier)
+    O.set_experimental(sm, sp, im, ig, sp_telemetry=True, ip_telemetry=True)
+    O.pipeline(to_oracle(O, cfg), L, R)
+    O.pipeline(to_oracle(O, cfg), L, R)
+    want_sp, want_ip = O.get_telemetry()
+    e = apg.Engine(cfg)
+    with apg.ExperimentalSubpixelScope(sm, sp, collect_telemetry=True), \
+            apg.ExperimentalInpaintScope(im, ig, collect_telemetry=True):
+        e.process(L, R)
+        e.process(L, R)
+        got_sp = apg.ExperimentalSubpixelScope.current_telemetry()
+        got_ip = apg.ExperimentalInpaintScope.current_telemetry()
+    e.close()
+    for k, v in want_sp.items():
+        if k == "sum_abs_delta":
+            assert got_sp.sum_abs_delta == pytest.approx(v, rel=1e-12)
+        else:
+            assert getattr(got_sp, k) == v, k
+    for k, v in want_ip.items():
+        assert getattr(got_ip, k) == v, k
+    assert got_sp.candidate_pixels > 0 and got_ip.total_invalid_pixels > 0
+    assert 0.0 <= got_sp.applied_ratio() <= 1.0 and 0.0 <= got_ip.fill_ratio() <= 1.0
+    # the batched form, two pairs of this size: the same counters as two engine frames
+    if not hier:
+        b = apg.Batch(cfg)
+        with apg.ExperimentalSubpixelScope(sm, sp, collect_telemetry=True), \
+                apg.ExperimentalInpaintScope(im, ig, collect_telemetry=True):
+            b.process([(L, R), (L, R)])
+            bsp = apg.ExperimentalSubpixelScope.current_telemetry()
+            bip = apg.ExperimentalInpaintScope.current_telemetry()
+        b.close()
+        assert bsp.candidate_pixels == want_sp["candidate_pixels"] and bip.route_counts == want_ip["route_counts"]
