@@ -213,7 +213,7 @@ __global__ void __launch_bounds__(128) cross_v_default_kernel(int w, int h, int 
 // sums of (valid low half) | (valid high half) << 8: a window difference is exact in every lane
 // because a window's sum is below 2^16 (host-checked for the arm length and cost_max) and its
 // counts are at most 2*lmax + 1 <= 255.  The centre pixel's range is staged with the arms.
-template <int RS>
+template <int RS, int KB>
 __global__ void __launch_bounds__(256) cross_v_count_kernel(int w, int h, int d0, int D, int Dp, int lmax, int tau,
                                                             int cols, const uint8_t* __restrict__ gray,
                                                             const int16_t* __restrict__ rmin,
@@ -272,11 +272,11 @@ __global__ void __launch_bounds__(256) cross_v_count_kernel(int w, int h, int d0
     ringc[tid] = 0;
     const size_t rowstride = (size_t)w * W2;
     const uint32_t* src = tin + ((size_t)ystart * w + x) * W2 + k;
-    uint32_t cur[kB], nxt[kB];
+    uint32_t cur[KB], nxt[KB];
 #pragma unroll
-    for (int i = 0; i < kB; ++i) cur[i] = ystart + i < yend ? __ldcs(src + i * rowstride) : 0u;
+    for (int i = 0; i < KB; ++i) cur[i] = ystart + i < yend ? __ldcs(src + i * rowstride) : 0u;
 #pragma unroll
-    for (int i = 0; i < kB; ++i) nxt[i] = ystart + kB + i < yend ? __ldcs(src + (kB + i) * rowstride) : 0u;
+    for (int i = 0; i < KB; ++i) nxt[i] = ystart + KB + i < yend ? __ldcs(src + (KB + i) * rowstride) : 0u;
     int pushed = ystart;
     uint32_t ps = 0;
     uint32_t pc = 0;  // low 16 bits used
@@ -285,23 +285,23 @@ __global__ void __launch_bounds__(256) cross_v_count_kernel(int w, int h, int d0
         const int need = min(h, min(yb + kQ, y1) + lmax);
         while (pushed < need) {
 #pragma unroll
-            for (int i = 0; i < kB; ++i) {
+            for (int i = 0; i < KB; ++i) {
                 if (pushed + i < yend) {
                     const uint32_t v = cur[i];
                     const bool lo_bad = (v & 0xFFFFu) == 0xFFFFu, hi_bad = v >= 0xFFFF0000u;
                     ps += v & ((lo_bad ? 0u : 0x0000FFFFu) | (hi_bad ? 0u : 0xFFFF0000u));
                     pc += (lo_bad ? 0u : 1u) + (hi_bad ? 0u : 0x100u);
-                    const int slot = ((pushed + i - ystart + 1) & (RS - 1)) * nthr + tid;
+                    const int slot = (int)((unsigned)(pushed + i - ystart + 1) % RS) * nthr + tid;
                     ring[slot] = ps;
                     ringc[slot] = (uint16_t)pc;
                 }
             }
-            pushed += kB;
+            pushed += KB;
 #pragma unroll
-            for (int i = 0; i < kB; ++i) cur[i] = nxt[i];
-            const int base = pushed + kB;
+            for (int i = 0; i < KB; ++i) cur[i] = nxt[i];
+            const int base = pushed + KB;
 #pragma unroll
-            for (int i = 0; i < kB; ++i)
+            for (int i = 0; i < KB; ++i)
                 nxt[i] = base + i < yend ? __ldcs(src + (size_t)(base + i - ystart) * rowstride) : 0u;
         }
 #pragma unroll
@@ -310,7 +310,8 @@ __global__ void __launch_bounds__(256) cross_v_count_kernel(int w, int h, int d0
             if (y >= y1) break;
             const int ai = ci * kSeg + (y - y0);
             const int a = y - armU[ai], b = y + armD[ai];  // inclusive window
-            const int sb = ((b - ystart + 1) & (RS - 1)) * nthr + tid, sa = ((a - ystart) & (RS - 1)) * nthr + tid;
+            const int sb = (int)((unsigned)(b - ystart + 1) % RS) * nthr + tid;
+            const int sa = (int)((unsigned)(a - ystart) % RS) * nthr + tid;
             const uint32_t sum = ring[sb] - ring[sa];
             const uint32_t cnt = (uint32_t)(uint16_t)(ringc[sb] - ringc[sa]);
             const uint32_t rg = s_rng[ai];
@@ -422,10 +423,11 @@ cudaError_t launch_cross_v(int w, int h, int d0, int D, int Dp, int lmax, int ta
         // any ranges: sum and count rings, batched loads
         const size_t extra = (size_t)cols * kSeg * 4 + (size_t)(2 * lmax + 2) * 4 + (size_t)cols * (kSeg + 2 * lmax) +
                              (size_t)cols * kSeg * 2;
-        auto go = [&](auto rs_tag) -> cudaError_t {
+        auto go = [&](auto rs_tag, auto kb_tag) -> cudaError_t {
             constexpr int RS = decltype(rs_tag)::value;
+            constexpr int KB = decltype(kb_tag)::value;
             const size_t smem = (size_t)RS * nthr * 6 + extra;
-            auto kern = cross_v_count_kernel<RS>;
+            auto kern = cross_v_count_kernel<RS, KB>;
             {
                 const cudaError_t e = allow_dynamic_smem(kern, smem);
                 if (e != cudaSuccess) return e;
@@ -436,9 +438,13 @@ cudaError_t launch_cross_v(int w, int h, int d0, int D, int Dp, int lmax, int ta
             return cudaGetLastError();
         };
         auto fits = [&](int rs) { return (size_t)rs * nthr * 6 + extra <= 200 * 1024; };
-        if (span <= 64 && fits(64)) return go(std::integral_constant<int, 64>());
-        if (span <= 128 && fits(128)) return go(std::integral_constant<int, 128>());
-        if (span <= 256 && fits(256)) return go(std::integral_constant<int, 256>());
+        // the default arm (lmax <= 17) with 8-row load batches: a ring of exactly the 52 live rows,
+        // whose smaller footprint fits five blocks on an SM instead of four
+        using I = std::integral_constant<int, 8>;
+        if (2 * lmax + 8 + kQ + 2 <= 52 && fits(52)) return go(std::integral_constant<int, 52>(), I());
+        if (span <= 64 && fits(64)) return go(std::integral_constant<int, 64>(), std::integral_constant<int, kB>());
+        if (span <= 128 && fits(128)) return go(std::integral_constant<int, 128>(), std::integral_constant<int, kB>());
+        if (span <= 256 && fits(256)) return go(std::integral_constant<int, 256>(), std::integral_constant<int, kB>());
     }
     const int RS = 2 * lmax + 2;
     const size_t smem = (size_t)RS * nthr * 8 + (size_t)cols * kSeg * 2;
