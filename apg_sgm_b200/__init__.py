@@ -211,11 +211,86 @@ _POLICIES = {"bounded_reuse": MemoryPolicy.BoundedReuse, "boundedreuse": MemoryP
              "release": MemoryPolicy.ReleasePerFrame, "releaseperframe": MemoryPolicy.ReleasePerFrame}
 
 
+class _ResultPool:
+    """apg_result_t objects (each owns one page-locked block holding a frame's four maps) lent to
+    the arrays that StereoSession.process returns.  A result goes back to the pool when the last
+    array viewing it is gone, so in a loop that drops each frame's arrays before the next call the
+    same one or two blocks serve every frame, with no allocation and no copy; results kept alive by
+    the caller simply make the pool lend a new block."""
+
+    def __init__(self, keep: int = 4):
+        self._free = []
+        self._keep = keep
+        self._mu = threading.Lock()
+        self._closed = False
+
+    def take(self):
+        with self._mu:
+            if self._free:
+                return self._free.pop()
+        r = lib().apg_result_create()
+        if not r:
+            raise MemoryError("apg_result_create failed")
+        return r
+
+    def give_back(self, r):
+        with self._mu:
+            if not self._closed and len(self._free) < self._keep:
+                self._free.append(r)
+                return
+        lib().apg_result_destroy(r)
+
+    def close(self):
+        with self._mu:
+            self._closed = True
+            free, self._free = self._free, []
+        for r in free:
+            lib().apg_result_destroy(r)
+
+
+class _ResultLease:
+    """Holds one pooled apg_result_t while any array views its maps."""
+
+    __slots__ = ("_pool", "_r")
+
+    def __init__(self, pool: _ResultPool, r):
+        self._pool, self._r = pool, r
+
+    def __del__(self):
+        try:
+            self._pool.give_back(self._r)
+        except Exception:
+            pass
+
+
+def _result_views(res, lease, w: int, h: int):
+    """The four maps of a filled apg_result_t as numpy arrays over its page-locked block (no copy);
+    the block stays lent to them (through `lease`) until the last of them is gone."""
+    L = lib()
+    n = w * h
+    pd = L.apg_result_get_disparity(res, None, None)
+    ptrs = (pd, L.apg_result_get_confidence(res, None, None), L.apg_result_get_invalid_reason(res, None, None),
+            L.apg_result_get_reliable_mask(res, None, None))
+    offs = [p - pd for p in ptrs]
+    if any(o < 0 or o > 9 * n for o in offs):
+        raise RuntimeError("result maps are not one block")
+    block = (C.c_uint8 * (10 * n)).from_address(pd)
+    block._lease = lease
+    disp = np.frombuffer(block, np.float32, n, offs[0]).reshape(h, w)
+    conf = np.frombuffer(block, np.float32, n, offs[1]).reshape(h, w)
+    reason = np.frombuffer(block, np.uint8, n, offs[2]).reshape(h, w)
+    rel = np.frombuffer(block, np.uint8, n, offs[3]).reshape(h, w)
+    return disp, conf, rel, reason
+
+
 class StereoSession:
     """Stateful streaming matcher session (PyStereoSession, binding.cpp:147-357).
 
     Calls on one session are serialised by a lock; independent sessions run concurrently
-    (ctypes releases the GIL for the duration of every library call)."""
+    (ctypes releases the GIL for the duration of every library call).  process() returns arrays
+    that view a page-locked result block the device copies landed in (binding.cpp:483-531 returns
+    views over a fresh per-call result in the same way): no copy, and the block is not reused
+    while any of them is alive."""
 
     def __init__(self, mode="balanced", threads=0, max_disparity=128, min_disparity=0, backend="auto",
                  memory_policy="release_per_frame", max_retained_bytes=0, hierarchical=False, hierarchical_radius=4,
@@ -259,7 +334,7 @@ class StereoSession:
         self._h = lib().apgcu_session_create_config(C.byref(cfg), int(mp), C.c_size_t(int(max_retained_bytes)))
         if not self._h:
             raise RuntimeError("failed to create session")
-        self._res = lib().apg_result_create()
+        self._results = _ResultPool()
         self._mu = threading.Lock()
 
     @property
@@ -276,26 +351,24 @@ class StereoSession:
             raise ValueError(f"Left and right images must have matching channel counts ({lv.channels} vs "
                              f"{rv.channels})")
         L = lib()
+        res = self._results.take()
+        lease = _ResultLease(self._results, res)
         with self._mu:
-            rc = L.apg_session_process(self._h, C.byref(lv), C.byref(rv), self._res)
+            rc = L.apg_session_process(self._h, C.byref(lv), C.byref(rv), res)
             if rc != 0:
                 msg = L.apg_session_get_last_error(self._h).decode()
                 raise RuntimeError(f"Stereo processing failed [{rc}]: {msg}")
-            w, h = C.c_int(), C.c_int()
-            n = lv.width * lv.height
-
-            def grab(fn, ctype, dtype):
-                p = fn(self._res, C.byref(w), C.byref(h))
-                return np.ctypeslib.as_array(C.cast(p, C.POINTER(ctype)), shape=(n,)).reshape(h.value, w.value).copy()
-
-            disp = grab(L.apg_result_get_disparity, C.c_float, np.float32)
-            conf = grab(L.apg_result_get_confidence, C.c_float, np.float32)
-            rel = grab(L.apg_result_get_reliable_mask, C.c_uint8, np.uint8)
-            reason = grab(L.apg_result_get_invalid_reason, C.c_uint8, np.uint8)
-            stats = self._stats(disp.shape[1], disp.shape[0])
+            disp, conf, rel, reason = _result_views(res, lease, lv.width, lv.height)
+            stats = self._stats(lv.width, lv.height)
         return StereoResult(disp, conf, rel, reason, stats)
 
     compute = process
+
+    def set_tuning(self, key: str, value: int):
+        """Engine tuning key for this session's frames (Engine.set_tuning's keys)."""
+        rc = lib().apgcu_session_set_tuning(self._h, key.encode(), int(value))
+        if rc != 0:
+            raise ValueError(f"invalid tuning {key}={value}")
 
     def _stats(self, w: int, h: int) -> PipelineStats:
         """PipelineStats of the last frame; the pixel counters come from the device
@@ -392,9 +465,8 @@ class StereoSession:
             if getattr(self, "_h", None):
                 lib().apg_session_destroy(self._h)
                 self._h = None
-            if getattr(self, "_res", None):
-                lib().apg_result_destroy(self._res)
-                self._res = None
+            if getattr(self, "_results", None):
+                self._results.close()  # results still lent to live arrays are freed when those go
         except Exception:
             pass
 

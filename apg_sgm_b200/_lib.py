@@ -200,6 +200,7 @@ _SIGS = {
     "apgcu_config_from_mode": (None, [C.c_int, C.c_int, C.POINTER(PipelineConfig)]),
     "apgcu_session_create_config": (C.c_void_p, [C.POINTER(PipelineConfig), C.c_int, C.c_size_t]),
     "apgcu_session_get_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_size_t)]),
+    "apgcu_session_set_tuning": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int]),
     "apgcu_session_estimate_bytes": (C.c_size_t, [C.c_void_p, C.c_int, C.c_int, C.c_int]),
     "apgcu_session_get_frame_counts": (C.c_int, [C.c_void_p, C.POINTER(C.c_ulonglong)]),
     "apgcu_session_hier_telemetry": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),

@@ -1056,7 +1056,7 @@ int Engine::run_refine(float* work) {
     if (e == cudaSuccess) e = launch_refine_pack(cc, L, arena_, stream_, &launches);
     for (int it = 0; it < iters && e == cudaSuccess; ++it) {
         e = launch_refine_count(L, arena_, work, (it % 2) == 0, stream_, &launches);
-        if (e == cudaSuccess) e = launch_refine_pass(cc, L, arena_, rtab_, it, work, stream_, &launches);
+        if (e == cudaSuccess) e = launch_refine_pass(cc, L, arena_, rtab_, it, work, refine_, stream_, &launches);
     }
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(refine_err_host_, state + kRefineErrWord * 4, sizeof(int), cudaMemcpyDeviceToHost, stream_);
@@ -1157,6 +1157,40 @@ int Engine::dump(int what, void* dst, size_t bytes) {
     return e == cudaSuccess ? kOk : cuda_fail(e, "dump");
 }
 
+int set_tuning(Engine* e, const char* key, int value) {
+    if (std::strcmp(key, "sgm_lanes") == 0) {
+        if (value != 0 && value != 8 && value != 16 && value != 32) return kInvalidConfig;
+        if (e) e->set_sgm_lanes(value);
+        return kOk;
+    }
+    if (std::strcmp(key, "cost_tile") == 0) {
+        if (value != 0 && value != 64 && value != 128 && value != 256) return kInvalidConfig;
+        if (e) e->set_cost_tile(value);
+        return kOk;
+    }
+    if (std::strcmp(key, "cost_kernel") == 0) {
+        if (value != 0 && value != 1) return kInvalidConfig;
+        if (e) e->set_cost_kernel(value);
+        return kOk;
+    }
+    if (std::strcmp(key, "fast_fused") == 0) {
+        if (value != 0 && value != 1) return kInvalidConfig;
+        if (e) e->set_fast_fused(value != 0);
+        return kOk;
+    }
+    if (std::strcmp(key, "refine_spin_limit") == 0) {
+        if (value < 0) return kInvalidConfig;
+        if (e) e->set_refine_spin_limit(value);
+        return kOk;
+    }
+    if (std::strcmp(key, "refine_window") == 0) {
+        if (value != 0 && value != 1) return kInvalidConfig;
+        if (e) e->set_refine_window(value);
+        return kOk;
+    }
+    return kInvalidConfig;
+}
+
 }  // namespace apgcu
 
 // ------------------------------------------------------------------------------------------------
@@ -1194,27 +1228,7 @@ const char* apgcu_engine_last_error(apgcu_engine_t e) { return e ? e->eng->last_
 
 int apgcu_engine_set_tuning(apgcu_engine_t e, const char* key, int value) {
     if (!e || !key) return apgcu::kInternalError;
-    if (std::strcmp(key, "sgm_lanes") == 0) {
-        if (value != 0 && value != 8 && value != 16 && value != 32) return apgcu::kInvalidConfig;
-        e->eng->set_sgm_lanes(value);
-        return 0;
-    }
-    if (std::strcmp(key, "cost_tile") == 0) {
-        if (value != 0 && value != 64 && value != 128 && value != 256) return apgcu::kInvalidConfig;
-        e->eng->set_cost_tile(value);
-        return 0;
-    }
-    if (std::strcmp(key, "cost_kernel") == 0) {
-        if (value != 0 && value != 1) return apgcu::kInvalidConfig;
-        e->eng->set_cost_kernel(value);
-        return 0;
-    }
-    if (std::strcmp(key, "fast_fused") == 0) {
-        if (value != 0 && value != 1) return apgcu::kInvalidConfig;
-        e->eng->set_fast_fused(value != 0);
-        return 0;
-    }
-    return apgcu::kInvalidConfig;
+    return apgcu::set_tuning(e->eng, key, value);
 }
 
 int apgcu_engine_set_debug(apgcu_engine_t e, int flags) {

@@ -101,6 +101,13 @@ struct RefineTables {
     void release();
 };
 int refine_band_count(int h);
+// Refiner tuning (Engine::set_refine_*): the poll budget of each cross-band wait before it gives up
+// and flags the frame (0: the default, about a second) and the right-image window form (0: shared
+// memory where every band fits on the device at once, 1: always the L1-read form).
+struct RefineTuning {
+    int spin_limit = 0;
+    int window = 0;
+};
 
 class Engine {
 public:
@@ -153,6 +160,10 @@ public:
     void set_fast_fused(bool on) { fast_fused_ = on; }
     void set_cost_tile(int t) { cost_tile_ = t; }
     void set_cost_kernel(int k) { cost_kernel_ = k; }
+    // refiner waits: polls before a cross-band wait gives up (0: about a second); shared-memory
+    // right-image window (0: where it fits, 1: never, the L1 form)
+    void set_refine_spin_limit(int n) { refine_.spin_limit = n; }
+    void set_refine_window(int mode) { refine_.window = mode; }
     // takes the calling thread's experimental scopes now (run_pre does so for every frame; the
     // batched form needs them before it builds SGM plans from sgm_launch)
     void capture_scope() { scope_ = experimental_scope(); }
@@ -207,6 +218,7 @@ private:
     bool fast_fused_ = false;
     int cost_tile_ = 0;
     int cost_kernel_ = 0;  // 0: pixel-run cost kernel where it applies, 1: column-tile kernel
+    RefineTuning refine_;
     cudaStream_t stream_ = nullptr;
     bool own_stream_ = false;
     unsigned char* arena_ = nullptr;
@@ -255,6 +267,10 @@ private:
     std::string err_;
 };
 
+// The tuning keys of apgcu_engine_set_tuning for engines and sessions; kInvalidConfig for an
+// unknown key or a value out of range.  A null engine only validates the key and value.
+int set_tuning(Engine* e, const char* key, int value);
+
 // Process-wide launch counter (reported by bench.py as gpu_launches).
 void count_launches(unsigned n);
 unsigned long long launch_count();
@@ -270,7 +286,7 @@ cudaError_t launch_refine_pack(const CostCtx& c, const Layout& L, unsigned char*
 size_t refine_pack_bytes(int n, bool c64);
 size_t refine_steps_bytes(int n);
 cudaError_t launch_refine_pass(const CostCtx& c, const Layout& L, unsigned char* arena, const RefineTables& tab,
-                               int it, float* work, cudaStream_t s, unsigned* launches);
+                               int it, float* work, const RefineTuning& tune, cudaStream_t s, unsigned* launches);
 size_t refine_scan_temp_bytes(int n);
 
 }  // namespace apgcu

@@ -15,7 +15,10 @@
 // subpixel is on and the three neighbours along the diagonal are inside the image and valid.
 //
 // The scratch is one array per device, shared by every call on that device: two calls that
-// overlap in time on one device (different streams or host threads) race on it.
+// overlap in time on one device (different streams or host threads) race on it.  The array is part
+// of this library's device code: with CUDA's default lazy module loading it is created in a
+// context by the first call there (together with the kernels), so callers make one warm-up call at
+// start-up; with eager loading every context that loads the library holds it from the start.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -35,6 +38,23 @@ static __device__ __align__(256) uint32_t g_rwta_keys[kMaxPixels];
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
 uint32_t* g_keys_ptr[kMaxDevices] = {};
+void* g_keys_ctx[kMaxDevices] = {};  // the context the cached address belongs to
+
+// cuCtxGetCurrent from the driver, found through the runtime (no link-time libcuda dependency)
+using CtxGetCurrent = int (*)(void**);
+CtxGetCurrent ctx_get_current() {
+    static CtxGetCurrent fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            f = nullptr;
+        }
+        return reinterpret_cast<CtxGetCurrent>(f);
+    }();
+    return fn;
+}
 
 // The keys start at all-ones ("no candidate"); every call clears the pixels it will use.
 __global__ void noalloc_clear_kernel(uint32_t* __restrict__ keys, int n) {
@@ -52,8 +72,15 @@ __global__ void noalloc_argmin_kernel(const uint16_t* __restrict__ vol, int w, i
     const int y = blockIdx.y;
     const int x0 = blockIdx.x * tx;
     const int ncols = min(tx, w - x0);
-    for (int i = threadIdx.x; i < ncols * D; i += blockDim.x) {
-        const int j = i / D, di = i - j * D;
+    // element i = j * D + di of the tile; each thread steps by blockDim.x = dq * D + dr elements
+    const int dq = blockDim.x / D, dr = blockDim.x - dq * D;
+    int j = threadIdx.x / D, di = threadIdx.x - j * D;
+    for (; j < ncols; j += dq, di += dr) {
+        if (di >= D) {
+            di -= D;
+            ++j;
+            if (j >= ncols) break;
+        }
         s_tile[j * sp + di] = vol[((size_t)y * w + x0 + j) * pitch + di];
     }
     __syncthreads();
@@ -101,7 +128,9 @@ __global__ void noalloc_finalize_kernel(const uint16_t* __restrict__ vol, const 
 }
 
 // Device address of this device's key array: looked up once per device, with that device
-// current, on the first call there.
+// current, on the first call there (which also loads the module under lazy loading).  The address
+// is remembered with the context it was found in and looked up again when the device's current
+// context is another one (the primary context was reset and created anew).
 int keys_for_device(uint32_t** out) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) {
@@ -109,14 +138,23 @@ int keys_for_device(uint32_t** out) {
         return APG_STATUS_UNSUPPORTED_BACKEND;
     }
     if (dev < 0 || dev >= kMaxDevices) return APG_STATUS_UNSUPPORTED_BACKEND;
+    const CtxGetCurrent current = ctx_get_current();
+    auto context = [&]() -> void* {
+        void* c = nullptr;
+        if (current && current(&c) != 0) c = nullptr;
+        return c;
+    };
     std::lock_guard<std::mutex> lock(g_mu);
-    if (!g_keys_ptr[dev]) {
+    const void* ctx = context();  // null before the runtime has made a context current on this thread
+    if (!g_keys_ptr[dev] || !ctx || g_keys_ctx[dev] != ctx) {
         void* p = nullptr;
         if (cudaGetSymbolAddress(&p, g_rwta_keys) != cudaSuccess || !p) {
             cudaGetLastError();
+            g_keys_ptr[dev] = nullptr;
             return APG_STATUS_INTERNAL_ERROR;
         }
         g_keys_ptr[dev] = static_cast<uint32_t*>(p);
+        g_keys_ctx[dev] = context();  // the lookup made the device's primary context current
     }
     *out = g_keys_ptr[dev];
     return APG_STATUS_OK;
@@ -133,11 +171,16 @@ extern "C" APGCU_API int apgcu_right_wta_noalloc(const uint16_t* d_cost, int wid
     if (width <= 0 || height <= 0) return APG_STATUS_EMPTY_INPUT;
     if (num_disparities <= 0 || num_disparities > APGCU_NOALLOC_MAX_DISPARITIES)
         return APG_STATUS_INVALID_DISPARITY_RANGE;
+    // disparities, x + d and x - d stay far inside int for every accepted size
+    if (min_disparity < -APGCU_NOALLOC_MAX_ABS_DISPARITY || min_disparity > APGCU_NOALLOC_MAX_ABS_DISPARITY)
+        return APG_STATUS_INVALID_DISPARITY_RANGE;
     if (pitch < num_disparities) return APG_STATUS_SIZE_MISMATCH;
     if ((long long)width * height > kMaxPixels || height > 65535) return APG_STATUS_RESOURCE_LIMIT_EXCEEDED;
     uint32_t* keys = nullptr;
     int rc = keys_for_device(&keys);
     if (rc != APG_STATUS_OK) return rc;
+    // an error left on this thread by earlier work must not be read as this call's
+    cudaGetLastError();
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const int n = width * height;
     const int D = num_disparities;
@@ -148,11 +191,15 @@ extern "C" APGCU_API int apgcu_right_wta_noalloc(const uint16_t* d_cost, int wid
     const size_t smem = (size_t)tx * sp * 2;
     const int blocks = (n + 255) / 256 < 148 * 8 ? (n + 255) / 256 : 148 * 8;
     noalloc_clear_kernel<<<blocks, 256, 0, s>>>(keys, n);
+    if (cudaGetLastError() != cudaSuccess) return APG_STATUS_INTERNAL_ERROR;
+    count_launches(1);
     noalloc_argmin_kernel<<<dim3((width + tx - 1) / tx, height), 256, smem, s>>>(d_cost, width, D, pitch,
                                                                                 min_disparity, tx, sp, keys);
+    if (cudaGetLastError() != cudaSuccess) return APG_STATUS_INTERNAL_ERROR;
+    count_launches(1);
     noalloc_finalize_kernel<<<blocks, 256, 0, s>>>(d_cost, keys, width, height, D, pitch, min_disparity,
                                                    subpixel ? 1 : 0, d_disparity_right);
-    count_launches(3);
     if (cudaGetLastError() != cudaSuccess) return APG_STATUS_INTERNAL_ERROR;
+    count_launches(1);
     return APG_STATUS_OK;
 }

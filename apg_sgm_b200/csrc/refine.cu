@@ -510,7 +510,7 @@ cudaError_t launch_refine_pack(const CostCtx& c, const Layout& L, unsigned char*
 size_t refine_pack_bytes(int n, bool c64) { return (size_t)n * 2 * (c64 ? sizeof(RPack<true>) : sizeof(RPack<false>)); }
 
 cudaError_t launch_refine_pass(const CostCtx& c, const Layout& L, unsigned char* arena, const RefineTables& tab,
-                               int it, float* work, cudaStream_t s, unsigned* launches) {
+                               int it, float* work, const RefineTuning& tune, cudaStream_t s, unsigned* launches) {
     const int fwd = (it % 2) == 0;
     const int n = L.w * L.h;
     const int nbands = refine_band_count(L.h);
@@ -533,8 +533,9 @@ cudaError_t launch_refine_pass(const CostCtx& c, const Layout& L, unsigned char*
     ++*launches;
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    // about a second of waiting at most per wait (spins of ~128 ns sleep plus the poll)
-    int spin_limit = 1 << 23;
+    // about a second of waiting at most per wait (spins of ~128 ns sleep plus the poll), unless the
+    // engine's tuning sets a smaller poll budget
+    int spin_limit = tune.spin_limit > 0 ? tune.spin_limit : 1 << 23;
     CostCtx cc = c;
     const void* lpk = arena + L.rf_pack;
     const void* rpk = c.census64 ? (const void*)(reinterpret_cast<const RPack<true>*>(lpk) + n)
@@ -546,7 +547,7 @@ cudaError_t launch_refine_pass(const CostCtx& c, const Layout& L, unsigned char*
     int wmask = 0;
     size_t wbytes = 0;
     const void* kern = c.census64 ? (const void*)refine_band_kernel<true, false> : (const void*)refine_band_kernel<false, false>;
-    if (!c.census64) {
+    if (!c.census64 && tune.window == 0) {
         int rs = 1;
         while (rs < c.D + kRing) rs <<= 1;
         const size_t bytes = (size_t)kBand * (rs + 1) * sizeof(RPack<false>);

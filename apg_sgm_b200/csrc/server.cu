@@ -79,10 +79,27 @@ public:
         {
             std::lock_guard<std::mutex> lk(mu_);
             stop_ = true;
+            // requests still queued never run: they complete now with an error, so that a thread
+            // waiting for one returns
+            for (const unsigned long long id : queue_) {
+                Req& q = *reqs_.at(id);
+                q.status = kInternalError;
+                q.err = "server stopped before the request ran";
+                q.t_done = Clock::now();
+                q.done = true;
+                ++failed_;
+            }
+            queue_.clear();
         }
+        cv_done_.notify_all();
         cv_work_.notify_all();
         cv_mem_.notify_all();
         for (auto& t : workers_) t.join();
+        {
+            // threads inside wait() leave before the members they read go away
+            std::unique_lock<std::mutex> lk(mu_);
+            cv_done_.wait(lk, [&] { return waiters_ == 0; });
+        }
         cudaSetDevice(device_);
         idle_.clear();
     }
@@ -107,12 +124,15 @@ public:
         std::unique_lock<std::mutex> lk(mu_);
         auto it = reqs_.find(id);
         if (it == reqs_.end()) return fail_locked(kInternalError, "unknown ticket");
+        ++waiters_;
         cv_done_.wait(lk, [&] { return it->second->done; });
         Req& q = *it->second;
         if (latency_ms) *latency_ms = std::chrono::duration<double, std::milli>(q.t_done - q.t_submit).count();
         const int st = q.status;
         if (st) err_ = q.err;
         reqs_.erase(it);
+        --waiters_;
+        cv_done_.notify_all();
         return st;
     }
 
@@ -243,13 +263,23 @@ private:
             Held h;
             if (rc == kOk) {
                 const PoolKey k{r.mode, r.width, r.height, r.channels, c.min_disparity, c.max_disparity};
+                bool stopped = false;
                 for (;;) {
                     bool wait_mem = false;
                     h = acquire_locked(k, c, &rc, &wait_mem);
-                    if (!wait_mem || stop_) break;
+                    if (!wait_mem) break;
+                    if (stop_) {
+                        stopped = true;  // no reservation was made: the request fails
+                        break;
+                    }
                     cv_mem_.wait(lk);
                 }
-                if (rc == kResourceLimitExceeded) msg = "request workspace exceeds the HBM admission budget";
+                if (stopped) {
+                    rc = kInternalError;
+                    msg = "server stopped while the request waited for device memory";
+                } else if (rc == kResourceLimitExceeded) {
+                    msg = "request workspace exceeds the HBM admission budget";
+                }
             }
             ++in_flight_;
             peak_in_flight_ = std::max(peak_in_flight_, (unsigned long long)in_flight_);
@@ -298,6 +328,7 @@ private:
     std::vector<std::thread> workers_;
     unsigned long long next_id_ = 0, completed_ = 0, failed_ = 0, evictions_ = 0, peak_in_flight_ = 0;
     int in_flight_ = 0;
+    int waiters_ = 0;  // threads inside wait()
     size_t reserved_ = 0, peak_reserved_ = 0;
     bool stop_ = false;
     std::string err_;

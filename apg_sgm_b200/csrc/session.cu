@@ -48,6 +48,7 @@ struct apg_session_s {
     double hier[6] = {};                 // Engine::hier_telemetry of the last frame
     int frame_w = 0, frame_h = 0;        // its size
     size_t peak_bytes = 0;
+    std::vector<std::pair<std::string, int>> tuning;  // apgcu_session_set_tuning, applied every frame
     std::mutex mu;
     ~apg_session_s() { delete eng; }
 };
@@ -232,6 +233,7 @@ int apg_session_process(apg_session_t s, const apg_image_view_t* left, const apg
             return APG_STATUS_UNSUPPORTED_BACKEND;
         }
         if (!s->eng) s->eng = new apgcu::Engine(s->cfg, 0, nullptr);
+        for (const auto& kv : s->tuning) apgcu::set_tuning(s->eng, kv.first.c_str(), kv.second);
         const bool was_reuse = s->opt.memory_policy == APG_MEMORY_BOUNDED_REUSE && w == s->last_w && h == s->last_h &&
                                s->cfg.max_disparity == s->last_dmax && s->eng->allocated_bytes() > 0;
         const size_t n = (size_t)w * h;
@@ -376,6 +378,21 @@ APGCU_API int apgcu_session_get_stats(apg_session_t s, double* stage_ms11, size_
         counters4[2] = s->peak_bytes;
         counters4[3] = s->eng ? s->eng->allocated_bytes() : 0;
     }
+    return APG_STATUS_OK;
+}
+
+APGCU_API int apgcu_session_set_tuning(apg_session_t s, const char* key, int value) {
+    if (!s || !key) return APG_STATUS_INTERNAL_ERROR;
+    std::lock_guard<std::mutex> lk(s->mu);
+    const int rc = apgcu::set_tuning(nullptr, key, value);
+    if (rc != APG_STATUS_OK) return rc;
+    for (auto& kv : s->tuning) {
+        if (kv.first == key) {
+            kv.second = value;
+            return APG_STATUS_OK;
+        }
+    }
+    s->tuning.emplace_back(key, value);
     return APG_STATUS_OK;
 }
 

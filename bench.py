@@ -89,67 +89,111 @@ def _profile_traffic(kernel: str, workload: str):
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 50 ms during the timed region."""
+    """SM clock and clock-event reasons of this rank's GPU, read through NVML every ~2 ms by a
+    background thread (reads only; no setting is touched).  mark() records host-time marks around
+    the timed region so its samples can be told apart from the rest of the sampled window (the
+    per-launch profile and the end-to-end legs that follow it, all with the GPU busy).  Falls back to
+    nvidia-smi at its fastest rate when NVML is not importable."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
-    def __init__(self, gpu_index: int):
-        self.idx = gpu_index
-        self.proc = None
-        self.lines = []
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.samples = []  # (host time, sm MHz, max sm MHz, reason names)
+        self.marks = {}
+        self._stop = threading.Event()
+        self._t = None
+        self._nvml = None
+
+    def _handle(self, nv):
+        try:
+            import torch
+            pr = torch.cuda.get_device_properties(self.dev)
+            bus = f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0"
+            return nv.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return nv.nvmlDeviceGetHandleByIndex(self.dev)
 
     def start(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self._t = threading.Thread(target=self._read, daemon=True)
-            self._t.start()
-        except FileNotFoundError:
-            self.proc = None
+            import pynvml as nv
+            nv.nvmlInit()
+            h = self._handle(nv)
+            smax = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                    "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                    "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                    "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+            self._nvml = nv
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            def poll():
+                while not self._stop.is_set():
+                    try:
+                        sm = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                        rs = int(nv.nvmlDeviceGetCurrentClocksEventReasons(h))
+                        self.samples.append((time.perf_counter(), sm, smax,
+                                             tuple(n for n, b in bits.items() if rs & b)))
+                    except Exception:
+                        pass
+                    self._stop.wait(0.002)
+        except Exception:
+            poll = self._poll_smi
+        self._t = threading.Thread(target=poll, daemon=True)
+        self._t.start()
+
+    def _poll_smi(self):
+        fields = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                  "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={fields}",
+                                     "--format=csv,noheader,nounits", "-lms", "20"],
+                                    stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except FileNotFoundError:
+            return
+        for line in proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            try:
+                self.samples.append((time.perf_counter(), float(parts[0]), float(parts[1]),
+                                     tuple(n for n, v in zip(self.REASONS, parts[2:6]) if v.lower() == "active")))
+            except (ValueError, IndexError):
+                pass
+            if self._stop.is_set():
+                break
+        proc.terminate()
 
     def wait_first(self, timeout: float = 5.0):
-        """Block until nvidia-smi has printed its first sample, so the timed region is covered."""
+        """Block until the first sample has arrived, so the timed region is covered."""
         t0 = time.time()
-        while self.proc and not self.lines and time.time() - t0 < timeout:
-            time.sleep(0.01)
-        self.lines.clear()
+        while not self.samples and time.time() - t0 < timeout:
+            time.sleep(0.001)
+
+    def mark(self, name: str):
+        self.marks[name] = time.perf_counter()
 
     def stop(self):
-        if not self.proc:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-        sm, smax, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            parts = [p.strip() for p in ln.split(",")]
-            if len(parts) < 9:
-                continue
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=5)
+        if self._nvml:
             try:
-                sm.append(float(parts[1]))
-                smax.append(float(parts[2]))
-            except ValueError:
-                continue
-            for n, v in zip(names, parts[5:9]):
-                if v.lower() == "active":
-                    reasons.add(n)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                self._nvml.nvmlShutdown()
+            except Exception:
+                pass
+        t0, t1 = self.marks.get("timed_start"), self.marks.get("timed_end")
+        timed = [s for s in self.samples if t0 is not None and t1 is not None and t0 <= s[0] <= t1]
+        busy = [s for s in self.samples if t0 is not None and s[0] >= t0]
+        use = timed or busy
+        reasons = sorted({r for s in use for r in s[3]})
+        return {"sm_mhz": statistics.median(s[1] for s in use) if use else None,
+                "sm_max_mhz": max(s[2] for s in use) if use else None,
+                "reasons": reasons, "samples": len(use), "samples_in_timed_region": len(timed),
+                "window": "timed region" if timed else "timed region through the end-to-end legs",
+                "source": "nvml" if self._nvml else "nvidia-smi"}
 
 
 def _algorithmic_bytes(name: str, w: int, h: int, D: int, volume_source: bool, npath: int = 4) -> float:
-    """Bytes a launch of `name` must move by design (roofline section).  Path sums
-    and volumes are u16 per voxel; a volume-fed sweep reads the cost volume once."""
+    """Bytes a launch of `name` must move by design: the stage-boundary traffic of the kernel with
+    u16 path sums and volumes per voxel; a volume-fed sweep reads the cost volume once."""
     n = w * h
     vol = n * D * 2.0 if volume_source else 0.0
     nfirst = npath - 1
@@ -458,7 +502,7 @@ def cpu_baseline(spec, mode, L, R, gpu_out, over=None):
 def run_b200(args, wl):
     import torch
     import apg_sgm_b200 as apg
-    from apg_sgm_b200 import synthetic as S
+    from apg_sgm_b200 import replicas, synthetic as S
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -511,6 +555,7 @@ def run_b200(args, wl):
         dist.barrier()
     torch.cuda.synchronize()
     launches0 = apg.kernel_launch_count()
+    sampler.mark("timed_start")
     with torch.cuda.stream(es):
         for k in range(args.steps):
             flush.zero_()  # L2 flush outside the timed step
@@ -518,8 +563,8 @@ def run_b200(args, wl):
             step(k)
             ends[k].record(es)
     torch.cuda.synchronize()
+    sampler.mark("timed_end")
     launches = apg.kernel_launch_count() - launches0
-    clocks = sampler.stop()
 
     # per-launch device times (a separate pass: the event after every launch is not in the timing)
     eng.set_debug(apg.DEBUG_PROFILE)
@@ -533,11 +578,9 @@ def run_b200(args, wl):
     torch.cuda.synchronize()
     eng.set_debug(0)
     dev_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
-    t = torch.tensor([dev_ms], dtype=torch.float64, device=dev)
     if dist:
         dist.barrier()
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    max_ms = float(t.item())
+    max_ms = replicas.max_over_ranks(dev_ms, dist, dev)  # the job's device time is the slowest rank's
     vox = w * h * D
     value = vox * args.steps * world / (max_ms / 1000.0)
 
@@ -573,14 +616,12 @@ def run_b200(args, wl):
     for k in range(args.steps):
         e2e_step(k)
     e2e_s = time.perf_counter() - t0
-    te = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
-    if dist:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = vox * args.steps * world / float(te.item())
+    e2e_value = vox * args.steps * world / replicas.max_over_ranks(e2e_s, dist, dev)
     lib.apg_result_destroy(res_c)
     lib.apg_session_destroy(sess_c)
 
-    # the same through the Python binding (StereoSession.process returns fresh numpy arrays)
+    # the same through the Python binding (StereoSession.process returns numpy views over a pooled
+    # page-locked result block)
     sess = apg.StereoSession(mode=MODE_NAMES[mode].lower() if mode != 2 else "high_quality", max_disparity=D,
                              memory_policy="bounded_reuse", hierarchical=bool(over.get("hier_enable")))
     for i in range(max(args.warmup, 3)):
@@ -590,6 +631,7 @@ def run_b200(args, wl):
     for k in range(npy):
         sess.process(*pairs[k % npairs])
     py_value = vox * npy / (time.perf_counter() - t0)
+    clocks = sampler.stop()
 
     # dominant kernel and its roofline
     peak, peak_kind = _peaks()
@@ -655,7 +697,7 @@ def run_batched(args):
     import ctypes as C
     import torch
     import apg_sgm_b200 as apg
-    from apg_sgm_b200 import _lib, synthetic as S
+    from apg_sgm_b200 import _lib, replicas, synthetic as S
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -737,18 +779,18 @@ def run_batched(args):
     torch.cuda.synchronize()
     launches0 = apg.kernel_launch_count()
     batch_ms = 0.0
+    sampler.mark("timed_start")
     for k in range(args.steps):
         flush.zero_()
         torch.cuda.synchronize()
         batch.process_device(recs)
         batch_ms += batch.last_time_ms
     torch.cuda.synchronize()
+    sampler.mark("timed_end")
     launches = apg.kernel_launch_count() - launches0
     clocks = sampler.stop()
-    t = torch.tensor([batch_ms, plain_ms], dtype=torch.float64, device=dev)
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    batch_ms, plain_ms = float(t[0]), float(t[1])
+    batch_ms = replicas.max_over_ranks(batch_ms, dist, dev)
+    plain_ms = replicas.max_over_ranks(plain_ms, dist, dev)
     value = vox * args.steps * world / (batch_ms / 1000.0)
     plain_value = vox * args.steps * world / (plain_ms / 1000.0)
 
@@ -879,6 +921,7 @@ def run_metrics(args):
     sampler.wait_first()
     launches0 = apg.kernel_launch_count()
     times = []
+    sampler.mark("timed_start")
     with torch.cuda.stream(s):
         for k in range(args.steps):
             flush.zero_()
@@ -887,6 +930,7 @@ def run_metrics(args):
             ends[k].record(s)
             times.append(float(_lib.lib().apgcu_metrics_last_kernel_ms()))
     torch.cuda.synchronize()
+    sampler.mark("timed_end")
     launches = apg.kernel_launch_count() - launches0
     clocks = sampler.stop()
     call_ms = [a.elapsed_time(b) for a, b in zip(starts, ends)]

@@ -64,7 +64,15 @@ APGCU_API int apgcu_engine_set_debug(apgcu_engine_t e, int flags);
  *   "sgm_lanes": lanes per SGM scanline chain, 8 / 16 / 32 (0 = default, 32);
  *   "cost_tile": columns per block of the cost kernel, 64 / 128 / 256 (0 = default for the range);
  *   "fast_fused": 1 = census-only Fast mode recomputes its costs inside the SGM sweeps and stores no
- *                 cost volume (less memory, slower); 0 = store the volume once (default).
+ *                 cost volume (less memory, slower); 0 = store the volume once (default);
+ *   "cost_kernel": 0 = pixel-run cost kernel where it applies (default), 1 = column-tile kernel;
+ *   "refine_window": 0 = HighQuality refiner reads the right-image window from shared memory where
+ *                 every band fits on the device at once (default), 1 = always through L1.
+ * And one key that bounds a wait rather than tuning speed:
+ *   "refine_spin_limit": polls (each ~128 ns) before a refiner band stops waiting for the band above
+ *                 (0 = default, about a second).  A wait that runs out sets the frame's error flag,
+ *                 every band returns, and the frame fails with APG_STATUS_INTERNAL_ERROR ("refine: a
+ *                 wavefront wait timed out"); the next frame starts clean.
  * Returns 0, or APG_STATUS_INVALID_CONFIG for an unknown key or value. */
 APGCU_API int apgcu_engine_set_tuning(apgcu_engine_t e, const char* key, int value);
 
@@ -143,6 +151,9 @@ APGCU_API apg_session_t apgcu_session_create_config(const apg_pipeline_config_t*
 /* PipelineStats of the last frame: stage_ms11 as apgcu_engine_stage_times; counters4 =
  * {frame_allocation_count, frame_reuse_count, peak_workspace_bytes, retained_workspace_bytes}. */
 APGCU_API int apgcu_session_get_stats(apg_session_t s, double* stage_ms11, size_t* counters4);
+/* The engine tuning keys of apgcu_engine_set_tuning for a session's engine (kept across
+ * ReleasePerFrame and the lazily created engine).  Returns 0 or APG_STATUS_INVALID_CONFIG. */
+APGCU_API int apgcu_session_set_tuning(apg_session_t s, const char* key, int value);
 /* Frame counters of the last frame (PipelineStats, src/pipeline.cpp:650-707), computed on the device:
  * counts8 = {valid_pixels, reliable_pixels, unreliable_pixels, refine_changed_pixels, lr_fail_pixels,
  * prior_support_count, sum of search-range widths, sum of geometric range widths}. */
@@ -313,17 +324,24 @@ APGCU_API const char* apgcu_server_last_error(apgcu_server_t s);
  * Enqueued only; synchronise the stream before reading the result.
  *
  * The first call on each device looks up the array's device address (cudaGetSymbolAddress) with
- * that device current; make that first call before any stream capture.  All calls on one device
- * share the array: calls that overlap in time on one device race and must be serialised by the
- * caller.
+ * that device current, and under CUDA's default lazy module loading that first call also loads the
+ * library's noalloc module into the context, which creates the 8 MiB array and the kernels there.
+ * So make one warm-up call per device at start-up, before any stream capture and before the hot
+ * path begins; with eager loading (CUDA_MODULE_LOADING=EAGER) every context that loads the library
+ * holds the array from the start.  The address is remembered per device together with the context
+ * it belongs to and looked up again if the device's current context changes.  All calls on one
+ * device share the array and it keeps the last call's keys (each call clears the pixels it uses):
+ * calls that overlap in time on one device race and must be serialised by the caller.
  *
  * Returns APG_STATUS_OK; APG_STATUS_EMPTY_INPUT for a NULL pointer or a non-positive size;
  * APG_STATUS_INVALID_DISPARITY_RANGE for num_disparities outside [1,
- * APGCU_NOALLOC_MAX_DISPARITIES]; APG_STATUS_SIZE_MISMATCH for pitch < num_disparities;
+ * APGCU_NOALLOC_MAX_DISPARITIES] or |min_disparity| > APGCU_NOALLOC_MAX_ABS_DISPARITY;
+ * APG_STATUS_SIZE_MISMATCH for pitch < num_disparities;
  * APG_STATUS_RESOURCE_LIMIT_EXCEEDED when width*height > APGCU_NOALLOC_MAX_PIXELS or height > 65535
  * (nothing is launched); APG_STATUS_UNSUPPORTED_BACKEND / APG_STATUS_INTERNAL_ERROR for CUDA failures. */
 #define APGCU_NOALLOC_MAX_PIXELS (1 << 21)
 #define APGCU_NOALLOC_MAX_DISPARITIES 1024
+#define APGCU_NOALLOC_MAX_ABS_DISPARITY (1 << 20)
 APGCU_API int apgcu_right_wta_noalloc(const uint16_t* d_cost, int width, int height, int min_disparity,
                                       int num_disparities, int pitch, int subpixel, float* d_disparity_right,
                                       void* stream);

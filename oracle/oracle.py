@@ -319,6 +319,16 @@ def wta(cfg: PipelineConfig, acc, rmin, rmax):
     return disp, best, second
 
 
+def wta_right(cfg: PipelineConfig, raw):
+    """Right-image disparity from the raw cost volume, (h, w, D) u16 (orc_wta_right, the restatement
+    of wta_right_from_left_volume, src/pipeline.cpp:24-85)."""
+    raw = np.ascontiguousarray(raw, np.uint16)
+    h, w, _ = raw.shape
+    out = np.empty((h, w), np.float32)
+    lib().orc_wta_right(C.byref(cfg), _p(raw), w, h, _p(out))
+    return out
+
+
 def rng_draws(seed: int, plan):
     """Concatenated draws of std::uniform_int_distribution(-r, r) over one mt19937(seed) for a
     list of (radius, count) pairs."""

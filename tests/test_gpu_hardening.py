@@ -141,3 +141,60 @@ def test_release_per_frame_keeps_nothing(apg):
     assert (alloc, reuse) == (2, 0) and peak > 0
     L.apg_result_destroy(r)
     L.apg_session_destroy(s)
+
+
+INTERNAL_ERROR = 8
+
+
+@pytest.mark.parametrize("policy", [0, 1])
+def test_refiner_wait_runs_out_then_session_recovers(apg, O, policy):
+    """A bounded device wait that runs out (the fault-recovery case of test_hardening.cpp:64-91,
+    made on the device without faulting it).  With the refiner's poll budget at one poll, a band
+    stops waiting for the band above almost at once: the kernel sets the frame's error word, every
+    band returns, and apg_session_process reports INTERNAL_ERROR with a last_error, counting no
+    frame.  The next frame on the same session, with the default budget, is bit-exact with the
+    oracle.  160x128 HighQuality has four refiner bands per pass, three of which wait."""
+    from helpers import synth, to_oracle
+    L = _lib_handle(apg)
+    cfg = apg.config_from_mode(2, 32)
+    s = L.apgcu_session_create_config(C.byref(cfg), policy, 0)
+    assert s
+    r = L.apg_result_create()
+    left, right = synth(160, 128, 32, patch=0.2, seed=9)
+    assert L.apgcu_session_set_tuning(s, b"refine_spin_limit", 1) == OK
+    assert L.apgcu_session_set_tuning(s, b"refine_spin_limit", -1) == 4  # INVALID_CONFIG
+    assert L.apgcu_session_set_tuning(s, b"no_such_key", 1) == 4
+    rc = L.apg_session_process(s, _view(left), _view(right), r)
+    assert rc == INTERNAL_ERROR, rc
+    assert b"wavefront wait timed out" in L.apg_session_get_last_error(s)
+    assert L.apg_session_get_frame_count(s) == 0
+    assert not L.apg_result_get_disparity(r, None, None)
+    assert L.apgcu_session_set_tuning(s, b"refine_spin_limit", 0) == OK
+    assert L.apg_session_process(s, _view(left), _view(right), r) == OK
+    assert L.apg_session_get_frame_count(s) == 1
+    assert L.apg_session_get_last_error(s) == b""
+    want = O.pipeline(to_oracle(O, cfg), left, right)
+    w, h = C.c_int(), C.c_int()
+    p = L.apg_result_get_disparity(r, C.byref(w), C.byref(h))
+    got = np.ctypeslib.as_array(C.cast(p, C.POINTER(C.c_float)), shape=(128, 160)).copy()
+    assert np.array_equal(got.view(np.uint32), want["disparity"].view(np.uint32))
+    L.apg_result_destroy(r)
+    L.apg_session_destroy(s)
+
+
+def test_engine_refiner_wait_runs_out(apg, O):
+    """The same through the engine entry point: the failed frame raises with the engine's error,
+    the next one (default budget) equals the oracle."""
+    from helpers import same_bits, synth, to_oracle
+    cfg = apg.config_from_mode(2, 32)
+    left, right = synth(160, 128, 32, patch=0.2, seed=10)
+    eng = apg.Engine(cfg)
+    eng.set_tuning("refine_spin_limit", 1)
+    with pytest.raises(RuntimeError, match="wavefront wait timed out"):
+        eng.process(left, right)
+    eng.set_tuning("refine_spin_limit", 0)
+    got = eng.process(left, right)
+    want = O.pipeline(to_oracle(O, cfg), left, right)
+    for k in ("disparity", "confidence", "invalid_reason", "reliable_mask"):
+        assert same_bits(got[k], want[k]), k
+    eng.close()

@@ -90,3 +90,28 @@ def test_server_pinned_buffers_match(apg):
         for k in KEYS:
             assert same_bits(got[k], want[i][k]), (i, k)
     srv.close()
+
+
+def test_session_results_are_views_of_pooled_blocks(apg):
+    """StereoSession.process returns arrays over the page-locked block the device copies landed in
+    (no copy).  A block is not reused while any array of its frame is alive, and is reused once
+    they are all gone; every frame equals the engine's."""
+    L1, R1 = synth(160, 96, 32, seed=1)
+    L2, R2 = synth(160, 96, 32, seed=2)
+    s = apg.StereoSession(mode="fast", max_disparity=32, memory_policy="bounded_reuse")
+    a = s.process(L1, R1)
+    a_disp = a.disparity.copy()
+    b = s.process(L2, R2)
+    assert a.disparity.ctypes.data != b.disparity.ctypes.data
+    assert np.array_equal(a.disparity.view(np.uint32), a_disp.view(np.uint32))
+    p = b.disparity.ctypes.data
+    del b
+    c = s.process(L2, R2)
+    assert c.disparity.ctypes.data == p
+    want = apg.Engine(apg.config_from_mode(0, 32)).process(L2, R2)
+    for k in ("disparity", "confidence", "invalid_reason", "reliable_mask"):
+        assert np.array_equal(np.ascontiguousarray(getattr(c, k)).view(np.uint8),
+                              np.ascontiguousarray(want[k]).view(np.uint8)), k
+    conf = c.confidence
+    del c
+    assert conf.base is not None and np.all((conf >= 0) & (conf <= 1))  # the view keeps its block

@@ -126,3 +126,30 @@ def test_served_into_caller_buffers(apg):
     with pytest.raises(ValueError):
         srv.submit(pool[0][2], pool[0][3], out={k: np.zeros((1, 1), np.float32) for k in KEYS})
     srv.close()
+
+
+def test_server_stop_completes_queued_requests(apg):
+    """Destroying a server with requests still queued completes them with an error, so a thread
+    waiting for one returns (no hang); the requests that ran are unaffected."""
+    import ctypes as C
+    import threading
+    import time
+
+    from apg_sgm_b200._lib import lib
+
+    L, R = synth(1280, 720, 128, cells=6, lo=0, hi=120, patch=0.2, seed=81)
+    srv = apg.Server(slots=1)
+    tickets = [srv.submit(L, R, mode=2, max_disparity=128) for _ in range(48)]
+    res = {}
+
+    def waiter():
+        lat = C.c_double()
+        res["rc"] = lib().apgcu_server_wait(srv._h, tickets[-1], C.byref(lat))
+
+    t = threading.Thread(target=waiter, daemon=True)
+    t.start()
+    time.sleep(0.05)
+    srv.close()  # joins the worker after its current request; the rest complete with an error
+    t.join(timeout=120)
+    assert not t.is_alive(), "a thread waiting on a queued request did not return after the server stopped"
+    assert res["rc"] in (0, 8), res

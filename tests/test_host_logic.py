@@ -206,3 +206,30 @@ def test_synthetic_generator_is_deterministic():
     specs = S.batched_mix()
     assert len(specs) == 64
     assert sum(s.width * s.height * s.max_disparity for s in specs) == 4_505_472_000
+
+
+def test_result_pool_lends_and_takes_back(apg):
+    """StereoSession's result pool: a result lent to live arrays is not lent again; it comes back
+    when the last array viewing it is gone; beyond `keep` idle results the rest are destroyed."""
+    from apg_sgm_b200 import _ResultLease, _ResultPool
+
+    pool = _ResultPool(keep=2)
+    a = pool.take()
+    b = pool.take()
+    assert a and b and a != b
+    la, lb = _ResultLease(pool, a), _ResultLease(pool, b)
+    holder = [la]
+    del la
+    assert pool._free == []          # still held
+    holder.clear()
+    assert pool._free == [a]         # back once nothing holds it
+    del lb
+    assert sorted(pool._free) == sorted([a, b])
+    c = pool.take()
+    assert c in (a, b)
+    extra = [pool.take() for _ in range(3)]
+    for r in extra + [c]:
+        pool.give_back(r)
+    assert len(pool._free) == 2      # the rest were destroyed
+    pool.close()
+    assert pool._free == []
