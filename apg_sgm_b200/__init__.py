@@ -216,35 +216,43 @@ class _ResultPool:
     the arrays that StereoSession.process returns.  A result goes back to the pool when the last
     array viewing it is gone, so in a loop that drops each frame's arrays before the next call the
     same one or two blocks serve every frame, with no allocation and no copy; results kept alive by
-    the caller simply make the pool lend a new block."""
+    the caller simply make the pool lend a new block.  No lock: a lease may be released by the
+    garbage collector on any thread at any allocation, even inside take() or give_back(), and the
+    list's append and pop are atomic on their own."""
 
     def __init__(self, keep: int = 4):
         self._free = []
         self._keep = keep
-        self._mu = threading.Lock()
         self._closed = False
 
     def take(self):
-        with self._mu:
-            if self._free:
-                return self._free.pop()
+        try:
+            return self._free.pop()
+        except IndexError:
+            pass
         r = lib().apg_result_create()
         if not r:
             raise MemoryError("apg_result_create failed")
         return r
 
     def give_back(self, r):
-        with self._mu:
-            if not self._closed and len(self._free) < self._keep:
-                self._free.append(r)
+        if not self._closed and len(self._free) < self._keep:
+            self._free.append(r)
+            if not self._closed:
+                return
+            try:  # closed meanwhile: close() may have missed it
+                self._free.remove(r)
+            except ValueError:
                 return
         lib().apg_result_destroy(r)
 
     def close(self):
-        with self._mu:
-            self._closed = True
-            free, self._free = self._free, []
-        for r in free:
+        self._closed = True
+        while True:
+            try:
+                r = self._free.pop()
+            except IndexError:
+                break
             lib().apg_result_destroy(r)
 
 

@@ -691,6 +691,7 @@ int Engine::sgm_launch(SgmLaunch* out, uint32_t** sbufs) const {
     pl.sp_tel = scope_.sp_telem ? ptr<apg_subpixel_telemetry_t>(L.tel) : nullptr;
     pl.store_final = (debug_ & 2) != 0;
     pl.lanes = sgm_lanes_;
+    pl.split = sgm_split_;
     for (int i = 0; i < L.nsbuf; ++i) sbufs[i] = ptr<uint32_t>(L.sbuf[i]);
     return L.nsbuf;
 }
@@ -1161,6 +1162,11 @@ int set_tuning(Engine* e, const char* key, int value) {
     if (std::strcmp(key, "sgm_lanes") == 0) {
         if (value != 0 && value != 8 && value != 16 && value != 32) return kInvalidConfig;
         if (e) e->set_sgm_lanes(value);
+        return kOk;
+    }
+    if (std::strcmp(key, "sgm_split") == 0) {
+        if (value < 0 || value > 2) return kInvalidConfig;
+        if (e) e->set_sgm_split(value);
         return kOk;
     }
     if (std::strcmp(key, "cost_tile") == 0) {

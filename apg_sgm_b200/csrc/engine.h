@@ -157,6 +157,7 @@ public:
     const std::string& last_error() const { return err_; }
     void set_debug(int f) { debug_ = f; }
     void set_sgm_lanes(int t) { sgm_lanes_ = t; }
+    void set_sgm_split(int v) { sgm_split_ = v; }
     void set_fast_fused(bool on) { fast_fused_ = on; }
     void set_cost_tile(int t) { cost_tile_ = t; }
     void set_cost_kernel(int k) { cost_kernel_ = k; }
@@ -215,6 +216,7 @@ private:
     int device_ = 0;
     int debug_ = 0;
     int sgm_lanes_ = 0;
+    int sgm_split_ = 0;  // last sweep over two warps per chain: 0 auto, 1 never, 2 always
     bool fast_fused_ = false;
     int cost_tile_ = 0;
     int cost_kernel_ = 0;  // 0: pixel-run cost kernel where it applies, 1: column-tile kernel

@@ -718,6 +718,212 @@ __device__ __forceinline__ void run_chain_vol(const SgmArgs& a, const uint32_t* 
     cp_wait<0>();
 }
 
+// ---- the last sweep split over two warps of one block
+//
+// One chain per block of two warps.  Warp 0 runs only the recurrence: its costs come through its
+// own cp.async ring, and each step's L goes to a shared-memory ring of kSplitSlots segments of
+// kSplitSeg steps.  Warp 1 adds the NB partial sums to each step's L (through its own cp.async
+// ring), writes the final sums into the WTA buffer and runs the WTA every 32 steps.  The recurrence
+// warp's step is about a third of the instructions of a step that also adds, buffers and
+// evaluates the sums, and it shares its SM's issue slots with the other chains' summing warps, so
+// the dependent chain of each step is what remains of its time.
+//
+// Hand-over by named barriers (bar.arrive / bar.sync over the block's 64 threads): warp 0 arrives
+// on FULL[s % 2] once segment s is written, warp 1 arrives on FREE[s % 2] once it has read it, and
+// each waits for the other's barrier before it touches that slot again.  Both warps walk the same
+// number of segments (the block's one chain has one length), so every barrier generation is
+// completed by exactly one arrival of each warp, and no warp arrives twice on one barrier before
+// the other has passed it.
+constexpr int kSplitSlots = 2;
+constexpr int kSplitSeg = 8;  // steps per segment (divides the 32-step WTA and P2 blocks)
+constexpr int kBarFull = 1;   // named barriers 1, 2: segment written
+constexpr int kBarFree = 3;   // named barriers 3, 4: segment read
+
+template <int K, int NB, int PFA, int PFB>
+struct SplitSmem {
+    static constexpr int cring = PFA * 32 * K;                         // warp 0: cost ring
+    static constexpr int lseg = kSplitSeg * 32 * K;                    // one segment of L
+    static constexpr int lring = kSplitSlots * lseg;
+    static constexpr int pring = PFB * NB * 32 * K;                    // warp 1: partial-sum ring
+    static constexpr int wta = wta_buf_words<K, 32>();                 // warp 1: final sums
+    static constexpr int words = cring + lring + pring + wta;
+};
+
+__device__ __forceinline__ void nbar_sync64(int id) { asm volatile("bar.sync %0, 64;\n" ::"r"(id) : "memory"); }
+__device__ __forceinline__ void nbar_arrive64(int id) { asm volatile("bar.arrive %0, 64;\n" ::"r"(id) : "memory"); }
+
+template <int K, int NB, int PFA, int PFB>
+__global__ void __launch_bounds__(64) sgm_last_split_kernel(SgmArgs a, DirTable tab) {
+    static_assert((PFA & (PFA - 1)) == 0 && (PFB & (PFB - 1)) == 0, "ring depths: powers of two");
+    using SM = SplitSmem<K, NB, PFA, PFB>;
+    extern __shared__ __align__(16) uint32_t s_dyn[];
+    uint32_t* s_c = s_dyn;
+    uint32_t* s_l = s_c + SM::cring;
+    uint32_t* s_p = s_l + SM::lring;
+    uint32_t* s_w = s_p + SM::pring;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int x0, y0, len;
+    scan_start(a, tab.dx[0], tab.dy[0], blockIdx.x, tab.nscan[0], x0, y0, len);
+    if (len == 0) return;  // the whole block (one chain)
+    const int W2 = a.Dp / 2;
+    const int step = tab.dy[0] * a.w + tab.dx[0];
+    const int p0 = y0 * a.w + x0;
+    const uint32_t dstep = (uint32_t)(step * W2);
+    const uint32_t off0 = (uint32_t)p0 * (uint32_t)W2 + (uint32_t)(lane * K);
+    const int nseg = (len + kSplitSeg - 1) / kSplitSeg;
+
+    if (warp == 0) {
+        // ---- the recurrence (process_pixel, src/sgm_optimizer.cpp:44-80)
+        auto issue = [&](int t, uint32_t off) {
+            if (t < len) cp_words<K>(s_c + (t & (PFA - 1)) * 32 * K + lane * K, a.cvol + off);
+            cp_commit();
+        };
+        uint32_t ioff = off0;
+#pragma unroll
+        for (int t = 0; t < PFA; ++t) {
+            issue(t, ioff);
+            ioff += dstep;
+        }
+        const uint32_t p1x2 = (uint32_t)a.pen.P1 * 0x00010001u;
+        uint32_t L[K];
+        uint32_t m = kInf;
+#pragma unroll
+        for (int k = 0; k < K; ++k) L[k] = kInf2;
+        int gnext = lane < len ? (int)__ldg(a.gray + p0 + lane * step) : 0;
+        int gcarry = 0, p2v = 0;
+        for (int seg = 0; seg < nseg; ++seg) {
+            if (seg >= kSplitSlots) nbar_sync64(kBarFree + seg % kSplitSlots);
+            uint32_t* lslot = s_l + (seg % kSplitSlots) * SM::lseg;
+#pragma unroll
+            for (int v = 0; v < kSplitSeg; ++v) {
+                const int t = seg * kSplitSeg + v;
+                if (t < len) {
+                    if ((t & 31) == 0) {
+                        // P2 of the steps [t, t + 32): lane j holds step t + j
+                        const int gcur = gnext;
+                        const int tn = t + 32 + lane;
+                        gnext = tn < len ? (int)__ldg(a.gray + p0 + tn * step) : 0;
+                        int gprev = __shfl_up_sync(0xffffffffu, gcur, 1);
+                        if (lane == 0) gprev = gcarry;
+                        gcarry = __shfl_sync(0xffffffffu, gcur, 31);
+                        p2v = adaptive_p2(a.pen, gcur - gprev);
+                    }
+                    cp_wait<PFA - 1>();
+                    const int P2 = __shfl_sync(0xffffffffu, p2v, t & 31);
+                    uint32_t c[K];
+                    lds_words<K>(s_c + (t & (PFA - 1)) * 32 * K + lane * K, c);
+#pragma unroll
+                    for (int k = 0; k < K; ++k) c[k] = __vminu2(c[k], kInf2);  // 0xFFFF -> 0x7FFF
+                    if (t == 0 || m >= kInf) {
+#pragma unroll
+                        for (int k = 0; k < K; ++k) L[k] = c[k];
+                    } else {
+                        const uint32_t mp2 = (m + (uint32_t)P2) * 0x00010001u;
+                        const uint32_t m2 = m * 0x00010001u;
+                        uint32_t up = __shfl_up_sync(0xffffffffu, L[K - 1], 1);
+                        uint32_t dn = __shfl_down_sync(0xffffffffu, L[0], 1);
+                        if (lane == 0) up = kInf2;
+                        if (lane == 31) dn = kInf2;
+                        uint32_t Ln[K];
+#pragma unroll
+                        for (int k = 0; k < K; ++k) {
+                            const uint32_t lo_nb = k == 0 ? up : L[k - 1];
+                            const uint32_t hi_nb = k == K - 1 ? dn : L[k + 1];
+                            const uint32_t lm = __byte_perm(lo_nb, L[k], 0x5432);
+                            const uint32_t lp = __byte_perm(L[k], hi_nb, 0x5432);
+                            const uint32_t b = __vminu2(L[k], __viaddmin_u16x2(__vminu2(lm, lp), p1x2, mp2));
+                            Ln[k] = __vadd2(c[k], __vsub2(b, m2));
+                        }
+#pragma unroll
+                        for (int k = 0; k < K; ++k) L[k] = Ln[k];
+                    }
+                    uint32_t mm;
+                    if constexpr (K == 1) {
+                        mm = min_halves(L[0]);
+                    } else {
+                        uint32_t acc = __vminu2(L[0], L[1]);
+#pragma unroll
+                        for (int k = 2; k < K; k += 2)
+                            acc = k + 1 < K ? __vimin3_u16x2(acc, L[k], L[k + 1]) : __vminu2(acc, L[k]);
+                        mm = min_halves(acc);
+                    }
+                    m = __reduce_min_sync(0xffffffffu, mm);
+                    uint32_t* dst = lslot + v * 32 * K + lane * K;
+#pragma unroll
+                    for (int k = 0; k < K; ++k) dst[k] = L[k];
+                    // the cost slot just read is refilled only after its words were consumed above
+                    issue(t + PFA, ioff);
+                    ioff += dstep;
+                }
+            }
+            __threadfence_block();
+            nbar_arrive64(kBarFull + seg % kSplitSlots);
+        }
+        cp_wait<0>();
+    } else {
+        // ---- partial sums, final sums, WTA (wta_impl, src/sgm_optimizer.cpp:465-536)
+        constexpr int PW = NB * 32 * K;  // words per partial-ring slot
+        auto issue = [&](int t, uint32_t off) {
+            if (t < len) {
+                uint32_t* sl = s_p + (t & (PFB - 1)) * PW;
+#pragma unroll
+                for (int b = 0; b < NB; ++b) cp_words<K>(sl + 32 * K * b + lane * K, tab.in[b] + off);
+            }
+            cp_commit();
+        };
+        uint32_t ioff = off0, off = off0;
+#pragma unroll
+        for (int t = 0; t < PFB; ++t) {
+            issue(t, ioff);
+            ioff += dstep;
+        }
+        for (int seg = 0; seg < nseg; ++seg) {
+            nbar_sync64(kBarFull + seg % kSplitSlots);
+            const uint32_t* lslot = s_l + (seg % kSplitSlots) * SM::lseg;
+#pragma unroll
+            for (int v = 0; v < kSplitSeg; ++v) {
+                const int t = seg * kSplitSeg + v;
+                if (t < len) {
+                    cp_wait<PFB - 1>();
+                    uint32_t sv[K];
+                    lds_words<K>(lslot + v * 32 * K + lane * K, sv);
+                    const uint32_t* sl = s_p + (t & (PFB - 1)) * PW;
+#pragma unroll
+                    for (int b = 0; b < NB; ++b) {
+                        uint32_t sb[K];
+                        lds_words<K>(sl + 32 * K * b + lane * K, sb);
+#pragma unroll
+                        for (int k = 0; k < K; ++k) sv[k] = __vaddus2(sv[k], sb[k]);
+                    }
+                    if (a.store_final) {
+                        uint32_t o[K];
+#pragma unroll
+                        for (int k = 0; k < K; ++k) o[k] = sv[k] | __vcmpgeu2(sv[k], kInf2);
+                        st_cg<K>(const_cast<uint32_t*>(tab.in[0]) + off, o);
+                    }
+                    uint32_t* wr = s_w + (t & 31) * (32 * K + 1) + lane * K;
+#pragma unroll
+                    for (int k = 0; k < K; ++k) wr[k] = sv[k];
+                    // the partial slot just read is refilled only after its words were consumed
+                    issue(t + PFB, ioff);
+                    ioff += dstep;
+                    off += dstep;
+                    if ((t & 31) == 31 || t == len - 1) {
+                        // the block's pixels [t0, t]: lane j runs the WTA of pixel t0 + j
+                        const int t0 = t & ~31;
+                        __syncwarp();
+                        if (t0 + lane <= t) wta_row<32 * K>(a, s_w + lane * (32 * K + 1), p0 + (t0 + lane) * step);
+                        __syncwarp();
+                    }
+                }
+            }
+            __threadfence_block();
+            if (seg + kSplitSlots < nseg) nbar_arrive64(kBarFree + seg % kSplitSlots);
+        }
+        cp_wait<0>();
+    }
+}
+
 // Prefetch depth PF (steps of loads in flight per chain) and unroll U (a multiple of PF, so ring
 // slots are compile-time registers; the sliding census ring also needs a multiple of 2K).  A
 // volume-fed sweep has few chains per SM, so it keeps many steps in flight to cover the HBM
@@ -874,12 +1080,38 @@ cudaError_t launch_first_tk(const SgmArgs& a, DirTable tab, bool census, cudaStr
     return cudaGetLastError();
 }
 
+// Whether the volume-fed last sweep runs split over two warps per chain: on request, else for up to
+// 128 padded disparities (wider ranges need more shared memory per chain than the split saves).
+bool use_split(int T, int K, bool census, int split) {
+    if (T != 32 || census || split == 1) return false;
+    return split == 2 || K <= 2;
+}
+
+template <int K, int NB>
+cudaError_t launch_last_split(const SgmArgs& a, const DirTable& tab, cudaStream_t st) {
+    constexpr int PFA = 8;
+    constexpr int PFB = K <= 2 ? 8 : 4;
+    const size_t smem = (size_t)SplitSmem<K, NB, PFA, PFB>::words * 4;
+    auto kern = sgm_last_split_kernel<K, NB, PFA, PFB>;
+    const cudaError_t e = allow_dynamic_smem(kern, smem);
+    if (e != cudaSuccess) return e;
+    kern<<<tab.nscan[0], 64, smem, st>>>(a, tab);
+    return cudaGetLastError();
+}
+
 template <int T, int K>
-cudaError_t launch_last_tk(const SgmArgs& a, DirTable tab, bool census, cudaStream_t st) {
+cudaError_t launch_last_tk(const SgmArgs& a, DirTable tab, bool census, int split, cudaStream_t st) {
     constexpr int C = 32 / T;
     tab.nscan[0] = nscan_of(a, tab.dx[0], tab.dy[0]);
     const int warps = (tab.nscan[0] + C - 1) / C;
     const int blocks = (warps + 3) / 4;
+    if constexpr (T == 32) {
+        if (use_split(T, K, census, split)) {
+            if (tab.nin == 1) return launch_last_split<K, 1>(a, tab, st);
+            if (tab.nin == 3) return launch_last_split<K, 3>(a, tab, st);
+            return cudaErrorInvalidValue;
+        }
+    }
 #define APGCU_LAST(NB)                                                                               \
     if (tab.nin == NB) {                                                                             \
         if (census) {                                                                                \
@@ -903,8 +1135,8 @@ cudaError_t launch_last_tk(const SgmArgs& a, DirTable tab, bool census, cudaStre
 }
 
 template <bool FIRST>
-cudaError_t dispatch(const SgmArgs& a, const DirTable& tab, bool census, int T, cudaStream_t st) {
-#define APGCU_TK(TT, KK) return FIRST ? launch_first_tk<TT, KK>(a, tab, census, st) : launch_last_tk<TT, KK>(a, tab, census, st)
+cudaError_t dispatch(const SgmArgs& a, const DirTable& tab, bool census, int T, int split, cudaStream_t st) {
+#define APGCU_TK(TT, KK) return FIRST ? launch_first_tk<TT, KK>(a, tab, census, st) : launch_last_tk<TT, KK>(a, tab, census, split, st)
     if (T == 8) {
         if (a.Dp == 64) APGCU_TK(8, 4);
         if (a.Dp == 128) APGCU_TK(8, 8);
@@ -1084,7 +1316,7 @@ cudaError_t launch_sgm_first(const SgmLaunch& l, int ndir, const int (*dirs)[2],
         tab.dy[i] = dirs[i][1];
         tab.out[i] = out[i];
     }
-    return dispatch<true>(a, tab, l.cvol == nullptr, sgm_lanes_for(l.Dp, l.lanes), st);
+    return dispatch<true>(a, tab, l.cvol == nullptr, sgm_lanes_for(l.Dp, l.lanes), l.split, st);
 }
 
 cudaError_t launch_sgm_last(const SgmLaunch& l, int dx, int dy, int nin, const uint32_t* const* in,
@@ -1097,7 +1329,7 @@ cudaError_t launch_sgm_last(const SgmLaunch& l, int dx, int dy, int nin, const u
     tab.dy[0] = dy;
     tab.nin = nin;
     for (int i = 0; i < nin; ++i) tab.in[i] = in[i];
-    return dispatch<false>(a, tab, l.cvol == nullptr, sgm_lanes_for(l.Dp, l.lanes), st);
+    return dispatch<false>(a, tab, l.cvol == nullptr, sgm_lanes_for(l.Dp, l.lanes), l.split, st);
 }
 
 cudaError_t launch_sgm_sum7(uint32_t* const* bufs, size_t words, cudaStream_t st) {

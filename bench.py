@@ -362,11 +362,7 @@ def _warm_server(apg, slots, pool):
     return srv
 
 
-def run_served(args):
-    """The served stream: requests of four sizes and three modes with Poisson arrivals, through
-    the served form (args.slots slots, continuous batching) and through the serial plain path
-    (one slot) on the same arrival stream; plus a saturation burst for each."""
-    import apg_sgm_b200 as apg
+def _served_pool():
     from apg_sgm_b200 import synthetic as S
     pool = {}
     for si, (w, h, D, cells, lo, hi) in enumerate(SERVED_SIZES):
@@ -375,11 +371,19 @@ def run_served(args):
                 spec = S.PairSpec(w, h, D, cells, lo, hi, 0.2 if mode == 2 else 0.0)
                 pool[(si, mode, sl)] = tuple(_pinned(a) for a in
                                              S.make_pair(spec, S.SEED_BASE + 1000 + si * 10 + mode * 2 + sl)[:2])
-    rates = [float(r) for r in args.rates.split(",")]
-    per_rate = max(1, args.requests // len(rates))
+    return pool
+
+
+def _served_measure(slots: int, rates, requests: int, burst_n: int = 1000) -> dict:
+    """The served stream: requests of four sizes and three modes with Poisson arrivals, through
+    the served form (`slots` slots, continuous batching) and through the serial plain path
+    (one slot) on the same arrival stream; plus a saturation burst for each."""
+    import apg_sgm_b200 as apg
+    pool = _served_pool()
+    per_rate = max(1, requests // len(rates))
     # one warm server per form for the whole run: every (mode, size) has its engines resident
     # (the served form: one per slot) before the first timed request
-    srv_served = _warm_server(apg, args.slots, pool)
+    srv_served = _warm_server(apg, slots, pool)
     srv_serial = _warm_server(apg, 1, pool)
     results = []
     for k, rate in enumerate(rates):
@@ -387,7 +391,7 @@ def run_served(args):
         served = _serve_stream(srv_served, pool, stream)
         serial = _serve_stream(srv_serial, pool, stream)
         results.append({"rate": rate, "requests": per_rate, "served": served, "serial": serial})
-    burst = _served_stream(min(per_rate, 1000), 0, 999)
+    burst = _served_stream(min(per_rate, burst_n), 0, 999)
     cap_served = _serve_stream(srv_served, pool, burst)
     cap_serial = _serve_stream(srv_serial, pool, burst)
     srv_served.close()
@@ -396,7 +400,15 @@ def run_served(args):
     # already on the device (sum of single-pair device times)
     bucket_ms = _bucket_device_ms(apg, pool)
     burst_device_s = sum(bucket_ms[(si, mode)] for _, si, mode, _ in burst) / 1000.0
-    device_bound = len(burst) / burst_device_s
+    return {"pool": pool, "per_rate": per_rate, "results": results, "burst": burst, "cap_served": cap_served,
+            "cap_serial": cap_serial, "bucket_ms": bucket_ms, "device_bound": len(burst) / burst_device_s}
+
+
+def run_served(args):
+    rates = [float(r) for r in args.rates.split(",")]
+    m = _served_measure(args.slots, rates, args.requests)
+    cap_served, cap_serial, results, per_rate = m["cap_served"], m["cap_serial"], m["results"], m["per_rate"]
+    bucket_ms, device_bound = m["bucket_ms"], m["device_bound"]
     mean_vox = float(np.mean([w * h * D for w, h, D, *_ in SERVED_SIZES]))
     top = results[-1]
     print(json.dumps({
@@ -406,20 +418,51 @@ def run_served(args):
         "data": "synthetic",
         "config": {"workload": "served_mixed_stream", "sizes": "640x480 D64, 1242x375 D192, 1280x720 D128, "
                    "1920x1080 D256", "modes": "70% Balanced, 20% Fast, 10% HighQuality", "arrivals": "Poisson",
-                   "rates": rates, "slots": args.slots, "hbm_budget_gb": 120, "pool_pairs": len(pool)},
+                   "rates": rates, "slots": args.slots, "hbm_budget_gb": 120, "pool_pairs": len(m["pool"])},
         "capacity": {"served_pairs_per_s": cap_served["pairs_per_s"], "serial_pairs_per_s": cap_serial["pairs_per_s"],
                      "speedup": cap_served["pairs_per_s"] / cap_serial["pairs_per_s"],
-                     "served_voxels_per_s": cap_served["pairs_per_s"] * mean_vox, "burst_requests": len(burst),
+                     "served_voxels_per_s": cap_served["pairs_per_s"] * mean_vox, "burst_requests": len(m["burst"]),
                      "device_bound_pairs_per_s": device_bound,
                      "served_over_device_bound": cap_served["pairs_per_s"] / device_bound,
                      "bucket_device_ms": {f"{SERVED_SIZES[si][0]}x{SERVED_SIZES[si][1]} D{SERVED_SIZES[si][2]} "
-                                          f"{MODE_NAMES[m]}": round(v, 4) for (si, m), v in sorted(bucket_ms.items())},
+                                          f"{MODE_NAMES[mo]}": round(v, 4) for (si, mo), v in sorted(bucket_ms.items())},
                      "served": cap_served, "serial": cap_serial},
         "rates": results,
         "latency_ms_at_top_rate": {"p50": top["served"]["p50_ms"], "p95": top["served"]["p95_ms"],
                                    "p99": top["served"]["p99_ms"]},
         "e2e": {"value": cap_served["pairs_per_s"], "unit": "pairs/s", "api": "apgcu_server_submit/wait (host buffers)"},
     }))
+
+
+def systems_records(args) -> dict:
+    """The two systems forms in brief, for the single-pair line: the 64-pair uneven batch (batched
+    vs plain, same outputs) and a short served stream (served vs serial plain, p50/p95/p99)."""
+    bm = _batched_measure(steps=3, warmup=2, clocks=False)
+    batched = {"workload": "64 uneven Balanced pairs (24x 640x480 D64, 24x 1242x375 D192, 16x 1280x720 D128)",
+               "steps": 3, "pairs_per_s": bm["npairs"] * 3 / (bm["batch_ms"] / 1000.0),
+               "plain_pairs_per_s": bm["npairs"] * 3 / (bm["plain_ms"] / 1000.0),
+               "speedup_vs_plain": bm["plain_ms"] / bm["batch_ms"], "identical_to_plain": bm["identical"],
+               "ms_per_batch": bm["batch_ms"] / 3, "plain_ms_per_batch": bm["plain_ms"] / 3,
+               "e2e_pairs_per_s": bm["npairs"] * bm["e2e_steps"] / bm["e2e_s"],
+               "how": "device time of apgcu_batch_process_device against the same pairs as sequential "
+                      "single-pair launches on one stream; inputs in HBM, L2 flushed between steps"}
+    rate = 400.0
+    sm = _served_measure(slots=4, rates=[rate], requests=args.served_requests, burst_n=args.served_requests)
+    r = sm["results"][0]
+    served = {"workload": "Poisson stream, sizes uniform over 640x480 D64 / 1242x375 D192 / 1280x720 D128 / "
+                          "1920x1080 D256, modes 70% Balanced / 20% Fast / 10% HighQuality",
+              "requests": sm["per_rate"], "offered_pairs_per_s": rate, "slots": 4,
+              "pairs_per_s": r["served"]["pairs_per_s"],
+              "p50_ms": r["served"]["p50_ms"], "p95_ms": r["served"]["p95_ms"], "p99_ms": r["served"]["p99_ms"],
+              "serial": {"pairs_per_s": r["serial"]["pairs_per_s"], "p50_ms": r["serial"]["p50_ms"],
+                         "p95_ms": r["serial"]["p95_ms"], "p99_ms": r["serial"]["p99_ms"]},
+              "capacity_pairs_per_s": sm["cap_served"]["pairs_per_s"],
+              "serial_capacity_pairs_per_s": sm["cap_serial"]["pairs_per_s"],
+              "capacity_speedup": sm["cap_served"]["pairs_per_s"] / sm["cap_serial"]["pairs_per_s"],
+              "device_bound_pairs_per_s": sm["device_bound"],
+              "how": "latency from submission to outputs on the host (apgcu_server_submit / wait); capacity "
+                     "from a saturation burst of the same mix; serial = the same server with one slot"}
+    return {"batched": batched, "served": served}
 
 
 def run_reference_batched(args):
@@ -529,6 +572,9 @@ def run_b200(args, wl):
     pairs = [tuple(_pinned(a) for a in S.make_pair(spec, S.SEED_BASE + rank * npairs + i)[:2]) for i in range(npairs)]
     cfg = apg.config_from_mode(mode, D, **over)
     eng = apg.Engine(cfg, device=local)
+    tuning = [(k, int(v)) for k, v in (t.split("=", 1) for t in args.tune)]
+    for k, v in tuning:
+        eng.set_tuning(k, v)
     es = torch.cuda.ExternalStream(eng.stream, device=dev)
     d_in = [(torch.from_numpy(l).to(dev), torch.from_numpy(r).to(dev)) for l, r in pairs]
     d_disp = torch.empty((h, w), dtype=torch.float32, device=dev)
@@ -597,6 +643,8 @@ def run_b200(args, wl):
         sess_c = lib.apgcu_session_create_config(C.byref(cfg), 1, 0)
     else:
         sess_c = lib.apg_session_create_ex(C.byref(opts))
+    for k, v in tuning:
+        lib.apgcu_session_set_tuning(sess_c, k.encode(), v)
     res_c = lib.apg_result_create()
     views = [(_lib.ImageView(l.ctypes.data, w, h, w, 1), _lib.ImageView(r.ctypes.data, w, h, w, 1)) for l, r in pairs]
     rw, rh = C.c_int(), C.c_int()
@@ -624,6 +672,8 @@ def run_b200(args, wl):
     # page-locked result block)
     sess = apg.StereoSession(mode=MODE_NAMES[mode].lower() if mode != 2 else "high_quality", max_disparity=D,
                              memory_policy="bounded_reuse", hierarchical=bool(over.get("hier_enable")))
+    for k, v in tuning:
+        sess.set_tuning(k, v)
     for i in range(max(args.warmup, 3)):
         sess.process(*pairs[i % npairs])
     npy = max(3, min(args.steps, 50))
@@ -663,7 +713,8 @@ def run_b200(args, wl):
         "vs_baseline": None, "dtype": "u16", "data": "synthetic",
         "config": {"workload": label, "mode": MODE_NAMES[mode], "width": w, "height": h, "max_disparity": D,
                    "pairs_per_step": 1, "distinct_pairs": npairs, "l2": "flushed between steps (256 MiB write)",
-                   "parallelism": f"replicas x{world}", **_scope_label(args)},
+                   "parallelism": f"replicas x{world}", **_scope_label(args),
+                   **({"tuning": dict(tuning)} if tuning else {})},
         "e2e": {"value": e2e_value, "unit": "voxels/s", "h2d_bytes_per_step": 2 * w * h,
                 "d2h_bytes_per_step": w * h * 10 + 64, "api": "apg_session_process (C API, BoundedReuse)" + (
                     "; session from apgcu_session_create_config" if over else ""),
@@ -681,35 +732,27 @@ def run_b200(args, wl):
         cb, parity = cpu_baseline(spec, mode, pairs[0][0], pairs[0][1], gpu0, over)
         out["cpu_baseline"] = cb
         out["parity_vs_cpu_baseline"] = "bit-exact" if parity else "MISMATCH"
-    if rank == 0:
-        print(json.dumps(out))
     del sess
     eng.close()
+    if rank == 0 and world == 1 and args.systems:
+        out.update(systems_records(args))
+    if rank == 0:
+        print(json.dumps(out))
     if dist:
         dist.barrier()
         dist.destroy_process_group()
 
 
-def run_batched(args):
+def _batched_measure(steps: int, warmup: int, local: int = 0, dist=None, rank: int = 0, world: int = 1,
+                     clocks: bool = True) -> dict:
     """The 64-pair uneven Balanced batch (24x 640x480 D64, 24x 1242x375 D192, 16x 1280x720 D128)
     through the batched form, against the same 64 pairs as sequential plain launches on one
     stream.  A step is the whole batch; inputs resident in HBM, L2 flushed between steps."""
-    import ctypes as C
     import torch
     import apg_sgm_b200 as apg
     from apg_sgm_b200 import _lib, replicas, synthetic as S
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     dev = torch.device("cuda", local)
-    torch.cuda.set_device(dev)
     specs = S.batched_mix()
     host = [tuple(_pinned(a) for a in S.make_pair(sp, S.SEED_BASE + rank * len(specs) + i)[:2])
             for i, sp in enumerate(specs)]
@@ -747,7 +790,7 @@ def run_batched(args):
                       o["reliable_mask"].data_ptr()) for sp, (l, r), o in zip(specs, d_in, o_batch)]
 
     # warm-up (the batched form tunes and captures its graphs here)
-    for _ in range(max(args.warmup, 3)):
+    for _ in range(max(warmup, 3)):
         with torch.cuda.stream(stream):
             plain_step()
         stream.synchronize()
@@ -757,11 +800,11 @@ def run_batched(args):
                     for a, b in zip(o_plain, o_batch) for k in a)
 
     # plain, timed on its stream
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    for k in range(args.steps):
+    for k in range(steps):
         with torch.cuda.stream(stream):
             flush.zero_()
             ev[k][0].record(stream)
@@ -771,31 +814,32 @@ def run_batched(args):
     plain_ms = sum(a.elapsed_time(b) for a, b in ev)
 
     # batched: device time of every call (start event to the latest bucket end)
-    sampler = ClockSampler(local)
-    sampler.start()
-    sampler.wait_first()
+    sampler = ClockSampler(local) if clocks else None
+    if sampler:
+        sampler.start()
+        sampler.wait_first()
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
     launches0 = apg.kernel_launch_count()
     batch_ms = 0.0
-    sampler.mark("timed_start")
-    for k in range(args.steps):
+    if sampler:
+        sampler.mark("timed_start")
+    for k in range(steps):
         flush.zero_()
         torch.cuda.synchronize()
         batch.process_device(recs)
         batch_ms += batch.last_time_ms
     torch.cuda.synchronize()
-    sampler.mark("timed_end")
+    if sampler:
+        sampler.mark("timed_end")
     launches = apg.kernel_launch_count() - launches0
-    clocks = sampler.stop()
+    clk = sampler.stop() if sampler else None
     batch_ms = replicas.max_over_ranks(batch_ms, dist, dev)
     plain_ms = replicas.max_over_ranks(plain_ms, dist, dev)
-    value = vox * args.steps * world / (batch_ms / 1000.0)
-    plain_value = vox * args.steps * world / (plain_ms / 1000.0)
 
     # end to end: host images in, host maps out, through apgcu_batch_process
-    e2e_steps = max(3, min(args.steps, 20))
+    e2e_steps = max(3, min(steps, 20))
     h_out = [{k: _pinned(np.zeros((sp.height, sp.width), dt)) for k, dt in
               (("disparity", np.float32), ("confidence", np.float32), ("invalid_reason", np.uint8),
                ("reliable_mask", np.uint8))} for sp in specs]
@@ -805,10 +849,35 @@ def run_batched(args):
     for _ in range(e2e_steps):
         batch.process([(l, r, sp.max_disparity) for sp, (l, r) in zip(specs, host)], out=h_out)
     e2e_s = time.perf_counter() - t0
-    e2e_value = vox * e2e_steps * world / e2e_s
+    batch.close()
+    for e in engines.values():
+        e.close()
+    return {"specs": specs, "host": host, "vox": vox, "npairs": npairs, "batch_ms": batch_ms, "plain_ms": plain_ms,
+            "identical": bool(identical), "launches": launches, "clocks": clk, "e2e_s": e2e_s,
+            "e2e_steps": e2e_steps}
+
+
+def run_batched(args):
+    """The 64-pair uneven batch as its own bench line (see _batched_measure)."""
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    torch.cuda.set_device(torch.device("cuda", local))
+    m = _batched_measure(args.steps, args.warmup, local, dist, rank, world)
+    specs, host, vox, npairs = m["specs"], m["host"], m["vox"], m["npairs"]
+    batch_ms, plain_ms = m["batch_ms"], m["plain_ms"]
+    value = vox * args.steps * world / (batch_ms / 1000.0)
+    plain_value = vox * args.steps * world / (plain_ms / 1000.0)
+    e2e_value = vox * m["e2e_steps"] * world / m["e2e_s"]
     h2d = sum(2 * sp.width * sp.height for sp in specs)
     d2h = sum(10 * sp.width * sp.height for sp in specs)
-
     peak, peak_kind = _peaks()
     # the whole pipeline against the stage-boundary byte model (36 B per voxel for Balanced)
     achieved = 36.0 * vox / (batch_ms / args.steps / 1000.0) / 1e9
@@ -824,13 +893,13 @@ def run_batched(args):
                   "pairs_per_s": npairs * args.steps * world / (plain_ms / 1000.0),
                   "how": "the 64 pairs as sequential single-pair launches on one stream"},
         "speedup_vs_plain": plain_ms / batch_ms,
-        "identical_to_plain": bool(identical),
+        "identical_to_plain": m["identical"],
         "e2e": {"value": e2e_value, "unit": "voxels/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "api": "apgcu_batch_process (host buffers)"},
-        "gpu_launches": launches,
+        "gpu_launches": m["launches"],
         "roofline": {"bound": "hbm", "kernel": "pipeline (36 B/voxel stage-boundary model)", "achieved": achieved,
                      "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None},
-        "clocks": clocks,
+        "clocks": m["clocks"],
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle import oracle as O
@@ -850,9 +919,6 @@ def run_batched(args):
                                              "scaled by the batch's pair counts"}
     if rank == 0:
         print(json.dumps(out))
-    batch.close()
-    for e in engines.values():
-        e.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -1155,7 +1221,15 @@ def main():
                          "stabilized, optionally :PARAM")
     ap.add_argument("--inpaint", default="legacy",
                     help="ExperimentalInpaintScope for the single-pair workloads: legacy | shadow_reclass, optionally :GAP")
+    ap.add_argument("--tune", action="append", default=[],
+                    help="engine tuning KEY=VALUE for the single-pair workloads' engines and sessions (repeatable)")
+    ap.add_argument("--no-systems", action="store_true",
+                    help="leave the batched and served sub-records out of the default (single GPU) line")
+    ap.add_argument("--served-requests", type=int, default=400,
+                    help="requests of the default line's served stream (and of its saturation burst)")
     args = ap.parse_args()
+    # the headline line (default workload, one GPU) carries the two systems forms in brief
+    args.systems = args.workload == "fast720" and not args.no_systems and args.gpus == 1
     if args.workload == "served":
         if args.impl == "reference":
             if int(os.environ.get("RANK", "0")) == 0:

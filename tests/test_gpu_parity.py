@@ -228,3 +228,26 @@ def test_range_dump_without_debug(apg, mode, dmin):
     want_max = np.maximum(np.minimum(dmax, x + 1), dmin).astype(np.int16)
     assert (rmin == dmin).all()
     assert (rmax == want_max[None, :]).all()
+
+
+@pytest.mark.parametrize("mode,w,h,dmax,over", [
+    (0, 200, 100, 48, {}), (1, 333, 90, 128, {}), (1, 150, 80, 200, {}), (1, 120, 90, 40, {"paths": 8}),
+    (2, 160, 96, 64, {}), (1, 97, 61, 24, {"min_disparity": -6}), (0, 64, 7, 16, {}),
+])
+def test_sgm_split_changes_no_result(apg, mode, w, h, dmax, over):
+    """The last sweep split over two warps per chain (tuning sgm_split=2) and the one-warp form
+    (sgm_split=1) give identical maps and path sums, for every range width and both path counts."""
+    L, R = synth(w, h, dmax, patch=0.2 if mode == 2 else 0.0, seed=23)
+    over = dict(over)
+    dmin = over.pop("min_disparity", 0)
+    cfg = apg.config_from_mode(mode, dmax, dmin, **over)
+    outs = []
+    for split in (1, 2):
+        e = apg.Engine(cfg, debug=apg.DEBUG_KEEP_SUM)
+        e.set_tuning("sgm_split", split)
+        o = e.process(L, R)
+        o["sgm_sum"] = e.dump("sgm_sum")
+        e.close()
+        outs.append(o)
+    for k in outs[0]:
+        assert same_bits(outs[0][k], outs[1][k]), k
