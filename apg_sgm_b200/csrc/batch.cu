@@ -1,17 +1,20 @@
 // Batched form: many stereo pairs, of uneven sizes, per call.
 //
 // Pairs are grouped into buckets of equal (width, height, channels, max_disparity).  A bucket owns
-// one engine (device workspace + stream) per pair slot.  A call runs, per bucket:
+// one engine (device workspace + stream) per pair slot.  A call runs:
 //   * every pair's phases before the SGM (aux, range, cost + cross-H + right argmin, cross-V) on
 //     its own stream, so the pairs' kernels overlap on the device;
-//   * ONE persistent SGM launch per phase for all the bucket's pairs (sgm_batch_kernel: warps pull
-//     (pair, direction, scanline) units from a work queue), so the latency-bound sweeps of small
-//     pairs fill the GPU together;
+//   * ONE persistent SGM launch per phase for the pairs of ALL buckets, whatever their sizes and
+//     disparity ranges (sgm_batch_mixed_kernel: warps pull (pair, direction, scanline) units,
+//     longest chains first, from one work queue, each unit running with its own pair's words per
+//     lane), so the latency-bound sweeps of every pair fill the GPU together;
 //   * every pair's phases after the SGM (confidence, LR, fill, median, frame counters) on its
 //     stream again.
-// The whole per-bucket sequence is captured once into a CUDA graph per (bucket, pair count) and
-// replayed; inputs are copied into the slots' fixed input buffers before the replay and the
-// outputs copied out after it.  Buckets run on their own streams, concurrently.
+// The whole sequence is captured once into a CUDA graph per batch composition (the buckets and
+// their pair counts) and replayed; inputs are copied into the slots' fixed input buffers before
+// the replay and the outputs copied out after it.  The option "unified_sgm" 0 (or 16 lanes per
+// chain from the tuner) runs each bucket on its own stream instead, with one SGM launch per phase
+// per bucket, captured per (bucket, pair count).
 //
 // Tuning (tile width of the cost kernel, lanes per SGM scanline, persistent-grid cap) is chosen
 // per (W, D) bucket by an autotuner that times the candidates on the bucket's first pair and
@@ -113,6 +116,7 @@ void tune_store_locked(const std::string& key, const Tuning& t) {
 class Batch {
 public:
     Batch(const apg_pipeline_config_t& cfg, int device) : cfg_(cfg), device_(device) {}
+    using Composition = std::vector<std::pair<BucketKey, int>>;  // buckets of a call and their pair counts
     ~Batch() { release(); }
 
     int process(int n, const apgcu_pair_t* pairs, bool device_buffers);
@@ -133,17 +137,31 @@ private:
     int enqueue(Bucket& b, int m, bool batched_sgm);
     int run_bucket(Bucket& b, int m, bool batched_sgm);
     int autotune(Bucket& b, const apgcu_pair_t& sample, bool device_buffers);
+    // one SGM launch per phase over every bucket of the call
+    struct Unified {
+        SgmBatchPlan plan;
+        cudaGraphExec_t graph = nullptr;
+        unsigned long long launches = 0;  // kernels per replay
+    };
+    int ensure_unified_streams();
+    int enqueue_unified(const Composition& comp, Unified& u);
+    int run_unified(const Composition& comp);
+    void drop_unified();
 
     apg_pipeline_config_t cfg_;
     int device_ = 0;
     bool use_graphs_ = true;
     bool use_batched_sgm_ = true;
+    bool use_unified_ = true;
     bool autotune_ = true;
     bool graph_capture_ = false;  // inside a capture: launches are counted at replay
     int forced_lanes_ = 0;
     int forced_max_blocks_ = -1;
     int forced_tile_ = -1;
     std::map<BucketKey, std::unique_ptr<Bucket>> buckets_;
+    std::map<Composition, Unified> unified_;
+    cudaStream_t ustream_ = nullptr;  // the unified sequence's stream
+    cudaEvent_t ufork_ = nullptr, usgm_done_ = nullptr, udone_ = nullptr;
     cudaStream_t start_stream_ = nullptr;
     cudaEvent_t start_ = nullptr;
     float last_ms_ = 0.f;
@@ -292,6 +310,127 @@ int Batch::run_bucket(Bucket& b, int m, bool batched_sgm) {
     return kOk;
 }
 
+int Batch::ensure_unified_streams() {
+    if (ustream_) return kOk;
+    if (cudaStreamCreateWithFlags(&ustream_, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ufork_, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&usgm_done_, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&udone_, cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(kInternalError, "batch stream creation failed");
+    }
+    return kOk;
+}
+
+void Batch::drop_unified() {
+    if (ustream_) cudaStreamSynchronize(ustream_);
+    for (auto& kv : unified_) {
+        if (kv.second.graph) cudaGraphExecDestroy(kv.second.graph);
+        sgm_batch_plan_destroy(&kv.second.plan);
+    }
+    unified_.clear();
+}
+
+// Every bucket's pairs: pre-SGM phases on the slot streams, the two SGM launches on ustream_ over
+// all pairs, post-SGM phases on the slot streams, everything joined back to ustream_.
+int Batch::enqueue_unified(const Composition& comp, Unified& u) {
+    cudaEventRecord(ufork_, ustream_);
+    for (const auto& bm : comp) {
+        Bucket& b = bucket_for(bm.first);
+        for (int k = 0; k < bm.second; ++k) {
+            Engine& e = *b.slots[k];
+            cudaStreamWaitEvent(e.stream(), ufork_, 0);
+            const int rc = e.enqueue_pre();
+            if (rc) return fail(rc, e.last_error());
+            cudaEventRecord(b.joined[k], e.stream());
+            cudaStreamWaitEvent(ustream_, b.joined[k], 0);
+        }
+    }
+    int max_blocks = forced_max_blocks_ >= 0 ? forced_max_blocks_ : 0;
+    const cudaError_t ce = launch_sgm_batch(u.plan, max_blocks, ustream_);
+    if (!graph_capture_) count_launches(2);
+    if (ce != cudaSuccess) return fail(kInternalError, std::string("batched SGM: ") + cudaGetErrorString(ce));
+    cudaEventRecord(usgm_done_, ustream_);
+    for (const auto& bm : comp) {
+        Bucket& b = bucket_for(bm.first);
+        for (int k = 0; k < bm.second; ++k) {
+            Engine& e = *b.slots[k];
+            cudaStreamWaitEvent(e.stream(), usgm_done_, 0);
+            const int rc = e.enqueue_post();
+            if (rc) return fail(rc, e.last_error());
+            cudaEventRecord(b.joined[k], e.stream());
+            cudaStreamWaitEvent(ustream_, b.joined[k], 0);
+        }
+    }
+    return kOk;
+}
+
+int Batch::run_unified(const Composition& comp) {
+    auto it = unified_.find(comp);
+    if (it == unified_.end()) {
+        std::vector<SgmLaunch> pl;
+        std::vector<uint32_t*> sb;
+        int nsbuf = 0;
+        for (const auto& bm : comp) {
+            Bucket& b = bucket_for(bm.first);
+            for (int k = 0; k < bm.second; ++k) {
+                SgmLaunch l;
+                uint32_t* s7[7];
+                nsbuf = b.slots[k]->sgm_launch(&l, s7);
+                pl.push_back(l);
+                sb.insert(sb.end(), s7, s7 + nsbuf);
+            }
+        }
+        Unified u;
+        const cudaError_t e = sgm_batch_plan_create(pl.data(), sb.data(), (int)pl.size(), nsbuf, 32, &u.plan);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return fail(kInternalError, std::string("batch plan: ") + cudaGetErrorString(e));
+        }
+        it = unified_.emplace(comp, u).first;
+    }
+    Unified& u = it->second;
+    // HighQuality refinement is not captured (as in run_bucket)
+    bool graph = use_graphs_;
+    for (const auto& bm : comp)
+        if (bucket_for(bm.first).slots[0]->refine_enabled()) graph = false;
+    if (!graph) return enqueue_unified(comp, u);
+    if (!u.graph) {
+        cudaGraph_t g = nullptr;
+        if (cudaStreamBeginCapture(ustream_, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+            cudaGetLastError();
+            return enqueue_unified(comp, u);
+        }
+        graph_capture_ = true;
+        const unsigned long long before = launch_count();
+        const int rc = enqueue_unified(comp, u);
+        const unsigned long long captured = launch_count() - before;
+        const cudaError_t ce = cudaStreamEndCapture(ustream_, &g);
+        graph_capture_ = false;
+        if (rc != kOk || ce != cudaSuccess) {
+            cudaGetLastError();
+            if (g) cudaGraphDestroy(g);
+            if (rc != kOk) return rc;
+            return fail(kInternalError, std::string("batch graph capture: ") + cudaGetErrorString(ce));
+        }
+        cudaGraphExec_t ex = nullptr;
+        const cudaError_t ie = cudaGraphInstantiate(&ex, g, 0);
+        cudaGraphDestroy(g);
+        if (ie != cudaSuccess) {
+            cudaGetLastError();
+            return fail(kInternalError, std::string("batch graph instantiate: ") + cudaGetErrorString(ie));
+        }
+        u.graph = ex;
+        u.launches = captured + 2;
+        count_launches(0);
+    } else {
+        count_launches((unsigned)u.launches);
+    }
+    const cudaError_t le = cudaGraphLaunch(u.graph, ustream_);
+    if (le != cudaSuccess) return fail(kInternalError, std::string("batch graph launch: ") + cudaGetErrorString(le));
+    return kOk;
+}
+
 // Times the candidate tunings on one pair of the bucket (a single-pair batch through the batched
 // SGM) and keeps the fastest; the caches make this happen once per (mode, W, H, D).
 int Batch::autotune(Bucket& b, const apgcu_pair_t& sample, bool device_buffers) {
@@ -313,6 +452,8 @@ int Batch::autotune(Bucket& b, const apgcu_pair_t& sample, bool device_buffers) 
         for (int lanes : {32, 16})
             for (int mb : {0, 2}) {
                 if (lanes == 16 && Dp > 256) continue;
+                // one launch serves every bucket: 32 lanes per chain, the occupancy-limited grid
+                if (use_unified_ && (lanes != 32 || mb != 0)) continue;
                 Tuning t;
                 t.sgm_lanes = lanes;
                 t.max_blocks_per_sm = mb;
@@ -420,9 +561,13 @@ int Batch::process(int n, const apgcu_pair_t* pairs, bool device_buffers) {
             sl->set_cost_tile(b.tune.cost_tile);
         }
         drop_plans(b);
+        drop_unified();  // graphs of compositions with this bucket hold its old tuning
     }
     cudaEventRecord(start_, start_stream_);
     std::vector<std::pair<Bucket*, const std::vector<int>*>> order;
+    std::vector<bool> batched_of;
+    Composition comp;
+    bool unified = use_unified_ && use_batched_sgm_;
     for (auto& g : groups) {
         Bucket& b = bucket_for(g.first);
         const std::vector<int>& idx = g.second;
@@ -440,6 +585,7 @@ int Batch::process(int n, const apgcu_pair_t* pairs, bool device_buffers) {
         const ExperimentalScope cur = experimental_scope();
         if (!same_scope(cur, b.scope)) {
             drop_plans(b);
+            drop_unified();
             b.scope = cur;
         }
         for (int k = 0; k < m; ++k) b.slots[k]->capture_scope();
@@ -448,12 +594,37 @@ int Batch::process(int n, const apgcu_pair_t* pairs, bool device_buffers) {
         uint32_t* s7[7];
         b.slots[0]->sgm_launch(&probe, s7);
         const bool batched = use_batched_sgm_ && sgm_batch_supported(Dp) && probe.cvol != nullptr;
-        if (batched) {
-            rc = ensure_plan(b, m);
+        if (!batched || b.tune.sgm_lanes != 32) unified = false;
+        batched_of.push_back(batched);
+        comp.emplace_back(g.first, m);
+        order.emplace_back(&b, &idx);
+    }
+    if (unified) {
+        int rc = ensure_unified_streams();
+        if (rc) return rc;
+        for (auto& o : order) {
+            cudaEventRecord(o.first->fork, o.first->stream);  // the bucket's uploads are enqueued
+            cudaStreamWaitEvent(ustream_, o.first->fork, 0);
+        }
+        rc = run_unified(comp);
+        if (rc) return rc;
+        cudaEventRecord(udone_, ustream_);
+    }
+    for (size_t bi = 0; bi < order.size(); ++bi) {
+        Bucket& b = *order[bi].first;
+        const std::vector<int>& idx = *order[bi].second;
+        const int m = (int)idx.size();
+        int rc = kOk;
+        if (unified) {
+            cudaStreamWaitEvent(b.stream, udone_, 0);
+        } else {
+            if (batched_of[bi]) {
+                rc = ensure_plan(b, m);
+                if (rc) return rc;
+            }
+            rc = run_bucket(b, m, batched_of[bi]);
             if (rc) return rc;
         }
-        rc = run_bucket(b, m, batched);
-        if (rc) return rc;
         for (int k = 0; k < m; ++k) {
             const apgcu_pair_t& p = pairs[idx[k]];
             rc = b.slots[k]->download(p.disparity, p.confidence, p.invalid_reason, p.reliable_mask, device_buffers,
@@ -461,7 +632,6 @@ int Batch::process(int n, const apgcu_pair_t* pairs, bool device_buffers) {
             if (rc) return fail(rc, b.slots[k]->last_error());
         }
         cudaEventRecord(b.done, b.stream);
-        order.emplace_back(&b, &idx);
     }
     for (auto& o : order) {
         const cudaError_t e = cudaStreamSynchronize(o.first->stream);
@@ -494,6 +664,7 @@ int Batch::set_option(const char* key, int value) {
     const std::string k(key);
     if (k == "graphs") use_graphs_ = value != 0;
     else if (k == "batched_sgm") use_batched_sgm_ = value != 0;
+    else if (k == "unified_sgm") use_unified_ = value != 0;
     else if (k == "autotune") autotune_ = value != 0;
     else if (k == "sgm_lanes") {
         if (value != 0 && value != 16 && value != 32) return kInvalidConfig;
@@ -512,6 +683,7 @@ int Batch::set_option(const char* key, int value) {
         drop_plans(*kv.second);
         kv.second->tuned = false;
     }
+    drop_unified();
     return kOk;
 }
 
@@ -524,6 +696,13 @@ size_t Batch::allocated_bytes() const {
 
 void Batch::release() {
     cudaSetDevice(device_);
+    drop_unified();
+    if (ufork_) cudaEventDestroy(ufork_);
+    if (usgm_done_) cudaEventDestroy(usgm_done_);
+    if (udone_) cudaEventDestroy(udone_);
+    if (ustream_) cudaStreamDestroy(ustream_);
+    ufork_ = usgm_done_ = udone_ = nullptr;
+    ustream_ = nullptr;
     for (auto& kv : buckets_) {
         Bucket& b = *kv.second;
         drop_plans(b);

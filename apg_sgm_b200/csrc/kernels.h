@@ -83,19 +83,22 @@ cudaError_t launch_sgm_last(const SgmLaunch& l, int dx, int dy, int nin, const u
 cudaError_t launch_sgm_sum7(uint32_t* const* bufs, size_t words, cudaStream_t s);
 int sgm_lanes_for(int Dp, int requested);
 
-// Batches: the SGM of many pairs with the same Dp (64, 128, 192 or 256), volume-fed, in two
-// persistent launches (every pair's first-phase directions, then every pair's last sweep + WTA).
+// Batches: the SGM of many pairs (Dp 64, 128, 192 or 256), volume-fed, in two persistent launches
+// (every pair's first-phase directions, then every pair's last sweep + WTA).
 struct SgmBatchPlan {
-    int npairs = 0, nsbuf = 0, Dp = 0, lanes = 32;
+    int npairs = 0, nsbuf = 0, Dp = 0, lanes = 32;  // Dp: the widest pair's padded range
+    bool mixed = false;                              // pairs of different Dp (one launch per phase all the same)
     int nseg_first = 0, total_first = 0, nseg_last = 0, total_last = 0;
-    size_t words = 0;  // 32-bit words of one pair's path-sum buffer
+    std::vector<size_t> words;  // per pair: 32-bit words of one path-sum buffer
     void* dev = nullptr;
     size_t off_first = 0, off_last = 0, off_queue = 0;
     std::vector<uint32_t*> sums;  // npairs x nsbuf path-sum buffers
 };
 bool sgm_batch_supported(int Dp);
 // pl[i]: pair i's launch arguments; sbufs[i*nsbuf + d]: its path-sum buffers (nsbuf 3 or 7);
-// lanes: 16 or 32 lanes per chain.  Uploads the work tables (synchronous).
+// lanes: 16 or 32 lanes per chain.  Pairs may differ in size and, with 32 lanes, in padded range
+// (Dp 64 .. 256): every phase is still one persistent launch whose warps take (pair, direction,
+// scanline) units of every pair.  Uploads the work tables (synchronous).
 cudaError_t sgm_batch_plan_create(const SgmLaunch* pl, uint32_t* const* sbufs, int npairs, int nsbuf, int lanes,
                                   SgmBatchPlan* plan);
 void sgm_batch_plan_destroy(SgmBatchPlan* plan);

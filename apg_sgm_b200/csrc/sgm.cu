@@ -1219,6 +1219,113 @@ __global__ void __launch_bounds__(128) sgm_batch_kernel(const BatchPair* __restr
     }
 }
 
+// Pairs of different padded ranges in one launch (32 lanes per chain): a warp's unit names its
+// pair, and the chain runs with that pair's words per lane K = Dp / 64 (up to KMAX).  Each warp's
+// shared-memory region holds the largest ring (and WTA buffer) any K of the launch needs.
+template <int K, int MODE, int NB>
+__host__ __device__ constexpr int mixed_pf() {
+    return MODE == kFirst ? first_pf<32>() : last_pf<K, 32, NB>();
+}
+template <int K, int MODE, int NB>
+__host__ __device__ constexpr int mixed_ring_words() {
+    return mixed_pf<K, MODE, NB>() * vol_slot_words<K, NB>();
+}
+template <int K, int MODE, int NB>
+__host__ __device__ constexpr int mixed_warp_words() {
+    return mixed_ring_words<K, MODE, NB>() + (MODE == kLast ? wta_buf_words<K, 32>() : 0);
+}
+template <int KMAX, int MODE, int NB>
+__host__ __device__ constexpr int mixed_region_words() {
+    int m = 0;
+    if (KMAX >= 1 && mixed_warp_words<1, MODE, NB>() > m) m = mixed_warp_words<1, MODE, NB>();
+    if (KMAX >= 2 && mixed_warp_words<2, MODE, NB>() > m) m = mixed_warp_words<2, MODE, NB>();
+    if (KMAX >= 3 && mixed_warp_words<3, MODE, NB>() > m) m = mixed_warp_words<3, MODE, NB>();
+    if (KMAX >= 4 && mixed_warp_words<4, MODE, NB>() > m) m = mixed_warp_words<4, MODE, NB>();
+    return m;
+}
+
+template <int K, int MODE, int NB>
+__device__ __forceinline__ void run_mixed_unit(const SgmArgs& a, const uint32_t* const* in, uint32_t* region,
+                                               const BatchSeg& sg, int scan, uint32_t* out) {
+    run_chain_vol<32, K, MODE, mixed_pf<K, MODE, NB>(), NB>(a, in, region, region + mixed_ring_words<K, MODE, NB>(),
+                                                            sg.dx, sg.dy, scan, sg.nscan, out);
+}
+
+template <int KMAX, int MODE, int NB>
+__global__ void __launch_bounds__(128) sgm_batch_mixed_kernel(const BatchPair* __restrict__ pairs,
+                                                              const BatchSeg* __restrict__ segs, int nseg, int total,
+                                                              int* __restrict__ queue) {
+    extern __shared__ __align__(16) uint32_t s_dyn[];
+    constexpr int per_warp = mixed_region_words<KMAX, MODE, NB>();
+    BatchSeg* s_seg = reinterpret_cast<BatchSeg*>(s_dyn + 4 * per_warp);
+    for (int i = threadIdx.x; i < nseg; i += blockDim.x) s_seg[i] = segs[i];
+    __syncthreads();
+    uint32_t* region = s_dyn + (threadIdx.x >> 5) * per_warp;
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        int unit = 0;
+        if (lane == 0) unit = atomicAdd(queue, 1);
+        unit = __shfl_sync(0xffffffffu, unit, 0);
+        if (unit >= total) break;
+        int lo = 0, hi = nseg - 1;  // the last segment whose first unit is <= unit
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (s_seg[mid].begin <= unit) lo = mid;
+            else hi = mid - 1;
+        }
+        const BatchSeg sg = s_seg[lo];
+        const BatchPair* bp = pairs + sg.pair;
+        const SgmArgs a = bp->a;
+        const uint32_t* in[NB > 0 ? NB : 1];
+#pragma unroll
+        for (int b = 0; b < NB; ++b) in[b] = bp->in[b];
+        uint32_t* out = MODE == kFirst ? bp->out[sg.dir] : nullptr;
+        const int scan = unit - sg.begin;  // one scanline per unit (32 lanes per chain)
+        switch (a.Dp >> 6) {
+            case 1: run_mixed_unit<1, MODE, NB>(a, in, region, sg, scan, out); break;
+            case 2: if constexpr (KMAX >= 2) run_mixed_unit<2, MODE, NB>(a, in, region, sg, scan, out); break;
+            case 3: if constexpr (KMAX >= 3) run_mixed_unit<3, MODE, NB>(a, in, region, sg, scan, out); break;
+            default: if constexpr (KMAX >= 4) run_mixed_unit<4, MODE, NB>(a, in, region, sg, scan, out); break;
+        }
+    }
+}
+
+template <int KMAX, int MODE, int NB>
+cudaError_t launch_batch_mixed_k(const BatchPair* pairs, const BatchSeg* segs, int nseg, int total, int* queue,
+                                 int max_blocks_per_sm, cudaStream_t st) {
+    auto kern = sgm_batch_mixed_kernel<KMAX, MODE, NB>;
+    const size_t smem = (size_t)4 * mixed_region_words<KMAX, MODE, NB>() * 4 + (size_t)nseg * sizeof(BatchSeg);
+    {
+        const cudaError_t e = allow_dynamic_smem(kern, smem);
+        if (e != cudaSuccess) return e;
+    }
+    int dev = 0, nsm = 148, occ = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, 128, smem);
+    if (e != cudaSuccess) return e;
+    if (occ < 1) return cudaErrorInvalidConfiguration;
+    if (max_blocks_per_sm > 0 && occ > max_blocks_per_sm) occ = max_blocks_per_sm;
+    int blocks = nsm * occ;
+    const int need = (total + 3) / 4;
+    if (blocks > need) blocks = need;
+    if (blocks < 1) blocks = 1;
+    kern<<<blocks, 128, smem, st>>>(pairs, segs, nseg, total, queue);
+    return cudaGetLastError();
+}
+
+template <int MODE, int NB>
+cudaError_t launch_batch_mixed(int Dp_max, const BatchPair* pairs, const BatchSeg* segs, int nseg, int total,
+                               int* queue, int max_blocks_per_sm, cudaStream_t st) {
+    switch (Dp_max >> 6) {
+        case 1: return launch_batch_mixed_k<1, MODE, NB>(pairs, segs, nseg, total, queue, max_blocks_per_sm, st);
+        case 2: return launch_batch_mixed_k<2, MODE, NB>(pairs, segs, nseg, total, queue, max_blocks_per_sm, st);
+        case 3: return launch_batch_mixed_k<3, MODE, NB>(pairs, segs, nseg, total, queue, max_blocks_per_sm, st);
+        case 4: return launch_batch_mixed_k<4, MODE, NB>(pairs, segs, nseg, total, queue, max_blocks_per_sm, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
 template <int T, int K, int MODE, int NB>
 constexpr int batch_pf() {
     return MODE == kFirst ? first_pf<T>() : last_pf<K, T, NB>();
@@ -1350,11 +1457,15 @@ cudaError_t sgm_batch_plan_create(const SgmLaunch* pl, uint32_t* const* sbufs, i
                                   SgmBatchPlan* plan) {
     *plan = SgmBatchPlan();
     if (npairs < 1 || (nsbuf != 3 && nsbuf != 7)) return cudaErrorInvalidValue;
-    const int Dp = pl[0].Dp;
-    if (!sgm_batch_supported(Dp)) return cudaErrorInvalidValue;
-    for (int i = 0; i < npairs; ++i)
-        if (pl[i].Dp != Dp || !pl[i].cvol) return cudaErrorInvalidValue;
     const int T = lanes == 16 ? 16 : 32;
+    int Dp = 0;
+    bool mixed = false;
+    for (int i = 0; i < npairs; ++i) {
+        if (!sgm_batch_supported(pl[i].Dp) || !pl[i].cvol) return cudaErrorInvalidValue;
+        if (i > 0 && pl[i].Dp != pl[0].Dp) mixed = true;
+        Dp = std::max(Dp, pl[i].Dp);
+    }
+    if (mixed && T != 32) return cudaErrorInvalidValue;  // mixed ranges run one scanline per warp
     const int C = 32 / T;
     static const int first4[3][2] = {{1, 0}, {-1, 0}, {0, 1}};
     static const int first8[7][2] = {{1, 0}, {-1, 0}, {0, 1}, {1, 1}, {1, -1}, {-1, 1}, {-1, -1}};
@@ -1403,8 +1514,10 @@ cudaError_t sgm_batch_plan_create(const SgmLaunch* pl, uint32_t* const* sbufs, i
     plan->npairs = npairs;
     plan->nsbuf = nsbuf;
     plan->Dp = Dp;
+    plan->mixed = mixed;
     plan->lanes = T;
-    plan->words = (size_t)pl[0].w * pl[0].h * (Dp / 2);
+    plan->words.resize(npairs);
+    for (int i = 0; i < npairs; ++i) plan->words[i] = (size_t)pl[i].w * pl[i].h * (pl[i].Dp / 2);
     // device tables: pairs | first segments | last segments | 2 queue counters
     const size_t b_pairs = sizeof(BatchPair) * npairs;
     const size_t b_first = sizeof(BatchSeg) * first.size();
@@ -1440,24 +1553,29 @@ cudaError_t launch_sgm_batch(const SgmBatchPlan& plan, int max_blocks_per_sm, cu
     unsigned char* base = static_cast<unsigned char*>(plan.dev);
     const BatchPair* pairs = reinterpret_cast<const BatchPair*>(base);
     int* queue = reinterpret_cast<int*>(base + plan.off_queue);
+    const BatchSeg* first = reinterpret_cast<const BatchSeg*>(base + plan.off_first);
+    const BatchSeg* last = reinterpret_cast<const BatchSeg*>(base + plan.off_last);
     cudaError_t e = cudaMemsetAsync(queue, 0, 2 * sizeof(int), st);
     if (e != cudaSuccess) return e;
-    e = launch_batch_dispatch<kFirst, 0>(plan.lanes, plan.Dp, pairs,
-                                         reinterpret_cast<const BatchSeg*>(base + plan.off_first), plan.nseg_first,
-                                         plan.total_first, queue, max_blocks_per_sm, st);
+    e = plan.mixed ? launch_batch_mixed<kFirst, 0>(plan.Dp, pairs, first, plan.nseg_first, plan.total_first, queue,
+                                                   max_blocks_per_sm, st)
+                   : launch_batch_dispatch<kFirst, 0>(plan.lanes, plan.Dp, pairs, first, plan.nseg_first,
+                                                      plan.total_first, queue, max_blocks_per_sm, st);
     if (e != cudaSuccess) return e;
     if (plan.nsbuf == 7) {
         for (int i = 0; i < plan.npairs; ++i) {
-            e = launch_sgm_sum7(plan.sums.data() + (size_t)i * 7, plan.words, st);
+            e = launch_sgm_sum7(plan.sums.data() + (size_t)i * 7, plan.words[i], st);
             if (e != cudaSuccess) return e;
         }
-        return launch_batch_dispatch<kLast, 1>(plan.lanes, plan.Dp, pairs,
-                                               reinterpret_cast<const BatchSeg*>(base + plan.off_last), plan.nseg_last,
-                                               plan.total_last, queue + 1, max_blocks_per_sm, st);
+        return plan.mixed ? launch_batch_mixed<kLast, 1>(plan.Dp, pairs, last, plan.nseg_last, plan.total_last,
+                                                         queue + 1, max_blocks_per_sm, st)
+                          : launch_batch_dispatch<kLast, 1>(plan.lanes, plan.Dp, pairs, last, plan.nseg_last,
+                                                            plan.total_last, queue + 1, max_blocks_per_sm, st);
     }
-    return launch_batch_dispatch<kLast, 3>(plan.lanes, plan.Dp, pairs,
-                                           reinterpret_cast<const BatchSeg*>(base + plan.off_last), plan.nseg_last,
-                                           plan.total_last, queue + 1, max_blocks_per_sm, st);
+    return plan.mixed ? launch_batch_mixed<kLast, 3>(plan.Dp, pairs, last, plan.nseg_last, plan.total_last, queue + 1,
+                                                     max_blocks_per_sm, st)
+                      : launch_batch_dispatch<kLast, 3>(plan.lanes, plan.Dp, pairs, last, plan.nseg_last,
+                                                        plan.total_last, queue + 1, max_blocks_per_sm, st);
 }
 
 }  // namespace apgcu

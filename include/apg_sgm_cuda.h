@@ -235,11 +235,13 @@ APGCU_API unsigned long long apgcu_kernel_launch_count(void);
 /* ---- Batched form: many pairs of uneven sizes per call.
  *
  * No counterpart in the reference (which processes one pair per call): pairs are grouped into
- * buckets of equal size and disparity range; each bucket's pairs run their per-pixel stages on
- * their own streams and share one persistent SGM launch per phase (a work queue of (pair,
- * direction, scanline) units); the per-bucket sequence is a cached CUDA graph; lanes per scanline
- * and the persistent-grid cap are autotuned per bucket.  Every pair's outputs equal what
- * apgcu_engine_process gives for it alone. */
+ * buckets of equal size and disparity range; every pair runs its per-pixel stages on its own
+ * stream, and the pairs of ALL buckets share one persistent SGM launch per phase (a work queue of
+ * (pair, direction, scanline) units over pairs of any size and padded range); the whole call is a
+ * cached CUDA graph per composition (buckets and pair counts); the cost kernel's tile width is
+ * autotuned per bucket.  With the option "unified_sgm" 0 each bucket runs on its own stream with
+ * its own SGM launches, and the tuner also chooses lanes per scanline and the persistent-grid cap.
+ * Every pair's outputs equal what apgcu_engine_process gives for it alone. */
 typedef struct apgcu_batch_s* apgcu_batch_t;
 typedef struct {
     const uint8_t* left;        /* host or device memory, as the call's device_buffers says */
@@ -260,8 +262,9 @@ APGCU_API const char* apgcu_batch_last_error(apgcu_batch_t b);
 /* Processes npairs pairs and returns when every output is written.  device_buffers != 0: inputs
  * and outputs are device pointers on the batch's device. */
 APGCU_API int apgcu_batch_process(apgcu_batch_t b, int npairs, const apgcu_pair_t* pairs, int device_buffers);
-/* Options (results never change): "graphs" 0/1, "batched_sgm" 0/1, "autotune" 0/1,
- * "sgm_lanes" 0/16/32 (0 = autotuned), "max_blocks_per_sm" -1 (autotuned) / 0 (occupancy) / N,
+/* Options (results never change): "graphs" 0/1, "batched_sgm" 0/1, "unified_sgm" 0/1 (one SGM
+ * launch per phase over all buckets, default 1), "autotune" 0/1, "sgm_lanes" 0/16/32 (0 =
+ * autotuned; 16 runs per bucket), "max_blocks_per_sm" -1 (autotuned) / 0 (occupancy) / N,
  * "cost_tile" 0 (autotuned) / 64 / 128 / 256. */
 APGCU_API int apgcu_batch_set_option(apgcu_batch_t b, const char* key, int value);
 APGCU_API size_t apgcu_batch_allocated_bytes(apgcu_batch_t b);

@@ -55,12 +55,27 @@ def test_batch_equals_single_pairs_and_replays(apg, mode):
     b.close()
 
 
-@pytest.mark.parametrize("opts", [{"graphs": 0}, {"batched_sgm": 0}, {"sgm_lanes": 16},
+@pytest.mark.parametrize("opts", [{"graphs": 0}, {"batched_sgm": 0}, {"sgm_lanes": 16}, {"unified_sgm": 0},
+                                  {"unified_sgm": 0, "graphs": 0},
                                   {"max_blocks_per_sm": 1, "autotune": 0}, {"cost_tile": 256}, {"cost_tile": 64}])
 def test_batch_options_change_no_result(apg, opts):
     pairs = _pairs(300, mix=[(160, 96, 64, 2), (200, 120, 128, 2)])
     b = apg.Batch(apg.config_from_mode(1, 128), **opts)
     _check(b.process(pairs), _single(apg, 1, pairs))
+    b.close()
+
+
+@pytest.mark.parametrize("mode", [1, 0])
+def test_batch_one_sgm_launch_over_all_ranges(apg, mode):
+    """Pairs of every padded range (Dp 64, 128, 192, 256) and four sizes share one persistent SGM
+    launch per phase; calls with another composition (a bucket missing, a bucket with more pairs)
+    build their own plan and graph, and a repeated composition replays its graph."""
+    mix = [(150, 80, 60, 2), (200, 100, 128, 1), (260, 60, 190, 2), (300, 50, 250, 1)]
+    b = apg.Batch(apg.config_from_mode(mode, 128))
+    comps = [(600, mix), (610, mix[1:]), (620, [(150, 80, 60, 3)] + mix[1:]), (630, mix)]
+    for seed, m in comps:
+        pairs = _pairs(seed, mix=m)
+        _check(b.process(pairs), _single(apg, mode, pairs))
     b.close()
 
 
