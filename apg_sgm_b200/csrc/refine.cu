@@ -24,7 +24,6 @@
 // the q-th accepted output at or after its start position P_it, and P_{it+1} follows on the device
 // from the pass's count.  No host work or synchronisation remains per frame.
 #include <algorithm>
-#include <cub/device/device_scan.cuh>
 #include <map>
 #include <mutex>
 #include <random>
@@ -38,7 +37,6 @@ namespace {
 
 constexpr int kBand = 32;
 constexpr int kPublish = 8;      // steps between progress publications
-constexpr int kUpBatch = 16;     // columns of the row above a band read at once
 constexpr int kMaxRejected = 64;  // rejected outputs tabulated per radius (expected: none)
 
 __global__ void refine_flags_kernel(int w, int h, const uint8_t* __restrict__ reliable, const int16_t* __restrict__ rmin,
@@ -49,6 +47,84 @@ __global__ void refine_flags_kernel(int w, int h, const uint8_t* __restrict__ re
         if (i == n) { flags[n] = 0; continue; }
         const int f = (!reliable[i] && rmax[i] > rmin[i] && work[i] >= 0.f) ? 1 : 0;
         flags[fwd ? i : n - 1 - i] = f;
+    }
+}
+
+// Exclusive prefix sum of the flags in place (the draw index of every pixel, and the pass's count
+// at index n): three launches without atomics or waits, so the result does not depend on
+// scheduling.  A tile is kScanThreads x kScanPer consecutive entries.
+constexpr int kScanThreads = 1024, kScanPer = 4, kScanTile = kScanThreads * kScanPer;
+
+// Exclusive prefix of v over the block and the block's total (s_warp: 32 ints).
+__device__ __forceinline__ int block_exclusive(int v, int* s_warp, int* total) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) s_warp[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        int t = lane < (int)(blockDim.x >> 5) ? s_warp[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, t, o);
+            if (lane >= o) t += y;
+        }
+        s_warp[lane] = t;
+    }
+    __syncthreads();
+    *total = s_warp[31];
+    const int before = wid ? s_warp[wid - 1] : 0;
+    __syncthreads();  // s_warp may be reused by the caller
+    return before + x - v;
+}
+
+__global__ void __launch_bounds__(kScanThreads) scan_tile_sums_kernel(const int* __restrict__ in, int n,
+                                                                      int* __restrict__ sums) {
+    __shared__ int s_warp[32];
+    const size_t base = (size_t)blockIdx.x * kScanTile + (size_t)threadIdx.x * kScanPer;
+    int v = 0;
+#pragma unroll
+    for (int k = 0; k < kScanPer; ++k)
+        if (base + k < (size_t)n) v += in[base + k];
+    int total = 0;
+    block_exclusive(v, s_warp, &total);
+    if (threadIdx.x == 0) sums[blockIdx.x] = total;
+}
+
+// One block: the tile sums [0, nt) into exclusive tile offsets, in place.
+__global__ void __launch_bounds__(kScanThreads) scan_tile_offsets_kernel(int* sums, int nt) {
+    __shared__ int s_warp[32];
+    int carry = 0;
+    for (int b = 0; b < nt; b += kScanThreads) {
+        const int i = b + (int)threadIdx.x;
+        const int v = i < nt ? sums[i] : 0;
+        int total = 0;
+        const int ex = block_exclusive(v, s_warp, &total);
+        if (i < nt) sums[i] = carry + ex;
+        carry += total;
+    }
+}
+
+__global__ void __launch_bounds__(kScanThreads) scan_apply_kernel(int* data, int n, const int* __restrict__ offs) {
+    __shared__ int s_warp[32];
+    const size_t base = (size_t)blockIdx.x * kScanTile + (size_t)threadIdx.x * kScanPer;
+    int v[kScanPer];
+    int sum = 0;
+#pragma unroll
+    for (int k = 0; k < kScanPer; ++k) {
+        v[k] = base + k < (size_t)n ? data[base + k] : 0;
+        sum += v[k];
+    }
+    int total = 0;
+    int run = offs[blockIdx.x] + block_exclusive(sum, s_warp, &total);
+#pragma unroll
+    for (int k = 0; k < kScanPer; ++k) {
+        if (base + k < (size_t)n) data[base + k] = run;
+        run += v[k];
     }
 }
 
@@ -207,27 +283,124 @@ __device__ __forceinline__ void cp16(void* dst, const void* src) {
                  : "memory");
 }
 
+// Shared state of one band's two warps.  The compute warp (warp 0) walks the band; the link warp
+// (warp 1) carries every exchange with the other bands, so that no GPU-scope fence or L2 round
+// trip sits in the compute warp's step loop:
+//   * it polls the band above's progress counter and copies the newly final columns of that
+//     band's last row into `up` (a ring of kUpRing columns), then raises `avail`;
+//   * it publishes how far this band's last row is final (`done`, raised by the compute warp at
+//     CTA scope) to this band's progress counter, behind a GPU-scope fence.
+// Causality runs compute warp -> (CTA-scope release / acquire) -> link warp -> (GPU-scope release /
+// acquire) -> the next band's link warp, which is the order the reference's in-place raster scan
+// implies for the row above.
+constexpr int kUpRing = 128;
+struct BandLink {
+    float up[kUpRing];  // row above the band: column c at up[c & (kUpRing - 1)]
+    int avail;          // columns [0, avail) of the row above are in `up` (link warp)
+    int used;           // columns [0, used) of `up` are no longer read (compute warp)
+    int done;           // columns [0, done) of the band's last row are final in `work` (compute warp)
+    int abort;          // the link warp gave up waiting (or saw the error word): the compute warp stops
+};
+
+// The link warp of band `band` (see BandLink).  Every wait is bounded: after spin_limit polls in
+// which nothing moved it sets the error word and `abort`, and after as many again it leaves.
+__device__ void band_link(BandLink* s_link, int band, int w, int h, int fwd, const float* work, int* progress,
+                          int* err, int spin_limit) {
+    const int lane = threadIdx.x & 31;
+    volatile BandLink* L = s_link;
+    volatile int* vprog = progress;
+    const int xs = fwd ? 1 : -1, xb = fwd ? 0 : w - 1;
+    const int y_above = band > 0 ? (fwd ? band * kBand - 1 : h - band * kBand) : 0;
+    const float* above = work + (size_t)y_above * w;
+    int fetched = band > 0 ? 0 : w;  // columns of the row above copied into the ring
+    int published = 0;
+    int idle = 0;
+    bool gave_up = false;
+    for (;;) {
+        bool moved = false;
+        // this band's last row, as far as the compute warp has released it
+        const int done = L->done;
+        if (done > published) {
+            if (lane == 0) {
+                fence_acq_rel();
+                vprog[band] = done;
+            }
+            published = done;
+            moved = true;
+        }
+        if (published >= w) break;
+        // the row above, as far as the band above has published it and the ring has room
+        if (fetched < w && !gave_up) {
+            int prog = 0;
+            if (lane == 0) prog = vprog[band - 1];
+            prog = __shfl_sync(0xffffffffu, prog, 0);
+            const int upto = min(min(prog, L->used + kUpRing), w);
+            if (upto > fetched) {
+                if (lane == 0) fence_acq_rel();
+                __syncwarp();
+                for (int col = fetched + lane; col < upto; col += 32)
+                    s_link->up[col & (kUpRing - 1)] = __ldcg(above + (xb + xs * col));
+                __syncwarp();
+                if (lane == 0) {
+                    __threadfence_block();
+                    L->avail = upto;
+                }
+                fetched = upto;
+                moved = true;
+            }
+        }
+        if (moved) {
+            idle = 0;
+            continue;
+        }
+        ++idle;
+        if (!gave_up && (idle > spin_limit || *(volatile int*)err)) {
+            if (lane == 0) {
+                atomicExch(err, 1);
+                L->abort = 1;
+            }
+            gave_up = true;
+            idle = 0;
+        } else if (gave_up && idle > spin_limit) {
+            break;  // the compute warp did not finish either: leave (the frame is already failed)
+        }
+        __nanosleep(64);
+    }
+}
+
 // WIN: each lane's right-image window ([x - dmax + 1, x - d0] of its row, sliding one pixel per
 // step) lives in shared memory, a ring of wmask + 1 records per lane (a power of two holding the
 // window plus the kRing steps copied ahead); every step copies the entering pixel with the step's
 // record, so the candidates' right pixels are shared-memory loads.  Without WIN they are global
-// loads kept warm in L1 by prefetches.
+// loads kept warm in L1 by prefetches.  Two warps per block: warp 0 computes, warp 1 links the
+// band to its neighbours (band_link).
 template <bool C64, bool WIN>
-__global__ void __launch_bounds__(32) refine_band_kernel(CostCtx c, int fwd, const RStep* __restrict__ steps,
+__global__ void __launch_bounds__(64) refine_band_kernel(CostCtx c, int fwd, const RStep* __restrict__ steps,
                                                          const RPack<C64>* __restrict__ lp,
                                                          const RPack<C64>* __restrict__ rp, float* work,
                                                          int* progress, int* err, int spin_limit, int wmask) {
     __shared__ float s_lut[kLutSize];
     __shared__ __align__(16) RStep s_ring[kRing][32];
     __shared__ __align__(16) RPack<C64> s_lpk[kRing][32];
-    const int lane = threadIdx.x;
-    for (int i = lane; i < kLutSize; i += 32) s_lut[i] = c.lut[i];
-    __syncwarp();
+    __shared__ BandLink s_link;
+    for (int i = threadIdx.x; i < kLutSize; i += blockDim.x) s_lut[i] = c.lut[i];
+    if (threadIdx.x == 0) {
+        s_link.avail = 0;
+        s_link.used = 0;
+        s_link.done = 0;
+        s_link.abort = 0;
+    }
+    __syncthreads();
     const int band = blockIdx.x;
     const int w = c.w, h = c.h;
+    if (threadIdx.x >= 32) {
+        band_link(&s_link, band, w, h, fwd, work, progress, err, spin_limit);
+        return;
+    }
+    volatile BandLink* link = &s_link;
+    const int lane = threadIdx.x;
     const int v = band * kBand + lane;  // pass-order row of this lane
     const bool row_ok = v < h;
-    volatile int* vprog = progress;
     // pass-order column u of this lane's row is image column x = xb + xs * u
     const int xs = fwd ? 1 : -1, xb = fwd ? 0 : w - 1;
     const int yrow = fwd ? v : h - 1 - v;
@@ -289,41 +462,31 @@ __global__ void __launch_bounds__(32) refine_band_kernel(CostCtx c, int fwd, con
     }
     int pe = xb + xs * (kAhead - lane) - eoff;  // entering pixel kAhead steps ahead of step t = 0
     float prev = -1.f;  // value of this lane's previous column (its left neighbour)
-    // values of the row above the band for columns [up_base, up_base + kUpBatch): lane k holds
-    // column up_base + k, read together once the band above has published them
-    int up_base = -kUpBatch;
-    float up_vals = -1.f;
-    const int y_above = band > 0 ? (fwd ? band * kBand - 1 : h - band * kBand) : 0;
+    int avail = band > 0 ? 0 : w;  // columns of the row above known to be in the link's ring
     bool abort = false;
     for (int t = 0; t < w + kBand - 1 && !abort; ++t) {
-        if (band > 0 && t < w && t >= up_base + kUpBatch) {
-            // lane 0 waits until the band above has finished its last row up to column t + kUpBatch
-            int got = 0;
-            if (lane == 0) {
-                const int target = min(t + kUpBatch, w);
+        float up_first = -1.f;  // the row above at column t (lane 0's up neighbour)
+        if (band > 0 && t < w) {
+            if (t >= avail) {
+                // wait until the link warp has the row above at least up to column t
                 int spins = 0;
                 for (;;) {
-                    got = vprog[band - 1];
-                    if (got >= target) break;
-                    if (++spins > spin_limit || *(volatile int*)err) {
-                        atomicExch(err, 1);
-                        got = -1;
+                    avail = link->avail;
+                    if (avail > t) break;
+                    if (link->abort || ++spins > spin_limit) {
+                        abort = true;
                         break;
                     }
-                    __nanosleep(64);
+                    __nanosleep(32);
                 }
+                if (abort) {
+                    if (lane == 0) atomicExch(err, 1);
+                    break;
+                }
+                __threadfence_block();
             }
-            got = __shfl_sync(0xffffffffu, got, 0);
-            if (got < 0) {
-                abort = true;
-                break;
-            }
-            fence_acq_rel();
-            up_base = t;
-            const int col = t + lane;
-            up_vals = (lane < kUpBatch && col < w) ? __ldcg(work + y_above * w + (xb + xs * col)) : -1.f;
+            if (lane == 0) up_first = s_link.up[t & (kUpRing - 1)];
         }
-        const float up_first = __shfl_sync(0xffffffffu, up_vals, (t - up_base) & 31);
         asm volatile("cp.async.wait_group %0;\n" ::"n"(kRing - 1) : "memory");
         if (!WIN && row_ok) prefetch_l1(rrow + min(max(pe, 0), w - 1));
         pe += xs;
@@ -368,18 +531,19 @@ __global__ void __launch_bounds__(32) refine_band_kernel(CostCtx c, int fwd, con
         // the slot just read is refilled only after its record was copied out above
         __syncwarp();
         issue(t + kRing);
-        // publish how far the band's last row is final (lane 31 is at column t - 31)
-        if ((t % kPublish) == kPublish - 1 && lane == kBand - 1) {
-            fence_acq_rel();
-            vprog[band] = max(0, min(t - (kBand - 1) + 1, w));
+        if ((t % kPublish) == kPublish - 1) {
+            // release to the link warp (CTA scope): how far the last row (lane 31, column t - 31)
+            // is final, and that the ring's columns up to t are read
+            __threadfence_block();
+            if (lane == kBand - 1) link->done = max(0, min(t - (kBand - 1) + 1, w));
+            if (lane == 0) link->used = min(t + 1, w);
         }
     }
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     __syncwarp();
-    if (lane == kBand - 1) {
-        fence_acq_rel();
-        vprog[band] = w;  // the whole band is final (or the pass was abandoned: let the next band finish)
-    }
+    __threadfence_block();
+    // the whole band is final (or the pass was abandoned: let the next band finish)
+    if (lane == kBand - 1) link->done = w;
 }
 
 // ---- host: the engine stream, its draw values and rejected indices per radius
@@ -419,11 +583,7 @@ const DrawTable& draw_table_locked(int radius, size_t length) {
 
 }  // namespace
 
-size_t refine_scan_temp_bytes(int n) {
-    size_t bytes = 0;
-    cub::DeviceScan::ExclusiveSum(nullptr, bytes, (int*)nullptr, (int*)nullptr, n + 1);
-    return bytes;
-}
+size_t refine_scan_temp_bytes(int n) { return (size_t)((n + 1 + kScanTile - 1) / kScanTile) * sizeof(int); }
 
 int refine_band_count(int h) { return (h + kBand - 1) / kBand; }
 
@@ -486,10 +646,14 @@ cudaError_t launch_refine_count(const Layout& L, unsigned char* arena, const flo
     refine_flags_kernel<<<blocks, 256, 0, s>>>(L.w, L.h, reinterpret_cast<const uint8_t*>(arena + L.reliable),
                                                 reinterpret_cast<const int16_t*>(arena + L.rmin),
                                                 reinterpret_cast<const int16_t*>(arena + L.rmax), work, fwd, flags);
-    size_t tmp = L.rf_scan_tmp_bytes;
-    cudaError_t e = cub::DeviceScan::ExclusiveSum(arena + L.rf_scan_tmp, tmp, flags, flags, n + 1, s);
-    *launches += 2;
-    if (e != cudaSuccess) return e;
+    // the draw indices: exclusive prefix sum of the n + 1 flags (the last one 0), in place
+    const int m = n + 1;
+    const int nt = (m + kScanTile - 1) / kScanTile;
+    int* sums = reinterpret_cast<int*>(arena + L.rf_scan_tmp);
+    scan_tile_sums_kernel<<<nt, kScanThreads, 0, s>>>(flags, m, sums);
+    scan_tile_offsets_kernel<<<1, kScanThreads, 0, s>>>(sums, nt);
+    scan_apply_kernel<<<nt, kScanThreads, 0, s>>>(flags, m, sums);
+    *launches += 4;
     return cudaGetLastError();
 }
 
@@ -556,7 +720,7 @@ cudaError_t launch_refine_pass(const CostCtx& c, const Layout& L, unsigned char*
             int per_sm = 0, dev = 0, nsm = 0;
             if (cudaGetDevice(&dev) == cudaSuccess &&
                 cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
-                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, wk, kBand, bytes) == cudaSuccess &&
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, wk, 2 * kBand, bytes) == cudaSuccess &&
                 per_sm * nsm >= nbands) {
                 wmask = rs - 1;
                 wbytes = bytes;
@@ -567,7 +731,7 @@ cudaError_t launch_refine_pass(const CostCtx& c, const Layout& L, unsigned char*
     }
     void* args[] = {&cc, &fwd_arg, (void*)&csteps, (void*)&lpk, (void*)&rpk, &work, &progress, &err, &spin_limit,
                     &wmask};
-    e = cudaLaunchCooperativeKernel(kern, dim3(nbands), dim3(kBand), args, wbytes, s);
+    e = cudaLaunchCooperativeKernel(kern, dim3(nbands), dim3(2 * kBand), args, wbytes, s);
     if (e != cudaSuccess) return e;
     ++*launches;
     // start of the next pass, and cleared progress counters
