@@ -39,7 +39,9 @@ namespace apgcu {
 
 namespace {
 
-constexpr int kT2Stride = 33;  // t2 row per |dgray|: popcounts 0..32 of a 32-bit census
+// t2[pop][|dgray|]: one row of 256 per popcount 0..32 of a 32-bit census, so a voxel's index is
+// one byte permute of the popcount and the absolute differences
+constexpr int kT2Rows = 33;
 
 struct RunGeom {
     int txc, ha, nx, nr, roff, rl, nrun, ntx, ntiles;
@@ -71,7 +73,7 @@ RunGeom run_geom(const CostCtx& c, int txc, int ha, bool cross, bool full, bool 
     g.ntiles = g.ntx * c.h;
     const bool stage_g = full || cross;
     size_t o = 0;
-    g.t2 = o; o = a16(o + (full ? 256 * kT2Stride * 4 : 0));
+    g.t2 = o; o = a16(o + (full ? 256 * kT2Rows * 4 : 0));
     g.lgt = o; o = a16(o + (full ? 511 * 4 : 0));
     g.q = o; o = a16(o + (full ? 0 : 65 * 4));
     g.magic = o; o = a16(o + (cross ? (2 * ha + 2) * 4 : 0));
@@ -94,20 +96,49 @@ __device__ __forceinline__ uint32_t pack_g(const uint8_t* gray, const uint8_t* g
     return (uint32_t)gray[i] | ((uint32_t)gx[i] << 8) | ((uint32_t)gy[i] << 16);
 }
 
-// Quantised cost of one (left, right) descriptor pair.
+// Quantised costs of two (left, right) descriptor pairs (disparities 2w and 2w + 1 of one lane),
+// packed low / high: the reference's float steps (src/cost_computer.cpp:247-264), each rounded on
+// its own, two lanes per packed f32x2 instruction.  (int)(v * scale + 0.5f) truncates a value in
+// [0.5, 2^23): adding 2^23 rounded toward zero leaves exactly 2^23 + trunc(v), so the integer is
+// the low mantissa bits; truncation saturates below zero in the reference, and here v >= 0.5.
+__device__ __forceinline__ unsigned long long f2add_rn(unsigned long long a, unsigned long long b) {
+    unsigned long long d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ unsigned long long f2add_rz(unsigned long long a, unsigned long long b) {
+    unsigned long long d;
+    asm("add.rz.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ unsigned long long f2mul_rn(unsigned long long a, unsigned long long b) {
+    unsigned long long d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ unsigned long long f2pack(float lo, float hi) {
+    return (unsigned long long)__float_as_uint(lo) | ((unsigned long long)__float_as_uint(hi) << 32);
+}
+
 template <bool FULL>
-__device__ __forceinline__ uint32_t run_cost(uint32_t lc, uint32_t lg, uint32_t rc, uint32_t rg, const float* s_t2,
-                                             const float* s_lgt, const uint32_t* s_q, float scale, uint32_t cmax) {
-    const int pop = __popc(lc ^ rc);
+__device__ __forceinline__ uint32_t run_cost2(uint32_t lc, uint32_t lg, uint32_t rc0, uint32_t rg0, uint32_t rc1,
+                                              uint32_t rg1, const float* s_t2, const float* s_lgt,
+                                              const uint32_t* s_q, unsigned long long scale2, uint32_t cmax2) {
+    const uint32_t pop0 = __popc(lc ^ rc0), pop1 = __popc(lc ^ rc1);
     if constexpr (!FULL) {
-        return s_q[pop];
+        return __byte_perm(s_q[pop0], s_q[pop1], 0x5410);
     } else {
-        const uint32_t ad = __vabsdiffu4(lg, rg);  // |dgray|, |dgx|, |dgy|
-        const float t = s_t2[(ad & 0xFFu) * kT2Stride + pop];
-        const float v = __fadd_rn(t, s_lgt[__dp4a(ad, 0x00010100u, 0u)]);
-        // truncation saturates below zero, so only the upper clamp remains
-        const uint32_t q = __float2uint_rz(__fadd_rn(__fmul_rn(v, scale), 0.5f));
-        return min(q, cmax);
+        const uint32_t ad0 = __vabsdiffu4(lg, rg0), ad1 = __vabsdiffu4(lg, rg1);  // |dgray|, |dgx|, |dgy|
+        // t2[pop][|dgray|] at pop * 256 + |dgray| (pop < 256, so its second byte is zero)
+        const float t0 = s_t2[__byte_perm(ad0, pop0, 0x5540)];
+        const float t1 = s_t2[__byte_perm(ad1, pop1, 0x5540)];
+        const float g0 = s_lgt[__dp4a(ad0, 0x00010100u, 0u)];
+        const float g1 = s_lgt[__dp4a(ad1, 0x00010100u, 0u)];
+        const unsigned long long v = f2add_rn(f2pack(t0, t1), f2pack(g0, g1));
+        const unsigned long long u = f2add_rn(f2mul_rn(v, scale2), 0x3F0000003F000000ull);  // + 0.5f
+        const unsigned long long q = f2add_rz(u, 0x4B0000004B000000ull);                    // + 2^23, toward 0
+        // the low 16 bits of each lane's mantissa are its integer (< 2^16 by the host's cost_max check)
+        return __vminu2(__byte_perm((uint32_t)q, (uint32_t)(q >> 32), 0x5410), cmax2);
     }
 }
 
@@ -151,8 +182,8 @@ __device__ __forceinline__ void run_steps(const CostCtx& c, const RunGeom& g, in
     constexpr int W2 = 32 * WPL;
     const int lane = threadIdx.x & 31;
     const int dbase = P * lane;  // first disparity index of this lane
-    const float scale = c.scale;
-    const uint32_t cmax = (uint32_t)c.cost_max;
+    const unsigned long long scale2 = f2pack(c.scale, c.scale);
+    const uint32_t cmax2 = (uint32_t)c.cost_max * 0x00010001u;
     // lanes wholly past the range load at the last in-bounds even base (dl + P <= D + roff keeps
     // every window entry inside the staged row; even keeps the 8-byte loads aligned) and are
     // masked; a lane with any disparity below D has dbase <= D - 1 < D + roff - P, so keeps its own
@@ -196,8 +227,8 @@ __device__ __forceinline__ void run_steps(const CostCtx& c, const RunGeom& g, in
             }
             wc[0] = NC[s];
             wg[0] = NG[s];
-            uint32_t q[P];
-            bool v[P];
+            uint32_t qp[WPL];  // quantised costs of disparities 2w | 2w + 1 << 16
+            uint32_t vm[WPL];  // their validity: 0xFFFF per valid half
             uint32_t rmask = 0xFFFFu;  // this lane's disparities inside the left pixel's range
             if (PRIOR) {
                 const uint32_t rg = s_rng[xi + s];
@@ -207,16 +238,34 @@ __device__ __forceinline__ void run_steps(const CostCtx& c, const RunGeom& g, in
                 rmask = ((1u << a1) - 1u) & ~((1u << a0) - 1u);
             }
 #pragma unroll
-            for (int j = 0; j < P; ++j) {
-                q[j] = run_cost<FULL>(L[s], LG[s], wc[j], wg[j], s_t2, s_lgt, s_q, scale, cmax);
-                v[j] = true;
-                if (!V) {
-                    const int di = dbase + j, xr = x - c.d0 - di;
-                    v[j] = x >= 0 && x < c.w && di < c.D && xr >= 0 && xr < c.w;
+            for (int w = 0; w < WPL; ++w) {
+                qp[w] = run_cost2<FULL>(L[s], LG[s], wc[2 * w], wg[2 * w], wc[2 * w + 1], wg[2 * w + 1], s_t2, s_lgt,
+                                        s_q, scale2, cmax2);
+                vm[w] = 0xFFFFFFFFu;
+                if (!V || PRIOR) {
+                    uint32_t m = 0;
+#pragma unroll
+                    for (int hs = 0; hs < 2; ++hs) {
+                        const int j = 2 * w + hs;
+                        bool ok = true;
+                        if (!V) {
+                            const int di = dbase + j, xr = x - c.d0 - di;
+                            ok = x >= 0 && x < c.w && di < c.D && xr >= 0 && xr < c.w;
+                        }
+                        if (PRIOR) ok = ok && ((rmask >> j) & 1u);
+                        if (ok) m |= 0xFFFFu << (16 * hs);
+                    }
+                    vm[w] = m;
                 }
-                if (PRIOR) v[j] = v[j] && ((rmask >> j) & 1u);
-                const uint32_t key = v[j] ? ((q[j] << 16) | (uint32_t)(dbase + j)) : kInvalidWord;
-                acc[j] = min(acc[j], key);
+#pragma unroll
+                for (int hs = 0; hs < 2; ++hs) {
+                    const int j = 2 * w + hs;
+                    // key (cost << 16 | disparity index), or the invalid word
+                    const uint32_t key = hs == 0 ? ((qp[w] << 16) | (uint32_t)(dbase + j))
+                                                 : ((qp[w] & 0xFFFF0000u) | (uint32_t)(dbase + j));
+                    const bool ok = (V && !PRIOR) || ((vm[w] >> (16 * hs)) & 1u);
+                    acc[j] = min(acc[j], ok ? key : kInvalidWord);
+                }
             }
             // the oldest minimum moves one lane up; lane 31's is complete for this run
             const uint32_t out = acc[P - 1];
@@ -227,12 +276,11 @@ __device__ __forceinline__ void run_steps(const CostCtx& c, const RunGeom& g, in
             acc[0] = lane ? in : kInvalidWord;
             if (CROSS) {
 #pragma unroll
-                for (int w = 0; w < WPL; ++w)
-                    pre[w] += (v[2 * w] ? q[2 * w] : 0u) | ((v[2 * w + 1] ? q[2 * w + 1] : 0u) << 16);
+                for (int w = 0; w < WPL; ++w) pre[w] += qp[w] & vm[w];
                 store_words<WPL>(pp + s * W2, pre);
                 if (PRIOR) {
 #pragma unroll
-                    for (int w = 0; w < WPL; ++w) cnt[w] += (v[2 * w] ? 1u : 0u) + (v[2 * w + 1] ? 0x100u : 0u);
+                    for (int w = 0; w < WPL; ++w) cnt[w] += __byte_perm(vm[w], 0u, 0x4420) & 0x0101u;  // (valid low) | (valid high) << 8
                     store_counts<WPL>(cp + s * W2, cnt);
                 }
             } else if (STORE) {
@@ -240,9 +288,7 @@ __device__ __forceinline__ void run_steps(const CostCtx& c, const RunGeom& g, in
                 if (V || (xi + s < g.txc && x < c.w)) {
                     uint32_t wd[WPL];
 #pragma unroll
-                    for (int w = 0; w < WPL; ++w)
-                        wd[w] = (v[2 * w] ? q[2 * w] : kInvalidCost) |
-                                ((v[2 * w + 1] ? q[2 * w + 1] : kInvalidCost) << 16);
+                    for (int w = 0; w < WPL; ++w) wd[w] = qp[w] | ~vm[w];  // invalid halves: 0xFFFF
                     store_words<WPL>(vp + (size_t)s * W2, wd);
                 }
             }
@@ -342,8 +388,8 @@ __global__ void __launch_bounds__(CROSS ? 512 : 256, CROSS ? (WPL > 2 ? 1 : 2) :
     uint32_t* s_em = reinterpret_cast<uint32_t*>(smem + g.emit) + run * g.rl;
 
     if (FULL) {
-        for (int i = tid; i < 256 * kT2Stride; i += nt) {
-            const int ad = i / kT2Stride, pop = i - ad * kT2Stride;
+        for (int i = tid; i < 256 * kT2Rows; i += nt) {
+            const int pop = i >> 8, ad = i & 255;
             const float lc = c.lut[kLutCensus + pop];
             s_t2[i] = c.use_ad ? __fadd_rn(lc, c.lut[kLutAd + ad]) : lc;
         }

@@ -31,7 +31,11 @@
 //     one disparity per step, so a horizontal sweep keeps them in a register ring and takes one
 //     new descriptor per step from the neighbouring lane (shuffle) or, at the group edge, from
 //     memory;
-//   * every load (costs or descriptors, path sums, gray) runs PF steps ahead in a register ring;
+//   * loads run PF steps ahead of use: the census-fed sweeps keep them in a register ring; the
+//     volume-fed sweeps (every mode's default) stage costs and partial sums through a per-warp
+//     shared-memory ring filled by cp.async, one commit group per step (run_chain_vol);
+//   * the volume-fed last sweep runs on two warps per chain: one for the recurrence, one for the
+//     partial sums and the WTA (sgm_last_split_kernel);
 //   * the last sweep adds its L to S, keeps the final sum in registers and runs the reference WTA
 //     (first minimum, second minimum outside |d-best| <= 1, legacy parabola) with two group
 //     min-reductions, so the final sum never returns to HBM.

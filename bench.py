@@ -684,14 +684,18 @@ def run_b200(args, wl):
     py_value = vox * npy / (time.perf_counter() - t0)
     clocks = sampler.stop()
 
-    # dominant kernel and its roofline
+    # dominant kernel and its roofline: the largest share of device time among the kernels with a
+    # byte model (the HBM-bound ones); a latency-bound stage that outweighs it (the HighQuality
+    # refiner's wavefront) is described beside it by its own model
     peak, peak_kind = _peaks()
     totals = {k: sum(v) for k, v in per_kernel.items() if k != "copy"}
-    top = max(totals, key=totals.get)
+    prof_total = sum(totals.values())
+    modelled = {k: v for k, v in totals.items()
+                if _algorithmic_bytes(k, w, h, D, volume_source=True, npath=cfg.paths) > 0}
+    top = max(modelled or totals, key=(modelled or totals).get)
     top_avg_ms = statistics.mean(per_kernel[top])
     alg = _algorithmic_bytes(top, w, h, D, volume_source=True, npath=cfg.paths)  # every mode's sweeps read a volume
     achieved = alg / (top_avg_ms / 1000.0) / 1e9
-    prof_total = sum(totals.values())
     roofline = {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_kind": peak_kind,
                 "traffic": _profile_traffic(top, label), "algorithmic_bytes_per_launch": alg,
@@ -707,6 +711,25 @@ def run_b200(args, wl):
     if top in ("cost", "cost+crossH"):
         roofline["note"] = ("issue-bound: integer and LUT work per voxel (ncu issue active ~73%, DRAM ~8%); "
                             "the HBM fraction of its 2 B/voxel output is shown for reference")
+    if "refine" in per_kernel:
+        # the refiner: passes x a wavefront over the frame; a pixel's update needs its left and up
+        # neighbours' values of the same pass, so a pass takes at least w + h - 1 dependent steps.
+        # Work unit per pixel and pass: its 32-byte record, its packed left pixel (8 B), two packed
+        # right-window pixels (16 B) and its value (4 B) = 60 B
+        ref_ms = statistics.mean(per_kernel["refine"])
+        passes = max(1, int(cfg.refine_iterations))
+        steps_min = w + h - 1
+        ref_bytes = 60.0 * w * h * passes
+        roofline["latency_bound"] = {
+            "kernel": "refine (HighQuality refiner: prep, band wavefront, draw indices)",
+            "ms_per_frame": ref_ms, "share": round(totals["refine"] / prof_total, 4), "passes": passes,
+            "min_dependent_steps_per_pass": steps_min,
+            "ns_per_dependent_step": ref_ms * 1e6 / passes / steps_min,
+            "algorithmic_bytes": ref_bytes,
+            "hbm_frac": round(ref_bytes / (ref_ms / 1000.0) / 1e9 / peak, 4),
+            "model": "each pass is a wavefront of at least w + h - 1 dependent steps (a pixel needs its "
+                     "left and up neighbours of the same pass); time = passes x steps x step latency, so "
+                     "ns_per_dependent_step is the figure to lower, the HBM fraction stays small by design"}
 
     out = {
         "metric": metric_name(mode, w, h, D, over), "value": value, "unit": "voxels/s", "n_gpus": world, "steps": args.steps,
