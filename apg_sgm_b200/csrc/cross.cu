@@ -207,124 +207,6 @@ __global__ void __launch_bounds__(128) cross_v_default_kernel(int w, int h, int 
     }
 }
 
-// The default-range vertical pass with two words (four disparities) per thread: the same prefix
-// ring, batched loads and chunked queries as cross_v_default_kernel, with the ring slot indexing,
-// the arm and divisor loads and the loop control of a row shared by twice the voxels (8-byte
-// loads, ring entries and stores).  KB rows per load batch keep a thread's bytes in flight.
-template <int RS, int KB>
-__global__ void __launch_bounds__(128) cross_v_pair_kernel(int w, int h, int d0, int D, int Dp, int lmax, int tau,
-                                                           int cols, const uint8_t* __restrict__ gray,
-                                                           const uint32_t* __restrict__ tin,
-                                                           uint32_t* __restrict__ cout,
-                                                           const uint32_t* __restrict__ magic) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    const int WP = Dp / 4;  // word pairs per pixel
-    const int nthr = WP * cols;
-    uint2* ring = reinterpret_cast<uint2*>(smem);                              // [RS][nthr]
-    uint32_t* s_magic = reinterpret_cast<uint32_t*>(ring + (size_t)RS * nthr);  // [2*lmax+2]
-    uint8_t* s_gray = reinterpret_cast<uint8_t*>(s_magic + 2 * lmax + 2);     // [cols][kSeg + 2*lmax]
-    uint8_t* armU = s_gray + cols * (kSeg + 2 * lmax);                         // [cols][kSeg]
-    uint8_t* armD = armU + cols * kSeg;
-    const int xb = blockIdx.x * cols;
-    const int y0 = blockIdx.y * kSeg;
-    const int y1 = min(h, y0 + kSeg);
-    const int tid = threadIdx.x;
-    const int gs = kSeg + 2 * lmax;  // staged gray rows [y0 - lmax, y0 + kSeg + lmax)
-
-    for (int i = tid; i < 2 * lmax + 2; i += blockDim.x) s_magic[i] = magic[i];
-    for (int i = tid; i < cols * gs; i += blockDim.x) {
-        const int r = i / cols, ci = i - r * cols;
-        const int yy = y0 - lmax + r, x = xb + ci;
-        s_gray[ci * gs + r] = (x < w && yy >= 0 && yy < h) ? gray[yy * w + x] : 0;
-    }
-    __syncthreads();
-    for (int i = tid; i < cols * kSeg; i += blockDim.x) {
-        const int ci = i / kSeg, r = i - ci * kSeg;
-        const int yy = y0 + r, x = xb + ci;
-        int u = 0, v = 0;
-        if (x < w && yy < h) {
-            const uint8_t* g = s_gray + ci * gs + lmax + r;  // g[0] = gray(x, yy)
-            const int c0 = g[0];
-            while (u < lmax && yy - u - 1 >= 0 && abs((int)g[-u - 1] - c0) <= tau) ++u;
-            while (v < lmax && yy + v + 1 < h && abs((int)g[v + 1] - c0) <= tau) ++v;
-        }
-        armU[i] = (uint8_t)u;
-        armD[i] = (uint8_t)v;
-    }
-    __syncthreads();
-    if (tid >= nthr) return;
-    const int ci = tid / WP, k = tid - ci * WP;  // words 2k, 2k + 1: disparity indices 4k .. 4k + 3
-    const int x = xb + ci;
-    if (x >= w) return;
-    // output halves that can be valid: d < dmax and d <= x
-    bool lane_ok[4];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) lane_ok[q] = (4 * k + q < D) && (d0 + 4 * k + q <= x);
-
-    const int ystart = max(0, y0 - lmax);
-    const int yend = min(h, y1 + lmax);  // rows read: [ystart, yend)
-    // ring slot of prefix P(r) (sum over rows [ystart, r]) is (r - ystart + 1) & (RS - 1); slot 0 = P(ystart - 1) = 0
-    ring[tid] = make_uint2(0u, 0u);
-    const size_t rowstride = (size_t)w * WP;  // in word pairs
-    const uint2* src = reinterpret_cast<const uint2*>(tin) + ((size_t)ystart * w + x) * WP + k;
-    uint2 cur[KB], nxt[KB];
-#pragma unroll
-    for (int i = 0; i < KB; ++i) cur[i] = ystart + i < yend ? __ldcs(src + i * rowstride) : make_uint2(0u, 0u);
-#pragma unroll
-    for (int i = 0; i < KB; ++i)
-        nxt[i] = ystart + KB + i < yend ? __ldcs(src + (KB + i) * rowstride) : make_uint2(0u, 0u);
-    int pushed = ystart;  // next row to add to the ring
-    uint2 ps = make_uint2(0u, 0u);
-    uint2* dst = reinterpret_cast<uint2*>(cout) + ((size_t)y0 * w + x) * WP + k;
-    for (int yb = y0; yb < y1; yb += kQ) {
-        // prefixes up to the last window of the chunk's rows, then kQ independent rows
-        const int need = min(h, min(yb + kQ, y1) + lmax);
-        while (pushed < need) {
-            // add the buffered batch (rows [pushed, pushed + KB)) and load the one after next
-#pragma unroll
-            for (int i = 0; i < KB; ++i) {
-                if (pushed + i < yend) {
-                    ps.x = __vadd2(ps.x, cur[i].x);
-                    ps.y = __vadd2(ps.y, cur[i].y);
-                    ring[((pushed + i - ystart + 1) & (RS - 1)) * nthr + tid] = ps;
-                }
-            }
-            pushed += KB;
-#pragma unroll
-            for (int i = 0; i < KB; ++i) cur[i] = nxt[i];
-            const int base = pushed + KB;
-#pragma unroll
-            for (int i = 0; i < KB; ++i)
-                nxt[i] = base + i < yend ? __ldcs(src + (size_t)(base + i - ystart) * rowstride) : make_uint2(0u, 0u);
-        }
-#pragma unroll
-        for (int i = 0; i < kQ; ++i) {
-            const int y = yb + i;
-            if (y >= y1) break;
-            const int ai = ci * kSeg + (y - y0);
-            const int a = y - armU[ai], b = y + armD[ai];  // inclusive window
-            const uint2 pb = ring[((b - ystart + 1) & (RS - 1)) * nthr + tid];
-            const uint2 pa = ring[((a - ystart) & (RS - 1)) * nthr + tid];
-            const uint32_t sum[2] = {__vsub2(pb.x, pa.x), __vsub2(pb.y, pa.y)};
-            const int len = b - a + 1;
-            const uint32_t mg = s_magic[len];
-            uint32_t word[2];
-#pragma unroll
-            for (int wd = 0; wd < 2; ++wd) {
-                word[wd] = 0;
-#pragma unroll
-                for (int hs = 0; hs < 2; ++hs) {
-                    const uint32_t sh = (sum[wd] >> (16 * hs)) & 0xFFFFu;
-                    const uint32_t q = lane_ok[2 * wd + hs] ? div_by_magic(sh, (uint32_t)len, mg) : kInvalidCost;
-                    word[wd] |= q << (16 * hs);
-                }
-            }
-            __stcs(dst + (size_t)i * rowstride, make_uint2(word[0], word[1]));
-        }
-        dst += (size_t)kQ * rowstride;
-    }
-}
-
 // Vertical pass for any ranges (per-pixel ranges of the prior, negative disparities, wide
 // ranges): the batched, power-of-two ring form above plus a prefix of valid counts.  Sums are plain
 // 32-bit running sums of the packed words with invalid halves zeroed, and counts are 16-bit running
@@ -519,31 +401,6 @@ cudaError_t launch_cross_v(int w, int h, int d0, int D, int Dp, int lmax, int ta
     // yb + kQ + lmax + kB - 2 are live, so a ring of 2*lmax + kB + kQ + 2 slots never overwrites
     // one before its last read
     const int span = 2 * lmax + kB + kQ + 2;
-    if (default_ranges && d0 >= 0 && Dp % 4 == 0) {
-        // two words per thread (cross_v_pair_kernel): 8-row load batches, a ring above the live rows
-        constexpr int KBP = 8;
-        const int WP = Dp / 4;
-        const int pcols = WP >= 128 ? 1 : 128 / WP;
-        const int pthr = WP * pcols;
-        const int pspan = 2 * lmax + KBP + kQ + 2;
-        const size_t extra = (size_t)(2 * lmax + 2) * 4 + (size_t)pcols * (kSeg + 2 * lmax) + (size_t)pcols * kSeg * 2;
-        auto go = [&](auto rs_tag) -> cudaError_t {
-            constexpr int RS = decltype(rs_tag)::value;
-            const size_t smem = (size_t)RS * pthr * 8 + extra;
-            auto kern = cross_v_pair_kernel<RS, KBP>;
-            {
-                const cudaError_t e = allow_dynamic_smem(kern, smem);
-                if (e != cudaSuccess) return e;
-            }
-            dim3 grid((w + pcols - 1) / pcols, (h + kSeg - 1) / kSeg);
-            kern<<<grid, 128, smem, s>>>(w, h, d0, D, Dp, lmax, tau, pcols, gray, tin, cout, magic);
-            return cudaGetLastError();
-        };
-        if (pthr <= 128) {
-            if (pspan <= 64) return go(std::integral_constant<int, 64>());
-            if (pspan <= 128) return go(std::integral_constant<int, 128>());
-        }
-    }
     if (default_ranges && d0 >= 0 && nthr <= 128) {
         const size_t extra = (size_t)(2 * lmax + 2) * 4 + (size_t)cols * (kSeg + 2 * lmax) + (size_t)cols * kSeg * 2;
         auto go = [&](auto rs_tag) -> cudaError_t {
