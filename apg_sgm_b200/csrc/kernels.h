@@ -71,7 +71,7 @@ struct SgmLaunch {
     apg_subpixel_telemetry_t* sp_tel = nullptr;  // telemetry counters (ExperimentalSubpixelScope), or none
     int store_final;  // last sweep: also write the final sum into in[0] (stage dumps)
     int lanes;        // lanes per scanline chain (8, 16, 32; 0 = default for Dp)
-    int split = 0;    // volume-fed last sweep over two warps per chain: 0 = where it pays (Dp <= 128),
+    int split = 0;    // volume-fed last sweep over two warps per chain: 0 = where it pays (Dp 64),
                       // 1 = never, 2 = always (32 lanes per chain only)
 };
 // First phase: ndir directions in one launch, direction i writing its path values to out[i].

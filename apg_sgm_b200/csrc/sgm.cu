@@ -740,8 +740,11 @@ __device__ __forceinline__ void run_chain_vol(const SgmArgs& a, const uint32_t* 
 // the other has passed it.
 constexpr int kSplitSlots = 2;
 constexpr int kSplitSeg = 8;  // steps per segment (divides the 32-step WTA and P2 blocks)
-constexpr int kBarFull = 1;   // named barriers 1, 2: segment written
-constexpr int kBarFree = 3;   // named barriers 3, 4: segment read
+// Barrier ids are immediates (a register id makes the compiler reserve all sixteen of a block's
+// barriers, which capped the SM at four of these blocks); the kernel has no __syncthreads, so ids
+// 0..3 are free.
+constexpr int kBarFull = 0;   // named barriers 0, 1: segment written
+constexpr int kBarFree = 2;   // named barriers 2, 3: segment read
 
 template <int K, int NB, int PFA, int PFB>
 struct SplitSmem {
@@ -753,8 +756,21 @@ struct SplitSmem {
     static constexpr int words = cring + lring + pring + wta;
 };
 
-__device__ __forceinline__ void nbar_sync64(int id) { asm volatile("bar.sync %0, 64;\n" ::"r"(id) : "memory"); }
-__device__ __forceinline__ void nbar_arrive64(int id) { asm volatile("bar.arrive %0, 64;\n" ::"r"(id) : "memory"); }
+template <int ID>
+__device__ __forceinline__ void nbar_sync64() { asm volatile("bar.sync %0, 64;\n" ::"n"(ID) : "memory"); }
+template <int ID>
+__device__ __forceinline__ void nbar_arrive64() { asm volatile("bar.arrive %0, 64;\n" ::"n"(ID) : "memory"); }
+// barrier `base + slot` for a slot of kSplitSlots = 2
+template <int BASE>
+__device__ __forceinline__ void nbar_sync_slot(int slot) {
+    if (slot) nbar_sync64<BASE + 1>();
+    else nbar_sync64<BASE>();
+}
+template <int BASE>
+__device__ __forceinline__ void nbar_arrive_slot(int slot) {
+    if (slot) nbar_arrive64<BASE + 1>();
+    else nbar_arrive64<BASE>();
+}
 
 template <int K, int NB, int PFA, int PFB>
 __global__ void __launch_bounds__(64) sgm_last_split_kernel(SgmArgs a, DirTable tab) {
@@ -796,7 +812,7 @@ __global__ void __launch_bounds__(64) sgm_last_split_kernel(SgmArgs a, DirTable 
         int gnext = lane < len ? (int)__ldg(a.gray + p0 + lane * step) : 0;
         int gcarry = 0, p2v = 0;
         for (int seg = 0; seg < nseg; ++seg) {
-            if (seg >= kSplitSlots) nbar_sync64(kBarFree + seg % kSplitSlots);
+            if (seg >= kSplitSlots) nbar_sync_slot<kBarFree>(seg % kSplitSlots);
             uint32_t* lslot = s_l + (seg % kSplitSlots) * SM::lseg;
 #pragma unroll
             for (int v = 0; v < kSplitSeg; ++v) {
@@ -861,7 +877,7 @@ __global__ void __launch_bounds__(64) sgm_last_split_kernel(SgmArgs a, DirTable 
                 }
             }
             __threadfence_block();
-            nbar_arrive64(kBarFull + seg % kSplitSlots);
+            nbar_arrive_slot<kBarFull>(seg % kSplitSlots);
         }
         cp_wait<0>();
     } else {
@@ -882,7 +898,7 @@ __global__ void __launch_bounds__(64) sgm_last_split_kernel(SgmArgs a, DirTable 
             ioff += dstep;
         }
         for (int seg = 0; seg < nseg; ++seg) {
-            nbar_sync64(kBarFull + seg % kSplitSlots);
+            nbar_sync_slot<kBarFull>(seg % kSplitSlots);
             const uint32_t* lslot = s_l + (seg % kSplitSlots) * SM::lseg;
 #pragma unroll
             for (int v = 0; v < kSplitSeg; ++v) {
@@ -922,7 +938,7 @@ __global__ void __launch_bounds__(64) sgm_last_split_kernel(SgmArgs a, DirTable 
                 }
             }
             __threadfence_block();
-            if (seg + kSplitSlots < nseg) nbar_arrive64(kBarFree + seg % kSplitSlots);
+            if (seg + kSplitSlots < nseg) nbar_arrive_slot<kBarFree>(seg % kSplitSlots);
         }
         cp_wait<0>();
     }
@@ -1084,11 +1100,13 @@ cudaError_t launch_first_tk(const SgmArgs& a, DirTable tab, bool census, cudaStr
     return cudaGetLastError();
 }
 
-// Whether the volume-fed last sweep runs split over two warps per chain: on request, else for up to
-// 128 padded disparities (wider ranges need more shared memory per chain than the split saves).
+// Whether the volume-fed last sweep runs split over two warps per chain: on request, else for 64
+// padded disparities.  Measured at 20 steps (one B200, last-sweep launch): 640x480 D64 0.111 vs
+// 0.142 ms split / one warp; 1280x720 D128 0.275 vs 0.272; 1242x375 D192 0.401 vs 0.201 (wider
+// ranges need more shared memory per chain than the split saves).
 bool use_split(int T, int K, bool census, int split) {
     if (T != 32 || census || split == 1) return false;
-    return split == 2 || K <= 2;
+    return split == 2 || K == 1;
 }
 
 template <int K, int NB>
@@ -1097,8 +1115,13 @@ cudaError_t launch_last_split(const SgmArgs& a, const DirTable& tab, cudaStream_
     constexpr int PFB = K <= 2 ? 8 : 4;
     const size_t smem = (size_t)SplitSmem<K, NB, PFA, PFB>::words * 4;
     auto kern = sgm_last_split_kernel<K, NB, PFA, PFB>;
-    const cudaError_t e = allow_dynamic_smem(kern, smem);
+    cudaError_t e = allow_dynamic_smem(kern, smem);
     if (e != cudaSuccess) return e;
+    // as many chains per SM as shared memory holds: ask for the largest shared-memory carveout
+    // (a hint the driver otherwise sizes to other limits), once per process
+    static const cudaError_t carve =
+        cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+    if (carve != cudaSuccess) cudaGetLastError();
     kern<<<tab.nscan[0], 64, smem, st>>>(a, tab);
     return cudaGetLastError();
 }

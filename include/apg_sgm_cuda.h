@@ -63,7 +63,7 @@ APGCU_API int apgcu_engine_set_debug(apgcu_engine_t e, int flags);
 /* Kernel tuning knobs (results never change, only speed):
  *   "sgm_lanes": lanes per SGM scanline chain, 8 / 16 / 32 (0 = default, 32);
  *   "sgm_split": the volume-fed last sweep with its recurrence and its sums / WTA on two warps per
- *                chain: 0 = for up to 128 padded disparities (default), 1 = never, 2 = always;
+ *                chain: 0 = for 64 padded disparities (default), 1 = never, 2 = always;
  *   "cost_tile": columns per block of the cost kernel, 64 / 128 / 256 (0 = default for the range);
  *   "fast_fused": 1 = census-only Fast mode recomputes its costs inside the SGM sweeps and stores no
  *                 cost volume (less memory, slower); 0 = store the volume once (default);
