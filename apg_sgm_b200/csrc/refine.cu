@@ -200,22 +200,6 @@ __device__ __forceinline__ float packed_cost(const CostCtx& c, const float* lut,
     return v;
 }
 
-// The same cost with the census and AD terms from one table t2[pop * 256 + |dgray|] holding the
-// reference's first add (census + AD, or census alone without AD), then + gradient: one dependent
-// shared-memory load and add fewer on the band wavefront's step.
-template <bool C64>
-__device__ __forceinline__ float band_cost(const CostCtx& c, const float* t2, const float* lut, const RPack<C64>& l,
-                                           const RPack<C64>& r) {
-    int pop;
-    if constexpr (C64) pop = __popcll(l.c ^ r.c);
-    else pop = __popc(l.c ^ r.c);
-    const uint32_t dd = __vabsdiffu4(l.g, r.g);  // |dgray|, |dgx|, |dgy|
-    float v = t2[(pop << 8) | (dd & 0xFFu)];
-    if (c.use_grad) v = __fadd_rn(v, lut[kLutGrad + ((dd >> 8) & 0xFFu) + (dd >> 16)]);
-    return v;
-}
-constexpr int band_t2_rows(bool c64) { return c64 ? 65 : 33; }
-
 // Everything about one pixel of a pass that does not depend on the wavefront, computed for all
 // pixels at once before the pass and laid out in pass order (index v * w + u): the value at the
 // start of the pass, its range, and the two static candidates -- the current value and the
@@ -300,64 +284,44 @@ __device__ __forceinline__ void cp16(void* dst, const void* src) {
 }
 
 // Shared state of one band's two warps.  The compute warp (warp 0) walks the band; the link warp
-// (warp 1) carries every exchange with the other bands, so that no fence and no global-memory
-// round trip sits in the compute warp's step loop:
+// (warp 1) carries every exchange with the other bands, so that no GPU-scope fence or L2 round
+// trip sits in the compute warp's step loop:
 //   * it polls the band above's progress counter and copies the newly final columns of that
 //     band's last row into `up` (a ring of kUpRing columns), then raises `avail`;
-//   * it writes this band's last row (handed over by the compute warp's lane 31 through the ring
-//     `last`, as far as `done`) to global memory, raises `copied`, and publishes the progress to
-//     this band's counter behind a GPU-scope fence.
-// The flags are shared-memory release stores and acquire loads (CTA scope), so the compute warp
-// never waits for its own outstanding global stores; causality runs compute warp -> (CTA-scope
-// release / acquire) -> link warp -> (GPU-scope release / acquire) -> the next band's link warp,
-// the order the reference's in-place raster scan implies for the row above.
+//   * it publishes how far this band's last row is final (`done`, raised by the compute warp at
+//     CTA scope) to this band's progress counter, behind a GPU-scope fence.
+// Causality runs compute warp -> (CTA-scope release / acquire) -> link warp -> (GPU-scope release /
+// acquire) -> the next band's link warp, which is the order the reference's in-place raster scan
+// implies for the row above.
 constexpr int kUpRing = 128;
-constexpr int kLastRing = 256;
 struct BandLink {
-    float up[kUpRing];      // row above the band: column c at up[c & (kUpRing - 1)]
-    float last[kLastRing];  // the band's last row: column c at last[c & (kLastRing - 1)]
-    int avail;              // columns [0, avail) of the row above are in `up` (link warp)
-    int done;               // columns [0, done) of the last row are in `last` (compute warp, lane 31)
-    int copied;             // columns [0, copied) of `last` are in global memory (link warp)
-    int abort;              // the link warp gave up waiting (or saw the error word): the compute warp stops
+    float up[kUpRing];  // row above the band: column c at up[c & (kUpRing - 1)]
+    int avail;          // columns [0, avail) of the row above are in `up` (link warp)
+    int used;           // columns [0, used) of `up` are no longer read (compute warp)
+    int done;           // columns [0, done) of the band's last row are final in `work` (compute warp)
+    int abort;          // the link warp gave up waiting (or saw the error word): the compute warp stops
 };
-
-__device__ __forceinline__ int ld_acquire_cta(const int* p) {
-    int v;
-    asm volatile("ld.acquire.cta.shared.u32 %0, [%1];" : "=r"(v) : "r"((unsigned)__cvta_generic_to_shared(p)) : "memory");
-    return v;
-}
-__device__ __forceinline__ void st_release_cta(int* p, int v) {
-    asm volatile("st.release.cta.shared.u32 [%0], %1;" ::"r"((unsigned)__cvta_generic_to_shared(p)), "r"(v) : "memory");
-}
 
 // The link warp of band `band` (see BandLink).  Every wait is bounded: after spin_limit polls in
 // which nothing moved it sets the error word and `abort`, and after as many again it leaves.
-__device__ void band_link(BandLink* L, int band, int w, int h, int fwd, float* work, int* progress, int* err,
-                          int spin_limit) {
+__device__ void band_link(BandLink* s_link, int band, int w, int h, int fwd, const float* work, int* progress,
+                          int* err, int spin_limit) {
     const int lane = threadIdx.x & 31;
+    volatile BandLink* L = s_link;
     volatile int* vprog = progress;
     const int xs = fwd ? 1 : -1, xb = fwd ? 0 : w - 1;
     const int y_above = band > 0 ? (fwd ? band * kBand - 1 : h - band * kBand) : 0;
     const float* above = work + (size_t)y_above * w;
-    // this band's last row (pass-order row band * kBand + kBand - 1), when the band has one
-    const int vlast = band * kBand + kBand - 1;
-    float* last_row = vlast < h ? work + (size_t)(fwd ? vlast : h - 1 - vlast) * w : nullptr;
     int fetched = band > 0 ? 0 : w;  // columns of the row above copied into the ring
     int published = 0;
     int idle = 0;
     bool gave_up = false;
     for (;;) {
         bool moved = false;
-        // this band's last row, as far as the compute warp has handed it over
-        const int done = ld_acquire_cta(&L->done);
+        // this band's last row, as far as the compute warp has released it
+        const int done = L->done;
         if (done > published) {
-            if (last_row)
-                for (int col = published + lane; col < done; col += 32)
-                    last_row[xb + xs * col] = L->last[col & (kLastRing - 1)];
-            __syncwarp();
             if (lane == 0) {
-                st_release_cta(&L->copied, done);
                 fence_acq_rel();
                 vprog[band] = done;
             }
@@ -365,23 +329,22 @@ __device__ void band_link(BandLink* L, int band, int w, int h, int fwd, float* w
             moved = true;
         }
         if (published >= w) break;
-        // the row above, as far as the band above has published it and the ring has room: once
-        // lane 31 has published done >= 1 (at step done + kBand - 2), lane 0 has read every column
-        // up to done + kBand - 2, whose slots may take columns up to done + kBand - 2 + kUpRing;
-        // before that, only the ring's first kUpRing columns
+        // the row above, as far as the band above has published it and the ring has room
         if (fetched < w && !gave_up) {
             int prog = 0;
             if (lane == 0) prog = vprog[band - 1];
             prog = __shfl_sync(0xffffffffu, prog, 0);
-            const int room = published > 0 ? published + kBand - 1 + kUpRing : kUpRing;
-            const int upto = min(min(prog, room), w);
+            const int upto = min(min(prog, L->used + kUpRing), w);
             if (upto > fetched) {
                 if (lane == 0) fence_acq_rel();
                 __syncwarp();
                 for (int col = fetched + lane; col < upto; col += 32)
-                    L->up[col & (kUpRing - 1)] = __ldcg(above + (xb + xs * col));
+                    s_link->up[col & (kUpRing - 1)] = __ldcg(above + (xb + xs * col));
                 __syncwarp();
-                if (lane == 0) st_release_cta(&L->avail, upto);
+                if (lane == 0) {
+                    __threadfence_block();
+                    L->avail = upto;
+                }
                 fetched = upto;
                 moved = true;
             }
@@ -394,7 +357,7 @@ __device__ void band_link(BandLink* L, int band, int w, int h, int fwd, float* w
         if (!gave_up && (idle > spin_limit || *(volatile int*)err)) {
             if (lane == 0) {
                 atomicExch(err, 1);
-                st_release_cta(&L->abort, 1);
+                L->abort = 1;
             }
             gave_up = true;
             idle = 0;
@@ -420,17 +383,11 @@ __global__ void __launch_bounds__(64) refine_band_kernel(CostCtx c, int fwd, con
     __shared__ __align__(16) RStep s_ring[kRing][32];
     __shared__ __align__(16) RPack<C64> s_lpk[kRing][32];
     __shared__ BandLink s_link;
-    extern __shared__ __align__(16) unsigned char s_dyn[];
-    float* s_t2 = reinterpret_cast<float*>(s_dyn);  // census (+ AD) table, band_t2_rows x 256
     for (int i = threadIdx.x; i < kLutSize; i += blockDim.x) s_lut[i] = c.lut[i];
-    for (int i = threadIdx.x; i < band_t2_rows(C64) * 256; i += blockDim.x) {
-        const float lc = c.lut[kLutCensus + (i >> 8)];
-        s_t2[i] = c.use_ad ? __fadd_rn(lc, c.lut[kLutAd + (i & 255)]) : lc;
-    }
     if (threadIdx.x == 0) {
         s_link.avail = 0;
+        s_link.used = 0;
         s_link.done = 0;
-        s_link.copied = 0;
         s_link.abort = 0;
     }
     __syncthreads();
@@ -440,6 +397,7 @@ __global__ void __launch_bounds__(64) refine_band_kernel(CostCtx c, int fwd, con
         band_link(&s_link, band, w, h, fwd, work, progress, err, spin_limit);
         return;
     }
+    volatile BandLink* link = &s_link;
     const int lane = threadIdx.x;
     const int v = band * kBand + lane;  // pass-order row of this lane
     const bool row_ok = v < h;
@@ -453,9 +411,8 @@ __global__ void __launch_bounds__(64) refine_band_kernel(CostCtx c, int fwd, con
     float* wrow = work + rowoff;
     const int d0 = c.d0, dmax = c.d0 + c.D;
     const int eoff = fwd ? d0 : dmax - 1;  // entering window pixel of column u: x(u) - eoff
-    // after the table: each lane's window ring, one record of padding
-    RPack<C64>* s_win = reinterpret_cast<RPack<C64>*>(s_dyn + band_t2_rows(C64) * 256 * sizeof(float)) + lane * (wmask + 2);
-    const bool last_lane = lane == kBand - 1 && row_ok;  // hands the band's last row to the link warp
+    extern __shared__ __align__(16) unsigned char s_dyn[];
+    RPack<C64>* s_win = reinterpret_cast<RPack<C64>*>(s_dyn) + lane * (wmask + 2);  // one record of padding
     auto copy_win = [&](int u) {
         const int pe = xb + xs * u - eoff;
         if ((unsigned)pe < (unsigned)w)
@@ -514,9 +471,9 @@ __global__ void __launch_bounds__(64) refine_band_kernel(CostCtx c, int fwd, con
                 // wait until the link warp has the row above at least up to column t
                 int spins = 0;
                 for (;;) {
-                    avail = ld_acquire_cta(&s_link.avail);
+                    avail = link->avail;
                     if (avail > t) break;
-                    if (ld_acquire_cta(&s_link.abort) || ++spins > spin_limit) {
+                    if (link->abort || ++spins > spin_limit) {
                         abort = true;
                         break;
                     }
@@ -526,6 +483,7 @@ __global__ void __launch_bounds__(64) refine_band_kernel(CostCtx c, int fwd, con
                     if (lane == 0) atomicExch(err, 1);
                     break;
                 }
+                __threadfence_block();
             }
             if (lane == 0) up_first = s_link.up[t & (kUpRing - 1)];
         }
@@ -553,10 +511,10 @@ __global__ void __launch_bounds__(64) refine_band_kernel(CostCtx c, int fwd, con
                 const int du = has_u ? min(max((int)roundf(up), lo), hi - 1) : 0;
                 const int xl = x - dl, xu = x - du;
                 const float cl = (has_l && (unsigned)xl < (unsigned)w)
-                                     ? band_cost<C64>(c, s_t2, s_lut, l, WIN ? s_win[xl & wmask] : rrow[xl])
+                                     ? packed_cost<C64>(c, s_lut, l, WIN ? s_win[xl & wmask] : rrow[xl])
                                      : 1e6f;
                 const float cu = (has_u && (unsigned)xu < (unsigned)w)
-                                     ? band_cost<C64>(c, s_t2, s_lut, l, WIN ? s_win[xu & wmask] : rrow[xu])
+                                     ? packed_cost<C64>(c, s_lut, l, WIN ? s_win[xu & wmask] : rrow[xu])
                                      : 1e6f;
                 // the reference's order: cur, left, up, cur + draw; the first strict minimum wins
                 float best_c = 1e9f;
@@ -566,35 +524,26 @@ __global__ void __launch_bounds__(64) refine_band_kernel(CostCtx c, int fwd, con
                 if (has_u && cu < best_c) { best_c = cu; best_d = du; }
                 if (has_draw && st.c_draw < best_c) { best_c = st.c_draw; best_d = d_draw; }
                 val = (float)best_d;
-                if (!last_lane) wrow[x] = val;  // the last row goes out through the link warp
+                wrow[x] = val;
             }
             prev = val;
-            if (last_lane) s_link.last[u & (kLastRing - 1)] = val;
         }
         // the slot just read is refilled only after its record was copied out above
         __syncwarp();
         issue(t + kRing);
-        if ((t % kPublish) == kPublish - 1 && lane == kBand - 1) {
-            // release to the link warp (CTA scope): the last row is in `last` up to column t - 31
-            const int done = max(0, min(t - (kBand - 1) + 1, w));
-            st_release_cta(&s_link.done, done);
-            // the next kPublish columns go to ring slots the link warp must have copied out: wait
-            // (bounded) until it has, which it does at once unless it gave up
-            const int need = done + kPublish - kLastRing;
-            int spins = 0;
-            while (ld_acquire_cta(&s_link.copied) < need) {
-                if (ld_acquire_cta(&s_link.abort) || ++spins > spin_limit) {
-                    atomicExch(err, 1);
-                    break;
-                }
-                __nanosleep(32);
-            }
+        if ((t % kPublish) == kPublish - 1) {
+            // release to the link warp (CTA scope): how far the last row (lane 31, column t - 31)
+            // is final, and that the ring's columns up to t are read
+            __threadfence_block();
+            if (lane == kBand - 1) link->done = max(0, min(t - (kBand - 1) + 1, w));
+            if (lane == 0) link->used = min(t + 1, w);
         }
     }
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     __syncwarp();
+    __threadfence_block();
     // the whole band is final (or the pass was abandoned: let the next band finish)
-    if (lane == kBand - 1) st_release_cta(&s_link.done, w);
+    if (lane == kBand - 1) link->done = w;
 }
 
 // ---- host: the engine stream, its draw values and rejected indices per radius
@@ -760,19 +709,12 @@ cudaError_t launch_refine_pass(const CostCtx& c, const Layout& L, unsigned char*
     // the right-image window in shared memory (32-bit census): a power-of-two ring per lane holding
     // the D window pixels plus the kRing copied ahead, when every band still fits on the device at once
     int wmask = 0;
-    // dynamic shared memory: the census (+ AD) table, then (shared-memory window) the lanes' rings
-    const size_t t2_bytes = (size_t)band_t2_rows(c.census64) * 256 * sizeof(float);
-    size_t wbytes = t2_bytes;
+    size_t wbytes = 0;
     const void* kern = c.census64 ? (const void*)refine_band_kernel<true, false> : (const void*)refine_band_kernel<false, false>;
-    {
-        const cudaError_t ae = c.census64 ? allow_dynamic_smem(refine_band_kernel<true, false>, t2_bytes)
-                                          : allow_dynamic_smem(refine_band_kernel<false, false>, t2_bytes);
-        if (ae != cudaSuccess) return ae;
-    }
     if (!c.census64 && tune.window == 0) {
         int rs = 1;
         while (rs < c.D + kRing) rs <<= 1;
-        const size_t bytes = t2_bytes + (size_t)kBand * (rs + 1) * sizeof(RPack<false>);
+        const size_t bytes = (size_t)kBand * (rs + 1) * sizeof(RPack<false>);
         auto wk = refine_band_kernel<false, true>;
         if (rs <= 512 && allow_dynamic_smem(wk, bytes) == cudaSuccess) {
             int per_sm = 0, dev = 0, nsm = 0;
