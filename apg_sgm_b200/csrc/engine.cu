@@ -239,6 +239,11 @@ Engine::Engine(const apg_pipeline_config_t& cfg, int device, cudaStream_t stream
     }
     for (auto& e : ev_) cudaEventCreate(&e);
     for (auto& e : pev_) cudaEventCreate(&e);
+    // the right-image WTA's finalize runs here beside the aggregation and the sweeps
+    if (cudaStreamCreateWithFlags(&side_stream_, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        side_stream_ = nullptr;
+    }
     // Cost LUTs on the host with std::exp, exactly as DiscreteCostLut (src/discrete_cost_lut.hpp:20-35).
     lut_host_.assign(kLutSize, 0.f);
     const float lc = std::max(cfg_.lambda_census, 1e-3f);
@@ -261,6 +266,7 @@ Engine::Engine(const apg_pipeline_config_t& cfg, int device, cudaStream_t stream
 Engine::~Engine() {
     release();
     if (copy_stream_) cudaStreamDestroy(copy_stream_);
+    if (side_stream_) cudaStreamDestroy(side_stream_);
     if (ev_maps_) cudaEventDestroy(ev_maps_);
     if (ev_copied_) cudaEventDestroy(ev_copied_);
     if (refine_err_host_) cudaFreeHost(refine_err_host_);
@@ -652,7 +658,19 @@ int Engine::run_pre(const uint8_t* dl, int lstride, const uint8_t* dr, int rstri
         sgm_src = ptr<uint32_t>(L.volA);
     }
     cudaEventRecord(ev_[3], s);
-    RUN(launch_right_wta_finalize(cc, ptr<uint32_t>(L.rkey), cfg_.subpixel, ptr<float>(L.disp_right), s), "right wta");
+    // the right-image disparity needs only the argmin keys: it is finalized on the side stream while
+    // the vertical aggregation and the sweeps run, and the confidence stage waits for it (serial
+    // when every launch is profiled)
+    rwta_forked_ = side_stream_ && !prof;
+    if (rwta_forked_) {
+        cudaEventRecord(ev_[10], s);
+        RUNC(cudaStreamWaitEvent(side_stream_, ev_[10], 0), "fork");
+        RUN(launch_right_wta_finalize(cc, ptr<uint32_t>(L.rkey), cfg_.subpixel, ptr<float>(L.disp_right), side_stream_),
+            "right wta");
+        cudaEventRecord(ev_[11], side_stream_);
+    } else {
+        RUN(launch_right_wta_finalize(cc, ptr<uint32_t>(L.rkey), cfg_.subpixel, ptr<float>(L.disp_right), s), "right wta");
+    }
     cudaEventRecord(ev_[4], s);
     if (L.cross) {
         const int tau = cfg_.color_threshold;
@@ -836,6 +854,7 @@ int Engine::run_post(float* d_disp, float* d_conf, uint8_t* d_reason, uint8_t* d
     ca.lr_check = cfg_.lr_check;
     ca.post_lr_max_diff = cfg_.post_lr_max_diff;
     ca.disp_out = ptr<float>(L.disp_lr);
+    if (rwta_forked_) RUNC(cudaStreamWaitEvent(s, ev_[11], 0), "join");  // the right-image disparity
     RUN(launch_conf_lr(ca, s), "confidence");
     if (debug_) RUNC(cudaMemcpyAsync(ptr<uint8_t>(L.reason_conf), ptr<uint8_t>(L.reason), n, cudaMemcpyDeviceToDevice, s), "dbg");
     if (early_conf_ || early_rel_ || early_reason_) {
@@ -1090,7 +1109,7 @@ void Engine::stage_times(double* ms) const {
     ms[1] = el(1, 2);   // prior / range
     ms[2] = el(2, 3);   // cost (+cross-H, +right argmin)
     ms[3] = el(4, 5);   // cross (vertical)
-    ms[4] = el(3, 4);   // right WTA
+    ms[4] = rwta_forked_ ? el(10, 11) : el(3, 4);   // right WTA (on the side stream when forked)
     ms[5] = el(5, 6);   // sgm (WTA fused into the last sweep)
     ms[6] = 0.0;        // wta: fused into the last SGM sweep
     ms[7] = el(6, 7);   // confidence (+LR when fused)

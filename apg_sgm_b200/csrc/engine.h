@@ -258,6 +258,8 @@ private:
     // host path: confidence / reliability (and reason, without refine) are final after the
     // confidence kernel; their device-to-host copies run on copy_stream_ while the rest finishes
     cudaStream_t copy_stream_ = nullptr;
+    cudaStream_t side_stream_ = nullptr;  // the right-image WTA finalize, beside aggregation and SGM
+    bool rwta_forked_ = false;            // the last frame finalized it there (join before confidence)
     cudaEvent_t ev_maps_ = nullptr, ev_copied_ = nullptr;
     float* early_conf_ = nullptr;
     uint8_t* early_reason_ = nullptr;

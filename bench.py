@@ -89,107 +89,109 @@ def _profile_traffic(kernel: str, workload: str):
     return None
 
 
+_SAMPLER_CHILD = r"""
+import sys, time
+path, bus, idx = sys.argv[1], sys.argv[2], int(sys.argv[3])
+import pynvml as nv
+nv.nvmlInit()
+try:
+    h = nv.nvmlDeviceGetHandleByPciBusId(bus) if bus else nv.nvmlDeviceGetHandleByIndex(idx)
+except Exception:
+    h = nv.nvmlDeviceGetHandleByIndex(idx)
+smax = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+with open(path, "w", buffering=1) as f:
+    while True:
+        sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+        rs = int(nv.nvmlDeviceGetCurrentClocksEventReasons(h))
+        f.write(f"{time.monotonic()} {sm} {smax} {rs}\n")
+        time.sleep(0.002)
+"""
+
+
 class ClockSampler:
     """SM clock and clock-event reasons of this rank's GPU, read through NVML every ~2 ms by a
-    background thread (reads only; no setting is touched).  mark() records host-time marks around
-    the timed region so its samples can be told apart from the rest of the sampled window (the
-    per-launch profile and the end-to-end legs that follow it, all with the GPU busy).  Falls back to
-    nvidia-smi at its fastest rate when NVML is not importable."""
+    separate process that writes timestamped samples to a file (reads only; no setting is
+    touched).  Nothing runs in the benchmark's own process meanwhile, so the timed launches never
+    wait for a sampling thread.  mark() records monotonic-clock marks around the timed region so
+    its samples can be told apart from the rest of the sampled window (the per-launch profile and
+    the end-to-end legs that follow it, all with the GPU busy)."""
 
-    REASONS = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+    REASON_BITS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40,
+                   "sw_power_cap": 0x4}
 
     def __init__(self, device_index: int):
         self.dev = device_index
-        self.samples = []  # (host time, sm MHz, max sm MHz, reason names)
         self.marks = {}
-        self._stop = threading.Event()
-        self._t = None
-        self._nvml = None
+        self.proc = None
+        self.path = None
 
-    def _handle(self, nv):
+    def start(self):
+        import tempfile
+        bus = ""
         try:
             import torch
             pr = torch.cuda.get_device_properties(self.dev)
             bus = f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0"
-            return nv.nvmlDeviceGetHandleByPciBusId(bus)
         except Exception:
-            return nv.nvmlDeviceGetHandleByIndex(self.dev)
-
-    def start(self):
+            pass
+        fd, self.path = tempfile.mkstemp(prefix="apg_clocks_", suffix=".txt")
+        os.close(fd)
         try:
-            import pynvml as nv
-            nv.nvmlInit()
-            h = self._handle(nv)
-            smax = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
-            bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
-                    "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
-                    "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
-                    "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
-            self._nvml = nv
+            self.proc = subprocess.Popen([sys.executable, "-c", _SAMPLER_CHILD, self.path, bus, str(self.dev)],
+                                         stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
 
-            def poll():
-                while not self._stop.is_set():
-                    try:
-                        sm = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
-                        rs = int(nv.nvmlDeviceGetCurrentClocksEventReasons(h))
-                        self.samples.append((time.perf_counter(), sm, smax,
-                                             tuple(n for n, b in bits.items() if rs & b)))
-                    except Exception:
-                        pass
-                    self._stop.wait(0.002)
-        except Exception:
-            poll = self._poll_smi
-        self._t = threading.Thread(target=poll, daemon=True)
-        self._t.start()
-
-    def _poll_smi(self):
-        fields = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-                  "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    def _samples(self):
+        out = []
         try:
-            proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={fields}",
-                                     "--format=csv,noheader,nounits", "-lms", "20"],
-                                    stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-        except FileNotFoundError:
-            return
-        for line in proc.stdout:
-            parts = [p.strip() for p in line.split(",")]
-            try:
-                self.samples.append((time.perf_counter(), float(parts[0]), float(parts[1]),
-                                     tuple(n for n, v in zip(self.REASONS, parts[2:6]) if v.lower() == "active")))
-            except (ValueError, IndexError):
-                pass
-            if self._stop.is_set():
-                break
-        proc.terminate()
+            with open(self.path) as f:
+                for line in f:
+                    parts = line.split()
+                    if len(parts) == 4:
+                        try:
+                            out.append((float(parts[0]), float(parts[1]), float(parts[2]), int(parts[3])))
+                        except ValueError:
+                            pass
+        except OSError:
+            pass
+        return out
 
-    def wait_first(self, timeout: float = 5.0):
-        """Block until the first sample has arrived, so the timed region is covered."""
+    def wait_first(self, timeout: float = 15.0):
+        """Block until the first sample has been written, so the timed region is covered."""
         t0 = time.time()
-        while not self.samples and time.time() - t0 < timeout:
-            time.sleep(0.001)
+        while self.proc and self.proc.poll() is None and time.time() - t0 < timeout:
+            if os.path.getsize(self.path) > 0:
+                return
+            time.sleep(0.005)
 
     def mark(self, name: str):
-        self.marks[name] = time.perf_counter()
+        self.marks[name] = time.monotonic()
 
     def stop(self):
-        self._stop.set()
-        if self._t:
-            self._t.join(timeout=5)
-        if self._nvml:
+        if self.proc:
+            self.proc.terminate()
             try:
-                self._nvml.nvmlShutdown()
-            except Exception:
-                pass
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        samples = self._samples()
+        try:
+            os.unlink(self.path)
+        except OSError:
+            pass
+        if not samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvml sampler unavailable"], "samples": 0}
         t0, t1 = self.marks.get("timed_start"), self.marks.get("timed_end")
-        timed = [s for s in self.samples if t0 is not None and t1 is not None and t0 <= s[0] <= t1]
-        busy = [s for s in self.samples if t0 is not None and s[0] >= t0]
+        timed = [x for x in samples if t0 is not None and t1 is not None and t0 <= x[0] <= t1]
+        busy = [x for x in samples if t0 is not None and x[0] >= t0]
         use = timed or busy
-        reasons = sorted({r for s in use for r in s[3]})
-        return {"sm_mhz": statistics.median(s[1] for s in use) if use else None,
-                "sm_max_mhz": max(s[2] for s in use) if use else None,
+        reasons = sorted({n for x in use for n, bit in self.REASON_BITS.items() if x[3] & bit})
+        return {"sm_mhz": statistics.median(x[1] for x in use) if use else None,
+                "sm_max_mhz": max(x[2] for x in use) if use else None,
                 "reasons": reasons, "samples": len(use), "samples_in_timed_region": len(timed),
                 "window": "timed region" if timed else "timed region through the end-to-end legs",
-                "source": "nvml" if self._nvml else "nvidia-smi"}
+                "source": "nvml (separate process)"}
 
 
 def _algorithmic_bytes(name: str, w: int, h: int, D: int, volume_source: bool, npath: int = 4) -> float:
