@@ -949,7 +949,7 @@ __global__ void __launch_bounds__(64) sgm_last_split_kernel(SgmArgs a, DirTable 
 // volume-fed sweep has few chains per SM, so it keeps many steps in flight to cover the HBM
 // latency under load; the census-fed sweeps load little per step.
 #ifndef APGCU_SGM_PF_VOLUME_FIRST
-#define APGCU_SGM_PF_VOLUME_FIRST 16  // 16 vs 8 steps: first phase 0.287 vs 0.293 ms at 720p D128
+#define APGCU_SGM_PF_VOLUME_FIRST 8  // 16 measured 2% faster per launch, but 27% slower Fast 720p steps beside the side stream's finalize
 #endif
 #ifndef APGCU_SGM_PF_VOLUME_LAST
 #define APGCU_SGM_PF_VOLUME_LAST 8
