@@ -457,58 +457,73 @@ __global__ void __launch_bounds__(CROSS ? 512 : 256, CROSS ? (WPL > 2 ? 1 : 2) :
         }
         if (CROSS) {
             __syncthreads();
+            // run offsets: the run totals become an exclusive prefix over the runs, per word, so a
+            // window's sum is two lookups whatever number of runs it spans (sums wrap modulo 2^32
+            // and counts modulo 2^16; the window differences are exact, as for the prefixes)
+            for (int k = tid; k < W2; k += nt) {
+                uint32_t acc = 0;
+                for (int j = 0; j < g.nrun; ++j) {
+                    const uint32_t v = s_tot[j * W2 + k];
+                    s_tot[j * W2 + k] = acc;
+                    acc += v;
+                }
+                if (PRIOR) {
+                    uint16_t accc = 0;
+                    for (int j = 0; j < g.nrun; ++j) {
+                        const uint16_t v = s_totc[j * W2 + k];
+                        s_totc[j * W2 + k] = accc;
+                        accc = (uint16_t)(accc + v);
+                    }
+                }
+            }
+            __syncthreads();
             // T(x, d) = floor(window sum / valid count) over [x - L(x), x + R(x)]; a thread takes
-            // two words of one pixel
-            constexpr int pairs = W2 / 2;
-            const int p = tid % pairs, k2 = 2 * p;
-            for (int xi = tid / pairs; xi < g.txc; xi += nt / pairs) {
+            // four words of one pixel, so the pixel's arms, divisor and border tests serve eight
+            // disparities and its loads are independent
+            constexpr int quads = W2 / 4;
+            for (int item = tid; item < g.txc * quads; item += nt) {
+                const int xi = item / quads, k4 = 4 * (item - xi * quads);
                 const int x = x0 + xi;
                 if (x >= c.w) break;
                 const uint32_t arm = s_arm[xi];
                 const int l = (int)(arm & 0xFFu), r = (int)((arm >> 8) & 0xFFu);
                 const int rlo = (int)((arm >> 16) & 0xFFu), rhi = (int)(arm >> 24);
                 const int sxi = xi + g.ha, a = sxi - l, b = sxi + r;
-                uint2 sb = *reinterpret_cast<const uint2*>(s_pre + b * W2 + k2);
-                const uint2 sa = a > 0 ? *reinterpret_cast<const uint2*>(s_pre + (a - 1) * W2 + k2) : make_uint2(0, 0);
-                for (int j = rlo; j < rhi; ++j) {
-                    const uint2 t = *reinterpret_cast<const uint2*>(s_tot + j * W2 + k2);
-                    sb.x += t.x;
-                    sb.y += t.y;
-                }
-                const uint32_t s0 = sb.x - sa.x, s1 = sb.y - sa.y;
-                uint32_t w0, w1;
+                const uint4 pb = *reinterpret_cast<const uint4*>(s_pre + b * W2 + k4);
+                const uint4 ob = *reinterpret_cast<const uint4*>(s_tot + rhi * W2 + k4);
+                const uint4 oa = *reinterpret_cast<const uint4*>(s_tot + rlo * W2 + k4);
+                const uint4 pa = a > 0 ? *reinterpret_cast<const uint4*>(s_pre + (a - 1) * W2 + k4) : make_uint4(0, 0, 0, 0);
+                const uint32_t sum[4] = {(pb.x + ob.x) - (pa.x + oa.x), (pb.y + ob.y) - (pa.y + oa.y),
+                                         (pb.z + ob.z) - (pa.z + oa.z), (pb.w + ob.w) - (pa.w + oa.w)};
+                uint32_t wd[4];
                 const uint32_t len = (uint32_t)(l + r + 1);
                 if constexpr (PRIOR) {
                     // valid counts of the window from the count prefix (two 8-bit counts per word),
                     // validity from the centre pixel's range (the tile kernel's rule)
-                    const uint32_t cb = *reinterpret_cast<const uint32_t*>(s_cnt + b * W2 + k2);
-                    const uint32_t ca = a > 0 ? *reinterpret_cast<const uint32_t*>(s_cnt + (a - 1) * W2 + k2) : 0u;
-                    uint32_t tlo = 0, thi = 0;
-                    for (int j = rlo; j < rhi; ++j) {
-                        const uint32_t t = *reinterpret_cast<const uint32_t*>(s_totc + j * W2 + k2);
-                        tlo += t & 0xFFFFu;
-                        thi += t >> 16;
-                    }
-                    const uint32_t n0 = ((cb & 0xFFFFu) - (ca & 0xFFFFu) + tlo) & 0xFFFFu;
-                    const uint32_t n1 = ((cb >> 16) - (ca >> 16) + thi) & 0xFFFFu;
+                    const uint2 cb = *reinterpret_cast<const uint2*>(s_cnt + b * W2 + k4);
+                    const uint2 ca = a > 0 ? *reinterpret_cast<const uint2*>(s_cnt + (a - 1) * W2 + k4) : make_uint2(0, 0);
+                    const uint2 tb = *reinterpret_cast<const uint2*>(s_totc + rhi * W2 + k4);
+                    const uint2 ta = *reinterpret_cast<const uint2*>(s_totc + rlo * W2 + k4);
+                    const uint32_t cw[4] = {(cb.x & 0xFFFFu) + (tb.x & 0xFFFFu) - (ca.x & 0xFFFFu) - (ta.x & 0xFFFFu),
+                                            (cb.x >> 16) + (tb.x >> 16) - (ca.x >> 16) - (ta.x >> 16),
+                                            (cb.y & 0xFFFFu) + (tb.y & 0xFFFFu) - (ca.y & 0xFFFFu) - (ta.y & 0xFFFFu),
+                                            (cb.y >> 16) + (tb.y >> 16) - (ca.y >> 16) - (ta.y >> 16)};
                     const uint32_t rg = s_rng[sxi];
                     const int lo = (int)(int16_t)(rg & 0xFFFFu), hi = (int)(int16_t)(rg >> 16);
-                    w0 = prior_word(c, s0, n0, k2, lo, hi, s_magic);
-                    w1 = prior_word(c, s1, n1, k2 + 1, lo, hi, s_magic);
-                    *reinterpret_cast<uint2*>(out_vol + ((size_t)row + x) * W2 + k2) = make_uint2(w0, w1);
-                    continue;
-                }
-                // every word of the pixel has its whole window valid (no padded words, x - d inside
-                // the image over the window for every d): one count, no per-word tests
-                if (c.D == c.Dp && len > 1 && x - l >= c.d0 + c.Dp - 1 && x + r <= c.w - 1 + c.d0) {
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) wd[q] = prior_word(c, sum[q], cw[q] & 0xFFFFu, k4 + q, lo, hi, s_magic);
+                } else if (c.D == c.Dp && len > 1 && x - l >= c.d0 + c.Dp - 1 && x + r <= c.w - 1 + c.d0) {
+                    // every word of the pixel has its whole window valid (no padded words, x - d inside
+                    // the image over the window for every d): one count, no per-word tests
                     const uint32_t mg = s_magic[len];
-                    w0 = __byte_perm(__umulhi(s0 & 0xFFFFu, mg), __umulhi(s0 >> 16, mg), 0x5410);
-                    w1 = __byte_perm(__umulhi(s1 & 0xFFFFu, mg), __umulhi(s1 >> 16, mg), 0x5410);
+#pragma unroll
+                    for (int q = 0; q < 4; ++q)
+                        wd[q] = __byte_perm(__umulhi(sum[q] & 0xFFFFu, mg), __umulhi(sum[q] >> 16, mg), 0x5410);
                 } else {
-                    w0 = agg_word(c, s0, k2, x, l, r, s_magic);
-                    w1 = agg_word(c, s1, k2 + 1, x, l, r, s_magic);
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) wd[q] = agg_word(c, sum[q], k4 + q, x, l, r, s_magic);
                 }
-                *reinterpret_cast<uint2*>(out_vol + ((size_t)row + x) * W2 + k2) = make_uint2(w0, w1);
+                *reinterpret_cast<uint4*>(out_vol + ((size_t)row + x) * W2 + k4) = make_uint4(wd[0], wd[1], wd[2], wd[3]);
             }
         }
     }
