@@ -199,6 +199,7 @@ int Batch::ensure_slots(Bucket& b, int m) {
         }
         e->set_sgm_lanes(b.tune.sgm_lanes);
         e->set_cost_tile(b.tune.cost_tile);
+        e->set_cost8(1);  // the batched SGM kernels read two-byte volumes
         b.slots.push_back(std::move(e));
         cudaEvent_t ev;
         if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {

@@ -48,6 +48,7 @@ struct CostCtx {
     float sp_param = 0.0f;
     int tile;          // cost kernel tile width (64, 128, 256; 0 = default for Dp)
     int kernel;        // cost kernel: 0 = pixel runs where they apply, 1 = column tiles always
+    int vol8 = 0;      // raw volume at one byte per voxel, 0xFF invalid (Fast census-only, pixel runs)
 };
 
 // Unquantised (float) cost, used by the refiner's local cost (src/refiner.cpp:14-36).

@@ -382,6 +382,7 @@ cudaError_t launch_cost(const CostCtx& c, int mode, int lmax, int tau, uint32_t*
     // mode: 0 = raw volume + right argmin, 1 = cross-H volume + right argmin,
     //       2 = right argmin only (fused Fast path)
     if (cost_runs_supported(c, mode, lmax)) return launch_cost_runs(c, mode, lmax, tau, vol, rkey, magic, s);
+    if (c.vol8) return cudaErrorInvalidValue;  // the byte volume is written by the pixel-run kernel only
     if (c.census64) {
         return c.prior_ranges ? launch_cost_m<true, true>(c, mode, lmax, tau, vol, rkey, magic, s)
                               : launch_cost_m<true, false>(c, mode, lmax, tau, vol, rkey, magic, s);

@@ -171,7 +171,7 @@ __device__ __forceinline__ void store_counts(uint16_t* p, const uint32_t (&c)[N]
 // every lane of the warp (no per-voxel tests).
 // PRIOR: every left pixel has its own range [lo, hi) (staged in s_rng); a voxel outside it is
 // invalid, and the aggregation also keeps a prefix of valid counts (s_cnt, s_totc).
-template <bool V, bool CROSS, bool STORE, bool FULL, int WPL, bool PRIOR>
+template <bool V, bool CROSS, bool STORE, bool FULL, int WPL, bool PRIOR, bool U8>
 __device__ __forceinline__ void run_steps(const CostCtx& c, const RunGeom& g, int row, int xbase, int xs, int xe,
                                           const uint32_t* s_lc, const uint32_t* s_lg, const uint32_t* s_rc,
                                           const uint32_t* s_rg, const float* s_t2, const float* s_lgt,
@@ -202,6 +202,8 @@ __device__ __forceinline__ void run_steps(const CostCtx& c, const RunGeom& g, in
     uint32_t* pp = s_pre + xs * W2 + WPL * lane;                             // prefix words of (xs)
     uint16_t* cp = s_cnt + xs * W2 + WPL * lane;                             // count words of (xs)
     uint32_t* vp = out_vol + ((size_t)row + (xbase + xs)) * W2 + WPL * lane;  // volume words of (xs)
+    // byte volume: the lane's 2 * WPL disparities of (xs) as WPL / 2 words
+    uint32_t* vp8 = out_vol + ((size_t)row + (xbase + xs)) * (W2 / 2) + (WPL / 2) * lane;
     for (int xi = xs; xi < xe; xi += 4) {
         const uint4 lc4 = *reinterpret_cast<const uint4*>(s_lc + xi);
         uint4 lg4 = make_uint4(0, 0, 0, 0);
@@ -289,7 +291,15 @@ __device__ __forceinline__ void run_steps(const CostCtx& c, const RunGeom& g, in
                     uint32_t wd[WPL];
 #pragma unroll
                     for (int w = 0; w < WPL; ++w) wd[w] = qp[w] | ~vm[w];  // invalid halves: 0xFFFF
-                    store_words<WPL>(vp + (size_t)s * W2, wd);
+                    if constexpr (U8) {
+                        // the low byte of each half: costs are below 255, the invalid 0xFFFF becomes 0xFF
+                        uint32_t wb[WPL / 2];
+#pragma unroll
+                        for (int w = 0; w < WPL / 2; ++w) wb[w] = __byte_perm(wd[2 * w], wd[2 * w + 1], 0x6420);
+                        store_words<WPL / 2>(vp8 + (size_t)s * (W2 / 2), wb);
+                    } else {
+                        store_words<WPL>(vp + (size_t)s * W2, wd);
+                    }
                 }
             }
         }
@@ -297,6 +307,7 @@ __device__ __forceinline__ void run_steps(const CostCtx& c, const RunGeom& g, in
         pp += 4 * W2;
         cp += 4 * W2;
         vp += 4 * (size_t)W2;
+        vp8 += 2 * (size_t)W2;
     }
     __syncwarp();
     if (xe > xs) {
@@ -363,7 +374,7 @@ __device__ __forceinline__ uint32_t prior_word(const CostCtx& c, uint32_t s, uin
 
 // With 192 or 256 padded disparities the aggregating kernel keeps one block per SM (registers for
 // the wider lane state, wider tiles: less halo); otherwise two.
-template <bool CROSS, bool STORE, bool FULL, int WPL, bool PRIOR>
+template <bool CROSS, bool STORE, bool FULL, int WPL, bool PRIOR, bool U8>
 __global__ void __launch_bounds__(CROSS ? 512 : 256, CROSS ? (WPL > 2 ? 1 : 2) : 1)
     cost_run_kernel(CostCtx c, RunGeom g, int lmax, int tau, uint32_t* __restrict__ out_vol,
                     uint32_t* __restrict__ rkey, const uint32_t* __restrict__ magic) {
@@ -447,11 +458,11 @@ __global__ void __launch_bounds__(CROSS ? 512 : 256, CROSS ? (WPL > 2 ? 1 : 2) :
             const bool ok = xa >= 0 && xb < c.w && P * lane + P - 1 < c.D && xa - (dlo + P - 1) >= 0 &&
                             xb - dlo <= c.w - 1;
             if (__all_sync(0xFFFFFFFFu, ok))
-                run_steps<true, CROSS, STORE, FULL, WPL, PRIOR>(c, g, row, xbase, xs, xe, s_lc, s_lg, s_rc, s_rg, s_t2,
+                run_steps<true, CROSS, STORE, FULL, WPL, PRIOR, U8>(c, g, row, xbase, xs, xe, s_lc, s_lg, s_rc, s_rg, s_t2,
                                                                 s_lgt, s_q, s_rng, s_pre, s_cnt, s_tot, s_totc, s_em,
                                                                 run, out_vol, rkey);
             else
-                run_steps<false, CROSS, STORE, FULL, WPL, PRIOR>(c, g, row, xbase, xs, xe, s_lc, s_lg, s_rc, s_rg,
+                run_steps<false, CROSS, STORE, FULL, WPL, PRIOR, U8>(c, g, row, xbase, xs, xe, s_lc, s_lg, s_rc, s_rg,
                                                                  s_t2, s_lgt, s_q, s_rng, s_pre, s_cnt, s_tot, s_totc,
                                                                  s_em, run, out_vol, rkey);
         }
@@ -565,12 +576,12 @@ int cross_tile(const CostCtx& c, int lmax, bool full) {
     return 32;
 }
 
-template <bool CROSS, bool STORE, bool FULL, int WPL, bool PRIOR>
+template <bool CROSS, bool STORE, bool FULL, int WPL, bool PRIOR, bool U8>
 cudaError_t launch_runs_w(const CostCtx& c, int txc, int lmax, int tau, uint32_t* vol, uint32_t* rkey,
                           const uint32_t* magic, cudaStream_t s) {
     const RunGeom g = run_geom(c, txc, CROSS ? lmax : 0, CROSS, FULL, PRIOR);
     const int nt = 32 * g.nrun;
-    auto kern = cost_run_kernel<CROSS, STORE, FULL, WPL, PRIOR>;
+    auto kern = cost_run_kernel<CROSS, STORE, FULL, WPL, PRIOR, U8>;
     cudaError_t e = allow_dynamic_smem(kern, g.total);
     if (e != cudaSuccess) return e;
     int per_sm = 0, dev = 0, nsm = 0;
@@ -587,11 +598,21 @@ cudaError_t launch_runs_w(const CostCtx& c, int txc, int lmax, int tau, uint32_t
 template <bool CROSS, bool STORE, bool FULL, bool PRIOR>
 cudaError_t launch_runs_p(const CostCtx& c, int txc, int lmax, int tau, uint32_t* vol, uint32_t* rkey,
                           const uint32_t* magic, cudaStream_t s) {
+    if constexpr (STORE && !CROSS && !FULL && !PRIOR) {
+        // the byte volume (Fast census-only costs below 255): 128 or 256 padded disparities
+        if (c.vol8) {
+            if (c.Dp == 128) return launch_runs_w<CROSS, STORE, FULL, 2, PRIOR, true>(c, txc, lmax, tau, vol, rkey, magic, s);
+            if (c.Dp == 256) return launch_runs_w<CROSS, STORE, FULL, 4, PRIOR, true>(c, txc, lmax, tau, vol, rkey, magic, s);
+            return cudaErrorInvalidValue;
+        }
+    } else {
+        if (c.vol8) return cudaErrorInvalidValue;
+    }
     switch (c.Dp) {
-        case 64: return launch_runs_w<CROSS, STORE, FULL, 1, PRIOR>(c, txc, lmax, tau, vol, rkey, magic, s);
-        case 128: return launch_runs_w<CROSS, STORE, FULL, 2, PRIOR>(c, txc, lmax, tau, vol, rkey, magic, s);
-        case 192: return launch_runs_w<CROSS, STORE, FULL, 3, PRIOR>(c, txc, lmax, tau, vol, rkey, magic, s);
-        default: return launch_runs_w<CROSS, STORE, FULL, 4, PRIOR>(c, txc, lmax, tau, vol, rkey, magic, s);
+        case 64: return launch_runs_w<CROSS, STORE, FULL, 1, PRIOR, false>(c, txc, lmax, tau, vol, rkey, magic, s);
+        case 128: return launch_runs_w<CROSS, STORE, FULL, 2, PRIOR, false>(c, txc, lmax, tau, vol, rkey, magic, s);
+        case 192: return launch_runs_w<CROSS, STORE, FULL, 3, PRIOR, false>(c, txc, lmax, tau, vol, rkey, magic, s);
+        default: return launch_runs_w<CROSS, STORE, FULL, 4, PRIOR, false>(c, txc, lmax, tau, vol, rkey, magic, s);
     }
 }
 

@@ -157,6 +157,19 @@ size_t Engine::workspace_bytes(const apg_pipeline_config_t& c, int w, int h, int
     return t;
 }
 
+// The largest census-only quantised cost (the table of the constructor, same float steps).
+static int max_census_cost(const apg_pipeline_config_t& c) {
+    const float lc = std::max(c.lambda_census, 1e-3f);
+    const float norm = 1.f + (c.use_ad ? c.eta_ad : 0.f) + (c.use_grad ? c.mu_grad : 0.f);
+    const float scale = static_cast<float>(c.cost_max) / std::max(norm, 1e-6f);
+    int m = 0;
+    for (int i = 0; i <= 64; ++i) {
+        const int q = static_cast<int>((1.f - std::exp(-static_cast<float>(i) / lc)) * scale + 0.5f);
+        m = std::max(m, std::min(std::max(q, 0), c.cost_max));
+    }
+    return m;
+}
+
 Layout Engine::make_layout(const apg_pipeline_config_t& c, int w, int h, int ch, int debug) {
     Layout L;
     L.w = w; L.h = h; L.ch = ch;
@@ -169,6 +182,15 @@ Layout Engine::make_layout(const apg_pipeline_config_t& c, int w, int h, int ch,
     L.fused_fast = !L.cross && c.census_type == APG_CENSUS_SYMMETRIC_9X7 && !c.use_ad && !c.use_grad &&
                    !c.prior_enable && !c.hier_enable && (debug & kLayoutFastFused) && !(debug & 4);
     L.raw_cost = (debug & 1) != 0;
+    // Fast census-only path with its volume stored: one byte per voxel when every quantised cost is
+    // below 255, so 0xFF marks the invalid voxels exactly (the sweeps' 32-lane form, the pixel-run
+    // cost kernel).  At a padded range of 256 it is the default: one B200, Fast 1920x1080 D256, 2.64
+    // vs 2.83 ms per frame (first phase 0.96 vs 1.20 ms).  At 128 only on request (kLayoutCost8):
+    // Fast 1280x720 D128 0.757 vs 0.749 ms, the first phase's chains there wait on the latency of
+    // each step (widening the bytes) more than on the volume's bytes.  kLayoutCost16 keeps two bytes.
+    L.cost8 = !L.cross && !L.fused_fast && c.census_type == APG_CENSUS_SYMMETRIC_9X7 && !c.use_ad && !c.use_grad &&
+              !c.prior_enable && !c.hier_enable && (L.Dp == 256 || (L.Dp == 128 && (debug & kLayoutCost8))) &&
+              !(debug & kLayoutCost16) && max_census_cost(c) < 255;
     const size_t n = (size_t)w * h;
     const size_t csz = c.census_type == APG_CENSUS_9X7 ? 8 : 4;
     const size_t vol = n * (size_t)L.Dp * 2;
@@ -188,7 +210,7 @@ Layout Engine::make_layout(const apg_pipeline_config_t& c, int w, int h, int ch,
     // volA: cross-H output T (Balanced/HQ), raw cost (Fast without fusion) or the first path-sum
     // buffer (fused Fast); volB: aggregated cost.  The first SGM phase writes one buffer per
     // direction (3 for Path4, 7 for Path8); buffer 0 reuses volA whenever volA is dead by then.
-    L.volA = take(vol);
+    L.volA = take(L.cost8 ? vol / 2 : vol);
     L.volB = L.cross ? take(vol) : 0;
     L.nsbuf = (c.paths == 8 ? 8 : 4) - 1;
     for (int i = 0; i < L.nsbuf; ++i) L.sbuf[i] = (i == 0 && (L.cross || L.fused_fast)) ? L.volA : take(vol);
@@ -357,9 +379,13 @@ int Engine::prepare(int w, int h, int ch) {
 }
 
 int Engine::prepare_arena(int w, int h, int ch) {
-    const Layout L = make_layout(cfg_, w, h, ch, debug_ | (fast_fused_ ? kLayoutFastFused : 0));
+    // the byte volume needs the pixel-run cost kernel and 32-lane sweeps
+    const bool cost16 = cost8_ == 1 || cost_kernel_ == 1 || (sgm_lanes_ != 0 && sgm_lanes_ != 32);
+    const Layout L = make_layout(cfg_, w, h, ch,
+                                 debug_ | (fast_fused_ ? kLayoutFastFused : 0) | (cost16 ? kLayoutCost16 : 0) |
+                                     (cost8_ == 2 ? kLayoutCost8 : 0));
     if (arena_ && arena_bytes_ >= L.total && lay_.w == w && lay_.h == h && lay_.ch == ch &&
-        lay_.raw_cost == L.raw_cost && lay_.fused_fast == L.fused_fast) {
+        lay_.raw_cost == L.raw_cost && lay_.fused_fast == L.fused_fast && lay_.cost8 == L.cost8) {
         return kOk;
     }
     if (arena_ && arena_bytes_ >= L.total) {
@@ -654,7 +680,9 @@ int Engine::run_pre(const uint8_t* dl, int lstride, const uint8_t* dr, int rstri
     } else if (L.fused_fast) {
         if (!L.raw_cost) RUN(launch_cost(cc, 2, lmax, 0, nullptr, ptr<uint32_t>(L.rkey), magic, s), "right argmin");
     } else {
-        RUN(launch_cost(cc, 0, lmax, 0, ptr<uint32_t>(L.volA), ptr<uint32_t>(L.rkey), magic, s), "cost");
+        CostCtx cv = cc;
+        cv.vol8 = L.cost8 ? 1 : 0;
+        RUN(launch_cost(cv, 0, lmax, 0, ptr<uint32_t>(L.volA), ptr<uint32_t>(L.rkey), magic, s), "cost");
         sgm_src = ptr<uint32_t>(L.volA);
     }
     cudaEventRecord(ev_[3], s);
@@ -710,6 +738,7 @@ int Engine::sgm_launch(SgmLaunch* out, uint32_t** sbufs) const {
     pl.store_final = (debug_ & 2) != 0;
     pl.lanes = sgm_lanes_;
     pl.split = sgm_split_;
+    pl.cost8 = (!L.cross && !L.fused_fast && L.cost8) ? 1 : 0;
     for (int i = 0; i < L.nsbuf; ++i) sbufs[i] = ptr<uint32_t>(L.sbuf[i]);
     return L.nsbuf;
 }
@@ -1186,6 +1215,11 @@ int set_tuning(Engine* e, const char* key, int value) {
     if (std::strcmp(key, "sgm_split") == 0) {
         if (value < 0 || value > 2) return kInvalidConfig;
         if (e) e->set_sgm_split(value);
+        return kOk;
+    }
+    if (std::strcmp(key, "cost8") == 0) {
+        if (value < 0 || value > 2) return kInvalidConfig;
+        if (e) e->set_cost8(value);
         return kOk;
     }
     if (std::strcmp(key, "cost_tile") == 0) {

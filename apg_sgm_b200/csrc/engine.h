@@ -29,6 +29,8 @@ enum Status : int {
 
 // Layout request bit beside the debug flags: Fast census-only sweeps recompute their costs.
 constexpr int kLayoutFastFused = 1 << 16;
+constexpr int kLayoutCost16 = 1 << 17;  // keep a Fast volume at two bytes per voxel
+constexpr int kLayoutCost8 = 1 << 18;   // one byte per voxel at a padded range of 128 too
 
 // Frame-size-dependent layout of the device arena.
 struct Layout {
@@ -36,6 +38,7 @@ struct Layout {
     bool fused_fast = false;  // Fast path: costs recomputed inside the SGM sweeps, no volume
     bool cross = false;
     bool raw_cost = false;    // debug: materialise the raw volume
+    bool cost8 = false;       // Fast path: the volume the sweeps read holds one byte per voxel (0xFF invalid)
     size_t total = 0;
     // offsets
     size_t in_left, in_right;
@@ -158,6 +161,7 @@ public:
     void set_debug(int f) { debug_ = f; }
     void set_sgm_lanes(int t) { sgm_lanes_ = t; }
     void set_sgm_split(int v) { sgm_split_ = v; }
+    void set_cost8(int mode) { cost8_ = mode; }
     void set_fast_fused(bool on) { fast_fused_ = on; }
     void set_cost_tile(int t) { cost_tile_ = t; }
     void set_cost_kernel(int k) { cost_kernel_ = k; }
@@ -217,6 +221,7 @@ private:
     int debug_ = 0;
     int sgm_lanes_ = 0;
     int sgm_split_ = 0;  // last sweep over two warps per chain: 0 auto, 1 never, 2 always
+    int cost8_ = 0;  // Fast volume at one byte per voxel: 0 = padded range 256, 1 = never, 2 = 128 and 256
     bool fast_fused_ = false;
     int cost_tile_ = 0;
     int cost_kernel_ = 0;  // 0: pixel-run cost kernel where it applies, 1: column-tile kernel

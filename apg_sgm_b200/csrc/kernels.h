@@ -73,6 +73,7 @@ struct SgmLaunch {
     int lanes;        // lanes per scanline chain (8, 16, 32; 0 = default for Dp)
     int split = 0;    // volume-fed last sweep over two warps per chain: 0 = where it pays (Dp 64),
                       // 1 = never, 2 = always (32 lanes per chain only)
+    int cost8 = 0;    // cvol holds one byte per voxel, 0xFF invalid (32 lanes, Dp 128 or 256)
 };
 // First phase: ndir directions in one launch, direction i writing its path values to out[i].
 cudaError_t launch_sgm_first(const SgmLaunch& l, int ndir, const int (*dirs)[2], uint32_t* const* out,

@@ -134,6 +134,7 @@ struct SgmArgs {
     float sp_param;
     apg_subpixel_telemetry_t* sp_tel;
     int store_final;
+    int cost8;  // cvol holds one byte per voxel (0xFF invalid)
 };
 
 // Directions of one launch; warps [warp_begin[i], warp_begin[i+1]) run direction i.
@@ -491,6 +492,43 @@ __device__ __forceinline__ void lds_words(const uint32_t* src, uint32_t (&v)[K])
 template <int K, int NB>
 __host__ __device__ constexpr int vol_slot_words() { return (K + NB * K) * 32; }
 
+// Cost words per lane in the volume and in a ring slot: K u16x2 words, or K / 2 words of the byte
+// volume.  A lane's words sit together, so a warp's cost loads and reads cover consecutive words.
+template <int K, bool C8>
+__host__ __device__ constexpr int cost_words() { return C8 ? K / 2 : K; }
+
+__device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t sel) {
+    uint32_t r;
+    asm("prmt.b32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "r"(sel));
+    return r;
+}
+
+// The lane's K cost words (u16x2) from its ring slot, the invalid marker clamped to 0x7FFF.  The
+// byte volume (C8) widens each byte to a halfword: a byte 0xFF (invalid) gets the high byte 0xFF,
+// through prmt's sign-replicating selectors on a word whose bit 7 per byte flags 0xFF, and the
+// clamp then gives the same 0x7FFF as the two-byte volume's 0xFFFF.
+template <int K, bool C8>
+__device__ __forceinline__ void load_costs(const uint32_t* src, uint32_t (&c)[K]) {
+    if constexpr (C8) {
+        static_assert(K % 2 == 0, "byte volume: an even number of words per lane");
+        uint32_t cb[K / 2];
+        lds_words<K / 2>(src, cb);
+#pragma unroll
+        for (int i = 0; i < K / 2; ++i) {
+            // per byte b: (~b & 0x7F) + 0x7F has bit 7 set unless the low seven bits of b are all
+            // set; with b's own bit 7 that leaves bit 7 set exactly where b == 0xFF
+            const uint32_t t = (~cb[i] & 0x7F7F7F7Fu) + 0x7F7F7F7Fu;
+            const uint32_t inv = ~t & cb[i] & 0x80808080u;
+            c[2 * i] = __vminu2(prmt(cb[i], inv, 0xD1C0u), kInf2);      // b0, sign(inv.b0), b1, sign(inv.b1)
+            c[2 * i + 1] = __vminu2(prmt(cb[i], inv, 0xF3E2u), kInf2);  // b2, sign(inv.b2), b3, sign(inv.b3)
+        }
+    } else {
+        lds_words<K>(src, c);
+#pragma unroll
+        for (int k = 0; k < K; ++k) c[k] = __vminu2(c[k], kInf2);  // 0xFFFF -> 0x7FFF
+    }
+}
+
 // Words per warp of the last sweep's WTA buffer: 32 pixels x (Dp/2 + 1) words (odd row stride, so
 // one lane per row reads without bank conflicts).
 template <int K, int T>
@@ -576,7 +614,7 @@ __device__ __forceinline__ void wta_row(const SgmArgs& a, const uint32_t* row, i
 // Steps run in blocks of T: at the start of a block lane j loads the gray level of step t0 + j
 // (prefetched one block ahead) and computes that step's adaptive P2, so a step costs one shuffle
 // for P2 instead of a load and the P2 arithmetic.  Addresses advance by a 32-bit word offset.
-template <int T, int K, int MODE, int PF, int NB>
+template <int T, int K, int MODE, int PF, int NB, bool C8 = false>
 __device__ __forceinline__ void run_chain_vol(const SgmArgs& a, const uint32_t* const* in, uint32_t* s_ring,
                                               uint32_t* s_wta, int dx, int dy, int s, int nscan, uint32_t* out) {
     static_assert((PF & (PF - 1)) == 0 && T % PF == 0, "PF: a power of two dividing T");
@@ -593,23 +631,27 @@ __device__ __forceinline__ void run_chain_vol(const SgmArgs& a, const uint32_t* 
     const int p0 = y0 * a.w + x0;
     const uint32_t p1x2 = (uint32_t)a.pen.P1 * 0x00010001u;
     const uint32_t dstep = (uint32_t)(step * W2);  // word offset per step (wraps for negative steps)
+    // the cost volume's words: W2 per pixel, or W2 / 2 for the byte volume (K / 2 per lane)
+    const uint32_t cstep = C8 ? (uint32_t)(step * (W2 / 2)) : dstep;
 
-    // loads of step t (word offset off) into slot t % PF; every step commits one group
-    auto issue = [&](int t, uint32_t off) {
+    // loads of step t (word offsets off, coff) into slot t % PF; every step commits one group
+    auto issue = [&](int t, uint32_t off, uint32_t coff) {
         if (t < len) {
             uint32_t* sl = s_ring + (t & (PF - 1)) * SW;
-            cp_words<K>(sl + lane * K, a.cvol + off);
+            cp_words<cost_words<K, C8>()>(sl + lane * cost_words<K, C8>(), a.cvol + coff);
 #pragma unroll
             for (int b = 0; b < NB; ++b) cp_words<K>(sl + 32 * K * (1 + b) + lane * K, in[b] + off);
         }
         cp_commit();
     };
     const uint32_t off0 = (uint32_t)p0 * (uint32_t)W2 + (uint32_t)(j * K);
-    uint32_t ioff = off0;  // offset of the next step to issue
+    const uint32_t coff0 = C8 ? (uint32_t)p0 * (uint32_t)(W2 / 2) + (uint32_t)(j * (K / 2)) : off0;
+    uint32_t ioff = off0, icoff = coff0;  // offsets of the next step to issue
 #pragma unroll
     for (int t = 0; t < PF; ++t) {
-        issue(t, ioff);
+        issue(t, ioff, icoff);
         ioff += dstep;
+        icoff += cstep;
     }
     uint32_t off = off0;  // offset of the current step
 
@@ -643,9 +685,7 @@ __device__ __forceinline__ void run_chain_vol(const SgmArgs& a, const uint32_t* 
                 if (t < len) {
                     const uint32_t* sl = s_ring + v * SW;
                     uint32_t c[K];
-                    lds_words<K>(sl + lane * K, c);
-#pragma unroll
-                    for (int k = 0; k < K; ++k) c[k] = __vminu2(c[k], kInf2);  // 0xFFFF -> 0x7FFF
+                    load_costs<K, C8>(sl + lane * cost_words<K, C8>(), c);
                     if (t == 0 || m >= kInf) {
 #pragma unroll
                         for (int k = 0; k < K; ++k) L[k] = c[k];
@@ -706,8 +746,9 @@ __device__ __forceinline__ void run_chain_vol(const SgmArgs& a, const uint32_t* 
                     }
                 }
                 // the slot just read is refilled only after its values were consumed above
-                issue(t + PF, ioff);
+                issue(t + PF, ioff, icoff);
                 ioff += dstep;
+                icoff += cstep;
                 off += dstep;
             }
         }
@@ -772,7 +813,7 @@ __device__ __forceinline__ void nbar_arrive_slot(int slot) {
     else nbar_arrive64<BASE>();
 }
 
-template <int K, int NB, int PFA, int PFB>
+template <int K, int NB, int PFA, int PFB, bool C8 = false>
 __global__ void __launch_bounds__(64) sgm_last_split_kernel(SgmArgs a, DirTable tab) {
     static_assert((PFA & (PFA - 1)) == 0 && (PFB & (PFB - 1)) == 0, "ring depths: powers of two");
     using SM = SplitSmem<K, NB, PFA, PFB>;
@@ -793,16 +834,19 @@ __global__ void __launch_bounds__(64) sgm_last_split_kernel(SgmArgs a, DirTable 
     const int nseg = (len + kSplitSeg - 1) / kSplitSeg;
 
     if (warp == 0) {
-        // ---- the recurrence (process_pixel, src/sgm_optimizer.cpp:44-80)
+        // ---- the recurrence (process_pixel, src/sgm_optimizer.cpp:44-80); the byte volume (C8)
+        // has K / 2 words per lane and W2 / 2 per pixel
         auto issue = [&](int t, uint32_t off) {
-            if (t < len) cp_words<K>(s_c + (t & (PFA - 1)) * 32 * K + lane * K, a.cvol + off);
+            if (t < len)
+                cp_words<cost_words<K, C8>()>(s_c + (t & (PFA - 1)) * 32 * K + lane * cost_words<K, C8>(), a.cvol + off);
             cp_commit();
         };
-        uint32_t ioff = off0;
+        const uint32_t cstep = C8 ? (uint32_t)(step * (W2 / 2)) : dstep;
+        uint32_t ioff = C8 ? (uint32_t)p0 * (uint32_t)(W2 / 2) + (uint32_t)(lane * (K / 2)) : off0;
 #pragma unroll
         for (int t = 0; t < PFA; ++t) {
             issue(t, ioff);
-            ioff += dstep;
+            ioff += cstep;
         }
         const uint32_t p1x2 = (uint32_t)a.pen.P1 * 0x00010001u;
         uint32_t L[K];
@@ -831,9 +875,7 @@ __global__ void __launch_bounds__(64) sgm_last_split_kernel(SgmArgs a, DirTable 
                     cp_wait<PFA - 1>();
                     const int P2 = __shfl_sync(0xffffffffu, p2v, t & 31);
                     uint32_t c[K];
-                    lds_words<K>(s_c + (t & (PFA - 1)) * 32 * K + lane * K, c);
-#pragma unroll
-                    for (int k = 0; k < K; ++k) c[k] = __vminu2(c[k], kInf2);  // 0xFFFF -> 0x7FFF
+                    load_costs<K, C8>(s_c + (t & (PFA - 1)) * 32 * K + lane * cost_words<K, C8>(), c);
                     if (t == 0 || m >= kInf) {
 #pragma unroll
                         for (int k = 0; k < K; ++k) L[k] = c[k];
@@ -873,7 +915,7 @@ __global__ void __launch_bounds__(64) sgm_last_split_kernel(SgmArgs a, DirTable 
                     for (int k = 0; k < K; ++k) dst[k] = L[k];
                     // the cost slot just read is refilled only after its words were consumed above
                     issue(t + PFA, ioff);
-                    ioff += dstep;
+                    ioff += cstep;
                 }
             }
             __threadfence_block();
@@ -996,7 +1038,7 @@ __device__ __forceinline__ int find_dir(const DirTable& tab, int warp) {
 }
 
 // First phase: every direction of the table at once, each chain writing its own sum buffer.
-template <int T, int K, bool CENSUS>
+template <int T, int K, bool CENSUS, bool C8 = false>
 __global__ void __launch_bounds__(128) sgm_first_kernel(SgmArgs a, DirTable tab) {
     __shared__ uint16_t s_q[65];
     if (CENSUS) {
@@ -1012,7 +1054,7 @@ __global__ void __launch_bounds__(128) sgm_first_kernel(SgmArgs a, DirTable tab)
     if constexpr (!CENSUS) {
         extern __shared__ __align__(16) uint32_t s_dyn[];
         uint32_t* ring = s_dyn + (threadIdx.x >> 5) * first_pf<T>() * vol_slot_words<K, 0>();
-        run_chain_vol<T, K, kFirst, first_pf<T>(), 0>(a, tab.in, ring, nullptr, dx, dy, s, tab.nscan[d], tab.out[d]);
+        run_chain_vol<T, K, kFirst, first_pf<T>(), 0, C8>(a, tab.in, ring, nullptr, dx, dy, s, tab.nscan[d], tab.out[d]);
         return;
     }
     if (CENSUS && dy == 0) {
@@ -1030,7 +1072,7 @@ __global__ void __launch_bounds__(128) sgm_first_kernel(SgmArgs a, DirTable tab)
 }
 
 // Last sweep (one direction): add the NB partial sums and run the WTA.
-template <int T, int K, bool CENSUS, int NB>
+template <int T, int K, bool CENSUS, int NB, bool C8 = false>
 __global__ void __launch_bounds__(128) sgm_last_kernel(SgmArgs a, DirTable tab) {
     __shared__ uint16_t s_q[65];
     if (CENSUS) {
@@ -1045,7 +1087,7 @@ __global__ void __launch_bounds__(128) sgm_last_kernel(SgmArgs a, DirTable tab) 
         constexpr int PF = last_pf<K, T, NB>();
         constexpr int per_warp = PF * vol_slot_words<K, NB>() + wta_buf_words<K, T>();
         uint32_t* ring = s_dyn + (threadIdx.x >> 5) * per_warp;
-        run_chain_vol<T, K, kLast, PF, NB>(a, tab.in, ring, ring + PF * vol_slot_words<K, NB>(), tab.dx[0], tab.dy[0],
+        run_chain_vol<T, K, kLast, PF, NB, C8>(a, tab.in, ring, ring + PF * vol_slot_words<K, NB>(), tab.dx[0], tab.dy[0],
                                            s, tab.nscan[0], nullptr);
         return;
     }
@@ -1091,6 +1133,10 @@ cudaError_t launch_first_tk(const SgmArgs& a, DirTable tab, bool census, cudaStr
         // one warp per block: chains of different lengths (directions) end independently
         const size_t smem = (size_t)first_pf<T>() * vol_slot_words<K, 0>() * 4;
         auto kern = sgm_first_kernel<T, K, false>;
+        if (a.cost8) {
+            if constexpr (T == 32 && K % 2 == 0) kern = sgm_first_kernel<T, K, false, true>;
+            else return cudaErrorInvalidValue;
+        }
         {
             const cudaError_t e = allow_dynamic_smem(kern, smem);
             if (e != cudaSuccess) return e;
@@ -1115,13 +1161,17 @@ cudaError_t launch_last_split(const SgmArgs& a, const DirTable& tab, cudaStream_
     constexpr int PFB = K <= 2 ? 8 : 4;
     const size_t smem = (size_t)SplitSmem<K, NB, PFA, PFB>::words * 4;
     auto kern = sgm_last_split_kernel<K, NB, PFA, PFB>;
+    if (a.cost8) {
+        if constexpr (K % 2 == 0) kern = sgm_last_split_kernel<K, NB, PFA, PFB, true>;
+        else return cudaErrorInvalidValue;
+    }
     cudaError_t e = allow_dynamic_smem(kern, smem);
     if (e != cudaSuccess) return e;
     // as many chains per SM as shared memory holds: ask for the largest shared-memory carveout
-    // (a hint the driver otherwise sizes to other limits), once per process
-    static const cudaError_t carve =
-        cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
-    if (carve != cudaSuccess) cudaGetLastError();
+    // (a hint the driver otherwise sizes to other limits)
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared) !=
+        cudaSuccess)
+        cudaGetLastError();
     kern<<<tab.nscan[0], 64, smem, st>>>(a, tab);
     return cudaGetLastError();
 }
@@ -1147,6 +1197,10 @@ cudaError_t launch_last_tk(const SgmArgs& a, DirTable tab, bool census, int spli
             /* one warp per block: shared memory is granted per chain, not per four */              \
             const size_t smem = (size_t)(last_pf<K, T, NB>() * vol_slot_words<K, NB>() + wta_buf_words<K, T>()) * 4; \
             auto kern = sgm_last_kernel<T, K, false, NB>;                                            \
+            if (a.cost8) {                                                                           \
+                if constexpr (T == 32 && K % 2 == 0) kern = sgm_last_kernel<T, K, false, NB, true>;  \
+                else return cudaErrorInvalidValue;                                                   \
+            }                                                                                        \
             {                                                                                        \
                 const cudaError_t e = allow_dynamic_smem(kern, smem);                                \
                 if (e != cudaSuccess) return e;                                                      \
@@ -1424,6 +1478,7 @@ SgmArgs make_args(const SgmLaunch& l) {
     a.sp_param = l.sp_param;
     a.sp_tel = l.sp_tel;
     a.store_final = l.store_final;
+    a.cost8 = l.cost8;
     return a;
 }
 

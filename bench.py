@@ -37,6 +37,7 @@ WORKLOADS = {
     "hq1080": (2, (1920, 1080, 256, 16, 0, 240, 0.2), "highquality_1920x1080_d256", {}),
     "hq720": (2, (1280, 720, 128, 12, 0, 120, 0.2), "highquality_1280x720_d128", {}),
     "balanced1080": (1, (1920, 1080, 256, 16, 0, 240, 0.0), "balanced_1920x1080_d256", {}),
+    "fast1080": (0, (1920, 1080, 256, 16, 0, 240, 0.0), "fast_1920x1080_d256", {}),
     "kitti1242": (1, (1242, 375, 192, 12, 0, 180, 0.0), "balanced_1242x375_d192", {}),
     # hierarchical coarse-to-fine search range (HierarchicalConfig defaults: R = 4, NearestValid)
     "balanced720_hier": (1, (1280, 720, 128, 12, 0, 120, 0.0), "balanced_1280x720_d128_hierarchical",

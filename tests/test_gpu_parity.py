@@ -31,6 +31,11 @@ def _cases():
         ("census9x7_fast_96x64", F, (96, 64, 32, 0), "synth", {"census_type": 0}, 0),
         ("path8_balanced_120x90_d40", B, (120, 90, 40, 0), "synth", {"paths": 8}, 0),
         ("fast_260x40_d200", F, (260, 40, 200, 0), "synth", {}, 0),
+        ("fast_333x90_d128", F, (333, 90, 128, 0), "synth", {}, 0),
+        # the one-byte Fast volume (a padded range of 256): a negative range, 8 paths
+        ("fast_300x64_d256", F, (300, 64, 256, 0), "synth", {}, 0),
+        ("fast_negative_120x60_d200_min_40", F, (120, 60, 200, -40), "synth", {}, 0),
+        ("fast_path8_150x80_d256", F, (150, 80, 256, 0), "synth", {"paths": 8}, 0),
         ("balanced_agg2_80x60", B, (80, 60, 24, 0), "synth", {"agg_iterations": 2}, 0),
         ("balanced_continuous_p2", B, (80, 60, 24, 0), "synth", {"piecewise_p2": 0}, 0),
         ("balanced_min8_max40", B, (120, 60, 40, 8), "synth", {}, 0),
@@ -128,6 +133,40 @@ def test_fast_fused_equals_unfused(apg, w, h, dmax):
     b = apg.Engine(cfg).process(L, R)
     for k in a:
         assert same_bits(a[k], b[k]), k
+
+
+@pytest.mark.parametrize("w,h,dmax,over", [
+    (333, 90, 128, {}), (300, 64, 256, {}), (97, 61, 100, {"min_disparity": -20}), (150, 80, 128, {"paths": 8}),
+    (64, 7, 120, {}), (150, 80, 128, {"sgm_split": 2}),
+])
+def test_cost8_changes_no_result(apg, w, h, dmax, over):
+    """The Fast volume at one byte per voxel (tuning cost8=2; the default at a padded range of 256)
+    and at two bytes (cost8=1) give identical maps and path sums, and the byte form takes half the
+    volume's bytes."""
+    L, R = synth(w, h, dmax, seed=29)
+    over = dict(over)
+    dmin = over.pop("min_disparity", 0)
+    split = over.pop("sgm_split", 0)
+    cfg = apg.config_from_mode(0, dmax, dmin, **over)
+    outs, sizes = [], []
+    for cost8 in (2, 1):
+        e = apg.Engine(cfg, debug=apg.DEBUG_KEEP_SUM)
+        e.set_tuning("cost8", cost8)
+        e.set_tuning("sgm_split", split)
+        o = e.process(L, R)
+        o["sgm_sum"] = e.dump("sgm_sum")
+        sizes.append(e.allocated_bytes)
+        e.close()
+        outs.append(o)
+    for k in outs[0]:
+        assert same_bits(outs[0][k], outs[1][k]), k
+    Dp = 128 if dmax - dmin <= 128 else 256
+    assert sizes[1] - sizes[0] >= w * h * Dp // 2
+    # the default: bytes at 256, two bytes at 128
+    e = apg.Engine(cfg, debug=apg.DEBUG_KEEP_SUM)
+    e.process(L, R)
+    assert e.allocated_bytes == sizes[0 if Dp == 256 else 1]
+    e.close()
 
 
 GOLDEN = {  # tests/test_api_contract.cpp:243-257 of the reference (w, h, invalid, reliable, disp, conf, inv, rel)

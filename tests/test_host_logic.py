@@ -190,6 +190,10 @@ def test_workspace_estimates():
     assert 4 * vol <= wf < 5 * vol      # Fast: the census cost volume and three first-phase path sums
     assert 4 * vol <= wb < 5 * vol      # Balanced: cross tmp (= first sum buffer), aggregated cost, 2 more sums
     assert apg.workspace_bytes(fast, 640, 480) < wf
+    # Fast at a padded range of 256: the census cost volume at one byte per voxel
+    w256 = apg.workspace_bytes(apg.config_from_mode(0, 256), 1920, 1080)
+    vol256 = 1920 * 1080 * 256 * 2
+    assert 3.5 * vol256 <= w256 < 4.5 * vol256
 
 
 def test_synthetic_generator_is_deterministic():
