@@ -55,6 +55,15 @@ namespace {
 constexpr uint32_t kInf = 0x7FFFu;
 constexpr uint32_t kInf2 = 0x7FFF7FFFu;
 
+// One step of the path recurrence per halfword, c + (b - m), as plain 32-bit arithmetic: every half
+// of b is at least m (b is a minimum over candidates that are each at least the previous step's
+// minimum m) and every result half stays below 0x10000 (costs are at most 0x7FFF and b - m at most
+// P2, which the configuration check keeps below 0x7FFF - P1), so no borrow or carry crosses the
+// halves and the result equals the per-halfword modular form.
+__device__ __forceinline__ uint32_t path_value(uint32_t c, uint32_t b, uint32_t m2) { return c + b - m2; }
+// Per-halfword unsigned saturating add: a + min(b, 0xFFFF - a) never carries out of a half.
+__device__ __forceinline__ uint32_t addus2(uint32_t a, uint32_t b) { return a + __vminu2(b, ~a); }
+
 enum Mode { kFirst = 0, kLast = 2 };
 constexpr int kMaxDirs = 8;
 
@@ -370,7 +379,7 @@ __device__ __forceinline__ void run_chain(const SgmArgs& a, const DirTable& tab,
                         const uint32_t lm = __byte_perm(lo_nb, L[k], 0x5432);  // (L[k] << 16) | (lo_nb >> 16)
                         const uint32_t lp = __byte_perm(L[k], hi_nb, 0x5432);  // (hi_nb << 16) | (L[k] >> 16)
                         const uint32_t b = __vminu2(L[k], __viaddmin_u16x2(__vminu2(lm, lp), p1x2, mp2));
-                        Ln[k] = __vadd2(c[k], __vsub2(b, m2));
+                        Ln[k] = path_value(c[k], b, m2);
                     }
 #pragma unroll
                     for (int k = 0; k < K; ++k) L[k] = Ln[k];
@@ -395,7 +404,7 @@ __device__ __forceinline__ void run_chain(const SgmArgs& a, const DirTable& tab,
                     for (int k = 0; k < K; ++k) {
                         uint32_t v = L[k];
 #pragma unroll
-                        for (int b = 0; b < NB; ++b) v = __vaddus2(v, sl.s[b][k]);
+                        for (int b = 0; b < NB; ++b) v = addus2(v, sl.s[b][k]);
                         sv[k] = v;
                     }
                     if (a.store_final) {
@@ -451,6 +460,7 @@ __device__ __forceinline__ void cp_async16(uint32_t* dst, const void* src) {
                  : "memory");
 }
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+
 template <int N>
 __device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
@@ -704,7 +714,7 @@ __device__ __forceinline__ void run_chain_vol(const SgmArgs& a, const uint32_t* 
                             const uint32_t lm = __byte_perm(lo_nb, L[k], 0x5432);
                             const uint32_t lp = __byte_perm(L[k], hi_nb, 0x5432);
                             const uint32_t b = __vminu2(L[k], __viaddmin_u16x2(__vminu2(lm, lp), p1x2, mp2));
-                            Ln[k] = __vadd2(c[k], __vsub2(b, m2));
+                            Ln[k] = path_value(c[k], b, m2);
                         }
 #pragma unroll
                         for (int k = 0; k < K; ++k) L[k] = Ln[k];
@@ -731,7 +741,7 @@ __device__ __forceinline__ void run_chain_vol(const SgmArgs& a, const uint32_t* 
                             uint32_t sb[K];
                             lds_words<K>(sl + 32 * K * (1 + b) + lane * K, sb);
 #pragma unroll
-                            for (int k = 0; k < K; ++k) sv[k] = __vaddus2(sv[k], sb[k]);
+                            for (int k = 0; k < K; ++k) sv[k] = addus2(sv[k], sb[k]);
                         }
                         if (a.store_final) {
                             uint32_t o[K];
@@ -894,7 +904,7 @@ __global__ void __launch_bounds__(64) sgm_last_split_kernel(SgmArgs a, DirTable 
                             const uint32_t lm = __byte_perm(lo_nb, L[k], 0x5432);
                             const uint32_t lp = __byte_perm(L[k], hi_nb, 0x5432);
                             const uint32_t b = __vminu2(L[k], __viaddmin_u16x2(__vminu2(lm, lp), p1x2, mp2));
-                            Ln[k] = __vadd2(c[k], __vsub2(b, m2));
+                            Ln[k] = path_value(c[k], b, m2);
                         }
 #pragma unroll
                         for (int k = 0; k < K; ++k) L[k] = Ln[k];
@@ -955,7 +965,7 @@ __global__ void __launch_bounds__(64) sgm_last_split_kernel(SgmArgs a, DirTable 
                         uint32_t sb[K];
                         lds_words<K>(sl + 32 * K * b + lane * K, sb);
 #pragma unroll
-                        for (int k = 0; k < K; ++k) sv[k] = __vaddus2(sv[k], sb[k]);
+                        for (int k = 0; k < K; ++k) sv[k] = addus2(sv[k], sb[k]);
                     }
                     if (a.store_final) {
                         uint32_t o[K];
@@ -1105,8 +1115,8 @@ __global__ void sgm_sum_kernel(uint4* __restrict__ dst, const uint4* __restrict_
 #pragma unroll
         for (int b = 0; b < 6; ++b) {
             const uint4 t = __ldcs(src[b] + i);
-            v.x = __vaddus2(v.x, t.x); v.y = __vaddus2(v.y, t.y);
-            v.z = __vaddus2(v.z, t.z); v.w = __vaddus2(v.w, t.w);
+            v.x = addus2(v.x, t.x); v.y = addus2(v.y, t.y);
+            v.z = addus2(v.z, t.z); v.w = addus2(v.w, t.w);
         }
         __stcg(dst + i, v);
     }
