@@ -4,10 +4,17 @@
 //
 // Vertical kernel: a CTA owns `cols` adjacent pixel columns x and a 256-row segment; each thread
 // owns one 32-bit word (two disparities) of one column and slides down the segment keeping the
-// column prefix sums (sum and count, 16-bit lanes) of the last 2*Lmax+2 rows in a shared-memory
-// ring, so every input voxel is read once (plus a 2*Lmax row halo per segment) and every output
+// column prefix sums (sum and count) of the last 2*Lmax+2 rows in a shared-memory ring, so every
+// input voxel is read once (plus a 2*Lmax row halo per segment) and every output
 // voxel is written once.  The up/down arms (build_cross_arms, :17-63) are computed once per
 // pixel into shared memory.  Bound: HBM, 4 bytes per voxel (read T, write C).
+//
+// Prefix sums are plain 32-bit running sums of the packed words (two disparities): a carry out of
+// the low half moves into the high half of the prefix, but a window's difference of two prefixes
+// is the 32-bit sum of the window's words, exact in both halves because the window's low halves
+// sum to less than 2^16: valid costs are host-checked ((2 * lmax + 1) * cost_max < 2^16), and an
+// invalid low half is either zeroed before it is added or, in the default-range kernel, sits only
+// below an invalid high half, whose window is never used.
 #include "common.cuh"
 #include "kernels.h"
 
@@ -64,8 +71,8 @@ __global__ void cross_v_kernel(int w, int h, int d0, int D, int Dp, int lmax, in
         while (r_next < need) {
             const uint32_t v = tin[((size_t)r_next * w + x) * W2 + k];
             const uint32_t inval = __vcmpeq2(v, kInvalidWord);
-            ps = __vadd2(ps, v & ~inval);
-            pc = __vadd2(pc, 0x00010001u & ~inval);
+            ps += v & ~inval;
+            pc += 0x00010001u & ~inval;
             ++r_next;
             const int slot = (r_next % RS) * nthr + tid;
             ring_s[slot] = ps;
@@ -73,8 +80,8 @@ __global__ void cross_v_kernel(int w, int h, int d0, int D, int Dp, int lmax, in
         }
         const int ai = ci * kSeg + (y - y0);
         const int a = y - armU[ai], b = y + armD[ai] + 1;
-        const uint32_t s = __vsub2(ring_s[(b % RS) * nthr + tid], ring_s[(a % RS) * nthr + tid]);
-        const uint32_t n = __vsub2(ring_c[(b % RS) * nthr + tid], ring_c[(a % RS) * nthr + tid]);
+        const uint32_t s = ring_s[(b % RS) * nthr + tid] - ring_s[(a % RS) * nthr + tid];
+        const uint32_t n = ring_c[(b % RS) * nthr + tid] - ring_c[(a % RS) * nthr + tid];
         const int lo = rmin[y * w + x], hi = rmax[y * w + x];
         uint32_t word = 0;
 #pragma unroll
@@ -93,7 +100,8 @@ __global__ void cross_v_kernel(int w, int h, int d0, int D, int Dp, int lmax, in
 // Vertical pass when every pixel has the default range [d0, min(dmax, x+1)) and d0 >= 0: then
 // T(x, y', d) is valid exactly when d <= x, for every row y', so the window count is the window
 // length and no count prefix is needed; lanes with d > x hold the invalid marker in every row and
-// their (wrapped) sums are never used.  Each thread keeps its column's prefix sums in a power-of-two shared
+// their (wrapped) sums are never used, and such a lane is never the low half of a word whose high
+// half is valid (d0 >= 0: validity only ends at the top of a pixel's range).  Each thread keeps its column's prefix sums in a power-of-two shared
 // ring and loads its input words kB rows at a time, one batch ahead of use (register double
 // buffer), so kB loads per thread are in flight; the gray column segment is staged in shared
 // memory for the arms.
@@ -172,7 +180,7 @@ __global__ void __launch_bounds__(128) cross_v_default_kernel(int w, int h, int 
 #pragma unroll
             for (int i = 0; i < kB; ++i) {
                 if (pushed + i < yend) {
-                    ps = __vadd2(ps, cur[i]);
+                    ps += cur[i];
                     ring[((pushed + i - ystart + 1) & (RS - 1)) * nthr + tid] = ps;
                 }
             }
@@ -190,8 +198,8 @@ __global__ void __launch_bounds__(128) cross_v_default_kernel(int w, int h, int 
             if (y >= y1) break;
             const int ai = ci * kSeg + (y - y0);
             const int a = y - armU[ai], b = y + armD[ai];  // inclusive window
-            const uint32_t sum = __vsub2(ring[((b - ystart + 1) & (RS - 1)) * nthr + tid],
-                                         ring[((a - ystart) & (RS - 1)) * nthr + tid]);
+            const uint32_t sum = ring[((b - ystart + 1) & (RS - 1)) * nthr + tid] -
+                                 ring[((a - ystart) & (RS - 1)) * nthr + tid];
             const int len = b - a + 1;
             const uint32_t mg = s_magic[len];
             uint32_t word = 0;
@@ -360,8 +368,8 @@ __global__ void cross_h_kernel(int w, int h, int d0, int D, int Dp, int lmax, in
         while (r_next < need) {
             const uint32_t v = vin[((size_t)y * w + r_next) * W2 + k];
             const uint32_t inval = __vcmpeq2(v, kInvalidWord);
-            ps = __vadd2(ps, v & ~inval);
-            pc = __vadd2(pc, 0x00010001u & ~inval);
+            ps += v & ~inval;
+            pc += 0x00010001u & ~inval;
             ++r_next;
             const int slot = (r_next % RS) * nthr + k;
             ring_s[slot] = ps;
@@ -372,8 +380,8 @@ __global__ void cross_h_kernel(int w, int h, int d0, int D, int Dp, int lmax, in
         while (l < lmax && x - l - 1 >= 0 && abs((int)g[x - l - 1] - c0) <= tau) ++l;
         while (r < lmax && x + r + 1 < w && abs((int)g[x + r + 1] - c0) <= tau) ++r;
         const int a = x - l, b = x + r + 1;
-        const uint32_t s = __vsub2(ring_s[(b % RS) * nthr + k], ring_s[(a % RS) * nthr + k]);
-        const uint32_t n = __vsub2(ring_c[(b % RS) * nthr + k], ring_c[(a % RS) * nthr + k]);
+        const uint32_t s = ring_s[(b % RS) * nthr + k] - ring_s[(a % RS) * nthr + k];
+        const uint32_t n = ring_c[(b % RS) * nthr + k] - ring_c[(a % RS) * nthr + k];
         const int lo = rmin[y * w + x], hi = rmax[y * w + x];
         uint32_t word = 0;
 #pragma unroll
