@@ -277,10 +277,13 @@ __device__ __forceinline__ void prefetch_l1(const void* p) {
 // counter and fences before reading the row above.
 __device__ __forceinline__ void fence_acq_rel() { asm volatile("fence.acq_rel.gpu;\n" ::: "memory"); }
 
+// The band kernel's copies into its rings carry no compiler memory clobber, so that the compiler
+// may interleave a step's copies with the step's dependent cost chain: a slot is written only by
+// copies issued after the cp.async.wait_group (which is a compiler barrier) that follows the
+// slot's last read, and read only after the wait_group that completes its copy.
 __device__ __forceinline__ void cp16(void* dst, const void* src) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
-                 "l"(src)
-                 : "memory");
+                 "l"(src));
 }
 
 // Shared state of one band's two warps.  The compute warp (warp 0) walks the band; the link warp
@@ -418,8 +421,7 @@ __global__ void __launch_bounds__(64) refine_band_kernel(CostCtx c, int fwd, con
         if ((unsigned)pe < (unsigned)w)
             asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(
                              (unsigned)__cvta_generic_to_shared(&s_win[pe & wmask])),
-                         "l"(rrow + pe)
-                         : "memory");
+                         "l"(rrow + pe));
     };
     // one cp.async group per step: this lane's record (and packed left pixel) of step t
     auto issue = [&](int t) {
@@ -435,8 +437,7 @@ __global__ void __launch_bounds__(64) refine_band_kernel(CostCtx c, int fwd, con
             } else {
                 asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(
                                  (unsigned)__cvta_generic_to_shared(&s_lpk[t % kRing][lane])),
-                             "l"(ls)
-                             : "memory");
+                             "l"(ls));
             }
         }
         // the window pixel entering at this column (also for the columns before the lane's first)
@@ -450,7 +451,7 @@ __global__ void __launch_bounds__(64) refine_band_kernel(CostCtx c, int fwd, con
         asm volatile("cp.async.commit_group;\n" ::: "memory");
     }
 #pragma unroll 1
-    for (int t = 0; t < kRing; ++t) issue(t);
+    for (int t = 0; t < kRing - 1; ++t) issue(t);
     // the right-image window a lane reads (its row, [x - dmax + 1, x - d0]) slides by one pixel
     // per step; every lane misses L1 at a different step and the warp waits for the slowest, so
     // the window's first kAhead steps are prefetched now and its entering edge kAhead steps ahead
@@ -487,7 +488,10 @@ __global__ void __launch_bounds__(64) refine_band_kernel(CostCtx c, int fwd, con
             }
             if (lane == 0) up_first = s_link.up[t & (kUpRing - 1)];
         }
-        asm volatile("cp.async.wait_group %0;\n" ::"n"(kRing - 1) : "memory");
+        // step t's copies have landed (kRing - 2 newer groups may be pending); slot (t - 1) % kRing
+        // was read in the previous step, so step t + kRing - 1 refills it now
+        asm volatile("cp.async.wait_group %0;\n" ::"n"(kRing - 2) : "memory");
+        issue(t + kRing - 1);
         if (!WIN && row_ok) prefetch_l1(rrow + min(max(pe, 0), w - 1));
         pe += xs;
         const float up_lane = __shfl_up_sync(0xffffffffu, prev, 1);
@@ -528,9 +532,6 @@ __global__ void __launch_bounds__(64) refine_band_kernel(CostCtx c, int fwd, con
             }
             prev = val;
         }
-        // the slot just read is refilled only after its record was copied out above
-        __syncwarp();
-        issue(t + kRing);
         if ((t % kPublish) == kPublish - 1) {
             // release to the link warp (CTA scope): how far the last row (lane 31, column t - 31)
             // is final, and that the ring's columns up to t are read
