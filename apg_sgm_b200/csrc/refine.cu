@@ -277,10 +277,9 @@ __device__ __forceinline__ void prefetch_l1(const void* p) {
 // counter and fences before reading the row above.
 __device__ __forceinline__ void fence_acq_rel() { asm volatile("fence.acq_rel.gpu;\n" ::: "memory"); }
 
-// The band kernel's copies into its rings carry no compiler memory clobber, so that the compiler
-// may interleave a step's copies with the step's dependent cost chain: a slot is written only by
-// copies issued after the cp.async.wait_group (which is a compiler barrier) that follows the
-// slot's last read, and read only after the wait_group that completes its copy.
+// The loader warp's copies into the step ring carry no compiler memory clobber: their order
+// against the compute warp's reads is set by the ring's mbarriers (a slot is refilled only after
+// the wait for its empty barrier, and read only after the wait for its full barrier).
 __device__ __forceinline__ void cp16(void* dst, const void* src) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
                  "l"(src));
@@ -371,20 +370,143 @@ __device__ void band_link(BandLink* s_link, int band, int w, int h, int fwd, con
     }
 }
 
+// ---- the band kernel's step ring: mbarriers between the loader warp and the compute warp
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t* b, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* b) {
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n}\n" ::"r"(smem_u32(b)) : "memory");
+}
+// arrives once every cp.async this thread issued before it has landed
+__device__ __forceinline__ void mbar_arrive_copies(uint64_t* b) {
+    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];\n" ::"r"(smem_u32(b)) : "memory");
+}
+__device__ __forceinline__ bool mbar_done(uint64_t* b, unsigned parity) {
+    unsigned ok;
+    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n}\n"
+                 : "=r"(ok)
+                 : "r"(smem_u32(b)), "r"(parity)
+                 : "memory");
+    return ok != 0;
+}
+// Waits, in every lane of the warp, for the completed phase `parity` of b; the warp leaves the
+// wait together.  False after `limit` polls (each followed by a sleep of `sleep_ns` when non-zero)
+// or once *stop is raised.
+__device__ __forceinline__ bool mbar_wait_warp(uint64_t* b, unsigned parity, int limit, const volatile int* stop,
+                                               int sleep_ns) {
+    for (int spins = 0;; ++spins) {
+        if (__all_sync(0xffffffffu, mbar_done(b, parity))) return true;
+        if (spins >= limit || (stop && *stop)) return false;
+        if (sleep_ns) __nanosleep(sleep_ns);
+    }
+}
+
+// Per-lane view of a band's row for one pass: pass-order column u of the lane's row is image
+// column xb + xs * u.
+template <bool C64>
+struct BandRow {
+    int lane, v, xs, xb, eoff;
+    bool ok;
+    const RStep* steps;       // this lane's records, pass order
+    const RPack<C64>* left;   // this lane's left pixels
+    const RPack<C64>* right;  // this lane's right-image row
+    float* work;
+    __device__ BandRow(const CostCtx& c, int band, int fwd, const RStep* all_steps, const RPack<C64>* lp,
+                       const RPack<C64>* rp, float* all_work) {
+        lane = threadIdx.x & 31;
+        v = band * kBand + lane;
+        ok = v < c.h;
+        xs = fwd ? 1 : -1;
+        xb = fwd ? 0 : c.w - 1;
+        const int yrow = fwd ? v : c.h - 1 - v;
+        const size_t rowoff = (size_t)(ok ? yrow : 0) * c.w;
+        steps = all_steps + (size_t)(ok ? v : 0) * c.w;
+        left = lp + rowoff;
+        right = rp + rowoff;
+        work = all_work + rowoff;
+        eoff = fwd ? c.d0 : c.d0 + c.D - 1;  // entering window pixel of column u: x(u) - eoff
+    }
+};
+
+// Shared memory of the band kernel besides the link state.
+template <bool C64>
+struct BandRing {
+    RStep rec[kRing][32];       // step t's records in slot t % kRing, one per lane
+    RPack<C64> lpk[kRing][32];  // and the lanes' packed left pixels
+    uint64_t full[kRing];       // slot filled (32 loader arrivals, each once its copies landed)
+    uint64_t empty[kRing];      // slot read (one arrival of the compute warp)
+    int stop;                   // the compute warp has stopped: the loader stops too
+};
+
+// The loader warp: copies step t's records, packed left pixels and (WIN) the window's entering
+// right-image pixels into slot t % kRing and signals full[slot] when they have landed, up to
+// kRing steps ahead of the compute warp, refilling a slot only once the compute warp has released
+// it.  Without WIN it keeps the right-image window warm in L1 instead: every lane misses L1 at a
+// different step and the compute warp waits for the slowest, so the window's first kAhead steps
+// are prefetched first and its entering edge kAhead steps ahead of the copies.
+template <bool C64, bool WIN>
+__device__ void band_loader(const CostCtx& c, const BandRow<C64>& r, BandRing<C64>* ring, RPack<C64>* s_win,
+                            int wmask, int spin_limit) {
+    const int w = c.w, lane = r.lane;
+    auto copy_win = [&](int u) {
+        const int pe = r.xb + r.xs * u - r.eoff;
+        if ((unsigned)pe < (unsigned)w)
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(smem_u32(&s_win[pe & wmask])),
+                         "l"(r.right + pe));
+    };
+    if (WIN && r.ok) {
+        // the rest of the window of the lane's first column: columns -(D - 1) .. -lane - 1
+        for (int u = -(c.D - 1); u < -lane; ++u) copy_win(u);
+    }
+    if (!WIN && r.ok) {
+        for (int k = -c.D; k <= kAhead; k += 8) prefetch_l1(r.right + min(max(r.xb + r.xs * k - r.eoff, 0), w - 1));
+    }
+    int pe = r.xb + r.xs * (kAhead - lane) - r.eoff;  // entering pixel kAhead steps ahead
+    const int nsteps = w + kBand - 1;
+    for (int t = 0; t < nsteps; ++t) {
+        const int slot = t % kRing;
+        if (t >= kRing &&
+            !mbar_wait_warp(&ring->empty[slot], ((t / kRing) - 1) & 1, spin_limit, &ring->stop, 64))
+            break;  // the compute warp stopped, or never released the slot: it fails the pass itself
+        const int u = t - lane;
+        if (r.ok && u >= 0 && u < w) {
+            const RStep* src = r.steps + u;
+            cp16(&ring->rec[slot][lane], src);
+            cp16(reinterpret_cast<unsigned char*>(&ring->rec[slot][lane]) + 16,
+                 reinterpret_cast<const unsigned char*>(src) + 16);
+            const RPack<C64>* ls = r.left + (r.xb + r.xs * u);
+            if constexpr (C64) {
+                cp16(&ring->lpk[slot][lane], ls);
+            } else {
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(smem_u32(&ring->lpk[slot][lane])),
+                             "l"(ls));
+            }
+        }
+        // the window pixel entering at this column (also for the columns before the lane's first)
+        if (WIN && r.ok && u < w) copy_win(u);
+        if (!WIN && r.ok) prefetch_l1(r.right + min(max(pe, 0), w - 1));
+        pe += r.xs;
+        mbar_arrive_copies(&ring->full[slot]);
+    }
+    // no copy may land after the block has left
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
 // WIN: each lane's right-image window ([x - dmax + 1, x - d0] of its row, sliding one pixel per
 // step) lives in shared memory, a ring of wmask + 1 records per lane (a power of two holding the
-// window plus the kRing steps copied ahead); every step copies the entering pixel with the step's
+// window plus the kRing steps copied ahead); the loader copies the entering pixel with the step's
 // record, so the candidates' right pixels are shared-memory loads.  Without WIN they are global
-// loads kept warm in L1 by prefetches.  Two warps per block: warp 0 computes, warp 1 links the
-// band to its neighbours (band_link).
+// loads kept warm in L1 by the loader's prefetches.  Three warps per block: warp 0 computes, warp 1
+// links the band to its neighbours (band_link), warp 2 loads the step ring (band_loader), so that
+// no copy or address arithmetic sits in the compute warp's step.
 template <bool C64, bool WIN>
-__global__ void __launch_bounds__(64) refine_band_kernel(CostCtx c, int fwd, const RStep* __restrict__ steps,
+__global__ void __launch_bounds__(96) refine_band_kernel(CostCtx c, int fwd, const RStep* __restrict__ steps,
                                                          const RPack<C64>* __restrict__ lp,
                                                          const RPack<C64>* __restrict__ rp, float* work,
                                                          int* progress, int* err, int spin_limit, int wmask) {
     __shared__ float s_lut[kLutSize];
-    __shared__ __align__(16) RStep s_ring[kRing][32];
-    __shared__ __align__(16) RPack<C64> s_lpk[kRing][32];
+    __shared__ __align__(16) BandRing<C64> s_ring;
     __shared__ BandLink s_link;
     for (int i = threadIdx.x; i < kLutSize; i += blockDim.x) s_lut[i] = c.lut[i];
     if (threadIdx.x == 0) {
@@ -392,95 +514,55 @@ __global__ void __launch_bounds__(64) refine_band_kernel(CostCtx c, int fwd, con
         s_link.used = 0;
         s_link.done = 0;
         s_link.abort = 0;
+        s_ring.stop = 0;
+        for (int i = 0; i < kRing; ++i) {
+            mbar_init(&s_ring.full[i], 32);
+            mbar_init(&s_ring.empty[i], 1);
+        }
     }
     __syncthreads();
     const int band = blockIdx.x;
-    const int w = c.w, h = c.h;
-    if (threadIdx.x >= 32) {
-        band_link(&s_link, band, w, h, fwd, work, progress, err, spin_limit);
+    const int w = c.w;
+    const int warp = threadIdx.x >> 5;
+    if (warp == 1) {
+        band_link(&s_link, band, w, c.h, fwd, work, progress, err, spin_limit);
+        return;
+    }
+    const BandRow<C64> r(c, band, fwd, steps, lp, rp, work);
+    extern __shared__ __align__(16) unsigned char s_dyn[];
+    RPack<C64>* s_win = reinterpret_cast<RPack<C64>*>(s_dyn) + r.lane * (wmask + 2);  // one record of padding
+    if (warp == 2) {
+        band_loader<C64, WIN>(c, r, &s_ring, s_win, wmask, spin_limit);
         return;
     }
     volatile BandLink* link = &s_link;
-    const int lane = threadIdx.x;
-    const int v = band * kBand + lane;  // pass-order row of this lane
-    const bool row_ok = v < h;
-    // pass-order column u of this lane's row is image column x = xb + xs * u
-    const int xs = fwd ? 1 : -1, xb = fwd ? 0 : w - 1;
-    const int yrow = fwd ? v : h - 1 - v;
-    const size_t rowoff = (size_t)(row_ok ? yrow : 0) * w;
-    const RStep* srow = steps + (size_t)(row_ok ? v : 0) * w;  // this lane's records, pass order
-    const RPack<C64>* lrow = lp + rowoff;                       // this lane's left pixels
-    const RPack<C64>* rrow = rp + rowoff;                       // this lane's right-image row
-    float* wrow = work + rowoff;
-    const int d0 = c.d0, dmax = c.d0 + c.D;
-    const int eoff = fwd ? d0 : dmax - 1;  // entering window pixel of column u: x(u) - eoff
-    extern __shared__ __align__(16) unsigned char s_dyn[];
-    RPack<C64>* s_win = reinterpret_cast<RPack<C64>*>(s_dyn) + lane * (wmask + 2);  // one record of padding
-    auto copy_win = [&](int u) {
-        const int pe = xb + xs * u - eoff;
-        if ((unsigned)pe < (unsigned)w)
-            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(
-                             (unsigned)__cvta_generic_to_shared(&s_win[pe & wmask])),
-                         "l"(rrow + pe));
-    };
-    // one cp.async group per step: this lane's record (and packed left pixel) of step t
-    auto issue = [&](int t) {
-        const int u = t - lane;
-        if (row_ok && u >= 0 && u < w) {
-            const RStep* src = srow + u;
-            cp16(&s_ring[t % kRing][lane], src);
-            cp16(reinterpret_cast<unsigned char*>(&s_ring[t % kRing][lane]) + 16,
-                 reinterpret_cast<const unsigned char*>(src) + 16);
-            const RPack<C64>* ls = lrow + (xb + xs * u);
-            if constexpr (C64) {
-                cp16(&s_lpk[t % kRing][lane], ls);
-            } else {
-                asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(
-                                 (unsigned)__cvta_generic_to_shared(&s_lpk[t % kRing][lane])),
-                             "l"(ls));
-            }
-        }
-        // the window pixel entering at this column (also for the columns before the lane's first)
-        if (WIN && row_ok && u < w) copy_win(u);
-        asm volatile("cp.async.commit_group;\n" ::: "memory");
-    };
-    if constexpr (WIN) {
-        // the rest of the window of the lane's first column: columns -(D - 1) .. -lane - 1
-        if (row_ok)
-            for (int u = -(c.D - 1); u < -lane; ++u) copy_win(u);
-        asm volatile("cp.async.commit_group;\n" ::: "memory");
-    }
-#pragma unroll 1
-    for (int t = 0; t < kRing - 1; ++t) issue(t);
-    // the right-image window a lane reads (its row, [x - dmax + 1, x - d0]) slides by one pixel
-    // per step; every lane misses L1 at a different step and the warp waits for the slowest, so
-    // the window's first kAhead steps are prefetched now and its entering edge kAhead steps ahead
-    if (!WIN && row_ok) {
-        for (int k = -c.D; k <= kAhead; k += 8) {
-            const int xr = min(max(xb + xs * k - eoff, 0), w - 1);
-            prefetch_l1(rrow + xr);
-        }
-    }
-    int pe = xb + xs * (kAhead - lane) - eoff;  // entering pixel kAhead steps ahead of step t = 0
+    const int lane = r.lane, v = r.v;
+    const bool row_ok = r.ok;
+    float* wrow = r.work;
+    const RPack<C64>* rrow = r.right;
     float prev = -1.f;  // value of this lane's previous column (its left neighbour)
     int avail = band > 0 ? 0 : w;  // columns of the row above known to be in the link's ring
     bool abort = false;
-    for (int t = 0; t < w + kBand - 1 && !abort; ++t) {
+    for (int t = 0; t < w + kBand - 1; ++t) {
         float up_first = -1.f;  // the row above at column t (lane 0's up neighbour)
         if (band > 0 && t < w) {
             if (t >= avail) {
-                // wait until the link warp has the row above at least up to column t
-                int spins = 0;
+                // wait until the link warp has the row above at least up to column t (lane 0
+                // polls, so that the warp decides together)
+                int spins = 0, state = 0;  // 1: available, 2: gave up
                 for (;;) {
-                    avail = link->avail;
-                    if (avail > t) break;
-                    if (link->abort || ++spins > spin_limit) {
-                        abort = true;
-                        break;
+                    if (lane == 0) {
+                        const int a = link->avail;
+                        state = a > t ? 1 : ((link->abort || ++spins > spin_limit) ? 2 : 0);
+                        if (state == 1) avail = a;
                     }
+                    state = __shfl_sync(0xffffffffu, state, 0);
+                    if (state) break;
                     __nanosleep(32);
                 }
-                if (abort) {
+                avail = __shfl_sync(0xffffffffu, avail, 0);
+                if (state == 2) {
+                    abort = true;
                     if (lane == 0) atomicExch(err, 1);
                     break;
                 }
@@ -488,23 +570,24 @@ __global__ void __launch_bounds__(64) refine_band_kernel(CostCtx c, int fwd, con
             }
             if (lane == 0) up_first = s_link.up[t & (kUpRing - 1)];
         }
-        // step t's copies have landed (kRing - 2 newer groups may be pending); slot (t - 1) % kRing
-        // was read in the previous step, so step t + kRing - 1 refills it now
-        asm volatile("cp.async.wait_group %0;\n" ::"n"(kRing - 2) : "memory");
-        issue(t + kRing - 1);
-        if (!WIN && row_ok) prefetch_l1(rrow + min(max(pe, 0), w - 1));
-        pe += xs;
+        // step t's slot has landed
+        const int slot = t % kRing;
+        if (!mbar_wait_warp(&s_ring.full[slot], (t / kRing) & 1, spin_limit, nullptr, 0)) {
+            abort = true;
+            if (lane == 0) atomicExch(err, 1);
+            break;
+        }
         const float up_lane = __shfl_up_sync(0xffffffffu, prev, 1);
         const int u = t - lane;
         if (row_ok && u >= 0 && u < w) {
-            const RStep st = s_ring[t % kRing][lane];
+            const RStep st = s_ring.rec[slot][lane];
             float val = st.cur;
             if (st.upd & 1) {
-                const int x = xb + xs * u;
+                const int x = r.xb + r.xs * u;
                 const int lo = (int)(short)(st.range & 0xFFFF), hi = st.range >> 16;
                 const int d_cur = (int)(short)(st.d_pack & 0xFFFF), d_draw = st.d_pack >> 16;
                 const bool has_cur = (st.upd & 2) != 0, has_draw = (st.upd & 4) != 0;
-                const RPack<C64> l = s_lpk[t % kRing][lane];
+                const RPack<C64> l = s_ring.lpk[slot][lane];
                 // dynamic candidates: left (forward) / right (backward) and up / down
                 float left = -1.f, up = -1.f;
                 if (u > 0) left = prev;
@@ -532,6 +615,9 @@ __global__ void __launch_bounds__(64) refine_band_kernel(CostCtx c, int fwd, con
             }
             prev = val;
         }
+        // every lane has read the slot (and its window pixels): the loader may refill it
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&s_ring.empty[slot]);
         if ((t % kPublish) == kPublish - 1) {
             // release to the link warp (CTA scope): how far the last row (lane 31, column t - 31)
             // is final, and that the ring's columns up to t are read
@@ -540,7 +626,7 @@ __global__ void __launch_bounds__(64) refine_band_kernel(CostCtx c, int fwd, con
             if (lane == 0) link->used = min(t + 1, w);
         }
     }
-    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    if (abort) *(volatile int*)&s_ring.stop = 1;
     __syncwarp();
     __threadfence_block();
     // the whole band is final (or the pass was abandoned: let the next band finish)
@@ -721,7 +807,7 @@ cudaError_t launch_refine_pass(const CostCtx& c, const Layout& L, unsigned char*
             int per_sm = 0, dev = 0, nsm = 0;
             if (cudaGetDevice(&dev) == cudaSuccess &&
                 cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
-                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, wk, 2 * kBand, bytes) == cudaSuccess &&
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, wk, 3 * kBand, bytes) == cudaSuccess &&
                 per_sm * nsm >= nbands) {
                 wmask = rs - 1;
                 wbytes = bytes;
@@ -732,7 +818,7 @@ cudaError_t launch_refine_pass(const CostCtx& c, const Layout& L, unsigned char*
     }
     void* args[] = {&cc, &fwd_arg, (void*)&csteps, (void*)&lpk, (void*)&rpk, &work, &progress, &err, &spin_limit,
                     &wmask};
-    e = cudaLaunchCooperativeKernel(kern, dim3(nbands), dim3(2 * kBand), args, wbytes, s);
+    e = cudaLaunchCooperativeKernel(kern, dim3(nbands), dim3(3 * kBand), args, wbytes, s);
     if (e != cudaSuccess) return e;
     ++*launches;
     // start of the next pass, and cleared progress counters
