@@ -25,6 +25,23 @@ namespace apgcu {
 namespace {
 constexpr int kSeg = 256;
 
+// Stores the word (two aggregated costs) at word index i of the output volume: as is, or (U8) as
+// two bytes of the byte volume, whose pixel slices hold Dp bytes: every valid aggregated cost is
+// below 255 (host-checked), and the invalid 0xFFFF keeps its low byte 0xFF as the marker.
+template <bool U8, bool STREAM>
+__device__ __forceinline__ void store_cost_word(uint32_t* out, size_t i, uint32_t word) {
+    if constexpr (U8) {
+        unsigned short* o = reinterpret_cast<unsigned short*>(out) + i;
+        const unsigned short b = (unsigned short)__byte_perm(word, 0u, 0x0020);  // bytes 0 and 2
+        if constexpr (STREAM) __stcs(o, b);
+        else *o = b;
+    } else {
+        if constexpr (STREAM) __stcs(out + i, word);
+        else out[i] = word;
+    }
+}
+
+template <bool U8>
 __global__ void cross_v_kernel(int w, int h, int d0, int D, int Dp, int lmax, int tau, int cols,
                                const uint8_t* __restrict__ gray, const int16_t* __restrict__ rmin,
                                const int16_t* __restrict__ rmax, const uint32_t* __restrict__ tin,
@@ -93,7 +110,7 @@ __global__ void cross_v_kernel(int w, int h, int d0, int D, int Dp, int lmax, in
             if (di < D && d >= lo && d < hi && nh > 0) q = div_by_magic(sh, nh, magic[nh]);
             word |= q << (16 * hs);
         }
-        cout[((size_t)y * w + x) * W2 + k] = word;
+        store_cost_word<U8, false>(cout, ((size_t)y * w + x) * W2 + k, word);
     }
 }
 
@@ -108,7 +125,7 @@ __global__ void cross_v_kernel(int w, int h, int d0, int D, int Dp, int lmax, in
 constexpr int kB = 16;
 constexpr int kQ = 8;  // output rows computed together (independent windows: their loads overlap)
 
-template <int RS>
+template <int RS, bool U8>
 __global__ void __launch_bounds__(128) cross_v_default_kernel(int w, int h, int d0, int D, int Dp, int lmax, int tau,
                                                               int cols, const uint8_t* __restrict__ gray,
                                                               const uint32_t* __restrict__ tin,
@@ -171,7 +188,7 @@ __global__ void __launch_bounds__(128) cross_v_default_kernel(int w, int h, int 
     for (int i = 0; i < kB; ++i) nxt[i] = ystart + kB + i < yend ? __ldcs(src + (kB + i) * rowstride) : 0u;
     int pushed = ystart;  // next row to add to the ring
     uint32_t ps = 0;
-    uint32_t* dst = cout + ((size_t)y0 * w + x) * W2 + k;
+    size_t dst = ((size_t)y0 * w + x) * W2 + k;  // word index of (x, y0), lane k
     for (int yb = y0; yb < y1; yb += kQ) {
         // prefixes up to the last window of the chunk's rows, then kQ independent rows
         const int need = min(h, min(yb + kQ, y1) + lmax);
@@ -209,7 +226,7 @@ __global__ void __launch_bounds__(128) cross_v_default_kernel(int w, int h, int 
                 const uint32_t q = lane_ok[hs] ? div_by_magic(sh, (uint32_t)len, mg) : kInvalidCost;
                 word |= q << (16 * hs);
             }
-            __stcs(dst + (size_t)i * rowstride, word);
+            store_cost_word<U8, true>(cout, dst + (size_t)i * rowstride, word);
         }
         dst += (size_t)kQ * rowstride;
     }
@@ -221,7 +238,7 @@ __global__ void __launch_bounds__(128) cross_v_default_kernel(int w, int h, int 
 // sums of (valid low half) | (valid high half) << 8: a window difference is exact in every lane
 // because a window's sum is below 2^16 (host-checked for the arm length and cost_max) and its
 // counts are at most 2*lmax + 1 <= 255.  The centre pixel's range is staged with the arms.
-template <int RS, int KB>
+template <int RS, int KB, bool U8>
 __global__ void __launch_bounds__(256) cross_v_count_kernel(int w, int h, int d0, int D, int Dp, int lmax, int tau,
                                                             int cols, const uint8_t* __restrict__ gray,
                                                             const int16_t* __restrict__ rmin,
@@ -288,7 +305,7 @@ __global__ void __launch_bounds__(256) cross_v_count_kernel(int w, int h, int d0
     int pushed = ystart;
     uint32_t ps = 0;
     uint32_t pc = 0;  // low 16 bits used
-    uint32_t* dst = cout + ((size_t)y0 * w + x) * W2 + k;
+    size_t dst = ((size_t)y0 * w + x) * W2 + k;  // word index of (x, y0), lane k
     for (int yb = y0; yb < y1; yb += kQ) {
         const int need = min(h, min(yb + kQ, y1) + lmax);
         while (pushed < need) {
@@ -334,7 +351,7 @@ __global__ void __launch_bounds__(256) cross_v_count_kernel(int w, int h, int d0
                 if (di < D && d >= lo && d < hi && nh > 0) q = div_by_magic(sh, nh, s_magic[nh]);
                 word |= q << (16 * hs);
             }
-            __stcs(dst + (size_t)i * rowstride, word);
+            store_cost_word<U8, true>(cout, dst + (size_t)i * rowstride, word);
         }
         dst += (size_t)kQ * rowstride;
     }
@@ -396,11 +413,10 @@ __global__ void cross_h_kernel(int w, int h, int d0, int D, int Dp, int lmax, in
         vout[((size_t)y * w + x) * W2 + k] = word;
     }
 }
-}  // namespace
-
-cudaError_t launch_cross_v(int w, int h, int d0, int D, int Dp, int lmax, int tau, const uint8_t* gray,
-                           const int16_t* rmin, const int16_t* rmax, const uint32_t* tin, uint32_t* cout,
-                           const uint32_t* magic, bool default_ranges, cudaStream_t s) {
+template <bool U8>
+cudaError_t launch_cross_v_t(int w, int h, int d0, int D, int Dp, int lmax, int tau, const uint8_t* gray,
+                             const int16_t* rmin, const int16_t* rmax, const uint32_t* tin, uint32_t* cout,
+                             const uint32_t* magic, bool default_ranges, cudaStream_t s) {
     const int W2 = Dp / 2;
     const int cols = W2 >= 128 ? 1 : 128 / W2;
     const int nthr = W2 * cols;
@@ -414,7 +430,7 @@ cudaError_t launch_cross_v(int w, int h, int d0, int D, int Dp, int lmax, int ta
         auto go = [&](auto rs_tag) -> cudaError_t {
             constexpr int RS = decltype(rs_tag)::value;
             const size_t smem = (size_t)RS * nthr * 4 + extra;
-            auto kern = cross_v_default_kernel<RS>;
+            auto kern = cross_v_default_kernel<RS, U8>;
             {
                 const cudaError_t e = allow_dynamic_smem(kern, smem);
                 if (e != cudaSuccess) return e;
@@ -435,7 +451,7 @@ cudaError_t launch_cross_v(int w, int h, int d0, int D, int Dp, int lmax, int ta
             constexpr int RS = decltype(rs_tag)::value;
             constexpr int KB = decltype(kb_tag)::value;
             const size_t smem = (size_t)RS * nthr * 6 + extra;
-            auto kern = cross_v_count_kernel<RS, KB>;
+            auto kern = cross_v_count_kernel<RS, KB, U8>;
             {
                 const cudaError_t e = allow_dynamic_smem(kern, smem);
                 if (e != cudaSuccess) return e;
@@ -457,13 +473,22 @@ cudaError_t launch_cross_v(int w, int h, int d0, int D, int Dp, int lmax, int ta
     const int RS = 2 * lmax + 2;
     const size_t smem = (size_t)RS * nthr * 8 + (size_t)cols * kSeg * 2;
     {
-        const cudaError_t e = allow_dynamic_smem(cross_v_kernel, smem);
+        const cudaError_t e = allow_dynamic_smem(cross_v_kernel<U8>, smem);
         if (e != cudaSuccess) return e;
     }
     dim3 grid((w + cols - 1) / cols, (h + kSeg - 1) / kSeg);
-    cross_v_kernel<<<grid, round_up(nthr, 32), smem, s>>>(w, h, d0, D, Dp, lmax, tau, cols, gray, rmin, rmax,
-                                                          tin, cout, magic);
+    cross_v_kernel<U8><<<grid, round_up(nthr, 32), smem, s>>>(w, h, d0, D, Dp, lmax, tau, cols, gray, rmin, rmax,
+                                                              tin, cout, magic);
     return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t launch_cross_v(int w, int h, int d0, int D, int Dp, int lmax, int tau, const uint8_t* gray,
+                           const int16_t* rmin, const int16_t* rmax, const uint32_t* tin, uint32_t* cout,
+                           const uint32_t* magic, bool default_ranges, bool out8, cudaStream_t s) {
+    if (out8) return launch_cross_v_t<true>(w, h, d0, D, Dp, lmax, tau, gray, rmin, rmax, tin, cout, magic, default_ranges, s);
+    return launch_cross_v_t<false>(w, h, d0, D, Dp, lmax, tau, gray, rmin, rmax, tin, cout, magic, default_ranges, s);
 }
 
 cudaError_t launch_cross_h(int w, int h, int d0, int D, int Dp, int lmax, int tau, const uint8_t* gray,

@@ -170,6 +170,22 @@ static int max_census_cost(const apg_pipeline_config_t& c) {
     return m;
 }
 
+// An upper bound of every quantised cost with AD and gradient terms: the cost kernels add the
+// census, AD and gradient tables (each non-decreasing in its index) at most at their largest
+// entries, then scale and round; computed in double with a margin over the kernels' float steps.
+static int max_full_cost(const apg_pipeline_config_t& c) {
+    if (!c.use_ad && !c.use_grad) return max_census_cost(c);
+    if (c.eta_ad < 0.f || c.mu_grad < 0.f) return c.cost_max;
+    const double lc = std::max(c.lambda_census, 1e-3f), la = std::max(c.lambda_ad, 1e-3f),
+                 lg = std::max(c.lambda_grad, 1e-3f);
+    double v = 1.0 - std::exp(-64.0 / lc);
+    if (c.use_ad) v += c.eta_ad * (1.0 - std::exp(-255.0 / la));
+    if (c.use_grad) v += c.mu_grad * (1.0 - std::exp(-510.0 / lg));
+    const float norm = 1.f + (c.use_ad ? c.eta_ad : 0.f) + (c.use_grad ? c.mu_grad : 0.f);
+    const double scale = (double)c.cost_max / std::max(norm, 1e-6f);
+    return std::min((int)(v * scale + 0.5 + 1e-3), c.cost_max);
+}
+
 Layout Engine::make_layout(const apg_pipeline_config_t& c, int w, int h, int ch, int debug) {
     Layout L;
     L.w = w; L.h = h; L.ch = ch;
@@ -188,9 +204,14 @@ Layout Engine::make_layout(const apg_pipeline_config_t& c, int w, int h, int ch,
     // vs 2.83 ms per frame (first phase 0.96 vs 1.20 ms).  At 128 only on request (kLayoutCost8):
     // Fast 1280x720 D128 0.757 vs 0.749 ms, the first phase's chains there wait on the latency of
     // each step (widening the bytes) more than on the volume's bytes.  kLayoutCost16 keeps two bytes.
-    L.cost8 = !L.cross && !L.fused_fast && c.census_type == APG_CENSUS_SYMMETRIC_9X7 && !c.use_ad && !c.use_grad &&
-              !c.prior_enable && !c.hier_enable && (L.Dp == 256 || (L.Dp == 128 && (debug & kLayoutCost8))) &&
-              !(debug & kLayoutCost16) && max_census_cost(c) < 255;
+    // The same holds for the aggregated volume of Balanced / HighQuality (one aggregation pass),
+    // written by the vertical aggregation: aggregated costs are window averages of quantised costs,
+    // so below 255 when every quantised cost is.
+    const bool fast8 = !L.cross && !L.fused_fast && c.census_type == APG_CENSUS_SYMMETRIC_9X7 && !c.use_ad &&
+                       !c.use_grad && !c.prior_enable && !c.hier_enable && max_census_cost(c) < 255;
+    const bool cross8 = L.cross && c.agg_iterations <= 1 && max_full_cost(c) < 255;
+    L.cost8 = (fast8 || cross8) && (L.Dp == 256 || (L.Dp == 128 && (debug & kLayoutCost8))) &&
+              !(debug & kLayoutCost16);
     const size_t n = (size_t)w * h;
     const size_t csz = c.census_type == APG_CENSUS_9X7 ? 8 : 4;
     const size_t vol = n * (size_t)L.Dp * 2;
@@ -210,8 +231,8 @@ Layout Engine::make_layout(const apg_pipeline_config_t& c, int w, int h, int ch,
     // volA: cross-H output T (Balanced/HQ), raw cost (Fast without fusion) or the first path-sum
     // buffer (fused Fast); volB: aggregated cost.  The first SGM phase writes one buffer per
     // direction (3 for Path4, 7 for Path8); buffer 0 reuses volA whenever volA is dead by then.
-    L.volA = take(L.cost8 ? vol / 2 : vol);
-    L.volB = L.cross ? take(vol) : 0;
+    L.volA = take(L.cost8 && !L.cross ? vol / 2 : vol);
+    L.volB = L.cross ? take(L.cost8 ? vol / 2 : vol) : 0;
     L.nsbuf = (c.paths == 8 ? 8 : 4) - 1;
     for (int i = 0; i < L.nsbuf; ++i) L.sbuf[i] = (i == 0 && (L.cross || L.fused_fast)) ? L.volA : take(vol);
     L.volRaw = L.raw_cost ? take(vol) : 0;
@@ -379,8 +400,10 @@ int Engine::prepare(int w, int h, int ch) {
 }
 
 int Engine::prepare_arena(int w, int h, int ch) {
-    // the byte volume needs the pixel-run cost kernel and 32-lane sweeps
-    const bool cost16 = cost8_ == 1 || cost_kernel_ == 1 || (sgm_lanes_ != 0 && sgm_lanes_ != 32);
+    // the byte volume needs 32-lane sweeps, and in Fast mode the pixel-run cost kernel (which
+    // writes it; the vertical aggregation writes it otherwise)
+    const bool cost16 =
+        cost8_ == 1 || (!cfg_.agg_enable && cost_kernel_ == 1) || (sgm_lanes_ != 0 && sgm_lanes_ != 32);
     const Layout L = make_layout(cfg_, w, h, ch,
                                  debug_ | (fast_fused_ ? kLayoutFastFused : 0) | (cost16 ? kLayoutCost16 : 0) |
                                      (cost8_ == 2 ? kLayoutCost8 : 0));
@@ -703,13 +726,13 @@ int Engine::run_pre(const uint8_t* dl, int lstride, const uint8_t* dr, int rstri
     if (L.cross) {
         const int tau = cfg_.color_threshold;
         RUN(launch_cross_v(w, h, d0, D, Dp, lmax, tau, ptr<uint8_t>(L.lgray), ptr<int16_t>(L.rmin), ptr<int16_t>(L.rmax),
-                           ptr<uint32_t>(L.volA), ptr<uint32_t>(L.volB), magic, !ranged(), s), "crossV");
+                           ptr<uint32_t>(L.volA), ptr<uint32_t>(L.volB), magic, !ranged(), L.cost8, s), "crossV");
         const int iters = std::max(1, cfg_.agg_iterations);
         for (int it = 1; it < iters; ++it) {
             RUN(launch_cross_h(w, h, d0, D, Dp, lmax, tau, ptr<uint8_t>(L.lgray), ptr<int16_t>(L.rmin), ptr<int16_t>(L.rmax),
                                ptr<uint32_t>(L.volB), ptr<uint32_t>(L.volA), magic, s), "crossH");
             RUN(launch_cross_v(w, h, d0, D, Dp, lmax, tau, ptr<uint8_t>(L.lgray), ptr<int16_t>(L.rmin), ptr<int16_t>(L.rmax),
-                               ptr<uint32_t>(L.volA), ptr<uint32_t>(L.volB), magic, !ranged(), s), "crossV");
+                               ptr<uint32_t>(L.volA), ptr<uint32_t>(L.volB), magic, !ranged(), false, s), "crossV");
         }
         sgm_src = ptr<uint32_t>(L.volB);
     }
@@ -738,7 +761,7 @@ int Engine::sgm_launch(SgmLaunch* out, uint32_t** sbufs) const {
     pl.store_final = (debug_ & 2) != 0;
     pl.lanes = sgm_lanes_;
     pl.split = sgm_split_;
-    pl.cost8 = (!L.cross && !L.fused_fast && L.cost8) ? 1 : 0;
+    pl.cost8 = (!L.fused_fast && L.cost8) ? 1 : 0;
     for (int i = 0; i < L.nsbuf; ++i) sbufs[i] = ptr<uint32_t>(L.sbuf[i]);
     return L.nsbuf;
 }
@@ -1153,7 +1176,7 @@ int Engine::dump(int what, void* dst, size_t bytes) {
     const size_t n = (size_t)L.w * L.h;
     const size_t csz = cfg_.census_type == APG_CENSUS_9X7 ? 8 : 4;
     size_t off = 0, sz = 0;
-    bool vol = false;
+    bool vol = false, vol8 = false;
     switch (what) {
         case 0: off = L.lgray; sz = n; break;
         case 1: off = L.lgx; sz = n; break;
@@ -1176,7 +1199,12 @@ int Engine::dump(int what, void* dst, size_t bytes) {
             }
             break;
         case 10: if (!L.raw_cost) return fail(kInternalError, "raw cost not materialised"); off = L.volRaw; vol = true; break;
-        case 11: if (!L.cross) return fail(kInternalError, "no aggregated volume"); off = L.volB; vol = true; break;
+        case 11:
+            if (!L.cross) return fail(kInternalError, "no aggregated volume");
+            off = L.volB;
+            vol = true;
+            vol8 = L.cost8;
+            break;
         case 12: if (!(debug_ & 2)) return fail(kInternalError, "path sum not kept"); off = L.sbuf[0]; vol = true; break;
         case 13: off = L.disp_wta; sz = n * 4; break;
         case 14: off = L.best; sz = n * 4; break;
@@ -1197,7 +1225,17 @@ int Engine::dump(int what, void* dst, size_t bytes) {
     if (vol) {
         // strip the disparity padding: D u16 of every Dp-long pixel run
         if (bytes < n * L.D * 2) return fail(kInternalError, "dump buffer too small");
-        e = cudaMemcpy2DAsync(dst, L.D * 2, arena_ + off, L.Dp * 2, L.D * 2, n, cudaMemcpyDeviceToHost, stream_);
+        if (vol8) {
+            // the byte volume, widened on the host (0xFF -> the invalid 0xFFFF)
+            std::vector<uint8_t> tmp(n * L.D);
+            e = cudaMemcpy2DAsync(tmp.data(), L.D, arena_ + off, L.Dp, L.D, n, cudaMemcpyDeviceToHost, stream_);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+            uint16_t* o = static_cast<uint16_t*>(dst);
+            if (e == cudaSuccess)
+                for (size_t i = 0; i < tmp.size(); ++i) o[i] = tmp[i] == 0xFF ? 0xFFFF : tmp[i];
+        } else {
+            e = cudaMemcpy2DAsync(dst, L.D * 2, arena_ + off, L.Dp * 2, L.D * 2, n, cudaMemcpyDeviceToHost, stream_);
+        }
     } else {
         if (bytes < sz) return fail(kInternalError, "dump buffer too small");
         e = cudaMemcpyAsync(dst, arena_ + off, sz, cudaMemcpyDeviceToHost, stream_);

@@ -44,10 +44,11 @@ cudaError_t launch_hier_range(const apg_pipeline_config_t& c, int w, int h, cons
                               const float* coarse_conf, int16_t* rmin, int16_t* rmax, float* d_prior,
                               unsigned long long* counts, cudaStream_t s);
 
-// cross.cu
+// cross.cu.  out8: cout is the byte volume (Dp bytes per pixel, 0xFF invalid; every valid
+// aggregated cost below 255).
 cudaError_t launch_cross_v(int w, int h, int d0, int D, int Dp, int lmax, int tau, const uint8_t* gray,
                            const int16_t* rmin, const int16_t* rmax, const uint32_t* tin, uint32_t* cout,
-                           const uint32_t* magic, bool default_ranges, cudaStream_t s);
+                           const uint32_t* magic, bool default_ranges, bool out8, cudaStream_t s);
 cudaError_t launch_cross_h(int w, int h, int d0, int D, int Dp, int lmax, int tau, const uint8_t* gray,
                            const int16_t* rmin, const int16_t* rmax, const uint32_t* vin, uint32_t* vout,
                            const uint32_t* magic, cudaStream_t s);

@@ -68,9 +68,10 @@ APGCU_API int apgcu_engine_set_debug(apgcu_engine_t e, int flags);
  *   "fast_fused": 1 = census-only Fast mode recomputes its costs inside the SGM sweeps and stores no
  *                 cost volume (less memory, slower); 0 = store the volume once (default);
  *   "cost_kernel": 0 = pixel-run cost kernel where it applies (default), 1 = column-tile kernel;
- *   "cost8": census-only Fast volume at one byte per voxel (0xFF invalid; exact while every
- *            quantised cost is below 255): 0 = at 256 padded disparities (default), 1 = never,
- *            2 = at 128 and 256;
+ *   "cost8": the volume the SGM sweeps read (the census-only Fast volume, or the aggregated
+ *            volume of one aggregation pass) at one byte per voxel (0xFF invalid; exact while
+ *            every quantised cost is below 255): 0 = at 256 padded disparities (default),
+ *            1 = never, 2 = at 128 and 256;
  *   "refine_window": 0 = HighQuality refiner reads the right-image window from shared memory where
  *                 every band fits on the device at once (default), 1 = always through L1.
  * And one key that bounds a wait rather than tuning speed:

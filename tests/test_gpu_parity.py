@@ -47,6 +47,11 @@ def _cases():
         ("column_1x33", B, (1, 33, 16, 0), "noise", {}, 0),
         ("pixel_1x1", F, (1, 1, 16, 0), "noise", {}, 0),
         ("hq_d256_300x100", H, (300, 100, 256, 0), "synth_patch", {}, 0),
+        # the aggregated volume at one byte per voxel (a padded range of 256): 4 and 8 paths, a
+        # negative range (per-pixel counts in the vertical pass)
+        ("balanced_300x64_d256", B, (300, 64, 256, 0), "synth", {}, 0),
+        ("path8_balanced_160x80_d256", B, (160, 80, 256, 0), "synth", {"paths": 8}, 0),
+        ("balanced_negative_200x60_d200_min_40", B, (200, 60, 200, -40), "synth", {}, 0),
         # refiner wavefront edges: a one-row last band, fewer columns than lanes, a negative range,
         # more passes with a wider random radius
         ("hq_band_edges_70x33", H, (70, 33, 24, 0), "synth_patch", {}, 0),
@@ -117,8 +122,10 @@ def test_stage_parity(case, O, apg):
     for k in ("disparity", "confidence", "invalid_reason", "reliable_mask"):
         assert same_bits(gpu[k], ora[k]), f"{name}: final {k} differs"
     assert np.all(np.isfinite(gpu["disparity"]))
-    neg = gpu["disparity"][gpu["disparity"] < 0]
-    assert np.all(neg == -1.0)
+    if dmin >= 0:
+        # with a non-negative range, a negative disparity is the invalid marker
+        neg = gpu["disparity"][gpu["disparity"] < 0]
+        assert np.all(neg == -1.0)
     assert np.all((gpu["confidence"] >= 0) & (gpu["confidence"] <= 1))
 
 
@@ -135,19 +142,22 @@ def test_fast_fused_equals_unfused(apg, w, h, dmax):
         assert same_bits(a[k], b[k]), k
 
 
-@pytest.mark.parametrize("w,h,dmax,over", [
-    (333, 90, 128, {}), (300, 64, 256, {}), (97, 61, 100, {"min_disparity": -20}), (150, 80, 128, {"paths": 8}),
-    (64, 7, 120, {}), (150, 80, 128, {"sgm_split": 2}),
+@pytest.mark.parametrize("mode,w,h,dmax,over", [
+    (0, 333, 90, 128, {}), (0, 300, 64, 256, {}), (0, 97, 61, 100, {"min_disparity": -20}),
+    (0, 150, 80, 128, {"paths": 8}), (0, 64, 7, 120, {}), (0, 150, 80, 128, {"sgm_split": 2}),
+    (1, 300, 64, 256, {}), (1, 150, 80, 128, {}), (1, 160, 90, 256, {"paths": 8}),
+    (1, 200, 64, 200, {"min_disparity": -40}), (1, 256, 128, 256, {"hier_enable": 1}), (2, 200, 96, 256, {}),
+    (1, 64, 9, 128, {"sgm_split": 2}),
 ])
-def test_cost8_changes_no_result(apg, w, h, dmax, over):
-    """The Fast volume at one byte per voxel (tuning cost8=2; the default at a padded range of 256)
-    and at two bytes (cost8=1) give identical maps and path sums, and the byte form takes half the
-    volume's bytes."""
-    L, R = synth(w, h, dmax, seed=29)
+def test_cost8_changes_no_result(apg, mode, w, h, dmax, over):
+    """The sweeps' volume at one byte per voxel (tuning cost8=2; the default at a padded range of
+    256) and at two bytes (cost8=1) give identical maps and path sums, and the byte form takes half
+    the volume's bytes: the raw census volume in Fast mode, the aggregated volume otherwise."""
+    L, R = synth(w, h, dmax, patch=0.2 if mode == 2 else 0.0, seed=29)
     over = dict(over)
     dmin = over.pop("min_disparity", 0)
     split = over.pop("sgm_split", 0)
-    cfg = apg.config_from_mode(0, dmax, dmin, **over)
+    cfg = apg.config_from_mode(mode, dmax, dmin, **over)
     outs, sizes = [], []
     for cost8 in (2, 1):
         e = apg.Engine(cfg, debug=apg.DEBUG_KEEP_SUM)
