@@ -82,7 +82,8 @@ cudaError_t launch_sgm_first(const SgmLaunch& l, int ndir, const int (*dirs)[2],
 // Last sweep (dx, dy): adds the nin (1 or 3) partial sums in[] and writes the WTA maps.
 cudaError_t launch_sgm_last(const SgmLaunch& l, int dx, int dy, int nin, const uint32_t* const* in, cudaStream_t s);
 // bufs[0] += bufs[1..6] (saturating u16 lanes), `words` 32-bit words each.
-cudaError_t launch_sgm_sum7(uint32_t* const* bufs, size_t words, cudaStream_t s);
+// Path8: adds bufs[1 .. nbuf) into bufs[0] (nbuf 5 or 7), saturating per halfword.
+cudaError_t launch_sgm_fold(uint32_t* const* bufs, int nbuf, size_t words, cudaStream_t s);
 int sgm_lanes_for(int Dp, int requested);
 
 // Batches: the SGM of many pairs (Dp 64, 128, 192 or 256), volume-fed, in two persistent launches

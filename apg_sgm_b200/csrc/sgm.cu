@@ -1105,16 +1105,17 @@ __global__ void __launch_bounds__(128) sgm_last_kernel(SgmArgs a, DirTable tab) 
     run_chain<T, K, kLast, CENSUS, 0, UR::PF, UR::U, NB>(a, tab, s_q, tab.dx[0], tab.dy[0], s, tab.nscan[0], nullptr);
 }
 
-// Path8: fold the seven first-phase buffers into the first one (saturating per halfword).
-__global__ void sgm_sum_kernel(uint4* __restrict__ dst, const uint4* __restrict__ b1, const uint4* __restrict__ b2,
-                               const uint4* __restrict__ b3, const uint4* __restrict__ b4,
-                               const uint4* __restrict__ b5, const uint4* __restrict__ b6, size_t n) {
+// Path8: fold the first NBUF first-phase buffers into the first one (saturating per halfword).
+struct FoldSrc {
+    const uint4* b[6];
+};
+template <int NBUF>
+__global__ void sgm_sum_kernel(uint4* __restrict__ dst, FoldSrc src, size_t n) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         uint4 v = __ldcg(dst + i);
-        const uint4* src[6] = {b1, b2, b3, b4, b5, b6};
 #pragma unroll
-        for (int b = 0; b < 6; ++b) {
-            const uint4 t = __ldcs(src[b] + i);
+        for (int b = 0; b < NBUF - 1; ++b) {
+            const uint4 t = __ldcs(src.b[b] + i);
             v.x = addus2(v.x, t.x); v.y = addus2(v.y, t.y);
             v.z = addus2(v.z, t.z); v.w = addus2(v.w, t.w);
         }
@@ -1531,13 +1532,15 @@ cudaError_t launch_sgm_last(const SgmLaunch& l, int dx, int dy, int nin, const u
     return dispatch<false>(a, tab, l.cvol == nullptr, sgm_lanes_for(l.Dp, l.lanes), l.split, st);
 }
 
-cudaError_t launch_sgm_sum7(uint32_t* const* bufs, size_t words, cudaStream_t st) {
+cudaError_t launch_sgm_fold(uint32_t* const* bufs, int nbuf, size_t words, cudaStream_t st) {
     const size_t n = words / 4;
     const int blocks = (int)std::min<size_t>((n + 255) / 256, 148 * 16);
-    sgm_sum_kernel<<<blocks, 256, 0, st>>>(reinterpret_cast<uint4*>(bufs[0]), reinterpret_cast<const uint4*>(bufs[1]),
-                                           reinterpret_cast<const uint4*>(bufs[2]), reinterpret_cast<const uint4*>(bufs[3]),
-                                           reinterpret_cast<const uint4*>(bufs[4]), reinterpret_cast<const uint4*>(bufs[5]),
-                                           reinterpret_cast<const uint4*>(bufs[6]), n);
+    FoldSrc src{};
+    for (int b = 1; b < nbuf; ++b) src.b[b - 1] = reinterpret_cast<const uint4*>(bufs[b]);
+    uint4* dst = reinterpret_cast<uint4*>(bufs[0]);
+    if (nbuf == 7) sgm_sum_kernel<7><<<blocks, 256, 0, st>>>(dst, src, n);
+    else if (nbuf == 5) sgm_sum_kernel<5><<<blocks, 256, 0, st>>>(dst, src, n);
+    else return cudaErrorInvalidValue;
     return cudaGetLastError();
 }
 
@@ -1656,7 +1659,7 @@ cudaError_t launch_sgm_batch(const SgmBatchPlan& plan, int max_blocks_per_sm, cu
     if (e != cudaSuccess) return e;
     if (plan.nsbuf == 7) {
         for (int i = 0; i < plan.npairs; ++i) {
-            e = launch_sgm_sum7(plan.sums.data() + (size_t)i * 7, plan.words[i], st);
+            e = launch_sgm_fold(plan.sums.data() + (size_t)i * 7, 7, plan.words[i], st);
             if (e != cudaSuccess) return e;
         }
         return plan.mixed ? launch_batch_mixed<kLast, 1>(plan.Dp, pairs, last, plan.nseg_last, plan.total_last,

@@ -201,10 +201,10 @@ def _algorithmic_bytes(name: str, w: int, h: int, D: int, volume_source: bool, n
     n = w * h
     vol = n * D * 2.0 if volume_source else 0.0
     nfirst = npath - 1
-    nin = 1 if npath == 8 else nfirst
+    nin = 3  # Path8: five first-phase buffers folded into one before the last sweep
     return {
         "sgm_first": nfirst * (n * D * 2.0 + vol),    # every first-phase sweep writes its own sums
-        "sgm_sum7": n * D * 16.0,                     # Path8: read 7 buffers, write 1
+        "sgm_fold5": n * D * 12.0,                    # Path8: read 5 buffers, write 1
         "sgm_last_wta": nin * n * D * 2.0 + vol + n * 12,  # read the partial sums, write the WTA maps
         "cost+crossH": n * D * 2.0,                   # write the horizontally aggregated volume
         "crossV": n * D * 4.0,                        # read T, write C
@@ -710,7 +710,7 @@ def run_b200(args, wl):
     roofline["hbm_frac_by_kernel"] = {
         k: round(_algorithmic_bytes(k, w, h, D, volume_source=True, npath=cfg.paths) /
                  (statistics.mean(per_kernel[k]) / 1000.0) / 1e9 / peak, 4)
-        for k in ("sgm_first", "sgm_sum7", "sgm_last_wta", "crossV") if k in per_kernel}
+        for k in ("sgm_first", "sgm_fold5", "sgm_last_wta", "crossV") if k in per_kernel}
     if top in ("cost", "cost+crossH"):
         roofline["note"] = ("issue-bound: integer and LUT work per voxel (ncu issue active ~73%, DRAM ~8%); "
                             "the HBM fraction of its 2 B/voxel output is shown for reference")
