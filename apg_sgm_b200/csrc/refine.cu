@@ -212,7 +212,8 @@ struct __align__(16) RStep {
     int d_pack;    // d_cur (low 16, signed) | d_draw (high 16, signed)
     int range;     // lo (low 16) | hi (high 16)
     int upd;       // bit 0: unreliable with a non-empty range; bit 1: cur is a candidate; bit 2: cur + draw is
-    int pad0, pad1;
+    int rcur;      // the start value as a neighbour candidate: roundf(cur) when cur >= 0, else -1
+    int pad1;
 };
 
 template <bool C64>
@@ -246,7 +247,8 @@ __global__ void refine_prep_kernel(CostCtx c, int fwd, const uint8_t* __restrict
         st.upd = (!reliable[i] && hi > lo) ? 1 : 0;
         int d_cur = 0, d_draw = 0;
         st.c_cur = st.c_draw = 1e9f;
-        st.pad0 = st.pad1 = 0;
+        st.rcur = st.cur >= 0.f ? (int)roundf(st.cur) : -1;
+        st.pad1 = 0;
         if (st.upd && st.cur >= 0.f) {
             const RPack<C64> l = lp[i];
             d_cur = min(max((int)roundf(st.cur), lo), hi - 1);
@@ -297,7 +299,8 @@ __device__ __forceinline__ void cp16(void* dst, const void* src) {
 // implies for the row above.
 constexpr int kUpRing = 128;
 struct BandLink {
-    float up[kUpRing];  // row above the band: column c at up[c & (kUpRing - 1)]
+    int up[kUpRing];    // row above the band as neighbour candidates (roundf(value) when value >= 0,
+                        // else -1): column c at up[c & (kUpRing - 1)]
     int avail;          // columns [0, avail) of the row above are in `up` (link warp)
     int used;           // columns [0, used) of `up` are no longer read (compute warp)
     int done;           // columns [0, done) of the band's last row are final in `work` (compute warp)
@@ -340,8 +343,10 @@ __device__ void band_link(BandLink* s_link, int band, int w, int h, int fwd, con
             if (upto > fetched) {
                 if (lane == 0) fence_acq_rel();
                 __syncwarp();
-                for (int col = fetched + lane; col < upto; col += 32)
-                    s_link->up[col & (kUpRing - 1)] = __ldcg(above + (xb + xs * col));
+                for (int col = fetched + lane; col < upto; col += 32) {
+                    const float a = __ldcg(above + (xb + xs * col));
+                    s_link->up[col & (kUpRing - 1)] = a >= 0.f ? (int)roundf(a) : -1;
+                }
                 __syncwarp();
                 if (lane == 0) {
                     __threadfence_block();
@@ -540,11 +545,14 @@ __global__ void __launch_bounds__(96) refine_band_kernel(CostCtx c, int fwd, con
     const bool row_ok = r.ok;
     float* wrow = r.work;
     const RPack<C64>* rrow = r.right;
-    float prev = -1.f;  // value of this lane's previous column (its left neighbour)
+    // Neighbour values travel as candidates: roundf(value) when value >= 0, else -1 (the
+    // reference takes a neighbour only when it is non-negative, rounded).  An updated value is an
+    // integer already; a start value's candidate comes with its record.
+    int prev = -1;  // candidate of this lane's previous column (its left neighbour)
     int avail = band > 0 ? 0 : w;  // columns of the row above known to be in the link's ring
     bool abort = false;
     for (int t = 0; t < w + kBand - 1; ++t) {
-        float up_first = -1.f;  // the row above at column t (lane 0's up neighbour)
+        int up_first = -1;  // the row above at column t (lane 0's up neighbour)
         if (band > 0 && t < w) {
             if (t >= avail) {
                 // wait until the link warp has the row above at least up to column t (lane 0
@@ -577,11 +585,11 @@ __global__ void __launch_bounds__(96) refine_band_kernel(CostCtx c, int fwd, con
             if (lane == 0) atomicExch(err, 1);
             break;
         }
-        const float up_lane = __shfl_up_sync(0xffffffffu, prev, 1);
+        const int up_lane = __shfl_up_sync(0xffffffffu, prev, 1);
         const int u = t - lane;
         if (row_ok && u >= 0 && u < w) {
             const RStep st = s_ring.rec[slot][lane];
-            float val = st.cur;
+            int cand = st.rcur;
             if (st.upd & 1) {
                 const int x = r.xb + r.xs * u;
                 const int lo = (int)(short)(st.range & 0xFFFF), hi = st.range >> 16;
@@ -589,13 +597,12 @@ __global__ void __launch_bounds__(96) refine_band_kernel(CostCtx c, int fwd, con
                 const bool has_cur = (st.upd & 2) != 0, has_draw = (st.upd & 4) != 0;
                 const RPack<C64> l = s_ring.lpk[slot][lane];
                 // dynamic candidates: left (forward) / right (backward) and up / down
-                float left = -1.f, up = -1.f;
-                if (u > 0) left = prev;
-                if (v > 0) up = lane > 0 ? up_lane : up_first;
-                const bool has_l = left >= 0.f, has_u = up >= 0.f;
+                const int left = u > 0 ? prev : -1;
+                const int up = v > 0 ? (lane > 0 ? up_lane : up_first) : -1;
+                const bool has_l = left >= 0, has_u = up >= 0;
                 // clamped into [lo, hi - 1] (hi > lo for an updated pixel), so only x - d needs a test
-                const int dl = has_l ? min(max((int)roundf(left), lo), hi - 1) : 0;
-                const int du = has_u ? min(max((int)roundf(up), lo), hi - 1) : 0;
+                const int dl = has_l ? min(max(left, lo), hi - 1) : 0;
+                const int du = has_u ? min(max(up, lo), hi - 1) : 0;
                 const int xl = x - dl, xu = x - du;
                 const float cl = (has_l && (unsigned)xl < (unsigned)w)
                                      ? packed_cost<C64>(c, s_lut, l, WIN ? s_win[xl & wmask] : rrow[xl])
@@ -610,10 +617,10 @@ __global__ void __launch_bounds__(96) refine_band_kernel(CostCtx c, int fwd, con
                 if (has_l && cl < best_c) { best_c = cl; best_d = dl; }
                 if (has_u && cu < best_c) { best_c = cu; best_d = du; }
                 if (has_draw && st.c_draw < best_c) { best_c = st.c_draw; best_d = d_draw; }
-                val = (float)best_d;
-                wrow[x] = val;
+                wrow[x] = (float)best_d;
+                cand = best_d >= 0 ? best_d : -1;
             }
-            prev = val;
+            prev = cand;
         }
         // every lane has read the slot (and its window pixels): the loader may refill it
         __syncwarp();
