@@ -306,6 +306,10 @@ __global__ void __launch_bounds__(256) cross_v_count_kernel(int w, int h, int d0
     uint32_t ps = 0;
     uint32_t pc = 0;  // low 16 bits used
     size_t dst = ((size_t)y0 * w + x) * W2 + k;  // word index of (x, y0), lane k
+    // ring slots kept incrementally (RS need not be a power of two): pslot is the slot of row
+    // `pushed`, yslot the slot of the prefix through the output row y, (y - ystart + 1) % RS
+    int pslot = 1;
+    int yslot = (y0 - ystart + 1) % RS;
     for (int yb = y0; yb < y1; yb += kQ) {
         const int need = min(h, min(yb + kQ, y1) + lmax);
         while (pushed < need) {
@@ -316,10 +320,11 @@ __global__ void __launch_bounds__(256) cross_v_count_kernel(int w, int h, int d0
                     const bool lo_bad = (v & 0xFFFFu) == 0xFFFFu, hi_bad = v >= 0xFFFF0000u;
                     ps += v & ((lo_bad ? 0u : 0x0000FFFFu) | (hi_bad ? 0u : 0xFFFF0000u));
                     pc += (lo_bad ? 0u : 1u) + (hi_bad ? 0u : 0x100u);
-                    const int slot = (int)((unsigned)(pushed + i - ystart + 1) % RS) * nthr + tid;
+                    const int slot = pslot * nthr + tid;
                     ring[slot] = ps;
                     ringc[slot] = (uint16_t)pc;
                 }
+                pslot = pslot + 1 == RS ? 0 : pslot + 1;
             }
             pushed += KB;
 #pragma unroll
@@ -334,9 +339,13 @@ __global__ void __launch_bounds__(256) cross_v_count_kernel(int w, int h, int d0
             const int y = yb + i;
             if (y >= y1) break;
             const int ai = ci * kSeg + (y - y0);
-            const int a = y - armU[ai], b = y + armD[ai];  // inclusive window
-            const int sb = (int)((unsigned)(b - ystart + 1) % RS) * nthr + tid;
-            const int sa = (int)((unsigned)(a - ystart) % RS) * nthr + tid;
+            // inclusive window [y - armU, y + armD]: the prefixes through y + armD and y - armU - 1
+            int sb = yslot + armD[ai], sa = yslot - armU[ai] - 1;
+            sb = sb >= RS ? sb - RS : sb;
+            sa = sa < 0 ? sa + RS : sa;
+            sb = sb * nthr + tid;
+            sa = sa * nthr + tid;
+            yslot = yslot + 1 == RS ? 0 : yslot + 1;
             const uint32_t sum = ring[sb] - ring[sa];
             const uint32_t cnt = (uint32_t)(uint16_t)(ringc[sb] - ringc[sa]);
             const uint32_t rg = s_rng[ai];
