@@ -125,7 +125,51 @@ __global__ void cross_v_kernel(int w, int h, int d0, int D, int Dp, int lmax, in
 constexpr int kB = 16;
 constexpr int kQ = 8;  // output rows computed together (independent windows: their loads overlap)
 
-template <int RS, bool U8>
+// WPT words (of two disparities) per thread: the arms, ring slots, window length and divisor of
+// an output row are shared by the thread's words, and its loads, ring accesses and stores are
+// WPT words wide.
+template <int WPT>
+struct Words {
+    uint32_t v[WPT];
+};
+template <int WPT>
+__device__ __forceinline__ Words<WPT> load_words(const uint32_t* p) {
+    Words<WPT> r;
+    if constexpr (WPT == 2) {
+        const uint2 t = __ldcs(reinterpret_cast<const uint2*>(p));
+        r.v[0] = t.x; r.v[1] = t.y;
+    } else {
+        r.v[0] = __ldcs(p);
+    }
+    return r;
+}
+template <int WPT>
+__device__ __forceinline__ void ring_put(uint32_t* p, const uint32_t (&v)[WPT]) {
+    if constexpr (WPT == 2) *reinterpret_cast<uint2*>(p) = make_uint2(v[0], v[1]);
+    else p[0] = v[0];
+}
+template <int WPT>
+__device__ __forceinline__ void ring_get(const uint32_t* p, uint32_t (&v)[WPT]) {
+    if constexpr (WPT == 2) {
+        const uint2 t = *reinterpret_cast<const uint2*>(p);
+        v[0] = t.x; v[1] = t.y;
+    } else {
+        v[0] = p[0];
+    }
+}
+// Stores WPT words from word index i (a multiple of WPT) of the output volume; see store_cost_word.
+template <bool U8, int WPT>
+__device__ __forceinline__ void store_cost_words(uint32_t* out, size_t i, const uint32_t (&wd)[WPT]) {
+    if constexpr (WPT == 1) {
+        store_cost_word<U8, true>(out, i, wd[0]);
+    } else if constexpr (U8) {
+        __stcs(reinterpret_cast<unsigned int*>(out) + i / 2, __byte_perm(wd[0], wd[1], 0x6420));
+    } else {
+        __stcs(reinterpret_cast<uint2*>(out + i), make_uint2(wd[0], wd[1]));
+    }
+}
+
+template <int RS, bool U8, int WPT>
 __global__ void __launch_bounds__(128) cross_v_default_kernel(int w, int h, int d0, int D, int Dp, int lmax, int tau,
                                                               int cols, const uint8_t* __restrict__ gray,
                                                               const uint32_t* __restrict__ tin,
@@ -133,9 +177,11 @@ __global__ void __launch_bounds__(128) cross_v_default_kernel(int w, int h, int 
                                                               const uint32_t* __restrict__ magic) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int W2 = Dp / 2;
-    const int nthr = W2 * cols;
-    uint32_t* ring = reinterpret_cast<uint32_t*>(smem);                      // [RS][nthr]
-    uint32_t* s_magic = ring + (size_t)RS * nthr;                              // [2*lmax+2]
+    const int tpc = W2 / WPT;      // threads per column
+    const int nthr = tpc * cols;   // threads with words
+    const int rw = W2 * cols;      // ring words per slot
+    uint32_t* ring = reinterpret_cast<uint32_t*>(smem);                      // [RS][rw]
+    uint32_t* s_magic = ring + (size_t)RS * rw;                                // [2*lmax+2]
     uint8_t* s_gray = reinterpret_cast<uint8_t*>(s_magic + 2 * lmax + 2);     // [cols][kSeg + 2*lmax]
     uint8_t* armU = s_gray + cols * (kSeg + 2 * lmax);                         // [cols][kSeg]
     uint8_t* armD = armU + cols * kSeg;
@@ -167,28 +213,33 @@ __global__ void __launch_bounds__(128) cross_v_default_kernel(int w, int h, int 
     }
     __syncthreads();
     if (tid >= nthr) return;
-    const int ci = tid / W2, k = tid - ci * W2;
+    const int ci = tid / tpc, k = (tid - ci * tpc) * WPT;  // the thread's first word
     const int x = xb + ci;
     if (x >= w) return;
+    const int roff = ci * W2 + k;  // the thread's words within a ring slot
     // output lanes that can be valid: d < dmax and d <= x
-    bool lane_ok[2];
+    bool lane_ok[2 * WPT];
 #pragma unroll
-    for (int hs = 0; hs < 2; ++hs) lane_ok[hs] = (2 * k + hs < D) && (d0 + 2 * k + hs <= x);
+    for (int hs = 0; hs < 2 * WPT; ++hs) lane_ok[hs] = (2 * k + hs < D) && (d0 + 2 * k + hs <= x);
 
     const int ystart = max(0, y0 - lmax);
     const int yend = min(h, y1 + lmax);  // rows read: [ystart, yend)
     // ring slot of prefix P(r) (sum over rows [ystart, r]) is (r - ystart + 1) & (RS - 1); slot 0 = P(ystart - 1) = 0
-    ring[tid] = 0;
+    {
+        uint32_t z[WPT] = {};
+        ring_put<WPT>(ring + roff, z);
+    }
     const size_t rowstride = (size_t)w * W2;
     const uint32_t* src = tin + ((size_t)ystart * w + x) * W2 + k;
-    uint32_t cur[kB], nxt[kB];
+    Words<WPT> cur[kB], nxt[kB];
 #pragma unroll
-    for (int i = 0; i < kB; ++i) cur[i] = ystart + i < yend ? __ldcs(src + i * rowstride) : 0u;
+    for (int i = 0; i < kB; ++i) cur[i] = ystart + i < yend ? load_words<WPT>(src + i * rowstride) : Words<WPT>{};
 #pragma unroll
-    for (int i = 0; i < kB; ++i) nxt[i] = ystart + kB + i < yend ? __ldcs(src + (kB + i) * rowstride) : 0u;
+    for (int i = 0; i < kB; ++i)
+        nxt[i] = ystart + kB + i < yend ? load_words<WPT>(src + (kB + i) * rowstride) : Words<WPT>{};
     int pushed = ystart;  // next row to add to the ring
-    uint32_t ps = 0;
-    size_t dst = ((size_t)y0 * w + x) * W2 + k;  // word index of (x, y0), lane k
+    uint32_t ps[WPT] = {};
+    size_t dst = ((size_t)y0 * w + x) * W2 + k;  // word index of (x, y0), word k
     for (int yb = y0; yb < y1; yb += kQ) {
         // prefixes up to the last window of the chunk's rows, then kQ independent rows
         const int need = min(h, min(yb + kQ, y1) + lmax);
@@ -197,8 +248,9 @@ __global__ void __launch_bounds__(128) cross_v_default_kernel(int w, int h, int 
 #pragma unroll
             for (int i = 0; i < kB; ++i) {
                 if (pushed + i < yend) {
-                    ps += cur[i];
-                    ring[((pushed + i - ystart + 1) & (RS - 1)) * nthr + tid] = ps;
+#pragma unroll
+                    for (int j = 0; j < WPT; ++j) ps[j] += cur[i].v[j];
+                    ring_put<WPT>(ring + ((pushed + i - ystart + 1) & (RS - 1)) * rw + roff, ps);
                 }
             }
             pushed += kB;
@@ -207,7 +259,7 @@ __global__ void __launch_bounds__(128) cross_v_default_kernel(int w, int h, int 
             const int base = pushed + kB;
 #pragma unroll
             for (int i = 0; i < kB; ++i)
-                nxt[i] = base + i < yend ? __ldcs(src + (size_t)(base + i - ystart) * rowstride) : 0u;
+                nxt[i] = base + i < yend ? load_words<WPT>(src + (size_t)(base + i - ystart) * rowstride) : Words<WPT>{};
         }
 #pragma unroll
         for (int i = 0; i < kQ; ++i) {
@@ -215,18 +267,25 @@ __global__ void __launch_bounds__(128) cross_v_default_kernel(int w, int h, int 
             if (y >= y1) break;
             const int ai = ci * kSeg + (y - y0);
             const int a = y - armU[ai], b = y + armD[ai];  // inclusive window
-            const uint32_t sum = ring[((b - ystart + 1) & (RS - 1)) * nthr + tid] -
-                                 ring[((a - ystart) & (RS - 1)) * nthr + tid];
+            uint32_t pb[WPT], pa[WPT];
+            ring_get<WPT>(ring + ((b - ystart + 1) & (RS - 1)) * rw + roff, pb);
+            ring_get<WPT>(ring + ((a - ystart) & (RS - 1)) * rw + roff, pa);
             const int len = b - a + 1;
             const uint32_t mg = s_magic[len];
-            uint32_t word = 0;
+            uint32_t wd[WPT];
 #pragma unroll
-            for (int hs = 0; hs < 2; ++hs) {
-                const uint32_t sh = (sum >> (16 * hs)) & 0xFFFFu;
-                const uint32_t q = lane_ok[hs] ? div_by_magic(sh, (uint32_t)len, mg) : kInvalidCost;
-                word |= q << (16 * hs);
+            for (int j = 0; j < WPT; ++j) {
+                const uint32_t sum = pb[j] - pa[j];
+                uint32_t word = 0;
+#pragma unroll
+                for (int hs = 0; hs < 2; ++hs) {
+                    const uint32_t sh = (sum >> (16 * hs)) & 0xFFFFu;
+                    const uint32_t q = lane_ok[2 * j + hs] ? div_by_magic(sh, (uint32_t)len, mg) : kInvalidCost;
+                    word |= q << (16 * hs);
+                }
+                wd[j] = word;
             }
-            store_cost_word<U8, true>(cout, dst + (size_t)i * rowstride, word);
+            store_cost_words<U8, WPT>(cout, dst + (size_t)i * rowstride, wd);
         }
         dst += (size_t)kQ * rowstride;
     }
@@ -238,7 +297,7 @@ __global__ void __launch_bounds__(128) cross_v_default_kernel(int w, int h, int 
 // sums of (valid low half) | (valid high half) << 8: a window difference is exact in every lane
 // because a window's sum is below 2^16 (host-checked for the arm length and cost_max) and its
 // counts are at most 2*lmax + 1 <= 255.  The centre pixel's range is staged with the arms.
-template <int RS, int KB, bool U8>
+template <int RS, int KB, bool U8, int WPT>
 __global__ void __launch_bounds__(256) cross_v_count_kernel(int w, int h, int d0, int D, int Dp, int lmax, int tau,
                                                             int cols, const uint8_t* __restrict__ gray,
                                                             const int16_t* __restrict__ rmin,
@@ -248,12 +307,14 @@ __global__ void __launch_bounds__(256) cross_v_count_kernel(int w, int h, int d0
                                                             const uint32_t* __restrict__ magic) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int W2 = Dp / 2;
-    const int nthr = W2 * cols;
-    uint32_t* ring = reinterpret_cast<uint32_t*>(smem);                  // [RS][nthr] sums
-    uint32_t* s_rng = ring + (size_t)RS * nthr;                          // [cols][kSeg] lo | hi << 16
+    const int tpc = W2 / WPT;     // threads per column
+    const int nthr = tpc * cols;  // threads with words
+    const int rw = W2 * cols;     // ring words per slot
+    uint32_t* ring = reinterpret_cast<uint32_t*>(smem);                  // [RS][rw] sums
+    uint32_t* s_rng = ring + (size_t)RS * rw;                            // [cols][kSeg] lo | hi << 16
     uint32_t* s_magic = s_rng + cols * kSeg;                             // [2*lmax+2]
-    uint16_t* ringc = reinterpret_cast<uint16_t*>(s_magic + 2 * lmax + 2);  // [RS][nthr] counts
-    uint8_t* s_gray = reinterpret_cast<uint8_t*>(ringc + (size_t)RS * nthr);  // [cols][kSeg + 2*lmax]
+    uint16_t* ringc = reinterpret_cast<uint16_t*>(s_magic + 2 * lmax + 2);  // [RS][rw] counts
+    uint8_t* s_gray = reinterpret_cast<uint8_t*>(ringc + (size_t)RS * rw);  // [cols][kSeg + 2*lmax]
     uint8_t* armU = s_gray + cols * (kSeg + 2 * lmax);                   // [cols][kSeg]
     uint8_t* armD = armU + cols * kSeg;
     const int xb = blockIdx.x * cols;
@@ -287,25 +348,31 @@ __global__ void __launch_bounds__(256) cross_v_count_kernel(int w, int h, int d0
     }
     __syncthreads();
     if (tid >= nthr) return;
-    const int ci = tid / W2, k = tid - ci * W2;
+    const int ci = tid / tpc, k = (tid - ci * tpc) * WPT;  // the thread's first word
     const int x = xb + ci;
     if (x >= w) return;
+    const int roff = ci * W2 + k;  // the thread's words within a ring slot
 
     const int ystart = max(0, y0 - lmax);
     const int yend = min(h, y1 + lmax);
-    ring[tid] = 0;
-    ringc[tid] = 0;
+    {
+        uint32_t z[WPT] = {};
+        ring_put<WPT>(ring + roff, z);
+        if constexpr (WPT == 2) *reinterpret_cast<uint32_t*>(ringc + roff) = 0u;
+        else ringc[roff] = 0;
+    }
     const size_t rowstride = (size_t)w * W2;
     const uint32_t* src = tin + ((size_t)ystart * w + x) * W2 + k;
-    uint32_t cur[KB], nxt[KB];
+    Words<WPT> cur[KB], nxt[KB];
 #pragma unroll
-    for (int i = 0; i < KB; ++i) cur[i] = ystart + i < yend ? __ldcs(src + i * rowstride) : 0u;
+    for (int i = 0; i < KB; ++i) cur[i] = ystart + i < yend ? load_words<WPT>(src + i * rowstride) : Words<WPT>{};
 #pragma unroll
-    for (int i = 0; i < KB; ++i) nxt[i] = ystart + KB + i < yend ? __ldcs(src + (KB + i) * rowstride) : 0u;
+    for (int i = 0; i < KB; ++i)
+        nxt[i] = ystart + KB + i < yend ? load_words<WPT>(src + (KB + i) * rowstride) : Words<WPT>{};
     int pushed = ystart;
-    uint32_t ps = 0;
-    uint32_t pc = 0;  // low 16 bits used
-    size_t dst = ((size_t)y0 * w + x) * W2 + k;  // word index of (x, y0), lane k
+    uint32_t ps[WPT] = {};
+    uint32_t pc[WPT] = {};  // low 16 bits used
+    size_t dst = ((size_t)y0 * w + x) * W2 + k;  // word index of (x, y0), word k
     // ring slots kept incrementally (RS need not be a power of two): pslot is the slot of row
     // `pushed`, yslot the slot of the prefix through the output row y, (y - ystart + 1) % RS
     int pslot = 1;
@@ -316,13 +383,18 @@ __global__ void __launch_bounds__(256) cross_v_count_kernel(int w, int h, int d0
 #pragma unroll
             for (int i = 0; i < KB; ++i) {
                 if (pushed + i < yend) {
-                    const uint32_t v = cur[i];
-                    const bool lo_bad = (v & 0xFFFFu) == 0xFFFFu, hi_bad = v >= 0xFFFF0000u;
-                    ps += v & ((lo_bad ? 0u : 0x0000FFFFu) | (hi_bad ? 0u : 0xFFFF0000u));
-                    pc += (lo_bad ? 0u : 1u) + (hi_bad ? 0u : 0x100u);
-                    const int slot = pslot * nthr + tid;
-                    ring[slot] = ps;
-                    ringc[slot] = (uint16_t)pc;
+#pragma unroll
+                    for (int j = 0; j < WPT; ++j) {
+                        const uint32_t v = cur[i].v[j];
+                        const bool lo_bad = (v & 0xFFFFu) == 0xFFFFu, hi_bad = v >= 0xFFFF0000u;
+                        ps[j] += v & ((lo_bad ? 0u : 0x0000FFFFu) | (hi_bad ? 0u : 0xFFFF0000u));
+                        pc[j] += (lo_bad ? 0u : 1u) + (hi_bad ? 0u : 0x100u);
+                    }
+                    const int slot = pslot * rw + roff;
+                    ring_put<WPT>(ring + slot, ps);
+                    if constexpr (WPT == 2)
+                        *reinterpret_cast<uint32_t*>(ringc + slot) = (pc[0] & 0xFFFFu) | (pc[1] << 16);
+                    else ringc[slot] = (uint16_t)pc[0];
                 }
                 pslot = pslot + 1 == RS ? 0 : pslot + 1;
             }
@@ -332,7 +404,7 @@ __global__ void __launch_bounds__(256) cross_v_count_kernel(int w, int h, int d0
             const int base = pushed + KB;
 #pragma unroll
             for (int i = 0; i < KB; ++i)
-                nxt[i] = base + i < yend ? __ldcs(src + (size_t)(base + i - ystart) * rowstride) : 0u;
+                nxt[i] = base + i < yend ? load_words<WPT>(src + (size_t)(base + i - ystart) * rowstride) : Words<WPT>{};
         }
 #pragma unroll
         for (int i = 0; i < kQ; ++i) {
@@ -343,24 +415,39 @@ __global__ void __launch_bounds__(256) cross_v_count_kernel(int w, int h, int d0
             int sb = yslot + armD[ai], sa = yslot - armU[ai] - 1;
             sb = sb >= RS ? sb - RS : sb;
             sa = sa < 0 ? sa + RS : sa;
-            sb = sb * nthr + tid;
-            sa = sa * nthr + tid;
+            sb = sb * rw + roff;
+            sa = sa * rw + roff;
             yslot = yslot + 1 == RS ? 0 : yslot + 1;
-            const uint32_t sum = ring[sb] - ring[sa];
-            const uint32_t cnt = (uint32_t)(uint16_t)(ringc[sb] - ringc[sa]);
+            uint32_t pb[WPT], pa[WPT], cnt[WPT];
+            ring_get<WPT>(ring + sb, pb);
+            ring_get<WPT>(ring + sa, pa);
+            if constexpr (WPT == 2) {
+                const uint32_t cb = *reinterpret_cast<const uint32_t*>(ringc + sb);
+                const uint32_t ca = *reinterpret_cast<const uint32_t*>(ringc + sa);
+                cnt[0] = (cb - ca) & 0xFFFFu;
+                cnt[1] = ((cb >> 16) - (ca >> 16)) & 0xFFFFu;
+            } else {
+                cnt[0] = (uint32_t)(uint16_t)(ringc[sb] - ringc[sa]);
+            }
             const uint32_t rg = s_rng[ai];
             const int lo = (int16_t)(rg & 0xFFFFu), hi = (int16_t)(rg >> 16);
-            uint32_t word = 0;
+            uint32_t wd[WPT];
 #pragma unroll
-            for (int hs = 0; hs < 2; ++hs) {
-                const int di = 2 * k + hs;
-                const int d = d0 + di;
-                const uint32_t sh = (sum >> (16 * hs)) & 0xFFFFu, nh = (cnt >> (8 * hs)) & 0xFFu;
-                uint32_t q = kInvalidCost;
-                if (di < D && d >= lo && d < hi && nh > 0) q = div_by_magic(sh, nh, s_magic[nh]);
-                word |= q << (16 * hs);
+            for (int j = 0; j < WPT; ++j) {
+                const uint32_t sum = pb[j] - pa[j];
+                uint32_t word = 0;
+#pragma unroll
+                for (int hs = 0; hs < 2; ++hs) {
+                    const int di = 2 * (k + j) + hs;
+                    const int d = d0 + di;
+                    const uint32_t sh = (sum >> (16 * hs)) & 0xFFFFu, nh = (cnt[j] >> (8 * hs)) & 0xFFu;
+                    uint32_t q = kInvalidCost;
+                    if (di < D && d >= lo && d < hi && nh > 0) q = div_by_magic(sh, nh, s_magic[nh]);
+                    word |= q << (16 * hs);
+                }
+                wd[j] = word;
             }
-            store_cost_word<U8, true>(cout, dst + (size_t)i * rowstride, word);
+            store_cost_words<U8, WPT>(cout, dst + (size_t)i * rowstride, wd);
         }
         dst += (size_t)kQ * rowstride;
     }
@@ -436,39 +523,49 @@ cudaError_t launch_cross_v_t(int w, int h, int d0, int D, int Dp, int lmax, int 
     const int span = 2 * lmax + kB + kQ + 2;
     if (default_ranges && d0 >= 0 && nthr <= 128) {
         const size_t extra = (size_t)(2 * lmax + 2) * 4 + (size_t)cols * (kSeg + 2 * lmax) + (size_t)cols * kSeg * 2;
-        auto go = [&](auto rs_tag) -> cudaError_t {
+        // two words per thread from 192 padded disparities (one B200, crossV per frame: 1920x1080
+        // D256 0.693 -> 0.590 ms, 1242x375 D192 0.139 -> 0.133; slower with fewer words per pixel:
+        // 1280x720 D128 0.176 -> 0.181, 640x480 D64 0.059 -> 0.075, where a block's arms weigh more)
+        auto go = [&](auto rs_tag, auto wpt_tag) -> cudaError_t {
             constexpr int RS = decltype(rs_tag)::value;
+            constexpr int WPT = decltype(wpt_tag)::value;
             const size_t smem = (size_t)RS * nthr * 4 + extra;
-            auto kern = cross_v_default_kernel<RS, U8>;
+            auto kern = cross_v_default_kernel<RS, U8, WPT>;
             {
                 const cudaError_t e = allow_dynamic_smem(kern, smem);
                 if (e != cudaSuccess) return e;
             }
             dim3 grid((w + cols - 1) / cols, (h + kSeg - 1) / kSeg);
-            kern<<<grid, 128, smem, s>>>(w, h, d0, D, Dp, lmax, tau, cols, gray, tin, cout, magic);
+            kern<<<grid, round_up(nthr / WPT, 32), smem, s>>>(w, h, d0, D, Dp, lmax, tau, cols, gray, tin, cout, magic);
             return cudaGetLastError();
         };
-        if (span <= 64) return go(std::integral_constant<int, 64>());
-        if (span <= 128) return go(std::integral_constant<int, 128>());
-        if (span <= 256) return go(std::integral_constant<int, 256>());
+        auto pick = [&](auto rs_tag) -> cudaError_t {
+            if (W2 >= 96) return go(rs_tag, std::integral_constant<int, 2>());
+            return go(rs_tag, std::integral_constant<int, 1>());
+        };
+        if (span <= 64) return pick(std::integral_constant<int, 64>());
+        if (span <= 128) return pick(std::integral_constant<int, 128>());
+        if (span <= 256) return pick(std::integral_constant<int, 256>());
     }
     if (nthr <= 256) {
         // any ranges: sum and count rings, batched loads
         const size_t extra = (size_t)cols * kSeg * 4 + (size_t)(2 * lmax + 2) * 4 + (size_t)cols * (kSeg + 2 * lmax) +
                              (size_t)cols * kSeg * 2;
+        // one word per thread: two (WPT = 2) made the kernel slower, 1.162 -> 1.305 ms per frame at
+        // HighQuality 1920x1080 D256 (its count ring leaves fewer warps per SM)
         auto go = [&](auto rs_tag, auto kb_tag) -> cudaError_t {
             constexpr int RS = decltype(rs_tag)::value;
             constexpr int KB = decltype(kb_tag)::value;
             const size_t smem = (size_t)RS * nthr * 6 + extra;
-            auto kern = cross_v_count_kernel<RS, KB, U8>;
-            {
+            auto launch = [&](auto kern, int wpt) -> cudaError_t {
                 const cudaError_t e = allow_dynamic_smem(kern, smem);
                 if (e != cudaSuccess) return e;
-            }
-            dim3 grid((w + cols - 1) / cols, (h + kSeg - 1) / kSeg);
-            kern<<<grid, round_up(nthr, 32), smem, s>>>(w, h, d0, D, Dp, lmax, tau, cols, gray, rmin, rmax, tin, cout,
-                                                        magic);
-            return cudaGetLastError();
+                dim3 grid((w + cols - 1) / cols, (h + kSeg - 1) / kSeg);
+                kern<<<grid, round_up(nthr / wpt, 32), smem, s>>>(w, h, d0, D, Dp, lmax, tau, cols, gray, rmin, rmax, tin,
+                                                                  cout, magic);
+                return cudaGetLastError();
+            };
+            return launch(cross_v_count_kernel<RS, KB, U8, 1>, 1);
         };
         auto fits = [&](int rs) { return (size_t)rs * nthr * 6 + extra <= 200 * 1024; };
         // the default arm (lmax <= 17) with 8-row load batches: a ring of exactly the 52 live rows,
