@@ -195,11 +195,28 @@ class ClockSampler:
                 "source": "nvml (separate process)"}
 
 
-def _algorithmic_bytes(name: str, w: int, h: int, D: int, volume_source: bool, npath: int = 4) -> float:
+def _volume_bytes(cfg, tuning) -> float:
+    """Bytes per voxel of the volume the sweeps read, as the engine lays it out: one at 256 padded
+    disparities for the census-only Fast volume and for the aggregated volume of one aggregation
+    pass (tuning cost8: 0 = at 256, 1 = never, 2 = also at 128; 32 lanes per chain), else two."""
+    t = dict(tuning)
+    Dp = (cfg.max_disparity - cfg.min_disparity + 63) // 64 * 64
+    fast_census = (not cfg.agg_enable and cfg.census_type == 1 and not cfg.use_ad and not cfg.use_grad
+                   and not cfg.prior_enable and not cfg.hier_enable and not t.get("fast_fused", 0)
+                   and t.get("cost_kernel", 0) != 1)
+    one_pass = bool(cfg.agg_enable) and cfg.agg_iterations <= 1
+    if t.get("cost8", 0) == 1 or t.get("sgm_lanes", 0) not in (0, 32) or not (fast_census or one_pass):
+        return 2.0
+    return 1.0 if Dp == 256 or (Dp == 128 and t.get("cost8", 0) == 2) else 2.0
+
+
+def _algorithmic_bytes(name: str, w: int, h: int, D: int, volume_source: bool, npath: int = 4,
+                       vb: float = 2.0) -> float:
     """Bytes a launch of `name` must move by design: the stage-boundary traffic of the kernel with
-    u16 path sums and volumes per voxel; a volume-fed sweep reads the cost volume once."""
+    u16 path sums and vb bytes per voxel of the volume the sweeps read (see _volume_bytes); a
+    volume-fed sweep reads that volume once."""
     n = w * h
-    vol = n * D * 2.0 if volume_source else 0.0
+    vol = n * D * vb if volume_source else 0.0
     nfirst = npath - 1
     nin = 3  # Path8: five first-phase buffers folded into one before the last sweep
     return {
@@ -207,8 +224,8 @@ def _algorithmic_bytes(name: str, w: int, h: int, D: int, volume_source: bool, n
         "sgm_fold5": n * D * 12.0,                    # Path8: read 5 buffers, write 1
         "sgm_last_wta": nin * n * D * 2.0 + vol + n * 12,  # read the partial sums, write the WTA maps
         "cost+crossH": n * D * 2.0,                   # write the horizontally aggregated volume
-        "crossV": n * D * 4.0,                        # read T, write C
-        "cost": n * D * 2.0,                          # write the raw volume
+        "crossV": n * D * (2.0 + vb),                 # read T, write C
+        "cost": n * D * vb,                           # write the raw volume
     }.get(name, 0.0)
 
 
@@ -693,13 +710,15 @@ def run_b200(args, wl):
     peak, peak_kind = _peaks()
     totals = {k: sum(v) for k, v in per_kernel.items() if k != "copy"}
     prof_total = sum(totals.values())
+    vb = _volume_bytes(cfg, tuning)
     modelled = {k: v for k, v in totals.items()
-                if _algorithmic_bytes(k, w, h, D, volume_source=True, npath=cfg.paths) > 0}
+                if _algorithmic_bytes(k, w, h, D, volume_source=True, npath=cfg.paths, vb=vb) > 0}
     top = max(modelled or totals, key=(modelled or totals).get)
     top_avg_ms = statistics.mean(per_kernel[top])
-    alg = _algorithmic_bytes(top, w, h, D, volume_source=True, npath=cfg.paths)  # every mode's sweeps read a volume
+    alg = _algorithmic_bytes(top, w, h, D, volume_source=True, npath=cfg.paths, vb=vb)  # every mode's sweeps read a volume
     achieved = alg / (top_avg_ms / 1000.0) / 1e9
     roofline = {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "volume_bytes_per_voxel": vb,
                 "frac": achieved / peak, "peak_kind": peak_kind,
                 "traffic": _profile_traffic(top, label), "algorithmic_bytes_per_launch": alg,
                 "avg_launch_ms": top_avg_ms,
@@ -708,7 +727,7 @@ def run_b200(args, wl):
     # the HBM-bound kernels (the SGM sweeps and the vertical aggregation) against the measured peak,
     # whichever kernel dominates; the cost kernels compute LUT costs and are issue-bound
     roofline["hbm_frac_by_kernel"] = {
-        k: round(_algorithmic_bytes(k, w, h, D, volume_source=True, npath=cfg.paths) /
+        k: round(_algorithmic_bytes(k, w, h, D, volume_source=True, npath=cfg.paths, vb=vb) /
                  (statistics.mean(per_kernel[k]) / 1000.0) / 1e9 / peak, 4)
         for k in ("sgm_first", "sgm_fold5", "sgm_last_wta", "crossV") if k in per_kernel}
     if top in ("cost", "cost+crossH"):
