@@ -457,7 +457,7 @@ __device__ void band_loader(const CostCtx& c, const BandRow<C64>& r, BandRing<C6
     auto copy_win = [&](int u) {
         const int pe = r.xb + r.xs * u - r.eoff;
         if ((unsigned)pe < (unsigned)w)
-            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(smem_u32(&s_win[pe & wmask])),
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(smem_u32(&s_win[(pe & wmask) * kBand])),
                          "l"(r.right + pe));
     };
     if (WIN && r.ok) {
@@ -500,9 +500,9 @@ __device__ void band_loader(const CostCtx& c, const BandRow<C64>& r, BandRing<C6
 
 // WIN: each lane's right-image window ([x - dmax + 1, x - d0] of its row, sliding one pixel per
 // step) lives in shared memory, a ring of wmask + 1 records per lane (a power of two holding the
-// window plus the kRing steps copied ahead); the loader copies the entering pixel with the step's
-// record, so the candidates' right pixels are shared-memory loads.  Without WIN they are global
-// loads kept warm in L1 by the loader's prefetches.  Three warps per block: warp 0 computes, warp 1
+// window plus the kRing steps copied ahead; the lanes' rings interleaved); the loader copies the
+// entering pixel with the step's record, so the candidates' right pixels are shared-memory loads.
+// Without WIN they are global loads kept warm in L1 by the loader's prefetches.  Three warps per block: warp 0 computes, warp 1
 // links the band to its neighbours (band_link), warp 2 loads the step ring (band_loader), so that
 // no copy or address arithmetic sits in the compute warp's step.
 template <bool C64, bool WIN>
@@ -535,7 +535,9 @@ __global__ void __launch_bounds__(96) refine_band_kernel(CostCtx c, int fwd, con
     }
     const BandRow<C64> r(c, band, fwd, steps, lp, rp, work);
     extern __shared__ __align__(16) unsigned char s_dyn[];
-    RPack<C64>* s_win = reinterpret_cast<RPack<C64>*>(s_dyn) + r.lane * (wmask + 2);  // one record of padding
+    // the lanes' window rings interleaved, record i of lane l at i * kBand + l: a step's loads of
+    // the 32 lanes fall in distinct banks whatever their offsets
+    RPack<C64>* s_win = reinterpret_cast<RPack<C64>*>(s_dyn) + r.lane;
     if (warp == 2) {
         band_loader<C64, WIN>(c, r, &s_ring, s_win, wmask, spin_limit);
         return;
@@ -605,10 +607,10 @@ __global__ void __launch_bounds__(96) refine_band_kernel(CostCtx c, int fwd, con
                 const int du = has_u ? min(max(up, lo), hi - 1) : 0;
                 const int xl = x - dl, xu = x - du;
                 const float cl = (has_l && (unsigned)xl < (unsigned)w)
-                                     ? packed_cost<C64>(c, s_lut, l, WIN ? s_win[xl & wmask] : rrow[xl])
+                                     ? packed_cost<C64>(c, s_lut, l, WIN ? s_win[(xl & wmask) * kBand] : rrow[xl])
                                      : 1e6f;
                 const float cu = (has_u && (unsigned)xu < (unsigned)w)
-                                     ? packed_cost<C64>(c, s_lut, l, WIN ? s_win[xu & wmask] : rrow[xu])
+                                     ? packed_cost<C64>(c, s_lut, l, WIN ? s_win[(xu & wmask) * kBand] : rrow[xu])
                                      : 1e6f;
                 // the reference's order: cur, left, up, cur + draw; the first strict minimum wins
                 float best_c = 1e9f;
