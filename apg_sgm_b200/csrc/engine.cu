@@ -309,6 +309,8 @@ Engine::Engine(const apg_pipeline_config_t& cfg, int device, cudaStream_t stream
 Engine::~Engine() {
     release();
     if (copy_stream_) cudaStreamDestroy(copy_stream_);
+    if (post_stream_) cudaStreamDestroy(post_stream_);
+    for (auto& ev : band_ev_) if (ev) cudaEventDestroy(ev);
     if (side_stream_) cudaStreamDestroy(side_stream_);
     if (ev_maps_) cudaEventDestroy(ev_maps_);
     if (ev_copied_) cudaEventDestroy(ev_copied_);
@@ -494,6 +496,14 @@ int Engine::process_host(const uint8_t* left, const uint8_t* right, int w, int h
             return fail(kInternalError, "copy stream creation failed");
         }
     }
+    if (!post_stream_) {
+        bool ok = cudaStreamCreateWithFlags(&post_stream_, cudaStreamNonBlocking) == cudaSuccess;
+        for (auto& ev : band_ev_) ok = ok && cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) == cudaSuccess;
+        if (!ok) {
+            cudaGetLastError();
+            return fail(kInternalError, "post stream creation failed");
+        }
+    }
     cudaError_t e;
     if (inputs_pinned) {
         e = cudaMemcpy2DAsync(ptr<uint8_t>(lay_.in_left), row, left, stride, row, h, cudaMemcpyHostToDevice, stream_);
@@ -513,26 +523,39 @@ int Engine::process_host(const uint8_t* left, const uint8_t* right, int w, int h
     early_rel_ = prel;
     early_reason_ = preason;
     early_issued_ = early_reason_done_ = false;
-    rc = run(ptr<uint8_t>(lay_.in_left), (int)row, ptr<uint8_t>(lay_.in_right), (int)row, ch, nullptr, nullptr, nullptr,
-             nullptr);
+    // as run(), with the last sweep in row bands where the path allows it (run_banded issues every
+    // output copy itself, the last one followed by ev_copied_)
+    nprof_ = 0;
+    if (debug_ & 8) cudaEventRecord(pev_[0], stream_);
+    bool banded = false;
+    rc = run_pre(ptr<uint8_t>(lay_.in_left), (int)row, ptr<uint8_t>(lay_.in_right), (int)row, ch);
+    if (rc == kOk) {
+        const int nb = host_band_count();
+        banded = nb > 1;
+        rc = banded ? run_banded(nb, pdisp, pconf, preason, prel) : run_sgm();
+        if (rc == kOk && !banded) rc = run_post(nullptr, nullptr, nullptr, nullptr);
+    }
     early_conf_ = nullptr;
     early_rel_ = nullptr;
     early_reason_ = nullptr;
     if (rc) {
+        cudaStreamSynchronize(post_stream_);
         cudaStreamSynchronize(copy_stream_);
         return rc;
     }
     e = cudaSuccess;
-    if (pdisp) e = cudaMemcpyAsync(pdisp, ptr<float>(lay_.disp_out), n * 4, cudaMemcpyDeviceToHost, stream_);
-    if (e == cudaSuccess && pconf && !early_issued_)
-        e = cudaMemcpyAsync(pconf, ptr<float>(lay_.confidence), n * 4, cudaMemcpyDeviceToHost, stream_);
-    if (e == cudaSuccess && preason && !early_reason_done_)
-        e = cudaMemcpyAsync(preason, ptr<uint8_t>(lay_.reason), n, cudaMemcpyDeviceToHost, stream_);
-    if (e == cudaSuccess && prel && !early_issued_)
-        e = cudaMemcpyAsync(prel, ptr<uint8_t>(lay_.reliable), n, cudaMemcpyDeviceToHost, stream_);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(counts_, ptr<unsigned long long>(lay_.stats), sizeof(counts_),
-                                              cudaMemcpyDeviceToHost, stream_);
-    if (e == cudaSuccess && early_issued_) e = cudaStreamWaitEvent(stream_, ev_copied_, 0);
+    if (!banded) {
+        if (pdisp) e = cudaMemcpyAsync(pdisp, ptr<float>(lay_.disp_out), n * 4, cudaMemcpyDeviceToHost, stream_);
+        if (e == cudaSuccess && pconf && !early_issued_)
+            e = cudaMemcpyAsync(pconf, ptr<float>(lay_.confidence), n * 4, cudaMemcpyDeviceToHost, stream_);
+        if (e == cudaSuccess && preason && !early_reason_done_)
+            e = cudaMemcpyAsync(preason, ptr<uint8_t>(lay_.reason), n, cudaMemcpyDeviceToHost, stream_);
+        if (e == cudaSuccess && prel && !early_issued_)
+            e = cudaMemcpyAsync(prel, ptr<uint8_t>(lay_.reliable), n, cudaMemcpyDeviceToHost, stream_);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(counts_, ptr<unsigned long long>(lay_.stats), sizeof(counts_),
+                                                  cudaMemcpyDeviceToHost, stream_);
+    }
+    if (e == cudaSuccess && (early_issued_ || banded)) e = cudaStreamWaitEvent(stream_, ev_copied_, 0);
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
     if (e != cudaSuccess) return cuda_fail(e, "output download");
     rc = check_refine();
@@ -985,6 +1008,127 @@ int Engine::run_post(float* d_disp, float* d_conf, uint8_t* d_reason, uint8_t* d
     return kOk;
 }
 
+// Banded host path.  The last sweep runs bottom-up, so its rows finish from the bottom of the
+// frame: it runs as nb launches over bands of rows (the chains' L and m carried between launches),
+// and after each band, on post_stream_, the confidence / LR of the band's rows, then the fill and
+// the median of the rows whose neighbourhoods are final (each stage reads one row above and below
+// its own), then on copy_stream_ the device-to-host copies of every map row that is final.  The
+// copies of all but the top band overlap the sweep.  Same kernels, same maps as run_sgm +
+// run_post; frame counters over the whole map at the end.
+int Engine::host_band_count() const {
+    const Layout& L = lay_;
+    if (host_bands_ == 1 || debug_ || !post_stream_ || !copy_stream_) return 0;
+    if (refine_enabled() || L.nsbuf != 3 || L.h < 256 || cfg_.median_radius > 1) return 0;
+    if (scope_.sp_telem || scope_.ip_telem) return 0;
+    const int gap = (scope_.ip_method == 0 && scope_.ip_gap == 32) ? cfg_.max_fill_gap : scope_.ip_gap;
+    if (!skip_fill_ && gap < 0) return 0;
+    SgmLaunch pl;
+    uint32_t* sb[7];
+    sgm_launch(&pl, sb);
+    if (!sgm_last_band_supported(pl, 3)) return 0;
+    // the chains' state between bands lives in the refiner's map, unused without the refiner
+    if ((size_t)32 * (L.Dp / 64 + 1) * 4 > (size_t)L.h * 4) return 0;
+    return host_bands_ > 1 ? std::min(host_bands_, (int)kMaxBands) : (int)kBands;
+}
+
+int Engine::run_banded(int nb, float* hdisp, float* hconf, uint8_t* hreason, uint8_t* hrel) {
+    const Layout& L = lay_;
+    const int w = L.w, h = L.h;
+    const size_t n = (size_t)w * h;
+    cudaStream_t s = stream_, ps = post_stream_, cs = copy_stream_;
+    unsigned launches = 0;
+    cudaError_t e = cudaSuccess;
+    const bool prof = false;
+    static const int first4[3][2] = {{1, 0}, {-1, 0}, {0, 1}};
+    SgmLaunch pl;
+    uint32_t* sb[7];
+    sgm_launch(&pl, sb);
+    RUN(launch_sgm_first(pl, 3, first4, sb, s), "sgm_first");
+    // the confidence stage reads the right-image disparity
+    if (rwta_forked_) RUNC(cudaStreamWaitEvent(ps, ev_[11], 0), "join");
+    ConfLrArgs ca;
+    ca.w = w; ca.h = h;
+    ca.disp = ptr<float>(L.disp_wta); ca.disp_right = ptr<float>(L.disp_right);
+    ca.best = ptr<float>(L.best); ca.second = ptr<float>(L.second);
+    ca.lgx = ptr<uint8_t>(L.lgx); ca.lgy = ptr<uint8_t>(L.lgy);
+    ca.uniqueness_ratio = cfg_.conf_uniqueness_ratio; ca.min_texture = cfg_.conf_min_texture;
+    ca.reliable_threshold = cfg_.conf_reliable_threshold; ca.conf_lr_max_diff = cfg_.conf_lr_max_diff;
+    ca.confidence = ptr<float>(L.confidence);
+    ca.reliable = ptr<uint8_t>(L.reliable);
+    ca.reason = ptr<uint8_t>(L.reason);
+    ca.fuse_lr = 1;
+    ca.lr_check = cfg_.lr_check;
+    ca.post_lr_max_diff = cfg_.post_lr_max_diff;
+    ca.disp_out = ptr<float>(L.disp_lr);
+    const bool fill = !skip_fill_;
+    const bool med = cfg_.median_radius == 1;
+    const int gap = (scope_.ip_method == 0 && scope_.ip_gap == 32) ? cfg_.max_fill_gap : scope_.ip_gap;
+    const float* lr_map = ptr<float>(L.disp_lr);
+    float* fill_map = ptr<float>(L.disp_fill);
+    const float* med_in = fill ? fill_map : lr_map;
+    const float* final_map = med ? ptr<float>(L.disp_out) : med_in;
+    const int dfinal = (fill ? 1 : 0) + (med ? 1 : 0);  // rows a final row needs below the LR rows
+    const int bs = round_up((h + nb - 1) / nb, 32);     // steps per band (the WTA's 32-step blocks)
+    uint32_t* carry = ptr<uint32_t>(L.disp_ref);
+    int fill_hi = h, fin_hi = h;  // rows [fill_hi, h) of the fill map, [fin_hi, h) of the final map are done
+    int band = 0;
+    for (int t0 = 0; t0 < h; t0 += bs, ++band) {
+        const int t1 = std::min(h, t0 + bs);
+        RUN(launch_sgm_last_band(pl, 0, -1, 3, sb, t0, t1, carry, s), "sgm_last_band");
+        RUNC(cudaEventRecord(band_ev_[2 * band], s), "event");
+        RUNC(cudaStreamWaitEvent(ps, band_ev_[2 * band], 0), "event");
+        const int ylo = h - t1, yhi = h - t0;
+        const bool top = ylo == 0;
+        // confidence + LR of the band's rows (each reads only its own row of the right-image map)
+        const size_t o = (size_t)ylo * w, rows = (size_t)(yhi - ylo) * w;
+        ConfLrArgs cb = ca;
+        cb.h = yhi - ylo;
+        cb.disp += o; cb.disp_right += o; cb.best += o; cb.second += o; cb.lgx += o; cb.lgy += o;
+        cb.confidence += o; cb.reliable += o; cb.reason += o; cb.disp_out += o;
+        RUN(launch_conf_lr(cb, ps), "confidence");
+        if (fill) {
+            const int flo = top ? 0 : ylo + 1;
+            if (flo < fill_hi)
+                RUN(launch_fill_rows(w, h, flo, fill_hi, gap, scope_.ip_method == 1, lr_map, ptr<uint8_t>(L.reason),
+                                     ptr<uint8_t>(L.lgray), ranged() ? ptr<float>(L.d_prior) : nullptr, fill_map, ps),
+                    "fill");
+            fill_hi = flo;
+        }
+        const int mlo = top ? 0 : ylo + dfinal;
+        if (med && mlo < fin_hi) RUN(launch_median3_rows(w, h, mlo, fin_hi, med_in, ptr<float>(L.disp_out), ps), "median");
+        RUNC(cudaEventRecord(band_ev_[2 * band + 1], ps), "event");
+        RUNC(cudaStreamWaitEvent(cs, band_ev_[2 * band + 1], 0), "event");
+        if (hconf) RUNC(cudaMemcpyAsync(hconf + o, ptr<float>(L.confidence) + o, rows * 4, cudaMemcpyDeviceToHost, cs), "conf out");
+        if (hrel) RUNC(cudaMemcpyAsync(hrel + o, ptr<uint8_t>(L.reliable) + o, rows, cudaMemcpyDeviceToHost, cs), "rel out");
+        if (hreason) RUNC(cudaMemcpyAsync(hreason + o, ptr<uint8_t>(L.reason) + o, rows, cudaMemcpyDeviceToHost, cs), "reason out");
+        if (hdisp && mlo < fin_hi) {
+            const size_t fo = (size_t)mlo * w;
+            RUNC(cudaMemcpyAsync(hdisp + fo, final_map + fo, (size_t)(fin_hi - mlo) * w * 4, cudaMemcpyDeviceToHost, cs),
+                 "disp out");
+        }
+        fin_hi = mlo;
+    }
+    cudaEventRecord(ev_[6], s);
+    cudaEventRecord(ev_[7], ps);
+    cudaEventRecord(ev_[8], ps);
+    // PipelineStats counters over the whole map (src/pipeline.cpp:650-707)
+    unsigned long long* st = ptr<unsigned long long>(L.stats);
+    RUNC(cudaMemsetAsync(st, 0, 64, ps), "stats init");
+    const bool planes = range_planes_needed();
+    RUN(launch_frame_stats((int)n, final_map, ptr<uint8_t>(L.reliable), ptr<uint8_t>(L.reason), nullptr, nullptr,
+                           planes ? ptr<int16_t>(L.rmin) : nullptr, planes ? ptr<int16_t>(L.rmax) : nullptr,
+                           planes ? 0ull : default_range_width_sum(), st, ps),
+        "frame stats");
+    if (prior_runs()) RUNC(cudaMemcpyAsync(st + 5, arena_ + L.pr_count, 4, cudaMemcpyDeviceToDevice, ps), "support count");
+    cudaEventRecord(ev_[9], ps);
+    RUNC(cudaStreamWaitEvent(cs, ev_[9], 0), "event");
+    RUNC(cudaMemcpyAsync(counts_, st, sizeof(counts_), cudaMemcpyDeviceToHost, cs), "counters out");
+    RUNC(cudaEventRecord(ev_copied_, cs), "event");
+    have_times_ = true;
+    count_launches(launches);
+    return kOk;
+}
+
 // HierarchicalStereo::estimate_search_range (src/hierarchical_stereo.cpp:113-431) after the
 // full-size aux planes: the half-size grays, the whole pipeline over them on the coarse engine
 // (same stream, its outputs stay in its arena), then every full-size pixel's range and guiding
@@ -1280,6 +1424,11 @@ int set_tuning(Engine* e, const char* key, int value) {
     if (std::strcmp(key, "refine_spin_limit") == 0) {
         if (value < 0) return kInvalidConfig;
         if (e) e->set_refine_spin_limit(value);
+        return kOk;
+    }
+    if (std::strcmp(key, "host_bands") == 0) {
+        if (value < 0 || value > Engine::kMaxBands) return kInvalidConfig;
+        if (e) e->set_host_bands(value);
         return kOk;
     }
     if (std::strcmp(key, "refine_window") == 0) {

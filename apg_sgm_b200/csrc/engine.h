@@ -169,6 +169,11 @@ public:
     // right-image window (0: where it fits, 1: never, the L1 form)
     void set_refine_spin_limit(int n) { refine_.spin_limit = n; }
     void set_refine_window(int mode) { refine_.window = mode; }
+    // host-output frames: the last sweep in this many row bands, each band's rows post-processed
+    // and copied out while the next band runs (0: kBands where the path allows it, 1: never)
+    void set_host_bands(int n) { host_bands_ = n; }
+    static constexpr int kBands = 6;
+    static constexpr int kMaxBands = 16;
     // takes the calling thread's experimental scopes now (run_pre does so for every frame; the
     // batched form needs them before it builds SGM plans from sgm_launch)
     void capture_scope() { scope_ = experimental_scope(); }
@@ -200,6 +205,10 @@ private:
     int run_pre(const uint8_t* dl, int lstride, const uint8_t* dr, int rstride, int ch);
     int run_sgm();
     int run_post(float* d_disp, float* d_conf, uint8_t* d_reason, uint8_t* d_reliable);
+    // run_sgm + run_post for host outputs with the last sweep in row bands (host_band_count() > 1):
+    // every map row goes to the host pointers on copy_stream_ as soon as it is final
+    int host_band_count() const;
+    int run_banded(int nb, float* hdisp, float* hconf, uint8_t* hreason, uint8_t* hrel);
     int run_prior();
     int run_hier();
     // per-pixel ranges: from the prior or from the hierarchical pass (every other frame has the
@@ -225,6 +234,7 @@ private:
     bool fast_fused_ = false;
     int cost_tile_ = 0;
     int cost_kernel_ = 0;  // 0: pixel-run cost kernel where it applies, 1: column-tile kernel
+    int host_bands_ = 0;   // see set_host_bands
     RefineTuning refine_;
     cudaStream_t stream_ = nullptr;
     bool own_stream_ = false;
@@ -266,6 +276,9 @@ private:
     cudaStream_t side_stream_ = nullptr;  // the right-image WTA finalize, beside aggregation and SGM
     bool rwta_forked_ = false;            // the last frame finalized it there (join before confidence)
     cudaEvent_t ev_maps_ = nullptr, ev_copied_ = nullptr;
+    // banded host path: the post-processing stream and the per-band events (sweep done, rows done)
+    cudaStream_t post_stream_ = nullptr;
+    cudaEvent_t band_ev_[2 * kMaxBands] = {};
     float* early_conf_ = nullptr;
     uint8_t* early_reason_ = nullptr;
     uint8_t* early_rel_ = nullptr;

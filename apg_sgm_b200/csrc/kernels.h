@@ -81,6 +81,13 @@ cudaError_t launch_sgm_first(const SgmLaunch& l, int ndir, const int (*dirs)[2],
                              cudaStream_t s);
 // Last sweep (dx, dy): adds the nin (1 or 3) partial sums in[] and writes the WTA maps.
 cudaError_t launch_sgm_last(const SgmLaunch& l, int dx, int dy, int nin, const uint32_t* const* in, cudaStream_t s);
+// The last sweep's steps [t_begin, t_end) only (t_begin a multiple of 32), the chains' state
+// between bands in `carry` (32 * (Dp / 64 + 1) words per chain): one warp per chain, volume-fed,
+// three partial sums, Dp 128 / 192 / 256.  A sequence of bands covering every step gives the maps of
+// launch_sgm_last.
+bool sgm_last_band_supported(const SgmLaunch& l, int nin);
+cudaError_t launch_sgm_last_band(const SgmLaunch& l, int dx, int dy, int nin, const uint32_t* const* in, int t_begin,
+                                 int t_end, uint32_t* carry, cudaStream_t s);
 // bufs[0] += bufs[1..6] (saturating u16 lanes), `words` 32-bit words each.
 // Path8: adds bufs[1 .. nbuf) into bufs[0] (nbuf 5 or 7), saturating per halfword.
 cudaError_t launch_sgm_fold(uint32_t* const* bufs, int nbuf, size_t words, cudaStream_t s);
@@ -132,6 +139,12 @@ cudaError_t launch_fill(int w, int h, int gap, int shadow, apg_inpaint_telemetry
                         const uint8_t* reason, const uint8_t* gray,
                         const float* d_prior, float* out, cudaStream_t s);
 cudaError_t launch_median(int w, int h, int r, const float* in, float* out, cudaStream_t s);
+// Rows [y_begin, y_end) only: the ballot fill (gap >= 0) and the 3x3 median; the rows they read
+// around the range (one above and one below) must be final.
+cudaError_t launch_fill_rows(int w, int h, int y_begin, int y_end, int gap, int shadow, const float* in,
+                             const uint8_t* reason, const uint8_t* gray, const float* d_prior, float* out,
+                             cudaStream_t s);
+cudaError_t launch_median3_rows(int w, int h, int y_begin, int y_end, const float* in, float* out, cudaStream_t s);
 cudaError_t launch_frame_stats(int n, const float* disp, const uint8_t* reliable, const uint8_t* reason,
                                const float* before, const float* after, const int16_t* rmin, const int16_t* rmax,
                                unsigned long long range_sum, unsigned long long* out5, cudaStream_t s);

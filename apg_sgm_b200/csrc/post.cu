@@ -244,15 +244,18 @@ __global__ void median_kernel(int w, int h, int r, const float* __restrict__ in,
 // gap.  The nearest stopper on each side comes from the segments' stopper masks (this segment,
 // then further ones while some lane's gap reaches them), so each pixel costs a few bit operations
 // instead of a walk.  Everything after the two neighbours is the per-pixel rule above.
-__global__ void fill_ballot_kernel(int w, int h, int gap, int shadow, const float* __restrict__ in,
-                                   const uint8_t* __restrict__ reason, const uint8_t* __restrict__ gray,
-                                   const float* __restrict__ d_prior, float* __restrict__ out) {
+// Rows [y_begin, y_end) of the frame (the whole frame, or one band of the host-output path).
+__global__ void fill_ballot_kernel(int w, int h, int y_begin, int y_end, int gap, int shadow,
+                                   const float* __restrict__ in, const uint8_t* __restrict__ reason,
+                                   const uint8_t* __restrict__ gray, const float* __restrict__ d_prior,
+                                   float* __restrict__ out) {
     const int lane = threadIdx.x & 31;
     const int nseg = (w + 31) >> 5;
-    const int total = nseg * h;  // segments of the frame (w * h / 32 + h, far below 2^31)
+    const int total = nseg * (y_end - y_begin);  // segments of the rows (w * h / 32 + h, far below 2^31)
     const int wstride = (gridDim.x * blockDim.x) >> 5;
     for (int sg = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; sg < total; sg += wstride) {
-        const int y = sg / nseg, s = sg - y * nseg;
+        const int yb = sg / nseg, s = sg - yb * nseg;
+        const int y = y_begin + yb;
         const int x = (s << 5) + lane;
         const float* row = in + (size_t)y * w;
         const bool inimg = x < w;
@@ -352,10 +355,12 @@ __device__ __forceinline__ void cswap(float& a, float& b) {
     b = hi;
 }
 
-__global__ void __launch_bounds__(kMedTX * kMedTY) median3_kernel(int w, int h, const float* __restrict__ in,
+// Rows [y_begin, y_end) of the frame (the window reads rows y_begin - 1 .. y_end inside the frame).
+__global__ void __launch_bounds__(kMedTX * kMedTY) median3_kernel(int w, int h, int y_begin, int y_end,
+                                                                  const float* __restrict__ in,
                                                                   float* __restrict__ out) {
     __shared__ float t[kMedTY + 2][kMedTX + 2];
-    const int x0 = blockIdx.x * kMedTX, y0 = blockIdx.y * kMedTY;
+    const int x0 = blockIdx.x * kMedTX, y0 = y_begin + blockIdx.y * kMedTY;
     const int tid = threadIdx.y * kMedTX + threadIdx.x;
     for (int i = tid; i < (kMedTY + 2) * (kMedTX + 2); i += kMedTX * kMedTY) {
         const int sy = i / (kMedTX + 2), sx = i - sy * (kMedTX + 2);
@@ -365,7 +370,7 @@ __global__ void __launch_bounds__(kMedTX * kMedTY) median3_kernel(int w, int h, 
     }
     __syncthreads();
     const int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
-    if (x >= w || y >= h) return;
+    if (x >= w || y >= y_end) return;
     float v[9];
     int cnt = 0;
 #pragma unroll
@@ -505,7 +510,7 @@ cudaError_t launch_fill(int w, int h, int gap, int shadow, apg_inpaint_telemetry
     if (gap >= 0) {
         const long long warps = (long long)((w + 31) / 32) * h;
         const int blocks = (int)std::min<long long>((warps + 7) / 8, 148 * 16);
-        fill_ballot_kernel<<<blocks, 256, 0, s>>>(w, h, gap, shadow, in, reason, gray, d_prior, out);
+        fill_ballot_kernel<<<blocks, 256, 0, s>>>(w, h, 0, h, gap, shadow, in, reason, gray, d_prior, out);
     } else {
         fill_kernel<<<grid_for(w * h), 256, 0, s>>>(w, h, gap, shadow, nullptr, in, reason, gray, d_prior, out);
     }
@@ -515,10 +520,27 @@ cudaError_t launch_fill(int w, int h, int gap, int shadow, apg_inpaint_telemetry
 cudaError_t launch_median(int w, int h, int r, const float* in, float* out, cudaStream_t s) {
     if (r == 1) {
         const dim3 grid((w + kMedTX - 1) / kMedTX, (h + kMedTY - 1) / kMedTY), block(kMedTX, kMedTY);
-        median3_kernel<<<grid, block, 0, s>>>(w, h, in, out);
+        median3_kernel<<<grid, block, 0, s>>>(w, h, 0, h, in, out);
     } else {
         median_kernel<<<grid_for(w * h), 256, 0, s>>>(w, h, r, in, out);
     }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fill_rows(int w, int h, int y_begin, int y_end, int gap, int shadow, const float* in,
+                             const uint8_t* reason, const uint8_t* gray, const float* d_prior, float* out,
+                             cudaStream_t s) {
+    if (gap < 0 || y_begin < 0 || y_end > h || y_end <= y_begin) return cudaErrorInvalidValue;
+    const long long warps = (long long)((w + 31) / 32) * (y_end - y_begin);
+    const int blocks = (int)std::min<long long>((warps + 7) / 8, 148 * 16);
+    fill_ballot_kernel<<<blocks, 256, 0, s>>>(w, h, y_begin, y_end, gap, shadow, in, reason, gray, d_prior, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_median3_rows(int w, int h, int y_begin, int y_end, const float* in, float* out, cudaStream_t s) {
+    if (y_begin < 0 || y_end > h || y_end <= y_begin) return cudaErrorInvalidValue;
+    const dim3 grid((w + kMedTX - 1) / kMedTX, (y_end - y_begin + kMedTY - 1) / kMedTY), block(kMedTX, kMedTY);
+    median3_kernel<<<grid, block, 0, s>>>(w, h, y_begin, y_end, in, out);
     return cudaGetLastError();
 }
 

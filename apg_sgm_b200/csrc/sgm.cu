@@ -144,6 +144,11 @@ struct SgmArgs {
     apg_subpixel_telemetry_t* sp_tel;
     int store_final;
     int cost8;  // cvol holds one byte per voxel (0xFF invalid)
+    // a band of the last sweep's steps, [t_begin, t_end) (the banded one-warp kernel only): the
+    // chains' L and m enter from `carry` when t_begin > 0 and leave there when t_end is short of
+    // the chain's end (32 * (K + 1) words per chain: K words of L, then m, each lane its column)
+    int t_begin, t_end;
+    uint32_t* carry;
 };
 
 // Directions of one launch; warps [warp_begin[i], warp_begin[i+1]) run direction i.
@@ -624,18 +629,30 @@ __device__ __forceinline__ void wta_row(const SgmArgs& a, const uint32_t* row, i
 // Steps run in blocks of T: at the start of a block lane j loads the gray level of step t0 + j
 // (prefetched one block ahead) and computes that step's adaptive P2, so a step costs one shuffle
 // for P2 instead of a load and the P2 arithmetic.  Addresses advance by a 32-bit word offset.
-template <int T, int K, int MODE, int PF, int NB, bool C8 = false>
+//
+// BAND: only the steps [a.t_begin, a.t_end) of the chain (t_begin a multiple of T = 32, one chain
+// per warp), starting from the L and m a previous band left in a.carry and leaving them there when
+// the chain goes on; the steps and the WTA of each step are those of the whole chain.
+template <int T, int K, int MODE, int PF, int NB, bool C8 = false, bool BAND = false>
 __device__ __forceinline__ void run_chain_vol(const SgmArgs& a, const uint32_t* const* in, uint32_t* s_ring,
                                               uint32_t* s_wta, int dx, int dy, int s, int nscan, uint32_t* out) {
     static_assert((PF & (PF - 1)) == 0 && T % PF == 0, "PF: a power of two dividing T");
+    static_assert(!BAND || (T == 32 && MODE == kLast), "bands: the one-warp last sweep");
     constexpr int SW = vol_slot_words<K, NB>();
     const int lane = threadIdx.x & 31;
     const int grp = lane / T, j = lane % T;
     const unsigned gmask = T == 32 ? 0xffffffffu : (((1u << T) - 1u) << (grp * T));
     int x0, y0, len;
     scan_start(a, dx, dy, s, nscan, x0, y0, len);
+    int tb = 0;             // first step of this launch
+    bool carry_out = false;  // the chain goes on after this band
+    if constexpr (BAND) {
+        tb = a.t_begin;
+        carry_out = a.t_end < len;
+        len = min(len, a.t_end);
+    }
     const int maxlen = __reduce_max_sync(0xffffffffu, len);
-    if (maxlen == 0) return;
+    if (maxlen <= tb) return;
     const int W2 = a.Dp / 2;
     const int step = dy * a.w + dx;
     const int p0 = y0 * a.w + x0;
@@ -654,12 +671,13 @@ __device__ __forceinline__ void run_chain_vol(const SgmArgs& a, const uint32_t* 
         }
         cp_commit();
     };
-    const uint32_t off0 = (uint32_t)p0 * (uint32_t)W2 + (uint32_t)(j * K);
-    const uint32_t coff0 = C8 ? (uint32_t)p0 * (uint32_t)(W2 / 2) + (uint32_t)(j * (K / 2)) : off0;
+    const uint32_t off0 = (uint32_t)p0 * (uint32_t)W2 + (uint32_t)(j * K) + (uint32_t)tb * dstep;
+    const uint32_t coff0 =
+        C8 ? (uint32_t)p0 * (uint32_t)(W2 / 2) + (uint32_t)(j * (K / 2)) + (uint32_t)tb * cstep : off0;
     uint32_t ioff = off0, icoff = coff0;  // offsets of the next step to issue
 #pragma unroll
     for (int t = 0; t < PF; ++t) {
-        issue(t, ioff, icoff);
+        issue(tb + t, ioff, icoff);
         ioff += dstep;
         icoff += cstep;
     }
@@ -669,10 +687,19 @@ __device__ __forceinline__ void run_chain_vol(const SgmArgs& a, const uint32_t* 
     uint32_t m = kInf;
 #pragma unroll
     for (int k = 0; k < K; ++k) L[k] = kInf2;
-    int gnext = j < len ? (int)__ldg(a.gray + p0 + j * step) : 0;
+    int gnext = tb + j < len ? (int)__ldg(a.gray + p0 + (tb + j) * step) : 0;
     int gcarry = 0;
+    if constexpr (BAND) {
+        if (tb > 0) {
+            const uint32_t* cs = a.carry + (size_t)s * (K + 1) * 32 + lane;
+#pragma unroll
+            for (int k = 0; k < K; ++k) L[k] = __ldcg(cs + k * 32);
+            m = __ldcg(cs + K * 32);
+            gcarry = (int)__ldg(a.gray + p0 + (tb - 1) * step);
+        }
+    }
 
-    for (int t0 = 0; t0 < maxlen; t0 += T) {
+    for (int t0 = tb; t0 < maxlen; t0 += T) {
         // P2 of the steps [t0, t0 + T): lane j holds step t0 + j
         const int gcur = gnext;
         {
@@ -768,6 +795,14 @@ __device__ __forceinline__ void run_chain_vol(const SgmArgs& a, const uint32_t* 
             if (t0 + j < len)
                 wta_row<K * T>(a, s_wta + grp * T * (K * T + 1) + j * (K * T + 1), p0 + (t0 + j) * step);
             __syncwarp();
+        }
+    }
+    if constexpr (BAND) {
+        if (carry_out) {
+            uint32_t* cs = a.carry + (size_t)s * (K + 1) * 32 + lane;
+#pragma unroll
+            for (int k = 0; k < K; ++k) __stcg(cs + k * 32, L[k]);
+            __stcg(cs + K * 32, m);
         }
     }
     cp_wait<0>();
@@ -1082,7 +1117,7 @@ __global__ void __launch_bounds__(128) sgm_first_kernel(SgmArgs a, DirTable tab)
 }
 
 // Last sweep (one direction): add the NB partial sums and run the WTA.
-template <int T, int K, bool CENSUS, int NB, bool C8 = false>
+template <int T, int K, bool CENSUS, int NB, bool C8 = false, bool BAND = false>
 __global__ void __launch_bounds__(128) sgm_last_kernel(SgmArgs a, DirTable tab) {
     __shared__ uint16_t s_q[65];
     if (CENSUS) {
@@ -1097,8 +1132,8 @@ __global__ void __launch_bounds__(128) sgm_last_kernel(SgmArgs a, DirTable tab) 
         constexpr int PF = last_pf<K, T, NB>();
         constexpr int per_warp = PF * vol_slot_words<K, NB>() + wta_buf_words<K, T>();
         uint32_t* ring = s_dyn + (threadIdx.x >> 5) * per_warp;
-        run_chain_vol<T, K, kLast, PF, NB, C8>(a, tab.in, ring, ring + PF * vol_slot_words<K, NB>(), tab.dx[0], tab.dy[0],
-                                           s, tab.nscan[0], nullptr);
+        run_chain_vol<T, K, kLast, PF, NB, C8, BAND>(a, tab.in, ring, ring + PF * vol_slot_words<K, NB>(), tab.dx[0],
+                                                 tab.dy[0], s, tab.nscan[0], nullptr);
         return;
     }
     using UR = Unroll<K, CENSUS, 0, kLast>;
@@ -1490,6 +1525,9 @@ SgmArgs make_args(const SgmLaunch& l) {
     a.sp_tel = l.sp_tel;
     a.store_final = l.store_final;
     a.cost8 = l.cost8;
+    a.t_begin = 0;
+    a.t_end = 0x7FFFFFFF;
+    a.carry = nullptr;
     return a;
 }
 
@@ -1530,6 +1568,52 @@ cudaError_t launch_sgm_last(const SgmLaunch& l, int dx, int dy, int nin, const u
     tab.nin = nin;
     for (int i = 0; i < nin; ++i) tab.in[i] = in[i];
     return dispatch<false>(a, tab, l.cvol == nullptr, sgm_lanes_for(l.Dp, l.lanes), l.split, st);
+}
+
+// ---- the last sweep in bands of steps (the host-output path copies each band's rows out while
+// the next band runs)
+
+namespace {
+template <int K, bool C8>
+cudaError_t launch_last_band_k(const SgmArgs& a, DirTable tab, cudaStream_t st) {
+    constexpr int NB = 3;
+    tab.nscan[0] = nscan_of(a, tab.dx[0], tab.dy[0]);
+    const size_t smem = (size_t)(last_pf<K, 32, NB>() * vol_slot_words<K, NB>() + wta_buf_words<K, 32>()) * 4;
+    auto kern = sgm_last_kernel<32, K, false, NB, C8, true>;
+    const cudaError_t e = allow_dynamic_smem(kern, smem);
+    if (e != cudaSuccess) return e;
+    kern<<<tab.nscan[0], 32, smem, st>>>(a, tab);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+bool sgm_last_band_supported(const SgmLaunch& l, int nin) {
+    if (nin != 3 || !l.cvol || l.store_final || l.sp_tel) return false;
+    if (l.Dp != 128 && l.Dp != 192 && l.Dp != 256) return false;
+    if (sgm_lanes_for(l.Dp, l.lanes) != 32) return false;
+    return !use_split(32, l.Dp / 64, false, l.split);
+}
+
+cudaError_t launch_sgm_last_band(const SgmLaunch& l, int dx, int dy, int nin, const uint32_t* const* in, int t_begin,
+                                 int t_end, uint32_t* carry, cudaStream_t st) {
+    if (!sgm_last_band_supported(l, nin) || t_begin < 0 || (t_begin & 31) || t_end <= t_begin || !carry)
+        return cudaErrorInvalidValue;
+    SgmArgs a = make_args(l);
+    a.t_begin = t_begin;
+    a.t_end = t_end;
+    a.carry = carry;
+    DirTable tab = {};
+    tab.n = 1;
+    tab.dx[0] = dx;
+    tab.dy[0] = dy;
+    tab.nin = nin;
+    for (int i = 0; i < nin; ++i) tab.in[i] = in[i];
+    switch (l.Dp) {
+        case 128: return a.cost8 ? launch_last_band_k<2, true>(a, tab, st) : launch_last_band_k<2, false>(a, tab, st);
+        case 192: return a.cost8 ? cudaErrorInvalidValue : launch_last_band_k<3, false>(a, tab, st);
+        default: return a.cost8 ? launch_last_band_k<4, true>(a, tab, st) : launch_last_band_k<4, false>(a, tab, st);
+    }
 }
 
 cudaError_t launch_sgm_fold(uint32_t* const* bufs, int nbuf, size_t words, cudaStream_t st) {

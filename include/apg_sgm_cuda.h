@@ -73,7 +73,13 @@ APGCU_API int apgcu_engine_set_debug(apgcu_engine_t e, int flags);
  *            every quantised cost is below 255): 0 = at 256 padded disparities (default),
  *            1 = never, 2 = at 128 and 256;
  *   "refine_window": 0 = HighQuality refiner reads the right-image window from shared memory where
- *                 every band fits on the device at once (default), 1 = always through L1.
+ *                 every band fits on the device at once (default), 1 = always through L1;
+ *   "host_bands": frames whose outputs go to host memory (apgcu_engine_process, the session) run
+ *                 the last SGM sweep in this many row bands, 2..16, and each band's finished map
+ *                 rows are post-processed and copied to the host while the next band runs:
+ *                 0 = 6 bands where the path allows it (default; Path4, 128..256 padded
+ *                 disparities, one warp per chain, no refiner, 3x3 or no median, no telemetry
+ *                 scope, at least 256 rows), 1 = never (one sweep, then the copies).
  * And one key that bounds a wait rather than tuning speed:
  *   "refine_spin_limit": polls (each ~128 ns) before a refiner band stops waiting for the band above
  *                 (0 = default, about a second).  A wait that runs out sets the frame's error flag,
