@@ -310,6 +310,8 @@ Engine::~Engine() {
     release();
     if (copy_stream_) cudaStreamDestroy(copy_stream_);
     if (post_stream_) cudaStreamDestroy(post_stream_);
+    if (sweep_stream_) cudaStreamDestroy(sweep_stream_);
+    if (ev_fork_) cudaEventDestroy(ev_fork_);
     for (auto& ev : band_ev_) if (ev) cudaEventDestroy(ev);
     if (side_stream_) cudaStreamDestroy(side_stream_);
     if (ev_maps_) cudaEventDestroy(ev_maps_);
@@ -488,22 +490,8 @@ int Engine::process_host(const uint8_t* left, const uint8_t* right, int w, int h
     uint8_t* preason = outputs_pinned ? reason : reinterpret_cast<uint8_t*>(pconf + n);
     uint8_t* prel = outputs_pinned ? reliable : preason + n;
     const size_t row = (size_t)w * ch;
-    if (!copy_stream_) {
-        if (cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking) != cudaSuccess ||
-            cudaEventCreateWithFlags(&ev_maps_, cudaEventDisableTiming) != cudaSuccess ||
-            cudaEventCreateWithFlags(&ev_copied_, cudaEventDisableTiming) != cudaSuccess) {
-            cudaGetLastError();
-            return fail(kInternalError, "copy stream creation failed");
-        }
-    }
-    if (!post_stream_) {
-        bool ok = cudaStreamCreateWithFlags(&post_stream_, cudaStreamNonBlocking) == cudaSuccess;
-        for (auto& ev : band_ev_) ok = ok && cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) == cudaSuccess;
-        if (!ok) {
-            cudaGetLastError();
-            return fail(kInternalError, "post stream creation failed");
-        }
-    }
+    rc = ensure_streams();
+    if (rc) return rc;
     cudaError_t e;
     if (inputs_pinned) {
         e = cudaMemcpy2DAsync(ptr<uint8_t>(lay_.in_left), row, left, stride, row, h, cudaMemcpyHostToDevice, stream_);
@@ -532,13 +520,14 @@ int Engine::process_host(const uint8_t* left, const uint8_t* right, int w, int h
     if (rc == kOk) {
         const int nb = host_band_count();
         banded = nb > 1;
-        rc = banded ? run_banded(nb, pdisp, pconf, preason, prel) : run_sgm();
+        rc = banded ? run_banded(nb, pdisp, pconf, preason, prel, true) : run_sgm();
         if (rc == kOk && !banded) rc = run_post(nullptr, nullptr, nullptr, nullptr);
     }
     early_conf_ = nullptr;
     early_rel_ = nullptr;
     early_reason_ = nullptr;
     if (rc) {
+        cudaStreamSynchronize(sweep_stream_);
         cudaStreamSynchronize(post_stream_);
         cudaStreamSynchronize(copy_stream_);
         return rc;
@@ -592,7 +581,53 @@ int Engine::process_device(const uint8_t* dl, const uint8_t* dr, int w, int h, i
     int rc = prepare(w, h, ch);
     if (rc) return rc;
     counts_fresh_ = false;
+    // one launch of the last sweep by default: with its post-processing in row bands beside it
+    // (the host path's form) the post kernels took SM slots from the sweep's bands, and
+    // device-only frames were slower (Fast 1280x720 D128 0.733 -> 0.790 ms, Balanced 1.090 ->
+    // 1.170 ms); tuning device_bands asks for it
+    if (device_bands_ > 1 && !debug_) {
+        rc = ensure_streams();
+        if (rc) return rc;
+        nprof_ = 0;
+        rc = run_pre(dl, stride, dr, stride, ch);
+        if (rc) return rc;
+        const int nb = host_band_count(true);
+        if (nb > 1) {
+            rc = run_banded(nb, d_disp, d_conf, d_reason, d_reliable, false);
+            if (rc == kOk) {
+                const cudaError_t e = cudaStreamWaitEvent(stream_, ev_copied_, 0);
+                if (e != cudaSuccess) return cuda_fail(e, "join");
+            }
+            return rc;
+        }
+        rc = run_sgm();
+        return rc == kOk ? run_post(d_disp, d_conf, d_reason, d_reliable) : rc;
+    }
     return run(dl, stride, dr, stride, ch, d_disp, d_conf, d_reason, d_reliable);
+}
+
+int Engine::ensure_streams() {
+    if (!copy_stream_) {
+        if (cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&ev_maps_, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&ev_copied_, cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(kInternalError, "copy stream creation failed");
+        }
+    }
+    if (!post_stream_) {
+        int least = 0, greatest = 0;
+        bool ok = cudaDeviceGetStreamPriorityRange(&least, &greatest) == cudaSuccess;
+        ok = ok && cudaStreamCreateWithPriority(&sweep_stream_, cudaStreamNonBlocking, greatest) == cudaSuccess;
+        ok = ok && cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming) == cudaSuccess;
+        ok = ok && cudaStreamCreateWithFlags(&post_stream_, cudaStreamNonBlocking) == cudaSuccess;
+        for (auto& ev : band_ev_) ok = ok && cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) == cudaSuccess;
+        if (!ok) {
+            cudaGetLastError();
+            return fail(kInternalError, "post stream creation failed");
+        }
+    }
+    return kOk;
 }
 
 int Engine::sync() {
@@ -1015,9 +1050,10 @@ int Engine::run_post(float* d_disp, float* d_conf, uint8_t* d_reason, uint8_t* d
 // its own), then on copy_stream_ the device-to-host copies of every map row that is final.  The
 // copies of all but the top band overlap the sweep.  Same kernels, same maps as run_sgm +
 // run_post; frame counters over the whole map at the end.
-int Engine::host_band_count() const {
+int Engine::host_band_count(bool device) const {
     const Layout& L = lay_;
-    if (host_bands_ == 1 || debug_ || !post_stream_ || !copy_stream_) return 0;
+    const int req = device ? device_bands_ : host_bands_;
+    if (req == 1 || (device && req == 0) || debug_ || !post_stream_ || !copy_stream_) return 0;
     if (refine_enabled() || L.nsbuf != 3 || L.h < 256 || cfg_.median_radius > 1) return 0;
     if (scope_.sp_telem || scope_.ip_telem) return 0;
     const int gap = (scope_.ip_method == 0 && scope_.ip_gap == 32) ? cfg_.max_fill_gap : scope_.ip_gap;
@@ -1028,14 +1064,15 @@ int Engine::host_band_count() const {
     if (!sgm_last_band_supported(pl, 3)) return 0;
     // the chains' state between bands lives in the refiner's map, unused without the refiner
     if ((size_t)32 * (L.Dp / 64 + 1) * 4 > (size_t)L.h * 4) return 0;
-    return host_bands_ > 1 ? std::min(host_bands_, (int)kMaxBands) : (int)kBands;
+    return req > 1 ? std::min(req, (int)kMaxBands) : (int)kBands;
 }
 
-int Engine::run_banded(int nb, float* hdisp, float* hconf, uint8_t* hreason, uint8_t* hrel) {
+int Engine::run_banded(int nb, float* hdisp, float* hconf, uint8_t* hreason, uint8_t* hrel, bool to_host) {
+    const cudaMemcpyKind kind = to_host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
     const Layout& L = lay_;
     const int w = L.w, h = L.h;
     const size_t n = (size_t)w * h;
-    cudaStream_t s = stream_, ps = post_stream_, cs = copy_stream_;
+    cudaStream_t s = stream_, ps = post_stream_, cs = copy_stream_, ss = sweep_stream_;
     unsigned launches = 0;
     cudaError_t e = cudaSuccess;
     const bool prof = false;
@@ -1044,6 +1081,8 @@ int Engine::run_banded(int nb, float* hdisp, float* hconf, uint8_t* hreason, uin
     uint32_t* sb[7];
     sgm_launch(&pl, sb);
     RUN(launch_sgm_first(pl, 3, first4, sb, s), "sgm_first");
+    RUNC(cudaEventRecord(ev_fork_, s), "event");
+    RUNC(cudaStreamWaitEvent(ss, ev_fork_, 0), "event");
     // the confidence stage reads the right-image disparity
     if (rwta_forked_) RUNC(cudaStreamWaitEvent(ps, ev_[11], 0), "join");
     ConfLrArgs ca;
@@ -1074,8 +1113,8 @@ int Engine::run_banded(int nb, float* hdisp, float* hconf, uint8_t* hreason, uin
     int band = 0;
     for (int t0 = 0; t0 < h; t0 += bs, ++band) {
         const int t1 = std::min(h, t0 + bs);
-        RUN(launch_sgm_last_band(pl, 0, -1, 3, sb, t0, t1, carry, s), "sgm_last_band");
-        RUNC(cudaEventRecord(band_ev_[2 * band], s), "event");
+        RUN(launch_sgm_last_band(pl, 0, -1, 3, sb, t0, t1, carry, ss), "sgm_last_band");
+        RUNC(cudaEventRecord(band_ev_[2 * band], ss), "event");
         RUNC(cudaStreamWaitEvent(ps, band_ev_[2 * band], 0), "event");
         const int ylo = h - t1, yhi = h - t0;
         const bool top = ylo == 0;
@@ -1098,17 +1137,17 @@ int Engine::run_banded(int nb, float* hdisp, float* hconf, uint8_t* hreason, uin
         if (med && mlo < fin_hi) RUN(launch_median3_rows(w, h, mlo, fin_hi, med_in, ptr<float>(L.disp_out), ps), "median");
         RUNC(cudaEventRecord(band_ev_[2 * band + 1], ps), "event");
         RUNC(cudaStreamWaitEvent(cs, band_ev_[2 * band + 1], 0), "event");
-        if (hconf) RUNC(cudaMemcpyAsync(hconf + o, ptr<float>(L.confidence) + o, rows * 4, cudaMemcpyDeviceToHost, cs), "conf out");
-        if (hrel) RUNC(cudaMemcpyAsync(hrel + o, ptr<uint8_t>(L.reliable) + o, rows, cudaMemcpyDeviceToHost, cs), "rel out");
-        if (hreason) RUNC(cudaMemcpyAsync(hreason + o, ptr<uint8_t>(L.reason) + o, rows, cudaMemcpyDeviceToHost, cs), "reason out");
+        if (hconf) RUNC(cudaMemcpyAsync(hconf + o, ptr<float>(L.confidence) + o, rows * 4, kind, cs), "conf out");
+        if (hrel) RUNC(cudaMemcpyAsync(hrel + o, ptr<uint8_t>(L.reliable) + o, rows, kind, cs), "rel out");
+        if (hreason) RUNC(cudaMemcpyAsync(hreason + o, ptr<uint8_t>(L.reason) + o, rows, kind, cs), "reason out");
         if (hdisp && mlo < fin_hi) {
             const size_t fo = (size_t)mlo * w;
-            RUNC(cudaMemcpyAsync(hdisp + fo, final_map + fo, (size_t)(fin_hi - mlo) * w * 4, cudaMemcpyDeviceToHost, cs),
-                 "disp out");
+            RUNC(cudaMemcpyAsync(hdisp + fo, final_map + fo, (size_t)(fin_hi - mlo) * w * 4, kind, cs), "disp out");
         }
         fin_hi = mlo;
     }
-    cudaEventRecord(ev_[6], s);
+    RUNC(cudaEventRecord(ev_[6], ss), "event");
+    RUNC(cudaStreamWaitEvent(s, ev_[6], 0), "event");
     cudaEventRecord(ev_[7], ps);
     cudaEventRecord(ev_[8], ps);
     // PipelineStats counters over the whole map (src/pipeline.cpp:650-707)
@@ -1122,7 +1161,7 @@ int Engine::run_banded(int nb, float* hdisp, float* hconf, uint8_t* hreason, uin
     if (prior_runs()) RUNC(cudaMemcpyAsync(st + 5, arena_ + L.pr_count, 4, cudaMemcpyDeviceToDevice, ps), "support count");
     cudaEventRecord(ev_[9], ps);
     RUNC(cudaStreamWaitEvent(cs, ev_[9], 0), "event");
-    RUNC(cudaMemcpyAsync(counts_, st, sizeof(counts_), cudaMemcpyDeviceToHost, cs), "counters out");
+    if (to_host) RUNC(cudaMemcpyAsync(counts_, st, sizeof(counts_), cudaMemcpyDeviceToHost, cs), "counters out");
     RUNC(cudaEventRecord(ev_copied_, cs), "event");
     have_times_ = true;
     count_launches(launches);
@@ -1429,6 +1468,11 @@ int set_tuning(Engine* e, const char* key, int value) {
     if (std::strcmp(key, "host_bands") == 0) {
         if (value < 0 || value > Engine::kMaxBands) return kInvalidConfig;
         if (e) e->set_host_bands(value);
+        return kOk;
+    }
+    if (std::strcmp(key, "device_bands") == 0) {
+        if (value < 0 || value > Engine::kMaxBands) return kInvalidConfig;
+        if (e) e->set_device_bands(value);
         return kOk;
     }
     if (std::strcmp(key, "refine_window") == 0) {

@@ -169,9 +169,11 @@ public:
     // right-image window (0: where it fits, 1: never, the L1 form)
     void set_refine_spin_limit(int n) { refine_.spin_limit = n; }
     void set_refine_window(int mode) { refine_.window = mode; }
-    // host-output frames: the last sweep in this many row bands, each band's rows post-processed
-    // and copied out while the next band runs (0: kBands where the path allows it, 1: never)
+    // the last sweep in this many row bands, each band's rows post-processed and copied to the
+    // outputs while the next band runs (0: kBands where the path allows it, 1: never)
     void set_host_bands(int n) { host_bands_ = n; }
+    // device-output frames (process_device) in that many bands: 0 = never (default)
+    void set_device_bands(int n) { device_bands_ = n; }
     static constexpr int kBands = 6;
     static constexpr int kMaxBands = 16;
     // takes the calling thread's experimental scopes now (run_pre does so for every frame; the
@@ -205,10 +207,12 @@ private:
     int run_pre(const uint8_t* dl, int lstride, const uint8_t* dr, int rstride, int ch);
     int run_sgm();
     int run_post(float* d_disp, float* d_conf, uint8_t* d_reason, uint8_t* d_reliable);
-    // run_sgm + run_post for host outputs with the last sweep in row bands (host_band_count() > 1):
-    // every map row goes to the host pointers on copy_stream_ as soon as it is final
-    int host_band_count() const;
-    int run_banded(int nb, float* hdisp, float* hconf, uint8_t* hreason, uint8_t* hrel);
+    // run_sgm + run_post with the last sweep in row bands (host_band_count() > 1): every map row
+    // goes to the output pointers (host, or device when !to_host) on copy_stream_ as soon as it is
+    // final; ev_copied_ follows the last copy
+    int host_band_count(bool device = false) const;
+    int run_banded(int nb, float* odisp, float* oconf, uint8_t* oreason, uint8_t* orel, bool to_host);
+    int ensure_streams();  // copy_stream_, post_stream_ and their events, created on first use
     int run_prior();
     int run_hier();
     // per-pixel ranges: from the prior or from the hierarchical pass (every other frame has the
@@ -235,6 +239,7 @@ private:
     int cost_tile_ = 0;
     int cost_kernel_ = 0;  // 0: pixel-run cost kernel where it applies, 1: column-tile kernel
     int host_bands_ = 0;   // see set_host_bands
+    int device_bands_ = 0;  // see set_device_bands
     RefineTuning refine_;
     cudaStream_t stream_ = nullptr;
     bool own_stream_ = false;
@@ -278,6 +283,10 @@ private:
     cudaEvent_t ev_maps_ = nullptr, ev_copied_ = nullptr;
     // banded host path: the post-processing stream and the per-band events (sweep done, rows done)
     cudaStream_t post_stream_ = nullptr;
+    // the sweep's bands run on a stream of the highest priority, so that the block scheduler
+    // places their blocks before those of the post-processing kernels beside them
+    cudaStream_t sweep_stream_ = nullptr;
+    cudaEvent_t ev_fork_ = nullptr;
     cudaEvent_t band_ev_[2 * kMaxBands] = {};
     float* early_conf_ = nullptr;
     uint8_t* early_reason_ = nullptr;

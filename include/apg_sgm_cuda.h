@@ -79,7 +79,12 @@ APGCU_API int apgcu_engine_set_debug(apgcu_engine_t e, int flags);
  *                 rows are post-processed and copied to the host while the next band runs:
  *                 0 = 6 bands where the path allows it (default; Path4, 128..256 padded
  *                 disparities, one warp per chain, no refiner, 3x3 or no median, no telemetry
- *                 scope, at least 256 rows), 1 = never (one sweep, then the copies).
+ *                 scope, at least 256 rows), 1 = never (one sweep, then the copies);
+ *   "device_bands": the same for apgcu_engine_process_device (the copies go to the caller's
+ *                 device buffers): 0 = never (default), 2..16 = that many bands.  The post kernels
+ *                 then run beside the sweep's bands; measured on one B200 that was slower at
+ *                 1280x720 (0.735 -> 0.786 ms Fast) and faster at 1920x1080 D256 Fast (2.570 ->
+ *                 2.400 ms with 6 bands).
  * And one key that bounds a wait rather than tuning speed:
  *   "refine_spin_limit": polls (each ~128 ns) before a refiner band stops waiting for the band above
  *                 (0 = default, about a second).  A wait that runs out sets the frame's error flag,

@@ -1,13 +1,15 @@
-"""Host-output frames with the last SGM sweep in row bands (tuning host_bands).
+"""Frames with the last SGM sweep in row bands (tuning host_bands).
 
-apgcu_engine_process and apg_session_process run the last (bottom-up) sweep as several launches
-over bands of rows, carrying each chain's path values between them, and post-process and copy
-out each band's finished rows while the next band sweeps.  Every case here runs the same pair
-with the banded path (default 6 bands, and 2 and 16) and with one sweep (host_bands=1), and
-compares the four maps bit for bit (a session test also the PipelineStats counters); two cases are
-also compared with the oracle.  The shapes cover each padded range the banded sweep takes (128, 192, 256; the byte
-volume at 256), heights that are not a multiple of the 32-step bands, the stages between the
-sweep and the maps switched off one at a time, hierarchical ranges and an experimental scope.
+apgcu_engine_process, apgcu_engine_process_device and apg_session_process run the last
+(bottom-up) sweep as several launches over bands of rows, carrying each chain's path values
+between them, and post-process and copy out each band's finished rows while the next band sweeps.
+Every case here runs the same pair with the banded path (default 6 bands, and 2, 3 and 16) and
+with one sweep (host_bands=1), and compares the four maps bit for bit (a session test also the
+PipelineStats counters); two cases are also compared with the oracle.  The shapes cover each
+padded range the banded sweep takes (128, 192, 256; the byte volume at 256), heights that are
+not a multiple of the 32-step bands, the stages between the sweep and the maps switched off one at
+a time, hierarchical ranges, an experimental scope and the device-output entry point (tuning
+device_bands there).
 """
 import numpy as np
 import pytest
@@ -103,3 +105,43 @@ def test_banded_under_experimental_scope(apg):
             outs.append(_run(apg, cfg, L, R, bands))
     for k in MAPS:
         assert same_bits(outs[0][k], outs[1][k]), k
+
+
+def _run_device(apg, cfg, L, R, bands, frames=2):
+    """apgcu_engine_process_device with torch device buffers; `frames` calls in a row into the same
+    outputs (the second frame's copies must not race the first's)."""
+    import torch
+    h, w = L.shape[:2]
+    e = apg.Engine(cfg)
+    e.set_tuning("device_bands", bands)
+    dl, dr = torch.from_numpy(L).cuda(), torch.from_numpy(R).cuda()
+    outs = {"disparity": torch.full((h, w), 7.0, dtype=torch.float32, device="cuda"),
+            "confidence": torch.full((h, w), 7.0, dtype=torch.float32, device="cuda"),
+            "invalid_reason": torch.full((h, w), 9, dtype=torch.uint8, device="cuda"),
+            "reliable_mask": torch.full((h, w), 9, dtype=torch.uint8, device="cuda")}
+    torch.cuda.synchronize()
+    for _ in range(frames):
+        e.process_device(dl.data_ptr(), dr.data_ptr(), w, h, w, 1, outs["disparity"].data_ptr(),
+                         outs["confidence"].data_ptr(), outs["invalid_reason"].data_ptr(),
+                         outs["reliable_mask"].data_ptr())
+    e.sync()
+    e.close()
+    return {k: v.cpu().numpy() for k, v in outs.items()}
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", [CASES[0], CASES[1], CASES[3], CASES[4]], ids=lambda c: c[0])
+def test_banded_device_path_changes_no_result(apg, case):
+    """The device-output entry point (apgcu_engine_process_device) with the banded sweep (tuning
+    device_bands; one sweep by default): maps in the caller's device buffers equal the one-sweep
+    form's and the host path's."""
+    _, mode, w, h, dmax, over = case
+    over = dict(over)
+    dmin = over.pop("min_disparity", 0)
+    L, R = synth(w, h, dmax, cells=8, lo=max(dmin, 0), hi=dmax - 8, seed=76)
+    cfg = apg.config_from_mode(mode, dmax, dmin, **over)
+    want = _run(apg, cfg, L, R, 1)
+    for bands in (0, 3, 6):
+        got = _run_device(apg, cfg, L, R, bands)
+        for k in MAPS:
+            assert same_bits(got[k], want[k]), f"host_bands={bands} {k}: {diff_report(got[k], want[k])}"
