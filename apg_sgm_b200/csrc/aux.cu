@@ -120,4 +120,11 @@ cudaError_t launch_aux(const AuxImage& left, const AuxImage& right, int ch, int 
     return cudaGetLastError();
 }
 
+cudaError_t launch_aux_one(const AuxImage& im, int ch, int w, int h, int census64, cudaStream_t s) {
+    dim3 grid((w + TX - 1) / TX, (h + TY - 1) / TY, 1), block(TX, BY);
+    if (census64) aux_kernel<true><<<grid, block, 0, s>>>(im, im, ch, w, h);
+    else aux_kernel<false><<<grid, block, 0, s>>>(im, im, ch, w, h);
+    return cudaGetLastError();
+}
+
 }  // namespace apgcu

@@ -312,6 +312,7 @@ Engine::~Engine() {
     if (post_stream_) cudaStreamDestroy(post_stream_);
     if (sweep_stream_) cudaStreamDestroy(sweep_stream_);
     if (ev_fork_) cudaEventDestroy(ev_fork_);
+    if (ev_right_) cudaEventDestroy(ev_right_);
     for (auto& ev : band_ev_) if (ev) cudaEventDestroy(ev);
     if (side_stream_) cudaStreamDestroy(side_stream_);
     if (ev_maps_) cudaEventDestroy(ev_maps_);
@@ -495,9 +496,14 @@ int Engine::process_host(const uint8_t* left, const uint8_t* right, int w, int h
     cudaError_t e;
     if (inputs_pinned) {
         e = cudaMemcpy2DAsync(ptr<uint8_t>(lay_.in_left), row, left, stride, row, h, cudaMemcpyHostToDevice, stream_);
+        // the right image on the copy stream, beside the left image's aux kernel (the previous
+        // frame's work on every stream ended before this call)
         if (e == cudaSuccess)
             e = cudaMemcpy2DAsync(ptr<uint8_t>(lay_.in_right), row, right, stride, row, h, cudaMemcpyHostToDevice,
-                                  stream_);
+                                  copy_stream_);
+        if (e == cudaSuccess) e = cudaEventRecord(ev_right_, copy_stream_);
+        right_on_copy_ = e == cudaSuccess && !(debug_ & 8);
+        if (e == cudaSuccess && (debug_ & 8)) e = cudaStreamWaitEvent(stream_, ev_right_, 0);
     } else {
         // the left image goes up while the right one is staged
         for (int y = 0; y < h; ++y) std::memcpy(pl + y * row, left + (size_t)y * stride, row);
@@ -620,6 +626,7 @@ int Engine::ensure_streams() {
         bool ok = cudaDeviceGetStreamPriorityRange(&least, &greatest) == cudaSuccess;
         ok = ok && cudaStreamCreateWithPriority(&sweep_stream_, cudaStreamNonBlocking, greatest) == cudaSuccess;
         ok = ok && cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming) == cudaSuccess;
+        ok = ok && cudaEventCreateWithFlags(&ev_right_, cudaEventDisableTiming) == cudaSuccess;
         ok = ok && cudaStreamCreateWithFlags(&post_stream_, cudaStreamNonBlocking) == cudaSuccess;
         for (auto& ev : band_ev_) ok = ok && cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) == cudaSuccess;
         if (!ok) {
@@ -721,7 +728,14 @@ int Engine::run_pre(const uint8_t* dl, int lstride, const uint8_t* dr, int rstri
                           ptr<uint32_t>(L.cl), ptr<unsigned long long>(L.cl)};
         const AuxImage ri{dr, rstride, ptr<uint8_t>(L.rgray), ptr<uint8_t>(L.rgx), ptr<uint8_t>(L.rgy),
                           ptr<uint32_t>(L.cr), ptr<unsigned long long>(L.cr)};
-        RUN(launch_aux(li, ri, ch, w, h, c64, s), "aux");
+        if (right_on_copy_) {
+            right_on_copy_ = false;
+            RUN(launch_aux_one(li, ch, w, h, c64, s), "aux");
+            RUNC(cudaStreamWaitEvent(s, ev_right_, 0), "right image");
+            RUN(launch_aux_one(ri, ch, w, h, c64, s), "aux");
+        } else {
+            RUN(launch_aux(li, ri, ch, w, h, c64, s), "aux");
+        }
     }
     cudaEventRecord(ev_[1], s);
     // search ranges: the hierarchical pass (frames of 32 x 32 and more) writes every pixel's
@@ -1107,12 +1121,28 @@ int Engine::run_banded(int nb, float* hdisp, float* hconf, uint8_t* hreason, uin
     const float* med_in = fill ? fill_map : lr_map;
     const float* final_map = med ? ptr<float>(L.disp_out) : med_in;
     const int dfinal = (fill ? 1 : 0) + (med ? 1 : 0);  // rows a final row needs below the LR rows
-    const int bs = round_up((h + nb - 1) / nb, 32);     // steps per band (the WTA's 32-step blocks)
+    // band boundaries in steps from the bottom row, multiples of the WTA's 32-step blocks: sizes
+    // shrink by about 0.7 a band (a row's copies take about 0.7 of its sweep time or less, so each
+    // band's copies end while the next band sweeps), and the top band, whose post-processing and
+    // copies follow the sweep, is small
+    int tb[kMaxBands + 1];
+    int nband = 0;
+    {
+        double wsum = 0.0, wk = 1.0;
+        for (int k = 0; k < nb; ++k, wk *= 0.7) wsum += wk;
+        double acc = 0.0;
+        wk = 1.0;
+        tb[0] = 0;
+        for (int k = 0; k < nb; ++k, wk *= 0.7) {
+            acc += wk;
+            const int t = k == nb - 1 ? h : std::min(h, round_up((int)(h * acc / wsum + 0.5), 32));
+            if (t > tb[nband]) tb[++nband] = t;
+        }
+    }
     uint32_t* carry = ptr<uint32_t>(L.disp_ref);
     int fill_hi = h, fin_hi = h;  // rows [fill_hi, h) of the fill map, [fin_hi, h) of the final map are done
-    int band = 0;
-    for (int t0 = 0; t0 < h; t0 += bs, ++band) {
-        const int t1 = std::min(h, t0 + bs);
+    for (int band = 0; band < nband; ++band) {
+        const int t0 = tb[band], t1 = tb[band + 1];
         RUN(launch_sgm_last_band(pl, 0, -1, 3, sb, t0, t1, carry, ss), "sgm_last_band");
         RUNC(cudaEventRecord(band_ev_[2 * band], ss), "event");
         RUNC(cudaStreamWaitEvent(ps, band_ev_[2 * band], 0), "event");

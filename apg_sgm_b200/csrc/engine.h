@@ -287,6 +287,10 @@ private:
     // places their blocks before those of the post-processing kernels beside them
     cudaStream_t sweep_stream_ = nullptr;
     cudaEvent_t ev_fork_ = nullptr;
+    // host path with page-locked inputs: the right image goes up on copy_stream_ (ev_right_ after
+    // it) while the left image's aux kernel runs; run_pre then waits for it before the right's
+    cudaEvent_t ev_right_ = nullptr;
+    bool right_on_copy_ = false;
     cudaEvent_t band_ev_[2 * kMaxBands] = {};
     float* early_conf_ = nullptr;
     uint8_t* early_reason_ = nullptr;

@@ -23,6 +23,8 @@ struct AuxImage {
 };
 cudaError_t launch_aux(const AuxImage& left, const AuxImage& right, int ch, int w, int h, int census64,
                        cudaStream_t s);
+// One image (the host path runs the left image's while the right one is still being uploaded).
+cudaError_t launch_aux_one(const AuxImage& im, int ch, int w, int h, int census64, cudaStream_t s);
 
 // cost.cu: mode 0 raw volume, 1 cross-H volume, 2 right argmin only; all update rkey.
 // Pixel-run form of the cost kernel (32-bit census, default ranges); launch_cost uses it where

@@ -1588,6 +1588,9 @@ cudaError_t launch_last_band_k(const SgmArgs& a, DirTable tab, cudaStream_t st) 
 
 }  // namespace
 
+// Not at 64 padded disparities, where the last sweep runs on two warps per chain: bands of the
+// one-warp kernel there were slower on the host path (Balanced 640x480 D64 e2e 37.6 -> 36.8 G
+// voxels/s) than the two-warp sweep followed by its copies.
 bool sgm_last_band_supported(const SgmLaunch& l, int nin) {
     if (nin != 3 || !l.cvol || l.store_final || l.sp_tel) return false;
     if (l.Dp != 128 && l.Dp != 192 && l.Dp != 256) return false;
